@@ -1,0 +1,190 @@
+/*
+ * pip_gpu.h -- C ABI of the B200 (sm_100a) two-fluid finite-volume step of PIP.
+ *
+ * The Fortran driver of PIP calls a fixed set of module procedures per time step
+ * (main.f90:31-68): cfl, run_solver, and through run_solver set_flux, source_PIP and
+ * PIPbnd.  Each entry point below replaces one of those calls.  All arrays crossing this
+ * boundary are the Fortran arrays themselves: FP64, column-major U(ix,jx,kx,nvar) with
+ * ghost cells included (Globalvar.f90:17), passed by address (c_loc / assumed size).
+ * The host keeps ownership of its arrays; the context owns the device copies.
+ *
+ * Errors: every int-returning call returns PIP_OK (0) or one of pip_status_code.  No call
+ * stops the process (the Fortran code's `stop` becomes a status code), mirroring the
+ * flag_stop convention of stop_sim (IO_rot.f90:625-674).
+ *
+ * Threading: one context per MPI rank and per device; calls on one context are not
+ * re-entrant.  Calls are synchronous with respect to the host buffers they take.
+ */
+#ifndef PIP_GPU_H
+#define PIP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIP_ABI_VERSION 1
+
+enum pip_status_code {
+  PIP_OK = 0,
+  PIP_ERR_PARAM = 1,   /* parameter block unsupported or inconsistent (get_parameters checks) */
+  PIP_ERR_CUDA = 2,    /* a CUDA runtime call failed; pip_last_cuda_error() has the code */
+  PIP_ERR_NAN = 3,     /* NaN in the state (stop_sim, IO_rot.f90:641-668) */
+  PIP_ERR_DT = 4,      /* dt <= 1e-12 (stop_sim, IO_rot.f90:636-640) */
+  PIP_ERR_ITER = 5,    /* an iterative solver or bounded device loop hit its limit */
+  PIP_ERR_STATE = 6,   /* call out of order, e.g. a step before any upload */
+  PIP_ERR_NOMEM = 7,   /* device allocation failed */
+  PIP_ERR_NULL = 8     /* a required pointer argument was NULL */
+};
+
+enum pip_precision {
+  PIP_FP64 = 0,        /* plain FP64 path: the drop-in, parity-checked against the oracle */
+  PIP_MIXED = 1        /* FP32 fluxes/state, FP64 coupling source and compensated RK sums */
+};
+
+/* Ionisation/recombination laws accepted in pip_params.flag_ir. */
+enum pip_ir_law {
+  PIP_IR_NONE = 0,
+  /* Gm_ion = ir_ion_coef*T^-1/2*exp(-ir_chi/T), Gm_rec = ir_rec_coef*T^-1/2 with
+   * T = gm*p_i/(2 rho_i) (get_Te_MHD, Scheme_rot.f90:104-110); the rates are frozen at
+   * the start of each step as set_IR is (main.f90:32-34).  This law is new: none of
+   * set_IR's types 1-4 (PIP_rot.f90:134-310) has it. */
+  PIP_IR_POWERLAW = 5
+};
+
+/*
+ * Parameter block: mirrors the globalvar module (Globalvar.f90) after get_parameters
+ * (Model_rot.f90:39-333) and set_coordinate (Model_rot.f90:394-458) have run.
+ * Supported subset (anything else returns PIP_ERR_PARAM):
+ *   flag_eqs=PIP (two-fluid), flag_sch=0, flag_hll=2, s_order=2, t_order=2, flag_time=0,
+ *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col=1 (constant col),
+ *   flag_pip_imp 0/1, flag_ir 0 or PIP_IR_POWERLAW with flag_ir_type 1 or 2,
+ *   flag_bnd in {1,2,3,4,5,6,7,10,11}, no resistivity/viscosity/gravity/ambipolar.
+ */
+typedef struct pip_params {
+  int32_t abi_version;     /* must equal PIP_ABI_VERSION */
+  int32_t ndim;            /* 1 or 2 */
+  int32_t ix, jx, kx;      /* cells per axis including ghosts: ix = ix0 + 2*margin(1) */
+  int32_t margin[3];       /* ghost layers per axis (Model_rot.f90:282-289,319-330) */
+  int32_t nvar_h;          /* neutral (hydro) variables: 5 */
+  int32_t nvar_m;          /* ion (MHD) variables: 8, or 9 with the Dedner psi */
+  int32_t flag_sch;        /* 0: HLL branch */
+  int32_t flag_hll;        /* 2: HLLD ions, HLLC neutrals */
+  int32_t s_order;         /* 2: minmod MUSCL */
+  int32_t t_order;         /* 2: midpoint RK2 */
+  int32_t flag_time;       /* 0: standard RK (Solver_rot.f90:203-220) */
+  int32_t flag_divb;       /* 1: Dedner 9-wave cleaning */
+  int32_t flag_col;        /* 1: alpha_c = col everywhere (set_collisional col_type 0) */
+  int32_t flag_pip_imp;    /* 0: explicit collision source; 1: exponential form */
+  int32_t flag_ir;         /* pip_ir_law */
+  int32_t flag_ir_type;    /* IR energy exchange: 1 Khomenko, 2 Singh (PIP_rot.f90:1399-1411) */
+  int32_t flag_heat;       /* 0 or 1 (implicit anisotropic conduction of the ions) */
+  int32_t hc_max;          /* BiCGstab iteration limit */
+  int32_t flag_bnd[6];     /* x_l, x_r, y_l, y_r, z_l, z_r boundary codes */
+  int32_t precision;       /* pip_precision */
+  int32_t fp_exact;        /* 1: FP64 kernels built without FMA contraction (bitwise
+                              comparable with an FMA-free CPU build); 0: contracted */
+  int32_t reserved_i[6];
+  double gm;               /* ratio of specific heats: gm_d/gm_n */
+  double safety;           /* CFL number */
+  double ro_lim, pr_lim;   /* density and pressure floors */
+  double col;              /* collision coefficient alpha_c */
+  double db_clean;         /* Dedner psi damping ratio */
+  double pip_imp_factor;   /* dt bound factor of the exponential collision form */
+  double t_ir;             /* unused by PIP_IR_POWERLAW; kept for set_IR parity */
+  double ir_chi;           /* ionisation potential in code temperature units */
+  double ir_ion_coef;      /* ionisation rate coefficient */
+  double ir_rec_coef;      /* recombination rate coefficient */
+  double kapper;           /* Spitzer coefficient: kappa_par = kapper*T^2.5 */
+  double hc_error;         /* BiCGstab relative residual target */
+  double reserved_d[7];
+  const double *dx;        /* ix cell widths (dsc(:,1)) */
+  const double *dy;        /* jx cell widths (dsc(:,2)); 1D: one entry, the reference sets 100 */
+  const double *dz;        /* kx cell widths (dsc(:,3)); one entry, the reference sets 100 */
+} pip_params;
+
+typedef struct pip_ctx pip_ctx;
+
+/* Replaces the tail of prologue (Initial_rot.f90:140-160): validates the parameters,
+ * allocates the device state and builds the boundary tables (initialize_bnd,
+ * Boundary_rot.f90:20-32, set_sym_mhd/hd :239-320). */
+int pip_ctx_create(const pip_params *p, pip_ctx **out);
+
+/* Replaces epilogue's release of the state (IO_rot.f90 epilogue). */
+void pip_ctx_destroy(pip_ctx *ctx);
+
+/* Host -> device copy of U_h(ix,jx,kx,nvar_h) and U_m(ix,jx,kx,nvar_m) (FP64, with ghosts).
+ * Called after the initial condition is set (Initial_rot.f90:46-140) or after restart
+ * (IO_rot.f90:405-459). */
+int pip_upload(pip_ctx *ctx, const double *U_h, const double *U_m);
+
+/* Device -> host copy of the current state including its ghost cells (every stage and
+ * pip_fill_ghosts keep them filled); feeds output() (IO_rot.f90:39-105), whose HDF5
+ * layout stays with the Fortran host. */
+int pip_download(pip_ctx *ctx, double *U_h, double *U_m);
+
+/* cfl(U_h,U_m,dt) (Scheme_rot.f90:183-213): floors and rewrites the state through
+ * primitives (cq2pv_mhd/hd, :132-179), returns the CFL time step (cfl_mhd :245-289,
+ * cfl_hd :215-243, cfl_pn_col :305-313) and the Dedner speed
+ * cmax = safety*min(dx,dy,dz)/dt (:203-211).  The cmax kept for the next pip_step is the
+ * value computed with this dt, as the Fortran global cmax is. Either pointer may be NULL. */
+int pip_cfl(pip_ctx *ctx, double *dt, double *cmax);
+
+/* run_solver(U_h,U_m) (Solver_rot.f90:42-81): t_order RK stages of fluxes (HLLD/HLLC),
+ * collisional source, conservative update and ghost fill with the given dt. */
+int pip_step(pip_ctx *ctx, double dt);
+
+/* The time loop of main.f90:31-68 on the device: repeats {cfl; run_solver; cfl;
+ * time += dt; stop_sim} until nsteps steps are done (nsteps <= 0: no step limit) or
+ * time >= t_end (t_end <= 0: no time limit).  The per-step dt and the stop checks stay on
+ * the device.  Returns the status of stop_sim (PIP_ERR_NAN / PIP_ERR_DT) if it fired.
+ * time_out and steps_done (either may be NULL) receive the simulation time and the number
+ * of steps taken. */
+int pip_run(pip_ctx *ctx, int64_t nsteps, double t_end, double *time_out, int64_t *steps_done);
+
+/* Simulation time kept by the context (Globalvar `time`); pip_run advances it. */
+int pip_set_time(pip_ctx *ctx, double time);
+int pip_get_time(pip_ctx *ctx, double *time);
+
+/* set_flux (Solver_rot.f90:124-159) for one direction dir (1..ndim) of the current state:
+ * F_h(ix,jx,kx,nvar_h) and F_m(ix,jx,kx,nvar_m) hold the flux through the face between
+ * cells i and i+1 (x) or j and j+1 (y) at index i (j), as in the Fortran F arrays.
+ * Faces adjacent to interior cells are computed; the other entries are set to zero.
+ * Uses the cmax of the last pip_cfl for the Dedner components. */
+int pip_flux(pip_ctx *ctx, int dir, double *F_h, double *F_m);
+
+/* source_PIP (PIP_rot.f90:1309-1429) on the current state with collision sub-step dt_coll.
+ * Like the Fortran routine it rewrites the state through primitives (cq2pv).  With
+ * flag_pip_imp=0 it returns S_h, S_m (the rates added by add_source); with
+ * flag_pip_imp=1 it returns the increments the exponential form adds to U0
+ * (-dt_coll*dS for the neutrals, +dt_coll*dS for the ions). */
+int pip_source(pip_ctx *ctx, double dt_coll, double *S_h, double *S_m);
+
+/* PIPbnd(U_h,U_m,0) (Boundary_rot.f90:34-52) on the device state; with one rank the
+ * MPI halo exchange (MPI_rot.f90:128-339) reduces to this ghost fill. */
+int pip_fill_ghosts(pip_ctx *ctx);
+
+/* stop_sim's flags for the device state (IO_rot.f90:625-674): *nan_flag = 1 if any
+ * variable of either species is NaN or Inf; *stop_flag = 1 if the NaN flag is set or
+ * the last dt was <= 1e-12.  Either pointer may be NULL. */
+int pip_status(pip_ctx *ctx, int *stop_flag, int *nan_flag);
+
+/* Implicit anisotropic conduction of the ion species over dt: HC(U_m,nvar_m,1)
+ * (HC_rot.f90:67-140) with the 9-point matrix (set_matrix_source_MHD2D9, :643-739) and
+ * BiCGstab (:187-299).  Returns PIP_ERR_ITER if hc_max iterations did not reach
+ * hc_error.  iters and relres (either may be NULL) receive the iteration count and the
+ * final relative residual. */
+int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
+
+/* Last CUDA error code seen by any context (cudaError_t as int), 0 if none. */
+int pip_last_cuda_error(void);
+
+/* Text for a pip_status_code. */
+const char *pip_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIP_GPU_H */

@@ -1,0 +1,180 @@
+"""ctypes wrapper of the FP64 CPU restatement (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` as the checker
+and by bench.py's CPU-baseline leg.  The product package never imports it.
+
+Parity status: unpinned by the reference's own tests (the reference ships none and cannot
+be built here); see pip_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Tuple
+
+import numpy as np
+
+from pip_b200.params import PipParams, Settings
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile."""
+    src = os.path.join(_HERE, "pip_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.POINTER
+        d = ctypes.c_double
+        dp = P(d)
+        vp = ctypes.c_void_p
+        L.orc_create.argtypes = [P(PipParams), P(ctypes.c_int)]
+        L.orc_create.restype = vp
+        L.orc_destroy.argtypes = [vp]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_get_threads.restype = ctypes.c_int
+        L.orc_set_state.argtypes = [vp, dp, dp]
+        L.orc_get_state.argtypes = [vp, dp, dp]
+        L.orc_set_time.argtypes = [vp, d]
+        L.orc_get_time.argtypes = [vp]
+        L.orc_get_time.restype = d
+        L.orc_get_cmax.argtypes = [vp]
+        L.orc_get_cmax.restype = d
+        L.orc_set_cmax.argtypes = [vp, d]
+        L.orc_cfl.argtypes = [vp, dp, dp]
+        L.orc_run_solver.argtypes = [vp, d]
+        L.orc_flux.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.orc_source.argtypes = [vp, d, dp, dp]
+        L.orc_bnd.argtypes = [vp]
+        L.orc_run.argtypes = [vp, ctypes.c_long, d, dp, P(ctypes.c_long), dp, ctypes.c_long]
+        L.orc_run.restype = ctypes.c_int
+        L.orc_has_nan.argtypes = [vp]
+        L.orc_has_nan.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+class Oracle:
+    """One simulation on the CPU restatement; mirrors the C ABI's call set."""
+
+    def __init__(self, s: Settings, U_h: np.ndarray, U_m: np.ndarray):
+        self.s = s
+        self.params, self._keep = s.to_params()
+        st = ctypes.c_int(0)
+        self.h = lib().orc_create(ctypes.byref(self.params), ctypes.byref(st))
+        if not self.h:
+            raise ValueError("oracle rejected the parameters (status %d)" % st.value)
+        self.shape_h = U_h.shape
+        self.shape_m = U_m.shape
+        self.set_state(U_h, U_m)
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, U_h, U_m):
+        U_h = np.ascontiguousarray(U_h, dtype=np.float64)
+        U_m = np.ascontiguousarray(U_m, dtype=np.float64)
+        lib().orc_set_state(self.h, _ptr(U_h), _ptr(U_m))
+
+    def state(self) -> Tuple[np.ndarray, np.ndarray]:
+        U_h = np.empty(self.shape_h)
+        U_m = np.empty(self.shape_m)
+        lib().orc_get_state(self.h, _ptr(U_h), _ptr(U_m))
+        return U_h, U_m
+
+    @property
+    def time(self) -> float:
+        return lib().orc_get_time(self.h)
+
+    @time.setter
+    def time(self, t: float):
+        lib().orc_set_time(self.h, float(t))
+
+    @property
+    def cmax(self) -> float:
+        return lib().orc_get_cmax(self.h)
+
+    @cmax.setter
+    def cmax(self, v: float):
+        lib().orc_set_cmax(self.h, float(v))
+
+    def cfl(self) -> Tuple[float, float]:
+        dt = ctypes.c_double()
+        cm = ctypes.c_double()
+        lib().orc_cfl(self.h, ctypes.byref(dt), ctypes.byref(cm))
+        return dt.value, cm.value
+
+    def run_solver(self, dt: float) -> None:
+        lib().orc_run_solver(self.h, float(dt))
+
+    def flux(self, direction: int):
+        F_h = np.zeros(self.shape_h)
+        F_m = np.zeros(self.shape_m)
+        lib().orc_flux(self.h, int(direction), _ptr(F_h), _ptr(F_m))
+        return F_h, F_m
+
+    def source(self, dt_coll: float):
+        S_h = np.zeros(self.shape_h)
+        S_m = np.zeros(self.shape_m)
+        lib().orc_source(self.h, float(dt_coll), _ptr(S_h), _ptr(S_m))
+        return S_h, S_m
+
+    def fill_ghosts(self) -> None:
+        lib().orc_bnd(self.h)
+
+    def prologue(self) -> None:
+        """The prologue's cfl and ghost fill (Initial_rot.f90:152-160)."""
+        dt, cm = self.cfl()
+        self.cmax = cm
+        self.fill_ghosts()
+
+    def run(self, nsteps: int = 0, t_end: float = 0.0, max_hist: int = 0):
+        t = ctypes.c_double()
+        n = ctypes.c_long()
+        hist = np.zeros(max(max_hist, 1))
+        status = lib().orc_run(self.h, int(nsteps), float(t_end), ctypes.byref(t), ctypes.byref(n),
+                               _ptr(hist), int(max_hist))
+        return status, t.value, n.value, hist[: min(n.value, max_hist)]
+
+    def has_nan(self) -> bool:
+        return bool(lib().orc_has_nan(self.h))
+
+
+def run_case(s: Settings, U_h, U_m, nsteps: int = 0, t_end: Optional[float] = None,
+             threads: int = 1, max_hist: int = 0):
+    """prologue + time loop; returns (status, time, steps, U_h, U_m, dt_hist)."""
+    set_threads(threads)
+    o = Oracle(s, U_h, U_m)
+    o.prologue()
+    status, t, n, hist = o.run(nsteps, t_end if t_end is not None else 0.0, max_hist)
+    Uh, Um = o.state()
+    o.close()
+    return status, t, n, Uh, Um, hist

@@ -1,0 +1,948 @@
+/*
+ * pip_oracle.c -- TEST INFRASTRUCTURE ONLY (see pip_oracle.h).
+ *
+ * FP64 CPU restatement of the PIP two-fluid step.  Each routine names the Fortran it
+ * restates.  Arrays use the Fortran layout U(ix,jx,kx,nvar), column-major, 0-based here:
+ * element (i,j,k,n) sits at i + ix*(j + jx*(k + kx*n)).  Whole-array passes with
+ * temporaries, as the Fortran does; expressions keep the Fortran evaluation order
+ * (left-to-right, parentheses as written) and the file is compiled without FMA
+ * contraction, so results match an -O2 x86-64 gfortran build up to libm differences.
+ */
+#include "pip_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define TINY 1.0e-20                 /* Globalvar.f90:101 */
+#define HLLC_EPSI 1.0e-10            /* HLL_rot.f90:12 */
+#define HLLC_ACC 1.03                /* HLL_rot.f90:12 */
+#define HLLG_FACTOR 1.001            /* HLL_rot.f90:702 */
+#define MU_P 0.5                     /* initialize_collisional, PIP_rot.f90:35 */
+#define MU_N 1.0                     /* PIP_rot.f90:36 */
+
+struct orc_ctx {
+  pip_params p;
+  int ix, jx, kx, nh, nm;
+  size_t nc;                         /* cells */
+  double *dx, *dy, *dz;
+  double *U_h, *U_m;
+  double *gm_ion, *gm_rec;           /* IR rates (PIP_IR_POWERLAW) */
+  int sym_m[6][9], sym_h[6][5];      /* set_sym_mhd / set_sym_hd */
+  double cmax, time, last_dt;
+};
+
+static int g_threads = 1;
+
+void orc_set_threads(int n) {
+  g_threads = n > 0 ? n : 1;
+#ifdef _OPENMP
+  omp_set_num_threads(g_threads);
+#endif
+}
+int orc_get_threads(void) { return g_threads; }
+
+static inline double fmx(double a, double b) { return a > b ? a : b; }
+static inline double fmn(double a, double b) { return a < b ? a : b; }
+static inline double sgn1(double b) { return copysign(1.0, b); }  /* sign(1.0d0,b) */
+
+#define AT(c, i, j, k) ((size_t)(i) + (size_t)(c)->ix * ((size_t)(j) + (size_t)(c)->jx * (size_t)(k)))
+
+/* ---------------------------------------------------------------- boundary tables */
+
+/* set_sym_mhd, Boundary_rot.f90:239-294 (dir is 1-based, face index f 0-based). */
+static void set_sym_mhd(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  for (int f = 0; f < 6; ++f)
+    for (int n = 0; n < 9; ++n) c->sym_m[f][n] = 1;
+  for (int f = 0; f < 2 * p->ndim; ++f) {
+    int dir = f / 2 + 1, b = p->flag_bnd[f];
+    /* Fortran indices below are 1-based variable numbers; subtract 1. */
+    if (b == 2) {
+      c->sym_m[f][1 + dir - 1] = -1;
+      c->sym_m[f][5 + dir - 1] = -1;
+    } else if (b == 3) {
+      c->sym_m[f][1 + dir - 1] = -1;
+      c->sym_m[f][6 + dir % 3 - 1] = -1;
+      c->sym_m[f][2 + (dir + 1) % 3 - 1] = -1;
+    } else if (b == 4) {
+      c->sym_m[f][1 + dir - 1] = -1;
+      c->sym_m[f][6 + (dir + 1) % 3 - 1] = -1;
+      c->sym_m[f][2 + dir % 3 - 1] = -1;
+    } else if (b == 5) {
+      c->sym_m[f][1 + dir - 1] = -1;
+      c->sym_m[f][5 + dir - 1] = -1;
+      c->sym_m[f][2 + (dir + 1) % 3 - 1] = -1;
+      c->sym_m[f][6 + (dir + 1) % 3 - 1] = -1;
+    } else if (b == 6) {
+      c->sym_m[f][1 + dir - 1] = -1;
+      c->sym_m[f][6 + dir % 3 - 1] = -1;
+      c->sym_m[f][6 + (dir + 1) % 3 - 1] = -1;
+    } else if (b == 7) {
+      c->sym_m[f][1] = -1;
+      c->sym_m[f][2] = -1;
+      c->sym_m[f][3] = -1;
+    }
+  }
+  if (p->flag_divb == 1) {
+    for (int f = 0; f < 2 * p->ndim; ++f) {
+      int b = p->flag_bnd[f];
+      if (b == 2 || b == 20 || b == 5) c->sym_m[f][8] = 1;
+      else if (b == 3 || b == 4 || b == 6 || b == 7) c->sym_m[f][8] = -1;
+    }
+  }
+}
+
+/* set_sym_hd, Boundary_rot.f90:296-320. */
+static void set_sym_hd(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  for (int f = 0; f < 6; ++f)
+    for (int n = 0; n < 5; ++n) c->sym_h[f][n] = 1;
+  for (int f = 0; f < 2 * p->ndim; ++f) {
+    int dir = f / 2 + 1, b = p->flag_bnd[f];
+    if (b == 2 || b == 20) {
+      c->sym_h[f][1 + dir - 1] = -1;
+    } else if (b == 3) {
+      c->sym_h[f][1 + dir - 1] = -1;
+      c->sym_h[f][2 + (dir + 1) % 3 - 1] = -1;
+    } else if (b == 4) {
+      c->sym_h[f][1 + dir - 1] = -1;
+      c->sym_h[f][2 + dir % 3 - 1] = -1;
+    } else if (b == 5) {
+      c->sym_h[f][1 + dir - 1] = -1;
+      c->sym_h[f][2 + (dir + 1) % 3 - 1] = -1;
+    } else if (b == 6) {
+      c->sym_h[f][1 + dir - 1] = -1;
+    }
+  }
+}
+
+/* boundary_control, Boundary_rot.f90:323-402, for one face and one species. */
+static void boundary_control(orc_ctx *c, double *U, int nvar, int dir, int upper, const int *sym,
+                             int type) {
+  int ig[3] = {c->ix, c->jx, c->kx};
+  int sl[3], el[3], dl[3], sr[3], er[3], dr[3];
+  const int *margin = c->p.margin;
+  for (int a = 0; a < 3; ++a) {
+    if (dir == a + 1) {
+      if (!upper) {
+        sl[a] = 1; el[a] = margin[a]; dl[a] = 1;
+        if (type == 1) { sr[a] = ig[a] - 2 * margin[a] + 1; er[a] = ig[a] - margin[a]; dr[a] = 1; }
+        else if (type == 2) { sr[a] = 2 * margin[a]; er[a] = margin[a] + 1; dr[a] = -1; }
+        else { sr[a] = margin[a] + 1; er[a] = margin[a] + 1; dr[a] = 1; }
+      } else {
+        sl[a] = ig[a] - margin[a] + 1; el[a] = ig[a]; dl[a] = 1;
+        if (type == 1) { sr[a] = margin[a] + 1; er[a] = 2 * margin[a]; dr[a] = 1; }
+        else if (type == 2) { sr[a] = ig[a] - margin[a]; er[a] = ig[a] - margin[a] * 2 + 1; dr[a] = -1; }
+        else { sr[a] = ig[a] - margin[a]; er[a] = ig[a] - margin[a]; dr[a] = 1; }
+      }
+    } else {
+      sl[a] = 1; el[a] = ig[a]; dl[a] = 1;
+      sr[a] = 1; er[a] = ig[a]; dr[a] = 1;
+    }
+  }
+  int same = 1;
+  for (int a = 0; a < 3; ++a)
+    if (el[a] - sl[a] != abs(er[a] - sr[a])) same = 0;
+  size_t nc = c->nc;
+  if (same) {
+    for (int n = 0; n < nvar; ++n) {
+      double s = (double)sym[n];
+      for (int k = 0; k <= el[2] - sl[2]; ++k)
+        for (int j = 0; j <= el[1] - sl[1]; ++j)
+          for (int i = 0; i <= el[0] - sl[0]; ++i) {
+            int li = sl[0] + i * dl[0] - 1, lj = sl[1] + j * dl[1] - 1, lk = sl[2] + k * dl[2] - 1;
+            int ri = sr[0] + i * dr[0] - 1, rj = sr[1] + j * dr[1] - 1, rk = sr[2] + k * dr[2] - 1;
+            U[AT(c, li, lj, lk) + n * nc] = s * U[AT(c, ri, rj, rk) + n * nc];
+          }
+    }
+  } else if (type == 10) {
+    /* free boundary: every ghost layer copies the first interior layer (no sign flip) */
+    int m = margin[dir - 1], src = sr[dir - 1] - 1;
+    for (int n = 0; n < nvar; ++n)
+      for (int q = 0; q < m; ++q) {
+        int dst = sl[dir - 1] - 1 + q;
+        if (dir == 1) {
+          for (int k = 0; k < c->kx; ++k)
+            for (int j = 0; j < c->jx; ++j)
+              U[AT(c, dst, j, k) + n * nc] = U[AT(c, src, j, k) + n * nc];
+        } else if (dir == 2) {
+          for (int k = 0; k < c->kx; ++k)
+            for (int i = 0; i < c->ix; ++i)
+              U[AT(c, i, dst, k) + n * nc] = U[AT(c, i, src, k) + n * nc];
+        } else {
+          for (int j = 0; j < c->jx; ++j)
+            for (int i = 0; i < c->ix; ++i)
+              U[AT(c, i, j, dst) + n * nc] = U[AT(c, i, j, src) + n * nc];
+        }
+      }
+  }
+}
+
+/* Type mapping of MHDbnd/HDbnd, Boundary_rot.f90:54-125. */
+static int bnd_type(int code) {
+  if (code == 3 || code == 4 || code == 5 || code == 6 || code == 7 || code == 11) return 2;
+  return code;
+}
+
+/* PIPbnd, Boundary_rot.f90:34-52 (one rank: mpi_bnd exchanges nothing). */
+void orc_bnd(orc_ctx *c) {
+  for (int f = 0; f < 2 * c->p.ndim; ++f)
+    boundary_control(c, c->U_m, c->nm, f / 2 + 1, f % 2, c->sym_m[f], bnd_type(c->p.flag_bnd[f]));
+  for (int f = 0; f < 2 * c->p.ndim; ++f)
+    boundary_control(c, c->U_h, c->nh, f / 2 + 1, f % 2, c->sym_h[f], bnd_type(c->p.flag_bnd[f]));
+}
+
+/* ---------------------------------------------------------------- conversions */
+
+/* u2v_hd, HLL_rot.f90:1136-1156. */
+static void u2v_hd(const orc_ctx *c, const double *U, double *V) {
+  const double gm = c->p.gm, ro_lim = c->p.ro_lim, pr_lim = c->p.pr_lim;
+  size_t nc = c->nc;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double ro = fmx(U[q], ro_lim);
+    double roi = 1.0 / ro;
+    double m1 = U[q + nc], m2 = U[q + 2 * nc], m3 = U[q + 3 * nc];
+    V[q] = ro;
+    V[q + nc] = m1 * roi;
+    V[q + 2 * nc] = m2 * roi;
+    V[q + 3 * nc] = m3 * roi;
+    double pr = (gm - 1.0) * (U[q + 4 * nc] - 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) * roi);
+    if (pr < pr_lim) pr = pr_lim;
+    V[q + 4 * nc] = pr;
+  }
+}
+
+/* u2v_mhd, HLL_rot.f90:1159-1186. */
+static void u2v_mhd(const orc_ctx *c, const double *U, double *V) {
+  const double gm = c->p.gm, ro_lim = c->p.ro_lim, pr_lim = c->p.pr_lim;
+  size_t nc = c->nc;
+  int divb = c->p.flag_divb == 1;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double ro = fmx(U[q], ro_lim);
+    double roi = 1.0 / ro;
+    double m1 = U[q + nc], m2 = U[q + 2 * nc], m3 = U[q + 3 * nc];
+    double b1 = U[q + 5 * nc], b2 = U[q + 6 * nc], b3 = U[q + 7 * nc];
+    V[q] = ro;
+    V[q + nc] = m1 * roi;
+    V[q + 2 * nc] = m2 * roi;
+    V[q + 3 * nc] = m3 * roi;
+    double pr = (gm - 1.0) * (U[q + 4 * nc] - 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) * roi -
+                              0.5 * (b1 * b1 + b2 * b2 + b3 * b3));
+    if (pr < pr_lim) pr = pr_lim;
+    V[q + 4 * nc] = pr;
+    V[q + 5 * nc] = b1;
+    V[q + 6 * nc] = b2;
+    V[q + 7 * nc] = b3;
+    if (divb) V[q + 8 * nc] = U[q + 8 * nc];
+  }
+}
+
+/* v2u_1, HLL_rot.f90:1189-1215. */
+static void v2u_1(const double *v, double *u, int mhd, int divb, double gm) {
+  u[0] = v[0];
+  u[1] = v[0] * v[1];
+  u[2] = v[0] * v[2];
+  u[3] = v[0] * v[3];
+  if (!mhd) {
+    u[4] = v[4] / (gm - 1.0) + 0.5 * v[0] * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
+  } else {
+    u[5] = v[5];
+    u[6] = v[6];
+    u[7] = v[7];
+    u[4] = v[4] / (gm - 1.0) + 0.5 * v[0] * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) +
+           0.5 * (v[5] * v[5] + v[6] * v[6] + v[7] * v[7]);
+    if (divb) u[8] = v[8];
+  }
+}
+
+/* cq2pv_hd, Scheme_rot.f90:132-150 (rewrites U; returns the primitive arrays). */
+static void cq2pv_hd(const orc_ctx *c, double *U, double *de, double *vx, double *vy, double *vz,
+                     double *pr) {
+  const double gm = c->p.gm, ro_lim = c->p.ro_lim, pr_lim = c->p.pr_lim;
+  size_t nc = c->nc;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double d = U[q];
+    double ux = U[q + nc] / d, uy = U[q + 2 * nc] / d, uz = U[q + 3 * nc] / d;
+    double p = (gm - 1.0) * (U[q + 4 * nc] - 0.5 * d * (ux * ux + uy * uy + uz * uz));
+    p = fmx(p, pr_lim);
+    d = fmx(d, ro_lim);
+    U[q] = d;
+    U[q + nc] = ux * d;
+    U[q + 2 * nc] = uy * d;
+    U[q + 3 * nc] = uz * d;
+    U[q + 4 * nc] = p / (gm - 1.0) + 0.5 * d * (ux * ux + uy * uy + uz * uz);
+    de[q] = d; vx[q] = ux; vy[q] = uy; vz[q] = uz; pr[q] = p;
+  }
+}
+
+/* cq2pv_mhd, Scheme_rot.f90:153-179. */
+static void cq2pv_mhd(const orc_ctx *c, double *U, double *de, double *vx, double *vy, double *vz,
+                      double *pr, double *bx, double *by, double *bz) {
+  const double gm = c->p.gm, ro_lim = c->p.ro_lim, pr_lim = c->p.pr_lim;
+  size_t nc = c->nc;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double d = U[q];
+    double ux = U[q + nc] / d, uy = U[q + 2 * nc] / d, uz = U[q + 3 * nc] / d;
+    double b1 = U[q + 5 * nc], b2 = U[q + 6 * nc], b3 = U[q + 7 * nc];
+    double p = (gm - 1.0) * (U[q + 4 * nc] - 0.5 * d * (ux * ux + uy * uy + uz * uz) -
+                             0.5 * (b1 * b1 + b2 * b2 + b3 * b3));
+    p = fmx(p, pr_lim);
+    d = fmx(d, ro_lim);
+    U[q] = d;
+    U[q + nc] = ux * d;
+    U[q + 2 * nc] = uy * d;
+    U[q + 3 * nc] = uz * d;
+    U[q + 4 * nc] = p / (gm - 1.0) + 0.5 * d * (ux * ux + uy * uy + uz * uz) +
+                    0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+    de[q] = d; vx[q] = ux; vy[q] = uy; vz[q] = uz; pr[q] = p;
+    if (bx) { bx[q] = b1; by[q] = b2; bz[q] = b3; }
+  }
+}
+
+/* ---------------------------------------------------------------- reconstruction */
+
+/* get_Side (HLL_rot.f90:15-63) with minmod_func (Util_rot.f90:59-76), s_order=2. */
+static void get_side(const orc_ctx *c, const double *V, double *VL, double *VR, int dir, int nvar) {
+  int ix = c->ix, jx = c->jx, kx = c->kx;
+  size_t nc = c->nc;
+  memset(VL, 0, sizeof(double) * nc * nvar);
+  memset(VR, 0, sizeof(double) * nc * nvar);
+  int len = dir == 1 ? ix : (dir == 2 ? jx : kx);
+  size_t stride = dir == 1 ? 1 : (dir == 2 ? (size_t)ix : (size_t)ix * jx);
+#pragma omp parallel for schedule(static)
+  for (int n = 0; n < nvar; ++n) {
+    for (int k = 0; k < (dir == 3 ? 1 : kx); ++k)
+      for (int j = 0; j < (dir == 2 ? 1 : jx); ++j)
+        for (int i = 0; i < (dir == 1 ? 1 : ix); ++i) {
+          size_t base = AT(c, i, j, k) + n * nc;
+          for (int s = 1; s <= len - 2; ++s) {
+            double v0 = V[base + (s - 1) * stride], v1 = V[base + s * stride],
+                   v2 = V[base + (s + 1) * stride];
+            double X = v2 - v1, Y = v1 - v0;
+            double SX = sgn1(X);
+            double du = SX * fmx(0.0, fmn(fabs(X), SX * Y));
+            VL[base + s * stride] = v1 + 0.5 * du;
+            VR[base + (s - 1) * stride] = v1 - 0.5 * du;
+          }
+        }
+  }
+  for (size_t q = 0; q < nc; ++q) {
+    VL[q] = fmx(VL[q], c->p.ro_lim);
+    VR[q] = fmx(VR[q], c->p.ro_lim);
+  }
+}
+
+/* ---------------------------------------------------------------- Riemann solvers */
+
+/* hllc_flux, HLL_rot.f90:615-687. */
+static void hllc_flux(const double *v_l, const double *v_r, double *flx, double gm) {
+  double u_l[5], u_r[5], flx_l[5], flx_r[5], st_l[5], st_r[5];
+  v2u_1(v_l, u_l, 0, 0, gm);
+  v2u_1(v_r, u_r, 0, 0, gm);
+  double pr_l = v_l[4], pr_r = v_r[4];
+  flx_l[0] = u_l[1];
+  flx_r[0] = u_r[1];
+  flx_l[1] = pr_l + u_l[1] * u_l[1] / u_l[0];
+  flx_r[1] = pr_r + u_r[1] * u_r[1] / u_r[0];
+  flx_l[2] = u_l[1] * u_l[2] / u_l[0];
+  flx_r[2] = u_r[1] * u_r[2] / u_r[0];
+  flx_l[3] = u_l[1] * u_l[3] / u_l[0];
+  flx_r[3] = u_r[1] * u_r[3] / u_r[0];
+  flx_l[4] = u_l[1] * (u_l[4] + pr_l) / u_l[0];
+  flx_r[4] = u_r[1] * (u_r[4] + pr_r) / u_r[0];
+  double cs_l = sqrt(gm * pr_l / u_l[0]);
+  double cs_r = sqrt(gm * pr_r / u_r[0]);
+  double vn_l = u_l[1] / u_l[0];
+  double vn_r = u_r[1] / u_r[0];
+  double sl = HLLC_ACC * fmn(vn_l - cs_l, vn_r - cs_r);
+  double sr = HLLC_ACC * fmx(vn_l + cs_l, vn_r + cs_r);
+  double sm = (u_r[1] * (sr - vn_r) - u_l[1] * (sl - vn_l) + pr_l - pr_r) /
+              (u_r[0] * (sr - vn_r) - u_l[0] * (sl - vn_l));
+  double pr_m = sm * u_l[0] * (sl - vn_l) - u_l[1] * (sl - vn_l) + pr_l;
+  st_l[0] = u_l[0] * (sl - vn_l) / (sl - sm);
+  st_r[0] = u_r[0] * (sr - vn_r) / (sr - sm);
+  st_l[1] = st_l[0] * sm;
+  st_r[1] = st_r[0] * sm;
+  st_l[2] = st_l[0] * u_l[2] / u_l[0];
+  st_r[2] = st_r[0] * u_r[2] / u_r[0];
+  st_l[3] = st_l[0] * u_l[3] / u_l[0];
+  st_r[3] = st_r[0] * u_r[3] / u_r[0];
+  st_l[4] = ((sl - vn_l) * u_l[4] - pr_l * vn_l + pr_m * sm) / (sl - sm);
+  st_r[4] = ((sr - vn_r) * u_r[4] - pr_r * vn_r + pr_m * sm) / (sr - sm);
+  double thl = (fabs(sl) + sl) / fmx(2.0 * sl, HLLC_EPSI);
+  double thm = (fabs(sm) + sm) / fmx(2.0 * sm, HLLC_EPSI);
+  double thr = 1.0 - (fabs(sr) + sr) / fmx(2.0 * sr, HLLC_EPSI);
+  for (int n = 0; n < 5; ++n)
+    flx[n] = thr * flx_r[n] + thl * flx_l[n] +
+             (1.0 - thl - thr) * (thm * (flx_l[n] + sl * (st_l[n] - u_l[n])) +
+                                  (1.0 - thm) * (flx_r[n] + sr * (st_r[n] - u_r[n])));
+}
+
+/* hlld_flux, HLL_rot.f90:691-910 (Miyoshi-Kusano HLLD with HLLC-G fallback). */
+static void hlld_flux(const double *v_l, const double *v_r, double *flx, int nvar, double gm,
+                      int divb, double cmax) {
+  double u_l[9], u_r[9], flx_l[9], flx_r[9], u_hll[9], u_l1[9], u_r1[9], u2[9];
+  for (int n = 0; n < 9; ++n) { flx[n] = 0.0; flx_l[n] = 0.0; flx_r[n] = 0.0; }
+  (void)nvar;
+  v2u_1(v_l, u_l, 1, divb, gm);
+  v2u_1(v_r, u_r, 1, divb, gm);
+
+  double b2_l = (v_l[5] * v_l[5] + v_l[6] * v_l[6] + v_l[7] * v_l[7]);
+  double pt_l = v_l[4] + 0.5 * b2_l;
+  double vbL = v_l[1] * v_l[5] + v_l[2] * v_l[6] + v_l[3] * v_l[7];
+  flx_l[0] = v_l[0] * v_l[1];
+  flx_l[1] = v_l[0] * (v_l[1] * v_l[1]) + v_l[4] + 0.5 * b2_l - v_l[5] * v_l[5];
+  flx_l[2] = v_l[0] * v_l[1] * v_l[2] - v_l[5] * v_l[6];
+  flx_l[3] = v_l[0] * v_l[1] * v_l[3] - v_l[5] * v_l[7];
+  flx_l[4] = (u_l[4] + pt_l) * v_l[1] - vbL * v_l[5];
+  flx_l[5] = 0.0;
+  flx_l[6] = v_l[1] * v_l[6] - v_l[5] * v_l[2];
+  flx_l[7] = v_l[1] * v_l[7] - v_l[5] * v_l[3];
+
+  double b2_r = (v_r[5] * v_r[5] + v_r[6] * v_r[6] + v_r[7] * v_r[7]);
+  double pt_r = v_r[4] + 0.5 * b2_r;
+  double vbR = v_r[1] * v_r[5] + v_r[2] * v_r[6] + v_r[3] * v_r[7];
+  flx_r[0] = v_r[0] * v_r[1];
+  flx_r[1] = v_r[0] * (v_r[1] * v_r[1]) + v_r[4] + 0.5 * b2_r - v_r[5] * v_r[5];
+  flx_r[2] = v_r[0] * v_r[1] * v_r[2] - v_r[5] * v_r[6];
+  flx_r[3] = v_r[0] * v_r[1] * v_r[3] - v_r[5] * v_r[7];
+  flx_r[4] = (u_r[4] + pt_r) * v_r[1] - vbR * v_r[5];
+  flx_r[5] = 0.0;
+  flx_r[6] = v_r[1] * v_r[6] - v_r[5] * v_r[2];
+  flx_r[7] = v_r[1] * v_r[7] - v_r[5] * v_r[3];
+
+  /* fast mode wave speed */
+  double f1 = gm * v_l[4];
+  double f2 = 4.0 * f1 * (v_l[5] * v_l[5]);
+  double vf_l = sqrt(((f1 + b2_l) + sqrt(fmx((f1 + b2_l) * (f1 + b2_l) - f2, 0.0))) / (2.0 * v_l[0]));
+  f1 = gm * v_r[4];
+  f2 = 4.0 * f1 * (v_r[5] * v_r[5]);
+  double vf_r = sqrt(((f1 + b2_r) + sqrt(fmx((f1 + b2_r) * (f1 + b2_r) - f2, 0.0))) / (2.0 * v_r[0]));
+
+  double sl = fmn(v_l[1], v_r[1]) - fmx(vf_l, vf_r);
+  double sr = fmx(v_l[1], v_r[1]) + fmx(vf_l, vf_r);
+
+  if (sl >= 0.0) {
+    for (int n = 0; n < 8; ++n) flx[n] = flx_l[n];
+  } else if (sr <= 0.0) {
+    for (int n = 0; n < 8; ++n) flx[n] = flx_r[n];
+  } else {
+    f1 = 1.0 / (sr - sl);
+    for (int n = 0; n < 8; ++n) u_hll[n] = f1 * (sr * u_r[n] - sl * u_l[n] - flx_r[n] + flx_l[n]);
+    double sm = u_hll[1] / u_hll[0];
+    double pt = pt_l + v_l[0] * (sl - v_l[1]) * (sm - v_l[1]);
+    double ro_l1 = v_l[0] * (sl - v_l[1]) / (sl - sm);
+    double ro_r1 = v_r[0] * (sr - v_r[1]) / (sr - sm);
+    double sal = fabs(u_hll[5]) / sqrt(ro_l1);
+    double sar = fabs(u_hll[5]) / sqrt(ro_r1);
+
+    if ((sl >= (sm - HLLG_FACTOR * sal)) || ((sm + HLLG_FACTOR * sar) >= sr)) {
+      /* revert to HLLC-G */
+      double vy_2 = u_hll[2] / u_hll[0];
+      double vz_2 = u_hll[3] / u_hll[0];
+      if (sm >= 0.0) {
+        u2[4] = ((sl - v_l[1]) * u_l[4] - pt_l * v_l[1] + pt * sm +
+                 u_hll[5] * (vbL - sm * u_hll[5] - vy_2 * u_hll[6] - vz_2 * u_hll[7])) /
+                (sl - sm);
+        u2[1] = ro_l1 * sm;
+        u2[2] = ro_l1 * vy_2;
+        u2[3] = ro_l1 * vz_2;
+        flx[0] = sl * (ro_l1 - v_l[0]) + flx_l[0];
+        for (int n = 1; n < 5; ++n) flx[n] = sl * (u2[n] - u_l[n]) + flx_l[n];
+        for (int n = 5; n < 8; ++n) flx[n] = sl * (u_hll[n] - v_l[n]) + flx_l[n];
+      } else {
+        u2[4] = ((sr - v_r[1]) * u_r[4] - pt_r * v_r[1] + pt * sm +
+                 u_hll[5] * (vbR - sm * u_hll[5] - vy_2 * u_hll[6] - vz_2 * u_hll[7])) /
+                (sr - sm);
+        u2[1] = ro_r1 * sm;
+        u2[2] = ro_r1 * vy_2;
+        u2[3] = ro_r1 * vz_2;
+        flx[0] = sr * (ro_r1 - v_r[0]) + flx_r[0];
+        for (int n = 1; n < 5; ++n) flx[n] = sr * (u2[n] - u_r[n]) + flx_r[n];
+        for (int n = 5; n < 8; ++n) flx[n] = sr * (u_hll[n] - v_r[n]) + flx_r[n];
+      }
+    } else {
+      /* intermediate state (L*) */
+      f1 = 1.0 / (v_l[0] * (sl - v_l[1]) * (sl - sm) - u_hll[5] * u_hll[5]);
+      u_l1[5] = u_hll[5];
+      u_l1[6] = v_l[6] * f1 * (v_l[0] * ((sl - v_l[1]) * (sl - v_l[1])) - u_hll[5] * u_hll[5]);
+      u_l1[7] = v_l[7] * f1 * (v_l[0] * ((sl - v_l[1]) * (sl - v_l[1])) - u_hll[5] * u_hll[5]);
+      double vy_l1 = v_l[2] - f1 * u_hll[5] * v_l[6] * (sm - v_l[1]);
+      double vz_l1 = v_l[3] - f1 * u_hll[5] * v_l[7] * (sm - v_l[1]);
+      u_l1[0] = ro_l1;
+      u_l1[4] = ((sl - v_l[1]) * u_l[4] - pt_l * v_l[1] + pt * sm +
+                 u_hll[5] * (vbL - sm * u_hll[5] - vy_l1 * u_l1[6] - vz_l1 * u_l1[7])) /
+                (sl - sm);
+      u_l1[1] = ro_l1 * sm;
+      u_l1[2] = ro_l1 * vy_l1;
+      u_l1[3] = ro_l1 * vz_l1;
+
+      /* intermediate state (R*) */
+      f1 = 1.0 / (v_r[0] * (sr - v_r[1]) * (sr - sm) - u_hll[5] * u_hll[5]);
+      u_r1[5] = u_hll[5];
+      u_r1[6] = v_r[6] * f1 * (v_r[0] * ((sr - v_r[1]) * (sr - v_r[1])) - u_hll[5] * u_hll[5]);
+      u_r1[7] = v_r[7] * f1 * (v_r[0] * ((sr - v_r[1]) * (sr - v_r[1])) - u_hll[5] * u_hll[5]);
+      double vy_r1 = v_r[2] - f1 * u_hll[5] * v_r[6] * (sm - v_r[1]);
+      double vz_r1 = v_r[3] - f1 * u_hll[5] * v_r[7] * (sm - v_r[1]);
+      u_r1[0] = ro_r1;
+      u_r1[4] = ((sr - v_r[1]) * u_r[4] - pt_r * v_r[1] + pt * sm +
+                 u_hll[5] * (vbR - sm * u_hll[5] - vy_r1 * u_r1[6] - vz_r1 * u_r1[7])) /
+                (sr - sm);
+      u_r1[1] = ro_r1 * sm;
+      u_r1[2] = ro_r1 * vy_r1;
+      u_r1[3] = ro_r1 * vz_r1;
+
+      /* rotational discontinuities */
+      double sl1 = sm - sal;
+      double sr1 = sm + sar;
+      if (sl1 >= 0.0) {
+        flx[0] = sl * (u_l1[0] - v_l[0]) + flx_l[0];
+        for (int n = 1; n < 5; ++n) flx[n] = sl * (u_l1[n] - u_l[n]) + flx_l[n];
+        for (int n = 5; n < 8; ++n) flx[n] = sl * (u_l1[n] - v_l[n]) + flx_l[n];
+      } else if (sr1 <= 0.0) {
+        flx[0] = sr * (u_r1[0] - v_r[0]) + flx_r[0];
+        for (int n = 1; n < 5; ++n) flx[n] = sr * (u_r1[n] - u_r[n]) + flx_r[n];
+        for (int n = 5; n < 8; ++n) flx[n] = sr * (u_r1[n] - v_r[n]) + flx_r[n];
+      } else {
+        /* central states */
+        double ro_ls = sqrt(ro_l1);
+        double ro_rs = sqrt(ro_r1);
+        f1 = 1.0 / (ro_ls + ro_rs);
+        f2 = copysign(1.0, u_hll[5]);
+        double vy_2 = f1 * (ro_ls * vy_l1 + ro_rs * vy_r1 + (u_r1[6] - u_l1[6]) * f2);
+        double vz_2 = f1 * (ro_ls * vz_l1 + ro_rs * vz_r1 + (u_r1[7] - u_l1[7]) * f2);
+        u2[5] = u_hll[5];
+        u2[6] = f1 * (ro_ls * u_r1[6] + ro_rs * u_l1[6] + ro_ls * ro_rs * (vy_r1 - vy_l1) * f2);
+        u2[7] = f1 * (ro_ls * u_r1[7] + ro_rs * u_l1[7] + ro_ls * ro_rs * (vz_r1 - vz_l1) * f2);
+        if (sm >= 0.0) {
+          u2[0] = ro_l1;
+          u2[4] = u_l1[4] - ro_ls * (vy_l1 * u_l1[6] + vz_l1 * u_l1[7] - vy_2 * u2[6] - vz_2 * u2[7]) * f2;
+          u2[1] = ro_l1 * sm;
+          u2[2] = ro_l1 * vy_2;
+          u2[3] = ro_l1 * vz_2;
+          flx[0] = sl1 * u2[0] - (sl1 - sl) * u_l1[0] - sl * v_l[0] + flx_l[0];
+          for (int n = 1; n < 5; ++n) flx[n] = sl1 * u2[n] - (sl1 - sl) * u_l1[n] - sl * u_l[n] + flx_l[n];
+          for (int n = 5; n < 8; ++n) flx[n] = sl1 * u2[n] - (sl1 - sl) * u_l1[n] - sl * v_l[n] + flx_l[n];
+        } else {
+          u2[0] = ro_r1;
+          u2[4] = u_r1[4] + ro_rs * (vy_r1 * u_r1[6] + vz_r1 * u_r1[7] - vy_2 * u2[6] - vz_2 * u2[7]) * f2;
+          u2[1] = ro_r1 * sm;
+          u2[2] = ro_r1 * vy_2;
+          u2[3] = ro_r1 * vz_2;
+          flx[0] = sr1 * u2[0] - (sr1 - sr) * u_r1[0] - sr * v_r[0] + flx_r[0];
+          for (int n = 1; n < 5; ++n) flx[n] = sr1 * u2[n] - (sr1 - sr) * u_r1[n] - sr * u_r[n] + flx_r[n];
+          for (int n = 5; n < 8; ++n) flx[n] = sr1 * u2[n] - (sr1 - sr) * u_r1[n] - sr * v_r[n] + flx_r[n];
+        }
+      }
+    }
+  }
+  if (divb) {
+    double ch = cmax;
+    flx[5] = 0.5 * (u_l[8] + u_r[8] - ch * (v_r[5] - v_l[5]));
+    flx[8] = 0.5 * (ch * ch * (v_l[5] + v_r[5]) - ch * (v_r[8] - v_l[8]));
+  }
+}
+
+/* Component permutations of set_HLLC_fluxes / set_HLLD_fluxes (HLL_rot.f90:295-461):
+ * direction 2 swaps (vx,vy) and (bx,by); direction 3 swaps (vx,vz) and (bx,bz). */
+static const int PERM_H[3][5] = {{0, 1, 2, 3, 4}, {0, 2, 1, 3, 4}, {0, 3, 2, 1, 4}};
+static const int PERM_M[3][9] = {{0, 1, 2, 3, 4, 5, 6, 7, 8},
+                                 {0, 2, 1, 3, 4, 6, 5, 7, 8},
+                                 {0, 3, 2, 1, 4, 7, 6, 5, 8}};
+
+/* set_HLLC_fluxes / set_HLLD_fluxes for one direction: F(.., n) of the face between
+ * s and s+1 along dir, for s = 0..len-2 and every cell of the other axes. */
+static void set_fluxes(const orc_ctx *c, double *F, const double *VL, const double *VR, int dir,
+                       int mhd) {
+  int ix = c->ix, jx = c->jx, kx = c->kx;
+  size_t nc = c->nc;
+  int nvar = mhd ? c->nm : c->nh;
+  int ie = dir == 1 ? ix - 1 : ix, je = dir == 2 ? jx - 1 : jx, ke = dir == 3 ? kx - 1 : kx;
+  const int *perm = mhd ? PERM_M[dir - 1] : PERM_H[dir - 1];
+  int divb = c->p.flag_divb == 1;
+  double gm = c->p.gm, cmax = c->cmax;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < ke; ++k)
+    for (int j = 0; j < je; ++j)
+      for (int i = 0; i < ie; ++i) {
+        double vl[9], vr[9], fl[9];
+        size_t q = AT(c, i, j, k);
+        for (int n = 0; n < nvar; ++n) {
+          vl[n] = VL[q + perm[n] * nc];
+          vr[n] = VR[q + perm[n] * nc];
+        }
+        if (mhd) hlld_flux(vl, vr, fl, nvar, gm, divb, cmax);
+        else hllc_flux(vl, vr, fl, gm);
+        for (int n = 0; n < nvar; ++n) F[q + perm[n] * nc] = fl[n];
+      }
+}
+
+/* hlld_fluxes_ideal / hllc_fluxes_ideal for one direction (HLL_rot.f90:94-121). */
+static void flux_dir(orc_ctx *c, int dir, double *F_h, double *F_m) {
+  size_t nc = c->nc;
+  double *V = malloc(sizeof(double) * nc * 9);
+  double *VL = malloc(sizeof(double) * nc * 9);
+  double *VR = malloc(sizeof(double) * nc * 9);
+  u2v_mhd(c, c->U_m, V);
+  get_side(c, V, VL, VR, dir, c->nm);
+  set_fluxes(c, F_m, VL, VR, dir, 1);
+  u2v_hd(c, c->U_h, V);
+  get_side(c, V, VL, VR, dir, c->nh);
+  set_fluxes(c, F_h, VL, VR, dir, 0);
+  free(V); free(VL); free(VR);
+}
+
+void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m) {
+  memset(F_h, 0, sizeof(double) * c->nc * c->nh);
+  memset(F_m, 0, sizeof(double) * c->nc * c->nm);
+  flux_dir(c, dir, F_h, F_m);
+}
+
+/* ---------------------------------------------------------------- sources */
+
+/* Ionisation/recombination rates of PIP_IR_POWERLAW (a new law) from the ion state U_m:
+ * pressure by get_Pr_MHD's expression and floor (Scheme_rot.f90:112-121, without its
+ * energy rewrite), temperature by get_Te_MHD (:104-110), Te = 0.5*gm*(pr/ro). */
+static void set_ir_rates(orc_ctx *c) {
+  size_t nc = c->nc;
+  double gm = c->p.gm, pr_lim = c->p.pr_lim;
+  const double *U = c->U_m;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double u1 = U[q], u2 = U[q + nc], u3 = U[q + 2 * nc], u4 = U[q + 3 * nc];
+    double u6 = U[q + 5 * nc], u7 = U[q + 6 * nc], u8 = U[q + 7 * nc];
+    double pr = (gm - 1.0) * (U[q + 4 * nc] -
+                              0.5 * ((u2 * u2 + u3 * u3 + u4 * u4) / u1 + u6 * u6 + u7 * u7 + u8 * u8));
+    pr = fmx(pr, pr_lim);
+    double te = 0.5 * gm * (pr / u1);
+    double rs = 1.0 / sqrt(te);
+    c->gm_rec[q] = c->p.ir_rec_coef * rs;
+    c->gm_ion[q] = c->p.ir_ion_coef * rs * exp(-c->p.ir_chi / te);
+  }
+}
+
+/* source_PIP, PIP_rot.f90:1309-1429 (explicit and exponential collision forms plus the
+ * IR block with flag_IR_type 1 or 2).  out_h/out_m receive S (explicit form) or the U0
+ * increments of the exponential form, plus the IR rates in S. */
+static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, double *S_h,
+                       double *S_m) {
+  size_t nc = c->nc;
+  double gm = c->p.gm, ac = c->p.col;
+  double *w = malloc(sizeof(double) * nc * 13);
+  double *nde = w, *nvx = w + nc, *nvy = w + 2 * nc, *nvz = w + 3 * nc, *npr = w + 4 * nc;
+  double *de = w + 5 * nc, *vx = w + 6 * nc, *vy = w + 7 * nc, *vz = w + 8 * nc, *pr = w + 9 * nc;
+  cq2pv_hd(c, c->U_h, nde, nvx, nvy, nvz, npr);
+  cq2pv_mhd(c, c->U_m, de, vx, vy, vz, pr, NULL, NULL, NULL);
+  double *U_h = c->U_h, *U_m = c->U_m;
+  int imp = c->p.flag_pip_imp == 1;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double te = pr[q] / de[q] * gm * MU_P;
+    double nte = npr[q] / nde[q] * gm * MU_N;
+    double ds[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (imp) {
+      double temp = dt_coll * (U_h[q] + U_m[q]);
+      double e = (1.0 - exp(-ac * temp));
+      ds[1] = (U_m[q] * U_h[q + nc] - U_h[q] * U_m[q + nc]) * e / temp;
+      ds[2] = (U_m[q] * U_h[q + 2 * nc] - U_h[q] * U_m[q + 2 * nc]) * e / temp;
+      ds[3] = (U_m[q] * U_h[q + 3 * nc] - U_h[q] * U_m[q + 3 * nc]) * e / temp;
+      double lambda = ac * (nde[q] + de[q]);
+      double kap = 3.0 * (gm - 1.0) * ac * (MU_P * nde[q] + MU_N * de[q]);
+      double dvx = nvx[q] - vx[q], dvy = nvy[q] - vy[q], dvz = nvz[q] - vz[q];
+      /* (nvz-vz)*nvz in the ion term is as written in PIP_rot.f90:1348 */
+      double B = -(1.0 / 3.0 * gm * kap / ((nde[q] + de[q]) * (kap - lambda)) *
+                   (de[q] * (dvx * vx[q] + dvy * vy[q] + dvz * nvz[q]) +
+                    nde[q] * (dvx * nvx[q] + dvy * nvy[q] + dvz * nvz[q])));
+      double D = -(gm / 6.0 * kap * (de[q] - nde[q]) / ((de[q] + nde[q]) * (kap - 2.0 * lambda)) *
+                   (dvx * dvx + dvy * dvy + dvz * dvz));
+      ds[4] = -((3.0 / gm) * ac * de[q] * nde[q] / kap *
+                (+(exp(-kap * dt_coll) - 1.0) * (nte - te) - (B + D) * exp(-kap * dt_coll) +
+                 B * exp(-lambda * dt_coll) + D * exp(-2.0 * lambda * dt_coll)) /
+                dt_coll);
+      for (int n = 0; n < 5; ++n) {
+        U_h0[q + n * nc] = U_h0[q + n * nc] - dt_coll * ds[n];
+        U_m0[q + n * nc] = U_m0[q + n * nc] + dt_coll * ds[n];
+      }
+    } else {
+      ds[1] = ac * (U_m[q] * U_h[q + nc] - U_h[q] * U_m[q + nc]);
+      ds[2] = ac * (U_m[q] * U_h[q + 2 * nc] - U_h[q] * U_m[q + 2 * nc]);
+      ds[3] = ac * (U_m[q] * U_h[q + 3 * nc] - U_h[q] * U_m[q + 3 * nc]);
+      ds[4] = ac * nde[q] * de[q] *
+              (0.5 * ((nvx[q] * nvx[q] - vx[q] * vx[q]) + (nvy[q] * nvy[q] - vy[q] * vy[q]) +
+                      (nvz[q] * nvz[q] - vz[q] * vz[q])) +
+               3.0 / gm / 2.0 * (nte - te));
+      for (int n = 0; n < 5; ++n) {
+        S_h[q + n * nc] = S_h[q + n * nc] - ds[n];
+        S_m[q + n * nc] = S_m[q + n * nc] + ds[n];
+      }
+    }
+    if (c->p.flag_ir != PIP_IR_NONE) {
+      double gr = c->gm_rec[q], gi = c->gm_ion[q];
+      ds[0] = gr * de[q] - gi * nde[q];
+      ds[1] = gr * de[q] * vx[q] - gi * nde[q] * nvx[q];
+      ds[2] = gr * de[q] * vy[q] - gi * nde[q] * nvy[q];
+      ds[3] = gr * de[q] * vz[q] - gi * nde[q] * nvz[q];
+      double kin = 0.5 * (gr * de[q] * (vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q]) -
+                          gi * nde[q] * (nvx[q] * nvx[q] + nvy[q] * nvy[q] + nvz[q] * nvz[q]));
+      if (c->p.flag_ir_type == 1)
+        ds[4] = kin - gi * npr[q] / (gm - 1.0) + 0.5 * gr * pr[q] / (gm - 1.0);
+      else
+        ds[4] = kin - gi * npr[q] / (gm - 1.0) + gr * pr[q] / (gm - 1.0);
+      for (int n = 0; n < 5; ++n) {
+        S_h[q + n * nc] = S_h[q + n * nc] + ds[n];
+        S_m[q + n * nc] = S_m[q + n * nc] - ds[n];
+      }
+    }
+  }
+  free(w);
+}
+
+void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m) {
+  size_t nc = c->nc;
+  memset(S_h, 0, sizeof(double) * nc * c->nh);
+  memset(S_m, 0, sizeof(double) * nc * c->nm);
+  if (c->p.flag_pip_imp == 1) {
+    /* report the U0 increments: run the form on zero U0 copies */
+    source_pip(c, S_h, S_m, dt_coll, S_h, S_m);
+  } else {
+    source_pip(c, NULL, NULL, dt_coll, S_h, S_m);
+  }
+}
+
+/* ---------------------------------------------------------------- CFL */
+
+/* cfl, Scheme_rot.f90:183-213 with cfl_mhd :245-289, cfl_hd :215-243, cfl_pn_col :305-313
+ * and cfl_pip_ir :315-327 (flag_IR_type 1/2 branch). */
+void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  double gm = p->gm, safety = p->safety, ac = p->col;
+  double *w = malloc(sizeof(double) * nc * 8);
+  double *de = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc, *pr = w + 4 * nc;
+  double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
+  int m0 = p->margin[0], m1 = p->margin[1], m2 = p->margin[2];
+
+  /* cfl_mhd */
+  cq2pv_mhd(c, c->U_m, de, vx, vy, vz, pr, bx, by, bz);
+  /* set_IR for the rates the following run_solver uses: from the rewritten ion state */
+  if (p->flag_ir != PIP_IR_NONE) set_ir_rates(c);
+  double dt_min = 10.0;
+#pragma omp parallel for collapse(2) reduction(min : dt_min) schedule(static)
+  for (int k = m2; k < c->kx - m2; ++k)
+    for (int j = m1; j < c->jx - m1; ++j)
+      for (int i = m0; i < c->ix - m0; ++i) {
+        size_t q = AT(c, i, j, k);
+        double gmin = fmn(fmn(c->dx[i], c->dy[j]), c->dz[k]);
+        double cs2 = gm * pr[q] / fmx(de[q], TINY);
+        double valf2 = (bx[q] * bx[q] + by[q] * by[q] + bz[q] * bz[q]) / fmx(de[q], TINY);
+        double vabs = sqrt(vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q]);
+        dt_min = fmn(dt_min, safety * gmin / (vabs + sqrt(cs2 + valf2)));
+      }
+  double dttemp = dt_min;
+
+  /* cfl_hd (flag_pip=1: starts from the MHD value) */
+  cq2pv_hd(c, c->U_h, de, vx, vy, vz, pr);
+  dt_min = dttemp;
+#pragma omp parallel for collapse(2) reduction(min : dt_min) schedule(static)
+  for (int k = m2; k < c->kx - m2; ++k)
+    for (int j = m1; j < c->jx - m1; ++j)
+      for (int i = m0; i < c->ix - m0; ++i) {
+        size_t q = AT(c, i, j, k);
+        double gmin = fmn(fmn(c->dx[i], c->dy[j]), c->dz[k]);
+        double cs = sqrt(gm * pr[q] / de[q]);
+        double vabs = sqrt(fmx(vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q], TINY));
+        dt_min = fmn(dt_min, safety * gmin / (vabs + cs));
+      }
+  dttemp = dt_min;
+
+  /* cfl_pn_col: maxima over all cells, ghosts included */
+  double mm = -INFINITY, mh = -INFINITY;
+#pragma omp parallel for reduction(max : mm, mh) schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    mm = fmx(mm, c->U_m[q] * ac);
+    mh = fmx(mh, c->U_h[q] * ac);
+  }
+  if (p->flag_pip_imp == 1) dttemp = fmn(dttemp, p->pip_imp_factor / fmx(mm, mh));
+  else dttemp = fmn(dttemp, fmn(safety, 0.3) / fmx(mm, mh));
+
+  /* cfl_pip_ir */
+  if (p->flag_ir != PIP_IR_NONE) {
+    double gr = -INFINITY, gi = -INFINITY;
+#pragma omp parallel for reduction(max : gr, gi) schedule(static)
+    for (size_t q = 0; q < nc; ++q) {
+      gr = fmx(gr, c->gm_rec[q]);
+      gi = fmx(gi, c->gm_ion[q]);
+    }
+    dttemp = fmn(dttemp, fmn(safety, 0.1) / fmx(fmx(gr, gi), 1.0e-5));
+  }
+
+  /* cmax for Dedner cleaning */
+  double cmax = c->cmax;
+  if (p->flag_divb >= 1) {
+    double g = INFINITY;
+    for (int i = 0; i < c->ix; ++i) g = fmn(g, c->dx[i]);
+    double gy = INFINITY, gz = INFINITY;
+    for (int j = 0; j < c->jx; ++j) gy = fmn(gy, c->dy[j]);
+    for (int k = 0; k < c->kx; ++k) gz = fmn(gz, c->dz[k]);
+    g = fmn(fmn(g, gy), gz);
+    cmax = safety * g / dttemp;
+  }
+  free(w);
+  if (dt_out) *dt_out = dttemp;
+  if (cmax_out) *cmax_out = cmax;
+}
+
+/* ---------------------------------------------------------------- integration */
+
+/* add_flux_rk HLL branch, Solver_rot.f90:383-405. */
+static void add_flux_rk(orc_ctx *c, const double *F, const double *U0, double *U, int nvar,
+                        double dt, int dir) {
+  size_t nc = c->nc;
+  int ix = c->ix, jx = c->jx, kx = c->kx;
+  if (dir == 1) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int n = 0; n < nvar; ++n)
+      for (int k = 0; k < kx; ++k)
+        for (int j = 0; j < jx; ++j)
+          for (int i = 1; i < ix; ++i) {
+            size_t q = AT(c, i, j, k) + n * nc;
+            U[q] = U0[q] - (dt / c->dx[i]) * (F[q] - F[q - 1]);
+          }
+  } else if (dir == 2) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int n = 0; n < nvar; ++n)
+      for (int k = 0; k < kx; ++k)
+        for (int j = 1; j < jx; ++j)
+          for (int i = 0; i < ix; ++i) {
+            size_t q = AT(c, i, j, k) + n * nc;
+            U[q] = U[q] - (dt / c->dy[j]) * (F[q] - F[q - ix]);
+          }
+  }
+}
+
+/* run_solver, Solver_rot.f90:42-81 with set_flux :124, set_source :162, time_integral
+ * :179-277 (flag_time=0), add_source :498-503, divb_cleaning_Dedner_source
+ * (Scheme_rot.f90:546-554) and PIPbnd after each stage and at the end. */
+void orc_run_solver(orc_ctx *c, double dt) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  int nh = c->nh, nm = c->nm, t_order = p->t_order;
+  double *U_h0 = malloc(sizeof(double) * nc * nh), *U_m0 = malloc(sizeof(double) * nc * nm);
+  memcpy(U_h0, c->U_h, sizeof(double) * nc * nh);
+  memcpy(U_m0, c->U_m, sizeof(double) * nc * nm);
+  double *F_h = calloc(nc * nh * 3, sizeof(double)), *F_m = calloc(nc * nm * 3, sizeof(double));
+  double *S_h = malloc(sizeof(double) * nc * nh), *S_m = malloc(sizeof(double) * nc * nm);
+  double dt_coll[2] = {dt * 0.5, dt * 0.5};
+  for (int istep = 1; istep <= t_order; ++istep) {
+    double dt_coll_i = dt_coll[t_order - istep];
+    for (int dir = 1; dir <= p->ndim; ++dir)
+      flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
+    memset(S_h, 0, sizeof(double) * nc * nh);
+    memset(S_m, 0, sizeof(double) * nc * nm);
+    source_pip(c, U_h0, U_m0, dt_coll_i, S_h, S_m);
+    double dt_sub = dt / (double)(t_order - istep + 1);
+    for (int dir = 1; dir <= p->ndim; ++dir)
+      add_flux_rk(c, F_h + (size_t)(dir - 1) * nc * nh, U_h0, c->U_h, nh, dt_sub, dir);
+    for (size_t q = 0; q < nc * nh; ++q) c->U_h[q] = c->U_h[q] + S_h[q] * dt_sub;
+    for (int dir = 1; dir <= p->ndim; ++dir)
+      add_flux_rk(c, F_m + (size_t)(dir - 1) * nc * nm, U_m0, c->U_m, nm, dt_sub, dir);
+    for (size_t q = 0; q < nc * nm; ++q) c->U_m[q] = c->U_m[q] + S_m[q] * dt_sub;
+    if (p->flag_divb == 1) {
+      double fac = exp(-dt_sub / dt * p->safety * p->db_clean);
+      double *ps = c->U_m + 8 * nc;
+      for (size_t q = 0; q < nc; ++q) ps[q] = ps[q] * fac;
+    }
+    orc_bnd(c);
+  }
+  orc_bnd(c);
+  free(U_h0); free(U_m0); free(F_h); free(F_m); free(S_h); free(S_m);
+}
+
+int orc_has_nan(const orc_ctx *c) {
+  size_t nc = c->nc;
+  int bad = 0;
+  for (size_t q = 0; q < nc * c->nm; ++q) bad |= !isfinite(c->U_m[q]);
+  for (size_t q = 0; q < nc * c->nh; ++q) bad |= !isfinite(c->U_h[q]);
+  return bad;
+}
+
+/* Time loop, main.f90:31-68: set_IR and cfl, run_solver, cfl again, time += dt,
+ * stop_sim (IO_rot.f90:625-674). */
+int orc_run(orc_ctx *c, long nsteps, double t_end, double *time_out, long *steps_done,
+            double *dt_hist, long max_hist) {
+  long n = 0;
+  int status = 0;
+  while ((nsteps <= 0 || n < nsteps) && (t_end <= 0.0 || c->time < t_end)) {
+    double dt, cmax, dtnew;
+    orc_cfl(c, &dt, &cmax);
+    c->cmax = cmax;
+    orc_run_solver(c, dt);
+    orc_cfl(c, &dtnew, NULL);
+    c->time = c->time + dt;
+    c->last_dt = dt;
+    if (dt_hist && n < max_hist) dt_hist[n] = dt;
+    ++n;
+    if (orc_has_nan(c)) { status = PIP_ERR_NAN; break; }
+    if (dt <= 1.0e-12) { status = PIP_ERR_DT; break; }
+  }
+  if (time_out) *time_out = c->time;
+  if (steps_done) *steps_done = n;
+  return status;
+}
+
+/* ---------------------------------------------------------------- lifecycle */
+
+orc_ctx *orc_create(const pip_params *p, int *status) {
+  *status = PIP_ERR_PARAM;
+  if (!p || p->ndim < 1 || p->ndim > 2 || p->kx != 1 || p->nvar_h != 5) return NULL;
+  if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return NULL;
+  orc_ctx *c = calloc(1, sizeof(orc_ctx));
+  c->p = *p;
+  c->ix = p->ix; c->jx = p->jx; c->kx = p->kx;
+  c->nh = p->nvar_h; c->nm = p->nvar_m;
+  c->nc = (size_t)c->ix * c->jx * c->kx;
+  c->dx = malloc(sizeof(double) * c->ix);
+  c->dy = malloc(sizeof(double) * c->jx);
+  c->dz = malloc(sizeof(double) * c->kx);
+  memcpy(c->dx, p->dx, sizeof(double) * c->ix);
+  memcpy(c->dy, p->dy, sizeof(double) * c->jx);
+  memcpy(c->dz, p->dz, sizeof(double) * c->kx);
+  c->U_h = calloc(c->nc * c->nh, sizeof(double));
+  c->U_m = calloc(c->nc * c->nm, sizeof(double));
+  c->gm_ion = calloc(c->nc, sizeof(double));
+  c->gm_rec = calloc(c->nc, sizeof(double));
+  set_sym_mhd(c);
+  set_sym_hd(c);
+  *status = PIP_OK;
+  return c;
+}
+
+void orc_destroy(orc_ctx *c) {
+  if (!c) return;
+  free(c->dx); free(c->dy); free(c->dz);
+  free(c->U_h); free(c->U_m); free(c->gm_ion); free(c->gm_rec);
+  free(c);
+}
+
+void orc_set_state(orc_ctx *c, const double *U_h, const double *U_m) {
+  memcpy(c->U_h, U_h, sizeof(double) * c->nc * c->nh);
+  memcpy(c->U_m, U_m, sizeof(double) * c->nc * c->nm);
+}
+
+void orc_get_state(const orc_ctx *c, double *U_h, double *U_m) {
+  memcpy(U_h, c->U_h, sizeof(double) * c->nc * c->nh);
+  memcpy(U_m, c->U_m, sizeof(double) * c->nc * c->nm);
+}
+
+void orc_set_time(orc_ctx *c, double t) { c->time = t; }
+double orc_get_time(const orc_ctx *c) { return c->time; }
+double orc_get_cmax(const orc_ctx *c) { return c->cmax; }
+void orc_set_cmax(orc_ctx *c, double cmax) { c->cmax = cmax; }

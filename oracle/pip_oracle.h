@@ -1,0 +1,58 @@
+/*
+ * pip_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU FP64 restatement of PIP's two-fluid finite-volume step, used as the correctness
+ * checker of the CUDA library and as the timed CPU baseline.  Only tests/, the smoke
+ * check and bench.py's CPU-baseline leg may load it; the product never does.
+ *
+ * Parity status: UNPINNED by the reference itself.  The reference ships no tests, golden
+ * vectors or fixtures for this path and cannot be built here (Fortran 90 + MPI + parallel
+ * HDF5, Makefile:29, MPI_rot.f90:7, Globalvar.f90:9; no Fortran compiler in the image).
+ * The restatement follows the cited Fortran statement by statement (operation order and
+ * parenthesisation kept, no FMA contraction) and is cross-checked by conservation,
+ * symmetry and analytic-rate tests and by an independent numpy restatement.
+ */
+#ifndef PIP_ORACLE_H
+#define PIP_ORACLE_H
+
+#include "../include/pip_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_ctx orc_ctx;
+
+orc_ctx *orc_create(const pip_params *p, int *status);
+void orc_destroy(orc_ctx *c);
+void orc_set_threads(int n);
+int orc_get_threads(void);
+void orc_set_state(orc_ctx *c, const double *U_h, const double *U_m);
+void orc_get_state(const orc_ctx *c, double *U_h, double *U_m);
+void orc_set_time(orc_ctx *c, double t);
+double orc_get_time(const orc_ctx *c);
+double orc_get_cmax(const orc_ctx *c);
+void orc_set_cmax(orc_ctx *c, double cmax);
+
+/* Scheme_rot.f90:183-213 (rewrites the state, returns dt and cmax). */
+void orc_cfl(orc_ctx *c, double *dt, double *cmax);
+/* Solver_rot.f90:42-81 with the given dt and the stored cmax. */
+void orc_run_solver(orc_ctx *c, double dt);
+/* Solver_rot.f90:124-159 for one direction (1-based), F arrays (ix,jx,kx,nvar). */
+void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m);
+/* PIP_rot.f90:1309-1429; returns S (explicit) or the U0 increments (exponential form). */
+void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m);
+/* Boundary_rot.f90:34-52. */
+void orc_bnd(orc_ctx *c);
+/* main.f90:31-68 loop; returns 0, PIP_ERR_NAN or PIP_ERR_DT.  dt_hist (may be NULL)
+ * receives up to max_hist per-step dt values. */
+int orc_run(orc_ctx *c, long nsteps, double t_end, double *time_out, long *steps_done,
+            double *dt_hist, long max_hist);
+/* stop_sim's NaN scan (IO_rot.f90:641-668) over both species. */
+int orc_has_nan(const orc_ctx *c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,241 @@
+"""ctypes binding of the C ABI (include/pip_gpu.h) in pip_b200/libpipgpu.so.
+
+This is the reference-facing surface in Python form: the same calls the Fortran driver
+makes through ISO_C_BINDING.  There is no CPU fallback: if the CUDA
+library is missing or no GPU is visible the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .params import PipParams, Settings
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpipgpu.so")
+
+PIP_OK = 0
+PIP_ERR_PARAM = 1
+PIP_ERR_CUDA = 2
+PIP_ERR_NAN = 3
+PIP_ERR_DT = 4
+PIP_ERR_ITER = 5
+PIP_ERR_STATE = 6
+PIP_ERR_NOMEM = 7
+PIP_ERR_NULL = 8
+
+# every extern "C" symbol include/pip_gpu.h declares
+EXPORTS = (
+    "pip_ctx_create", "pip_ctx_destroy", "pip_upload", "pip_download", "pip_cfl", "pip_step",
+    "pip_run", "pip_set_time", "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts",
+    "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
+    # include/pip_bench.h
+    "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run",
+)
+
+_lib = None
+
+
+class PipError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = "%s failed: %s (%d)" % (where, strerror(code), code)
+        if code == PIP_ERR_CUDA:
+            msg += ", cudaError %d" % lib().pip_last_cuda_error()
+        super().__init__(msg)
+
+
+def lib(path: Optional[str] = None):
+    """Load libpipgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError("libpipgpu.so is missing: run `python -m pip_b200.build` "
+                           "(or __graft_entry__.build()) first")
+    L = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    d = ctypes.c_double
+    dp = P(d)
+    vp = ctypes.c_void_p
+    i = ctypes.c_int
+    L.pip_ctx_create.argtypes = [P(PipParams), P(vp)]
+    L.pip_ctx_create.restype = i
+    L.pip_ctx_destroy.argtypes = [vp]
+    L.pip_ctx_destroy.restype = None
+    L.pip_upload.argtypes = [vp, dp, dp]
+    L.pip_download.argtypes = [vp, dp, dp]
+    L.pip_cfl.argtypes = [vp, dp, dp]
+    L.pip_step.argtypes = [vp, d]
+    L.pip_run.argtypes = [vp, ctypes.c_int64, d, dp, P(ctypes.c_int64)]
+    L.pip_set_time.argtypes = [vp, d]
+    L.pip_get_time.argtypes = [vp, dp]
+    L.pip_flux.argtypes = [vp, i, dp, dp]
+    L.pip_source.argtypes = [vp, d, dp, dp]
+    L.pip_fill_ghosts.argtypes = [vp]
+    L.pip_status.argtypes = [vp, P(i), P(i)]
+    L.pip_conduction.argtypes = [vp, d, P(i), dp]
+    L.pip_last_cuda_error.argtypes = []
+    L.pip_strerror.argtypes = [i]
+    L.pip_strerror.restype = ctypes.c_char_p
+    # measurement hooks (include/pip_bench.h)
+    L.pip_run_timed.argtypes = [vp, ctypes.c_int64, d, dp, P(ctypes.c_int64), P(ctypes.c_float)]
+    L.pip_bench_stage_ms.argtypes = [vp, i, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)]
+    L.pip_kernels_per_run.argtypes = [vp, ctypes.c_int64]
+    L.pip_kernels_per_run.restype = ctypes.c_int64
+    for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",
+                 "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts", "pip_status",
+                 "pip_conduction", "pip_last_cuda_error", "pip_run_timed", "pip_bench_stage_ms"):
+        getattr(L, name).restype = i
+    _lib = L
+    return L
+
+
+def strerror(code: int) -> str:
+    return lib().pip_strerror(int(code)).decode()
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("arrays must be C-contiguous float64 (Fortran U(ix,jx,kx,nvar) order)")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(code: int, where: str) -> int:
+    if code != PIP_OK:
+        raise PipError(code, where)
+    return code
+
+
+class Context:
+    """One device-resident two-fluid simulation (a ``pip_ctx``).
+
+    Method names follow the Fortran routines they replace: ``cfl`` (Scheme_rot.f90:183),
+    ``run_solver`` (Solver_rot.f90:42), ``set_flux`` (:124), ``source_pip``
+    (PIP_rot.f90:1309), ``pipbnd`` (Boundary_rot.f90:34).
+    """
+
+    def __init__(self, s: Settings):
+        self.s = s
+        self.params, self._keep = s.to_params()
+        h = ctypes.c_void_p()
+        _check(lib().pip_ctx_create(ctypes.byref(self.params), ctypes.byref(h)), "pip_ctx_create")
+        self.h = h
+        ix, jx, _ = s.shape
+        self.shape_h = (s.nvar_h, jx, ix)
+        self.shape_m = (s.nvar_m, jx, ix)
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().pip_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ state
+    def upload(self, U_h: np.ndarray, U_m: np.ndarray) -> None:
+        U_h = np.ascontiguousarray(U_h, dtype=np.float64)
+        U_m = np.ascontiguousarray(U_m, dtype=np.float64)
+        if U_h.shape != self.shape_h or U_m.shape != self.shape_m:
+            raise ValueError("state shapes %s/%s, expected %s/%s"
+                             % (U_h.shape, U_m.shape, self.shape_h, self.shape_m))
+        _check(lib().pip_upload(self.h, _ptr(U_h), _ptr(U_m)), "pip_upload")
+
+    def download(self, out_h: Optional[np.ndarray] = None,
+                 out_m: Optional[np.ndarray] = None) -> Tuple[np.ndarray, np.ndarray]:
+        U_h = out_h if out_h is not None else np.empty(self.shape_h)
+        U_m = out_m if out_m is not None else np.empty(self.shape_m)
+        _check(lib().pip_download(self.h, _ptr(U_h), _ptr(U_m)), "pip_download")
+        return U_h, U_m
+
+    # ------------------------------------------------------------------ the step
+    def cfl(self) -> Tuple[float, float]:
+        dt = ctypes.c_double()
+        cm = ctypes.c_double()
+        _check(lib().pip_cfl(self.h, ctypes.byref(dt), ctypes.byref(cm)), "pip_cfl")
+        return dt.value, cm.value
+
+    def run_solver(self, dt: float) -> None:
+        _check(lib().pip_step(self.h, float(dt)), "pip_step")
+
+    def run(self, nsteps: int = 0, t_end: float = 0.0, check: bool = True) -> Tuple[int, float, int]:
+        """Time loop on the device; returns (status, time, steps)."""
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        st = lib().pip_run(self.h, int(nsteps), float(t_end), ctypes.byref(t), ctypes.byref(n))
+        if check and st not in (PIP_OK, PIP_ERR_NAN, PIP_ERR_DT):
+            raise PipError(st, "pip_run")
+        return st, t.value, n.value
+
+    @property
+    def time(self) -> float:
+        t = ctypes.c_double()
+        _check(lib().pip_get_time(self.h, ctypes.byref(t)), "pip_get_time")
+        return t.value
+
+    @time.setter
+    def time(self, t: float) -> None:
+        _check(lib().pip_set_time(self.h, float(t)), "pip_set_time")
+
+    # ------------------------------------------------------------------ unit entry points
+    def set_flux(self, direction: int) -> Tuple[np.ndarray, np.ndarray]:
+        F_h = np.empty(self.shape_h)
+        F_m = np.empty(self.shape_m)
+        _check(lib().pip_flux(self.h, int(direction), _ptr(F_h), _ptr(F_m)), "pip_flux")
+        return F_h, F_m
+
+    def source_pip(self, dt_coll: float) -> Tuple[np.ndarray, np.ndarray]:
+        S_h = np.empty(self.shape_h)
+        S_m = np.empty(self.shape_m)
+        _check(lib().pip_source(self.h, float(dt_coll), _ptr(S_h), _ptr(S_m)), "pip_source")
+        return S_h, S_m
+
+    def pipbnd(self) -> None:
+        _check(lib().pip_fill_ghosts(self.h), "pip_fill_ghosts")
+
+    def status(self) -> Tuple[int, int]:
+        stop = ctypes.c_int()
+        nan = ctypes.c_int()
+        _check(lib().pip_status(self.h, ctypes.byref(stop), ctypes.byref(nan)), "pip_status")
+        return stop.value, nan.value
+
+    def prologue(self) -> None:
+        """The prologue's cfl and ghost fill (Initial_rot.f90:152-160)."""
+        self.cfl()
+        self.pipbnd()
+
+    # ------------------------------------------------------------------ measurement hooks
+    def run_timed(self, nsteps: int = 0, t_end: float = 0.0) -> Tuple[int, float, int, float]:
+        """pip_run plus the device time of the loop (ms, CUDA events on the context stream)."""
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        ms = ctypes.c_float()
+        st = lib().pip_run_timed(self.h, int(nsteps), float(t_end), ctypes.byref(t),
+                                 ctypes.byref(n), ctypes.byref(ms))
+        if st not in (PIP_OK, PIP_ERR_NAN, PIP_ERR_DT):
+            raise PipError(st, "pip_run_timed")
+        return st, t.value, n.value, ms.value
+
+    def stage_ms(self, nsteps: int) -> Tuple[float, float, float]:
+        """Mean device time of one stage-1 launch, one stage-2 launch and one step (ms)."""
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _check(lib().pip_bench_stage_ms(self.h, int(nsteps), ctypes.byref(a), ctypes.byref(b),
+                                        ctypes.byref(c)), "pip_bench_stage_ms")
+        return a.value, b.value, c.value
+
+    def kernels_per_run(self, nsteps: int) -> int:
+        return int(lib().pip_kernels_per_run(self.h, int(nsteps)))

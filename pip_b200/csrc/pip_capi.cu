@@ -1,0 +1,623 @@
+// pip_capi.cu -- C ABI of the two-fluid step (include/pip_gpu.h): context, host<->device
+// copies and the device-side time loop.
+//
+// The context owns two device arrays of NV = nvm + 5 planes (A: current state / U0 / U2,
+// B: U1), a small control block (DevCtrl) and lazily allocated scratch for the unit-level
+// entry points.  pip_run keeps dt, time and the stop flags on the device and replays a
+// captured CUDA graph of K steps (2 kernels per step) between host polls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/pip_bench.h"
+#include "../../include/pip_gpu.h"
+#include "pip_kernels.cuh"
+
+using pip::DevCtrl;
+using pip::KParams;
+
+static int g_last_cuda_error = 0;
+
+struct pip_ctx {
+  pip_params p{};
+  std::vector<double> dx, dy, dz;
+  KParams kp{};
+  const pip::Launchers *L = nullptr;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double *A = nullptr, *B = nullptr;  // NV planes each
+  double *d_dx = nullptr, *d_dy = nullptr;
+  double *scratch = nullptr;          // NV planes for pip_flux / pip_source
+  int *d_flag = nullptr;
+  DevCtrl *ctrl = nullptr;
+  DevCtrl *h_ctrl = nullptr;          // pinned mirror
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  bool uploaded = false;
+  double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
+  int nplanes() const { return kp.nvm + 5; }
+  size_t plane_bytes() const { return sizeof(double) * (size_t)kp.nc; }
+};
+
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t e__ = (call);                      \
+    if (e__ != cudaSuccess) {                      \
+      g_last_cuda_error = (int)e__;                \
+      return PIP_ERR_CUDA;                         \
+    }                                              \
+  } while (0)
+
+namespace {
+
+// set_sym_mhd (Boundary_rot.f90:239-294), sign per ion variable for face f (0-based).
+void sym_mhd(const pip_params &p, int f, signed char *out) {
+  for (int n = 0; n < 9; ++n) out[n] = 1;
+  const int dir = f / 2 + 1, b = p.flag_bnd[f];
+  auto flip = [&](int var1) { out[var1 - 1] = -1; };  // 1-based variable number
+  switch (b) {
+    case 2: flip(1 + dir); flip(5 + dir); break;
+    case 3: flip(1 + dir); flip(6 + dir % 3); flip(2 + (dir + 1) % 3); break;
+    case 4: flip(1 + dir); flip(6 + (dir + 1) % 3); flip(2 + dir % 3); break;
+    case 5: flip(1 + dir); flip(5 + dir); flip(2 + (dir + 1) % 3); flip(6 + (dir + 1) % 3); break;
+    case 6: flip(1 + dir); flip(6 + dir % 3); flip(6 + (dir + 1) % 3); break;
+    case 7: flip(2); flip(3); flip(4); break;
+    default: break;
+  }
+  if (p.flag_divb == 1) {
+    if (b == 2 || b == 20 || b == 5) out[8] = 1;
+    else if (b == 3 || b == 4 || b == 6 || b == 7) out[8] = -1;
+  }
+}
+
+// set_sym_hd (Boundary_rot.f90:296-320).
+void sym_hd(const pip_params &p, int f, signed char *out) {
+  for (int n = 0; n < 5; ++n) out[n] = 1;
+  const int dir = f / 2 + 1, b = p.flag_bnd[f];
+  auto flip = [&](int var1) { out[var1 - 1] = -1; };
+  switch (b) {
+    case 2: case 20: flip(1 + dir); break;
+    case 3: flip(1 + dir); flip(2 + (dir + 1) % 3); break;
+    case 4: flip(1 + dir); flip(2 + dir % 3); break;
+    case 5: flip(1 + dir); flip(2 + (dir + 1) % 3); break;
+    case 6: flip(1 + dir); break;
+    default: break;
+  }
+}
+
+// boundary_control type of a face code (MHDbnd/HDbnd, Boundary_rot.f90:62-80).
+int bnd_type(int code) {
+  switch (code) {
+    case 3: case 4: case 5: case 6: case 7: case 11: return 2;
+    default: return code;
+  }
+}
+
+// Source index of ghost layer l on side s of an axis with n cells and m ghost layers
+// (boundary_control's sr ranges, Boundary_rot.f90:338-368), 0-based.
+int ghost_source(int type, int side, int l, int n, int m) {
+  if (side == 0) {
+    if (type == 1) return n - 2 * m + l;
+    if (type == 2) return 2 * m - 1 - l;
+    return m;  // type 10
+  }
+  if (type == 1) return m + l;
+  if (type == 2) return n - m - 1 - l;
+  return n - m - 1;
+}
+
+bool supported_bnd(int code) {
+  switch (code) {
+    case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 10: case 11: return true;
+    default: return false;
+  }
+}
+
+int validate(const pip_params *p) {
+  if (!p) return PIP_ERR_NULL;
+  if (p->abi_version != PIP_ABI_VERSION) return PIP_ERR_PARAM;
+  if (p->ndim != 1 && p->ndim != 2) return PIP_ERR_PARAM;
+  if (p->kx != 1 || p->nvar_h != 5) return PIP_ERR_PARAM;
+  if (p->ndim == 1 && p->flag_divb != 0) return PIP_ERR_PARAM;
+  if (p->flag_divb != 0 && p->flag_divb != 1) return PIP_ERR_PARAM;
+  if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return PIP_ERR_PARAM;
+  if (p->flag_sch != 0 || p->flag_hll != 2 || p->s_order != 2 || p->t_order != 2 || p->flag_time != 0)
+    return PIP_ERR_PARAM;
+  if (p->flag_col != 1) return PIP_ERR_PARAM;
+  if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
+  if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
+  if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
+  if (p->precision != PIP_FP64) return PIP_ERR_PARAM;
+  if (p->flag_heat != 0) return PIP_ERR_PARAM;
+  const int m0 = p->margin[0], m1 = p->margin[1];
+  if (m0 < 2 || m0 > pip::kMaxMargin || p->margin[2] != 0) return PIP_ERR_PARAM;
+  if (p->ndim == 1 && (m1 != 0 || p->jx != 1)) return PIP_ERR_PARAM;
+  if (p->ndim == 2 && m1 != m0) return PIP_ERR_PARAM;
+  if (p->ix - 2 * m0 < 4) return PIP_ERR_PARAM;
+  if (p->ndim == 2 && p->jx - 2 * m1 < 4) return PIP_ERR_PARAM;
+  for (int f = 0; f < 2 * p->ndim; ++f)
+    if (!supported_bnd(p->flag_bnd[f])) return PIP_ERR_PARAM;
+  if (!p->dx || !p->dy || !p->dz) return PIP_ERR_NULL;
+  if (!(p->gm > 1.0) || !(p->safety > 0.0)) return PIP_ERR_PARAM;
+  return PIP_OK;
+}
+
+void build_kparams(pip_ctx *c) {
+  const pip_params &p = c->p;
+  KParams &k = c->kp;
+  k.ndim = p.ndim;
+  k.ix = p.ix;
+  k.jx = p.jx;
+  k.m0 = p.margin[0];
+  k.m1 = p.ndim == 2 ? p.margin[1] : 0;
+  k.nx = p.ix - 2 * k.m0;
+  k.ny = p.ndim == 2 ? p.jx - 2 * k.m1 : 1;
+  k.nvm = p.nvar_m;
+  k.imp = p.flag_pip_imp;
+  k.ir = p.flag_ir == PIP_IR_POWERLAW;
+  k.ir_type = p.flag_ir_type;
+  k.nc = (long long)p.ix * p.jx;
+  k.gm = p.gm;
+  k.ro_lim = p.ro_lim;
+  k.pr_lim = p.pr_lim;
+  k.ac = p.col;
+  k.safety = p.safety;
+  double g = INFINITY;
+  for (double v : c->dx) g = std::min(g, v);
+  double gy = INFINITY, gz = INFINITY;
+  for (double v : c->dy) gy = std::min(gy, v);
+  for (double v : c->dz) gz = std::min(gz, v);
+  k.sg_all = p.safety * std::min(std::min(g, gy), gz);
+  k.col_lim = p.flag_pip_imp == 1 ? p.pip_imp_factor : std::min(p.safety, 0.3);
+  k.ir_lim = std::min(p.safety, 0.1);
+  k.ir_chi = p.ir_chi;
+  k.ir_ion = p.ir_ion_coef;
+  k.ir_rec = p.ir_rec_coef;
+  // divb_cleaning_Dedner_source factor exp(-dt_sub/dt*safety*db_clean), dt_sub/dt = 1/2, 1
+  k.decay[0] = std::exp(-0.5 * p.safety * p.db_clean);
+  k.decay[1] = std::exp(-1.0 * p.safety * p.db_clean);
+  k.dz0 = c->dz[0];
+  for (int s = 0; s < 2; ++s) {
+    const int fx = s, fy = 2 + s;
+    k.typex[s] = bnd_type(p.flag_bnd[fx]);
+    for (int l = 0; l < pip::kMaxMargin; ++l)
+      k.gx[s][l] = l < k.m0 ? ghost_source(k.typex[s], s, l, p.ix, k.m0) : -1;
+    signed char sm[9], sh[5];
+    sym_mhd(p, fx, sm);
+    sym_hd(p, fx, sh);
+    for (int n = 0; n < k.nvm; ++n) k.symx[s][n] = sm[n];
+    for (int n = 0; n < 5; ++n) k.symx[s][k.nvm + n] = sh[n];
+    if (p.ndim == 2) {
+      k.typey[s] = bnd_type(p.flag_bnd[fy]);
+      for (int l = 0; l < pip::kMaxMargin; ++l)
+        k.gy[s][l] = l < k.m1 ? ghost_source(k.typey[s], s, l, p.jx, k.m1) : -1;
+      sym_mhd(p, fy, sm);
+      sym_hd(p, fy, sh);
+      for (int n = 0; n < k.nvm; ++n) k.symy[s][n] = sm[n];
+      for (int n = 0; n < 5; ++n) k.symy[s][k.nvm + n] = sh[n];
+    } else {
+      k.typey[s] = 1;
+      for (int l = 0; l < pip::kMaxMargin; ++l) k.gy[s][l] = -1;
+      for (int n = 0; n < pip::kMaxPlanes; ++n) k.symy[s][n] = 1;
+    }
+  }
+}
+
+// Host copy of the device finalize_dt (same IEEE operations, same order).
+double finalize_dt_host(const KParams &k, const DevCtrl &c, int slot) {
+  double dt, rho, gr;
+  std::memcpy(&dt, &c.red_dt[slot], sizeof(double));
+  std::memcpy(&rho, &c.red_rho[slot], sizeof(double));
+  std::memcpy(&gr, &c.red_gr[slot], sizeof(double));
+  dt = std::fmin(dt, k.col_lim / rho);
+  if (k.ir) dt = std::fmin(dt, k.ir_lim / std::fmax(gr, 1.0e-5));
+  return dt;
+}
+
+void reset_slot(DevCtrl &h, int slot) {
+  const double ten = 10.0;
+  std::memcpy(&h.red_dt[slot], &ten, sizeof(double));
+  h.red_rho[slot] = 0ull;
+  h.red_gr[slot] = 0ull;
+}
+
+int sync_ctrl_to_host(pip_ctx *c) {
+  CK(cudaMemcpyAsync(c->h_ctrl, c->ctrl, sizeof(DevCtrl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int push_ctrl(pip_ctx *c) {
+  CK(cudaMemcpyAsync(c->ctrl, c->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice, c->stream));
+  return PIP_OK;
+}
+
+// K steps of [stage 1, stage 2] as launched by pip_run.
+int launch_steps(pip_ctx *c, int k) {
+  for (int s = 0; s < k; ++s) {
+    cudaError_t e = c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 1, 0, c->stream);
+    if (e == cudaSuccess) e = c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 1, -1, c->stream);
+    if (e != cudaSuccess) {
+      g_last_cuda_error = (int)e;
+      return PIP_ERR_CUDA;
+    }
+  }
+  return PIP_OK;
+}
+
+int ensure_graph(pip_ctx *c, int k) {
+  if (c->graph && c->graph_steps == k) return PIP_OK;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int st = launch_steps(c, k);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (st != PIP_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  CK(e);
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
+  c->graph_steps = k;
+  return PIP_OK;
+}
+
+int ensure_scratch(pip_ctx *c) {
+  if (!c->scratch) CK(cudaMalloc(&c->scratch, c->plane_bytes() * c->nplanes()));
+  return PIP_OK;
+}
+
+int set_device(pip_ctx *c) {
+  CK(cudaSetDevice(c->device));
+  return PIP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pip_ctx_create(const pip_params *p, pip_ctx **out) {
+  if (!out) return PIP_ERR_NULL;
+  *out = nullptr;
+  int st = validate(p);
+  if (st != PIP_OK) return st;
+  pip_ctx *c = new (std::nothrow) pip_ctx();
+  if (!c) return PIP_ERR_NOMEM;
+  c->p = *p;
+  c->dx.assign(p->dx, p->dx + p->ix);
+  c->dy.assign(p->dy, p->dy + p->jx);
+  c->dz.assign(p->dz, p->dz + p->kx);
+  c->p.dx = c->p.dy = c->p.dz = nullptr;
+  build_kparams(c);
+  c->L = p->fp_exact ? &pip::launchers_exact() : &pip::launchers_fast();
+  auto fail = [&](cudaError_t e) {
+    g_last_cuda_error = (int)e;
+    pip_ctx_destroy(c);
+    return e == cudaErrorMemoryAllocation ? PIP_ERR_NOMEM : PIP_ERR_CUDA;
+  };
+  cudaError_t e = cudaGetDevice(&c->device);
+  if (e != cudaSuccess) return fail(e);
+  if ((e = c->L->prepare()) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  const size_t state = c->plane_bytes() * c->nplanes();
+  if ((e = cudaMalloc(&c->A, state)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&c->B, state)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&c->d_dx, sizeof(double) * p->ix)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&c->d_dy, sizeof(double) * p->jx)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&c->ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&c->d_flag, sizeof(int))) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocHost(&c->h_ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
+  std::memset(c->h_ctrl, 0, sizeof(DevCtrl));
+  if ((e = cudaMemcpy(c->d_dx, c->dx.data(), sizeof(double) * p->ix, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemcpy(c->d_dy, c->dy.data(), sizeof(double) * p->jx, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemset(c->A, 0, state)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(c->B, 0, state)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemcpy(c->ctrl, c->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(e);
+  c->kp.dx = c->d_dx;
+  c->kp.dy = c->d_dy;
+  *out = c;
+  return PIP_OK;
+}
+
+void pip_ctx_destroy(pip_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  cudaFree(c->A);
+  cudaFree(c->B);
+  cudaFree(c->d_dx);
+  cudaFree(c->d_dy);
+  cudaFree(c->scratch);
+  cudaFree(c->ctrl);
+  cudaFree(c->d_flag);
+  if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
+  if (!c || !U_h || !U_m) return PIP_ERR_NULL;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  const size_t pb = c->plane_bytes();
+  CK(cudaMemcpyAsync(c->A, U_m, pb * c->kp.nvm, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->A + (size_t)c->kp.nvm * c->kp.nc, U_h, pb * 5, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->uploaded = true;
+  return PIP_OK;
+}
+
+int pip_download(pip_ctx *c, double *U_h, double *U_m) {
+  if (!c || !U_h || !U_m) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  const size_t pb = c->plane_bytes();
+  CK(cudaMemcpyAsync(U_m, c->A, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(U_h, c->A + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  reset_slot(*c->h_ctrl, 0);
+  if (push_ctrl(c)) return PIP_ERR_CUDA;
+  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+  const double d = finalize_dt_host(c->kp, *c->h_ctrl, 0);
+  c->dt = d;
+  if (c->p.flag_divb >= 1) c->cmax = c->kp.sg_all / d;
+  if (dt) *dt = d;
+  if (cmax) *cmax = c->cmax;
+  return PIP_OK;
+}
+
+int pip_step(pip_ctx *c, double dt) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  DevCtrl &h = *c->h_ctrl;
+  h.dt = dt;
+  h.cmax = c->cmax;
+  h.done = 0;
+  h.nan_flag = 0;
+  h.status = 0;
+  h.blocks_done = 0;
+  if (push_ctrl(c)) return PIP_ERR_CUDA;
+  CK(c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 0, 0, c->stream));
+  CK(c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 0, 0, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_dt = dt;
+  return PIP_OK;
+}
+
+static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
+                    int64_t *steps_done, float *device_ms) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  if ((t_end > 0.0 && c->time >= t_end)) {
+    if (time_out) *time_out = c->time;
+    if (steps_done) *steps_done = 0;
+    return PIP_OK;
+  }
+  DevCtrl &h = *c->h_ctrl;
+  std::memset(&h, 0, sizeof(DevCtrl));
+  h.time = c->time;
+  h.t_end = t_end > 0.0 ? t_end : 0.0;
+  h.nsteps = nsteps > 0 ? nsteps : 0;
+  h.cmax = c->cmax;
+  reset_slot(h, 0);
+  reset_slot(h, 1);
+  if (push_ctrl(c)) return PIP_ERR_CUDA;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (device_ms) {
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    if (nsteps > 0 && !(t_end > 0.0) && nsteps >= 32) {
+      int st0 = ensure_graph(c, 32);  // instantiate before the timed region
+      if (st0 != PIP_OK) return st0;
+    }
+    CK(cudaEventRecord(ev0, c->stream));
+  }
+  // cfl of the first step (main.f90:36); later steps get it fused into stage 2
+  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  const int K = 32;
+  int st = PIP_OK;
+  if (nsteps > 0 && !(t_end > 0.0)) {
+    // known step count: whole graphs, then the remainder launched directly
+    int64_t left = nsteps;
+    if (left >= K) {
+      if ((st = ensure_graph(c, K)) != PIP_OK) return st;
+      for (; left >= K; left -= K) CK(cudaGraphLaunch(c->graph, c->stream));
+    }
+    if (left > 0 && (st = launch_steps(c, (int)left)) != PIP_OK) return st;
+    if (device_ms) CK(cudaEventRecord(ev1, c->stream));
+    if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+  } else {
+    if ((st = ensure_graph(c, K)) != PIP_OK) return st;
+    for (;;) {
+      CK(cudaGraphLaunch(c->graph, c->stream));
+      if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+      if (h.done || h.nan_flag) break;
+    }
+    if (device_ms) {
+      CK(cudaEventRecord(ev1, c->stream));
+      CK(cudaEventSynchronize(ev1));
+    }
+  }
+  if (device_ms) {
+    CK(cudaEventElapsedTime(device_ms, ev0, ev1));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  c->time = h.time;
+  c->dt = h.dt;
+  c->last_dt = h.dt;
+  c->cmax = h.cmax;
+  if (time_out) *time_out = h.time;
+  if (steps_done) *steps_done = h.step;
+  if (h.nan_flag) return PIP_ERR_NAN;
+  if (h.status) return h.status;
+  return PIP_OK;
+}
+
+int pip_run(pip_ctx *c, int64_t nsteps, double t_end, double *time_out, int64_t *steps_done) {
+  return run_loop(c, nsteps, t_end, time_out, steps_done, nullptr);
+}
+
+int pip_run_timed(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
+                  int64_t *steps_done, float *device_ms) {
+  if (!device_ms) return PIP_ERR_NULL;
+  return run_loop(c, nsteps, t_end, time_out, steps_done, device_ms);
+}
+
+int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *msstep) {
+  if (!c || !ms1 || !ms2 || !msstep) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (nsteps <= 0) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  DevCtrl &h = *c->h_ctrl;
+  std::memset(&h, 0, sizeof(DevCtrl));
+  h.time = c->time;
+  h.nsteps = nsteps;
+  reset_slot(h, 0);
+  reset_slot(h, 1);
+  if (push_ctrl(c)) return PIP_ERR_CUDA;
+  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  for (int s = 0; s < nsteps; ++s) {
+    CK(cudaEventRecord(ev[3 * s], c->stream));
+    CK(c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 1, 0, c->stream));
+    CK(cudaEventRecord(ev[3 * s + 1], c->stream));
+    CK(c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 1, -1, c->stream));
+    CK(cudaEventRecord(ev[3 * s + 2], c->stream));
+  }
+  if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+  double t1 = 0.0, t2 = 0.0;
+  for (int s = 0; s < nsteps; ++s) {
+    float a = 0.f, b = 0.f;
+    CK(cudaEventElapsedTime(&a, ev[3 * s], ev[3 * s + 1]));
+    CK(cudaEventElapsedTime(&b, ev[3 * s + 1], ev[3 * s + 2]));
+    t1 += a;
+    t2 += b;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  c->time = h.time;
+  *ms1 = (float)(t1 / nsteps);
+  *ms2 = (float)(t2 / nsteps);
+  *msstep = (float)((t1 + t2) / nsteps);
+  return PIP_OK;
+}
+
+int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
+  (void)c;
+  return 1 + 2 * (nsteps > 0 ? nsteps : 0);
+}
+
+int pip_set_time(pip_ctx *c, double t) {
+  if (!c) return PIP_ERR_NULL;
+  c->time = t;
+  return PIP_OK;
+}
+
+int pip_get_time(pip_ctx *c, double *t) {
+  if (!c || !t) return PIP_ERR_NULL;
+  *t = c->time;
+  return PIP_OK;
+}
+
+int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
+  if (!c || !F_h || !F_m) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (dir < 1 || dir > c->kp.ndim) return PIP_ERR_PARAM;
+  if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
+  const size_t pb = c->plane_bytes();
+  CK(cudaMemsetAsync(c->scratch, 0, pb * c->nplanes(), c->stream));
+  CK(c->L->flux(c->kp, c->A, c->scratch, dir, c->cmax, c->stream));
+  CK(cudaMemcpyAsync(F_m, c->scratch, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(F_h, c->scratch + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
+  if (!c || !S_h || !S_m) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
+  const size_t pb = c->plane_bytes();
+  CK(c->L->source(c->kp, c->A, c->scratch, dt_coll, c->stream));
+  CK(cudaMemcpyAsync(S_m, c->scratch, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(S_h, c->scratch + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_fill_ghosts(pip_ctx *c) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(c->L->ghosts(c->kp, c->A, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_status(pip_ctx *c, int *stop_flag, int *nan_flag) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  int h = 0;
+  CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+  CK(c->L->nan_scan(c->kp, c->A, c->d_flag, c->stream));
+  CK(cudaMemcpyAsync(&h, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (nan_flag) *nan_flag = h;
+  if (stop_flag) *stop_flag = (h || c->last_dt <= 1.0e-12) ? 1 : 0;
+  return PIP_OK;
+}
+
+int pip_conduction(pip_ctx *c, double dt, int *iters, double *relres) {
+  (void)dt;
+  if (!c) return PIP_ERR_NULL;
+  if (iters) *iters = 0;
+  if (relres) *relres = 0.0;
+  return PIP_ERR_PARAM;  // flag_heat contexts are rejected at creation
+}
+
+int pip_last_cuda_error(void) { return g_last_cuda_error; }
+
+const char *pip_strerror(int code) {
+  switch (code) {
+    case PIP_OK: return "ok";
+    case PIP_ERR_PARAM: return "unsupported or inconsistent parameters";
+    case PIP_ERR_CUDA: return "CUDA runtime error";
+    case PIP_ERR_NAN: return "NaN in the state";
+    case PIP_ERR_DT: return "time step <= 1e-12";
+    case PIP_ERR_ITER: return "iteration limit reached";
+    case PIP_ERR_STATE: return "call out of order";
+    case PIP_ERR_NOMEM: return "device allocation failed";
+    case PIP_ERR_NULL: return "NULL argument";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

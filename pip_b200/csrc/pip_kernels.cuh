@@ -1,0 +1,65 @@
+// pip_kernels.cuh -- kernel parameter blocks shared by the FP64 kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pip {
+
+constexpr int kMaxMargin = 3;
+constexpr int kMaxPlanes = 14;   // 9 ion + 5 neutral
+
+// Scalars and tables of one simulation, passed by value to every kernel.
+struct KParams {
+  int ndim;          // 1 or 2
+  int ix, jx;        // array extents with ghosts
+  int nx, ny;        // interior extents
+  int m0, m1;        // ghost layers in x and y
+  int nvm;           // ion planes (8 or 9); neutral planes follow
+  int imp;           // exponential collision form
+  int ir;            // PIP_IR_POWERLAW active
+  int ir_type;       // IR energy form 1 or 2
+  long long nc;      // ix*jx
+  double gm, ro_lim, pr_lim, ac, safety;
+  double sg_all;     // safety*min over all dx, dy, dz (numerator of cmax)
+  double col_lim;    // min(safety,0.3) or pip_imp_factor (cfl_pn_col)
+  double ir_lim;     // min(safety,0.1) (cfl_pip_ir)
+  double ir_chi, ir_ion, ir_rec;
+  double decay[2];   // Dedner psi factor exp(-(dt_sub/dt)*safety*db_clean) per stage
+  double dz0;        // dz(1)
+  const double *dx, *dy;
+  // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]
+  int gx[2][kMaxMargin], gy[2][kMaxMargin];
+  signed char symx[2][kMaxPlanes], symy[2][kMaxPlanes];
+  int typex[2], typey[2];
+};
+
+// Device-resident loop state of pip_run (main.f90's time, dt and stop flags).
+struct DevCtrl {
+  double dt, cmax, time, time_next, t_end;
+  long long step, nsteps;
+  unsigned long long red_dt[2];   // min CFL candidate (positive doubles as ordered bits)
+  unsigned long long red_rho[2];  // max rho*alpha_c
+  unsigned long long red_gr[2];   // max IR rate
+  int last, done, nan_flag, status;
+  unsigned int blocks_done;       // last-block-done counter of the stage-2 kernel
+};
+
+// Host launchers (one set per arithmetic flavour: FMA-contracted or FMA-free).
+struct Launchers {
+  cudaError_t (*prepare)();
+  cudaError_t (*stage)(const KParams &p, int stage, const double *Us, const double *U0, double *Uo,
+                       DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s);
+  cudaError_t (*cfl)(const KParams &p, double *U, DevCtrl *ctrl, int slot, cudaStream_t s);
+  cudaError_t (*ghosts)(const KParams &p, double *U, cudaStream_t s);
+  cudaError_t (*flux)(const KParams &p, const double *U, double *F, int dir, double cmax,
+                      cudaStream_t s);
+  cudaError_t (*source)(const KParams &p, double *U, double *S, double dt_coll, cudaStream_t s);
+  cudaError_t (*nan_scan)(const KParams &p, const double *U, int *flag, cudaStream_t s);
+};
+
+const Launchers &launchers_fast();
+const Launchers &launchers_exact();
+
+}  // namespace pip

@@ -1,0 +1,811 @@
+// pip_step_impl.cuh -- FP64 kernels of the two-fluid step.  Included by pip_fp64_fast.cu
+// (FMA contraction on) and pip_fp64_exact.cu (-fmad=false, bitwise comparable with the
+// CPU restatement); PIP_FLAVOUR names the namespace and PIP_LAUNCHERS the table getter.
+//
+// Layout in HBM: one array of NV = nvm + 5 planes, each plane the Fortran
+// (ix,jx) slab with ghosts (x fastest): ion planes 0..nvm-1 (ro, mx, my, mz, en, bx, by,
+// bz[, psi]) then neutral planes nvm..nvm+4 (ro, mx, my, mz, en).  A step uses two such
+// arrays: A holds U0 and receives U2 in place, B receives U1.
+#pragma once
+
+#include "pip_kernels.cuh"
+#include "pip_physics.cuh"
+
+namespace pip {
+namespace PIP_FLAVOUR {
+
+constexpr int kH = 2;  // stencil half-width of minmod MUSCL
+
+template <int NDIM> struct Tile;
+template <> struct Tile<2> {
+  static constexpr int TX = 32, TY = 8, NT = 256;
+};
+template <> struct Tile<1> {
+  static constexpr int TX = 128, TY = 1, NT = 128;
+};
+
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double((long long)b);
+}
+
+// dt of the step from the reduced CFL terms (cfl, Scheme_rot.f90:183-213): the minimum
+// CFL candidate (seeded with cfl_mhd's 10.0), cfl_pn_col and cfl_pip_ir.
+__device__ __forceinline__ double finalize_dt(const KParams &p, const DevCtrl *c, int slot) {
+  double dt = bitsd(c->red_dt[slot]);
+  double rho = bitsd(c->red_rho[slot]);
+  dt = fmin(dt, p.col_lim / rho);
+  if (p.ir) dt = fmin(dt, p.ir_lim / fmax(bitsd(c->red_gr[slot]), 1.0e-5));
+  return dt;
+}
+
+// Ionisation/recombination rates of PIP_IR_POWERLAW from the ion state (get_Pr_MHD's
+// pressure with floor, Scheme_rot.f90:112-121; get_Te_MHD's temperature, :104-110).
+template <int NVM>
+__device__ __forceinline__ void ir_rates(const double (&u)[NVM], const KParams &p, double &gr,
+                                         double &gi) {
+  const double gm = p.gm;
+  double pr = (gm - 1.0) * (u[4] - 0.5 * ((u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] +
+                                          u[5] * u[5] + u[6] * u[6] + u[7] * u[7]));
+  pr = fmax(pr, p.pr_lim);
+  const double te = 0.5 * gm * (pr / u[0]);
+  const double rs = 1.0 / sqrt(te);
+  gr = p.ir_rec * rs;
+  gi = p.ir_ion * rs * exp(-p.ir_chi / te);
+}
+
+// Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
+// rewritten states um/uh and their primitives.
+template <int NVM>
+__device__ __forceinline__ void collision_ds(const double (&um)[NVM], const double (&uh)[5],
+                                             const Prim<double> &qm, const Prim<double> &qh,
+                                             const KParams &p, double dt_coll, double (&ds)[5]) {
+  const double gm = p.gm, ac = p.ac;
+  const double te = qm.pr / qm.de * gm * kMuP;
+  const double nte = qh.pr / qh.de * gm * kMuN;
+  ds[0] = 0.0;
+  if (p.imp) {
+    const double temp = dt_coll * (uh[0] + um[0]);
+    const double e = (1.0 - exp(-ac * temp));
+    ds[1] = (um[0] * uh[1] - uh[0] * um[1]) * e / temp;
+    ds[2] = (um[0] * uh[2] - uh[0] * um[2]) * e / temp;
+    ds[3] = (um[0] * uh[3] - uh[0] * um[3]) * e / temp;
+    const double nde = qh.de, de = qm.de;
+    const double lambda = ac * (nde + de);
+    const double kap = 3.0 * (gm - 1.0) * ac * (kMuP * nde + kMuN * de);
+    const double dvx = qh.vx - qm.vx, dvy = qh.vy - qm.vy, dvz = qh.vz - qm.vz;
+    // the ion term multiplies (nvz-vz) by nvz, as PIP_rot.f90:1348 does
+    const double B = -(1.0 / 3.0 * gm * kap / ((nde + de) * (kap - lambda)) *
+                       (de * (dvx * qm.vx + dvy * qm.vy + dvz * qh.vz) +
+                        nde * (dvx * qh.vx + dvy * qh.vy + dvz * qh.vz)));
+    const double D = -(gm / 6.0 * kap * (de - nde) / ((de + nde) * (kap - 2.0 * lambda)) *
+                       (dvx * dvx + dvy * dvy + dvz * dvz));
+    ds[4] = -((3.0 / gm) * ac * de * nde / kap *
+              (+(exp(-kap * dt_coll) - 1.0) * (nte - te) - (B + D) * exp(-kap * dt_coll) +
+               B * exp(-lambda * dt_coll) + D * exp(-2.0 * lambda * dt_coll)) /
+              dt_coll);
+  } else {
+    ds[1] = ac * (um[0] * uh[1] - uh[0] * um[1]);
+    ds[2] = ac * (um[0] * uh[2] - uh[0] * um[2]);
+    ds[3] = ac * (um[0] * uh[3] - uh[0] * um[3]);
+    ds[4] = ac * qh.de * qm.de *
+            (0.5 * ((qh.vx * qh.vx - qm.vx * qm.vx) + (qh.vy * qh.vy - qm.vy * qm.vy) +
+                    (qh.vz * qh.vz - qm.vz * qm.vz)) +
+             3.0 / gm / 2.0 * (nte - te));
+  }
+}
+
+// IR exchange of source_PIP (PIP_rot.f90:1370-1411, flag_IR_type 1 or 2).
+__device__ __forceinline__ void ir_ds(const Prim<double> &qm, const Prim<double> &qh, double gr,
+                                      double gi, const KParams &p, double (&ds)[5]) {
+  const double gm = p.gm;
+  ds[0] = gr * qm.de - gi * qh.de;
+  ds[1] = gr * qm.de * qm.vx - gi * qh.de * qh.vx;
+  ds[2] = gr * qm.de * qm.vy - gi * qh.de * qh.vy;
+  ds[3] = gr * qm.de * qm.vz - gi * qh.de * qh.vz;
+  const double kin = 0.5 * (gr * qm.de * (qm.vx * qm.vx + qm.vy * qm.vy + qm.vz * qm.vz) -
+                            gi * qh.de * (qh.vx * qh.vx + qh.vy * qh.vy + qh.vz * qh.vz));
+  if (p.ir_type == 1)
+    ds[4] = kin - gi * qh.pr / (gm - 1.0) + 0.5 * gr * qm.pr / (gm - 1.0);
+  else
+    ds[4] = kin - gi * qh.pr / (gm - 1.0) + gr * qm.pr / (gm - 1.0);
+}
+
+// Splits a cell's NV planes into ion and neutral arrays.
+template <int NVM>
+__device__ __forceinline__ void load_cell(const double *__restrict__ U, long long q, long long nc,
+                                          double (&um)[NVM], double (&uh)[5]) {
+#pragma unroll
+  for (int n = 0; n < NVM; ++n) um[n] = U[q + n * nc];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) uh[n] = U[q + (NVM + n) * nc];
+}
+
+// Writes a cell and every ghost cell the boundary conditions copy from it (PIPbnd after
+// the stage: x faces first, then y faces, Boundary_rot.f90:54-125 order, so a corner
+// ghost carries both sign flips).
+template <int NDIM, int NVM>
+__device__ __forceinline__ void store_cell(double *U, const KParams &p, int gi, int gj,
+                                           const double (&um)[NVM], const double (&uh)[5]) {
+  const long long nc = p.nc;
+  const long long q = (long long)gj * p.ix + gi;
+#pragma unroll
+  for (int n = 0; n < NVM; ++n) U[q + n * nc] = um[n];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) U[q + (NVM + n) * nc] = uh[n];
+  // ghost targets along x and y (at most 2*margin each)
+  int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
+  int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
+  for (int s = 0; s < 2; ++s)
+    for (int l = 0; l < p.m0; ++l)
+      if (p.gx[s][l] == gi) {
+        tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
+        sx[ntx] = s;
+        ++ntx;
+      }
+  if (NDIM == 2) {
+    for (int s = 0; s < 2; ++s)
+      for (int l = 0; l < p.m1; ++l)
+        if (p.gy[s][l] == gj) {
+          ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
+          sy[nty] = s;
+          ++nty;
+        }
+  }
+  for (int a = 0; a < ntx; ++a) {
+    const long long qg = (long long)gj * p.ix + tx[a];
+    const signed char *sg = p.symx[sx[a]];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) U[qg + n * nc] = (double)sg[n] * um[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[qg + (NVM + n) * nc] = (double)sg[NVM + n] * uh[n];
+    for (int b = 0; b < nty; ++b) {
+      const long long qc = (long long)ty[b] * p.ix + tx[a];
+      const signed char *sh = p.symy[sy[b]];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) U[qc + n * nc] = (double)sh[n] * ((double)sg[n] * um[n]);
+#pragma unroll
+      for (int n = 0; n < 5; ++n)
+        U[qc + (NVM + n) * nc] = (double)sh[NVM + n] * ((double)sg[NVM + n] * uh[n]);
+    }
+  }
+  for (int b = 0; b < nty; ++b) {
+    const long long qg = (long long)ty[b] * p.ix + gi;
+    const signed char *sh = p.symy[sy[b]];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) U[qg + n * nc] = (double)sh[n] * um[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[qg + (NVM + n) * nc] = (double)sh[NVM + n] * uh[n];
+  }
+}
+
+// Block-wide min/max into the reduction slots (one atomic per block).
+template <int NT>
+__device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double gr, DevCtrl *ctrl,
+                                                 int slot) {
+  __shared__ double s_red[3][NT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+    rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
+  }
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  if (l == 0) {
+    s_red[0][w] = dtc;
+    s_red[1][w] = rho;
+    s_red[2][w] = gr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NT / 32; ++k) {
+      dtc = fmin(dtc, s_red[0][k]);
+      rho = fmax(rho, s_red[1][k]);
+      gr = fmax(gr, s_red[2][k]);
+    }
+    // all values are positive (or +0), so the bit patterns order like the doubles
+    atomicMin(&ctrl->red_dt[slot], dbits(dtc));
+    atomicMax(&ctrl->red_rho[slot], dbits(rho));
+    atomicMax(&ctrl->red_gr[slot], dbits(gr));
+  }
+}
+
+// One RK stage of run_solver (Solver_rot.f90:59-71) fused into one kernel per tile:
+// u2v + get_Side minmod + HLLD/HLLC for every face of the tile (set_flux), the
+// collisional/IR source (set_source), add_flux_rk + add_source + Dedner decay
+// (time_integral) and the ghost fill (PIPbnd).  STAGE 2 optionally fuses the two cfl
+// calls that follow run_solver and open the next step (main.f90:47 and :36): epi = 1
+// applies one cq2pv rewrite; epi = 2 applies two and reduces the next dt; epi = -1 takes
+// 1 or 2 from the control block's last-step flag.
+template <int NDIM, int NVM, int STAGE>
+__global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
+stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
+             DevCtrl *ctrl, int dt_mode, int epi) {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
+  constexpr int NV = NVM + 5;
+  constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
+  constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
+  extern __shared__ double smem[];
+  double *sV = smem;
+  double *sFx = sV + NV * RR;
+  double *sFy = sFx + NV * NFX;
+  __shared__ double s_dt, s_cmax;
+  __shared__ long long s_step;
+  __shared__ int s_exit, s_epi;
+
+  const int tid = threadIdx.x;
+  const bool block0 = blockIdx.x == 0 && blockIdx.y == 0;
+  if (tid == 0) {
+    int ex = 0;
+    if (STAGE == 1) {
+      if (ctrl->done || ctrl->nan_flag) ex = 1;
+    } else {
+      if (ctrl->done) ex = 1;
+    }
+    double dt, cmax;
+    if (STAGE == 1 && dt_mode == 1) {
+      const long long st = ctrl->step;
+      dt = finalize_dt(p, ctrl, (int)(st & 1));
+      cmax = p.sg_all / dt;
+    } else {
+      dt = ctrl->dt;
+      cmax = ctrl->cmax;
+    }
+    s_dt = dt;
+    s_cmax = cmax;
+    s_step = ctrl->step;
+    s_exit = ex;
+    s_epi = (STAGE == 2 && epi < 0) ? (ctrl->last ? 1 : 2) : epi;
+  }
+  __syncthreads();
+  if (s_exit) {
+    if (STAGE == 1 && block0 && tid == 0) {
+      if (ctrl->nan_flag && ctrl->status == 0) ctrl->status = 3;  // PIP_ERR_NAN
+      ctrl->done = 1;
+    }
+    return;
+  }
+  const double dt = s_dt, cmax = s_cmax;
+  if (STAGE == 1 && dt_mode == 1 && block0 && tid == 0) {
+    // loop bookkeeping of main.f90:31,58 for this step
+    const long long st = ctrl->step;
+    ctrl->dt = dt;
+    ctrl->cmax = cmax;
+    const double tn = ctrl->time + dt;
+    ctrl->time_next = tn;
+    ctrl->last = ((ctrl->t_end > 0.0 && tn >= ctrl->t_end) ||
+                  (ctrl->nsteps > 0 && st + 1 >= ctrl->nsteps)) ? 1 : 0;
+    const int ns = (int)((st + 1) & 1);
+    ctrl->red_dt[ns] = dbits(10.0);
+    ctrl->red_rho[ns] = 0ull;
+    ctrl->red_gr[ns] = 0ull;
+  }
+
+  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
+  const int i0 = p.m0 + blockIdx.x * TX;
+  const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
+  const long long nc = p.nc;
+
+  // ---- 1. stage state of the tile and its halo -> primitives in shared memory
+  for (int idx = tid; idx < RR; idx += NT) {
+    const int ri = idx % RX, rj = idx / RX;
+    if (NDIM == 2 && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
+    const int gi = i0 - kH + ri, gj = NDIM == 2 ? j0 - kH + rj : 0;
+    if (gi >= p.ix || gj >= p.jx) continue;
+    double um[NVM], uh[5], vm[NVM], vh[5];
+    load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
+    u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
+    u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) sV[n * RR + idx] = vm[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+  }
+  __syncthreads();
+
+  // ---- 2. face fluxes (set_flux): x faces then y faces of the tile
+  const int iend = p.m0 + p.nx, jend = NDIM == 2 ? p.m1 + p.ny : 1;
+  for (int f = tid; f < NFX + NFY; f += NT) {
+    int a, s, perm_y;
+    double *Fout;
+    int fo, nf;
+    if (f < NFX) {
+      const int fi = f % (TX + 1), fj = f / (TX + 1);
+      if (i0 + fi - 1 >= iend || (NDIM == 2 && j0 + fj >= jend)) continue;
+      a = (NDIM == 2 ? (fj + kH) * RX : 0) + fi + kH - 1;  // left cell of the face
+      s = 1;
+      perm_y = 0;
+      Fout = sFx;
+      fo = f;
+      nf = NFX;
+    } else {
+      const int g = f - NFX, fi = g % TX, fj = g / TX;
+      if (i0 + fi >= iend || j0 + fj - 1 >= jend) continue;
+      a = (fj + kH - 1) * RX + fi + kH;  // lower cell of the face
+      s = RX;
+      perm_y = 1;
+      Fout = sFy;
+      fo = g;
+      nf = NFY;
+    }
+    {
+      double vl[NVM], vr[NVM], fx[NVM];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) {
+        // direction 2 swaps (vx,vy) and (bx,by) (set_HLLD_fluxes, HLL_rot.f90:365-383)
+        const int src = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        const double *v = sV + src * RR + a;
+        const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+        vl[n] = v1 + 0.5 * minmod<double>(v0, v1, v2);
+        vr[n] = v2 - 0.5 * minmod<double>(v1, v2, v3);
+      }
+      vl[0] = fmax(vl[0], ro_lim);
+      vr[0] = fmax(vr[0], ro_lim);
+      hlld_flux<double, NVM>(vl, vr, fx, gm, cmax);
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) {
+        const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        Fout[dst * nf + fo] = fx[n];
+      }
+    }
+    {
+      double vl[5], vr[5], fx[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        const int src = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
+        const double *v = sV + (NVM + src) * RR + a;
+        const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+        vl[n] = v1 + 0.5 * minmod<double>(v0, v1, v2);
+        vr[n] = v2 - 0.5 * minmod<double>(v1, v2, v3);
+      }
+      vl[0] = fmax(vl[0], ro_lim);
+      vr[0] = fmax(vr[0], ro_lim);
+      hllc_flux<double>(vl, vr, fx, gm);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
+        Fout[(NVM + dst) * nf + fo] = fx[n];
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- 3. per-cell source, update, epilogue
+  const int ti = tid % TX, tj = tid / TX;
+  const int gi = i0 + ti, gj = j0 + tj;
+  const bool valid = gi < iend && (NDIM == 1 || gj < jend);
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  if (valid) {
+    const long long q = (long long)gj * p.ix + gi;
+    const double dt_sub = STAGE == 1 ? dt / 2.0 : dt / 1.0;  // dt/(t_order-istep+1)
+    const double dt_coll = dt * 0.5;                          // set_dt_coll, t_order=2
+    double a_m[NVM], a_h[5];  // U0 of the cell
+    load_cell<NVM>(U0, q, nc, a_m, a_h);
+    double s_m[NVM], s_h[5];  // stage state of the cell
+    if (STAGE == 1) {
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) s_m[n] = a_m[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) s_h[n] = a_h[n];
+    } else {
+      load_cell<NVM>(Us, q, nc, s_m, s_h);
+    }
+    double gr = 0.0, gion = 0.0;
+    if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
+
+    // exponential form: U0 carries the collision increments of the earlier stages
+    if (p.imp && STAGE == 2) {
+      double r_m[NVM], r_h[5], ds[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) r_m[n] = a_m[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
+      const Prim<double> qh = cq2pv_hd<double>(r_h, gm, ro_lim, pr_lim);
+      const Prim<double> qm = cq2pv_mhd<double, NVM>(r_m, gm, ro_lim, pr_lim);
+      collision_ds<NVM>(r_m, r_h, qm, qh, p, dt_coll, ds);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        a_h[n] = a_h[n] - dt_coll * ds[n];
+        a_m[n] = a_m[n] + dt_coll * ds[n];
+      }
+    }
+    // source_PIP on the stage state (rewrites it through primitives first)
+    double S_m[5], S_h[5];
+    {
+      const Prim<double> qh = cq2pv_hd<double>(s_h, gm, ro_lim, pr_lim);
+      const Prim<double> qm = cq2pv_mhd<double, NVM>(s_m, gm, ro_lim, pr_lim);
+      double ds[5];
+      collision_ds<NVM>(s_m, s_h, qm, qh, p, dt_coll, ds);
+      if (p.imp) {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          a_h[n] = a_h[n] - dt_coll * ds[n];
+          a_m[n] = a_m[n] + dt_coll * ds[n];
+          S_h[n] = 0.0;
+          S_m[n] = 0.0;
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          S_h[n] = 0.0 - ds[n];
+          S_m[n] = 0.0 + ds[n];
+        }
+      }
+      if (p.ir) {
+        ir_ds(qm, qh, gr, gion, p, ds);
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          S_h[n] = S_h[n] + ds[n];
+          S_m[n] = S_m[n] - ds[n];
+        }
+      }
+    }
+    // time_integral: add_flux_rk (x, then y) and add_source, per species
+    const double cx = dt_sub / p.dx[gi];
+    const double cy = NDIM == 2 ? dt_sub / p.dy[gj] : 0.0;
+    const int fxl = tj * (TX + 1) + ti, fyl = tj * TX + ti;
+    double n_m[NVM], n_h[5];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const double u0 = n < NVM ? a_m[n] : a_h[n - NVM];
+      double u = u0 - cx * (sFx[n * NFX + fxl + 1] - sFx[n * NFX + fxl]);
+      if (NDIM == 2) u = u - cy * (sFy[n * NFY + fyl + TX] - sFy[n * NFY + fyl]);
+      if (n < NVM) {
+        u = n < 5 ? u + S_m[n] * dt_sub : u + 0.0;
+        n_m[n] = u;
+      } else {
+        n_h[n - NVM] = u + S_h[n - NVM] * dt_sub;
+      }
+    }
+    if (NVM == 9) n_m[NVM - 1] = n_m[NVM - 1] * p.decay[STAGE - 1];
+
+    // fused cfl rewrites (and the next step's CFL terms)
+    const int ep = s_epi;
+    if (ep >= 1) {
+      const Prim<double> qm = cq2pv_mhd<double, NVM>(n_m, gm, ro_lim, pr_lim);
+      const Prim<double> qh = cq2pv_hd<double>(n_h, gm, ro_lim, pr_lim);
+      (void)qm;
+      (void)qh;
+    }
+    if (ep == 2) {
+      const Prim<double> qm = cq2pv_mhd<double, NVM>(n_m, gm, ro_lim, pr_lim);
+      const Prim<double> qh = cq2pv_hd<double>(n_h, gm, ro_lim, pr_lim);
+      const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+      const double sg = p.safety * gmin;
+      dtc = fmin(cfl_mhd_cell<double>(qm, n_m[5], n_m[6], n_m[7], gm, sg),
+                 cfl_hd_cell<double>(qh, gm, sg));
+      rhoc = fmax(n_m[0] * p.ac, n_h[0] * p.ac);
+      if (p.ir) {
+        double g1, g2;
+        ir_rates<NVM>(n_m, p, g1, g2);
+        grc = fmax(g1, g2);
+      }
+    }
+    bool bad = false;
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) bad |= !isfinite(n_m[n]);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
+    if (bad) atomicOr(&ctrl->nan_flag, 1);
+    store_cell<NDIM, NVM>(Uo, p, gi, gj, n_m, n_h);
+  }
+  if (STAGE == 2 && s_epi == 2) {
+    block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
+  }
+  if (STAGE == 2 && dt_mode == 1) {
+    // end of step, done by the last block to finish (every block has read the control
+    // block by then): time += dt and stop_sim's dt check (main.f90:58-66, IO_rot.f90:636)
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const unsigned int nb = gridDim.x * gridDim.y;
+      if (atomicAdd(&ctrl->blocks_done, 1u) == nb - 1) {
+        __threadfence();
+        ctrl->blocks_done = 0u;
+        ctrl->time = ctrl->time_next;
+        ctrl->step = s_step + 1;
+        if (ctrl->last) ctrl->done = 1;
+        if (dt <= 1.0e-12) {
+          ctrl->done = 1;
+          if (ctrl->status == 0) ctrl->status = 4;  // PIP_ERR_DT
+        }
+      }
+    }
+  }
+}
+
+// cfl (Scheme_rot.f90:183-213) as a standalone pass over every cell: cq2pv rewrite of
+// both species in place, CFL candidates of interior cells, rho*alpha_c and IR maxima of all
+// cells into reduction slot `slot`.
+template <int NVM>
+__global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, DevCtrl *ctrl,
+                                                  int slot) {
+  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  const long long nc = p.nc;
+  for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
+    double um[NVM], uh[5];
+    load_cell<NVM>(U, q, nc, um, uh);
+    const Prim<double> qm = cq2pv_mhd<double, NVM>(um, gm, ro_lim, pr_lim);
+    const Prim<double> qh = cq2pv_hd<double>(uh, gm, ro_lim, pr_lim);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[q + n * nc] = um[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[q + (NVM + n) * nc] = uh[n];
+    const int i = (int)(q % p.ix), j = (int)(q / p.ix);
+    const bool interior = i >= p.m0 && i < p.ix - p.m0 && j >= p.m1 && j < p.jx - p.m1;
+    if (interior) {
+      const double gmin = fmin(fmin(p.dx[i], p.dy[j]), p.dz0);
+      const double sg = p.safety * gmin;
+      dtc = fmin(dtc, fmin(cfl_mhd_cell<double>(qm, um[5], um[6], um[7], gm, sg),
+                           cfl_hd_cell<double>(qh, gm, sg)));
+    }
+    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (p.ir) {
+      double g1, g2;
+      ir_rates<NVM>(um, p, g1, g2);
+      grc = fmax(grc, fmax(g1, g2));
+    }
+  }
+  block_reduce_cfl<256>(dtc, rhoc, grc, ctrl, slot);
+}
+
+// PIPbnd (Boundary_rot.f90:34-125): x ghost columns for every row, then (2D) y ghost rows
+// for every column; boundary_control types 1 (periodic), 2 (mirror with sign table) and
+// 10 (copy of the first interior layer).
+__global__ void ghosts_x_kernel(const KParams p, double *U, int nplanes) {
+  const long long nc = p.nc;
+  const int ng = 2 * p.m0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)ng * p.jx;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(t % ng), j = (int)(t / ng);
+    const int side = g / p.m0, l = g % p.m0;
+    const int dst = side == 0 ? l : p.ix - p.m0 + l;
+    const int src = p.gx[side][l];
+    for (int n = 0; n < nplanes; ++n) {
+      const double v = U[(long long)j * p.ix + src + n * nc];
+      U[(long long)j * p.ix + dst + n * nc] = p.typex[side] == 10 ? v : (double)p.symx[side][n] * v;
+    }
+  }
+}
+
+__global__ void ghosts_y_kernel(const KParams p, double *U, int nplanes) {
+  const long long nc = p.nc;
+  const int ng = 2 * p.m1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)ng * p.ix;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % p.ix), g = (int)(t / p.ix);
+    const int side = g / p.m1, l = g % p.m1;
+    const int dst = side == 0 ? l : p.jx - p.m1 + l;
+    const int src = p.gy[side][l];
+    for (int n = 0; n < nplanes; ++n) {
+      const double v = U[(long long)src * p.ix + i + n * nc];
+      U[(long long)dst * p.ix + i + n * nc] = p.typey[side] == 10 ? v : (double)p.symy[side][n] * v;
+    }
+  }
+}
+
+// set_flux for one direction, faces adjacent to interior cells only; F has NV planes.
+template <int NVM>
+__global__ void flux_kernel(const KParams p, const double *__restrict__ U, double *F, int dir,
+                            double cmax) {
+  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
+  const long long nc = p.nc;
+  const int ni = dir == 1 ? p.nx + 1 : p.nx;
+  const int nj = dir == 1 ? (p.ndim == 2 ? p.ny : 1) : p.ny + 1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)ni * nj;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int fi = (int)(t % ni), fj = (int)(t / ni);
+    int i, j;
+    long long s;
+    if (dir == 1) {
+      i = p.m0 - 1 + fi;
+      j = p.ndim == 2 ? p.m1 + fj : 0;
+      s = 1;
+    } else {
+      i = p.m0 + fi;
+      j = p.m1 - 1 + fj;
+      s = p.ix;
+    }
+    const long long qa = (long long)j * p.ix + i;
+    double V[4][NVM + 5];
+    for (int c = 0; c < 4; ++c) {
+      double um[NVM], uh[5], vm[NVM], vh[5];
+      load_cell<NVM>(U, qa + (c - 1) * s, nc, um, uh);
+      u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
+      u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
+      for (int n = 0; n < NVM; ++n) V[c][n] = vm[n];
+      for (int n = 0; n < 5; ++n) V[c][NVM + n] = vh[n];
+    }
+    const bool py = dir == 2;
+    {
+      double vl[NVM], vr[NVM], fx[NVM];
+      for (int n = 0; n < NVM; ++n) {
+        const int src = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        vl[n] = V[1][src] + 0.5 * minmod<double>(V[0][src], V[1][src], V[2][src]);
+        vr[n] = V[2][src] - 0.5 * minmod<double>(V[1][src], V[2][src], V[3][src]);
+      }
+      vl[0] = fmax(vl[0], ro_lim);
+      vr[0] = fmax(vr[0], ro_lim);
+      hlld_flux<double, NVM>(vl, vr, fx, gm, cmax);
+      for (int n = 0; n < NVM; ++n) {
+        const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        F[qa + dst * nc] = fx[n];
+      }
+    }
+    {
+      double vl[5], vr[5], fx[5];
+      for (int n = 0; n < 5; ++n) {
+        const int src = NVM + (py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n);
+        vl[n] = V[1][src] + 0.5 * minmod<double>(V[0][src], V[1][src], V[2][src]);
+        vr[n] = V[2][src] - 0.5 * minmod<double>(V[1][src], V[2][src], V[3][src]);
+      }
+      vl[0] = fmax(vl[0], ro_lim);
+      vr[0] = fmax(vr[0], ro_lim);
+      hllc_flux<double>(vl, vr, fx, gm);
+      for (int n = 0; n < 5; ++n) {
+        const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
+        F[qa + (NVM + dst) * nc] = fx[n];
+      }
+    }
+  }
+}
+
+// source_PIP over every cell (PIP_rot.f90:1309-1429): rewrites U and writes S (NV planes);
+// with the exponential form S receives the U0 increments (-/+ dt_coll*dS).
+template <int NVM>
+__global__ void source_kernel(const KParams p, double *U, double *S, double dt_coll) {
+  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
+  const long long nc = p.nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc;
+       q += (long long)gridDim.x * blockDim.x) {
+    double um[NVM], uh[5];
+    load_cell<NVM>(U, q, nc, um, uh);
+    double gr = 0.0, gion = 0.0;
+    if (p.ir) ir_rates<NVM>(um, p, gr, gion);
+    const Prim<double> qh = cq2pv_hd<double>(uh, gm, ro_lim, pr_lim);
+    const Prim<double> qm = cq2pv_mhd<double, NVM>(um, gm, ro_lim, pr_lim);
+    double ds[5], sm[5], sh[5];
+    collision_ds<NVM>(um, uh, qm, qh, p, dt_coll, ds);
+    for (int n = 0; n < 5; ++n) {
+      if (p.imp) {
+        sh[n] = 0.0 - dt_coll * ds[n];
+        sm[n] = 0.0 + dt_coll * ds[n];
+      } else {
+        sh[n] = 0.0 - ds[n];
+        sm[n] = 0.0 + ds[n];
+      }
+    }
+    if (p.ir) {
+      ir_ds(qm, qh, gr, gion, p, ds);
+      for (int n = 0; n < 5; ++n) {
+        sh[n] = sh[n] + ds[n];
+        sm[n] = sm[n] - ds[n];
+      }
+    }
+    for (int n = 0; n < 5; ++n) {
+      U[q + n * nc] = um[n];
+      U[q + (NVM + n) * nc] = uh[n];
+      S[q + n * nc] = sm[n];
+      S[q + (NVM + n) * nc] = sh[n];
+    }
+    for (int n = 5; n < NVM; ++n) S[q + n * nc] = 0.0;
+  }
+}
+
+__global__ void nan_kernel(const double *__restrict__ U, long long n, int *flag) {
+  int bad = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(U[t]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// ---------------------------------------------------------------- host launchers
+
+template <int NDIM, int NVM>
+constexpr size_t stage_smem_bytes() {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY;
+  constexpr int RR = (TX + 2 * kH) * (NDIM == 2 ? TY + 2 * kH : 1);
+  constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
+  return sizeof(double) * (NVM + 5) * (RR + NFX + NFY);
+}
+
+template <int NDIM, int NVM, int STAGE>
+static cudaError_t set_stage_attr() {
+  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)stage_smem_bytes<NDIM, NVM>());
+}
+
+// Raises the dynamic shared-memory limit of every stage-kernel instance on the current
+// device; called once per context so that graph capture sees launches only.
+static cudaError_t prepare() {
+  cudaError_t e;
+  if ((e = set_stage_attr<1, 8, 1>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<1, 8, 2>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<2, 8, 1>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<2, 8, 2>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr<2, 9, 1>()) != cudaSuccess) return e;
+  return set_stage_attr<2, 9, 2>();
+}
+
+template <int NDIM, int NVM, int STAGE>
+static cudaError_t launch_stage_t(const KParams &p, const double *Us, const double *U0, double *Uo,
+                                  DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
+  const size_t shm = stage_smem_bytes<NDIM, NVM>();
+  dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
+  stage_kernel<NDIM, NVM, STAGE><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_stage(const KParams &p, int stage, const double *Us, const double *U0,
+                                double *Uo, DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
+  if (p.ndim == 1) {
+    return stage == 1 ? launch_stage_t<1, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
+                      : launch_stage_t<1, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
+  }
+  if (p.nvm == 9)
+    return stage == 1 ? launch_stage_t<2, 9, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
+                      : launch_stage_t<2, 9, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
+  return stage == 1 ? launch_stage_t<2, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
+                    : launch_stage_t<2, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
+}
+
+static int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static cudaError_t launch_cfl(const KParams &p, double *U, DevCtrl *ctrl, int slot,
+                              cudaStream_t s) {
+  const int g = grid_for(p.nc, 256);
+  if (p.nvm == 9) cfl_kernel<9><<<g, 256, 0, s>>>(p, U, ctrl, slot);
+  else cfl_kernel<8><<<g, 256, 0, s>>>(p, U, ctrl, slot);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_ghosts(const KParams &p, double *U, cudaStream_t s) {
+  const int np = p.nvm + 5;
+  ghosts_x_kernel<<<grid_for(2ll * p.m0 * p.jx, 256), 256, 0, s>>>(p, U, np);
+  if (p.ndim == 2) ghosts_y_kernel<<<grid_for(2ll * p.m1 * p.ix, 256), 256, 0, s>>>(p, U, np);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_flux(const KParams &p, const double *U, double *F, int dir, double cmax,
+                               cudaStream_t s) {
+  const long long n = (long long)(p.nx + 1) * (p.ndim == 2 ? p.ny + 1 : 1);
+  if (p.nvm == 9) flux_kernel<9><<<grid_for(n, 128), 128, 0, s>>>(p, U, F, dir, cmax);
+  else flux_kernel<8><<<grid_for(n, 128), 128, 0, s>>>(p, U, F, dir, cmax);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_source(const KParams &p, double *U, double *S, double dt_coll,
+                                 cudaStream_t s) {
+  if (p.nvm == 9) source_kernel<9><<<grid_for(p.nc, 128), 128, 0, s>>>(p, U, S, dt_coll);
+  else source_kernel<8><<<grid_for(p.nc, 128), 128, 0, s>>>(p, U, S, dt_coll);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_nan(const KParams &p, const double *U, int *flag, cudaStream_t s) {
+  const long long n = p.nc * (p.nvm + 5);
+  nan_kernel<<<grid_for(n, 256), 256, 0, s>>>(U, n, flag);
+  return cudaGetLastError();
+}
+
+}  // namespace PIP_FLAVOUR
+
+const Launchers &PIP_LAUNCHERS() {
+  static const Launchers L = {PIP_FLAVOUR::prepare,       PIP_FLAVOUR::launch_stage,
+                              PIP_FLAVOUR::launch_cfl,    PIP_FLAVOUR::launch_ghosts,
+                              PIP_FLAVOUR::launch_flux,   PIP_FLAVOUR::launch_source,
+                              PIP_FLAVOUR::launch_nan};
+  return L;
+}
+
+}  // namespace pip

@@ -1,0 +1,322 @@
+"""Parameter block of the PIP two-fluid step (mirror of ``pip_params`` in include/pip_gpu.h).
+
+``Settings`` reads a PIP ``setting.txt`` the way ``get_parameters`` does
+(Model_rot.f90:39-253, lines of the form ``value:key;comment`` split by ``get_word``,
+Util_rot.f90:5-12), derives the sizes (Model_rot.f90:254-333) and builds the uniform grid
+of ``set_coordinate`` (Model_rot.f90:394-458).  ``Settings.to_params()`` returns the
+ctypes structure the C ABI takes.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import List, Tuple
+
+import numpy as np
+
+PIP_ABI_VERSION = 1
+PIP_FP64 = 0
+PIP_MIXED = 1
+PIP_IR_NONE = 0
+PIP_IR_POWERLAW = 5
+
+# boundary codes the C ABI accepts (boundary_control types 1, 2 and 10, and the codes
+# MHDbnd/HDbnd map onto type 2, Boundary_rot.f90:62-80)
+SUPPORTED_BND = (1, 2, 3, 4, 5, 6, 7, 10, 11)
+
+
+class PipParams(ctypes.Structure):
+    """ctypes mirror of ``struct pip_params`` (field order and types must match)."""
+
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("ix", ctypes.c_int32),
+        ("jx", ctypes.c_int32),
+        ("kx", ctypes.c_int32),
+        ("margin", ctypes.c_int32 * 3),
+        ("nvar_h", ctypes.c_int32),
+        ("nvar_m", ctypes.c_int32),
+        ("flag_sch", ctypes.c_int32),
+        ("flag_hll", ctypes.c_int32),
+        ("s_order", ctypes.c_int32),
+        ("t_order", ctypes.c_int32),
+        ("flag_time", ctypes.c_int32),
+        ("flag_divb", ctypes.c_int32),
+        ("flag_col", ctypes.c_int32),
+        ("flag_pip_imp", ctypes.c_int32),
+        ("flag_ir", ctypes.c_int32),
+        ("flag_ir_type", ctypes.c_int32),
+        ("flag_heat", ctypes.c_int32),
+        ("hc_max", ctypes.c_int32),
+        ("flag_bnd", ctypes.c_int32 * 6),
+        ("precision", ctypes.c_int32),
+        ("fp_exact", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 6),
+        ("gm", ctypes.c_double),
+        ("safety", ctypes.c_double),
+        ("ro_lim", ctypes.c_double),
+        ("pr_lim", ctypes.c_double),
+        ("col", ctypes.c_double),
+        ("db_clean", ctypes.c_double),
+        ("pip_imp_factor", ctypes.c_double),
+        ("t_ir", ctypes.c_double),
+        ("ir_chi", ctypes.c_double),
+        ("ir_ion_coef", ctypes.c_double),
+        ("ir_rec_coef", ctypes.c_double),
+        ("kapper", ctypes.c_double),
+        ("hc_error", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 7),
+        ("dx", ctypes.POINTER(ctypes.c_double)),
+        ("dy", ctypes.POINTER(ctypes.c_double)),
+        ("dz", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+def get_word(line: str) -> Tuple[str, str]:
+    """``get_word`` (Util_rot.f90:5-12): key between ':' and ';', value before ':'."""
+    ind_s = line.find(":")
+    ind_e = line.find(";")
+    if ind_s < 0:
+        return "", ""
+    key = line[ind_s + 1: ind_e if ind_e >= 0 else len(line)].strip()
+    return key, line[:ind_s].strip()
+
+
+def _fortran_real(text: str) -> float:
+    # list-directed read accepts 1.d0 / 1.0e-3 / 0001.d0
+    return float(text.strip().lower().replace("d", "e"))
+
+
+@dataclasses.dataclass
+class Settings:
+    """The subset of ``globalvar`` the two-fluid step reads, with PIP's defaults."""
+
+    flag_eqs: str = "PIP"
+    ndim: int = 1
+    ix0: int = 64               # interior cells (setting.txt ``ix``)
+    jx0: int = 1
+    kx0: int = 1
+    gm_d: float = 5.0
+    gm_n: float = 3.0
+    safety: float = 0.3
+    flag_sch: int = 0
+    flag_hll: int = 2
+    s_order: int = 2
+    t_order: int = 2
+    flag_time: int = 0
+    flag_divb: int = 0
+    db_clean: float = 0.7
+    ro_lim: float = 1.0e-8
+    pr_lim: float = 1.0e-8
+    flag_bnd: List[int] = dataclasses.field(default_factory=lambda: [10, 10, 10, 10, 10, 10])
+    n_fraction: float = 0.5
+    col: float = 100.0
+    flag_col: int = 1
+    flag_pip_imp: int = 0
+    pip_imp_factor: float = 10.0
+    flag_ir: int = 0
+    flag_ir_type: int = 1
+    t_ir: float = 1.0
+    ir_chi: float = 5.0
+    ir_ion_coef: float = 0.0
+    ir_rec_coef: float = 0.0
+    flag_heat: int = 0
+    kapper: float = 0.0
+    hc_max: int = 500
+    hc_error: float = 1.0e-10
+    flag_resi: int = 0
+    flag_amb: int = 0
+    flag_visc: int = 0
+    flag_grav: int = 0
+    tend: float = -1.0
+    precision: int = PIP_FP64
+    fp_exact: int = 0
+    start: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    end: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+
+    # ---------------------------------------------------------------- derived values
+    @property
+    def gm(self) -> float:
+        return self.gm_d / float(self.gm_n)
+
+    @property
+    def margin(self) -> Tuple[int, int, int]:
+        """Ghost layers (Model_rot.f90:282-289,319-330), HLL branch."""
+        m = self.s_order + min(self.flag_resi, 1) + min(self.flag_amb, 1)
+        if self.flag_heat >= 1:
+            m += 1
+        if self.ndim == 1:
+            return (m, 0, 0)
+        if self.ndim == 2:
+            return (m, m, 0)
+        return (m, m, m)
+
+    @property
+    def divb(self) -> int:
+        return 0 if self.ndim == 1 else self.flag_divb   # Model_rot.f90:309
+
+    @property
+    def nvar_m(self) -> int:
+        return 8 + (1 if self.divb in (1, 2) else 0)
+
+    @property
+    def nvar_h(self) -> int:
+        return 5
+
+    @property
+    def shape(self) -> Tuple[int, int, int]:
+        """(ix, jx, kx) including ghosts (Model_rot.f90:331-333)."""
+        m = self.margin
+        jx0 = self.jx0 if self.ndim >= 2 else 1
+        kx0 = self.kx0 if self.ndim >= 3 else 1
+        return (self.ix0 + 2 * m[0], jx0 + 2 * m[1], kx0 + 2 * m[2])
+
+    # ---------------------------------------------------------------- grid
+    def coordinates(self):
+        """``set_coordinate`` (Model_rot.f90:394-458) for one rank: returns
+        (x, y, z, dx, dy, dz) with the cumulative-sum construction of the reference."""
+        ix, jx, kx = self.shape
+        m = self.margin
+        start = list(self.start)
+        end = list(self.end)
+        if self.ndim <= 2:
+            start[2] = 0.0
+            end[2] = 0.0
+            if self.ndim <= 1:
+                start[1] = 0.0
+                end[1] = 0.0
+        dr = [(end[0] - start[0]) / (ix - 2 * m[0]),
+              (end[1] - start[1]) / (jx - 2 * m[1]),
+              (end[2] - start[2]) / (kx - 2 * m[2])]
+        dx = np.full(ix, dr[0])
+        dy = np.full(jx, dr[1])
+        dz = np.full(kx, dr[2])
+        if self.ndim <= 2:
+            dz[0] = 100.0
+            if self.ndim <= 1:
+                dy[0] = 100.0
+        out = []
+        for n, (n_cells, d) in enumerate(((ix, dx), (jx, dy), (kx, dz))):
+            c = np.zeros(n_cells)
+            z0 = m[n]                       # Fortran zeros(n) = margin+1, 0-based margin
+            c[z0] = start[n] + 0.5 * dr[n]
+            for i in range(z0 + 1, n_cells):
+                c[i] = c[i - 1] + d[i - 1]
+            for i in range(z0 - 1, -1, -1):
+                c[i] = c[i + 1] - d[i]
+            out.append(c)
+        return out[0], out[1], out[2], dx, dy, dz
+
+    # ---------------------------------------------------------------- checks
+    def validate(self) -> None:
+        """Raise ValueError for settings outside the supported two-fluid path."""
+        bad = []
+        if self.flag_eqs != "PIP":
+            bad.append("flag_eqs must be PIP (two-fluid)")
+        if self.ndim not in (1, 2):
+            bad.append("ndim must be 1 or 2")
+        if self.flag_sch != 0 or self.flag_hll != 2:
+            bad.append("only flag_sch=0, flag_hll=2 (HLLD/HLLC) is supported")
+        if self.s_order != 2 or self.t_order != 2 or self.flag_time != 0:
+            bad.append("only s_order=2, t_order=2, flag_time=0 is supported")
+        if self.flag_col != 1:
+            bad.append("only flag_col=1 (constant alpha_c) is supported")
+        if self.flag_resi or self.flag_amb or self.flag_visc or self.flag_grav:
+            bad.append("resistivity, ambipolar, viscosity and gravity are not supported")
+        if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW):
+            bad.append("flag_ir must be 0 or %d" % PIP_IR_POWERLAW)
+        if self.flag_ir and self.flag_ir_type not in (1, 2):
+            bad.append("flag_ir_type must be 1 or 2")
+        for f in range(2 * self.ndim):
+            if self.flag_bnd[f] not in SUPPORTED_BND:
+                bad.append("flag_bnd[%d]=%d unsupported" % (f, self.flag_bnd[f]))
+        if bad:
+            raise ValueError("; ".join(bad))
+
+    # ---------------------------------------------------------------- C struct
+    def to_params(self) -> Tuple[PipParams, tuple]:
+        """Return (PipParams, keepalive) where keepalive holds the dx/dy/dz buffers."""
+        ix, jx, kx = self.shape
+        _, _, _, dx, dy, dz = self.coordinates()
+        dx = np.ascontiguousarray(dx, dtype=np.float64)
+        dy = np.ascontiguousarray(dy, dtype=np.float64)
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        p = PipParams()
+        p.abi_version = PIP_ABI_VERSION
+        p.ndim = self.ndim
+        p.ix, p.jx, p.kx = ix, jx, kx
+        for n, m in enumerate(self.margin):
+            p.margin[n] = m
+        p.nvar_h = self.nvar_h
+        p.nvar_m = self.nvar_m
+        p.flag_sch = self.flag_sch
+        p.flag_hll = self.flag_hll
+        p.s_order = self.s_order
+        p.t_order = self.t_order
+        p.flag_time = self.flag_time
+        p.flag_divb = self.divb
+        p.flag_col = self.flag_col
+        p.flag_pip_imp = self.flag_pip_imp
+        p.flag_ir = self.flag_ir
+        p.flag_ir_type = self.flag_ir_type
+        p.flag_heat = self.flag_heat
+        p.hc_max = self.hc_max
+        for n in range(6):
+            p.flag_bnd[n] = self.flag_bnd[n]
+        p.precision = self.precision
+        p.fp_exact = self.fp_exact
+        p.gm = self.gm
+        p.safety = self.safety
+        p.ro_lim = self.ro_lim
+        p.pr_lim = self.pr_lim
+        p.col = self.col
+        p.db_clean = self.db_clean
+        p.pip_imp_factor = self.pip_imp_factor
+        p.t_ir = self.t_ir
+        p.ir_chi = self.ir_chi
+        p.ir_ion_coef = self.ir_ion_coef
+        p.ir_rec_coef = self.ir_rec_coef
+        p.kapper = self.kapper
+        p.hc_error = self.hc_error
+        dptr = ctypes.POINTER(ctypes.c_double)
+        p.dx = dx.ctypes.data_as(dptr)
+        p.dy = dy.ctypes.data_as(dptr)
+        p.dz = dz.ctypes.data_as(dptr)
+        return p, (dx, dy, dz)
+
+    # ---------------------------------------------------------------- setting.txt
+    @classmethod
+    def from_setting_text(cls, text: str) -> "Settings":
+        """Parse ``setting.txt`` content like ``get_parameters`` (Model_rot.f90:39-253)."""
+        s = cls()
+        ints = {"ndim": "ndim", "ix": "ix0", "jx": "jx0", "kx": "kx0",
+                "flag_sch": "flag_sch", "s_order": "s_order", "t_order": "t_order",
+                "flag_divb": "flag_divb", "flag_pip_imp": "flag_pip_imp",
+                "flag_col": "flag_col", "flag_IR": "flag_ir", "flag_IR_type": "flag_ir_type",
+                "flag_heat": "flag_heat", "hc_max": "hc_max", "flag_hll": "flag_hll",
+                "flag_time": "flag_time", "flag_resi": "flag_resi", "flag_amb": "flag_amb",
+                "flag_visc": "flag_visc", "flag_grav": "flag_grav"}
+        reals = {"gm_d": "gm_d", "gm_n": "gm_n", "safety": "safety", "db_clean": "db_clean",
+                 "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
+                 "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",
+                 "kapper": "kapper", "tend": "tend"}
+        bnd = {"flag_bnd_x_l": 0, "flag_bnd_x_r": 1, "flag_bnd_y_l": 2, "flag_bnd_y_r": 3,
+               "flag_bnd_z_l": 4, "flag_bnd_z_r": 5}
+        for raw in text.splitlines():
+            key, val = get_word(raw)
+            if not key:
+                continue
+            if key == "flag_eqs":
+                s.flag_eqs = val.strip()
+            elif key in ints:
+                setattr(s, ints[key], int(_fortran_real(val)))
+            elif key in reals:
+                setattr(s, reals[key], _fortran_real(val))
+            elif key in bnd:
+                s.flag_bnd[bnd[key]] = int(_fortran_real(val))
+        return s
+
+    def overrides(self, **kw) -> "Settings":
+        return dataclasses.replace(self, **kw)
+
