@@ -8,14 +8,16 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-* value: cell-updates/s = interior cells x steps / device time (CUDA events on the
-  library's stream around the device loop, state resident in HBM; the two state arrays
-  (2 x 118 MB) exceed the 126 MB L2, so no flush between steps).
+* value: cell-updates/s of the FP32-mixed form = interior cells x steps / device time
+  (CUDA events on the library's stream around the device loop, state resident in HBM; the
+  state arrays exceed the 126 MB L2, so no flush between steps).  The plain FP64 path is
+  timed the same way ("fp64"), and the relative L1 error of the mixed state against the
+  FP64 state after the same steps is reported per variable.
 * e2e: the same metric through the public C ABI with pinned host buffers:
   pip_upload + pip_run + pip_download, copies inside the timed region.
 * roofline: the stage-2 kernel (the heavier of the two per-step kernels) against the
-  measured HBM copy bandwidth; algorithmic bytes per cell of that kernel = read U1 and U0,
-  write U2 = 3 x 14 x 8 B.
+  measured HBM copy bandwidth; algorithmic bytes per cell of that kernel: FP64 read U1 and
+  U0, write U2 = 3 x 14 x 8 B; mixed read U1, U0.hi, U0.lo, write U2.hi, U2.lo = 14 x 20 B.
 * cpu_baseline: the CPU restatement on all host cores, bounded sample of the same workload.
 * --impl reference: the reference's own algorithm on host cores (the reference is Fortran +
   MPI + HDF5 and cannot be built on this image; its CPU restatement runs instead).
@@ -42,6 +44,9 @@ WORKLOAD = ("2D two-fluid Orszag-Tang vortex 1024x1024 (+2 ghosts), periodic, 90
             "by mass, alpha_c=1e3, gamma=5/3, Dedner psi, CFL 0.3, minmod-MUSCL + HLLD/HLLC, RK2")
 FP64_BYTES_PER_CELL_STEP = 5 * 14 * 8     # stage 1: R U0 + W U1; stage 2: R U1, U0 + W U2
 FP64_BYTES_PER_CELL_STAGE2 = 3 * 14 * 8
+# mixed: stage 1 R hi + W U1 (4+4 B); stage 2 R U1, hi, lo + W hi, lo (5 x 4 B), per plane
+MIXED_BYTES_PER_CELL_STEP = 14 * (8 + 20)
+MIXED_BYTES_PER_CELL_STAGE2 = 14 * 20
 
 
 def measured_peaks():
@@ -192,6 +197,67 @@ def run_reference(args):
     return 0
 
 
+def measure(n, precision, steps, warmup, dist, local):
+    """Device-resident timing of one precision form on OT n x n: returns timings, the
+    state after warmup+steps steps and per-kernel durations."""
+    import torch
+    from pip_b200 import capi, ics
+    s, Uh, Um = ics.orszag_tang(n, precision=precision)
+    ctx = capi.Context(s)
+    ctx.upload(Uh, Um)
+    ctx.prologue()
+    ctx.run(nsteps=warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        st, t, nstep, ms = ctx.run_timed(nsteps=steps)
+    torch.cuda.synchronize()
+    if st != 0 or nstep != steps:
+        raise RuntimeError("timed run ended with status %d after %d steps" % (st, nstep))
+    state = ctx.download()
+    launches = ctx.kernels_per_run(steps)
+    ms1, ms2, msstep = ctx.stage_ms(min(200, steps))
+    ctx.close()
+    return dict(ms=ms, state=state, launches=launches, clocks=clk.summary(), ms1=ms1, ms2=ms2,
+                msstep=msstep, settings=s, U=(Uh, Um))
+
+
+def e2e_run(s, Uh, Um, steps, warmup, dist):
+    """pip_upload (pinned host) + pip_run + pip_download through the C ABI, wall clock."""
+    import torch
+    from pip_b200 import capi
+    pin = lambda a: torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+    ph, pm, oh, om = pin(Uh), pin(Um), pin(Uh), pin(Um)
+    ph[...] = Uh
+    pm[...] = Um
+    ctx = capi.Context(s)
+    ctx.upload(ph, pm)
+    ctx.run(nsteps=warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.upload(ph, pm)
+    ctx.run(nsteps=steps)
+    ctx.download(oh, om)
+    e2e_s = time.perf_counter() - t0
+    ctx.close()
+    return e2e_s, Uh.nbytes + Um.nbytes
+
+
+def rel_l1_interior(a, b, m):
+    import numpy as np
+    out = []
+    for x, y in zip(a, b):
+        xi = x[:, m:-m, m:-m].reshape(x.shape[0], -1)
+        yi = y[:, m:-m, m:-m].reshape(y.shape[0], -1)
+        num = np.abs(xi - yi).sum(axis=1)
+        den = np.abs(yi).sum(axis=1)
+        out.append(np.where(den > 0, num / np.where(den > 0, den, 1.0), num))
+    return np.concatenate(out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,8 +272,8 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
 
-    import numpy as np
     import torch
+    from pip_b200.params import PIP_FP64, PIP_MIXED
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -221,72 +287,35 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    from pip_b200 import build, capi, ics
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        tt = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    from pip_b200 import build
     build.build()
     n = args.n
     cells = n * n
-    s, Uh, Um = ics.orszag_tang(n)
-
-    # ---------------------------------------------------------------- device-resident value
-    ctx = capi.Context(s)
-    ctx.upload(Uh, Um)
-    ctx.prologue()
-    ctx.run(nsteps=args.warmup)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        st, t, nstep, ms = ctx.run_timed(nsteps=args.steps)
-    torch.cuda.synchronize()
-    if st != 0 or nstep != args.steps:
-        raise RuntimeError("timed run ended with status %d after %d steps" % (st, nstep))
-    ms_max = ms
-    if dist:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_max = float(tt.item())
-    value = world * cells * args.steps / (ms_max * 1e-3)
-    launches = ctx.kernels_per_run(args.steps)
-
-    # ---------------------------------------------------------------- per-kernel roofline
-    nk = min(200, args.steps)
-    ms1, ms2, msstep = ctx.stage_ms(nk)
+    f64 = measure(n, PIP_FP64, args.steps, args.warmup, dist, local)
+    mix = measure(n, PIP_MIXED, args.steps, args.warmup, dist, local)
+    l1 = rel_l1_interior(mix["state"], f64["state"], 2)
+    ms64 = max_over_ranks(f64["ms"])
+    msmx = max_over_ranks(mix["ms"])
+    v64 = world * cells * args.steps / (ms64 * 1e-3)
+    vmx = world * cells * args.steps / (msmx * 1e-3)
     peak, peak_kind = measured_peaks()
-    achieved2 = FP64_BYTES_PER_CELL_STAGE2 * cells / (ms2 * 1e-3) / 1e9
-    traffic = ncu_traffic("stage2_fp64_ot1024")
-    ctx.close()
-
-    # ---------------------------------------------------------------- e2e through the C ABI
-    shape_h, shape_m = Uh.shape, Um.shape
-    ph = torch.empty(shape_h, dtype=torch.float64, pin_memory=True).numpy()
-    pm = torch.empty(shape_m, dtype=torch.float64, pin_memory=True).numpy()
-    ph[...] = Uh
-    pm[...] = Um
-    oh = torch.empty(shape_h, dtype=torch.float64, pin_memory=True).numpy()
-    om = torch.empty(shape_m, dtype=torch.float64, pin_memory=True).numpy()
-    ctx = capi.Context(s)
-    ctx.upload(ph, pm)
-    ctx.run(nsteps=args.warmup)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ctx.upload(ph, pm)
-    ctx.run(nsteps=args.steps)
-    ctx.download(oh, om)
-    e2e_s = time.perf_counter() - t0
-    ctx.close()
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    state_bytes = (Uh.nbytes + Um.nbytes)
+    a64 = FP64_BYTES_PER_CELL_STAGE2 * cells / (f64["ms2"] * 1e-3) / 1e9
+    amx = MIXED_BYTES_PER_CELL_STAGE2 * cells / (mix["ms2"] * 1e-3) / 1e9
+    e2e_s, state_bytes = e2e_run(mix["settings"], mix["U"][0], mix["U"][1], args.steps,
+                                 args.warmup, dist)
+    e2e_s = max_over_ranks(e2e_s)
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps,
-           "how": "pip_upload (pinned host) + pip_run(%d steps) + pip_download, wall clock "
-                  "around the synchronous C ABI calls" % args.steps}
-
+           "how": "FP32-mixed: pip_upload (pinned FP64 host arrays) + pip_run(%d steps) + "
+                  "pip_download, wall clock around the synchronous C ABI calls" % args.steps}
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -296,23 +325,36 @@ def main():
         cpu = cpu_sample()
         cpu.pop("s_per_step", None)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": cells, "precision": "fp64 (plain drop-in path)",
-                   "l2": "inputs larger than L2 (2 x %.0f MB state arrays vs 126 MB L2)"
-                         % (state_bytes / 1e6),
+        "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64-mixed", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": cells,
+                   "precision": "FP32-mixed (FP32 fluxes/state, FP64 source and compensated "
+                                "RK accumulation)",
+                   "l2": "inputs larger than L2 (FP64 state 2 x %.0f MB, mixed 3 x %.0f MB vs "
+                         "126 MB L2)" % (state_bytes / 1e6, state_bytes / 2e6),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "achieved": achieved2, "peak": peak, "unit": "GB/s",
-                     "frac": achieved2 / peak, "traffic": traffic,
-                     "kernel": "stage_kernel<2,9,2> (stage 2: fluxes+source+update+2x cfl)",
-                     "algorithmic_bytes_per_cell": FP64_BYTES_PER_CELL_STAGE2,
-                     "peak_kind": peak_kind, "ms_stage1": ms1, "ms_stage2": ms2,
-                     "step_achieved_gbs": FP64_BYTES_PER_CELL_STEP * cells / (msstep * 1e-3) / 1e9},
+        "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
+                 "roofline": {"bound": "hbm", "achieved": a64, "peak": peak, "unit": "GB/s",
+                              "frac": a64 / peak,
+                              "traffic": ncu_traffic("stage2_fp64_ot1024"),
+                              "algorithmic_bytes_per_cell": FP64_BYTES_PER_CELL_STAGE2,
+                              "ms_stage1": f64["ms1"], "ms_stage2": f64["ms2"]},
+                 "gpu_launches": f64["launches"], "clocks": f64["clocks"]},
+        "mixed_over_fp64": vmx / v64,
+        "l1_mixed_vs_fp64": {"max": float(l1.max()), "per_variable": [float(x) for x in l1],
+                             "variables": "ion ro,mx,my,mz,en,bx,by,bz,psi; neutral ro,mx,my,mz,en",
+                             "after_steps": args.warmup + args.steps},
+        "roofline": {"bound": "hbm", "achieved": amx, "peak": peak, "unit": "GB/s",
+                     "frac": amx / peak, "traffic": ncu_traffic("stage2_mixed_ot1024"),
+                     "kernel": "mixed stage_kernel<2,9,2> (stage 2: fluxes+source+update+cfl)",
+                     "algorithmic_bytes_per_cell": MIXED_BYTES_PER_CELL_STAGE2,
+                     "peak_kind": peak_kind, "ms_stage1": mix["ms1"], "ms_stage2": mix["ms2"],
+                     "step_achieved_gbs": MIXED_BYTES_PER_CELL_STEP * cells / (mix["msstep"] * 1e-3) / 1e9},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "gpu_launches": mix["launches"],
+        "clocks": mix["clocks"],
     }
     print(json.dumps(line), flush=True)
     if dist:

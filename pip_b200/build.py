@@ -22,6 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 EXTRA_FLAGS = {
     "pip_fp64_exact.cu": ["-fmad=false"],
+    "pip_mixed.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
 }
 
 

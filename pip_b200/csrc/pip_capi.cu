@@ -29,7 +29,9 @@ struct pip_ctx {
   const pip::Launchers *L = nullptr;
   int device = 0;
   cudaStream_t stream = nullptr;
-  double *A = nullptr, *B = nullptr;  // NV planes each
+  double *A = nullptr, *B = nullptr;  // NV planes each (FP64 form; A stages the mixed form)
+  float *Ahi = nullptr, *Alo = nullptr, *Bf = nullptr;  // FP32-mixed form
+  bool mixed = false;
   double *d_dx = nullptr, *d_dy = nullptr;
   double *scratch = nullptr;          // NV planes for pip_flux / pip_source
   int *d_flag = nullptr;
@@ -131,7 +133,7 @@ int validate(const pip_params *p) {
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
-  if (p->precision != PIP_FP64) return PIP_ERR_PARAM;
+  if (p->precision != PIP_FP64 && p->precision != PIP_MIXED) return PIP_ERR_PARAM;
   if (p->flag_heat != 0) return PIP_ERR_PARAM;
   const int m0 = p->margin[0], m1 = p->margin[1];
   if (m0 < 2 || m0 > pip::kMaxMargin || p->margin[2] != 0) return PIP_ERR_PARAM;
@@ -236,11 +238,39 @@ int push_ctrl(pip_ctx *c) {
   return PIP_OK;
 }
 
+// One RK stage of the context's precision form.
+cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
+  if (c->mixed) {
+    if (stage == 1)
+      return pip::mixed_stage(c->kp, 1, c->Ahi, c->Ahi, nullptr, c->Bf, nullptr, c->ctrl, dt_mode,
+                              epi, c->stream);
+    return pip::mixed_stage(c->kp, 2, c->Bf, c->Ahi, c->Alo, c->Ahi, c->Alo, c->ctrl, dt_mode, epi,
+                            c->stream);
+  }
+  if (stage == 1) return c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, dt_mode, epi, c->stream);
+  return c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, dt_mode, epi, c->stream);
+}
+
+cudaError_t do_cfl(pip_ctx *c, int slot) {
+  if (c->mixed) return pip::mixed_cfl(c->kp, c->Ahi, c->Alo, c->ctrl, slot, c->stream);
+  return c->L->cfl(c->kp, c->A, c->ctrl, slot, c->stream);
+}
+
+// The mixed form keeps its state in (hi, lo); these move it through the FP64 array A.
+cudaError_t to_fp64(pip_ctx *c) {
+  if (!c->mixed) return cudaSuccess;
+  return pip::mixed_join(c->Ahi, c->Alo, c->A, c->kp.nc * c->nplanes(), c->stream);
+}
+cudaError_t from_fp64(pip_ctx *c) {
+  if (!c->mixed) return cudaSuccess;
+  return pip::mixed_split(c->A, c->Ahi, c->Alo, c->kp.nc * c->nplanes(), c->stream);
+}
+
 // K steps of [stage 1, stage 2] as launched by pip_run.
 int launch_steps(pip_ctx *c, int k) {
   for (int s = 0; s < k; ++s) {
-    cudaError_t e = c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 1, 0, c->stream);
-    if (e == cudaSuccess) e = c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 1, -1, c->stream);
+    cudaError_t e = do_stage(c, 1, 1, 0);
+    if (e == cudaSuccess) e = do_stage(c, 2, 1, -1);
     if (e != cudaSuccess) {
       g_last_cuda_error = (int)e;
       return PIP_ERR_CUDA;
@@ -299,6 +329,7 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   c->p.dx = c->p.dy = c->p.dz = nullptr;
   build_kparams(c);
   c->L = p->fp_exact ? &pip::launchers_exact() : &pip::launchers_fast();
+  c->mixed = p->precision == PIP_MIXED;
   auto fail = [&](cudaError_t e) {
     g_last_cuda_error = (int)e;
     pip_ctx_destroy(c);
@@ -307,10 +338,19 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   cudaError_t e = cudaGetDevice(&c->device);
   if (e != cudaSuccess) return fail(e);
   if ((e = c->L->prepare()) != cudaSuccess) return fail(e);
+  if (c->mixed && (e = pip::mixed_prepare()) != cudaSuccess) return fail(e);
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
   const size_t state = c->plane_bytes() * c->nplanes();
   if ((e = cudaMalloc(&c->A, state)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&c->B, state)) != cudaSuccess) return fail(e);
+  if (c->mixed) {
+    const size_t fstate = state / 2;
+    if ((e = cudaMalloc(&c->Ahi, fstate)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->Alo, fstate)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->Bf, fstate)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->Bf, 0, fstate)) != cudaSuccess) return fail(e);
+  } else if ((e = cudaMalloc(&c->B, state)) != cudaSuccess) {
+    return fail(e);
+  }
   if ((e = cudaMalloc(&c->d_dx, sizeof(double) * p->ix)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&c->d_dy, sizeof(double) * p->jx)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&c->ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
@@ -322,7 +362,7 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   if ((e = cudaMemcpy(c->d_dy, c->dy.data(), sizeof(double) * p->jx, cudaMemcpyHostToDevice)) != cudaSuccess)
     return fail(e);
   if ((e = cudaMemset(c->A, 0, state)) != cudaSuccess) return fail(e);
-  if ((e = cudaMemset(c->B, 0, state)) != cudaSuccess) return fail(e);
+  if (c->B && (e = cudaMemset(c->B, 0, state)) != cudaSuccess) return fail(e);
   if ((e = cudaMemcpy(c->ctrl, c->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice)) != cudaSuccess)
     return fail(e);
   c->kp.dx = c->d_dx;
@@ -338,6 +378,9 @@ void pip_ctx_destroy(pip_ctx *c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   cudaFree(c->A);
   cudaFree(c->B);
+  cudaFree(c->Ahi);
+  cudaFree(c->Alo);
+  cudaFree(c->Bf);
   cudaFree(c->d_dx);
   cudaFree(c->d_dy);
   cudaFree(c->scratch);
@@ -354,6 +397,7 @@ int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
   const size_t pb = c->plane_bytes();
   CK(cudaMemcpyAsync(c->A, U_m, pb * c->kp.nvm, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->A + (size_t)c->kp.nvm * c->kp.nc, U_h, pb * 5, cudaMemcpyHostToDevice, c->stream));
+  CK(from_fp64(c));
   CK(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
   return PIP_OK;
@@ -364,6 +408,7 @@ int pip_download(pip_ctx *c, double *U_h, double *U_m) {
   if (!c->uploaded) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
+  CK(to_fp64(c));
   CK(cudaMemcpyAsync(U_m, c->A, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(U_h, c->A + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -376,7 +421,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
   if (set_device(c)) return PIP_ERR_CUDA;
   reset_slot(*c->h_ctrl, 0);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
-  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  CK(do_cfl(c, 0));
   if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
   const double d = finalize_dt_host(c->kp, *c->h_ctrl, 0);
   c->dt = d;
@@ -399,8 +444,8 @@ int pip_step(pip_ctx *c, double dt) {
   h.status = 0;
   h.blocks_done = 0;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
-  CK(c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 0, 0, c->stream));
-  CK(c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 0, 0, c->stream));
+  CK(do_stage(c, 1, 0, 0));
+  CK(do_stage(c, 2, 0, 0));
   CK(cudaStreamSynchronize(c->stream));
   c->last_dt = dt;
   return PIP_OK;
@@ -437,7 +482,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
     CK(cudaEventRecord(ev0, c->stream));
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
-  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  CK(do_cfl(c, 0));
   const int K = 32;
   int st = PIP_OK;
   if (nsteps > 0 && !(t_end > 0.0)) {
@@ -500,14 +545,14 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
   reset_slot(h, 0);
   reset_slot(h, 1);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
-  CK(c->L->cfl(c->kp, c->A, c->ctrl, 0, c->stream));
+  CK(do_cfl(c, 0));
   std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
   for (auto &e : ev) CK(cudaEventCreate(&e));
   for (int s = 0; s < nsteps; ++s) {
     CK(cudaEventRecord(ev[3 * s], c->stream));
-    CK(c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, 1, 0, c->stream));
+    CK(do_stage(c, 1, 1, 0));
     CK(cudaEventRecord(ev[3 * s + 1], c->stream));
-    CK(c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, 1, -1, c->stream));
+    CK(do_stage(c, 2, 1, -1));
     CK(cudaEventRecord(ev[3 * s + 2], c->stream));
   }
   if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
@@ -548,6 +593,7 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
   if (!c || !F_h || !F_m) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
   if (dir < 1 || dir > c->kp.ndim) return PIP_ERR_PARAM;
+  if (c->mixed) return PIP_ERR_STATE;  // unit-level entry points are FP64 only
   if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(cudaMemsetAsync(c->scratch, 0, pb * c->nplanes(), c->stream));
@@ -561,7 +607,7 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
 
 int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
   if (!c || !S_h || !S_m) return PIP_ERR_NULL;
-  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->uploaded || c->mixed) return PIP_ERR_STATE;
   if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(c->L->source(c->kp, c->A, c->scratch, dt_coll, c->stream));
@@ -576,7 +622,9 @@ int pip_fill_ghosts(pip_ctx *c) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
+  CK(to_fp64(c));
   CK(c->L->ghosts(c->kp, c->A, c->stream));
+  CK(from_fp64(c));
   CK(cudaStreamSynchronize(c->stream));
   return PIP_OK;
 }
@@ -587,6 +635,7 @@ int pip_status(pip_ctx *c, int *stop_flag, int *nan_flag) {
   if (set_device(c)) return PIP_ERR_CUDA;
   int h = 0;
   CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+  CK(to_fp64(c));
   CK(c->L->nan_scan(c->kp, c->A, c->d_flag, c->stream));
   CK(cudaMemcpyAsync(&h, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

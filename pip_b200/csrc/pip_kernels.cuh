@@ -62,4 +62,14 @@ struct Launchers {
 const Launchers &launchers_fast();
 const Launchers &launchers_exact();
 
+// FP32-mixed form (pip_mixed.cu): A = (hi, lo) FP32 pair, B = FP32 stage state.
+cudaError_t mixed_prepare();
+cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
+                        const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
+                        int epi, cudaStream_t s);
+cudaError_t mixed_cfl(const KParams &p, float *hi, float *lo, DevCtrl *ctrl, int slot,
+                      cudaStream_t s);
+cudaError_t mixed_split(const double *U, float *hi, float *lo, long long n, cudaStream_t s);
+cudaError_t mixed_join(const float *hi, const float *lo, double *U, long long n, cudaStream_t s);
+
 }  // namespace pip

@@ -1,0 +1,684 @@
+// pip_mixed.cu -- FP32-mixed form of the two-fluid step.
+//
+// Storage: the stage state and the fluxes are FP32.  U0 (array A) is kept as an FP32
+// pair (hi, lo) with hi + lo = the FP64 value, so that the conservative update
+// U2 = U0 - dt*div(F) + dt*S is accumulated in FP64 across the RK stages (compensated
+// accumulation) and the stored state keeps ~48 significant bits.  The collisional and
+// ionisation/recombination source (the stiff part) is evaluated in FP64.  The cq2pv
+// rewrites of the FP64 path change a state only below the pair's precision except where
+// a density or pressure floor fires; this form applies the floors (in FP64) and skips the
+// round trip otherwise.
+//
+// Bytes per cell and step (14 planes): stage 1 reads hi and writes U1 (8 B/plane), stage 2
+// reads U1, hi, lo and writes hi, lo (20 B/plane): 392 B.
+//
+// Compiled with -ftz=true -prec-div=false -prec-sqrt=false: FP32 division and square root
+// are the approximate hardware forms; FP64 arithmetic is unaffected.
+#include "pip_kernels.cuh"
+#include "pip_physics.cuh"
+
+namespace pip {
+namespace mixed {
+
+constexpr int kH = 2;
+template <int NDIM> struct Tile;
+template <> struct Tile<2> {
+  static constexpr int TX = 32, TY = 8, NT = 256;
+};
+template <> struct Tile<1> {
+  static constexpr int TX = 128, TY = 1, NT = 128;
+};
+
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double((long long)b);
+}
+
+__device__ __forceinline__ double finalize_dt(const KParams &p, const DevCtrl *c, int slot) {
+  double dt = bitsd(c->red_dt[slot]);
+  double rho = bitsd(c->red_rho[slot]);
+  dt = fmin(dt, p.col_lim / rho);
+  if (p.ir) dt = fmin(dt, p.ir_lim / fmax(bitsd(c->red_gr[slot]), 1.0e-5));
+  return dt;
+}
+
+// FP64 primitives of a conserved cell (cq2pv's expressions, without the rewrite).
+template <int NVM>
+__device__ __forceinline__ Prim<double> prim_mhd(const double (&u)[NVM], const KParams &p) {
+  Prim<double> q;
+  const double de = u[0];
+  q.vx = u[1] / de;
+  q.vy = u[2] / de;
+  q.vz = u[3] / de;
+  q.pr = fmax((p.gm - 1.0) * (u[4] - 0.5 * de * (q.vx * q.vx + q.vy * q.vy + q.vz * q.vz) -
+                              0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7])), p.pr_lim);
+  q.de = fmax(de, p.ro_lim);
+  return q;
+}
+__device__ __forceinline__ Prim<double> prim_hd(const double (&u)[5], const KParams &p) {
+  Prim<double> q;
+  const double de = u[0];
+  q.vx = u[1] / de;
+  q.vy = u[2] / de;
+  q.vz = u[3] / de;
+  q.pr = fmax((p.gm - 1.0) * (u[4] - 0.5 * de * (q.vx * q.vx + q.vy * q.vy + q.vz * q.vz)), p.pr_lim);
+  q.de = fmax(de, p.ro_lim);
+  return q;
+}
+
+// Density/pressure floors of cq2pv (Scheme_rot.f90:171-178), applied only when they fire.
+template <int NVM>
+__device__ __forceinline__ void floors_mhd(double (&u)[NVM], const KParams &p) {
+  const double de = u[0];
+  const double k = 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / de;
+  const double b = 0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
+  const double pr = (p.gm - 1.0) * (u[4] - k - b);
+  if (pr <= p.pr_lim || de <= p.ro_lim) cq2pv_mhd<double, NVM>(u, p.gm, p.ro_lim, p.pr_lim);
+}
+__device__ __forceinline__ void floors_hd(double (&u)[5], const KParams &p) {
+  const double de = u[0];
+  const double pr = (p.gm - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / de);
+  if (pr <= p.pr_lim || de <= p.ro_lim) cq2pv_hd<double>(u, p.gm, p.ro_lim, p.pr_lim);
+}
+
+template <int NVM>
+__device__ __forceinline__ void ir_rates(const double (&u)[NVM], const KParams &p, double &gr,
+                                         double &gi) {
+  const double gm = p.gm;
+  double pr = (gm - 1.0) * (u[4] - 0.5 * ((u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] +
+                                          u[5] * u[5] + u[6] * u[6] + u[7] * u[7]));
+  pr = fmax(pr, p.pr_lim);
+  const double te = 0.5 * gm * (pr / u[0]);
+  const double rs = 1.0 / sqrt(te);
+  gr = p.ir_rec * rs;
+  gi = p.ir_ion * rs * exp(-p.ir_chi / te);
+}
+
+// FP64 collisional dS (PIP_rot.f90:1333-1368) from FP64 primitives.
+template <int NVM>
+__device__ __forceinline__ void collision_ds(const double (&um)[NVM], const double (&uh)[5],
+                                             const Prim<double> &qm, const Prim<double> &qh,
+                                             const KParams &p, double dt_coll, double (&ds)[5]) {
+  const double gm = p.gm, ac = p.ac;
+  const double te = qm.pr / qm.de * gm * kMuP;
+  const double nte = qh.pr / qh.de * gm * kMuN;
+  ds[0] = 0.0;
+  if (p.imp) {
+    const double temp = dt_coll * (uh[0] + um[0]);
+    const double e = (1.0 - exp(-ac * temp));
+    ds[1] = (um[0] * uh[1] - uh[0] * um[1]) * e / temp;
+    ds[2] = (um[0] * uh[2] - uh[0] * um[2]) * e / temp;
+    ds[3] = (um[0] * uh[3] - uh[0] * um[3]) * e / temp;
+    const double nde = qh.de, de = qm.de;
+    const double lambda = ac * (nde + de);
+    const double kap = 3.0 * (gm - 1.0) * ac * (kMuP * nde + kMuN * de);
+    const double dvx = qh.vx - qm.vx, dvy = qh.vy - qm.vy, dvz = qh.vz - qm.vz;
+    const double B = -(1.0 / 3.0 * gm * kap / ((nde + de) * (kap - lambda)) *
+                       (de * (dvx * qm.vx + dvy * qm.vy + dvz * qh.vz) +
+                        nde * (dvx * qh.vx + dvy * qh.vy + dvz * qh.vz)));
+    const double D = -(gm / 6.0 * kap * (de - nde) / ((de + nde) * (kap - 2.0 * lambda)) *
+                       (dvx * dvx + dvy * dvy + dvz * dvz));
+    ds[4] = -((3.0 / gm) * ac * de * nde / kap *
+              (+(exp(-kap * dt_coll) - 1.0) * (nte - te) - (B + D) * exp(-kap * dt_coll) +
+               B * exp(-lambda * dt_coll) + D * exp(-2.0 * lambda * dt_coll)) /
+              dt_coll);
+  } else {
+    ds[1] = ac * (um[0] * uh[1] - uh[0] * um[1]);
+    ds[2] = ac * (um[0] * uh[2] - uh[0] * um[2]);
+    ds[3] = ac * (um[0] * uh[3] - uh[0] * um[3]);
+    ds[4] = ac * qh.de * qm.de *
+            (0.5 * ((qh.vx * qh.vx - qm.vx * qm.vx) + (qh.vy * qh.vy - qm.vy * qm.vy) +
+                    (qh.vz * qh.vz - qm.vz * qm.vz)) +
+             3.0 / gm / 2.0 * (nte - te));
+  }
+}
+
+__device__ __forceinline__ void ir_ds(const Prim<double> &qm, const Prim<double> &qh, double gr,
+                                      double gi, const KParams &p, double (&ds)[5]) {
+  const double gm = p.gm;
+  ds[0] = gr * qm.de - gi * qh.de;
+  ds[1] = gr * qm.de * qm.vx - gi * qh.de * qh.vx;
+  ds[2] = gr * qm.de * qm.vy - gi * qh.de * qh.vy;
+  ds[3] = gr * qm.de * qm.vz - gi * qh.de * qh.vz;
+  const double kin = 0.5 * (gr * qm.de * (qm.vx * qm.vx + qm.vy * qm.vy + qm.vz * qm.vz) -
+                            gi * qh.de * (qh.vx * qh.vx + qh.vy * qh.vy + qh.vz * qh.vz));
+  if (p.ir_type == 1)
+    ds[4] = kin - gi * qh.pr / (gm - 1.0) + 0.5 * gr * qm.pr / (gm - 1.0);
+  else
+    ds[4] = kin - gi * qh.pr / (gm - 1.0) + gr * qm.pr / (gm - 1.0);
+}
+
+// Stores one plane value (and its ghost images) -- the sign tables of PIPbnd.
+constexpr int kMaxTargets = 2 * kMaxMargin + (2 * kMaxMargin) * (2 * kMaxMargin) + 2 * kMaxMargin;
+struct Targets {
+  int n, q[kMaxTargets];
+  signed char sx[kMaxTargets], sy[kMaxTargets];
+};
+
+template <int NDIM>
+__device__ __forceinline__ void ghost_targets(const KParams &p, int gi, int gj, Targets &t) {
+  int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
+  int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
+  for (int s = 0; s < 2; ++s)
+    for (int l = 0; l < p.m0; ++l)
+      if (p.gx[s][l] == gi) {
+        tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
+        sx[ntx++] = s;
+      }
+  if (NDIM == 2)
+    for (int s = 0; s < 2; ++s)
+      for (int l = 0; l < p.m1; ++l)
+        if (p.gy[s][l] == gj) {
+          ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
+          sy[nty++] = s;
+        }
+  t.n = 0;
+  for (int a = 0; a < ntx; ++a) {
+    t.q[t.n] = gj * p.ix + tx[a];
+    t.sx[t.n] = (signed char)sx[a];
+    t.sy[t.n] = -1;
+    ++t.n;
+    for (int b = 0; b < nty; ++b) {
+      t.q[t.n] = ty[b] * p.ix + tx[a];
+      t.sx[t.n] = (signed char)sx[a];
+      t.sy[t.n] = (signed char)sy[b];
+      ++t.n;
+    }
+  }
+  for (int b = 0; b < nty; ++b) {
+    t.q[t.n] = ty[b] * p.ix + gi;
+    t.sx[t.n] = -1;
+    t.sy[t.n] = (signed char)sy[b];
+    ++t.n;
+  }
+}
+
+__device__ __forceinline__ float gsign(const KParams &p, const Targets &t, int k, int plane) {
+  float s = 1.0f;
+  if (t.sx[k] >= 0) s *= (float)p.symx[t.sx[k]][plane];
+  if (t.sy[k] >= 0) s *= (float)p.symy[t.sy[k]][plane];
+  return s;
+}
+
+template <int NT>
+__device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double gr, DevCtrl *ctrl,
+                                                 int slot) {
+  __shared__ double s_red[3][NT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+    rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
+  }
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  if (l == 0) {
+    s_red[0][w] = dtc;
+    s_red[1][w] = rho;
+    s_red[2][w] = gr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NT / 32; ++k) {
+      dtc = fmin(dtc, s_red[0][k]);
+      rho = fmax(rho, s_red[1][k]);
+      gr = fmax(gr, s_red[2][k]);
+    }
+    atomicMin(&ctrl->red_dt[slot], dbits(dtc));
+    atomicMax(&ctrl->red_rho[slot], dbits(rho));
+    atomicMax(&ctrl->red_gr[slot], dbits(gr));
+  }
+}
+
+// One RK stage (see the FP64 stage_kernel for the structure).  Stage 1: Us = A.hi,
+// U0 = A.hi, output B (FP32).  Stage 2: Us = B, U0 = A.hi + A.lo, output A (hi, lo).
+template <int NDIM, int NVM, int STAGE>
+__global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 3 : 4)
+stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
+             float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi) {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
+  constexpr int NV = NVM + 5;
+  constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
+  constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
+  extern __shared__ float smf[];
+  float *sV = smf;
+  float *sFx = sV + NV * RR;
+  float *sFy = sFx + NV * NFX;
+  __shared__ double s_dt, s_cmax;
+  __shared__ long long s_step;
+  __shared__ int s_exit, s_epi;
+
+  const int tid = threadIdx.x;
+  const bool block0 = blockIdx.x == 0 && blockIdx.y == 0;
+  if (tid == 0) {
+    int ex = STAGE == 1 ? (ctrl->done || ctrl->nan_flag) : ctrl->done;
+    double dt, cmax;
+    if (STAGE == 1 && dt_mode == 1) {
+      dt = finalize_dt(p, ctrl, (int)(ctrl->step & 1));
+      cmax = p.sg_all / dt;
+    } else {
+      dt = ctrl->dt;
+      cmax = ctrl->cmax;
+    }
+    s_dt = dt;
+    s_cmax = cmax;
+    s_step = ctrl->step;
+    s_exit = ex;
+    s_epi = (STAGE == 2 && epi < 0) ? (ctrl->last ? 1 : 2) : epi;
+  }
+  __syncthreads();
+  if (s_exit) {
+    if (STAGE == 1 && block0 && tid == 0) {
+      if (ctrl->nan_flag && ctrl->status == 0) ctrl->status = 3;
+      ctrl->done = 1;
+    }
+    return;
+  }
+  const double dt = s_dt;
+  const float cmaxf = (float)s_cmax;
+  if (STAGE == 1 && dt_mode == 1 && block0 && tid == 0) {
+    const long long st = ctrl->step;
+    ctrl->dt = dt;
+    ctrl->cmax = s_cmax;
+    const double tn = ctrl->time + dt;
+    ctrl->time_next = tn;
+    ctrl->last = ((ctrl->t_end > 0.0 && tn >= ctrl->t_end) ||
+                  (ctrl->nsteps > 0 && st + 1 >= ctrl->nsteps)) ? 1 : 0;
+    const int ns = (int)((st + 1) & 1);
+    ctrl->red_dt[ns] = dbits(10.0);
+    ctrl->red_rho[ns] = 0ull;
+    ctrl->red_gr[ns] = 0ull;
+  }
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  const int i0 = p.m0 + blockIdx.x * TX;
+  const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
+  const long long nc = p.nc;
+
+  // ---- 1. FP32 primitives of the tile and its halo
+  for (int idx = tid; idx < RR; idx += NT) {
+    const int ri = idx % RX, rj = idx / RX;
+    if (NDIM == 2 && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
+    const int gi = i0 - kH + ri, gj = NDIM == 2 ? j0 - kH + rj : 0;
+    if (gi >= p.ix || gj >= p.jx) continue;
+    const long long q = (long long)gj * p.ix + gi;
+    float um[NVM], uh[5], vm[NVM], vh[5];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) um[n] = Us[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uh[n] = Us[q + (NVM + n) * nc];
+    u2v_mhd<float, NVM>(um, vm, gmf, rolf, prlf);
+    u2v_hd<float>(uh, vh, gmf, rolf, prlf);
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) sV[n * RR + idx] = vm[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+  }
+  __syncthreads();
+
+  // ---- 2. FP32 face fluxes
+  const int iend = p.m0 + p.nx, jend = NDIM == 2 ? p.m1 + p.ny : 1;
+  for (int f = tid; f < NFX + NFY; f += NT) {
+    int a, s, py, fo, nf;
+    float *Fout;
+    if (f < NFX) {
+      const int fi = f % (TX + 1), fj = f / (TX + 1);
+      if (i0 + fi - 1 >= iend || (NDIM == 2 && j0 + fj >= jend)) continue;
+      a = (NDIM == 2 ? (fj + kH) * RX : 0) + fi + kH - 1;
+      s = 1;
+      py = 0;
+      Fout = sFx;
+      fo = f;
+      nf = NFX;
+    } else {
+      const int g = f - NFX, fi = g % TX, fj = g / TX;
+      if (i0 + fi >= iend || j0 + fj - 1 >= jend) continue;
+      a = (fj + kH - 1) * RX + fi + kH;
+      s = RX;
+      py = 1;
+      Fout = sFy;
+      fo = g;
+      nf = NFY;
+    }
+    {
+      float vl[NVM], vr[NVM], fx[NVM];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) {
+        const int src = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        const float *v = sV + src * RR + a;
+        const float v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+        vl[n] = v1 + 0.5f * minmod<float>(v0, v1, v2);
+        vr[n] = v2 - 0.5f * minmod<float>(v1, v2, v3);
+      }
+      vl[0] = fmaxf(vl[0], rolf);
+      vr[0] = fmaxf(vr[0], rolf);
+      hlld_flux<float, NVM>(vl, vr, fx, gmf, cmaxf);
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) {
+        const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
+        Fout[dst * nf + fo] = fx[n];
+      }
+    }
+    {
+      float vl[5], vr[5], fx[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        const int src = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
+        const float *v = sV + (NVM + src) * RR + a;
+        const float v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+        vl[n] = v1 + 0.5f * minmod<float>(v0, v1, v2);
+        vr[n] = v2 - 0.5f * minmod<float>(v1, v2, v3);
+      }
+      vl[0] = fmaxf(vl[0], rolf);
+      vr[0] = fmaxf(vr[0], rolf);
+      hllc_flux<float>(vl, vr, fx, gmf);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
+        Fout[(NVM + dst) * nf + fo] = fx[n];
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- 3. FP64 source and compensated update
+  const int ti = tid % TX, tj = tid / TX;
+  const int gi = i0 + ti, gj = j0 + tj;
+  const bool valid = gi < iend && (NDIM == 1 || gj < jend);
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  if (valid) {
+    const long long q = (long long)gj * p.ix + gi;
+    const double dt_sub = STAGE == 1 ? dt / 2.0 : dt;
+    const double dt_coll = dt * 0.5;
+    double a_m[NVM], a_h[5], s_m[NVM], s_h[5];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) {
+      a_m[n] = (double)U0hi[q + n * nc];
+      if (STAGE == 2) a_m[n] += (double)U0lo[q + n * nc];
+    }
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      a_h[n] = (double)U0hi[q + (NVM + n) * nc];
+      if (STAGE == 2) a_h[n] += (double)U0lo[q + (NVM + n) * nc];
+    }
+    if (STAGE == 1) {
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) s_m[n] = a_m[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) s_h[n] = a_h[n];
+    } else {
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) s_m[n] = (double)Us[q + n * nc];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) s_h[n] = (double)Us[q + (NVM + n) * nc];
+    }
+    double gr = 0.0, gion = 0.0;
+    if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
+    if (p.imp && STAGE == 2) {
+      double ds[5];
+      const Prim<double> qh = prim_hd(a_h, p);
+      const Prim<double> qm = prim_mhd<NVM>(a_m, p);
+      collision_ds<NVM>(a_m, a_h, qm, qh, p, dt_coll, ds);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        a_h[n] = a_h[n] - dt_coll * ds[n];
+        a_m[n] = a_m[n] + dt_coll * ds[n];
+      }
+    }
+    double S_m[5], S_h[5];
+    {
+      const Prim<double> qh = prim_hd(s_h, p);
+      const Prim<double> qm = prim_mhd<NVM>(s_m, p);
+      double ds[5];
+      collision_ds<NVM>(s_m, s_h, qm, qh, p, dt_coll, ds);
+      if (p.imp) {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          a_h[n] = a_h[n] - dt_coll * ds[n];
+          a_m[n] = a_m[n] + dt_coll * ds[n];
+          S_h[n] = 0.0;
+          S_m[n] = 0.0;
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          S_h[n] = -ds[n];
+          S_m[n] = ds[n];
+        }
+      }
+      if (p.ir) {
+        ir_ds(qm, qh, gr, gion, p, ds);
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          S_h[n] += ds[n];
+          S_m[n] -= ds[n];
+        }
+      }
+    }
+    const double cx = dt_sub / p.dx[gi];
+    const double cy = NDIM == 2 ? dt_sub / p.dy[gj] : 0.0;
+    const int fxl = tj * (TX + 1) + ti, fyl = tj * TX + ti;
+    double n_m[NVM], n_h[5];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      double u = n < NVM ? a_m[n] : a_h[n - NVM];
+      u -= cx * (double)(sFx[n * NFX + fxl + 1] - sFx[n * NFX + fxl]);
+      if (NDIM == 2) u -= cy * (double)(sFy[n * NFY + fyl + TX] - sFy[n * NFY + fyl]);
+      if (n < NVM) {
+        if (n < 5) u += S_m[n] * dt_sub;
+        n_m[n] = u;
+      } else {
+        n_h[n - NVM] = u + S_h[n - NVM] * dt_sub;
+      }
+    }
+    if (NVM == 9) n_m[NVM - 1] *= p.decay[STAGE - 1];
+    const int ep = s_epi;
+    if (ep >= 1) {
+      floors_mhd<NVM>(n_m, p);
+      floors_hd(n_h, p);
+    }
+    if (ep == 2) {
+      // CFL terms of the next step in FP32 from the new state
+      float um[NVM], uh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) um[n] = (float)n_m[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uh[n] = (float)n_h[n];
+      const Prim<float> qm = cq2pv_mhd<float, NVM>(um, gmf, rolf, prlf);
+      const Prim<float> qh = cq2pv_hd<float>(uh, gmf, rolf, prlf);
+      const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+      const float sg = (float)(p.safety * gmin);
+      dtc = (double)fminf(cfl_mhd_cell<float>(qm, um[5], um[6], um[7], gmf, sg),
+                          cfl_hd_cell<float>(qh, gmf, sg));
+      rhoc = fmax(n_m[0] * p.ac, n_h[0] * p.ac);
+      if (p.ir) {
+        double g1, g2;
+        ir_rates<NVM>(n_m, p, g1, g2);
+        grc = fmax(g1, g2);
+      }
+    }
+    bool bad = false;
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) bad |= !isfinite(n_m[n]);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
+    if (bad) atomicOr(&ctrl->nan_flag, 1);
+    Targets tg;
+    ghost_targets<NDIM>(p, gi, gj, tg);
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const double u = n < NVM ? n_m[n] : n_h[n - NVM];
+      const float hi = (float)u;
+      const float lo = (float)(u - (double)hi);
+      Ohi[q + n * nc] = hi;
+      if (STAGE == 2) Olo[q + n * nc] = lo;
+      for (int k = 0; k < tg.n; ++k) {
+        const float sgn = gsign(p, tg, k, n);
+        Ohi[tg.q[k] + n * nc] = sgn * hi;
+        if (STAGE == 2) Olo[tg.q[k] + n * nc] = sgn * lo;
+      }
+    }
+  }
+  if (STAGE == 2 && s_epi == 2) block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
+  if (STAGE == 2 && dt_mode == 1) {
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const unsigned int nb = gridDim.x * gridDim.y;
+      if (atomicAdd(&ctrl->blocks_done, 1u) == nb - 1) {
+        __threadfence();
+        ctrl->blocks_done = 0u;
+        ctrl->time = ctrl->time_next;
+        ctrl->step = s_step + 1;
+        if (ctrl->last) ctrl->done = 1;
+        if (dt <= 1.0e-12) {
+          ctrl->done = 1;
+          if (ctrl->status == 0) ctrl->status = 4;
+        }
+      }
+    }
+  }
+}
+
+// cfl over every cell for the mixed state: floors (in FP64 on hi+lo) and FP32 CFL terms.
+template <int NVM>
+__global__ void __launch_bounds__(256) cfl_kernel(const KParams p, float *Uhi, float *Ulo,
+                                                  DevCtrl *ctrl, int slot) {
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  const long long nc = p.nc;
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
+    double um[NVM], uh[5];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) um[n] = (double)Uhi[q + n * nc] + (double)Ulo[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n)
+      uh[n] = (double)Uhi[q + (NVM + n) * nc] + (double)Ulo[q + (NVM + n) * nc];
+    floors_mhd<NVM>(um, p);
+    floors_hd(uh, p);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      float h = (float)um[n];
+      Uhi[q + n * nc] = h;
+      Ulo[q + n * nc] = (float)(um[n] - (double)h);
+      h = (float)uh[n];
+      Uhi[q + (NVM + n) * nc] = h;
+      Ulo[q + (NVM + n) * nc] = (float)(uh[n] - (double)h);
+    }
+    const int i = (int)(q % p.ix), j = (int)(q / p.ix);
+    const bool interior = i >= p.m0 && i < p.ix - p.m0 && j >= p.m1 && j < p.jx - p.m1;
+    if (interior) {
+      float fm[NVM], fh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) fm[n] = (float)um[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
+      const Prim<float> qm = cq2pv_mhd<float, NVM>(fm, gmf, rolf, prlf);
+      const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
+      const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[j]), p.dz0));
+      dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
+                                    cfl_hd_cell<float>(qh, gmf, sg)));
+    }
+    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (p.ir) {
+      double g1, g2;
+      ir_rates<NVM>(um, p, g1, g2);
+      grc = fmax(grc, fmax(g1, g2));
+    }
+  }
+  block_reduce_cfl<256>(dtc, rhoc, grc, ctrl, slot);
+}
+
+// FP64 <-> (hi, lo) conversions of whole state arrays.
+__global__ void split_kernel(const double *__restrict__ U, float *hi, float *lo, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const double u = U[t];
+    const float h = (float)u;
+    hi[t] = h;
+    lo[t] = (float)(u - (double)h);
+  }
+}
+__global__ void join_kernel(const float *__restrict__ hi, const float *__restrict__ lo, double *U,
+                            long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    U[t] = (double)hi[t] + (double)lo[t];
+}
+
+template <int NDIM, int NVM>
+constexpr size_t smem_bytes() {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY;
+  constexpr int RR = (TX + 2 * kH) * (NDIM == 2 ? TY + 2 * kH : 1);
+  constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
+  return sizeof(float) * (NVM + 5) * (RR + NFX + NFY);
+}
+
+template <int NDIM, int NVM, int STAGE>
+static cudaError_t set_attr() {
+  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes<NDIM, NVM>());
+}
+
+template <int NDIM, int NVM, int STAGE>
+static cudaError_t launch_t(const KParams &p, const float *Us, const float *U0hi, const float *U0lo,
+                            float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi,
+                            cudaStream_t s) {
+  constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
+  dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
+  stage_kernel<NDIM, NVM, STAGE><<<grid, NT, smem_bytes<NDIM, NVM>(), s>>>(
+      p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi);
+  return cudaGetLastError();
+}
+
+static int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+}  // namespace mixed
+
+cudaError_t mixed_prepare() {
+  cudaError_t e;
+  if ((e = mixed::set_attr<1, 8, 1>()) != cudaSuccess) return e;
+  if ((e = mixed::set_attr<1, 8, 2>()) != cudaSuccess) return e;
+  if ((e = mixed::set_attr<2, 8, 1>()) != cudaSuccess) return e;
+  if ((e = mixed::set_attr<2, 8, 2>()) != cudaSuccess) return e;
+  if ((e = mixed::set_attr<2, 9, 1>()) != cudaSuccess) return e;
+  return mixed::set_attr<2, 9, 2>();
+}
+
+cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
+                        const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
+                        int epi, cudaStream_t s) {
+  using namespace mixed;
+  if (p.ndim == 1)
+    return stage == 1 ? launch_t<1, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
+                      : launch_t<1, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
+  if (p.nvm == 9)
+    return stage == 1 ? launch_t<2, 9, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
+                      : launch_t<2, 9, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
+  return stage == 1 ? launch_t<2, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
+                    : launch_t<2, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
+}
+
+cudaError_t mixed_cfl(const KParams &p, float *hi, float *lo, DevCtrl *ctrl, int slot,
+                      cudaStream_t s) {
+  const int g = mixed::grid_for(p.nc, 256);
+  if (p.nvm == 9) mixed::cfl_kernel<9><<<g, 256, 0, s>>>(p, hi, lo, ctrl, slot);
+  else mixed::cfl_kernel<8><<<g, 256, 0, s>>>(p, hi, lo, ctrl, slot);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_split(const double *U, float *hi, float *lo, long long n, cudaStream_t s) {
+  mixed::split_kernel<<<mixed::grid_for(n, 256), 256, 0, s>>>(U, hi, lo, n);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_join(const float *hi, const float *lo, double *U, long long n, cudaStream_t s) {
+  mixed::join_kernel<<<mixed::grid_for(n, 256), 256, 0, s>>>(hi, lo, U, n);
+  return cudaGetLastError();
+}
+
+}  // namespace pip

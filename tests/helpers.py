@@ -10,12 +10,13 @@ def interior(U, s):
 
 
 def rel_l1(a, b):
-    """Relative L1 error per variable: sum|a-b| / max(sum|b|, tiny)."""
+    """Relative L1 error per variable: sum|a-b| / sum|b|.  A variable that is zero in
+    both arrays scores 0; one that is zero only in b scores its absolute L1."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     num = np.abs(a - b).reshape(a.shape[0], -1).sum(axis=1)
     den = np.abs(b).reshape(b.shape[0], -1).sum(axis=1)
-    return num / np.maximum(den, 1e-300)
+    return np.where(den > 0, num / np.where(den > 0, den, 1.0), num)
 
 
 def max_rel_l1(pairs):

@@ -14,7 +14,7 @@ from pip_b200 import capi, ics
 pytestmark = pytest.mark.gpu
 
 TOL_FP64 = 1e-10      # relative L1 per variable, FMA build vs oracle
-TOL_EXP = 1e-12       # FMA-free build where exp() (GPU vs libm, <= 1 ulp) enters
+TOL_EXP = 1e-10       # FMA-free build where exp() (GPU vs libm, <= 1 ulp) enters: drop-in bar
 
 
 def run_gpu(s, Uh, Um, nsteps=0, t_end=0.0):
