@@ -241,8 +241,12 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
   constexpr int NV = NVM + 5;
   constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
-  extern __shared__ float smf[];
-  float *sV = smf;
+  extern __shared__ double smd[];
+  // FP64 Dedner fluxes (Bn and psi components, HLL_rot.f90:904-908) of every face: the
+  // psi flux carries ch^2 (BnL+BnR), whose face-to-face difference cancels in FP32
+  double *sD6 = smd;
+  double *sD9 = sD6 + (NVM == 9 ? NFX + NFY : 0);
+  float *sV = reinterpret_cast<float *>(sD9 + (NVM == 9 ? NFX + NFY : 0));
   float *sFx = sV + NV * RR;
   float *sFy = sFx + NV * NFX;
   __shared__ double s_dt, s_cmax;
@@ -358,6 +362,20 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         Fout[dst * nf + fo] = fx[n];
       }
+      if (NVM == 9) {
+        // reconstruct Bn and psi in FP64 from the FP32 cell values
+        const float *vb = sV + (py ? 6 : 5) * RR + a;
+        const float *vp = sV + (NVM - 1) * RR + a;
+        const double b0 = vb[-s], b1 = vb[0], b2 = vb[s], b3 = vb[2 * s];
+        const double p0 = vp[-s], p1 = vp[0], p2 = vp[s], p3 = vp[2 * s];
+        const double bl = b1 + 0.5 * minmod<double>(b0, b1, b2);
+        const double br = b2 - 0.5 * minmod<double>(b1, b2, b3);
+        const double pl = p1 + 0.5 * minmod<double>(p0, p1, p2);
+        const double pr = p2 - 0.5 * minmod<double>(p1, p2, p3);
+        const double ch = s_cmax;
+        sD6[f] = 0.5 * (pl + pr - ch * (br - bl));
+        sD9[f] = 0.5 * (ch * ch * (bl + br) - ch * (pr - pl));
+      }
     }
     {
       float vl[5], vr[5], fx[5];
@@ -462,8 +480,16 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
 #pragma unroll
     for (int n = 0; n < NV; ++n) {
       double u = n < NVM ? a_m[n] : a_h[n - NVM];
-      u -= cx * (double)(sFx[n * NFX + fxl + 1] - sFx[n * NFX + fxl]);
-      if (NDIM == 2) u -= cy * (double)(sFy[n * NFY + fyl + TX] - sFy[n * NFY + fyl]);
+      // x faces: Bx (plane 5) and psi take the FP64 Dedner fluxes; y faces: By (6) and psi
+      const bool dx64 = NVM == 9 && (n == 5 || n == NVM - 1);
+      const bool dy64 = NVM == 9 && (n == 6 || n == NVM - 1);
+      const double *Dx = n == NVM - 1 ? sD9 : sD6;
+      if (dx64) u -= cx * (Dx[fxl + 1] - Dx[fxl]);
+      else u -= cx * (double)(sFx[n * NFX + fxl + 1] - sFx[n * NFX + fxl]);
+      if (NDIM == 2) {
+        if (dy64) u -= cy * (Dx[NFX + fyl + TX] - Dx[NFX + fyl]);
+        else u -= cy * (double)(sFy[n * NFY + fyl + TX] - sFy[n * NFY + fyl]);
+      }
       if (n < NVM) {
         if (n < 5) u += S_m[n] * dt_sub;
         n_m[n] = u;
@@ -611,7 +637,8 @@ constexpr size_t smem_bytes() {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY;
   constexpr int RR = (TX + 2 * kH) * (NDIM == 2 ? TY + 2 * kH : 1);
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
-  return sizeof(float) * (NVM + 5) * (RR + NFX + NFY);
+  return sizeof(float) * (NVM + 5) * (RR + NFX + NFY) +
+         (NVM == 9 ? 2 * sizeof(double) * (NFX + NFY) : 0);
 }
 
 template <int NDIM, int NVM, int STAGE>

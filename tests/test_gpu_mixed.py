@@ -28,14 +28,29 @@ def compare(s, Uh, Um, nsteps=0, t_end=0.0):
     return a, b, err_h, err_m
 
 
+# The Dedner potential psi is driven by div B, a truncation-level difference of B; FP32
+# flux rounding perturbs B by ~1e-7 relative, which is a large relative perturbation of
+# div B, so psi carries ~1e-3 relative L1 against FP64 while the 13 physical fields (8 MHD,
+# 5 hydro) stay at ~1e-7.  psi is held to this looser bound.
+TOL_PSI = 1e-2
+
+
 def test_mixed_orszag_tang(gpu_lib):
     s, Uh, Um = ics.orszag_tang(128)
     a, b, eh, em = compare(s, Uh, Um, nsteps=300)
     assert a[1] == b[1] == 300
     assert abs(a[0] - b[0]) <= 1e-5 * a[0]
     # vz / bz / mz stay exactly zero in this 2D problem; the others carry the check
-    err = max(np.nanmax(eh), np.nanmax(em))
-    assert err <= TOL_MIXED, (eh, em)
+    physical = max(eh.max(), em[:8].max())
+    assert physical <= TOL_MIXED, (eh, em)
+    assert em[8] <= TOL_PSI, em
+
+
+def test_mixed_orszag_tang_no_cleaning(gpu_lib):
+    """Without Dedner cleaning every stored variable meets 1e-5."""
+    s, Uh, Um = ics.orszag_tang(128, flag_divb=0)
+    a, b, eh, em = compare(s, Uh, Um, nsteps=300)
+    assert max(eh.max(), em.max()) <= TOL_MIXED, (eh, em)
 
 
 def test_mixed_brio_wu(gpu_lib):
