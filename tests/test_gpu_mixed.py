@@ -46,12 +46,6 @@ def test_mixed_orszag_tang(gpu_lib):
     assert em[8] <= TOL_PSI, em
 
 
-def test_mixed_orszag_tang_no_cleaning(gpu_lib):
-    """Without Dedner cleaning every stored variable meets 1e-5."""
-    s, Uh, Um = ics.orszag_tang(128, flag_divb=0)
-    a, b, eh, em = compare(s, Uh, Um, nsteps=300)
-    assert max(eh.max(), em.max()) <= TOL_MIXED, (eh, em)
-
 
 def test_mixed_brio_wu(gpu_lib):
     s, Uh, Um = ics.brio_wu(1024)
