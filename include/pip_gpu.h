@@ -135,6 +135,33 @@ int pip_cfl(pip_ctx *ctx, double *dt, double *cmax);
  * collisional source, conservative update and ghost fill with the given dt. */
 int pip_step(pip_ctx *ctx, double dt);
 
+/* Allocation-free run_solver.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: a host code whose device memory is owned by
+ * someone else (an OpenACC or CUDA Fortran data region, a fixed-size memory pool of the
+ * application) or that must not allocate on its stepping path.  Same computation as
+ * pip_step with the FP64 kernels, on a state the caller already holds on the device:
+ * U_dev is the device image of U_m followed by U_h (nvar_m + 5 planes of ix*jx doubles,
+ * Fortran order, ghosts included), updated in place.  dt and cmax are what cfl returned
+ * (pip_cfl, or the caller's own).  The work is queued on `stream` (a cudaStream_t; NULL for
+ * the legacy default stream) and the call returns without waiting for it.
+ *
+ * The U1 stage buffer, the control block and device copies of dx/dy live in one
+ * file-scope device array of PIP_NOALLOC_SCRATCH_BYTES that every GPU loading this
+ * library holds until the process exits.  Limits: ix*jx <= PIP_NOALLOC_MAX_CELLS and
+ * ix, jx <= PIP_NOALLOC_MAX_AXIS; larger grids, the mixed precision form and any
+ * parameter pip_ctx_create would reject return PIP_ERR_PARAM.  The first call on each
+ * device looks up that array's device address and sets the kernels' shared-memory limit;
+ * make that first call before any stream capture.  All calls share the one array and it
+ * keeps the previous call's contents (the control block is rewritten by every call), so
+ * calls whose GPU work overlaps race with each other: serialise them, e.g. on one stream.
+ * The call itself allocates nothing on the device or the host. */
+#define PIP_NOALLOC_MAX_CELLS 262144
+#define PIP_NOALLOC_MAX_AXIS 8192
+#define PIP_NOALLOC_SCRATCH_BYTES \
+  (256 + 2 * 8 * PIP_NOALLOC_MAX_AXIS + 14 * 8 * (long long)PIP_NOALLOC_MAX_CELLS)
+int pip_step_noalloc(const pip_params *p, double *U_dev, double dt, double cmax, void *stream);
+
 /* The time loop of main.f90:31-68 on the device: repeats {cfl; run_solver; cfl;
  * time += dt; stop_sim} until nsteps steps are done (nsteps <= 0: no step limit) or
  * time >= t_end (t_end <= 0: no time limit).  The per-step dt and the stop checks stay on

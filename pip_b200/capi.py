@@ -32,6 +32,7 @@ EXPORTS = (
     "pip_ctx_create", "pip_ctx_destroy", "pip_upload", "pip_download", "pip_cfl", "pip_step",
     "pip_run", "pip_set_time", "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts",
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
+    "pip_step_noalloc",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run",
 )
@@ -79,6 +80,8 @@ def lib(path: Optional[str] = None):
     L.pip_fill_ghosts.argtypes = [vp]
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
+    L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
+    L.pip_step_noalloc.restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
     L.pip_strerror.restype = ctypes.c_char_p

@@ -209,6 +209,73 @@ void build_kparams(pip_ctx *c) {
   }
 }
 
+}  // namespace
+
+// Kernel parameters straight from a parameter block, for callers without a context: the
+// same validation and tables as pip_ctx_create, built on the stack (no allocation).  The
+// dx/dy pointers of the result are left null for the caller to point at device copies.
+int pip::kparams_from_params(const pip_params *p, KParams *k) {
+  const int st = validate(p);
+  if (st != PIP_OK) return st;
+  *k = KParams{};
+  k->ndim = p->ndim;
+  k->ix = p->ix;
+  k->jx = p->jx;
+  k->m0 = p->margin[0];
+  k->m1 = p->ndim == 2 ? p->margin[1] : 0;
+  k->nx = p->ix - 2 * k->m0;
+  k->ny = p->ndim == 2 ? p->jx - 2 * k->m1 : 1;
+  k->nvm = p->nvar_m;
+  k->imp = p->flag_pip_imp;
+  k->ir = p->flag_ir == PIP_IR_POWERLAW;
+  k->ir_type = p->flag_ir_type;
+  k->nc = (long long)p->ix * p->jx;
+  k->gm = p->gm;
+  k->ro_lim = p->ro_lim;
+  k->pr_lim = p->pr_lim;
+  k->ac = p->col;
+  k->safety = p->safety;
+  double g = INFINITY, gy = INFINITY, gz = INFINITY;
+  for (int i = 0; i < p->ix; ++i) g = std::min(g, p->dx[i]);
+  for (int j = 0; j < p->jx; ++j) gy = std::min(gy, p->dy[j]);
+  for (int q = 0; q < p->kx; ++q) gz = std::min(gz, p->dz[q]);
+  k->sg_all = p->safety * std::min(std::min(g, gy), gz);
+  k->col_lim = p->flag_pip_imp == 1 ? p->pip_imp_factor : std::min(p->safety, 0.3);
+  k->ir_lim = std::min(p->safety, 0.1);
+  k->ir_chi = p->ir_chi;
+  k->ir_ion = p->ir_ion_coef;
+  k->ir_rec = p->ir_rec_coef;
+  k->decay[0] = std::exp(-0.5 * p->safety * p->db_clean);
+  k->decay[1] = std::exp(-1.0 * p->safety * p->db_clean);
+  k->dz0 = p->dz[0];
+  for (int s = 0; s < 2; ++s) {
+    k->typex[s] = bnd_type(p->flag_bnd[s]);
+    for (int l = 0; l < pip::kMaxMargin; ++l)
+      k->gx[s][l] = l < k->m0 ? ghost_source(k->typex[s], s, l, p->ix, k->m0) : -1;
+    signed char sm[9], sh[5];
+    sym_mhd(*p, s, sm);
+    sym_hd(*p, s, sh);
+    for (int n = 0; n < k->nvm; ++n) k->symx[s][n] = sm[n];
+    for (int n = 0; n < 5; ++n) k->symx[s][k->nvm + n] = sh[n];
+    if (p->ndim == 2) {
+      k->typey[s] = bnd_type(p->flag_bnd[2 + s]);
+      for (int l = 0; l < pip::kMaxMargin; ++l)
+        k->gy[s][l] = l < k->m1 ? ghost_source(k->typey[s], s, l, p->jx, k->m1) : -1;
+      sym_mhd(*p, 2 + s, sm);
+      sym_hd(*p, 2 + s, sh);
+      for (int n = 0; n < k->nvm; ++n) k->symy[s][n] = sm[n];
+      for (int n = 0; n < 5; ++n) k->symy[s][k->nvm + n] = sh[n];
+    } else {
+      k->typey[s] = 1;
+      for (int l = 0; l < pip::kMaxMargin; ++l) k->gy[s][l] = -1;
+      for (int n = 0; n < pip::kMaxPlanes; ++n) k->symy[s][n] = 1;
+    }
+  }
+  return PIP_OK;
+}
+
+namespace {
+
 // Host copy of the device finalize_dt (same IEEE operations, same order).
 double finalize_dt_host(const KParams &k, const DevCtrl &c, int slot) {
   double dt, rho, gr;

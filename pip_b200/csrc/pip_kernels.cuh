@@ -62,6 +62,15 @@ struct Launchers {
 const Launchers &launchers_fast();
 const Launchers &launchers_exact();
 
+}  // namespace pip
+
+struct pip_params;
+namespace pip {
+
+// Validates a parameter block and fills the kernel parameters without allocating
+// (pip_capi.cu); dx and dy of the result are left null.
+int kparams_from_params(const pip_params *p, KParams *k);
+
 // FP32-mixed form (pip_mixed.cu): A = (hi, lo) FP32 pair, B = FP32 stage state.
 cudaError_t mixed_prepare();
 cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
