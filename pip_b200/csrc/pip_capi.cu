@@ -32,7 +32,7 @@ struct pip_ctx {
   double *A = nullptr, *B = nullptr;  // NV planes each (FP64 form; A stages the mixed form)
   float *Ahi = nullptr, *Alo = nullptr, *Bf = nullptr;  // FP32-mixed form
   bool mixed = false;
-  double *d_dx = nullptr, *d_dy = nullptr;
+  double *d_dx = nullptr, *d_dy = nullptr, *d_rdx = nullptr, *d_rdy = nullptr;
   double *scratch = nullptr;          // NV planes for pip_flux / pip_source
   int *d_flag = nullptr;
   DevCtrl *ctrl = nullptr;
@@ -164,6 +164,8 @@ void build_kparams(pip_ctx *c) {
   k.ir_type = p.flag_ir_type;
   k.nc = (long long)p.ix * p.jx;
   k.gm = p.gm;
+  k.igm1 = 1.0 / (p.gm - 1.0);
+  k.c32g = 3.0 / p.gm / 2.0;
   k.ro_lim = p.ro_lim;
   k.pr_lim = p.pr_lim;
   k.ac = p.col;
@@ -231,6 +233,8 @@ int pip::kparams_from_params(const pip_params *p, KParams *k) {
   k->ir_type = p->flag_ir_type;
   k->nc = (long long)p->ix * p->jx;
   k->gm = p->gm;
+  k->igm1 = 1.0 / (p->gm - 1.0);
+  k->c32g = 3.0 / p->gm / 2.0;
   k->ro_lim = p->ro_lim;
   k->pr_lim = p->pr_lim;
   k->ac = p->col;
@@ -434,6 +438,19 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
     return fail(e);
   c->kp.dx = c->d_dx;
   c->kp.dy = c->d_dy;
+  if (c->mixed) {
+    std::vector<double> r(c->dx.size()), ry(c->dy.size());
+    for (size_t i = 0; i < r.size(); ++i) r[i] = 1.0 / c->dx[i];
+    for (size_t j = 0; j < ry.size(); ++j) ry[j] = 1.0 / c->dy[j];
+    if ((e = cudaMalloc(&c->d_rdx, sizeof(double) * r.size())) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->d_rdy, sizeof(double) * ry.size())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(c->d_rdx, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(e);
+    if ((e = cudaMemcpy(c->d_rdy, ry.data(), sizeof(double) * ry.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(e);
+    c->kp.rdx = c->d_rdx;
+    c->kp.rdy = c->d_rdy;
+  }
   *out = c;
   return PIP_OK;
 }
@@ -450,6 +467,8 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->Bf);
   cudaFree(c->d_dx);
   cudaFree(c->d_dy);
+  cudaFree(c->d_rdx);
+  cudaFree(c->d_rdy);
   cudaFree(c->scratch);
   cudaFree(c->ctrl);
   cudaFree(c->d_flag);

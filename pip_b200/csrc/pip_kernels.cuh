@@ -22,6 +22,8 @@ struct KParams {
   int ir_type;       // IR energy form 1 or 2
   long long nc;      // ix*jx
   double gm, ro_lim, pr_lim, ac, safety;
+  double igm1;       // 1/(gm-1)
+  double c32g;       // 3/gm/2 of the explicit collision energy term
   double sg_all;     // safety*min over all dx, dy, dz (numerator of cmax)
   double col_lim;    // min(safety,0.3) or pip_imp_factor (cfl_pn_col)
   double ir_lim;     // min(safety,0.1) (cfl_pip_ir)
@@ -29,6 +31,7 @@ struct KParams {
   double decay[2];   // Dedner psi factor exp(-(dt_sub/dt)*safety*db_clean) per stage
   double dz0;        // dz(1)
   const double *dx, *dy;
+  const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]
   int gx[2][kMaxMargin], gy[2][kMaxMargin];
   signed char symx[2][kMaxPlanes], symy[2][kMaxPlanes];

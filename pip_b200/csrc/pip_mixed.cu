@@ -23,7 +23,7 @@ namespace mixed {
 constexpr int kH = 2;
 template <int NDIM> struct Tile;
 template <> struct Tile<2> {
-  static constexpr int TX = 32, TY = 8, NT = 256;
+  static constexpr int TX = 32, TY = 7, NT = 256;  // 487 faces = two rounds of 256 threads
 };
 template <> struct Tile<1> {
   static constexpr int TX = 128, TY = 1, NT = 128;
@@ -49,9 +49,10 @@ template <int NVM>
 __device__ __forceinline__ Prim<double> prim_mhd(const double (&u)[NVM], const KParams &p) {
   Prim<double> q;
   const double de = u[0];
-  q.vx = u[1] / de;
-  q.vy = u[2] / de;
-  q.vz = u[3] / de;
+  const double inv = 1.0 / de;
+  q.vx = u[1] * inv;
+  q.vy = u[2] * inv;
+  q.vz = u[3] * inv;
   q.pr = fmax((p.gm - 1.0) * (u[4] - 0.5 * de * (q.vx * q.vx + q.vy * q.vy + q.vz * q.vz) -
                               0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7])), p.pr_lim);
   q.de = fmax(de, p.ro_lim);
@@ -60,17 +61,28 @@ __device__ __forceinline__ Prim<double> prim_mhd(const double (&u)[NVM], const K
 __device__ __forceinline__ Prim<double> prim_hd(const double (&u)[5], const KParams &p) {
   Prim<double> q;
   const double de = u[0];
-  q.vx = u[1] / de;
-  q.vy = u[2] / de;
-  q.vz = u[3] / de;
+  const double inv = 1.0 / de;
+  q.vx = u[1] * inv;
+  q.vy = u[2] * inv;
+  q.vz = u[3] * inv;
   q.pr = fmax((p.gm - 1.0) * (u[4] - 0.5 * de * (q.vx * q.vx + q.vy * q.vy + q.vz * q.vz)), p.pr_lim);
   q.de = fmax(de, p.ro_lim);
   return q;
 }
 
-// Density/pressure floors of cq2pv (Scheme_rot.f90:171-178), applied only when they fire.
+// Density/pressure floors of cq2pv (Scheme_rot.f90:171-178), applied only when they fire;
+// an FP32 estimate skips the FP64 test far from the floors.
 template <int NVM>
 __device__ __forceinline__ void floors_mhd(double (&u)[NVM], const KParams &p) {
+  {
+    const float d = (float)u[0];
+    const float pf = (float)(p.gm - 1.0) *
+                     ((float)u[4] - 0.5f * ((float)u[1] * (float)u[1] + (float)u[2] * (float)u[2] +
+                                            (float)u[3] * (float)u[3]) / d -
+                      0.5f * ((float)u[5] * (float)u[5] + (float)u[6] * (float)u[6] +
+                              (float)u[7] * (float)u[7]));
+    if (d > 2.0f * (float)p.ro_lim && pf > 2.0f * (float)p.pr_lim + 1e-3f * (float)u[4]) return;
+  }
   const double de = u[0];
   const double k = 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / de;
   const double b = 0.5 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
@@ -78,6 +90,13 @@ __device__ __forceinline__ void floors_mhd(double (&u)[NVM], const KParams &p) {
   if (pr <= p.pr_lim || de <= p.ro_lim) cq2pv_mhd<double, NVM>(u, p.gm, p.ro_lim, p.pr_lim);
 }
 __device__ __forceinline__ void floors_hd(double (&u)[5], const KParams &p) {
+  {
+    const float d = (float)u[0];
+    const float pf = (float)(p.gm - 1.0) *
+                     ((float)u[4] - 0.5f * ((float)u[1] * (float)u[1] + (float)u[2] * (float)u[2] +
+                                            (float)u[3] * (float)u[3]) / d);
+    if (d > 2.0f * (float)p.ro_lim && pf > 2.0f * (float)p.pr_lim + 1e-3f * (float)u[4]) return;
+  }
   const double de = u[0];
   const double pr = (p.gm - 1.0) * (u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / de);
   if (pr <= p.pr_lim || de <= p.ro_lim) cq2pv_hd<double>(u, p.gm, p.ro_lim, p.pr_lim);
@@ -102,10 +121,10 @@ __device__ __forceinline__ void collision_ds(const double (&um)[NVM], const doub
                                              const Prim<double> &qm, const Prim<double> &qh,
                                              const KParams &p, double dt_coll, double (&ds)[5]) {
   const double gm = p.gm, ac = p.ac;
-  const double te = qm.pr / qm.de * gm * kMuP;
-  const double nte = qh.pr / qh.de * gm * kMuN;
   ds[0] = 0.0;
   if (p.imp) {
+    const double te = qm.pr / qm.de * gm * kMuP;
+    const double nte = qh.pr / qh.de * gm * kMuN;
     const double temp = dt_coll * (uh[0] + um[0]);
     const double e = (1.0 - exp(-ac * temp));
     ds[1] = (um[0] * uh[1] - uh[0] * um[1]) * e / temp;
@@ -128,10 +147,12 @@ __device__ __forceinline__ void collision_ds(const double (&um)[NVM], const doub
     ds[1] = ac * (um[0] * uh[1] - uh[0] * um[1]);
     ds[2] = ac * (um[0] * uh[2] - uh[0] * um[2]);
     ds[3] = ac * (um[0] * uh[3] - uh[0] * um[3]);
+    // 3/gm/2 (nte - te) with te = 0.5 gm pr/de, nte = gm npr/nde: the gm cancels
+    const double dte = 1.5 * (qh.pr / qh.de - 0.5 * (qm.pr / qm.de));
     ds[4] = ac * qh.de * qm.de *
             (0.5 * ((qh.vx * qh.vx - qm.vx * qm.vx) + (qh.vy * qh.vy - qm.vy * qm.vy) +
                     (qh.vz * qh.vz - qm.vz * qm.vz)) +
-             3.0 / gm / 2.0 * (nte - te));
+             dte);
   }
 }
 
@@ -150,15 +171,21 @@ __device__ __forceinline__ void ir_ds(const Prim<double> &qm, const Prim<double>
     ds[4] = kin - gi * qh.pr / (gm - 1.0) + gr * qm.pr / (gm - 1.0);
 }
 
-// Stores one plane value (and its ghost images) -- the sign tables of PIPbnd.
-constexpr int kMaxTargets = 2 * kMaxMargin + (2 * kMaxMargin) * (2 * kMaxMargin) + 2 * kMaxMargin;
-struct Targets {
-  int n, q[kMaxTargets];
-  signed char sx[kMaxTargets], sy[kMaxTargets];
-};
+// Ghost images of one updated cell (PIPbnd after the stage, x faces then y faces, so a
+// corner ghost carries both sign flips).  Only cells within 2*margin of a boundary can be
+// a ghost source; the caller tests that first.  The values are re-read from the planes the
+// same thread has just written.
+template <int NDIM>
+__device__ __forceinline__ bool near_boundary(const KParams &p, int gi, int gj) {
+  return gi < 2 * p.m0 || gi >= p.ix - 2 * p.m0 ||
+         (NDIM == 2 && (gj < 2 * p.m1 || gj >= p.jx - 2 * p.m1));
+}
 
 template <int NDIM>
-__device__ __forceinline__ void ghost_targets(const KParams &p, int gi, int gj, Targets &t) {
+__device__ __noinline__ void write_ghosts(const KParams &p, int gi, int gj, float *hi, float *lo,
+                                          int nplanes) {
+  const long long nc = p.nc;
+  const long long q = (long long)gj * p.ix + gi;
   int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
   int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
   for (int s = 0; s < 2; ++s)
@@ -174,32 +201,29 @@ __device__ __forceinline__ void ghost_targets(const KParams &p, int gi, int gj, 
           ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
           sy[nty++] = s;
         }
-  t.n = 0;
-  for (int a = 0; a < ntx; ++a) {
-    t.q[t.n] = gj * p.ix + tx[a];
-    t.sx[t.n] = (signed char)sx[a];
-    t.sy[t.n] = -1;
-    ++t.n;
+#pragma unroll 1
+  for (int n = 0; n < nplanes; ++n) {
+    const float h = hi[q + n * nc];
+    const float w = lo ? lo[q + n * nc] : 0.0f;
+    for (int a = 0; a < ntx; ++a) {
+      const float g = (float)p.symx[sx[a]][n];
+      const long long t = (long long)gj * p.ix + tx[a];
+      hi[t + n * nc] = g * h;
+      if (lo) lo[t + n * nc] = g * w;
+      for (int b = 0; b < nty; ++b) {
+        const float g2 = (float)p.symy[sy[b]][n];
+        const long long c = (long long)ty[b] * p.ix + tx[a];
+        hi[c + n * nc] = g2 * (g * h);
+        if (lo) lo[c + n * nc] = g2 * (g * w);
+      }
+    }
     for (int b = 0; b < nty; ++b) {
-      t.q[t.n] = ty[b] * p.ix + tx[a];
-      t.sx[t.n] = (signed char)sx[a];
-      t.sy[t.n] = (signed char)sy[b];
-      ++t.n;
+      const float g2 = (float)p.symy[sy[b]][n];
+      const long long t = (long long)ty[b] * p.ix + gi;
+      hi[t + n * nc] = g2 * h;
+      if (lo) lo[t + n * nc] = g2 * w;
     }
   }
-  for (int b = 0; b < nty; ++b) {
-    t.q[t.n] = ty[b] * p.ix + gi;
-    t.sx[t.n] = -1;
-    t.sy[t.n] = (signed char)sy[b];
-    ++t.n;
-  }
-}
-
-__device__ __forceinline__ float gsign(const KParams &p, const Targets &t, int k, int plane) {
-  float s = 1.0f;
-  if (t.sx[k] >= 0) s *= (float)p.symx[t.sx[k]][plane];
-  if (t.sy[k] >= 0) s *= (float)p.symy[t.sy[k]][plane];
-  return s;
 }
 
 template <int NT>
@@ -295,6 +319,7 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
     ctrl->red_gr[ns] = 0ull;
   }
   const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  const float igm1f = (float)p.igm1;
   const int i0 = p.m0 + blockIdx.x * TX;
   const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
   const long long nc = p.nc;
@@ -356,7 +381,7 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
       }
       vl[0] = fmaxf(vl[0], rolf);
       vr[0] = fmaxf(vr[0], rolf);
-      hlld_flux<float, NVM>(vl, vr, fx, gmf, cmaxf);
+      hlld_flux_rcp<float, NVM>(vl, vr, fx, gmf, igm1f, cmaxf);
 #pragma unroll
       for (int n = 0; n < NVM; ++n) {
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
@@ -389,7 +414,7 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
       }
       vl[0] = fmaxf(vl[0], rolf);
       vr[0] = fmaxf(vr[0], rolf);
-      hllc_flux<float>(vl, vr, fx, gmf);
+      hllc_flux_rcp<float>(vl, vr, fx, gmf, igm1f);
 #pragma unroll
       for (int n = 0; n < 5; ++n) {
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
@@ -402,7 +427,7 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
   // ---- 3. FP64 source and compensated update
   const int ti = tid % TX, tj = tid / TX;
   const int gi = i0 + ti, gj = j0 + tj;
-  const bool valid = gi < iend && (NDIM == 1 || gj < jend);
+  const bool valid = tj < TY && gi < iend && (NDIM == 1 || gj < jend);
   double dtc = 10.0, rhoc = 0.0, grc = 0.0;
   if (valid) {
     const long long q = (long long)gj * p.ix + gi;
@@ -473,8 +498,8 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
         }
       }
     }
-    const double cx = dt_sub / p.dx[gi];
-    const double cy = NDIM == 2 ? dt_sub / p.dy[gj] : 0.0;
+    const double cx = dt_sub * p.rdx[gi];
+    const double cy = NDIM == 2 ? dt_sub * p.rdy[gj] : 0.0;
     const int fxl = tj * (TX + 1) + ti, fyl = tj * TX + ti;
     double n_m[NVM], n_h[5];
 #pragma unroll
@@ -498,7 +523,7 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
       }
     }
     if (NVM == 9) n_m[NVM - 1] *= p.decay[STAGE - 1];
-    const int ep = s_epi;
+    const int ep = STAGE == 1 ? 0 : s_epi;  // stage 1 is never followed by a cfl
     if (ep >= 1) {
       floors_mhd<NVM>(n_m, p);
       floors_hd(n_h, p);
@@ -529,21 +554,14 @@ stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, c
 #pragma unroll
     for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
     if (bad) atomicOr(&ctrl->nan_flag, 1);
-    Targets tg;
-    ghost_targets<NDIM>(p, gi, gj, tg);
 #pragma unroll
     for (int n = 0; n < NV; ++n) {
       const double u = n < NVM ? n_m[n] : n_h[n - NVM];
       const float hi = (float)u;
-      const float lo = (float)(u - (double)hi);
       Ohi[q + n * nc] = hi;
-      if (STAGE == 2) Olo[q + n * nc] = lo;
-      for (int k = 0; k < tg.n; ++k) {
-        const float sgn = gsign(p, tg, k, n);
-        Ohi[tg.q[k] + n * nc] = sgn * hi;
-        if (STAGE == 2) Olo[tg.q[k] + n * nc] = sgn * lo;
-      }
+      if (STAGE == 2) Olo[q + n * nc] = (float)(u - (double)hi);
     }
+    if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, Ohi, STAGE == 2 ? Olo : nullptr, NV);
   }
   if (STAGE == 2 && s_epi == 2) block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   if (STAGE == 2 && dt_mode == 1) {

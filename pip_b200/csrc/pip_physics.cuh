@@ -109,6 +109,45 @@ __device__ __forceinline__ Prim<R> cq2pv_hd(R (&u)[5], R gm, R ro_lim, R pr_lim)
   return q;
 }
 
+// cq2pv with one division per species (reciprocal form, see below).
+template <typename R, int NVM>
+__device__ __forceinline__ Prim<R> cq2pv_mhd_rcp(R (&u)[NVM], R gm, R igm1, R ro_lim, R pr_lim) {
+  Prim<R> q;
+  R de = u[0];
+  const R inv = R(1) / de;
+  R vx = u[1] * inv, vy = u[2] * inv, vz = u[3] * inv;
+  const R kin = vx * vx + vy * vy + vz * vz;
+  const R bb = u[5] * u[5] + u[6] * u[6] + u[7] * u[7];
+  R pr = (gm - R(1)) * (u[4] - R(0.5) * de * kin - R(0.5) * bb);
+  pr = rmax(pr, pr_lim);
+  de = rmax(de, ro_lim);
+  u[0] = de;
+  u[1] = vx * de;
+  u[2] = vy * de;
+  u[3] = vz * de;
+  u[4] = pr * igm1 + R(0.5) * de * kin + R(0.5) * bb;
+  q.de = de; q.vx = vx; q.vy = vy; q.vz = vz; q.pr = pr;
+  return q;
+}
+template <typename R>
+__device__ __forceinline__ Prim<R> cq2pv_hd_rcp(R (&u)[5], R gm, R igm1, R ro_lim, R pr_lim) {
+  Prim<R> q;
+  R de = u[0];
+  const R inv = R(1) / de;
+  R vx = u[1] * inv, vy = u[2] * inv, vz = u[3] * inv;
+  const R kin = vx * vx + vy * vy + vz * vz;
+  R pr = (gm - R(1)) * (u[4] - R(0.5) * de * kin);
+  pr = rmax(pr, pr_lim);
+  de = rmax(de, ro_lim);
+  u[0] = de;
+  u[1] = vx * de;
+  u[2] = vy * de;
+  u[3] = vz * de;
+  u[4] = pr * igm1 + R(0.5) * de * kin;
+  q.de = de; q.vx = vx; q.vy = vy; q.vz = vz; q.pr = pr;
+  return q;
+}
+
 // CFL candidates of one interior cell (cfl_mhd Scheme_rot.f90:279-283, cfl_hd :229-233),
 // from the primitives of the cq2pv rewrite.  sg = safety*gmin.
 template <typename R>
@@ -370,6 +409,257 @@ __device__ __forceinline__ void hlld_flux(const R (&v_l)[NVM], const R (&v_r)[NV
   for (int n = 0; n < 8; ++n) flx[n] = out[n];
   if (NVM == 9) {
     // Dedner flux (HLL_rot.f90:904-908) with ch = cmax
+    const R ch = cmax;
+    flx[5] = R(0.5) * (v_l[NVM - 1] + v_r[NVM - 1] - ch * (v_r[5] - v_l[5]));
+    flx[NVM - 1] = R(0.5) * (ch * ch * (v_l[5] + v_r[5]) - ch * (v_r[NVM - 1] - v_l[NVM - 1]));
+  }
+}
+
+// ---------------------------------------------------------------- reciprocal forms
+//
+// The same Riemann solvers with the divisions folded: a shared denominator is inverted
+// once, u/rho of a state built as rho*v is taken as v, and p/(gm-1) uses a precomputed
+// 1/(gm-1).  Results differ from the literal forms above by a few ulps per face; they are
+// used by the FMA build (held to 1e-10 relative L1 against the oracle over whole runs)
+// and by the FP32-mixed form.
+
+__device__ __forceinline__ double rrsqrt(double a) { return rsqrt(a); }
+__device__ __forceinline__ float rrsqrt(float a) { return rsqrtf(a); }
+
+// HLLC smooth switch (|s|+s)/max(2s,eps) without a division: 1 for s >= eps/2, 0 for s<=0.
+template <typename R>
+__device__ __forceinline__ R hllc_switch(R s) {
+  return s >= R(0.5 * kHllcEpsi) ? R(1) : (s > R(0) ? R(2) * s * R(1.0 / kHllcEpsi) : R(0));
+}
+
+template <typename R>
+__device__ __forceinline__ void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R gm,
+                                              R igm1) {
+  R u_l[5], u_r[5], fl[5], fr[5], stl[5], str[5];
+  const R ke_l = v_l[1] * v_l[1] + v_l[2] * v_l[2] + v_l[3] * v_l[3];
+  const R ke_r = v_r[1] * v_r[1] + v_r[2] * v_r[2] + v_r[3] * v_r[3];
+  u_l[0] = v_l[0]; u_l[1] = v_l[0] * v_l[1]; u_l[2] = v_l[0] * v_l[2]; u_l[3] = v_l[0] * v_l[3];
+  u_l[4] = v_l[4] * igm1 + R(0.5) * v_l[0] * ke_l;
+  u_r[0] = v_r[0]; u_r[1] = v_r[0] * v_r[1]; u_r[2] = v_r[0] * v_r[2]; u_r[3] = v_r[0] * v_r[3];
+  u_r[4] = v_r[4] * igm1 + R(0.5) * v_r[0] * ke_r;
+  const R pr_l = v_l[4], pr_r = v_r[4];
+  const R vn_l = v_l[1], vn_r = v_r[1];
+  fl[0] = u_l[1];
+  fr[0] = u_r[1];
+  fl[1] = pr_l + u_l[1] * vn_l;
+  fr[1] = pr_r + u_r[1] * vn_r;
+  fl[2] = u_l[2] * vn_l;
+  fr[2] = u_r[2] * vn_r;
+  fl[3] = u_l[3] * vn_l;
+  fr[3] = u_r[3] * vn_r;
+  fl[4] = (u_l[4] + pr_l) * vn_l;
+  fr[4] = (u_r[4] + pr_r) * vn_r;
+  const R cs_l = rsqrt_(gm * pr_l / v_l[0]);
+  const R cs_r = rsqrt_(gm * pr_r / v_r[0]);
+  const R sl = R(kHllcAcc) * rmin(vn_l - cs_l, vn_r - cs_r);
+  const R sr = R(kHllcAcc) * rmax(vn_l + cs_l, vn_r + cs_r);
+  const R ql = u_l[0] * (sl - vn_l), qr = u_r[0] * (sr - vn_r);
+  const R sm = (u_r[1] * (sr - vn_r) - u_l[1] * (sl - vn_l) + pr_l - pr_r) / (qr - ql);
+  const R pr_m = sm * ql - u_l[1] * (sl - vn_l) + pr_l;
+  const R il = R(1) / (sl - sm), ir = R(1) / (sr - sm);
+  stl[0] = ql * il;
+  str[0] = qr * ir;
+  stl[1] = stl[0] * sm;
+  str[1] = str[0] * sm;
+  stl[2] = stl[0] * v_l[2];
+  str[2] = str[0] * v_r[2];
+  stl[3] = stl[0] * v_l[3];
+  str[3] = str[0] * v_r[3];
+  stl[4] = ((sl - vn_l) * u_l[4] - pr_l * vn_l + pr_m * sm) * il;
+  str[4] = ((sr - vn_r) * u_r[4] - pr_r * vn_r + pr_m * sm) * ir;
+  const R thl = hllc_switch(sl);
+  const R thm = hllc_switch(sm);
+  const R thr = R(1) - hllc_switch(sr);
+#pragma unroll
+  for (int n = 0; n < 5; ++n)
+    flx[n] = thr * fr[n] + thl * fl[n] +
+             (R(1) - thl - thr) * (thm * (fl[n] + sl * (stl[n] - u_l[n])) +
+                                   (R(1) - thm) * (fr[n] + sr * (str[n] - u_r[n])));
+}
+
+template <typename R, int NVM>
+__device__ __forceinline__ void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM],
+                                              R gm, R igm1, R cmax) {
+  const R b2_l = (v_l[5] * v_l[5] + v_l[6] * v_l[6] + v_l[7] * v_l[7]);
+  const R b2_r = (v_r[5] * v_r[5] + v_r[6] * v_r[6] + v_r[7] * v_r[7]);
+  const R el = v_l[4] * igm1 + R(0.5) * v_l[0] * (v_l[1] * v_l[1] + v_l[2] * v_l[2] + v_l[3] * v_l[3]) +
+               R(0.5) * b2_l;
+  const R er = v_r[4] * igm1 + R(0.5) * v_r[0] * (v_r[1] * v_r[1] + v_r[2] * v_r[2] + v_r[3] * v_r[3]) +
+               R(0.5) * b2_r;
+  R u_l[8], u_r[8];
+  u_l[0] = v_l[0]; u_l[1] = v_l[0] * v_l[1]; u_l[2] = v_l[0] * v_l[2]; u_l[3] = v_l[0] * v_l[3];
+  u_l[4] = el; u_l[5] = v_l[5]; u_l[6] = v_l[6]; u_l[7] = v_l[7];
+  u_r[0] = v_r[0]; u_r[1] = v_r[0] * v_r[1]; u_r[2] = v_r[0] * v_r[2]; u_r[3] = v_r[0] * v_r[3];
+  u_r[4] = er; u_r[5] = v_r[5]; u_r[6] = v_r[6]; u_r[7] = v_r[7];
+  const R pt_l = v_l[4] + R(0.5) * b2_l;
+  const R pt_r = v_r[4] + R(0.5) * b2_r;
+  const R vbL = v_l[1] * v_l[5] + v_l[2] * v_l[6] + v_l[3] * v_l[7];
+  const R vbR = v_r[1] * v_r[5] + v_r[2] * v_r[6] + v_r[3] * v_r[7];
+  R fl[8], fr[8];
+  fl[0] = u_l[1];
+  fl[1] = u_l[1] * v_l[1] + pt_l - v_l[5] * v_l[5];
+  fl[2] = u_l[1] * v_l[2] - v_l[5] * v_l[6];
+  fl[3] = u_l[1] * v_l[3] - v_l[5] * v_l[7];
+  fl[4] = (u_l[4] + pt_l) * v_l[1] - vbL * v_l[5];
+  fl[5] = R(0);
+  fl[6] = v_l[1] * v_l[6] - v_l[5] * v_l[2];
+  fl[7] = v_l[1] * v_l[7] - v_l[5] * v_l[3];
+  fr[0] = u_r[1];
+  fr[1] = u_r[1] * v_r[1] + pt_r - v_r[5] * v_r[5];
+  fr[2] = u_r[1] * v_r[2] - v_r[5] * v_r[6];
+  fr[3] = u_r[1] * v_r[3] - v_r[5] * v_r[7];
+  fr[4] = (u_r[4] + pt_r) * v_r[1] - vbR * v_r[5];
+  fr[5] = R(0);
+  fr[6] = v_r[1] * v_r[6] - v_r[5] * v_r[2];
+  fr[7] = v_r[1] * v_r[7] - v_r[5] * v_r[3];
+
+  R f1 = gm * v_l[4];
+  const R vf_l = rsqrt_(((f1 + b2_l) + rsqrt_(rmax((f1 + b2_l) * (f1 + b2_l) - R(4) * f1 * (v_l[5] * v_l[5]), R(0)))) /
+                        (R(2) * v_l[0]));
+  f1 = gm * v_r[4];
+  const R vf_r = rsqrt_(((f1 + b2_r) + rsqrt_(rmax((f1 + b2_r) * (f1 + b2_r) - R(4) * f1 * (v_r[5] * v_r[5]), R(0)))) /
+                        (R(2) * v_r[0]));
+  const R sl = rmin(v_l[1], v_r[1]) - rmax(vf_l, vf_r);
+  const R sr = rmax(v_l[1], v_r[1]) + rmax(vf_l, vf_r);
+
+  R out[8];
+  if (sl >= R(0)) {
+#pragma unroll
+    for (int n = 0; n < 8; ++n) out[n] = fl[n];
+  } else if (sr <= R(0)) {
+#pragma unroll
+    for (int n = 0; n < 8; ++n) out[n] = fr[n];
+  } else {
+    f1 = R(1) / (sr - sl);
+    R uh[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) uh[n] = f1 * (sr * u_r[n] - sl * u_l[n] - fr[n] + fl[n]);
+    const R iuh0 = R(1) / uh[0];
+    const R sm = uh[1] * iuh0;
+    const R pt = pt_l + v_l[0] * (sl - v_l[1]) * (sm - v_l[1]);
+    const R ilm = R(1) / (sl - sm), irm = R(1) / (sr - sm);
+    const R ro_l1 = v_l[0] * (sl - v_l[1]) * ilm;
+    const R ro_r1 = v_r[0] * (sr - v_r[1]) * irm;
+    const R rs_l = rrsqrt(ro_l1), rs_r = rrsqrt(ro_r1);
+    const R bn = uh[5], bn2 = bn * bn;
+    const R sal = rabs(bn) * rs_l;
+    const R sar = rabs(bn) * rs_r;
+
+    if ((sl >= (sm - R(kHllgFactor) * sal)) || ((sm + R(kHllgFactor) * sar) >= sr)) {
+      const R vy_2 = uh[2] * iuh0;
+      const R vz_2 = uh[3] * iuh0;
+      if (sm >= R(0)) {
+        const R e2 = ((sl - v_l[1]) * u_l[4] - pt_l * v_l[1] + pt * sm +
+                      bn * (vbL - sm * bn - vy_2 * uh[6] - vz_2 * uh[7])) * ilm;
+        out[0] = sl * (ro_l1 - v_l[0]) + fl[0];
+        out[1] = sl * (ro_l1 * sm - u_l[1]) + fl[1];
+        out[2] = sl * (ro_l1 * vy_2 - u_l[2]) + fl[2];
+        out[3] = sl * (ro_l1 * vz_2 - u_l[3]) + fl[3];
+        out[4] = sl * (e2 - u_l[4]) + fl[4];
+#pragma unroll
+        for (int n = 5; n < 8; ++n) out[n] = sl * (uh[n] - v_l[n]) + fl[n];
+      } else {
+        const R e2 = ((sr - v_r[1]) * u_r[4] - pt_r * v_r[1] + pt * sm +
+                      bn * (vbR - sm * bn - vy_2 * uh[6] - vz_2 * uh[7])) * irm;
+        out[0] = sr * (ro_r1 - v_r[0]) + fr[0];
+        out[1] = sr * (ro_r1 * sm - u_r[1]) + fr[1];
+        out[2] = sr * (ro_r1 * vy_2 - u_r[2]) + fr[2];
+        out[3] = sr * (ro_r1 * vz_2 - u_r[3]) + fr[3];
+        out[4] = sr * (e2 - u_r[4]) + fr[4];
+#pragma unroll
+        for (int n = 5; n < 8; ++n) out[n] = sr * (uh[n] - v_r[n]) + fr[n];
+      }
+    } else {
+      R ul1[8], ur1[8];
+      const R dl = v_l[0] * (sl - v_l[1]);
+      f1 = R(1) / (dl * (sl - sm) - bn2);
+      const R gl = f1 * (dl * (sl - v_l[1]) - bn2);
+      ul1[5] = bn;
+      ul1[6] = v_l[6] * gl;
+      ul1[7] = v_l[7] * gl;
+      const R vy_l1 = v_l[2] - f1 * bn * v_l[6] * (sm - v_l[1]);
+      const R vz_l1 = v_l[3] - f1 * bn * v_l[7] * (sm - v_l[1]);
+      ul1[0] = ro_l1;
+      ul1[4] = ((sl - v_l[1]) * u_l[4] - pt_l * v_l[1] + pt * sm +
+                bn * (vbL - sm * bn - vy_l1 * ul1[6] - vz_l1 * ul1[7])) * ilm;
+      ul1[1] = ro_l1 * sm;
+      ul1[2] = ro_l1 * vy_l1;
+      ul1[3] = ro_l1 * vz_l1;
+
+      const R dr = v_r[0] * (sr - v_r[1]);
+      f1 = R(1) / (dr * (sr - sm) - bn2);
+      const R gr = f1 * (dr * (sr - v_r[1]) - bn2);
+      ur1[5] = bn;
+      ur1[6] = v_r[6] * gr;
+      ur1[7] = v_r[7] * gr;
+      const R vy_r1 = v_r[2] - f1 * bn * v_r[6] * (sm - v_r[1]);
+      const R vz_r1 = v_r[3] - f1 * bn * v_r[7] * (sm - v_r[1]);
+      ur1[0] = ro_r1;
+      ur1[4] = ((sr - v_r[1]) * u_r[4] - pt_r * v_r[1] + pt * sm +
+                bn * (vbR - sm * bn - vy_r1 * ur1[6] - vz_r1 * ur1[7])) * irm;
+      ur1[1] = ro_r1 * sm;
+      ur1[2] = ro_r1 * vy_r1;
+      ur1[3] = ro_r1 * vz_r1;
+
+      const R sl1 = sm - sal;
+      const R sr1 = sm + sar;
+      if (sl1 >= R(0)) {
+        out[0] = sl * (ul1[0] - v_l[0]) + fl[0];
+#pragma unroll
+        for (int n = 1; n < 5; ++n) out[n] = sl * (ul1[n] - u_l[n]) + fl[n];
+#pragma unroll
+        for (int n = 5; n < 8; ++n) out[n] = sl * (ul1[n] - v_l[n]) + fl[n];
+      } else if (sr1 <= R(0)) {
+        out[0] = sr * (ur1[0] - v_r[0]) + fr[0];
+#pragma unroll
+        for (int n = 1; n < 5; ++n) out[n] = sr * (ur1[n] - u_r[n]) + fr[n];
+#pragma unroll
+        for (int n = 5; n < 8; ++n) out[n] = sr * (ur1[n] - v_r[n]) + fr[n];
+      } else {
+        const R ro_ls = ro_l1 * rs_l;   // sqrt(ro_l1)
+        const R ro_rs = ro_r1 * rs_r;
+        f1 = R(1) / (ro_ls + ro_rs);
+        const R f2 = rsign1(bn);
+        const R vy_2 = f1 * (ro_ls * vy_l1 + ro_rs * vy_r1 + (ur1[6] - ul1[6]) * f2);
+        const R vz_2 = f1 * (ro_ls * vz_l1 + ro_rs * vz_r1 + (ur1[7] - ul1[7]) * f2);
+        R u2[8];
+        u2[5] = bn;
+        u2[6] = f1 * (ro_ls * ur1[6] + ro_rs * ul1[6] + ro_ls * ro_rs * (vy_r1 - vy_l1) * f2);
+        u2[7] = f1 * (ro_ls * ur1[7] + ro_rs * ul1[7] + ro_ls * ro_rs * (vz_r1 - vz_l1) * f2);
+        if (sm >= R(0)) {
+          u2[0] = ro_l1;
+          u2[4] = ul1[4] - ro_ls * (vy_l1 * ul1[6] + vz_l1 * ul1[7] - vy_2 * u2[6] - vz_2 * u2[7]) * f2;
+          u2[1] = ro_l1 * sm;
+          u2[2] = ro_l1 * vy_2;
+          u2[3] = ro_l1 * vz_2;
+          out[0] = sl1 * u2[0] - (sl1 - sl) * ul1[0] - sl * v_l[0] + fl[0];
+#pragma unroll
+          for (int n = 1; n < 5; ++n) out[n] = sl1 * u2[n] - (sl1 - sl) * ul1[n] - sl * u_l[n] + fl[n];
+#pragma unroll
+          for (int n = 5; n < 8; ++n) out[n] = sl1 * u2[n] - (sl1 - sl) * ul1[n] - sl * v_l[n] + fl[n];
+        } else {
+          u2[0] = ro_r1;
+          u2[4] = ur1[4] + ro_rs * (vy_r1 * ur1[6] + vz_r1 * ur1[7] - vy_2 * u2[6] - vz_2 * u2[7]) * f2;
+          u2[1] = ro_r1 * sm;
+          u2[2] = ro_r1 * vy_2;
+          u2[3] = ro_r1 * vz_2;
+          out[0] = sr1 * u2[0] - (sr1 - sr) * ur1[0] - sr * v_r[0] + fr[0];
+#pragma unroll
+          for (int n = 1; n < 5; ++n) out[n] = sr1 * u2[n] - (sr1 - sr) * ur1[n] - sr * u_r[n] + fr[n];
+#pragma unroll
+          for (int n = 5; n < 8; ++n) out[n] = sr1 * u2[n] - (sr1 - sr) * ur1[n] - sr * v_r[n] + fr[n];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 8; ++n) flx[n] = out[n];
+  if (NVM == 9) {
     const R ch = cmax;
     flx[5] = R(0.5) * (v_l[NVM - 1] + v_r[NVM - 1] - ch * (v_r[5] - v_l[5]));
     flx[NVM - 1] = R(0.5) * (ch * ch * (v_l[5] + v_r[5]) - ch * (v_r[NVM - 1] - v_l[NVM - 1]));

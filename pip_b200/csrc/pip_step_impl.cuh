@@ -17,12 +17,48 @@ namespace PIP_FLAVOUR {
 constexpr int kH = 2;  // stencil half-width of minmod MUSCL
 
 template <int NDIM> struct Tile;
+// 32x7 cells: 33x7 x faces + 32x8 y faces = 487 faces = two rounds of 256 threads.
 template <> struct Tile<2> {
-  static constexpr int TX = 32, TY = 8, NT = 256;
+  static constexpr int TX = 32, TY = 7, NT = 256;
 };
 template <> struct Tile<1> {
   static constexpr int TX = 128, TY = 1, NT = 128;
 };
+
+// Conversions and Riemann solvers of this flavour: the literal reference expressions
+// (FMA-free build) or the reciprocal forms (FMA build).
+template <int NVM>
+__device__ __forceinline__ Prim<double> rt_mhd(double (&u)[NVM], const KParams &p) {
+#if PIP_RCP
+  return cq2pv_mhd_rcp<double, NVM>(u, p.gm, p.igm1, p.ro_lim, p.pr_lim);
+#else
+  return cq2pv_mhd<double, NVM>(u, p.gm, p.ro_lim, p.pr_lim);
+#endif
+}
+__device__ __forceinline__ Prim<double> rt_hd(double (&u)[5], const KParams &p) {
+#if PIP_RCP
+  return cq2pv_hd_rcp<double>(u, p.gm, p.igm1, p.ro_lim, p.pr_lim);
+#else
+  return cq2pv_hd<double>(u, p.gm, p.ro_lim, p.pr_lim);
+#endif
+}
+template <int NVM>
+__device__ __forceinline__ void riemann_mhd(const double (&vl)[NVM], const double (&vr)[NVM],
+                                            double (&f)[NVM], const KParams &p, double cmax) {
+#if PIP_RCP
+  hlld_flux_rcp<double, NVM>(vl, vr, f, p.gm, p.igm1, cmax);
+#else
+  hlld_flux<double, NVM>(vl, vr, f, p.gm, cmax);
+#endif
+}
+__device__ __forceinline__ void riemann_hd(const double (&vl)[5], const double (&vr)[5],
+                                           double (&f)[5], const KParams &p) {
+#if PIP_RCP
+  hllc_flux_rcp<double>(vl, vr, f, p.gm, p.igm1);
+#else
+  hllc_flux<double>(vl, vr, f, p.gm);
+#endif
+}
 
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
@@ -123,9 +159,50 @@ __device__ __forceinline__ void load_cell(const double *__restrict__ U, long lon
   for (int n = 0; n < 5; ++n) uh[n] = U[q + (NVM + n) * nc];
 }
 
-// Writes a cell and every ghost cell the boundary conditions copy from it (PIPbnd after
-// the stage: x faces first, then y faces, Boundary_rot.f90:54-125 order, so a corner
-// ghost carries both sign flips).
+// Ghost images of one updated cell (PIPbnd after the stage: x faces first, then y faces,
+// Boundary_rot.f90:54-125 order, so a corner ghost carries both sign flips).  Only cells
+// within 2*margin of a boundary can be a ghost source; the values are re-read from the
+// planes the same thread has just written.
+template <int NDIM>
+__device__ __forceinline__ bool near_boundary(const KParams &p, int gi, int gj) {
+  return gi < 2 * p.m0 || gi >= p.ix - 2 * p.m0 ||
+         (NDIM == 2 && (gj < 2 * p.m1 || gj >= p.jx - 2 * p.m1));
+}
+
+template <int NDIM>
+__device__ __forceinline__ void write_ghosts(const KParams &p, int gi, int gj, double *U, int nplanes) {
+  const long long nc = p.nc;
+  const long long q = (long long)gj * p.ix + gi;
+  int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
+  int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
+  for (int s = 0; s < 2; ++s)
+    for (int l = 0; l < p.m0; ++l)
+      if (p.gx[s][l] == gi) {
+        tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
+        sx[ntx++] = s;
+      }
+  if (NDIM == 2)
+    for (int s = 0; s < 2; ++s)
+      for (int l = 0; l < p.m1; ++l)
+        if (p.gy[s][l] == gj) {
+          ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
+          sy[nty++] = s;
+        }
+#pragma unroll 1
+  for (int n = 0; n < nplanes; ++n) {
+    const double v = U[q + n * nc];
+    for (int a = 0; a < ntx; ++a) {
+      const double g = (double)p.symx[sx[a]][n];
+      U[(long long)gj * p.ix + tx[a] + n * nc] = g * v;
+      for (int b = 0; b < nty; ++b)
+        U[(long long)ty[b] * p.ix + tx[a] + n * nc] = (double)p.symy[sy[b]][n] * (g * v);
+    }
+    for (int b = 0; b < nty; ++b)
+      U[(long long)ty[b] * p.ix + gi + n * nc] = (double)p.symy[sy[b]][n] * v;
+  }
+}
+
+// Writes a cell and its ghost images.
 template <int NDIM, int NVM>
 __device__ __forceinline__ void store_cell(double *U, const KParams &p, int gi, int gj,
                                            const double (&um)[NVM], const double (&uh)[5]) {
@@ -135,50 +212,7 @@ __device__ __forceinline__ void store_cell(double *U, const KParams &p, int gi, 
   for (int n = 0; n < NVM; ++n) U[q + n * nc] = um[n];
 #pragma unroll
   for (int n = 0; n < 5; ++n) U[q + (NVM + n) * nc] = uh[n];
-  // ghost targets along x and y (at most 2*margin each)
-  int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
-  int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
-  for (int s = 0; s < 2; ++s)
-    for (int l = 0; l < p.m0; ++l)
-      if (p.gx[s][l] == gi) {
-        tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
-        sx[ntx] = s;
-        ++ntx;
-      }
-  if (NDIM == 2) {
-    for (int s = 0; s < 2; ++s)
-      for (int l = 0; l < p.m1; ++l)
-        if (p.gy[s][l] == gj) {
-          ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
-          sy[nty] = s;
-          ++nty;
-        }
-  }
-  for (int a = 0; a < ntx; ++a) {
-    const long long qg = (long long)gj * p.ix + tx[a];
-    const signed char *sg = p.symx[sx[a]];
-#pragma unroll
-    for (int n = 0; n < NVM; ++n) U[qg + n * nc] = (double)sg[n] * um[n];
-#pragma unroll
-    for (int n = 0; n < 5; ++n) U[qg + (NVM + n) * nc] = (double)sg[NVM + n] * uh[n];
-    for (int b = 0; b < nty; ++b) {
-      const long long qc = (long long)ty[b] * p.ix + tx[a];
-      const signed char *sh = p.symy[sy[b]];
-#pragma unroll
-      for (int n = 0; n < NVM; ++n) U[qc + n * nc] = (double)sh[n] * ((double)sg[n] * um[n]);
-#pragma unroll
-      for (int n = 0; n < 5; ++n)
-        U[qc + (NVM + n) * nc] = (double)sh[NVM + n] * ((double)sg[NVM + n] * uh[n]);
-    }
-  }
-  for (int b = 0; b < nty; ++b) {
-    const long long qg = (long long)ty[b] * p.ix + gi;
-    const signed char *sh = p.symy[sy[b]];
-#pragma unroll
-    for (int n = 0; n < NVM; ++n) U[qg + n * nc] = (double)sh[n] * um[n];
-#pragma unroll
-    for (int n = 0; n < 5; ++n) U[qg + (NVM + n) * nc] = (double)sh[NVM + n] * uh[n];
-  }
+  if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, U, NVM + 5);
 }
 
 // Block-wide min/max into the reduction slots (one atomic per block).
@@ -343,7 +377,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       }
       vl[0] = fmax(vl[0], ro_lim);
       vr[0] = fmax(vr[0], ro_lim);
-      hlld_flux<double, NVM>(vl, vr, fx, gm, cmax);
+      riemann_mhd<NVM>(vl, vr, fx, p, cmax);
 #pragma unroll
       for (int n = 0; n < NVM; ++n) {
         const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
@@ -362,7 +396,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       }
       vl[0] = fmax(vl[0], ro_lim);
       vr[0] = fmax(vr[0], ro_lim);
-      hllc_flux<double>(vl, vr, fx, gm);
+      riemann_hd(vl, vr, fx, p);
 #pragma unroll
       for (int n = 0; n < 5; ++n) {
         const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
@@ -375,7 +409,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   // ---- 3. per-cell source, update, epilogue
   const int ti = tid % TX, tj = tid / TX;
   const int gi = i0 + ti, gj = j0 + tj;
-  const bool valid = gi < iend && (NDIM == 1 || gj < jend);
+  const bool valid = tj < TY && gi < iend && (NDIM == 1 || gj < jend);
   double dtc = 10.0, rhoc = 0.0, grc = 0.0;
   if (valid) {
     const long long q = (long long)gj * p.ix + gi;
@@ -402,8 +436,8 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       for (int n = 0; n < NVM; ++n) r_m[n] = a_m[n];
 #pragma unroll
       for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
-      const Prim<double> qh = cq2pv_hd<double>(r_h, gm, ro_lim, pr_lim);
-      const Prim<double> qm = cq2pv_mhd<double, NVM>(r_m, gm, ro_lim, pr_lim);
+      const Prim<double> qh = rt_hd(r_h, p);
+      const Prim<double> qm = rt_mhd<NVM>(r_m, p);
       collision_ds<NVM>(r_m, r_h, qm, qh, p, dt_coll, ds);
 #pragma unroll
       for (int n = 0; n < 5; ++n) {
@@ -414,8 +448,8 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     // source_PIP on the stage state (rewrites it through primitives first)
     double S_m[5], S_h[5];
     {
-      const Prim<double> qh = cq2pv_hd<double>(s_h, gm, ro_lim, pr_lim);
-      const Prim<double> qm = cq2pv_mhd<double, NVM>(s_m, gm, ro_lim, pr_lim);
+      const Prim<double> qh = rt_hd(s_h, p);
+      const Prim<double> qm = rt_mhd<NVM>(s_m, p);
       double ds[5];
       collision_ds<NVM>(s_m, s_h, qm, qh, p, dt_coll, ds);
       if (p.imp) {
@@ -462,16 +496,16 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     if (NVM == 9) n_m[NVM - 1] = n_m[NVM - 1] * p.decay[STAGE - 1];
 
     // fused cfl rewrites (and the next step's CFL terms)
-    const int ep = s_epi;
+    const int ep = STAGE == 1 ? 0 : s_epi;  // stage 1 is never followed by a cfl
     if (ep >= 1) {
-      const Prim<double> qm = cq2pv_mhd<double, NVM>(n_m, gm, ro_lim, pr_lim);
-      const Prim<double> qh = cq2pv_hd<double>(n_h, gm, ro_lim, pr_lim);
+      const Prim<double> qm = rt_mhd<NVM>(n_m, p);
+      const Prim<double> qh = rt_hd(n_h, p);
       (void)qm;
       (void)qh;
     }
     if (ep == 2) {
-      const Prim<double> qm = cq2pv_mhd<double, NVM>(n_m, gm, ro_lim, pr_lim);
-      const Prim<double> qh = cq2pv_hd<double>(n_h, gm, ro_lim, pr_lim);
+      const Prim<double> qm = rt_mhd<NVM>(n_m, p);
+      const Prim<double> qh = rt_hd(n_h, p);
       const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
       const double sg = p.safety * gmin;
       dtc = fmin(cfl_mhd_cell<double>(qm, n_m[5], n_m[6], n_m[7], gm, sg),
@@ -528,8 +562,8 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
-    const Prim<double> qm = cq2pv_mhd<double, NVM>(um, gm, ro_lim, pr_lim);
-    const Prim<double> qh = cq2pv_hd<double>(uh, gm, ro_lim, pr_lim);
+    const Prim<double> qm = rt_mhd<NVM>(um, p);
+    const Prim<double> qh = rt_hd(uh, p);
 #pragma unroll
     for (int n = 0; n < 5; ++n) U[q + n * nc] = um[n];
 #pragma unroll
@@ -629,7 +663,7 @@ __global__ void flux_kernel(const KParams p, const double *__restrict__ U, doubl
       }
       vl[0] = fmax(vl[0], ro_lim);
       vr[0] = fmax(vr[0], ro_lim);
-      hlld_flux<double, NVM>(vl, vr, fx, gm, cmax);
+      riemann_mhd<NVM>(vl, vr, fx, p, cmax);
       for (int n = 0; n < NVM; ++n) {
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         F[qa + dst * nc] = fx[n];
@@ -644,7 +678,7 @@ __global__ void flux_kernel(const KParams p, const double *__restrict__ U, doubl
       }
       vl[0] = fmax(vl[0], ro_lim);
       vr[0] = fmax(vr[0], ro_lim);
-      hllc_flux<double>(vl, vr, fx, gm);
+      riemann_hd(vl, vr, fx, p);
       for (int n = 0; n < 5; ++n) {
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
         F[qa + (NVM + dst) * nc] = fx[n];
@@ -665,8 +699,8 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
     load_cell<NVM>(U, q, nc, um, uh);
     double gr = 0.0, gion = 0.0;
     if (p.ir) ir_rates<NVM>(um, p, gr, gion);
-    const Prim<double> qh = cq2pv_hd<double>(uh, gm, ro_lim, pr_lim);
-    const Prim<double> qm = cq2pv_mhd<double, NVM>(um, gm, ro_lim, pr_lim);
+    const Prim<double> qh = rt_hd(uh, p);
+    const Prim<double> qm = rt_mhd<NVM>(um, p);
     double ds[5], sm[5], sh[5];
     collision_ds<NVM>(um, uh, qm, qh, p, dt_coll, ds);
     for (int n = 0; n < 5; ++n) {
