@@ -1,0 +1,54 @@
+/*
+ * pip_ensemble.h -- batched ensembles of independent 1D two-fluid runs.
+ *
+ * No counterpart in the reference: PIP runs one simulation per process.  An ensemble holds
+ * many 1D runs of different sizes and parameters (each described by its own pip_params,
+ * ndim = 1, precision = PIP_MIXED) and advances all of them to an end time in one
+ * persistent kernel launch, captured in a CUDA graph: each thread block takes whole runs
+ * from a work queue ordered longest first and steps each with its own dt.  Per-run
+ * arithmetic is that of the single-run FP32-mixed form.
+ */
+#ifndef PIP_ENSEMBLE_H
+#define PIP_ENSEMBLE_H
+
+#include <stdint.h>
+
+#include "pip_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pip_ensemble pip_ensemble;
+
+/* n parameter blocks, one per run (validated as pip_ctx_create does). */
+int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out);
+void pip_ensemble_destroy(pip_ensemble *e);
+
+/* Host -> device copy of one run's U_h, U_m (FP64, Fortran layout, ghosts included); resets
+ * that run's time and step count. */
+int pip_ensemble_upload(pip_ensemble *e, int member, const double *U_h, const double *U_m);
+
+/* Advances every run to t_end (t_end <= 0: no time limit) or by max_steps steps
+ * (max_steps <= 0: no step limit) in one graph launch.  device_ms (may be NULL) receives
+ * the device time of the launch. */
+int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *device_ms);
+
+/* One run's state (U_h/U_m may be NULL), time, step count and stop status (0, PIP_ERR_NAN or
+ * PIP_ERR_DT). */
+int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, double *time,
+                        int64_t *steps, int *status);
+
+/* Launch configuration: threads per block (128, 256, 512, 1024) and blocks per SM. */
+int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm);
+
+/* Autotuner: times every configuration the device can hold on a probe run to t_probe from
+ * the current state (restored afterwards), keeps the fastest and reports it. */
+int pip_ensemble_tune(pip_ensemble *e, double t_probe, int *threads, int *ctas_per_sm,
+                      float *best_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

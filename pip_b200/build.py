@@ -23,6 +23,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 EXTRA_FLAGS = {
     "pip_fp64_exact.cu": ["-fmad=false"],
     "pip_mixed.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "pip_ensemble.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
 }
 
 
@@ -44,8 +45,9 @@ def _deps_mtime() -> float:
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     """Compile every csrc/*.cu for sm_100a and link libpipgpu.so; returns its path."""
-    hdr = os.path.join(os.path.dirname(HERE), "include", "pip_gpu.h")
-    newest = max(_deps_mtime(), os.path.getmtime(hdr))
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    newest = max([_deps_mtime(), os.path.getmtime(os.path.abspath(__file__))] +
+                 [os.path.getmtime(os.path.join(inc, f)) for f in os.listdir(inc)])
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
     os.makedirs(BUILD, exist_ok=True)

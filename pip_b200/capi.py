@@ -35,6 +35,9 @@ EXPORTS = (
     "pip_step_noalloc",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run",
+    # include/pip_ensemble.h
+    "pip_ensemble_create", "pip_ensemble_destroy", "pip_ensemble_upload", "pip_ensemble_run",
+    "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
 )
 
 _lib = None
@@ -89,6 +92,18 @@ def lib(path: Optional[str] = None):
     L.pip_run_timed.argtypes = [vp, ctypes.c_int64, d, dp, P(ctypes.c_int64), P(ctypes.c_float)]
     L.pip_bench_stage_ms.argtypes = [vp, i, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)]
     L.pip_kernels_per_run.argtypes = [vp, ctypes.c_int64]
+    # batched ensembles (include/pip_ensemble.h)
+    L.pip_ensemble_create.argtypes = [P(PipParams), i, P(vp)]
+    L.pip_ensemble_destroy.argtypes = [vp]
+    L.pip_ensemble_destroy.restype = None
+    L.pip_ensemble_upload.argtypes = [vp, i, dp, dp]
+    L.pip_ensemble_run.argtypes = [vp, d, ctypes.c_int64, P(ctypes.c_float)]
+    L.pip_ensemble_member.argtypes = [vp, i, dp, dp, dp, P(ctypes.c_int64), P(i)]
+    L.pip_ensemble_set_config.argtypes = [vp, i, i]
+    L.pip_ensemble_tune.argtypes = [vp, d, P(i), P(i), P(ctypes.c_float)]
+    for name in ("pip_ensemble_create", "pip_ensemble_upload", "pip_ensemble_run",
+                 "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune"):
+        getattr(L, name).restype = i
     L.pip_kernels_per_run.restype = ctypes.c_int64
     for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",
                  "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts", "pip_status",

@@ -1,0 +1,718 @@
+// pip_ensemble.cu -- batched ensemble of independent 1D two-fluid runs in one persistent
+// launch (FP32-mixed form).
+//
+// Each CTA takes a run from a work queue (runs ordered longest first), owns the whole
+// run and advances it to its end time with its own dt: per step stage 1, stage 2 and the
+// fused cfl, with block-wide reductions and no grid synchronisation.  Within a stage the
+// CTA walks the run in chunks of NT-1 cells: primitives of the chunk and its halo into
+// shared memory, the NT faces of the chunk (one per thread), then the per-cell update.
+// The per-cell arithmetic is the mixed stage kernel's (pip_mixed_cell.cuh and the same
+// Riemann solvers), so a member evolves exactly as a single-run mixed context does.
+//
+// Packed storage: member r's planes start at off[r] floats in three arrays (hi, lo, U1),
+// NV = 13 planes of ix_r floats each.  A run's KParams (with its dx tables) sits in a
+// device array.  The launch (queue reset + persistent kernel) is captured in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "../../include/pip_ensemble.h"
+#include "../../include/pip_gpu.h"
+#include "pip_kernels.cuh"
+#include "pip_mixed_cell.cuh"
+#include "pip_physics.cuh"
+
+namespace pip {
+namespace ens {
+
+constexpr int NVM = 8, NV = 13, kH = 2;
+
+struct Member {
+  long long off;      // first float of the member's planes in hi/lo/U1
+  int kp;             // index of its KParams
+};
+
+struct RunState {
+  double time, dt;
+  long long steps;
+  int status;         // 0, PIP_ERR_NAN (3) or PIP_ERR_DT (4)
+  int pad;
+};
+
+__device__ __forceinline__ double finalize_dt(const KParams &p, double red_dt, double red_rho,
+                                              double red_gr) {
+  double dt = fmin(red_dt, p.col_lim / red_rho);
+  if (p.ir) dt = fmin(dt, p.ir_lim / fmax(red_gr, 1.0e-5));
+  return dt;
+}
+
+template <int NT>
+__device__ __forceinline__ void block_minmax(double &dtc, double &rho, double &gr, double *s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+    rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
+  }
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  __syncthreads();
+  if (l == 0) {
+    s_red[w] = dtc;
+    s_red[NT / 32 + w] = rho;
+    s_red[2 * (NT / 32) + w] = gr;
+  }
+  __syncthreads();
+  dtc = s_red[0];
+  rho = s_red[NT / 32];
+  gr = s_red[2 * (NT / 32)];
+  for (int k = 1; k < NT / 32; ++k) {
+    dtc = fmin(dtc, s_red[k]);
+    rho = fmax(rho, s_red[NT / 32 + k]);
+    gr = fmax(gr, s_red[2 * (NT / 32) + k]);
+  }
+}
+
+// One RK stage of a member (the 1D mixed stage kernel's arithmetic, chunk by chunk).
+// Returns, for stage 2 with ep == 2, this thread's CFL terms of the next step.
+template <int NT, int STAGE>
+__device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *Alo, float *Bf,
+                          double dt, int ep, float *sV, float *sF, double &dtc, double &rhoc,
+                          double &grc, int &bad) {
+  constexpr int CN = NT - 1;          // cells per chunk
+  constexpr int RX = CN + 2 * kH;     // region cells
+  const int tid = threadIdx.x;
+  const long long nc = p.nc;
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  const float igm1f = (float)p.igm1;
+  const int iend = p.m0 + p.nx;
+  float *Ohi = STAGE == 1 ? Bf : Ahi;
+  for (int c0 = p.m0; c0 < iend; c0 += CN) {
+    const int cn = min(CN, iend - c0);
+    // primitives of the chunk and its halo
+    for (int idx = tid; idx < cn + 2 * kH; idx += NT) {
+      const int gi = c0 - kH + idx;
+      float um[NVM], uh[5], vm[NVM], vh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) um[n] = Us[gi + n * nc];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uh[n] = Us[gi + (NVM + n) * nc];
+      u2v_mhd<float, NVM>(um, vm, gmf, rolf, prlf);
+      u2v_hd<float>(uh, vh, gmf, rolf, prlf);
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) sV[n * RX + idx] = vm[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) sV[(NVM + n) * RX + idx] = vh[n];
+    }
+    __syncthreads();
+    // faces: face t lies between cells c0-1+t and c0+t
+    if (tid <= cn) {
+      const int a = tid + kH - 1;
+      {
+        float vl[NVM], vr[NVM], fx[NVM];
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) {
+          const float *v = sV + n * RX + a;
+          const float v0 = v[-1], v1 = v[0], v2 = v[1], v3 = v[2];
+          vl[n] = v1 + 0.5f * minmod<float>(v0, v1, v2);
+          vr[n] = v2 - 0.5f * minmod<float>(v1, v2, v3);
+        }
+        vl[0] = fmaxf(vl[0], rolf);
+        vr[0] = fmaxf(vr[0], rolf);
+        hlld_flux_rcp<float, NVM>(vl, vr, fx, gmf, igm1f, 0.0f);
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) sF[n * NT + tid] = fx[n];
+      }
+      {
+        float vl[5], vr[5], fx[5];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          const float *v = sV + (NVM + n) * RX + a;
+          const float v0 = v[-1], v1 = v[0], v2 = v[1], v3 = v[2];
+          vl[n] = v1 + 0.5f * minmod<float>(v0, v1, v2);
+          vr[n] = v2 - 0.5f * minmod<float>(v1, v2, v3);
+        }
+        vl[0] = fmaxf(vl[0], rolf);
+        vr[0] = fmaxf(vr[0], rolf);
+        hllc_flux_rcp<float>(vl, vr, fx, gmf, igm1f);
+#pragma unroll
+        for (int n = 0; n < 5; ++n) sF[(NVM + n) * NT + tid] = fx[n];
+      }
+    }
+    __syncthreads();
+    // per-cell source and update
+    if (tid < cn) {
+      const int gi = c0 + tid;
+      const double dt_sub = STAGE == 1 ? dt / 2.0 : dt;
+      const double dt_coll = dt * 0.5;
+      double a_m[NVM], a_h[5], s_m[NVM], s_h[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) {
+        a_m[n] = (double)Ahi[gi + n * nc];
+        if (STAGE == 2) a_m[n] += (double)Alo[gi + n * nc];
+      }
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        a_h[n] = (double)Ahi[gi + (NVM + n) * nc];
+        if (STAGE == 2) a_h[n] += (double)Alo[gi + (NVM + n) * nc];
+      }
+      if (STAGE == 1) {
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) s_m[n] = a_m[n];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) s_h[n] = a_h[n];
+      } else {
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) s_m[n] = (double)Us[gi + n * nc];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) s_h[n] = (double)Us[gi + (NVM + n) * nc];
+      }
+      double gr = 0.0, gion = 0.0;
+      if (p.ir) mixed::ir_rates<NVM>(a_m, p, gr, gion);
+      if (p.imp && STAGE == 2) {
+        double ds[5];
+        const Prim<double> qh = mixed::prim_hd(a_h, p);
+        const Prim<double> qm = mixed::prim_mhd<NVM>(a_m, p);
+        mixed::collision_ds<NVM>(a_m, a_h, qm, qh, p, dt_coll, ds);
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          a_h[n] = a_h[n] - dt_coll * ds[n];
+          a_m[n] = a_m[n] + dt_coll * ds[n];
+        }
+      }
+      double S_m[5], S_h[5];
+      {
+        const Prim<double> qh = mixed::prim_hd(s_h, p);
+        const Prim<double> qm = mixed::prim_mhd<NVM>(s_m, p);
+        double ds[5];
+        mixed::collision_ds<NVM>(s_m, s_h, qm, qh, p, dt_coll, ds);
+        if (p.imp) {
+#pragma unroll
+          for (int n = 0; n < 5; ++n) {
+            a_h[n] = a_h[n] - dt_coll * ds[n];
+            a_m[n] = a_m[n] + dt_coll * ds[n];
+            S_h[n] = 0.0;
+            S_m[n] = 0.0;
+          }
+        } else {
+#pragma unroll
+          for (int n = 0; n < 5; ++n) {
+            S_h[n] = -ds[n];
+            S_m[n] = ds[n];
+          }
+        }
+        if (p.ir) {
+          mixed::ir_ds(qm, qh, gr, gion, p, ds);
+#pragma unroll
+          for (int n = 0; n < 5; ++n) {
+            S_h[n] += ds[n];
+            S_m[n] -= ds[n];
+          }
+        }
+      }
+      const double cx = dt_sub * p.rdx[gi];
+      double n_m[NVM], n_h[5];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) {
+        double u = n < NVM ? a_m[n] : a_h[n - NVM];
+        u -= cx * (double)(sF[n * NT + tid + 1] - sF[n * NT + tid]);
+        if (n < NVM) {
+          if (n < 5) u += S_m[n] * dt_sub;
+          n_m[n] = u;
+        } else {
+          n_h[n - NVM] = u + S_h[n - NVM] * dt_sub;
+        }
+      }
+      if (ep >= 1) {
+        mixed::floors_mhd<NVM>(n_m, p);
+        mixed::floors_hd(n_h, p);
+      }
+      if (ep == 2) {
+        float um[NVM], uh[5];
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) um[n] = (float)n_m[n];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) uh[n] = (float)n_h[n];
+        const Prim<float> qm = cq2pv_mhd<float, NVM>(um, gmf, rolf, prlf);
+        const Prim<float> qh = cq2pv_hd<float>(uh, gmf, rolf, prlf);
+        const double gmin = fmin(fmin(p.dx[gi], p.dy[0]), p.dz0);
+        const float sg = (float)(p.safety * gmin);
+        dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, um[5], um[6], um[7], gmf, sg),
+                                      cfl_hd_cell<float>(qh, gmf, sg)));
+        rhoc = fmax(rhoc, fmax(n_m[0] * p.ac, n_h[0] * p.ac));
+        if (p.ir) {
+          double g1, g2;
+          mixed::ir_rates<NVM>(n_m, p, g1, g2);
+          grc = fmax(grc, fmax(g1, g2));
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) bad |= !isfinite(n_m[n]);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
+#pragma unroll
+      for (int n = 0; n < NV; ++n) {
+        const double u = n < NVM ? n_m[n] : n_h[n - NVM];
+        const float hi = (float)u;
+        Ohi[gi + n * nc] = hi;
+        if (STAGE == 2) Alo[gi + n * nc] = (float)(u - (double)hi);
+      }
+      if (mixed::near_boundary<1>(p, gi, 0))
+        mixed::write_ghosts<1>(p, gi, 0, Ohi, STAGE == 2 ? Alo : nullptr, NV);
+    }
+    __syncthreads();
+  }
+}
+
+// Persistent ensemble kernel: CTAs take runs from the queue until it is empty.
+template <int NT>
+__global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const KParams *kps,
+                                                      const int *order, int nmem, float *hi,
+                                                      float *lo, float *U1, RunState *st,
+                                                      unsigned *queue, double t_end,
+                                                      long long max_steps) {
+  constexpr int CN = NT - 1, RX = CN + 2 * kH;
+  extern __shared__ float smem[];
+  float *sV = smem;
+  float *sF = sV + NV * RX;
+  __shared__ double s_red[3 * (NT / 32)];
+  __shared__ KParams sp;
+  __shared__ int s_r;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_r = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int rq = s_r;
+    if (rq >= nmem) return;
+    const int r = order[rq];
+    if (tid == 0) sp = kps[mem[r].kp];
+    __syncthreads();
+    const KParams &p = sp;
+    const long long nc = p.nc;
+    float *Ahi = hi + mem[r].off, *Alo = lo + mem[r].off, *B = U1 + mem[r].off;
+    RunState rs = st[r];
+    if (rs.status != 0 || (t_end > 0.0 && rs.time >= t_end)) {
+      __syncthreads();
+      continue;
+    }
+    // cfl of the first step: floors of every cell (cq2pv, Scheme_rot.f90:132-179) and the
+    // CFL terms (the mixed cfl kernel's arithmetic)
+    double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+    const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+    for (int i = tid; i < p.ix; i += NT) {
+      double um[NVM], uh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) um[n] = (double)Ahi[i + n * nc] + (double)Alo[i + n * nc];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uh[n] = (double)Ahi[i + (NVM + n) * nc] + (double)Alo[i + (NVM + n) * nc];
+      mixed::floors_mhd<NVM>(um, p);
+      mixed::floors_hd(uh, p);
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        float h = (float)um[n];
+        Ahi[i + n * nc] = h;
+        Alo[i + n * nc] = (float)(um[n] - (double)h);
+        h = (float)uh[n];
+        Ahi[i + (NVM + n) * nc] = h;
+        Alo[i + (NVM + n) * nc] = (float)(uh[n] - (double)h);
+      }
+      if (i >= p.m0 && i < p.ix - p.m0) {
+        float fm[NVM], fh[5];
+#pragma unroll
+        for (int n = 0; n < NVM; ++n) fm[n] = (float)um[n];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
+        const Prim<float> qm = cq2pv_mhd<float, NVM>(fm, gmf, rolf, prlf);
+        const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
+        const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[0]), p.dz0));
+        dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
+                                      cfl_hd_cell<float>(qh, gmf, sg)));
+      }
+      rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+      if (p.ir) {
+        double g1, g2;
+        mixed::ir_rates<NVM>(um, p, g1, g2);
+        grc = fmax(grc, fmax(g1, g2));
+      }
+    }
+    block_minmax<NT>(dtc, rhoc, grc, s_red);
+    double dt = finalize_dt(p, dtc, rhoc, grc);
+    int bad = 0;
+    // the time loop (main.f90:31-68) of this run
+    for (;;) {
+      const double tn = rs.time + dt;
+      const bool last = (t_end > 0.0 && tn >= t_end) || (max_steps > 0 && rs.steps + 1 >= max_steps);
+      double d1 = 10.0, r1 = 0.0, g1 = 0.0;
+      run_stage<NT, 1>(p, Ahi, Ahi, Alo, B, dt, 0, sV, sF, d1, r1, g1, bad);
+      double d2 = 10.0, r2 = 0.0, g2 = 0.0;
+      run_stage<NT, 2>(p, B, Ahi, Alo, B, dt, last ? 1 : 2, sV, sF, d2, r2, g2, bad);
+      rs.time = tn;
+      rs.steps += 1;
+      rs.dt = dt;
+      const int anybad = __syncthreads_or(bad);
+      if (anybad) {
+        rs.status = 3;  // PIP_ERR_NAN
+        break;
+      }
+      if (dt <= 1.0e-12) {
+        rs.status = 4;  // PIP_ERR_DT
+        break;
+      }
+      if (last) break;
+      block_minmax<NT>(d2, r2, g2, s_red);
+      dt = finalize_dt(p, d2, r2, g2);
+    }
+    if (tid == 0) st[r] = rs;
+    __syncthreads();
+  }
+}
+
+constexpr size_t smem_bytes(int nt) { return sizeof(float) * NV * ((nt - 1 + 2 * kH) + nt); }
+
+cudaError_t launch(int nt, int grid, cudaStream_t s, const Member *mem, const KParams *kps,
+                   const int *order, int nmem, float *hi, float *lo, float *U1, RunState *st,
+                   unsigned *queue, double t_end, long long max_steps) {
+#define PIP_ENS_CASE(NTV)                                                                       \
+  case NTV:                                                                                     \
+    ensemble_kernel<NTV><<<grid, NTV, smem_bytes(NTV), s>>>(mem, kps, order, nmem, hi, lo, U1, \
+                                                            st, queue, t_end, max_steps);       \
+    break;
+  switch (nt) {
+    PIP_ENS_CASE(128)
+    PIP_ENS_CASE(256)
+    PIP_ENS_CASE(512)
+    PIP_ENS_CASE(1024)
+    default: return cudaErrorInvalidValue;
+  }
+#undef PIP_ENS_CASE
+  return cudaGetLastError();
+}
+
+cudaError_t prepare() {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(ensemble_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes(512))) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(ensemble_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes(1024));
+}
+
+int max_ctas_per_sm(int nt) {
+  int n = 0;
+  cudaError_t e = cudaSuccess;
+  switch (nt) {
+    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<128>, 128, smem_bytes(128)); break;
+    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<256>, 256, smem_bytes(256)); break;
+    case 512: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<512>, 512, smem_bytes(512)); break;
+    case 1024: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<1024>, 1024, smem_bytes(1024)); break;
+    default: return 0;
+  }
+  return e == cudaSuccess ? n : 0;
+}
+
+}  // namespace ens
+}  // namespace pip
+
+// ------------------------------------------------------------------------------ C ABI
+
+using pip::ens::Member;
+using pip::ens::RunState;
+
+struct pip_ensemble {
+  int n = 0;
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::vector<pip::KParams> kp;
+  std::vector<Member> mem;
+  std::vector<long long> cost;
+  long long total_floats = 0;
+  Member *d_mem = nullptr;
+  pip::KParams *d_kp = nullptr;
+  int *d_order = nullptr;
+  float *hi = nullptr, *lo = nullptr, *U1 = nullptr;
+  float *save_hi = nullptr, *save_lo = nullptr;  // state snapshot for the autotuner
+  double *d_dx = nullptr;                         // dx, 1/dx, dy tables of all members
+  double *stage64 = nullptr;                      // FP64 staging of one member
+  RunState *d_st = nullptr;
+  unsigned *d_queue = nullptr;
+  int threads = 256, ctas_per_sm = 2;
+  cudaGraphExec_t graph = nullptr;
+  double graph_t_end = -1.0;
+  long long graph_steps = -1;
+  int graph_threads = 0, graph_ctas = 0;
+};
+
+static int g_ens_cuda_error = 0;
+#define EK(call)                        \
+  do {                                  \
+    cudaError_t e__ = (call);           \
+    if (e__ != cudaSuccess) {           \
+      g_ens_cuda_error = (int)e__;      \
+      return PIP_ERR_CUDA;              \
+    }                                   \
+  } while (0)
+
+extern "C" {
+
+int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
+  if (!members || !out) return PIP_ERR_NULL;
+  *out = nullptr;
+  if (n <= 0) return PIP_ERR_PARAM;
+  pip_ensemble *e = new (std::nothrow) pip_ensemble();
+  if (!e) return PIP_ERR_NOMEM;
+  e->n = n;
+  e->kp.resize(n);
+  e->mem.resize(n);
+  e->cost.resize(n);
+  long long off = 0, dxoff = 0;
+  std::vector<double> dxtab;
+  for (int r = 0; r < n; ++r) {
+    const pip_params &p = members[r];
+    if (p.ndim != 1 || p.precision != PIP_MIXED) {
+      delete e;
+      return PIP_ERR_PARAM;
+    }
+    int st = pip::kparams_from_params(&p, &e->kp[r]);
+    if (st != PIP_OK) {
+      delete e;
+      return st;
+    }
+    e->mem[r].off = off;
+    e->mem[r].kp = r;
+    off += (long long)pip::ens::NV * p.ix;
+    // dx, 1/dx and dy of this member, pointed at after the upload of the table
+    for (int i = 0; i < p.ix; ++i) dxtab.push_back(p.dx[i]);
+    for (int i = 0; i < p.ix; ++i) dxtab.push_back(1.0 / p.dx[i]);
+    dxtab.push_back(p.dy[0]);
+    e->kp[r].dx = reinterpret_cast<const double *>(dxoff);
+    e->kp[r].rdx = reinterpret_cast<const double *>(dxoff + p.ix);
+    e->kp[r].dy = reinterpret_cast<const double *>(dxoff + 2 * p.ix);
+    e->kp[r].rdy = nullptr;
+    dxoff += 2 * p.ix + 1;
+    e->cost[r] = (long long)p.ix * p.ix;
+  }
+  e->total_floats = off;
+  auto fail = [&](cudaError_t c) {
+    g_ens_cuda_error = (int)c;
+    pip_ensemble_destroy(e);
+    return c == cudaErrorMemoryAllocation ? PIP_ERR_NOMEM : PIP_ERR_CUDA;
+  };
+  cudaError_t c;
+  if ((c = cudaGetDevice(&e->device)) != cudaSuccess) return fail(c);
+  cudaDeviceProp prop;
+  if ((c = cudaGetDeviceProperties(&prop, e->device)) != cudaSuccess) return fail(c);
+  e->sms = prop.multiProcessorCount;
+  if ((c = pip::ens::prepare()) != cudaSuccess) return fail(c);
+  if ((c = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(c);
+  const size_t fb = sizeof(float) * (size_t)off;
+  if ((c = cudaMalloc(&e->hi, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->lo, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->U1, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemset(e->hi, 0, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemset(e->lo, 0, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemset(e->U1, 0, fb)) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->d_dx, sizeof(double) * dxtab.size())) != cudaSuccess) return fail(c);
+  if ((c = cudaMemcpy(e->d_dx, dxtab.data(), sizeof(double) * dxtab.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(c);
+  for (int r = 0; r < n; ++r) {
+    e->kp[r].dx = e->d_dx + reinterpret_cast<long long>(e->kp[r].dx);
+    e->kp[r].rdx = e->d_dx + reinterpret_cast<long long>(e->kp[r].rdx);
+    e->kp[r].dy = e->d_dx + reinterpret_cast<long long>(e->kp[r].dy);
+  }
+  if ((c = cudaMalloc(&e->d_kp, sizeof(pip::KParams) * n)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemcpy(e->d_kp, e->kp.data(), sizeof(pip::KParams) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(c);
+  if ((c = cudaMalloc(&e->d_mem, sizeof(Member) * n)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemcpy(e->d_mem, e->mem.data(), sizeof(Member) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(c);
+  // longest runs first (cost ~ cells x steps ~ ix^2)
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e->cost[a] > e->cost[b]; });
+  if ((c = cudaMalloc(&e->d_order, sizeof(int) * n)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemcpy(e->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(c);
+  if ((c = cudaMalloc(&e->d_st, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
+  if ((c = cudaMemset(e->d_st, 0, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->d_queue, sizeof(unsigned))) != cudaSuccess) return fail(c);
+  int maxix = 0;
+  for (int r = 0; r < n; ++r) maxix = std::max(maxix, members[r].ix);
+  if ((c = cudaMalloc(&e->stage64, sizeof(double) * pip::ens::NV * maxix)) != cudaSuccess) return fail(c);
+  *out = e;
+  return PIP_OK;
+}
+
+void pip_ensemble_destroy(pip_ensemble *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  cudaFree(e->hi);
+  cudaFree(e->lo);
+  cudaFree(e->U1);
+  cudaFree(e->save_hi);
+  cudaFree(e->save_lo);
+  cudaFree(e->d_dx);
+  cudaFree(e->d_kp);
+  cudaFree(e->d_mem);
+  cudaFree(e->d_order);
+  cudaFree(e->d_st);
+  cudaFree(e->d_queue);
+  cudaFree(e->stage64);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int pip_ensemble_upload(pip_ensemble *e, int member, const double *U_h, const double *U_m) {
+  if (!e || !U_h || !U_m) return PIP_ERR_NULL;
+  if (member < 0 || member >= e->n) return PIP_ERR_PARAM;
+  EK(cudaSetDevice(e->device));
+  const pip::KParams &k = e->kp[member];
+  const size_t pb = sizeof(double) * (size_t)k.nc;
+  EK(cudaMemcpyAsync(e->stage64, U_m, pb * 8, cudaMemcpyHostToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->stage64 + 8 * k.nc, U_h, pb * 5, cudaMemcpyHostToDevice, e->stream));
+  EK(pip::mixed_split(e->stage64, e->hi + e->mem[member].off, e->lo + e->mem[member].off,
+                      pip::ens::NV * k.nc, e->stream));
+  RunState z;
+  std::memset(&z, 0, sizeof z);
+  EK(cudaMemcpyAsync(e->d_st + member, &z, sizeof z, cudaMemcpyHostToDevice, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  return PIP_OK;
+}
+
+int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, double *time,
+                        int64_t *steps, int *status) {
+  if (!e) return PIP_ERR_NULL;
+  if (member < 0 || member >= e->n) return PIP_ERR_PARAM;
+  EK(cudaSetDevice(e->device));
+  const pip::KParams &k = e->kp[member];
+  const size_t pb = sizeof(double) * (size_t)k.nc;
+  RunState rs;
+  EK(cudaMemcpyAsync(&rs, e->d_st + member, sizeof rs, cudaMemcpyDeviceToHost, e->stream));
+  if (U_h && U_m) {
+    EK(pip::mixed_join(e->hi + e->mem[member].off, e->lo + e->mem[member].off, e->stage64,
+                       pip::ens::NV * k.nc, e->stream));
+    EK(cudaMemcpyAsync(U_m, e->stage64, pb * 8, cudaMemcpyDeviceToHost, e->stream));
+    EK(cudaMemcpyAsync(U_h, e->stage64 + 8 * k.nc, pb * 5, cudaMemcpyDeviceToHost, e->stream));
+  }
+  EK(cudaStreamSynchronize(e->stream));
+  if (time) *time = rs.time;
+  if (steps) *steps = rs.steps;
+  if (status) *status = rs.status;
+  return PIP_OK;
+}
+
+int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm) {
+  if (!e) return PIP_ERR_NULL;
+  if (threads != 128 && threads != 256 && threads != 512 && threads != 1024) return PIP_ERR_PARAM;
+  const int mx = pip::ens::max_ctas_per_sm(threads);
+  if (ctas_per_sm < 1 || ctas_per_sm > mx) return PIP_ERR_PARAM;
+  e->threads = threads;
+  e->ctas_per_sm = ctas_per_sm;
+  return PIP_OK;
+}
+
+static int ens_enqueue(pip_ensemble *e, double t_end, long long max_steps) {
+  EK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), e->stream));
+  EK(pip::ens::launch(e->threads, e->sms * e->ctas_per_sm, e->stream, e->d_mem, e->d_kp, e->d_order,
+                      e->n, e->hi, e->lo, e->U1, e->d_st, e->d_queue, t_end, max_steps));
+  return PIP_OK;
+}
+
+int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *device_ms) {
+  if (!e) return PIP_ERR_NULL;
+  if (!(t_end > 0.0) && max_steps <= 0) return PIP_ERR_PARAM;
+  EK(cudaSetDevice(e->device));
+  // one graph per (end time, step limit, configuration): queue reset + persistent kernel
+  if (!e->graph || e->graph_t_end != t_end || e->graph_steps != max_steps ||
+      e->graph_threads != e->threads || e->graph_ctas != e->ctas_per_sm) {
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    EK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = ens_enqueue(e, t_end, max_steps);
+    cudaError_t c = cudaStreamEndCapture(e->stream, &g);
+    if (st != PIP_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    EK(c);
+    c = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    EK(c);
+    e->graph_t_end = t_end;
+    e->graph_steps = max_steps;
+    e->graph_threads = e->threads;
+    e->graph_ctas = e->ctas_per_sm;
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (device_ms) {
+    EK(cudaEventCreate(&a));
+    EK(cudaEventCreate(&b));
+    EK(cudaEventRecord(a, e->stream));
+  }
+  EK(cudaGraphLaunch(e->graph, e->stream));
+  if (device_ms) EK(cudaEventRecord(b, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  if (device_ms) {
+    EK(cudaEventElapsedTime(device_ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  return PIP_OK;
+}
+
+// Autotuner: times every (threads, CTAs per SM) the device can hold on a short run from
+// the current state (restored after each trial) and keeps the fastest.
+int pip_ensemble_tune(pip_ensemble *e, double t_probe, int *threads, int *ctas_per_sm, float *best_ms) {
+  if (!e) return PIP_ERR_NULL;
+  if (!(t_probe > 0.0)) return PIP_ERR_PARAM;
+  EK(cudaSetDevice(e->device));
+  const size_t fb = sizeof(float) * (size_t)e->total_floats;
+  if (!e->save_hi) EK(cudaMalloc(&e->save_hi, fb));
+  if (!e->save_lo) EK(cudaMalloc(&e->save_lo, fb));
+  std::vector<RunState> st0(e->n);
+  EK(cudaMemcpyAsync(e->save_hi, e->hi, fb, cudaMemcpyDeviceToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->save_lo, e->lo, fb, cudaMemcpyDeviceToDevice, e->stream));
+  EK(cudaMemcpyAsync(st0.data(), e->d_st, sizeof(RunState) * e->n, cudaMemcpyDeviceToHost, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  float best = 1e30f;
+  int bt = e->threads, bc = e->ctas_per_sm;
+  const int cand_t[4] = {128, 256, 512, 1024};
+  for (int ti = 0; ti < 4; ++ti) {
+    const int mx = std::min(pip::ens::max_ctas_per_sm(cand_t[ti]), 8);
+    for (int cps = 1; cps <= mx; ++cps) {
+      e->threads = cand_t[ti];
+      e->ctas_per_sm = cps;
+      // probe run: every member advances to t_probe from the saved state
+      EK(cudaMemcpyAsync(e->hi, e->save_hi, fb, cudaMemcpyDeviceToDevice, e->stream));
+      EK(cudaMemcpyAsync(e->lo, e->save_lo, fb, cudaMemcpyDeviceToDevice, e->stream));
+      EK(cudaMemcpyAsync(e->d_st, st0.data(), sizeof(RunState) * e->n, cudaMemcpyHostToDevice, e->stream));
+      float ms = 0.f;
+      const int st = pip_ensemble_run(e, t_probe, 0, &ms);
+      if (st != PIP_OK) return st;
+      if (ms < best) {
+        best = ms;
+        bt = cand_t[ti];
+        bc = cps;
+      }
+    }
+  }
+  EK(cudaMemcpyAsync(e->hi, e->save_hi, fb, cudaMemcpyDeviceToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->lo, e->save_lo, fb, cudaMemcpyDeviceToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->d_st, st0.data(), sizeof(RunState) * e->n, cudaMemcpyHostToDevice, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  e->threads = bt;
+  e->ctas_per_sm = bc;
+  if (threads) *threads = bt;
+  if (ctas_per_sm) *ctas_per_sm = bc;
+  if (best_ms) *best_ms = best;
+  return PIP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+"""Batched ensembles of independent 1D two-fluid runs (include/pip_ensemble.h)."""
+from __future__ import annotations
+
+import ctypes
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import capi, ics
+from .params import PIP_MIXED, PipParams, Settings
+
+
+class Ensemble:
+    """Many 1D runs advanced together by one persistent launch (FP32-mixed form)."""
+
+    def __init__(self, members: Sequence[Tuple[Settings, np.ndarray, np.ndarray]]):
+        self.settings = [s.overrides(precision=PIP_MIXED) for s, _, _ in members]
+        arr = (PipParams * len(members))()
+        self._keep = []
+        for r, s in enumerate(self.settings):
+            p, keep = s.to_params()
+            arr[r] = p
+            self._keep.append(keep)
+        self._arr = arr
+        h = ctypes.c_void_p()
+        capi._check(capi.lib().pip_ensemble_create(arr, len(members), ctypes.byref(h)),
+                    "pip_ensemble_create")
+        self.h = h
+        self.n = len(members)
+        self.shapes = [(U_h.shape, U_m.shape) for _, U_h, U_m in members]
+        for r, (_, U_h, U_m) in enumerate(members):
+            self.upload(r, U_h, U_m)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            capi.lib().pip_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, r: int, U_h: np.ndarray, U_m: np.ndarray) -> None:
+        U_h = np.ascontiguousarray(U_h, dtype=np.float64)
+        U_m = np.ascontiguousarray(U_m, dtype=np.float64)
+        capi._check(capi.lib().pip_ensemble_upload(self.h, r, capi._ptr(U_h), capi._ptr(U_m)),
+                    "pip_ensemble_upload")
+
+    def run(self, t_end: float = 0.0, max_steps: int = 0) -> float:
+        """Advance every run; returns the device time of the launch in ms."""
+        ms = ctypes.c_float()
+        capi._check(capi.lib().pip_ensemble_run(self.h, float(t_end), int(max_steps), ctypes.byref(ms)),
+                    "pip_ensemble_run")
+        return ms.value
+
+    def member(self, r: int, state: bool = True):
+        """(U_h, U_m, time, steps, status) of run r."""
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        st = ctypes.c_int()
+        if state:
+            sh, sm = self.shapes[r]
+            U_h, U_m = np.empty(sh), np.empty(sm)
+            ph, pm = capi._ptr(U_h), capi._ptr(U_m)
+        else:
+            U_h = U_m = None
+            ph = pm = None
+        capi._check(capi.lib().pip_ensemble_member(self.h, r, ph, pm, ctypes.byref(t),
+                                                   ctypes.byref(n), ctypes.byref(st)),
+                    "pip_ensemble_member")
+        return U_h, U_m, t.value, n.value, st.value
+
+    def set_config(self, threads: int, ctas_per_sm: int) -> None:
+        capi._check(capi.lib().pip_ensemble_set_config(self.h, int(threads), int(ctas_per_sm)),
+                    "pip_ensemble_set_config")
+
+    def tune(self, t_probe: float) -> Tuple[int, int, float]:
+        """Autotune (threads per block, blocks per SM) on a probe run; returns the choice."""
+        th, cp, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        capi._check(capi.lib().pip_ensemble_tune(self.h, float(t_probe), ctypes.byref(th),
+                                                 ctypes.byref(cp), ctypes.byref(ms)),
+                    "pip_ensemble_tune")
+        return th.value, cp.value, ms.value
+
+
+def shock_tube_ensemble(n_runs: int = 512, seed: int = 4242, nx_max: Optional[int] = None):
+    """Members of the seeded 1D shock-tube ensemble (ics.ensemble_members)."""
+    out = []
+    for m in ics.ensemble_members(n_runs, seed):
+        if nx_max is not None:
+            m = dict(m, nx=min(m["nx"], nx_max))
+        out.append(ics.shock_tube_member(**m))
+    return out

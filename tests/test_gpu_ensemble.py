@@ -1,0 +1,75 @@
+"""Batched ensemble of 1D two-fluid runs (include/pip_ensemble.h) against single runs."""
+import numpy as np
+import pytest
+
+from helpers import rel_l1
+from pip_b200 import capi, ics
+from pip_b200.ensemble import Ensemble, shock_tube_ensemble
+from pip_b200.params import PIP_FP64, PIP_MIXED
+
+pytestmark = pytest.mark.gpu
+
+T_END = 0.02
+
+
+def members():
+    return shock_tube_ensemble(n_runs=7, seed=11, nx_max=300) + \
+        [ics.shock_tube_member(64, col=1.0e4, pratio=20.0, dratio=10.0, ion_frac=0.05)]
+
+
+def single(s, Uh, Um, precision, nsteps=0, t_end=0.0):
+    with capi.Context(s.overrides(precision=precision)) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        st, t, n = c.run(nsteps=nsteps, t_end=t_end)
+        return st, t, n, c.download()
+
+
+def test_ensemble_matches_single_runs(gpu_lib):
+    mem = members()
+    with Ensemble(mem) as e:
+        e.run(t_end=T_END)
+        for r, (s, Uh, Um) in enumerate(mem):
+            eh, em, t, n, st = e.member(r)
+            assert st == 0 and t >= T_END
+            # the single-run mixed form does the same per-cell arithmetic; FMA contraction
+            # may differ between the two kernels, so they agree to FP32 rounding
+            st1, t1, n1, (h1, m1) = single(s, Uh, Um, PIP_MIXED, nsteps=n)
+            assert abs(t1 - t) <= 1e-6 * t
+            assert max(rel_l1(eh, h1).max(), rel_l1(em, m1).max()) <= 1e-5
+            # the FP64 single run after the same number of steps
+            st2, t2, n2, (h2, m2) = single(s, Uh, Um, PIP_FP64, nsteps=n)
+            assert abs(t2 - t) <= 1e-5 * t
+            assert max(rel_l1(eh, h2).max(), rel_l1(em, m2).max()) <= 1e-5
+
+
+def test_ensemble_configurations_agree(gpu_lib):
+    mem = members()[:4]
+    out = []
+    for threads, cps in ((128, 1), (256, 2), (1024, 1)):
+        with Ensemble(mem) as e:
+            e.set_config(threads, cps)
+            e.run(t_end=0.01)
+            out.append([e.member(r) for r in range(len(mem))])
+    # each configuration is its own kernel instance: FMA contraction may differ, so the
+    # runs agree to FP32 rounding rather than bit for bit
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert a[3] == b[3] and abs(a[2] - b[2]) <= 1e-6 * a[2]
+            assert max(rel_l1(a[0], b[0]).max(), rel_l1(a[1], b[1]).max()) <= 1e-6
+
+
+def test_autotuner_picks_a_valid_configuration(gpu_lib):
+    mem = members()
+    with Ensemble(mem) as e:
+        threads, cps, ms = e.tune(t_probe=0.002)
+        assert threads in (128, 256, 512, 1024) and cps >= 1 and ms > 0
+        # tuning restores the state: a run from here equals a run of a fresh ensemble
+        e.run(t_end=0.005)
+        a = [e.member(r) for r in range(len(mem))]
+    with Ensemble(mem) as f:
+        f.run(t_end=0.005)
+        for r in range(len(mem)):
+            b = f.member(r)
+            assert a[r][3] == b[3]
+            assert rel_l1(a[r][1], b[1]).max() <= 1e-6
