@@ -11,6 +11,16 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <cmath>
+
+// Functions here compile for the device and, for host-side tests of the adjoint, for the
+// host.
+#if defined(__CUDACC__)
+#define PIP_HD __host__ __device__ __forceinline__
+#else
+#define PIP_HD inline
+#endif
+
 namespace pip {
 
 constexpr double kTiny = 1.0e-20;        // Globalvar.f90:101
@@ -20,22 +30,22 @@ constexpr double kHllgFactor = 1.001;    // HLL_rot.f90:702
 constexpr double kMuP = 0.5;             // PIP_rot.f90:35
 constexpr double kMuN = 1.0;             // PIP_rot.f90:36
 
-template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return fmax(a, b); }
-template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return fmin(a, b); }
-template <> __device__ __forceinline__ float rmax<float>(float a, float b) { return fmaxf(a, b); }
-template <> __device__ __forceinline__ float rmin<float>(float a, float b) { return fminf(a, b); }
-__device__ __forceinline__ double rsqrt_(double a) { return sqrt(a); }
-__device__ __forceinline__ float rsqrt_(float a) { return sqrtf(a); }
-__device__ __forceinline__ double rabs(double a) { return fabs(a); }
-__device__ __forceinline__ float rabs(float a) { return fabsf(a); }
-__device__ __forceinline__ double rsign1(double b) { return copysign(1.0, b); }
-__device__ __forceinline__ float rsign1(float b) { return copysignf(1.0f, b); }
+template <typename R> PIP_HD R rmax(R a, R b) { return std::fmax(a, b); }
+template <typename R> PIP_HD R rmin(R a, R b) { return std::fmin(a, b); }
+template <> PIP_HD float rmax<float>(float a, float b) { return std::fmax(a, b); }
+template <> PIP_HD float rmin<float>(float a, float b) { return std::fmin(a, b); }
+PIP_HD double rsqrt_(double a) { return std::sqrt(a); }
+PIP_HD float rsqrt_(float a) { return std::sqrt(a); }
+PIP_HD double rabs(double a) { return std::fabs(a); }
+PIP_HD float rabs(float a) { return std::fabs(a); }
+PIP_HD double rsign1(double b) { return std::copysign(1.0, b); }
+PIP_HD float rsign1(float b) { return std::copysign(1.0f, b); }
 
 // ---------------------------------------------------------------- conversions
 
 // u2v_mhd (HLL_rot.f90:1159-1186): conserved -> primitive with density/pressure floors.
 template <typename R, int NVM>
-__device__ __forceinline__ void u2v_mhd(const R (&u)[NVM], R (&v)[NVM], R gm, R ro_lim, R pr_lim) {
+PIP_HD void u2v_mhd(const R (&u)[NVM], R (&v)[NVM], R gm, R ro_lim, R pr_lim) {
   R ro = rmax(u[0], ro_lim);
   R roi = R(1) / ro;
   v[0] = ro;
@@ -53,7 +63,7 @@ __device__ __forceinline__ void u2v_mhd(const R (&u)[NVM], R (&v)[NVM], R gm, R 
 
 // u2v_hd (HLL_rot.f90:1136-1156).
 template <typename R>
-__device__ __forceinline__ void u2v_hd(const R (&u)[5], R (&v)[5], R gm, R ro_lim, R pr_lim) {
+PIP_HD void u2v_hd(const R (&u)[5], R (&v)[5], R gm, R ro_lim, R pr_lim) {
   R ro = rmax(u[0], ro_lim);
   R roi = R(1) / ro;
   v[0] = ro;
@@ -72,7 +82,7 @@ template <typename R> struct Prim {
 // cq2pv_mhd (Scheme_rot.f90:153-179): floors and rewrites the conserved ion state through
 // primitives, in place.  Returns the primitives.
 template <typename R, int NVM>
-__device__ __forceinline__ Prim<R> cq2pv_mhd(R (&u)[NVM], R gm, R ro_lim, R pr_lim) {
+PIP_HD Prim<R> cq2pv_mhd(R (&u)[NVM], R gm, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
   R vx = u[1] / de, vy = u[2] / de, vz = u[3] / de;
@@ -93,7 +103,7 @@ __device__ __forceinline__ Prim<R> cq2pv_mhd(R (&u)[NVM], R gm, R ro_lim, R pr_l
 
 // cq2pv_hd (Scheme_rot.f90:132-150).
 template <typename R>
-__device__ __forceinline__ Prim<R> cq2pv_hd(R (&u)[5], R gm, R ro_lim, R pr_lim) {
+PIP_HD Prim<R> cq2pv_hd(R (&u)[5], R gm, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
   R vx = u[1] / de, vy = u[2] / de, vz = u[3] / de;
@@ -111,7 +121,7 @@ __device__ __forceinline__ Prim<R> cq2pv_hd(R (&u)[5], R gm, R ro_lim, R pr_lim)
 
 // cq2pv with one division per species (reciprocal form, see below).
 template <typename R, int NVM>
-__device__ __forceinline__ Prim<R> cq2pv_mhd_rcp(R (&u)[NVM], R gm, R igm1, R ro_lim, R pr_lim) {
+PIP_HD Prim<R> cq2pv_mhd_rcp(R (&u)[NVM], R gm, R igm1, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
   const R inv = R(1) / de;
@@ -130,7 +140,7 @@ __device__ __forceinline__ Prim<R> cq2pv_mhd_rcp(R (&u)[NVM], R gm, R igm1, R ro
   return q;
 }
 template <typename R>
-__device__ __forceinline__ Prim<R> cq2pv_hd_rcp(R (&u)[5], R gm, R igm1, R ro_lim, R pr_lim) {
+PIP_HD Prim<R> cq2pv_hd_rcp(R (&u)[5], R gm, R igm1, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
   const R inv = R(1) / de;
@@ -151,7 +161,7 @@ __device__ __forceinline__ Prim<R> cq2pv_hd_rcp(R (&u)[5], R gm, R igm1, R ro_li
 // CFL candidates of one interior cell (cfl_mhd Scheme_rot.f90:279-283, cfl_hd :229-233),
 // from the primitives of the cq2pv rewrite.  sg = safety*gmin.
 template <typename R>
-__device__ __forceinline__ R cfl_mhd_cell(const Prim<R>& q, R bx, R by, R bz, R gm, R sg) {
+PIP_HD R cfl_mhd_cell(const Prim<R>& q, R bx, R by, R bz, R gm, R sg) {
   R dm = rmax(q.de, R(kTiny));
   R cs2 = gm * q.pr / dm;
   R valf2 = (bx * bx + by * by + bz * bz) / dm;
@@ -159,7 +169,7 @@ __device__ __forceinline__ R cfl_mhd_cell(const Prim<R>& q, R bx, R by, R bz, R 
   return sg / (vabs + rsqrt_(cs2 + valf2));
 }
 template <typename R>
-__device__ __forceinline__ R cfl_hd_cell(const Prim<R>& q, R gm, R sg) {
+PIP_HD R cfl_hd_cell(const Prim<R>& q, R gm, R sg) {
   R cs = rsqrt_(gm * q.pr / q.de);
   R vabs = rsqrt_(rmax(q.vx * q.vx + q.vy * q.vy + q.vz * q.vz, R(kTiny)));
   return sg / (vabs + cs);
@@ -169,7 +179,7 @@ __device__ __forceinline__ R cfl_hd_cell(const Prim<R>& q, R gm, R sg) {
 
 // minmod_func (Util_rot.f90:59-76): slope at cell 1 of the triple (v0, v1, v2).
 template <typename R>
-__device__ __forceinline__ R minmod(R v0, R v1, R v2) {
+PIP_HD R minmod(R v0, R v1, R v2) {
   R X = v2 - v1, Y = v1 - v0;
   R SX = rsign1(X);
   return SX * rmax(R(0), rmin(rabs(X), SX * Y));
@@ -179,7 +189,7 @@ __device__ __forceinline__ R minmod(R v0, R v1, R v2) {
 
 // hllc_flux (HLL_rot.f90:615-687), primitive states (ro, vn, vt1, vt2, pr).
 template <typename R>
-__device__ __forceinline__ void hllc_flux(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R gm) {
+PIP_HD void hllc_flux(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R gm) {
   const R gm1 = gm - R(1);
   R u_l[5], u_r[5], fl[5], fr[5], stl[5], str[5];
   u_l[0] = v_l[0]; u_l[1] = v_l[0] * v_l[1]; u_l[2] = v_l[0] * v_l[2]; u_l[3] = v_l[0] * v_l[3];
@@ -230,7 +240,7 @@ __device__ __forceinline__ void hllc_flux(const R (&v_l)[5], const R (&v_r)[5], 
 // Dedner flux of (Bn, psi) when NVM == 9.  States are primitive
 // (ro, vn, vt1, vt2, pr, Bn, Bt1, Bt2[, psi]).
 template <typename R, int NVM>
-__device__ __forceinline__ void hlld_flux(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM],
+PIP_HD void hlld_flux(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM],
                                           R gm, R cmax) {
   const R gm1 = gm - R(1);
   // v2u_1 energies (HLL_rot.f90:1201-1213)
@@ -423,17 +433,29 @@ __device__ __forceinline__ void hlld_flux(const R (&v_l)[NVM], const R (&v_r)[NV
 // used by the FMA build (held to 1e-10 relative L1 against the oracle over whole runs)
 // and by the FP32-mixed form.
 
-__device__ __forceinline__ double rrsqrt(double a) { return rsqrt(a); }
-__device__ __forceinline__ float rrsqrt(float a) { return rsqrtf(a); }
+PIP_HD double rrsqrt(double a) {
+#if defined(__CUDA_ARCH__)
+  return rsqrt(a);
+#else
+  return 1.0 / std::sqrt(a);
+#endif
+}
+PIP_HD float rrsqrt(float a) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(a);
+#else
+  return 1.0f / std::sqrt(a);
+#endif
+}
 
 // HLLC smooth switch (|s|+s)/max(2s,eps) without a division: 1 for s >= eps/2, 0 for s<=0.
 template <typename R>
-__device__ __forceinline__ R hllc_switch(R s) {
+PIP_HD R hllc_switch(R s) {
   return s >= R(0.5 * kHllcEpsi) ? R(1) : (s > R(0) ? R(2) * s * R(1.0 / kHllcEpsi) : R(0));
 }
 
 template <typename R>
-__device__ __forceinline__ void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R gm,
+PIP_HD void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R gm,
                                               R igm1) {
   R u_l[5], u_r[5], fl[5], fr[5], stl[5], str[5];
   const R ke_l = v_l[1] * v_l[1] + v_l[2] * v_l[2] + v_l[3] * v_l[3];
@@ -483,7 +505,7 @@ __device__ __forceinline__ void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[
 }
 
 template <typename R, int NVM>
-__device__ __forceinline__ void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM],
+PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM],
                                               R gm, R igm1, R cmax) {
   const R b2_l = (v_l[5] * v_l[5] + v_l[6] * v_l[6] + v_l[7] * v_l[7]);
   const R b2_r = (v_r[5] * v_r[5] + v_r[6] * v_r[6] + v_r[7] * v_r[7]);
