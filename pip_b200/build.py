@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpipgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+          "-Xcompiler", "-Wno-unknown-pragmas", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 EXTRA_FLAGS = {
     "pip_fp64_exact.cu": ["-fmad=false"],
     "pip_mixed.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],

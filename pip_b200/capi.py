@@ -38,6 +38,9 @@ EXPORTS = (
     # include/pip_ensemble.h
     "pip_ensemble_create", "pip_ensemble_destroy", "pip_ensemble_upload", "pip_ensemble_run",
     "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
+    # include/pip_adjoint.h
+    "pip_adj_create", "pip_adj_destroy", "pip_adj_set_col", "pip_adj_forward",
+    "pip_adj_backward", "pip_adj_dt",
 )
 
 _lib = None
@@ -101,6 +104,13 @@ def lib(path: Optional[str] = None):
     L.pip_ensemble_member.argtypes = [vp, i, dp, dp, dp, P(ctypes.c_int64), P(i)]
     L.pip_ensemble_set_config.argtypes = [vp, i, i]
     L.pip_ensemble_tune.argtypes = [vp, d, P(i), P(i), P(ctypes.c_float)]
+    L.pip_adj_create.argtypes = [P(PipParams), ctypes.c_int64, i, P(vp)]
+    L.pip_adj_destroy.argtypes = [vp]
+    L.pip_adj_destroy.restype = None
+    L.pip_adj_set_col.argtypes = [vp, d]
+    L.pip_adj_forward.argtypes = [vp, vp, vp, ctypes.c_int64, P(ctypes.c_float)]
+    L.pip_adj_backward.argtypes = [vp, vp, vp, dp, P(ctypes.c_float)]
+    L.pip_adj_dt.argtypes = [vp, dp, ctypes.c_int64, P(ctypes.c_int64)]
     for name in ("pip_ensemble_create", "pip_ensemble_upload", "pip_ensemble_run",
                  "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune"):
         getattr(L, name).restype = i

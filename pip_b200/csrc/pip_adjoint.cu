@@ -1,0 +1,896 @@
+// pip_adjoint.cu -- discrete adjoint of the FP64 two-fluid step (include/pip_adjoint.h).
+//
+// Forward model of one step n (the kernels of pip_run, main.f90:31-68, Solver_rot.f90:42-81):
+//   dt_n = CFL(z_n)                             (cfl, Scheme_rot.f90:183-213)
+//   U1   = z_n + dt_n/2 * G(z_n)                (stage 1)
+//   U2   = z_n + dt_n   * G(U1)                 (stage 2)
+//   z_n+1 = fill(rewrite(U2))                   (PIPbnd, cq2pv rewrites of the two cfl calls)
+// with G(U) = -div F(MUSCL-minmod(u2v(U))) + S(cq2pv(U)) on interior cells and fill() the
+// ghost copy of Boundary_rot.f90.  The reverse sweep of a step, for a cotangent La of z_n+1:
+//   fold(La)                                    ghost cotangents -> their interior sources
+//   Lb   = (dt_n G'(U1))^T La                   stage_vjp_kernel, stage 2
+//   fold(Lb)
+//   La   = La + Lb + (dt_n/2 G'(z_n))^T Lb      stage_vjp_kernel, stage 1, in place
+//   La  += (dL/ddt_n) dCFL/dz_n, dL/dalpha_c   finalize_kernel
+// where dL/ddt_n = (<La, G(U1)> + <Lb, G(z_n)>/2) is accumulated by the two stage kernels
+// from face fluxes and cell sources, and the CFL derivative is taken at the cell (or the
+// collision bound) that set dt_n.  States z_n, U1 of a segment of K steps are recomputed
+// from the segment's checkpoint with the recorded dt (bitwise the forward trajectory).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/pip_adjoint.h"
+#include "../../include/pip_gpu.h"
+#include "pip_adjoint_physics.cuh"
+#include "pip_kernels.cuh"
+
+namespace pip {
+namespace adjk {
+
+constexpr int NVM = 8, NV = 13;
+
+template <int NDIM> struct VT;
+template <> struct VT<2> {
+  static constexpr int TX = 32, TY = 8, NT = 256;
+};
+template <> struct VT<1> {
+  static constexpr int TX = 256, TY = 1, NT = 256;
+};
+
+// Output tile TX x TY cells; primitives on the tile plus 3 cells along each axis (the
+// 4-cell MUSCL stencils of the faces within 2 cells of the tile); faces k+1/2 for
+// k = i0-2 .. i0+TX (x) and the same along y.
+template <int NDIM> struct Geo {
+  static constexpr int TX = VT<NDIM>::TX, TY = VT<NDIM>::TY, NT = VT<NDIM>::NT;
+  static constexpr int HV = 3;
+  static constexpr int RX = TX + 2 * HV, RY = NDIM == 2 ? TY + 2 * HV : 1, RR = RX * RY;
+  static constexpr int NFX = (TX + 3) * TY;
+  static constexpr int NFY = NDIM == 2 ? TX * (TY + 3) : 0;
+  static constexpr int NF = NFX + NFY;
+  static constexpr size_t smem =
+      sizeof(double) * ((size_t)NV * RR + 2ull * NV * NF) + sizeof(unsigned long long) * NF;
+};
+
+// Per-block CFL candidates of stage 1 (the state z_n).
+struct CandPart {
+  double cmin;
+  long long cidx;
+  double rmax;
+  long long ridx;
+  int ckind;  // 0 ions, 1 neutrals
+  int rsp;    // species of rmax: 0 ions, 1 neutrals
+};
+
+__device__ __forceinline__ bool interior(const KParams &p, int i, int j) {
+  return i >= p.m0 && i < p.m0 + p.nx && (p.ndim == 1 || (j >= p.m1 && j < p.m1 + p.ny));
+}
+
+// direction 2 swaps (vx, vy) and (bx, by) (set_HLLD_fluxes, HLL_rot.f90:365-383)
+__device__ __forceinline__ int perm_m(int n) {
+  return n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n;
+}
+__device__ __forceinline__ int perm_h(int n) { return n == 1 ? 2 : n == 2 ? 1 : n; }
+
+// minmod derivative of the slope at cell 1 of (v0, v1, v2) with respect to v_q
+__device__ __forceinline__ double dmm(int mode, int q) {
+  if (mode == 1) return q == 1 ? -1.0 : (q == 2 ? 1.0 : 0.0);
+  if (mode == 2) return q == 0 ? -1.0 : (q == 1 ? 1.0 : 0.0);
+  return 0.0;
+}
+
+// Reverse of one face: MUSCL-minmod face states from the primitives in shared memory
+// (cells a - s, a, a + s, a + 2s along the face normal), the density floors and the
+// Riemann solvers.  lamF: cotangent of the face flux (natural variable order).  Writes the
+// cotangents of the two face states (gL, gR, natural order, after the floors), the minmod
+// branches and returns <F, lamF>.
+template <int RR>
+__device__ __forceinline__ double face_vjp(const KParams &p, const double *sV, int a, int s, bool ydir,
+                                           const double (&lamF)[NV], double *gL, double *gR,
+                                           int nf, int f, unsigned long long &modes) {
+  double fdot = 0.0;
+  modes = 0ull;
+  {
+    double vl[8], vr[8], af[8], avl[8], avr[8], flx[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int src = ydir ? perm_m(n) : n;
+      const double *v = sV + src * RR + a;
+      const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+      const int mL = adj::minmod_mode(v0, v1, v2), mR = adj::minmod_mode(v1, v2, v3);
+      modes |= (unsigned long long)(mL | (mR << 2)) << (4 * src);
+      vl[n] = v1 + 0.5 * minmod<double>(v0, v1, v2);
+      vr[n] = v2 - 0.5 * minmod<double>(v1, v2, v3);
+      af[n] = lamF[src];
+      avl[n] = 0.0;
+      avr[n] = 0.0;
+    }
+    const bool fl0 = vl[0] < p.ro_lim, fr0 = vr[0] < p.ro_lim;
+    vl[0] = fmax(vl[0], p.ro_lim);
+    vr[0] = fmax(vr[0], p.ro_lim);
+    adj::hlld_vjp(vl, vr, af, p.gm, p.igm1, avl, avr, flx);
+    if (fl0) avl[0] = 0.0;
+    if (fr0) avr[0] = 0.0;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int src = ydir ? perm_m(n) : n;
+      fdot += flx[n] * af[n];
+      gL[src * nf + f] = avl[n];
+      gR[src * nf + f] = avr[n];
+    }
+  }
+  {
+    double vl[5], vr[5], af[5], avl[5], avr[5], flx[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      const int src = ydir ? perm_h(n) : n;
+      const double *v = sV + (NVM + src) * RR + a;
+      const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
+      const int mL = adj::minmod_mode(v0, v1, v2), mR = adj::minmod_mode(v1, v2, v3);
+      modes |= (unsigned long long)(mL | (mR << 2)) << (4 * (NVM + src));
+      vl[n] = v1 + 0.5 * minmod<double>(v0, v1, v2);
+      vr[n] = v2 - 0.5 * minmod<double>(v1, v2, v3);
+      af[n] = lamF[NVM + src];
+      avl[n] = 0.0;
+      avr[n] = 0.0;
+    }
+    const bool fl0 = vl[0] < p.ro_lim, fr0 = vr[0] < p.ro_lim;
+    vl[0] = fmax(vl[0], p.ro_lim);
+    vr[0] = fmax(vr[0], p.ro_lim);
+    adj::hllc_vjp(vl, vr, af, p.gm, p.igm1, avl, avr, flx);
+    if (fl0) avl[0] = 0.0;
+    if (fr0) avr[0] = 0.0;
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      const int src = ydir ? perm_h(n) : n;
+      fdot += flx[n] * af[n];
+      gL[(NVM + src) * nf + f] = avl[n];
+      gR[(NVM + src) * nf + f] = avr[n];
+    }
+  }
+  return fdot;
+}
+
+// Adds the contributions of the four faces k = c-2 .. c+1 (local indices f0 .. f0+3*df) of
+// one direction to the primitive cotangents of cell c.
+__device__ __forceinline__ void gather_dir(const double *gL, const double *gR,
+                                           const unsigned long long *sM, int nf, int f0, int df,
+                                           double (&av)[NV]) {
+  const int fa = f0, fb = f0 + df, fc = f0 + 2 * df, fd = f0 + 3 * df;  // k = c-2, c-1, c, c+1
+  const unsigned long long ma = sM[fa], mb = sM[fb], mc = sM[fc], md = sM[fd];
+#pragma unroll
+  for (int n = 0; n < NV; ++n) {
+    const int sh = 4 * n;
+    // face k = c-2: cell c is k+2 (third cell of the right stencil)
+    const double gRa = gR[n * nf + fa];
+    double acc = -0.5 * gRa * dmm((int)((ma >> (sh + 2)) & 3ull), 2);
+    // face k = c-1: cell c is k+1 (right cell)
+    const double gLb = gL[n * nf + fb], gRb = gR[n * nf + fb];
+    acc += gRb + 0.5 * gLb * dmm((int)((mb >> sh) & 3ull), 2) -
+           0.5 * gRb * dmm((int)((mb >> (sh + 2)) & 3ull), 1);
+    // face k = c: cell c is k (left cell)
+    const double gLc = gL[n * nf + fc], gRc = gR[n * nf + fc];
+    acc += gLc + 0.5 * gLc * dmm((int)((mc >> sh) & 3ull), 1) -
+           0.5 * gRc * dmm((int)((mc >> (sh + 2)) & 3ull), 0);
+    // face k = c+1: cell c is k-1 (first cell of the left stencil)
+    const double gLd = gL[n * nf + fd];
+    acc += 0.5 * gLd * dmm((int)((md >> sh) & 3ull), 0);
+    av[n] += acc;
+  }
+}
+
+// Reverse of one RK stage over a tile of the whole (ghosted) array.  Us: stage input
+// state; lam: cotangent of the stage output (interior cells); out: cotangent of Us (every
+// cell), plus acc + lam at interior cells when acc is given (stage 1: the U0 terms).
+template <int NDIM>
+__global__ void __launch_bounds__(VT<NDIM>::NT, 1)
+stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *__restrict__ lam,
+                 const double *acc, double *out, const double *dtp, double fac,
+                 double *part_dot, double *part_dac, CandPart *cand) {
+  using G = Geo<NDIM>;
+  constexpr int TX = G::TX, TY = G::TY, NT = G::NT, HV = G::HV, RX = G::RX, RR = G::RR;
+  constexpr int NFX = G::NFX, NF = G::NF;
+  extern __shared__ double smem[];
+  double *sV = smem;
+  double *gL = sV + NV * RR;
+  double *gR = gL + NV * NF;
+  unsigned long long *sM = reinterpret_cast<unsigned long long *>(gR + NV * NF);
+  __shared__ double s_red[4][NT / 32];
+  __shared__ long long s_idx[2][NT / 32];
+  __shared__ int s_kind[2][NT / 32];
+
+  const int tid = threadIdx.x;
+  const double dt_sub = fac * (*dtp);
+  const long long nc = p.nc;
+  const int i0 = blockIdx.x * TX, j0 = NDIM == 2 ? blockIdx.y * TY : 0;
+
+  // ---- 1. primitives of the tile and its stencil reach
+  for (int idx = tid; idx < RR; idx += NT) {
+    const int ri = idx % RX, rj = idx / RX;
+    const bool ox = ri < HV || ri >= TX + HV, oy = NDIM == 2 && (rj < HV || rj >= TY + HV);
+    if (ox && oy) continue;
+    const int gi = i0 - HV + ri, gj = NDIM == 2 ? j0 - HV + rj : 0;
+    if (gi < 0 || gi >= p.ix || gj < 0 || gj >= p.jx) {
+#pragma unroll
+      for (int n = 0; n < NV; ++n) sV[n * RR + idx] = 0.0;
+      continue;
+    }
+    const long long q = (long long)gj * p.ix + gi;
+    double um[8], uh[5], vm[8], vh[5];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) um[n] = Us[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uh[n] = Us[q + (NVM + n) * nc];
+    u2v_mhd<double, 8>(um, vm, p.gm, p.ro_lim, p.pr_lim);
+    u2v_hd<double>(uh, vh, p.gm, p.ro_lim, p.pr_lim);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) sV[n * RR + idx] = vm[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+  }
+  __syncthreads();
+
+  // ---- 2. faces
+  double dot = 0.0;
+  for (int f = tid; f < NF; f += NT) {
+    int ca_i, ca_j, cb_i, cb_j, a, s;
+    bool ydir, owned;
+    if (f < NFX) {
+      const int fl = f % (TX + 3), fj = f / (TX + 3);
+      ca_i = i0 - 2 + fl;
+      ca_j = j0 + fj;
+      cb_i = ca_i + 1;
+      cb_j = ca_j;
+      a = (NDIM == 2 ? (fj + HV) * RX : 0) + fl - 2 + HV;
+      s = 1;
+      ydir = false;
+      owned = fl >= 2 && fl < TX + 2;
+    } else {
+      const int g = f - NFX, fi = g % TX, fk = g / TX;
+      ca_i = i0 + fi;
+      ca_j = j0 - 2 + fk;
+      cb_i = ca_i;
+      cb_j = ca_j + 1;
+      a = (fk - 2 + HV) * RX + fi + HV;
+      s = RX;
+      ydir = true;
+      owned = fk >= 2 && fk < TY + 2;
+    }
+    const bool in_a = interior(p, ca_i, ca_j), in_b = interior(p, cb_i, cb_j);
+    if (!in_a && !in_b) {
+#pragma unroll
+      for (int n = 0; n < NV; ++n) {
+        gL[n * NF + f] = 0.0;
+        gR[n * NF + f] = 0.0;
+      }
+      sM[f] = 0ull;
+      continue;
+    }
+    double ca = 0.0, cb = 0.0;
+    if (!ydir) {
+      if (in_a) ca = dt_sub / p.dx[ca_i];
+      if (in_b) cb = dt_sub / p.dx[cb_i];
+    } else {
+      if (in_a) ca = dt_sub / p.dy[ca_j];
+      if (in_b) cb = dt_sub / p.dy[cb_j];
+    }
+    const long long qa = (long long)ca_j * p.ix + ca_i, qb = (long long)cb_j * p.ix + cb_i;
+    double lamF[NV];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const double la = in_a ? lam[qa + n * nc] : 0.0;
+      const double lb = in_b ? lam[qb + n * nc] : 0.0;
+      lamF[n] = -ca * la + cb * lb;
+    }
+    unsigned long long m;
+    const double fd = face_vjp<RR>(p, sV, a, s, ydir, lamF, gL, gR, NF, f, m);
+    sM[f] = m;
+    if (owned) dot += fd;
+  }
+  __syncthreads();
+
+  // ---- 3. cells: gather, u2v, source, output
+  const int ti = tid % TX, tj = tid / TX;
+  const int gi = i0 + ti, gj = j0 + tj;
+  double dac = 0.0;
+  double cmin = 1.0e300, rmax = -1.0e300;
+  long long cidx = -1, ridx = -1;
+  int ckind = 0, rsp = 0;
+  if (tj < TY && gi < p.ix && gj < p.jx) {
+    const long long q = (long long)gj * p.ix + gi;
+    double av[NV];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) av[n] = 0.0;
+    gather_dir(gL, gR, sM, NF, tj * (TX + 3) + ti, 1, av);
+    if (NDIM == 2) gather_dir(gL, gR, sM, NF, NFX + tj * TX + ti, TX, av);
+    double um[8], uh[5];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) um[n] = Us[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uh[n] = Us[q + (NVM + n) * nc];
+    double aum[8] = {0, 0, 0, 0, 0, 0, 0, 0}, auh[5] = {0, 0, 0, 0, 0};
+    {
+      double avm[8], avh[5];
+#pragma unroll
+      for (int n = 0; n < 8; ++n) avm[n] = av[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) avh[n] = av[NVM + n];
+      adj::u2v_mhd_vjp(um, avm, p.gm, p.ro_lim, p.pr_lim, aum);
+      adj::u2v_hd_vjp(uh, avh, p.gm, p.ro_lim, p.pr_lim, auh);
+    }
+    const bool in = interior(p, gi, gj);
+    if (in) {
+      double lm[NV];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) lm[n] = lam[q + n * nc];
+      double ads[5];
+      ads[0] = 0.0;
+#pragma unroll
+      for (int k = 1; k < 5; ++k) ads[k] = dt_sub * (lm[k] - lm[NVM + k]);
+      const double d = adj::collision_vjp(um, uh, ads, p.gm, p.igm1, p.ac, p.ro_lim, p.pr_lim, aum, auh);
+      dac += d;
+      dot += p.ac * d;
+      if (acc) {
+#pragma unroll
+        for (int n = 0; n < 8; ++n) aum[n] += acc[q + n * nc] + lm[n];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) auh[n] += acc[q + (NVM + n) * nc] + lm[NVM + n];
+      }
+      if (cand) {
+        double wm[8], wh[5];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) wm[n] = um[n];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) wh[n] = uh[n];
+        const Prim<double> qm = cq2pv_mhd_rcp<double, 8>(wm, p.gm, p.igm1, p.ro_lim, p.pr_lim);
+        const Prim<double> qh = cq2pv_hd_rcp<double>(wh, p.gm, p.igm1, p.ro_lim, p.pr_lim);
+        const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+        const double sg = p.safety * gmin;
+        const double cm = cfl_mhd_cell<double>(qm, wm[5], wm[6], wm[7], p.gm, sg);
+        const double ch = cfl_hd_cell<double>(qh, p.gm, sg);
+        cmin = fmin(cm, ch);
+        ckind = cm <= ch ? 0 : 1;
+        cidx = q;
+        const double rm = um[0] * p.ac, rh = uh[0] * p.ac;
+        rmax = fmax(rm, rh);
+        rsp = rm >= rh ? 0 : 1;
+        ridx = q;
+      }
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) out[q + n * nc] = aum[n];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) out[q + (NVM + n) * nc] = auh[n];
+  }
+
+  // ---- 4. block reductions (fixed order: deterministic)
+  const int w = tid / 32, l = tid % 32;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dot += __shfl_xor_sync(0xffffffffu, dot, o);
+    dac += __shfl_xor_sync(0xffffffffu, dac, o);
+    if (cand) {
+      const double c2 = __shfl_xor_sync(0xffffffffu, cmin, o);
+      const long long i2 = __shfl_xor_sync(0xffffffffu, cidx, o);
+      const int k2 = __shfl_xor_sync(0xffffffffu, ckind, o);
+      if (c2 < cmin || (c2 == cmin && i2 >= 0 && (cidx < 0 || i2 < cidx))) {
+        cmin = c2;
+        cidx = i2;
+        ckind = k2;
+      }
+      const double r2 = __shfl_xor_sync(0xffffffffu, rmax, o);
+      const long long j2 = __shfl_xor_sync(0xffffffffu, ridx, o);
+      const int s2 = __shfl_xor_sync(0xffffffffu, rsp, o);
+      if (r2 > rmax || (r2 == rmax && j2 >= 0 && (ridx < 0 || j2 < ridx))) {
+        rmax = r2;
+        ridx = j2;
+        rsp = s2;
+      }
+    }
+  }
+  if (l == 0) {
+    s_red[0][w] = dot;
+    s_red[1][w] = dac;
+    s_red[2][w] = cmin;
+    s_red[3][w] = rmax;
+    s_idx[0][w] = cidx;
+    s_idx[1][w] = ridx;
+    s_kind[0][w] = ckind;
+    s_kind[1][w] = rsp;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    double sd = 0.0, sa = 0.0;
+    for (int k = 0; k < NT / 32; ++k) {
+      sd += s_red[0][k];
+      sa += s_red[1][k];
+    }
+    part_dot[bid] = sd;
+    part_dac[bid] = sa;
+    if (cand) {
+      CandPart c;
+      c.cmin = 1.0e300;
+      c.cidx = -1;
+      c.ckind = 0;
+      c.rmax = -1.0e300;
+      c.ridx = -1;
+      c.rsp = 0;
+      for (int k = 0; k < NT / 32; ++k) {
+        const long long i2 = s_idx[0][k];
+        if (i2 >= 0 && (s_red[2][k] < c.cmin || (s_red[2][k] == c.cmin && (c.cidx < 0 || i2 < c.cidx)))) {
+          c.cmin = s_red[2][k];
+          c.cidx = i2;
+          c.ckind = s_kind[0][k];
+        }
+        const long long j2 = s_idx[1][k];
+        if (j2 >= 0 && (s_red[3][k] > c.rmax || (s_red[3][k] == c.rmax && (c.ridx < 0 || j2 < c.ridx)))) {
+          c.rmax = s_red[3][k];
+          c.ridx = j2;
+          c.rsp = s_kind[1][k];
+        }
+      }
+      cand[bid] = c;
+    }
+  }
+}
+
+// Adjoint of the ghost fill (Boundary_rot.f90:54-125 as done by the stage kernels' ghost
+// writes): each interior cell within 2*margin of a boundary gathers the cotangents of the
+// ghost cells copied from it (x ghosts, y ghosts and corners, with their sign tables).
+// Ghost entries are left as they are; consumers read interior cells only.
+__global__ void fold_kernel(const KParams p, double *lam) {
+  const long long nint = (long long)p.nx * p.ny;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nint;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int gi = p.m0 + (int)(t % p.nx), gj = (p.ndim == 2 ? p.m1 : 0) + (int)(t / p.nx);
+    const bool nb = gi < 2 * p.m0 || gi >= p.ix - 2 * p.m0 ||
+                    (p.ndim == 2 && (gj < 2 * p.m1 || gj >= p.jx - 2 * p.m1));
+    if (!nb) continue;
+    int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
+    int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
+    for (int s = 0; s < 2; ++s)
+      for (int l = 0; l < p.m0; ++l)
+        if (p.gx[s][l] == gi) {
+          tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
+          sx[ntx++] = s;
+        }
+    if (p.ndim == 2)
+      for (int s = 0; s < 2; ++s)
+        for (int l = 0; l < p.m1; ++l)
+          if (p.gy[s][l] == gj) {
+            ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
+            sy[nty++] = s;
+          }
+    if (ntx == 0 && nty == 0) continue;
+    const long long nc = p.nc;
+    const long long q = (long long)gj * p.ix + gi;
+    for (int n = 0; n < NV; ++n) {
+      double add = 0.0;
+      for (int a = 0; a < ntx; ++a) {
+        const double g = (double)p.symx[sx[a]][n];
+        add += g * lam[(long long)gj * p.ix + tx[a] + n * nc];
+        for (int b = 0; b < nty; ++b)
+          add += (double)p.symy[sy[b]][n] * g * lam[(long long)ty[b] * p.ix + tx[a] + n * nc];
+      }
+      for (int b = 0; b < nty; ++b)
+        add += (double)p.symy[sy[b]][n] * lam[(long long)ty[b] * p.ix + gi + n * nc];
+      lam[q + n * nc] += add;
+    }
+  }
+}
+
+// One block: dL/ddt_n from the stage partials, the CFL bound that set dt_n and its
+// gradient (added to lamz at that cell), dL/dalpha_c accumulated into *dcol.
+__global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb,
+                                                       const double *p1dot, const double *p1dac,
+                                                       const double *p2dot, const double *p2dac,
+                                                       const CandPart *cand, const double *dtp,
+                                                       const double *z, double *lamz, double *dcol,
+                                                       double *ldt_out) {
+  __shared__ double s_a[256], s_b[256], s_c[256], s_r[256];
+  __shared__ long long s_ci[256], s_ri[256];
+  __shared__ int s_ck[256], s_rs[256];
+  const int t = threadIdx.x;
+  double sd = 0.0, sa = 0.0, cm = 1.0e300, rm = -1.0e300;
+  long long ci = -1, ri = -1;
+  int ck = 0, rs = 0;
+  for (int b = t; b < nb; b += 256) {
+    sd += p1dot[b] + p2dot[b];
+    sa += p1dac[b] + p2dac[b];
+    const CandPart c = cand[b];
+    if (c.cidx >= 0 && (c.cmin < cm || (c.cmin == cm && (ci < 0 || c.cidx < ci)))) {
+      cm = c.cmin;
+      ci = c.cidx;
+      ck = c.ckind;
+    }
+    if (c.ridx >= 0 && (c.rmax > rm || (c.rmax == rm && (ri < 0 || c.ridx < ri)))) {
+      rm = c.rmax;
+      ri = c.ridx;
+      rs = c.rsp;
+    }
+  }
+  s_a[t] = sd;
+  s_b[t] = sa;
+  s_c[t] = cm;
+  s_r[t] = rm;
+  s_ci[t] = ci;
+  s_ri[t] = ri;
+  s_ck[t] = ck;
+  s_rs[t] = rs;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (t < h) {
+      s_a[t] += s_a[t + h];
+      s_b[t] += s_b[t + h];
+      const long long i2 = s_ci[t + h];
+      if (i2 >= 0 && (s_c[t + h] < s_c[t] || (s_c[t + h] == s_c[t] && (s_ci[t] < 0 || i2 < s_ci[t])))) {
+        s_c[t] = s_c[t + h];
+        s_ci[t] = i2;
+        s_ck[t] = s_ck[t + h];
+      }
+      const long long j2 = s_ri[t + h];
+      if (j2 >= 0 && (s_r[t + h] > s_r[t] || (s_r[t + h] == s_r[t] && (s_ri[t] < 0 || j2 < s_ri[t])))) {
+        s_r[t] = s_r[t + h];
+        s_ri[t] = j2;
+        s_rs[t] = s_rs[t + h];
+      }
+    }
+    __syncthreads();
+  }
+  if (t != 0) return;
+  const double dt = *dtp;
+  const double ldt = s_a[0] / dt;
+  double dac = s_b[0];
+  const double cmin = s_c[0];
+  const double dtcol = p.col_lim / s_r[0];
+  const long long nc = p.nc;
+  if (dtcol < cmin && dtcol < 10.0 && s_ri[0] >= 0) {
+    // dt = col_lim / (alpha_c * rho) at the densest cell (cfl_pn_col, Scheme_rot.f90:305-313)
+    const long long q = s_ri[0];
+    const int plane = s_rs[0] == 0 ? 0 : NVM;
+    const double rho = z[q + plane * nc];
+    lamz[q + plane * nc] += ldt * (-dtcol / rho);
+    dac += ldt * (-dtcol / p.ac);
+  } else if (cmin < 10.0 && s_ci[0] >= 0) {
+    const long long q = s_ci[0];
+    const int gi = (int)(q % p.ix), gj = (int)(q / p.ix);
+    const double gmin = fmin(fmin(p.dx[gi], p.ndim == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+    const double sg = p.safety * gmin;
+    if (s_ck[0] == 0) {
+      double u[8], g[8];
+      for (int n = 0; n < 8; ++n) u[n] = z[q + n * nc];
+      adj::cfl_mhd_grad(u, p.gm, p.ro_lim, p.pr_lim, sg, g);
+      for (int n = 0; n < 8; ++n) lamz[q + n * nc] += ldt * g[n];
+    } else {
+      double u[5], g[5];
+      for (int n = 0; n < 5; ++n) u[n] = z[q + (NVM + n) * nc];
+      adj::cfl_hd_grad(u, p.gm, p.ro_lim, p.pr_lim, sg, g);
+      for (int n = 0; n < 5; ++n) lamz[q + (NVM + n) * nc] += ldt * g[n];
+    }
+  }
+  *dcol += dac;
+  if (ldt_out) *ldt_out = ldt;
+}
+
+template <int NDIM>
+cudaError_t launch_stage_vjp(const KParams &p, const double *Us, const double *lam, const double *acc,
+                             double *out, const double *dtp, double fac, double *pdot, double *pdac,
+                             CandPart *cand, cudaStream_t s) {
+  using G = Geo<NDIM>;
+  dim3 grid((p.ix + G::TX - 1) / G::TX, NDIM == 2 ? (p.jx + G::TY - 1) / G::TY : 1);
+  stage_vjp_kernel<NDIM><<<grid, G::NT, G::smem, s>>>(p, Us, lam, acc, out, dtp, fac, pdot, pdac, cand);
+  return cudaGetLastError();
+}
+
+int vjp_blocks(const KParams &p) {
+  if (p.ndim == 2) return ((p.ix + Geo<2>::TX - 1) / Geo<2>::TX) * ((p.jx + Geo<2>::TY - 1) / Geo<2>::TY);
+  return (p.ix + Geo<1>::TX - 1) / Geo<1>::TX;
+}
+
+cudaError_t prepare() {
+  cudaError_t e = cudaFuncSetAttribute(stage_vjp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Geo<2>::smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_vjp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Geo<1>::smem);
+}
+
+}  // namespace adjk
+}  // namespace pip
+
+using pip::DevCtrl;
+using pip::KParams;
+using pip::adjk::CandPart;
+
+struct pip_adj {
+  pip_params p{};
+  KParams kp{};
+  const pip::Launchers *L = nullptr;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t max_steps = 0, steps = 0;
+  int K = 25;
+  int nseg_max = 0;
+  size_t state_elems = 0;
+  double *A = nullptr, *B = nullptr;
+  std::vector<double *> ckpt;   // nseg_max states
+  std::vector<double *> segz;   // K-1 states (z_1 .. z_K-1 of a segment)
+  std::vector<double *> segu;   // K states (U1 of each step of a segment)
+  double *La = nullptr, *Lb = nullptr;
+  double *dt_hist = nullptr;
+  double *d_dx = nullptr, *d_dy = nullptr;
+  double *p1dot = nullptr, *p1dac = nullptr, *p2dot = nullptr, *p2dac = nullptr;
+  CandPart *cand = nullptr;
+  double *dcol = nullptr;
+  DevCtrl *ctrl = nullptr;
+  DevCtrl *h_ctrl = nullptr;
+  int nb = 0;
+  bool have_forward = false;
+};
+
+#define ACK(call)                                  \
+  do {                                             \
+    cudaError_t e__ = (call);                      \
+    if (e__ != cudaSuccess) {                      \
+      pip::record_cuda_error((int)e__);                 \
+      return PIP_ERR_CUDA;                         \
+    }                                              \
+  } while (0)
+
+namespace {
+
+int grid_fold(const KParams &k) {
+  long long n = (long long)k.nx * k.ny;
+  long long b = (n + 255) / 256;
+  if (b > 148 * 8) b = 148 * 8;
+  return (int)std::max(1ll, b);
+}
+
+cudaError_t launch_vjp(pip_adj *a, int stage, const double *Us, const double *lam, const double *acc,
+                       double *out, const double *dtp) {
+  const double fac = stage == 1 ? 0.5 : 1.0;
+  double *pd = stage == 1 ? a->p1dot : a->p2dot;
+  double *pa = stage == 1 ? a->p1dac : a->p2dac;
+  CandPart *c = stage == 1 ? a->cand : nullptr;
+  if (a->kp.ndim == 2)
+    return pip::adjk::launch_stage_vjp<2>(a->kp, Us, lam, acc, out, dtp, fac, pd, pa, c, a->stream);
+  return pip::adjk::launch_stage_vjp<1>(a->kp, Us, lam, acc, out, dtp, fac, pd, pa, c, a->stream);
+}
+
+void reset_slot(DevCtrl &h, int slot) {
+  const double ten = 10.0;
+  std::memcpy(&h.red_dt[slot], &ten, sizeof(double));
+  h.red_rho[slot] = 0ull;
+  h.red_gr[slot] = 0ull;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every, pip_adj **out) {
+  if (!out) return PIP_ERR_NULL;
+  *out = nullptr;
+  if (!p) return PIP_ERR_NULL;
+  KParams k;
+  int st = pip::kparams_from_params(p, &k);
+  if (st != PIP_OK) return st;
+  if (p->precision != PIP_FP64 || p->flag_divb != 0 || p->flag_pip_imp != 0 ||
+      p->flag_ir != PIP_IR_NONE || p->flag_heat != 0)
+    return PIP_ERR_PARAM;
+  if (max_steps <= 0) return PIP_ERR_PARAM;
+  pip_adj *a = new (std::nothrow) pip_adj();
+  if (!a) return PIP_ERR_NOMEM;
+  a->p = *p;
+  a->p.dx = a->p.dy = a->p.dz = nullptr;
+  a->kp = k;
+  a->L = p->fp_exact ? &pip::launchers_exact() : &pip::launchers_fast();
+  a->max_steps = max_steps;
+  a->K = checkpoint_every > 0 ? checkpoint_every : 25;
+  a->nseg_max = (int)((max_steps + a->K - 1) / a->K);
+  a->state_elems = (size_t)k.nc * (k.nvm + 5);
+  const size_t sb = a->state_elems * sizeof(double);
+  auto fail = [&](cudaError_t e) {
+    pip::record_cuda_error((int)e);
+    pip_adj_destroy(a);
+    return e == cudaErrorMemoryAllocation ? PIP_ERR_NOMEM : PIP_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaGetDevice(&a->device)) != cudaSuccess) return fail(e);
+  if ((e = a->L->prepare()) != cudaSuccess) return fail(e);
+  if ((e = pip::adjk::prepare()) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->A, sb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->B, sb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->La, sb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->Lb, sb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(a->B, 0, sb)) != cudaSuccess) return fail(e);
+  a->ckpt.assign(a->nseg_max, nullptr);
+  for (auto &x : a->ckpt)
+    if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
+  a->segz.assign(a->K > 1 ? a->K - 1 : 0, nullptr);
+  for (auto &x : a->segz)
+    if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
+  a->segu.assign(a->K, nullptr);
+  for (auto &x : a->segu) {
+    if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x, 0, sb)) != cudaSuccess) return fail(e);
+  }
+  if ((e = cudaMalloc(&a->dt_hist, sizeof(double) * max_steps)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->d_dx, sizeof(double) * p->ix)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->d_dy, sizeof(double) * p->jx)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemcpy(a->d_dx, p->dx, sizeof(double) * p->ix, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemcpy(a->d_dy, p->dy, sizeof(double) * p->jx, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return fail(e);
+  a->kp.dx = a->d_dx;
+  a->kp.dy = a->d_dy;
+  a->nb = pip::adjk::vjp_blocks(a->kp);
+  if ((e = cudaMalloc(&a->p1dot, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->p1dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->p2dot, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->p2dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->cand, sizeof(CandPart) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->dcol, sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocHost(&a->h_ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
+  std::memset(a->h_ctrl, 0, sizeof(DevCtrl));
+  *out = a;
+  return PIP_OK;
+}
+
+void pip_adj_destroy(pip_adj *a) {
+  if (!a) return;
+  cudaSetDevice(a->device);
+  if (a->stream) cudaStreamSynchronize(a->stream);
+  double *bufs[] = {a->A, a->B, a->La, a->Lb, a->dt_hist, a->d_dx, a->d_dy,
+                    a->p1dot, a->p1dac, a->p2dot, a->p2dac, a->dcol};
+  for (double *b : bufs)
+    if (b) cudaFree(b);
+  for (double *b : a->ckpt)
+    if (b) cudaFree(b);
+  for (double *b : a->segz)
+    if (b) cudaFree(b);
+  for (double *b : a->segu)
+    if (b) cudaFree(b);
+  if (a->cand) cudaFree(a->cand);
+  if (a->ctrl) cudaFree(a->ctrl);
+  if (a->h_ctrl) cudaFreeHost(a->h_ctrl);
+  if (a->stream) cudaStreamDestroy(a->stream);
+  delete a;
+}
+
+int pip_adj_set_col(pip_adj *a, double col) {
+  if (!a) return PIP_ERR_NULL;
+  if (!(col >= 0.0) || !std::isfinite(col)) return PIP_ERR_PARAM;
+  a->p.col = col;
+  a->kp.ac = col;
+  a->have_forward = false;
+  return PIP_OK;
+}
+
+int pip_adj_forward(pip_adj *a, const double *U0, double *UN, int64_t nsteps, float *device_ms) {
+  if (!a || !U0 || !UN) return PIP_ERR_NULL;
+  if (nsteps <= 0 || nsteps > a->max_steps) return PIP_ERR_PARAM;
+  ACK(cudaSetDevice(a->device));
+  const size_t sb = a->state_elems * sizeof(double);
+  DevCtrl &h = *a->h_ctrl;
+  std::memset(&h, 0, sizeof(DevCtrl));
+  h.nsteps = nsteps;
+  reset_slot(h, 0);
+  reset_slot(h, 1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (device_ms) {
+    ACK(cudaEventCreate(&e0));
+    ACK(cudaEventCreate(&e1));
+  }
+  ACK(cudaMemcpyAsync(a->ctrl, a->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice, a->stream));
+  if (device_ms) ACK(cudaEventRecord(e0, a->stream));
+  ACK(cudaMemcpyAsync(a->A, U0, sb, cudaMemcpyDeviceToDevice, a->stream));
+  // the loop of pip_run: cfl of the first step, then [stage 1, stage 2] per step
+  ACK(a->L->cfl(a->kp, a->A, a->ctrl, 0, a->stream));
+  for (int64_t n = 0; n < nsteps; ++n) {
+    if (n % a->K == 0)
+      ACK(cudaMemcpyAsync(a->ckpt[n / a->K], a->A, sb, cudaMemcpyDeviceToDevice, a->stream));
+    ACK(a->L->stage(a->kp, 1, a->A, a->A, a->B, a->ctrl, 1, 0, a->stream));
+    ACK(cudaMemcpyAsync(a->dt_hist + n, &a->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice,
+                        a->stream));
+    ACK(a->L->stage(a->kp, 2, a->B, a->A, a->A, a->ctrl, 1, -1, a->stream));
+  }
+  ACK(cudaMemcpyAsync(UN, a->A, sb, cudaMemcpyDeviceToDevice, a->stream));
+  if (device_ms) ACK(cudaEventRecord(e1, a->stream));
+  ACK(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(DevCtrl), cudaMemcpyDeviceToHost, a->stream));
+  ACK(cudaStreamSynchronize(a->stream));
+  if (device_ms) {
+    ACK(cudaEventElapsedTime(device_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  a->steps = h.step;
+  a->have_forward = h.step == nsteps && !h.nan_flag && h.status == 0;
+  if (h.nan_flag) return PIP_ERR_NAN;
+  if (h.status) return h.status;
+  if (h.step != nsteps) return PIP_ERR_STATE;
+  return PIP_OK;
+}
+
+int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, float *device_ms) {
+  if (!a || !gN || !g0) return PIP_ERR_NULL;
+  if (!a->have_forward) return PIP_ERR_STATE;
+  ACK(cudaSetDevice(a->device));
+  const size_t sb = a->state_elems * sizeof(double);
+  const KParams &kp = a->kp;
+  DevCtrl &h = *a->h_ctrl;
+  std::memset(&h, 0, sizeof(DevCtrl));
+  reset_slot(h, 0);
+  reset_slot(h, 1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (device_ms) {
+    ACK(cudaEventCreate(&e0));
+    ACK(cudaEventCreate(&e1));
+  }
+  ACK(cudaMemcpyAsync(a->ctrl, a->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice, a->stream));
+  if (device_ms) ACK(cudaEventRecord(e0, a->stream));
+  ACK(cudaMemcpyAsync(a->La, gN, sb, cudaMemcpyDeviceToDevice, a->stream));
+  ACK(cudaMemsetAsync(a->dcol, 0, sizeof(double), a->stream));
+  const int64_t N = a->steps;
+  const int nseg = (int)((N + a->K - 1) / a->K);
+  const int gf = grid_fold(kp);
+  for (int s = nseg - 1; s >= 0; --s) {
+    const int64_t n0 = (int64_t)s * a->K;
+    const int len = (int)std::min<int64_t>(a->K, N - n0);
+    auto zp = [&](int j) -> double * { return j == 0 ? a->ckpt[s] : a->segz[j - 1]; };
+    // recompute z_n, U1_n of the segment with the recorded dt
+    for (int j = 0; j < len; ++j) {
+      ACK(cudaMemcpyAsync(&a->ctrl->dt, a->dt_hist + n0 + j, sizeof(double), cudaMemcpyDeviceToDevice,
+                          a->stream));
+      ACK(a->L->stage(kp, 1, zp(j), zp(j), a->segu[j], a->ctrl, 0, 0, a->stream));
+      if (j + 1 < len) ACK(a->L->stage(kp, 2, a->segu[j], zp(j), zp(j + 1), a->ctrl, 0, 2, a->stream));
+    }
+    // reverse sweep
+    for (int j = len - 1; j >= 0; --j) {
+      const double *dtp = a->dt_hist + n0 + j;
+      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->La);
+      ACK(cudaGetLastError());
+      ACK(launch_vjp(a, 2, a->segu[j], a->La, nullptr, a->Lb, dtp));
+      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->Lb);
+      ACK(cudaGetLastError());
+      ACK(launch_vjp(a, 1, zp(j), a->Lb, a->La, a->La, dtp));
+      pip::adjk::finalize_kernel<<<1, 256, 0, a->stream>>>(kp, a->nb, a->p1dot, a->p1dac, a->p2dot,
+                                                            a->p2dac, a->cand, dtp, zp(j), a->La,
+                                                            a->dcol, nullptr);
+      ACK(cudaGetLastError());
+    }
+  }
+  ACK(cudaMemcpyAsync(g0, a->La, sb, cudaMemcpyDeviceToDevice, a->stream));
+  if (device_ms) ACK(cudaEventRecord(e1, a->stream));
+  double dc = 0.0;
+  ACK(cudaMemcpyAsync(&a->h_ctrl->dt, a->dcol, sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+  ACK(cudaStreamSynchronize(a->stream));
+  dc = a->h_ctrl->dt;
+  if (g_col) *g_col = dc;
+  if (device_ms) {
+    ACK(cudaEventElapsedTime(device_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  return PIP_OK;
+}
+
+int pip_adj_dt(pip_adj *a, double *dt, int64_t n, int64_t *steps) {
+  if (!a) return PIP_ERR_NULL;
+  if (steps) *steps = a->steps;
+  if (dt && n > 0) {
+    ACK(cudaSetDevice(a->device));
+    const int64_t m = std::min(n, a->steps);
+    if (m > 0) ACK(cudaMemcpy(dt, a->dt_hist, sizeof(double) * m, cudaMemcpyDeviceToHost));
+  }
+  return PIP_OK;
+}
+
+}  // extern "C"

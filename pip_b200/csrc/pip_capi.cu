@@ -213,6 +213,8 @@ void build_kparams(pip_ctx *c) {
 
 }  // namespace
 
+void pip::record_cuda_error(int code) { g_last_cuda_error = code; }
+
 // Kernel parameters straight from a parameter block, for callers without a context: the
 // same validation and tables as pip_ctx_create, built on the stack (no allocation).  The
 // dx/dy pointers of the result are left null for the caller to point at device copies.

@@ -447,12 +447,11 @@ struct pip_ensemble {
   int graph_threads = 0, graph_ctas = 0;
 };
 
-static int g_ens_cuda_error = 0;
 #define EK(call)                        \
   do {                                  \
     cudaError_t e__ = (call);           \
     if (e__ != cudaSuccess) {           \
-      g_ens_cuda_error = (int)e__;      \
+      pip::record_cuda_error((int)e__);      \
       return PIP_ERR_CUDA;              \
     }                                   \
   } while (0)
@@ -498,7 +497,7 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
   }
   e->total_floats = off;
   auto fail = [&](cudaError_t c) {
-    g_ens_cuda_error = (int)c;
+    pip::record_cuda_error((int)c);
     pip_ensemble_destroy(e);
     return c == cudaErrorMemoryAllocation ? PIP_ERR_NOMEM : PIP_ERR_CUDA;
   };

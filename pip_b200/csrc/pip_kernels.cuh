@@ -70,6 +70,9 @@ const Launchers &launchers_exact();
 struct pip_params;
 namespace pip {
 
+// Records a CUDA error code for pip_last_cuda_error (pip_capi.cu).
+void record_cuda_error(int code);
+
 // Validates a parameter block and fills the kernel parameters without allocating
 // (pip_capi.cu); dx and dy of the result are left null.
 int kparams_from_params(const pip_params *p, KParams *k);
