@@ -54,6 +54,16 @@ int pip_adj_forward(pip_adj *a, const double *U0, double *UN, int64_t nsteps, fl
  * (recomputation included). */
 int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, float *device_ms);
 
+/* Unit-level pieces of the reverse sweep (for tests).  pip_adj_stage_vjp: for one RK stage
+ * (stage 1 advances by dt/2, stage 2 by dt) from the stage state Us, writes the cotangent
+ * of Us (every cell, device) for the cotangent lam of the stage output on interior cells
+ * (device; ghost entries ignored), with *dot = dt_sub <lam, dU/d(dt_sub)> and
+ * *dcol = <lam, dU/dalpha_c>.  pip_adj_fold: the adjoint of the ghost fill in place --
+ * the cotangent of every ghost cell is added to the interior cell it copies. */
+int pip_adj_stage_vjp(pip_adj *a, int stage, const double *Us, const double *lam, double *out,
+                      double dt, double *dot, double *dcol);
+int pip_adj_fold(pip_adj *a, double *lam);
+
 /* The dt of each step of the last forward run (host array of n >= steps entries) and the
  * number of steps. */
 int pip_adj_dt(pip_adj *a, double *dt, int64_t n, int64_t *steps);

@@ -111,6 +111,32 @@ class AdjointRun:
         self.backward_ms = ms.value
         return g0, gc.value
 
+    def stage_vjp(self, stage: int, Us: torch.Tensor, lam: torch.Tensor, dt: float):
+        """Unit-level reverse of one RK stage: (cotangent of Us, dt_sub <lam, dU/d dt_sub>,
+        <lam, dU/dalpha_c>) for the cotangent lam of the stage output (interior cells)."""
+        Us = self._check_state(Us)
+        lam = self._check_state(lam)
+        out = torch.empty_like(Us)
+        dot = ctypes.c_double()
+        dcol = ctypes.c_double()
+        torch.cuda.current_stream().synchronize()
+        st = lib().pip_adj_stage_vjp(self.h, int(stage), ctypes.c_void_p(Us.data_ptr()),
+                                     ctypes.c_void_p(lam.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                     float(dt), ctypes.byref(dot), ctypes.byref(dcol))
+        if st != PIP_OK:
+            raise PipError(st, "pip_adj_stage_vjp")
+        return out, dot.value, dcol.value
+
+    def fold(self, lam: torch.Tensor) -> torch.Tensor:
+        """Adjoint of the ghost fill (a copy of lam with ghost cotangents added to their
+        interior sources; ghost entries left as they were)."""
+        lam = self._check_state(lam).clone()
+        torch.cuda.current_stream().synchronize()
+        st = lib().pip_adj_fold(self.h, ctypes.c_void_p(lam.data_ptr()))
+        if st != PIP_OK:
+            raise PipError(st, "pip_adj_fold")
+        return lam
+
     def dt_history(self) -> np.ndarray:
         n = ctypes.c_int64()
         out = np.empty(self.nsteps)

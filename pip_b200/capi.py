@@ -40,7 +40,7 @@ EXPORTS = (
     "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
     # include/pip_adjoint.h
     "pip_adj_create", "pip_adj_destroy", "pip_adj_set_col", "pip_adj_forward",
-    "pip_adj_backward", "pip_adj_dt",
+    "pip_adj_backward", "pip_adj_dt", "pip_adj_stage_vjp", "pip_adj_fold",
 )
 
 _lib = None
@@ -111,6 +111,8 @@ def lib(path: Optional[str] = None):
     L.pip_adj_forward.argtypes = [vp, vp, vp, ctypes.c_int64, P(ctypes.c_float)]
     L.pip_adj_backward.argtypes = [vp, vp, vp, dp, P(ctypes.c_float)]
     L.pip_adj_dt.argtypes = [vp, dp, ctypes.c_int64, P(ctypes.c_int64)]
+    L.pip_adj_stage_vjp.argtypes = [vp, i, vp, vp, vp, d, dp, dp]
+    L.pip_adj_fold.argtypes = [vp, vp]
     for name in ("pip_ensemble_create", "pip_ensemble_upload", "pip_ensemble_run",
                  "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune"):
         getattr(L, name).restype = i

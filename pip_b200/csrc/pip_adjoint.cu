@@ -627,6 +627,7 @@ struct pip_adj {
   double *p1dot = nullptr, *p1dac = nullptr, *p2dot = nullptr, *p2dac = nullptr;
   CandPart *cand = nullptr;
   double *dcol = nullptr;
+  double *d_dt = nullptr;         // dt of the unit-level stage VJP
   DevCtrl *ctrl = nullptr;
   DevCtrl *h_ctrl = nullptr;
   int nb = 0;
@@ -737,6 +738,7 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
   if ((e = cudaMalloc(&a->p2dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->cand, sizeof(CandPart) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->dcol, sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&a->h_ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
   std::memset(a->h_ctrl, 0, sizeof(DevCtrl));
@@ -749,7 +751,7 @@ void pip_adj_destroy(pip_adj *a) {
   cudaSetDevice(a->device);
   if (a->stream) cudaStreamSynchronize(a->stream);
   double *bufs[] = {a->A, a->B, a->La, a->Lb, a->dt_hist, a->d_dx, a->d_dy,
-                    a->p1dot, a->p1dac, a->p2dot, a->p2dac, a->dcol};
+                    a->p1dot, a->p1dac, a->p2dot, a->p2dac, a->dcol, a->d_dt};
   for (double *b : bufs)
     if (b) cudaFree(b);
   for (double *b : a->ckpt)
@@ -879,6 +881,38 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  return PIP_OK;
+}
+
+int pip_adj_stage_vjp(pip_adj *a, int stage, const double *Us, const double *lam, double *out,
+                      double dt, double *dot, double *dcol) {
+  if (!a || !Us || !lam || !out) return PIP_ERR_NULL;
+  if ((stage != 1 && stage != 2) || !(dt > 0.0)) return PIP_ERR_PARAM;
+  ACK(cudaSetDevice(a->device));
+  ACK(cudaMemcpyAsync(a->d_dt, &dt, sizeof(double), cudaMemcpyHostToDevice, a->stream));
+  ACK(launch_vjp(a, stage, Us, lam, nullptr, out, a->d_dt));
+  std::vector<double> pd(a->nb), pa(a->nb);
+  ACK(cudaMemcpyAsync(pd.data(), stage == 1 ? a->p1dot : a->p2dot, sizeof(double) * a->nb,
+                      cudaMemcpyDeviceToHost, a->stream));
+  ACK(cudaMemcpyAsync(pa.data(), stage == 1 ? a->p1dac : a->p2dac, sizeof(double) * a->nb,
+                      cudaMemcpyDeviceToHost, a->stream));
+  ACK(cudaStreamSynchronize(a->stream));
+  double sd = 0.0, sa = 0.0;
+  for (int b = 0; b < a->nb; ++b) {
+    sd += pd[b];
+    sa += pa[b];
+  }
+  if (dot) *dot = sd;
+  if (dcol) *dcol = sa;
+  return PIP_OK;
+}
+
+int pip_adj_fold(pip_adj *a, double *lam) {
+  if (!a || !lam) return PIP_ERR_NULL;
+  ACK(cudaSetDevice(a->device));
+  pip::adjk::fold_kernel<<<grid_fold(a->kp), 256, 0, a->stream>>>(a->kp, lam);
+  ACK(cudaGetLastError());
+  ACK(cudaStreamSynchronize(a->stream));
   return PIP_OK;
 }
 

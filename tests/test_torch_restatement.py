@@ -6,6 +6,7 @@ import pytest
 import torch
 
 import torch_pip2d as T
+from generic_state import generic_state
 from oracle import oracle as O
 from pip_b200 import ics
 
@@ -18,15 +19,22 @@ def prologue_state(s, Uh, Um):
     return o, Uh0, Um0
 
 
-@pytest.mark.parametrize("col", [10.0, 300.0])
-def test_torch_restatement_matches_oracle(col):
-    s, Uh, Um = ics.wave_damping(16, 8, amp=3.0e-2, col=col)
+CASES = {
+    "periodic": dict(col=10.0),
+    "collision_dt": dict(col=300.0),
+    "reflect_outflow": dict(col=10.0, flag_bnd=[2, 2, 10, 10, 1, 1]),
+    "outflow_reflect": dict(col=10.0, flag_bnd=[10, 10, 2, 2, 1, 1]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_torch_restatement_matches_oracle(case):
+    s, _, _ = ics.wave_damping(16, 8, **CASES[case])
+    Uh, Um = generic_state(s, 3)
     o, Uh0, Um0 = prologue_state(s, Uh, Um)
     U0 = torch.from_numpy(np.concatenate([Um0, Uh0], axis=0))
-    _, _, _, dx, dy, _ = s.coordinates()
     with torch.no_grad():
-        UN, dts = T.run(U0, col, 12, s.gm, s.safety, s.ro_lim, s.pr_lim,
-                        torch.from_numpy(dx), torch.from_numpy(dy))
+        UN, dts = T.run(U0, CASES[case]["col"], 12, T.Geom(s))
     st, t, n, hist = o.run(nsteps=12, max_hist=12)
     o_h, o_m = o.state()
     o.close()
@@ -40,14 +48,27 @@ def test_torch_restatement_matches_oracle(col):
         assert err <= 1e-12 * max(den, 1e-300) or err < 1e-15 * got[v].size, (v, err, den)
 
 
+def test_torch_restatement_matches_oracle_1d():
+    s, _, _ = ics.brio_wu(48, col=30.0)
+    Uh, Um = generic_state(s, 4)
+    o, Uh0, Um0 = prologue_state(s, Uh, Um)
+    U0 = torch.from_numpy(np.concatenate([Um0, Uh0], axis=0))
+    with torch.no_grad():
+        UN, dts = T.run(U0, 30.0, 10, T.Geom(s))
+    st, t, n, hist = o.run(nsteps=10, max_hist=10)
+    o_h, o_m = o.state()
+    o.close()
+    np.testing.assert_allclose(np.array([float(d) for d in dts]), hist, rtol=1e-13, atol=0)
+    ref = np.concatenate([o_m, o_h], axis=0)
+    np.testing.assert_allclose(UN.numpy(), ref, rtol=1e-11, atol=1e-14)
+
+
 def test_torch_restatement_gradient_is_finite_and_nonzero():
     s, Uh, Um = ics.wave_damping(16, 8, amp=3.0e-2)
     _, Uh0, Um0 = prologue_state(s, Uh, Um)
     U0 = torch.from_numpy(np.concatenate([Um0, Uh0], axis=0)).requires_grad_(True)
     ac = torch.tensor(10.0, dtype=torch.float64, requires_grad=True)
-    _, _, _, dx, dy, _ = s.coordinates()
-    UN, _ = T.run(U0, ac, 4, s.gm, s.safety, s.ro_lim, s.pr_lim,
-                  torch.from_numpy(dx), torch.from_numpy(dy))
+    UN, _ = T.run(U0, ac, 4, T.Geom(s))
     loss = (UN[2, 2:-2, 2:-2] ** 2).sum() + (UN[8, 2:-2, 2:-2] ** 2).sum()
     loss.backward()
     assert torch.isfinite(U0.grad).all() and torch.isfinite(ac.grad)

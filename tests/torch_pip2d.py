@@ -2,16 +2,18 @@
 
 A third transcription of main.f90:31-68 / run_solver (Solver_rot.f90:42-81) for the case
 the discrete adjoint supports (flag_sch=0, flag_hll=2, s_order=2, t_order=2, ndim=2,
-flag_divb=0, explicit collisions flag_pip_imp=0, no IR), periodic boundaries, written with
+flag_divb=0, explicit collisions flag_pip_imp=0, no IR), ndim 1 or 2, written with
 whole-array torch operations in float64 so that ``torch.autograd`` gives an FP64 reference
 gradient of a short run.  Branches (minmod, HLLD fan regions, HLLC-G fallback, min/max of
-wave speeds, floors, the CFL minimum) are ``torch.where`` / ``minimum`` / ``maximum``
-selections, i.e. differentiated on the side taken -- the same convention as the hand-written
-adjoint it checks.  Expressions follow the literal Fortran forms (HLL_rot.f90,
+wave speeds, floors, the CFL minimum) are explicit ``torch.where`` selections with the tie
+rules of the hand-written adjoint it checks (minmod slope 0 when min(|X|, sign(X) Y) <= 0,
+else X when |X| <= sign(X) Y; the left operand of a min/max on a tie; the first cell of a
+CFL minimum), so that autograd differentiates the same branch even on a kink (ties are exact
+at reflecting and outflow boundaries and wherever two limited slopes coincide).  Expressions follow the literal Fortran forms (HLL_rot.f90,
 Scheme_rot.f90, PIP_rot.f90) like the C oracle.
 
 State: tensor (13, jx, ix) -- ion planes ro, mx, my, mz, en, bx, by, bz then neutral planes
-ro, mx, my, mz, en; margin 2.
+ro, mx, my, mz, en; margin 2 (jx = 1 in 1D).  Boundary codes 1, 2 and 10.
 """
 import torch
 
@@ -26,6 +28,16 @@ M = 2  # margin
 
 def _sgn1(x):
     return torch.copysign(torch.ones_like(x), x)
+
+
+def _min(a, b):
+    """min with the left operand on a tie."""
+    return torch.where(a <= b, a, b)
+
+
+def _max(a, b):
+    """max with the left operand on a tie."""
+    return torch.where(a >= b, a, b)
 
 
 def u2v_mhd(U, gm, ro_lim, pr_lim):                       # HLL_rot.f90:1159-1186
@@ -51,7 +63,8 @@ def face_states(V, ro_lim):
     X = V[..., 2:] - V[..., 1:-1]
     Y = V[..., 1:-1] - V[..., :-2]
     SX = _sgn1(X)
-    du = SX * torch.clamp(torch.minimum(torch.abs(X), SX * Y), min=0.0)
+    m = torch.minimum(torch.abs(X), SX * Y)
+    du = torch.where(m > 0.0, torch.where(torch.abs(X) <= SX * Y, X, Y), torch.zeros_like(X))
     VLs = V[..., 1:-1] + 0.5 * du     # VL at cells 1 .. n-2
     VRs = V[..., 1:-1] - 0.5 * du     # VR at faces 0 .. n-3
     L = VLs[..., :-1]
@@ -78,8 +91,8 @@ def hllc(vl, vr, gm):                                     # HLL_rot.f90:615-687
     csr = torch.sqrt(gm * prr / ur[0])
     vnl = ul[1] / ul[0]
     vnr = ur[1] / ur[0]
-    sl = ACC * torch.minimum(vnl - csl, vnr - csr)
-    sr = ACC * torch.maximum(vnl + csl, vnr + csr)
+    sl = ACC * _min(vnl - csl, vnr - csr)
+    sr = ACC * _max(vnl + csl, vnr + csr)
     sm = ((ur[1] * (sr - vnr) - ul[1] * (sl - vnl) + prl - prr) /
           (ur[0] * (sr - vnr) - ul[0] * (sl - vnl)))
     prm = sm * ul[0] * (sl - vnl) - ul[1] * (sl - vnl) + prl
@@ -91,7 +104,10 @@ def hllc(vl, vr, gm):                                     # HLL_rot.f90:615-687
                         ((sr - vnr) * ur[4] - prr * vnr + prm * sm) / (sr - sm)])
 
     def th(s):
-        return (torch.abs(s) + s) / torch.clamp(2.0 * s, min=EPSI)
+        # (|s| + s) / max(2 s, 1e-10) as a selection: the same values, and a gradient without
+        # the 1e10-scaled terms that cancel in the quotient form
+        return torch.where(s >= 0.5 * EPSI, torch.ones_like(s),
+                           torch.where(s > 0.0, 2.0 * s / EPSI, torch.zeros_like(s)))
     thl, thm = th(sl), th(sm)
     thr = 1.0 - th(sr)
     return (thr * fr + thl * fl + (1.0 - thl - thr) *
@@ -122,11 +138,14 @@ def hlld(vl, vr, gm):                                     # HLL_rot.f90:691-910,
     def vfast(v, b2):
         f1 = gm * v[4]
         f2 = 4.0 * f1 * (v[5] * v[5])
-        return torch.sqrt(((f1 + b2) + torch.sqrt(torch.clamp((f1 + b2) * (f1 + b2) - f2, min=0.0)))
-                          / (2.0 * v[0]))
-    vf = torch.maximum(vfast(vl, b2l), vfast(vr, b2r))
-    sl = torch.minimum(vl[1], vr[1]) - vf
-    sr = torch.maximum(vl[1], vr[1]) + vf
+        disc = (f1 + b2) * (f1 + b2) - f2
+        disc = torch.where(disc > 0.0, disc, torch.zeros_like(disc))
+        dd = torch.where(disc > 0.0, torch.sqrt(torch.where(disc > 0.0, disc, torch.ones_like(disc))),
+                         torch.zeros_like(disc))
+        return torch.sqrt(((f1 + b2) + dd) / (2.0 * v[0]))
+    vf = _max(vfast(vl, b2l), vfast(vr, b2r))
+    sl = _min(vl[1], vr[1]) - vf
+    sr = _max(vl[1], vr[1]) + vf
     f1 = 1.0 / (sr - sl)
     uh = f1 * (sr * ur - sl * ul - fr + fl)
     sm = uh[1] / uh[0]
@@ -194,25 +213,89 @@ PERM_M_Y = [0, 2, 1, 3, 4, 6, 5, 7]
 PERM_H_Y = [0, 2, 1, 3, 4]
 
 
-def flux_div(U, gm, ro_lim, pr_lim, dx, dy):
-    """-div F on the interior cells: (13, ny, nx) (set_flux + add_flux_rk, x then y)."""
+class Geom:
+    """Grid and boundary description of a run: ndim, margin, boundary codes (1 periodic,
+    2 reflecting, 10 outflow; Boundary_rot.f90:323-402 with set_sym_mhd/hd :239-320) and the
+    cell widths."""
+
+    def __init__(self, s):
+        self.ndim = s.ndim
+        self.flag_bnd = list(s.flag_bnd)
+        _, _, _, dx, dy, _ = s.coordinates()
+        self.dx = torch.from_numpy(dx)
+        self.dy = torch.from_numpy(dy)
+        self.gm, self.safety, self.ro_lim, self.pr_lim = s.gm, s.safety, s.ro_lim, s.pr_lim
+
+    def sl(self):
+        """Interior slice of a (13, jx, ix) array."""
+        return (slice(None), slice(M, -M) if self.ndim == 2 else slice(None), slice(M, -M))
+
+
+def _ghost_sources(code, n, upper):
+    """0-based source index of each ghost layer (lower: layers 0..M-1, upper: n-M..n-1)."""
+    if code == 1:
+        return [n - 2 * M + l for l in range(M)] if not upper else [M + l for l in range(M)]
+    if code == 2:
+        return [2 * M - 1 - l for l in range(M)] if not upper else [n - M - 1 - l for l in range(M)]
+    if code == 10:
+        return [M] * M if not upper else [n - M - 1] * M
+    raise ValueError("boundary code %d not covered" % code)
+
+
+def _sym(code, direction):
+    """Per-plane signs of the ghost copies (13 planes) for a face of the given direction."""
+    sg = [1.0] * 13
+    if code == 2:
+        sg[direction] = -1.0            # normal momentum (ions)
+        sg[4 + direction] = -1.0        # normal field
+        sg[NVM + direction] = -1.0      # normal momentum (neutrals)
+    return torch.tensor(sg, dtype=torch.float64)
+
+
+def fill(Ui, g):
+    """PIPbnd: ghost cells of the interior array Ui (13, ny, nx) -- x faces, then y faces
+    (whole rows, so corners take both copies)."""
+    n = Ui.shape[2] + 2 * M
+    U = torch.cat([Ui[:, :, :M], Ui, Ui[:, :, :M]], dim=2)      # placeholder ghost columns
+    lo = _ghost_sources(g.flag_bnd[0], n, False)
+    hi = _ghost_sources(g.flag_bnd[1], n, True)
+    U = torch.cat([_sym(g.flag_bnd[0], 1)[:, None, None] * U[:, :, lo],
+                   U[:, :, M:n - M],
+                   _sym(g.flag_bnd[1], 1)[:, None, None] * U[:, :, hi]], dim=2)
+    if g.ndim == 1:
+        return U
+    m = U.shape[1] + 2 * M
+    U = torch.cat([U[:, :M], U, U[:, :M]], dim=1)
+    lo = _ghost_sources(g.flag_bnd[2], m, False)
+    hi = _ghost_sources(g.flag_bnd[3], m, True)
+    return torch.cat([_sym(g.flag_bnd[2], 2)[:, None, None] * U[:, lo, :],
+                      U[:, M:m - M, :],
+                      _sym(g.flag_bnd[3], 2)[:, None, None] * U[:, hi, :]], dim=1)
+
+
+def fill_periodic(Ui):
+    """Ghost cells by periodic copy (flag_bnd = 1): x first, then y."""
+    U = torch.cat([Ui[:, :, -M:], Ui, Ui[:, :, :M]], dim=2)
+    return torch.cat([U[:, -M:, :], U, U[:, :M, :]], dim=1)
+
+
+def fluxes(U, g):
+    """x and y face fluxes adjacent to interior cells: Fx (13, ny, ix-3), Fy (13, jx-3, nx)."""
+    gm, ro_lim, pr_lim = g.gm, g.ro_lim, g.pr_lim
     Vm = u2v_mhd(U[:NVM], gm, ro_lim, pr_lim)
     Vh = u2v_hd(U[NVM:], gm, ro_lim, pr_lim)
-    # x faces on interior rows
-    Lm, Rm = face_states(Vm[:, M:-M, :], ro_lim)
-    Lh, Rh = face_states(Vh[:, M:-M, :], ro_lim)
-    Fx = torch.cat([hlld(Lm, Rm, gm), hllc(Lh, Rh, gm)], dim=0)       # faces 1 .. ix-3
-    # y faces on interior columns (variables permuted)
+    rows = slice(M, -M) if g.ndim == 2 else slice(None)
+    Lm, Rm = face_states(Vm[:, rows, :], ro_lim)
+    Lh, Rh = face_states(Vh[:, rows, :], ro_lim)
+    Fx = torch.cat([hlld(Lm, Rm, gm), hllc(Lh, Rh, gm)], dim=0)
+    if g.ndim == 1:
+        return Fx, None
     Vmy = Vm[PERM_M_Y][:, :, M:-M].transpose(1, 2)
     Vhy = Vh[PERM_H_Y][:, :, M:-M].transpose(1, 2)
     Lm, Rm = face_states(Vmy, ro_lim)
     Lh, Rh = face_states(Vhy, ro_lim)
-    Fym = hlld(Lm, Rm, gm)[PERM_M_Y]
-    Fyh = hllc(Lh, Rh, gm)[PERM_H_Y]
-    Fy = torch.cat([Fym, Fyh], dim=0).transpose(1, 2)                 # (13, faces 1..jx-3, nx)
-    dxi = dx[M:-M][None, None, :]
-    dyj = dy[M:-M][None, :, None]
-    return Fx, Fy, dxi, dyj
+    Fy = torch.cat([hlld(Lm, Rm, gm)[PERM_M_Y], hllc(Lh, Rh, gm)[PERM_H_Y]], dim=0).transpose(1, 2)
+    return Fx, Fy
 
 
 def cq2pv(u, gm, ro_lim, pr_lim, mhd):                    # Scheme_rot.f90:132-179
@@ -253,35 +336,35 @@ def source(Ui, gm, ac, ro_lim, pr_lim):
     return torch.cat([Sm, -ds], dim=0)
 
 
-def fill_periodic(Ui):
-    """Ghost cells by periodic copy (flag_bnd = 1): x first, then y."""
-    U = torch.cat([Ui[:, :, -M:], Ui, Ui[:, :, :M]], dim=2)
-    return torch.cat([U[:, -M:, :], U, U[:, :M, :]], dim=1)
-
-
-def stage(Us, U0, dt_sub, gm, ac, ro_lim, pr_lim, dx, dy):
-    Fx, Fy, dxi, dyj = flux_div(Us, gm, ro_lim, pr_lim, dx, dy)
-    S = source(Us[:, M:-M, M:-M], gm, ac, ro_lim, pr_lim)
-    u0 = U0[:, M:-M, M:-M]
-    u = u0 - (dt_sub / dxi) * (Fx[:, :, 1:] - Fx[:, :, :-1])
-    u = u - (dt_sub / dyj) * (Fy[:, 1:, :] - Fy[:, :-1, :])
+def stage(Us, U0, dt_sub, ac, g):
+    """One RK stage (add_flux_rk x then y, add_source) and the ghost fill."""
+    Fx, Fy = fluxes(Us, g)
+    sl = g.sl()
+    S = source(Us[sl], g.gm, ac, g.ro_lim, g.pr_lim)
+    u = U0[sl] - (dt_sub / g.dx[M:-M][None, None, :]) * (Fx[:, :, 1:] - Fx[:, :, :-1])
+    if g.ndim == 2:
+        u = u - (dt_sub / g.dy[M:-M][None, :, None]) * (Fy[:, 1:, :] - Fy[:, :-1, :])
     u = u + S * dt_sub
-    return fill_periodic(u)
+    return fill(u, g)
 
 
-def rewrite(U, gm, ro_lim, pr_lim):
-    um, qm = cq2pv(U[:NVM], gm, ro_lim, pr_lim, True)
-    uh, qh = cq2pv(U[NVM:], gm, ro_lim, pr_lim, False)
+def rewrite(U, g):
+    um, qm = cq2pv(U[:NVM], g.gm, g.ro_lim, g.pr_lim, True)
+    uh, qh = cq2pv(U[NVM:], g.gm, g.ro_lim, g.pr_lim, False)
     return torch.cat([um, uh], dim=0), qm, qh
 
 
-def cfl_dt(U, gm, safety, ac, ro_lim, pr_lim, dx, dy):
+def cfl_dt(U, ac, g):
     """cfl (Scheme_rot.f90:183-213) for a state; returns (rewritten state, dt)."""
-    W, qm, qh = rewrite(U, gm, ro_lim, pr_lim)
-    sl = (slice(M, -M), slice(M, -M))
+    W, qm, qh = rewrite(U, g)
+    sl = g.sl()[1:]
+    gm, safety = g.gm, g.safety
     de, vx, vy, vz, pr = [q[sl] for q in qm]
     bx, by, bz = [W[n][sl] for n in (5, 6, 7)]
-    gmin = torch.minimum(dx[M:-M][None, :], dy[M:-M][:, None])
+    if g.ndim == 2:
+        gmin = torch.minimum(g.dx[M:-M][None, :], g.dy[M:-M][:, None])
+    else:
+        gmin = torch.minimum(g.dx[M:-M], g.dy[0:1])[None, :]
     dm = torch.clamp(de, min=TINY)
     cs2 = gm * pr / dm
     valf2 = (bx * bx + by * by + bz * bz) / dm
@@ -291,25 +374,26 @@ def cfl_dt(U, gm, safety, ac, ro_lim, pr_lim, dx, dy):
     cs = torch.sqrt(gm * npr / nde)
     nvabs = torch.sqrt(torch.clamp(nvx * nvx + nvy * nvy + nvz * nvz, min=TINY))
     cand_h = safety * gmin / (nvabs + cs)
-    dt = torch.minimum(cand_m, cand_h).min()
-    rho = torch.maximum(W[0][sl] * ac, W[NVM][sl] * ac).max()
-    dt = torch.minimum(dt, min(safety, 0.3) / rho)
+    cand = _min(cand_m, cand_h).reshape(-1)
+    dt = cand[torch.argmin(cand)]                       # the first cell on a tie
+    rcell = _max(W[0][sl] * ac, W[NVM][sl] * ac).reshape(-1)
+    rho = rcell[torch.argmax(rcell)]
+    dtc = min(safety, 0.3) / rho
+    dt = torch.where(dtc < dt, dtc, dt)
     return W, dt
 
 
-def run(U0, ac, nsteps, gm, safety, ro_lim, pr_lim, dx, dy):
-    """nsteps steps of the time loop from U0 (13, jx, ix), periodic; returns the final state
-    (after the last cfl rewrite) and the list of dt."""
-    U = U0
+def run(U0, ac, nsteps, g):
+    """nsteps steps of the time loop from U0 (13, jx, ix); returns the final state (after the
+    last cfl rewrite) and the list of dt."""
     dts = []
-    W, dt = cfl_dt(U, gm, safety, ac, ro_lim, pr_lim, dx, dy)
+    W, dt = cfl_dt(U0, ac, g)
     for n in range(nsteps):
-        U0s = W
-        U1 = stage(U0s, U0s, dt / 2.0, gm, ac, ro_lim, pr_lim, dx, dy)
-        U2 = stage(U1, U0s, dt / 1.0, gm, ac, ro_lim, pr_lim, dx, dy)
+        U1 = stage(W, W, dt / 2.0, ac, g)
+        U2 = stage(U1, W, dt / 1.0, ac, g)
         dts.append(dt)
-        W1, _, _ = rewrite(U2, gm, ro_lim, pr_lim)         # cfl after run_solver
+        W1, _, _ = rewrite(U2, g)                      # cfl after run_solver
         if n + 1 == nsteps:
             return W1, dts
-        W, dt = cfl_dt(W1, gm, safety, ac, ro_lim, pr_lim, dx, dy)   # cfl of the next step
+        W, dt = cfl_dt(W1, ac, g)                      # cfl of the next step
     return W, dts
