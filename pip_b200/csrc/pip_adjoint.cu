@@ -8,9 +8,9 @@
 // with G(U) = -div F(MUSCL-minmod(u2v(U))) + S(cq2pv(U)) on interior cells and fill() the
 // ghost copy of Boundary_rot.f90.  The reverse sweep of a step, for a cotangent La of z_n+1:
 //   fold(La)                                    ghost cotangents -> their interior sources
-//   Lb   = (dt_n G'(U1))^T La                   stage_vjp_kernel, stage 2
+//   Lb   = (dt_n G'(U1))^T La                   reverse stage 2 (faces, then cells)
 //   fold(Lb)
-//   La   = La + Lb + (dt_n/2 G'(z_n))^T Lb      stage_vjp_kernel, stage 1, in place
+//   La   = La + Lb + (dt_n/2 G'(z_n))^T Lb      reverse stage 1, in place
 //   La  += (dL/ddt_n) dCFL/dz_n, dL/dalpha_c   finalize_kernel
 // where dL/ddt_n = (<La, G(U1)> + <Lb, G(z_n)>/2) is accumulated by the two stage kernels
 // from face fluxes and cell sources, and the CFL derivative is taken at the cell (or the
@@ -34,27 +34,9 @@ namespace adjk {
 
 constexpr int NVM = 8, NV = 13;
 
-template <int NDIM> struct VT;
-template <> struct VT<2> {
-  static constexpr int TX = 32, TY = 8, NT = 256;
-};
-template <> struct VT<1> {
-  static constexpr int TX = 256, TY = 1, NT = 256;
-};
-
-// Output tile TX x TY cells; primitives on the tile plus 3 cells along each axis (the
-// 4-cell MUSCL stencils of the faces within 2 cells of the tile); faces k+1/2 for
-// k = i0-2 .. i0+TX (x) and the same along y.
-template <int NDIM> struct Geo {
-  static constexpr int TX = VT<NDIM>::TX, TY = VT<NDIM>::TY, NT = VT<NDIM>::NT;
-  static constexpr int HV = 3;
-  static constexpr int RX = TX + 2 * HV, RY = NDIM == 2 ? TY + 2 * HV : 1, RR = RX * RY;
-  static constexpr int NFX = (TX + 3) * TY;
-  static constexpr int NFY = NDIM == 2 ? TX * (TY + 3) : 0;
-  static constexpr int NF = NFX + NFY;
-  static constexpr size_t smem =
-      sizeof(double) * ((size_t)NV * RR + 2ull * NV * NF) + sizeof(unsigned long long) * NF;
-};
+// Thread-block sizes of the reverse-stage kernels.
+constexpr int kFaceThreads = 128;   // one face per thread, register bound (255 per thread)
+constexpr int kCellThreads = 256;
 
 // Per-block CFL candidates of stage 1 (the state z_n).
 struct CandPart {
@@ -88,10 +70,11 @@ __device__ __forceinline__ double dmm(int mode, int q) {
 // Riemann solvers.  lamF: cotangent of the face flux (natural variable order).  Writes the
 // cotangents of the two face states (gL, gR, natural order, after the floors), the minmod
 // branches and returns <F, lamF>.
-template <int RR>
-__device__ __forceinline__ double face_vjp(const KParams &p, const double *sV, int a, int s, bool ydir,
+__device__ __forceinline__ double face_vjp(const KParams &p, const double *__restrict__ V,
+                                           long long a, long long s, bool ydir,
                                            const double (&lamF)[NV], double *gL, double *gR,
-                                           int nf, int f, unsigned long long &modes) {
+                                           long long nf, long long f, unsigned long long &modes) {
+  const long long RR = p.nc;  // plane stride of the primitives
   double fdot = 0.0;
   modes = 0ull;
   {
@@ -99,7 +82,7 @@ __device__ __forceinline__ double face_vjp(const KParams &p, const double *sV, i
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
       const int src = ydir ? perm_m(n) : n;
-      const double *v = sV + src * RR + a;
+      const double *v = V + src * RR + a;
       const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
       const int mL = adj::minmod_mode(v0, v1, v2), mR = adj::minmod_mode(v1, v2, v3);
       modes |= (unsigned long long)(mL | (mR << 2)) << (4 * src);
@@ -128,7 +111,7 @@ __device__ __forceinline__ double face_vjp(const KParams &p, const double *sV, i
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       const int src = ydir ? perm_h(n) : n;
-      const double *v = sV + (NVM + src) * RR + a;
+      const double *v = V + (NVM + src) * RR + a;
       const double v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
       const int mL = adj::minmod_mode(v0, v1, v2), mR = adj::minmod_mode(v1, v2, v3);
       modes |= (unsigned long long)(mL | (mR << 2)) << (4 * (NVM + src));
@@ -155,158 +138,162 @@ __device__ __forceinline__ double face_vjp(const KParams &p, const double *sV, i
   return fdot;
 }
 
-// Adds the contributions of the four faces k = c-2 .. c+1 (local indices f0 .. f0+3*df) of
-// one direction to the primitive cotangents of cell c.
-__device__ __forceinline__ void gather_dir(const double *gL, const double *gR,
-                                           const unsigned long long *sM, int nf, int f0, int df,
+// Adds the contributions of the faces k = c-2 .. c+1 of one direction (face k between
+// cells k and k+1; face data at index base + k*df, only faces 0 <= k < kmax exist) to the
+// primitive cotangents of cell c.
+__device__ __forceinline__ void gather_dir(const double *__restrict__ gL, const double *__restrict__ gR,
+                                           const unsigned long long *__restrict__ M, long long nf,
+                                           long long base, long long df, int c, int kmax,
                                            double (&av)[NV]) {
-  const int fa = f0, fb = f0 + df, fc = f0 + 2 * df, fd = f0 + 3 * df;  // k = c-2, c-1, c, c+1
-  const unsigned long long ma = sM[fa], mb = sM[fb], mc = sM[fc], md = sM[fd];
 #pragma unroll
-  for (int n = 0; n < NV; ++n) {
-    const int sh = 4 * n;
-    // face k = c-2: cell c is k+2 (third cell of the right stencil)
-    const double gRa = gR[n * nf + fa];
-    double acc = -0.5 * gRa * dmm((int)((ma >> (sh + 2)) & 3ull), 2);
-    // face k = c-1: cell c is k+1 (right cell)
-    const double gLb = gL[n * nf + fb], gRb = gR[n * nf + fb];
-    acc += gRb + 0.5 * gLb * dmm((int)((mb >> sh) & 3ull), 2) -
-           0.5 * gRb * dmm((int)((mb >> (sh + 2)) & 3ull), 1);
-    // face k = c: cell c is k (left cell)
-    const double gLc = gL[n * nf + fc], gRc = gR[n * nf + fc];
-    acc += gLc + 0.5 * gLc * dmm((int)((mc >> sh) & 3ull), 1) -
-           0.5 * gRc * dmm((int)((mc >> (sh + 2)) & 3ull), 0);
-    // face k = c+1: cell c is k-1 (first cell of the left stencil)
-    const double gLd = gL[n * nf + fd];
-    acc += 0.5 * gLd * dmm((int)((md >> sh) & 3ull), 0);
-    av[n] += acc;
+  for (int r = 0; r < 4; ++r) {
+    const int k = c - 2 + r;
+    if (k < 0 || k >= kmax) continue;
+    const long long f = base + (long long)k * df;
+    const unsigned long long m = M[f];
+    if (m == 0ull && r != 1 && r != 2) continue;   // slope terms only: nothing to add
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      const int sh = 4 * n;
+      const int mL = (int)((m >> sh) & 3ull), mR = (int)((m >> (sh + 2)) & 3ull);
+      const double l = gL[n * nf + f], rr = gR[n * nf + f];
+      double add;
+      if (r == 0)        // cell c is k+2: third cell of the right stencil
+        add = -0.5 * rr * dmm(mR, 2);
+      else if (r == 1)   // cell c is k+1: right cell
+        add = rr + 0.5 * l * dmm(mL, 2) - 0.5 * rr * dmm(mR, 1);
+      else if (r == 2)   // cell c is k: left cell
+        add = l + 0.5 * l * dmm(mL, 1) - 0.5 * rr * dmm(mR, 0);
+      else               // cell c is k-1: first cell of the left stencil
+        add = 0.5 * l * dmm(mL, 0);
+      av[n] += add;
+    }
   }
 }
 
-// Reverse of one RK stage over a tile of the whole (ghosted) array.  Us: stage input
-// state; lam: cotangent of the stage output (interior cells); out: cotangent of Us (every
-// cell), plus acc + lam at interior cells when acc is given (stage 1: the U0 terms).
-template <int NDIM>
-__global__ void __launch_bounds__(VT<NDIM>::NT, 1)
-stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *__restrict__ lam,
-                 const double *acc, double *out, const double *dtp, double fac,
-                 double *part_dot, double *part_dac, CandPart *cand) {
-  using G = Geo<NDIM>;
-  constexpr int TX = G::TX, TY = G::TY, NT = G::NT, HV = G::HV, RX = G::RX, RR = G::RR;
-  constexpr int NFX = G::NFX, NF = G::NF;
-  extern __shared__ double smem[];
-  double *sV = smem;
-  double *gL = sV + NV * RR;
-  double *gR = gL + NV * NF;
-  unsigned long long *sM = reinterpret_cast<unsigned long long *>(gR + NV * NF);
-  __shared__ double s_red[4][NT / 32];
-  __shared__ long long s_idx[2][NT / 32];
-  __shared__ int s_kind[2][NT / 32];
-
-  const int tid = threadIdx.x;
-  const double dt_sub = fac * (*dtp);
+// Primitives of every cell (u2v_mhd / u2v_hd, HLL_rot.f90:1136-1186).
+__global__ void u2v_kernel(const KParams p, const double *__restrict__ U, double *__restrict__ V) {
   const long long nc = p.nc;
-  const int i0 = blockIdx.x * TX, j0 = NDIM == 2 ? blockIdx.y * TY : 0;
-
-  // ---- 1. primitives of the tile and its stencil reach
-  for (int idx = tid; idx < RR; idx += NT) {
-    const int ri = idx % RX, rj = idx / RX;
-    const bool ox = ri < HV || ri >= TX + HV, oy = NDIM == 2 && (rj < HV || rj >= TY + HV);
-    if (ox && oy) continue;
-    const int gi = i0 - HV + ri, gj = NDIM == 2 ? j0 - HV + rj : 0;
-    if (gi < 0 || gi >= p.ix || gj < 0 || gj >= p.jx) {
-#pragma unroll
-      for (int n = 0; n < NV; ++n) sV[n * RR + idx] = 0.0;
-      continue;
-    }
-    const long long q = (long long)gj * p.ix + gi;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc;
+       q += (long long)gridDim.x * blockDim.x) {
     double um[8], uh[5], vm[8], vh[5];
 #pragma unroll
-    for (int n = 0; n < 8; ++n) um[n] = Us[q + n * nc];
+    for (int n = 0; n < 8; ++n) um[n] = U[q + n * nc];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) uh[n] = Us[q + (NVM + n) * nc];
+    for (int n = 0; n < 5; ++n) uh[n] = U[q + (NVM + n) * nc];
     u2v_mhd<double, 8>(um, vm, p.gm, p.ro_lim, p.pr_lim);
     u2v_hd<double>(uh, vh, p.gm, p.ro_lim, p.pr_lim);
 #pragma unroll
-    for (int n = 0; n < 8; ++n) sV[n * RR + idx] = vm[n];
+    for (int n = 0; n < 8; ++n) V[q + n * nc] = vm[n];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+    for (int n = 0; n < 5; ++n) V[q + (NVM + n) * nc] = vh[n];
   }
-  __syncthreads();
+}
 
-  // ---- 2. faces
+// Reverse of the face fluxes of one RK stage: one thread per face.  x faces (j, i) lie
+// between cells (j, i) and (j, i+1), y faces (j, i) between (j, i) and (j+1, i); a face is
+// stored at the index j*ix + i of its lower cell.  For faces next to an interior cell: the
+// flux cotangent from the cotangent lam of the stage output, the reverse of the MUSCL face
+// states and the Riemann solver (face_vjp), written as (gL, gR, minmod branches); other
+// faces are written as zero.  Per block: sum of <F, lamF> (the flux part of dt_sub
+// <lam, dU/d(dt_sub)>).
+__global__ void __launch_bounds__(kFaceThreads)
+face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__restrict__ lam,
+                const double *dtp, double fac, double *gx, unsigned long long *mx, double *gy,
+                unsigned long long *my, double *part_dot, double *part_dac) {
+  __shared__ double s_red[kFaceThreads / 32];
+  const long long nc = p.nc;
+  const double dt_sub = fac * (*dtp);
+  const long long nfx = (long long)p.jx * (p.ix - 1);
+  const long long nfy = p.ndim == 2 ? (long long)(p.jx - 1) * p.ix : 0;
   double dot = 0.0;
-  for (int f = tid; f < NF; f += NT) {
-    int ca_i, ca_j, cb_i, cb_j, a, s;
-    bool ydir, owned;
-    if (f < NFX) {
-      const int fl = f % (TX + 3), fj = f / (TX + 3);
-      ca_i = i0 - 2 + fl;
-      ca_j = j0 + fj;
-      cb_i = ca_i + 1;
-      cb_j = ca_j;
-      a = (NDIM == 2 ? (fj + HV) * RX : 0) + fl - 2 + HV;
-      s = 1;
-      ydir = false;
-      owned = fl >= 2 && fl < TX + 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < nfx + nfy) {
+    const bool ydir = t >= nfx;
+    int ia, ja, ib, jb;
+    if (!ydir) {
+      ja = (int)(t / (p.ix - 1));
+      ia = (int)(t % (p.ix - 1));
+      ib = ia + 1;
+      jb = ja;
     } else {
-      const int g = f - NFX, fi = g % TX, fk = g / TX;
-      ca_i = i0 + fi;
-      ca_j = j0 - 2 + fk;
-      cb_i = ca_i;
-      cb_j = ca_j + 1;
-      a = (fk - 2 + HV) * RX + fi + HV;
-      s = RX;
-      ydir = true;
-      owned = fk >= 2 && fk < TY + 2;
+      const long long u = t - nfx;
+      ja = (int)(u / p.ix);
+      ia = (int)(u % p.ix);
+      ib = ia;
+      jb = ja + 1;
     }
-    const bool in_a = interior(p, ca_i, ca_j), in_b = interior(p, cb_i, cb_j);
+    const long long qa = (long long)ja * p.ix + ia, qb = (long long)jb * p.ix + ib;
+    double *g = ydir ? gy : gx;
+    unsigned long long *mm = ydir ? my : mx;
+    const bool in_a = interior(p, ia, ja), in_b = interior(p, ib, jb);
     if (!in_a && !in_b) {
 #pragma unroll
-      for (int n = 0; n < NV; ++n) {
-        gL[n * NF + f] = 0.0;
-        gR[n * NF + f] = 0.0;
-      }
-      sM[f] = 0ull;
-      continue;
-    }
-    double ca = 0.0, cb = 0.0;
-    if (!ydir) {
-      if (in_a) ca = dt_sub / p.dx[ca_i];
-      if (in_b) cb = dt_sub / p.dx[cb_i];
+      for (int n = 0; n < 2 * NV; ++n) g[n * nc + qa] = 0.0;
+      mm[qa] = 0ull;
     } else {
-      if (in_a) ca = dt_sub / p.dy[ca_j];
-      if (in_b) cb = dt_sub / p.dy[cb_j];
-    }
-    const long long qa = (long long)ca_j * p.ix + ca_i, qb = (long long)cb_j * p.ix + cb_i;
-    double lamF[NV];
+      double ca = 0.0, cb = 0.0;
+      if (!ydir) {
+        if (in_a) ca = dt_sub / p.dx[ia];
+        if (in_b) cb = dt_sub / p.dx[ib];
+      } else {
+        if (in_a) ca = dt_sub / p.dy[ja];
+        if (in_b) cb = dt_sub / p.dy[jb];
+      }
+      double lamF[NV];
 #pragma unroll
-    for (int n = 0; n < NV; ++n) {
-      const double la = in_a ? lam[qa + n * nc] : 0.0;
-      const double lb = in_b ? lam[qb + n * nc] : 0.0;
-      lamF[n] = -ca * la + cb * lb;
+      for (int n = 0; n < NV; ++n) {
+        const double la = in_a ? lam[qa + n * nc] : 0.0;
+        const double lb = in_b ? lam[qb + n * nc] : 0.0;
+        lamF[n] = -ca * la + cb * lb;
+      }
+      unsigned long long m;
+      dot = face_vjp(p, V, qa, ydir ? (long long)p.ix : 1ll, ydir, lamF, g, g + NV * nc, nc, qa, m);
+      mm[qa] = m;
     }
-    unsigned long long m;
-    const double fd = face_vjp<RR>(p, sV, a, s, ydir, lamF, gL, gR, NF, f, m);
-    sM[f] = m;
-    if (owned) dot += fd;
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+  if (threadIdx.x % 32 == 0) s_red[threadIdx.x / 32] = dot;
   __syncthreads();
+  if (threadIdx.x == 0) {
+    double sd = 0.0;
+    for (int k = 0; k < kFaceThreads / 32; ++k) sd += s_red[k];
+    part_dot[blockIdx.x] = sd;
+    part_dac[blockIdx.x] = 0.0;
+  }
+}
 
-  // ---- 3. cells: gather, u2v, source, output
-  const int ti = tid % TX, tj = tid / TX;
-  const int gi = i0 + ti, gj = j0 + tj;
-  double dac = 0.0;
+// Reverse of one RK stage per cell (every cell of the ghosted array): the face-state
+// cotangents of the faces whose MUSCL stencils reach the cell (face_vjp_kernel's output)
+// through minmod, u2v, the explicit collision source (interior cells), the U0 terms
+// acc + lam of stage 1 (interior cells, when acc is given), and for stage 1 the CFL
+// candidates of the cell (cand).  Per block: dt_sub <lam, S>, dS/dalpha_c . lam.
+__global__ void __launch_bounds__(kCellThreads)
+cell_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *__restrict__ lam,
+                const double *acc, double *out, const double *dtp, double fac,
+                const double *__restrict__ gx, const unsigned long long *__restrict__ mx,
+                const double *__restrict__ gy, const unsigned long long *__restrict__ my,
+                double *part_dot, double *part_dac, CandPart *cand) {
+  constexpr int NT = kCellThreads;
+  __shared__ double s_red[4][NT / 32];
+  __shared__ long long s_idx[2][NT / 32];
+  __shared__ int s_kind[2][NT / 32];
+  const int tid = threadIdx.x;
+  const double dt_sub = fac * (*dtp);
+  const long long nc = p.nc;
+  double dot = 0.0, dac = 0.0;
   double cmin = 1.0e300, rmax = -1.0e300;
   long long cidx = -1, ridx = -1;
   int ckind = 0, rsp = 0;
-  if (tj < TY && gi < p.ix && gj < p.jx) {
-    const long long q = (long long)gj * p.ix + gi;
+  const long long q = blockIdx.x * (long long)NT + tid;
+  if (q < nc) {
+    const int gi = (int)(q % p.ix), gj = (int)(q / p.ix);
     double av[NV];
 #pragma unroll
     for (int n = 0; n < NV; ++n) av[n] = 0.0;
-    gather_dir(gL, gR, sM, NF, tj * (TX + 3) + ti, 1, av);
-    if (NDIM == 2) gather_dir(gL, gR, sM, NF, NFX + tj * TX + ti, TX, av);
+    gather_dir(gx, gx + NV * nc, mx, nc, (long long)gj * p.ix, 1, gi, p.ix - 1, av);
+    if (p.ndim == 2) gather_dir(gy, gy + NV * nc, my, nc, gi, p.ix, gj, p.jx - 1, av);
     double um[8], uh[5];
 #pragma unroll
     for (int n = 0; n < 8; ++n) um[n] = Us[q + n * nc];
@@ -322,8 +309,7 @@ stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *_
       adj::u2v_mhd_vjp(um, avm, p.gm, p.ro_lim, p.pr_lim, aum);
       adj::u2v_hd_vjp(uh, avh, p.gm, p.ro_lim, p.pr_lim, auh);
     }
-    const bool in = interior(p, gi, gj);
-    if (in) {
+    if (interior(p, gi, gj)) {
       double lm[NV];
 #pragma unroll
       for (int n = 0; n < NV; ++n) lm[n] = lam[q + n * nc];
@@ -348,7 +334,7 @@ stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *_
         for (int n = 0; n < 5; ++n) wh[n] = uh[n];
         const Prim<double> qm = cq2pv_mhd_rcp<double, 8>(wm, p.gm, p.igm1, p.ro_lim, p.pr_lim);
         const Prim<double> qh = cq2pv_hd_rcp<double>(wh, p.gm, p.igm1, p.ro_lim, p.pr_lim);
-        const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+        const double gmin = fmin(fmin(p.dx[gi], p.ndim == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
         const double sg = p.safety * gmin;
         const double cm = cfl_mhd_cell<double>(qm, wm[5], wm[6], wm[7], p.gm, sg);
         const double ch = cfl_hd_cell<double>(qh, p.gm, sg);
@@ -367,7 +353,7 @@ stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *_
     for (int n = 0; n < 5; ++n) out[q + (NVM + n) * nc] = auh[n];
   }
 
-  // ---- 4. block reductions (fixed order: deterministic)
+  // block reductions (fixed order: deterministic)
   const int w = tid / 32, l = tid % 32;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -404,14 +390,13 @@ stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *_
   }
   __syncthreads();
   if (tid == 0) {
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
     double sd = 0.0, sa = 0.0;
     for (int k = 0; k < NT / 32; ++k) {
       sd += s_red[0][k];
       sa += s_red[1][k];
     }
-    part_dot[bid] = sd;
-    part_dac[bid] = sa;
+    part_dot[blockIdx.x] = sd;
+    part_dac[blockIdx.x] = sa;
     if (cand) {
       CandPart c;
       c.cmin = 1.0e300;
@@ -434,23 +419,18 @@ stage_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *_
           c.rsp = s_kind[1][k];
         }
       }
-      cand[bid] = c;
+      cand[blockIdx.x] = c;
     }
   }
 }
 
 // Adjoint of the ghost fill (Boundary_rot.f90:54-125 as done by the stage kernels' ghost
-// writes): each interior cell within 2*margin of a boundary gathers the cotangents of the
-// ghost cells copied from it (x ghosts, y ghosts and corners, with their sign tables).
-// Ghost entries are left as they are; consumers read interior cells only.
-__global__ void fold_kernel(const KParams p, double *lam) {
-  const long long nint = (long long)p.nx * p.ny;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nint;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int gi = p.m0 + (int)(t % p.nx), gj = (p.ndim == 2 ? p.m1 : 0) + (int)(t / p.nx);
-    const bool nb = gi < 2 * p.m0 || gi >= p.ix - 2 * p.m0 ||
-                    (p.ndim == 2 && (gj < 2 * p.m1 || gj >= p.jx - 2 * p.m1));
-    if (!nb) continue;
+// writes): each interior cell within 2*margin of a boundary (the list `cells`) gathers the
+// cotangents of the ghost cells copied from it (x ghosts, y ghosts and corners, with their
+// sign tables).  Ghost entries are left as they are; consumers read interior cells only.
+__global__ void fold_kernel(const KParams p, double *lam, const int *cells, int ncells) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncells; t += gridDim.x * blockDim.x) {
+    const int gi = cells[t] % p.ix, gj = cells[t] / p.ix;
     int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
     int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
     for (int s = 0; s < 2; ++s)
@@ -486,7 +466,7 @@ __global__ void fold_kernel(const KParams p, double *lam) {
 
 // One block: dL/ddt_n from the stage partials, the CFL bound that set dt_n and its
 // gradient (added to lamz at that cell), dL/dalpha_c accumulated into *dcol.
-__global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb,
+__global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb, int ncand,
                                                        const double *p1dot, const double *p1dac,
                                                        const double *p2dot, const double *p2dac,
                                                        const CandPart *cand, const double *dtp,
@@ -502,6 +482,8 @@ __global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb,
   for (int b = t; b < nb; b += 256) {
     sd += p1dot[b] + p2dot[b];
     sa += p1dac[b] + p2dac[b];
+  }
+  for (int b = t; b < ncand; b += 256) {
     const CandPart c = cand[b];
     if (c.cidx >= 0 && (c.cmin < cm || (c.cmin == cm && (ci < 0 || c.cidx < ci)))) {
       cm = c.cmin;
@@ -577,28 +559,29 @@ __global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb,
   if (ldt_out) *ldt_out = ldt;
 }
 
-template <int NDIM>
+// One reverse stage: primitives of Us, faces, cells.  Partial sums: face blocks first (nbf),
+// then cell blocks.
 cudaError_t launch_stage_vjp(const KParams &p, const double *Us, const double *lam, const double *acc,
-                             double *out, const double *dtp, double fac, double *pdot, double *pdac,
-                             CandPart *cand, cudaStream_t s) {
-  using G = Geo<NDIM>;
-  dim3 grid((p.ix + G::TX - 1) / G::TX, NDIM == 2 ? (p.jx + G::TY - 1) / G::TY : 1);
-  stage_vjp_kernel<NDIM><<<grid, G::NT, G::smem, s>>>(p, Us, lam, acc, out, dtp, fac, pdot, pdac, cand);
+                             double *out, const double *dtp, double fac, double *V, double *gx,
+                             unsigned long long *mx, double *gy, unsigned long long *my,
+                             double *pdot, double *pdac, int nbf, CandPart *cand, cudaStream_t s) {
+  const long long nc = p.nc;
+  const int gu = (int)std::min<long long>((nc + 255) / 256, 148 * 8);
+  u2v_kernel<<<gu, 256, 0, s>>>(p, Us, V);
+  face_vjp_kernel<<<nbf, kFaceThreads, 0, s>>>(p, V, lam, dtp, fac, gx, mx, gy, my, pdot, pdac);
+  const int nbc = (int)((nc + kCellThreads - 1) / kCellThreads);
+  cell_vjp_kernel<<<nbc, kCellThreads, 0, s>>>(p, Us, lam, acc, out, dtp, fac, gx, mx, gy, my,
+                                               pdot + nbf, pdac + nbf, cand);
   return cudaGetLastError();
 }
 
-int vjp_blocks(const KParams &p) {
-  if (p.ndim == 2) return ((p.ix + Geo<2>::TX - 1) / Geo<2>::TX) * ((p.jx + Geo<2>::TY - 1) / Geo<2>::TY);
-  return (p.ix + Geo<1>::TX - 1) / Geo<1>::TX;
+int face_blocks(const KParams &p) {
+  const long long nf = (long long)p.jx * (p.ix - 1) + (p.ndim == 2 ? (long long)(p.jx - 1) * p.ix : 0);
+  return (int)((nf + kFaceThreads - 1) / kFaceThreads);
 }
+int cell_blocks(const KParams &p) { return (int)((p.nc + kCellThreads - 1) / kCellThreads); }
 
-cudaError_t prepare() {
-  cudaError_t e = cudaFuncSetAttribute(stage_vjp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)Geo<2>::smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_vjp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)Geo<1>::smem);
-}
+cudaError_t prepare() { return cudaSuccess; }
 
 }  // namespace adjk
 }  // namespace pip
@@ -628,6 +611,12 @@ struct pip_adj {
   CandPart *cand = nullptr;
   double *dcol = nullptr;
   double *d_dt = nullptr;         // dt of the unit-level stage VJP
+  double *V = nullptr;            // primitives of the stage state
+  double *gx = nullptr, *gy = nullptr;            // face-state cotangents (2*13 planes)
+  unsigned long long *mx = nullptr, *my = nullptr; // minmod branches per face
+  int nbf = 0, nbc = 0;
+  int *d_fold = nullptr;          // interior cells within 2*margin of a boundary
+  int nfold = 0;
   DevCtrl *ctrl = nullptr;
   DevCtrl *h_ctrl = nullptr;
   int nb = 0;
@@ -645,11 +634,18 @@ struct pip_adj {
 
 namespace {
 
-int grid_fold(const KParams &k) {
-  long long n = (long long)k.nx * k.ny;
-  long long b = (n + 255) / 256;
-  if (b > 148 * 8) b = 148 * 8;
-  return (int)std::max(1ll, b);
+int grid_fold(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 4)); }
+
+// Interior cells that can be the source of a ghost copy (within 2*margin of a boundary).
+std::vector<int> fold_cells(const KParams &k) {
+  std::vector<int> c;
+  const int j0 = k.ndim == 2 ? k.m1 : 0, j1 = k.ndim == 2 ? k.m1 + k.ny : 1;
+  for (int j = j0; j < j1; ++j)
+    for (int i = k.m0; i < k.m0 + k.nx; ++i)
+      if (i < 2 * k.m0 || i >= k.ix - 2 * k.m0 ||
+          (k.ndim == 2 && (j < 2 * k.m1 || j >= k.jx - 2 * k.m1)))
+        c.push_back(j * k.ix + i);
+  return c;
 }
 
 cudaError_t launch_vjp(pip_adj *a, int stage, const double *Us, const double *lam, const double *acc,
@@ -658,9 +654,8 @@ cudaError_t launch_vjp(pip_adj *a, int stage, const double *Us, const double *la
   double *pd = stage == 1 ? a->p1dot : a->p2dot;
   double *pa = stage == 1 ? a->p1dac : a->p2dac;
   CandPart *c = stage == 1 ? a->cand : nullptr;
-  if (a->kp.ndim == 2)
-    return pip::adjk::launch_stage_vjp<2>(a->kp, Us, lam, acc, out, dtp, fac, pd, pa, c, a->stream);
-  return pip::adjk::launch_stage_vjp<1>(a->kp, Us, lam, acc, out, dtp, fac, pd, pa, c, a->stream);
+  return pip::adjk::launch_stage_vjp(a->kp, Us, lam, acc, out, dtp, fac, a->V, a->gx, a->mx, a->gy,
+                                     a->my, pd, pa, a->nbf, c, a->stream);
 }
 
 void reset_slot(DevCtrl &h, int slot) {
@@ -731,12 +726,30 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
     return fail(e);
   a->kp.dx = a->d_dx;
   a->kp.dy = a->d_dy;
-  a->nb = pip::adjk::vjp_blocks(a->kp);
+  a->nbf = pip::adjk::face_blocks(a->kp);
+  a->nbc = pip::adjk::cell_blocks(a->kp);
+  a->nb = a->nbf + a->nbc;
+  if ((e = cudaMalloc(&a->V, sb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->gx, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->gy, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->mx, sizeof(unsigned long long) * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->my, sizeof(unsigned long long) * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(a->gy, 0, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(a->my, 0, sizeof(unsigned long long) * (size_t)k.nc)) != cudaSuccess) return fail(e);
+  {
+    const std::vector<int> fc = fold_cells(a->kp);
+    a->nfold = (int)fc.size();
+    if ((e = cudaMalloc(&a->d_fold, sizeof(int) * std::max<size_t>(1, fc.size()))) != cudaSuccess)
+      return fail(e);
+    if (!fc.empty() && (e = cudaMemcpy(a->d_fold, fc.data(), sizeof(int) * fc.size(),
+                                       cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(e);
+  }
   if ((e = cudaMalloc(&a->p1dot, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->p1dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->p2dot, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->p2dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&a->cand, sizeof(CandPart) * a->nb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&a->cand, sizeof(CandPart) * a->nbc)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->dcol, sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->ctrl, sizeof(DevCtrl))) != cudaSuccess) return fail(e);
@@ -751,7 +764,7 @@ void pip_adj_destroy(pip_adj *a) {
   cudaSetDevice(a->device);
   if (a->stream) cudaStreamSynchronize(a->stream);
   double *bufs[] = {a->A, a->B, a->La, a->Lb, a->dt_hist, a->d_dx, a->d_dy,
-                    a->p1dot, a->p1dac, a->p2dot, a->p2dac, a->dcol, a->d_dt};
+                    a->p1dot, a->p1dac, a->p2dot, a->p2dac, a->dcol, a->d_dt, a->V, a->gx, a->gy};
   for (double *b : bufs)
     if (b) cudaFree(b);
   for (double *b : a->ckpt)
@@ -761,6 +774,9 @@ void pip_adj_destroy(pip_adj *a) {
   for (double *b : a->segu)
     if (b) cudaFree(b);
   if (a->cand) cudaFree(a->cand);
+  if (a->d_fold) cudaFree(a->d_fold);
+  if (a->mx) cudaFree(a->mx);
+  if (a->my) cudaFree(a->my);
   if (a->ctrl) cudaFree(a->ctrl);
   if (a->h_ctrl) cudaFreeHost(a->h_ctrl);
   if (a->stream) cudaStreamDestroy(a->stream);
@@ -842,7 +858,7 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
   ACK(cudaMemsetAsync(a->dcol, 0, sizeof(double), a->stream));
   const int64_t N = a->steps;
   const int nseg = (int)((N + a->K - 1) / a->K);
-  const int gf = grid_fold(kp);
+  const int gf = grid_fold(a->nfold);
   for (int s = nseg - 1; s >= 0; --s) {
     const int64_t n0 = (int64_t)s * a->K;
     const int len = (int)std::min<int64_t>(a->K, N - n0);
@@ -857,13 +873,13 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
     // reverse sweep
     for (int j = len - 1; j >= 0; --j) {
       const double *dtp = a->dt_hist + n0 + j;
-      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->La);
+      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->La, a->d_fold, a->nfold);
       ACK(cudaGetLastError());
       ACK(launch_vjp(a, 2, a->segu[j], a->La, nullptr, a->Lb, dtp));
-      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->Lb);
+      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->Lb, a->d_fold, a->nfold);
       ACK(cudaGetLastError());
       ACK(launch_vjp(a, 1, zp(j), a->Lb, a->La, a->La, dtp));
-      pip::adjk::finalize_kernel<<<1, 256, 0, a->stream>>>(kp, a->nb, a->p1dot, a->p1dac, a->p2dot,
+      pip::adjk::finalize_kernel<<<1, 256, 0, a->stream>>>(kp, a->nb, a->nbc, a->p1dot, a->p1dac, a->p2dot,
                                                             a->p2dac, a->cand, dtp, zp(j), a->La,
                                                             a->dcol, nullptr);
       ACK(cudaGetLastError());
@@ -910,7 +926,7 @@ int pip_adj_stage_vjp(pip_adj *a, int stage, const double *Us, const double *lam
 int pip_adj_fold(pip_adj *a, double *lam) {
   if (!a || !lam) return PIP_ERR_NULL;
   ACK(cudaSetDevice(a->device));
-  pip::adjk::fold_kernel<<<grid_fold(a->kp), 256, 0, a->stream>>>(a->kp, lam);
+  pip::adjk::fold_kernel<<<grid_fold(a->nfold), 256, 0, a->stream>>>(a->kp, lam, a->d_fold, a->nfold);
   ACK(cudaGetLastError());
   ACK(cudaStreamSynchronize(a->stream));
   return PIP_OK;

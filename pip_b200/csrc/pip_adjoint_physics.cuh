@@ -489,37 +489,35 @@ PIP_HD int hlld_vjp(const double (&vl)[8], const double (&vr)[8], const double (
            a_rsr = 0, a_bn = 0, a_bn2 = 0, a_sal = 0, a_sar = 0, a_iuh0 = 0;
     double out[8];
     if ((sl >= (sm - kHllgFactor * sal)) || ((sm + kHllgFactor * sar) >= sr)) {
-      // HLLC-G (HLL_rot.f90:776-807)
+      // HLLC-G (HLL_rot.f90:776-807).  The side is selected element by element (no pointer
+      // to one side's arrays), so that every array stays in registers.
       const double vy2 = uh[2] * iuh0, vz2 = uh[3] * iuh0;
       const bool left = sm >= 0.0;
-      const double *v = left ? vl : vr;
-      const double *u = left ? ul : ur;
-      const double *fx = left ? fl : fr;
+      double us[8], st[8];
+#pragma unroll
+      for (int n = 0; n < 8; ++n) us[n] = left ? ul[n] : ur[n];
+      const double v1 = left ? vl[1] : vr[1];
       const double S = left ? sl : sr;
       const double ro1 = left ? rol1 : ror1;
       const double iS = left ? ilm : irm;
       const double pts = left ? ptl : ptr;
       const double vb = left ? vbL : vbR;
       const double Q = vb - sm * bn - vy2 * uh[6] - vz2 * uh[7];
-      const double E = (S - v[1]) * u[4] - pts * v[1] + pt * sm + bn * Q;
+      const double E = (S - v1) * us[4] - pts * v1 + pt * sm + bn * Q;
       const double e2 = E * iS;
-      double st[8];
       st[0] = ro1; st[1] = ro1 * sm; st[2] = ro1 * vy2; st[3] = ro1 * vz2; st[4] = e2;
       st[5] = uh[5]; st[6] = uh[6]; st[7] = uh[7];
-      for (int n = 0; n < 8; ++n) out[n] = S * (st[n] - u[n]) + fx[n];
+#pragma unroll
+      for (int n = 0; n < 8; ++n) out[n] = S * (st[n] - us[n]) + (left ? fl[n] : fr[n]);
       region = left ? 2 : 3;
       // reverse
-      double *a_u = left ? a_ul : a_ur;
-      double *a_fx = left ? a_fl : a_fr;
-      double *a_v = left ? a_vl : a_vr;
-      double a_S = 0, a_st[8];
+      double a_S = 0, a_st[8], a_us[8];
+#pragma unroll
       for (int n = 0; n < 8; ++n) {
-        a_fx[n] += a_f[n];
-        a_S += a_f[n] * (st[n] - u[n]);
+        a_S += a_f[n] * (st[n] - us[n]);
         a_st[n] = S * a_f[n];
-        a_u[n] -= S * a_f[n];
+        a_us[n] = -S * a_f[n];
       }
-      a_rol1 += 0.0;
       double a_ro1 = a_st[0] + sm * a_st[1] + vy2 * a_st[2] + vz2 * a_st[3];
       a_sm += ro1 * a_st[1];
       double a_vy2 = ro1 * a_st[2], a_vz2 = ro1 * a_st[3];
@@ -528,14 +526,14 @@ PIP_HD int hlld_vjp(const double (&vl)[8], const double (&vr)[8], const double (
       a_uh[7] += a_st[7];
       const double aE = iS * a_st[4];
       const double a_iS = E * a_st[4];
-      a_S += u[4] * aE;
-      a_v[1] -= (u[4] + pts) * aE;
-      a_u[4] += (S - v[1]) * aE;
-      double a_pts = -v[1] * aE;
+      a_S += us[4] * aE;
+      const double a_v1 = -(us[4] + pts) * aE;
+      a_us[4] += (S - v1) * aE;
+      const double a_pts = -v1 * aE;
       a_pt += sm * aE;
       a_sm += pt * aE;
       a_bn += (Q - bn * sm) * aE;
-      double a_vb = bn * aE;
+      const double a_vb = bn * aE;
       a_sm -= bn * bn * aE;
       a_vy2 -= bn * uh[6] * aE;
       a_uh[6] -= bn * vy2 * aE;
@@ -544,19 +542,25 @@ PIP_HD int hlld_vjp(const double (&vl)[8], const double (&vr)[8], const double (
       a_uh[2] += iuh0 * a_vy2;
       a_uh[3] += iuh0 * a_vz2;
       a_iuh0 += uh[2] * a_vy2 + uh[3] * a_vz2;
-      if (left) {
-        a_sl += a_S;
-        a_rol1 += a_ro1;
-        a_ilm += a_iS;
-        a_ptl += a_pts;
-        a_vbL += a_vb;
-      } else {
-        a_sr += a_S;
-        a_ror1 += a_ro1;
-        a_irm += a_iS;
-        a_ptr += a_pts;
-        a_vbR += a_vb;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        a_fl[n] += left ? a_f[n] : 0.0;
+        a_fr[n] += left ? 0.0 : a_f[n];
+        a_ul[n] += left ? a_us[n] : 0.0;
+        a_ur[n] += left ? 0.0 : a_us[n];
       }
+      a_vl[1] += left ? a_v1 : 0.0;
+      a_vr[1] += left ? 0.0 : a_v1;
+      a_sl += left ? a_S : 0.0;
+      a_sr += left ? 0.0 : a_S;
+      a_rol1 += left ? a_ro1 : 0.0;
+      a_ror1 += left ? 0.0 : a_ro1;
+      a_ilm += left ? a_iS : 0.0;
+      a_irm += left ? 0.0 : a_iS;
+      a_ptl += left ? a_pts : 0.0;
+      a_ptr += left ? 0.0 : a_pts;
+      a_vbL += left ? a_vb : 0.0;
+      a_vbR += left ? 0.0 : a_vb;
     } else {
       StarSide L, Rt;
       star_forward(vl, ul, sl, ilm, sm, bn, bn2, pt, ptl, vbL, rol1, L);
@@ -599,58 +603,64 @@ PIP_HD int hlld_vjp(const double (&vl)[8], const double (&vr)[8], const double (
         u2[7] = f1c * B7;
         const bool left = sm >= 0.0;
         region = left ? 6 : 7;
-        const StarSide &P = left ? L : Rt;
+        double Pu1[8], us[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+          Pu1[n] = left ? L.u1[n] : Rt.u1[n];
+          us[n] = left ? ul[n] : ur[n];
+        }
+        const double Pvy1 = left ? L.vy1 : Rt.vy1, Pvz1 = left ? L.vz1 : Rt.vz1;
         const double ro1 = left ? rol1 : ror1;
         const double ros = left ? rols : rors;
         const double S1 = left ? sl1 : sr1;
         const double S = left ? sl : sr;
         const double sg = left ? -1.0 : 1.0;   // u2[4] = P.u1[4] + sg*ros*W*f2
-        const double *u = left ? ul : ur;
-        const double *fx = left ? fl : fr;
-        const double W = P.vy1 * P.u1[6] + P.vz1 * P.u1[7] - vy2 * u2[6] - vz2 * u2[7];
+        const double W = Pvy1 * Pu1[6] + Pvz1 * Pu1[7] - vy2 * u2[6] - vz2 * u2[7];
         u2[0] = ro1;
-        u2[4] = P.u1[4] + sg * ros * W * f2;
+        u2[4] = Pu1[4] + sg * ros * W * f2;
         u2[1] = ro1 * sm;
         u2[2] = ro1 * vy2;
         u2[3] = ro1 * vz2;
-        double a_S1 = 0, a_S = 0, a_u2[8];
-        double *a_P = left ? a_L : a_R;
-        double *a_u = left ? a_ul : a_ur;
-        double *a_fx = left ? a_fl : a_fr;
+        double a_S1 = 0, a_S = 0, a_u2[8], a_P[8];
+#pragma unroll
         for (int n = 0; n < 8; ++n) {
-          out[n] = S1 * u2[n] - (S1 - S) * P.u1[n] - S * u[n] + fx[n];
-          a_fx[n] += a_f[n];
-          a_S1 += a_f[n] * (u2[n] - P.u1[n]);
-          a_S += a_f[n] * (P.u1[n] - u[n]);
+          out[n] = S1 * u2[n] - (S1 - S) * Pu1[n] - S * us[n] + (left ? fl[n] : fr[n]);
+          a_S1 += a_f[n] * (u2[n] - Pu1[n]);
+          a_S += a_f[n] * (Pu1[n] - us[n]);
           a_u2[n] = S1 * a_f[n];
-          a_P[n] -= (S1 - S) * a_f[n];
-          a_u[n] -= S * a_f[n];
+          a_P[n] = -(S1 - S) * a_f[n];
+          a_fl[n] += left ? a_f[n] : 0.0;
+          a_fr[n] += left ? 0.0 : a_f[n];
+          a_ul[n] -= left ? S * a_f[n] : 0.0;
+          a_ur[n] -= left ? 0.0 : S * a_f[n];
         }
         // u2[4]
         a_P[4] += a_u2[4];
         double a_ros = sg * W * f2 * a_u2[4];
         const double a_W = sg * ros * f2 * a_u2[4];
-        double a_Pvy1 = P.u1[6] * a_W, a_Pvz1 = P.u1[7] * a_W;
-        a_P[6] += P.vy1 * a_W;
-        a_P[7] += P.vz1 * a_W;
+        const double a_Pvy1 = Pu1[6] * a_W, a_Pvz1 = Pu1[7] * a_W;
+        a_P[6] += Pvy1 * a_W;
+        a_P[7] += Pvz1 * a_W;
         double a_vy2 = -u2[6] * a_W, a_vz2 = -u2[7] * a_W;
         a_u2[6] -= vy2 * a_W;
         a_u2[7] -= vz2 * a_W;
         // u2[0..3]
-        double a_ro1 = a_u2[0] + sm * a_u2[1] + vy2 * a_u2[2] + vz2 * a_u2[3];
+        const double a_ro1 = a_u2[0] + sm * a_u2[1] + vy2 * a_u2[2] + vz2 * a_u2[3];
         a_sm += ro1 * a_u2[1];
         a_vy2 += ro1 * a_u2[2];
         a_vz2 += ro1 * a_u2[3];
         a_bn += a_u2[5];
-        if (left) {
-          a_rol1 += a_ro1;
-          a_vyl1 += a_Pvy1;
-          a_vzl1 += a_Pvz1;
-        } else {
-          a_ror1 += a_ro1;
-          a_vyr1 += a_Pvy1;
-          a_vzr1 += a_Pvz1;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+          a_L[n] += left ? a_P[n] : 0.0;
+          a_R[n] += left ? 0.0 : a_P[n];
         }
+        a_rol1 += left ? a_ro1 : 0.0;
+        a_ror1 += left ? 0.0 : a_ro1;
+        a_vyl1 += left ? a_Pvy1 : 0.0;
+        a_vyr1 += left ? 0.0 : a_Pvy1;
+        a_vzl1 += left ? a_Pvz1 : 0.0;
+        a_vzr1 += left ? 0.0 : a_Pvz1;
         double a_rols = left ? a_ros : 0.0, a_rors = left ? 0.0 : a_ros;
         // u2[6] = f1c*B6, u2[7] = f1c*B7
         double a_f1c = B6 * a_u2[6] + B7 * a_u2[7];
