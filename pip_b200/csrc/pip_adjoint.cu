@@ -34,8 +34,15 @@ namespace adjk {
 
 constexpr int NVM = 8, NV = 13;
 
-// Thread-block sizes of the reverse-stage kernels.
-constexpr int kFaceThreads = 128;   // one face per thread, register bound (255 per thread)
+// Thread-block sizes of the reverse-stage kernels and their minimum resident blocks per SM
+// (register budget: 65536 / (threads * blocks) per thread).
+#ifndef PIP_ADJ_FACE_MINB
+#define PIP_ADJ_FACE_MINB 2
+#endif
+#ifndef PIP_ADJ_CELL_MINB
+#define PIP_ADJ_CELL_MINB 2
+#endif
+constexpr int kFaceThreads = 128;   // one face per thread
 constexpr int kCellThreads = 256;
 
 // Per-block CFL candidates of stage 1 (the state z_n).
@@ -197,7 +204,7 @@ __global__ void u2v_kernel(const KParams p, const double *__restrict__ U, double
 // states and the Riemann solver (face_vjp), written as (gL, gR, minmod branches); other
 // faces are written as zero.  Per block: sum of <F, lamF> (the flux part of dt_sub
 // <lam, dU/d(dt_sub)>).
-__global__ void __launch_bounds__(kFaceThreads)
+__global__ void __launch_bounds__(kFaceThreads, PIP_ADJ_FACE_MINB)
 face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__restrict__ lam,
                 const double *dtp, double fac, double *gx, unsigned long long *mx, double *gy,
                 unsigned long long *my, double *part_dot, double *part_dac) {
@@ -269,7 +276,7 @@ face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__r
 // through minmod, u2v, the explicit collision source (interior cells), the U0 terms
 // acc + lam of stage 1 (interior cells, when acc is given), and for stage 1 the CFL
 // candidates of the cell (cand).  Per block: dt_sub <lam, S>, dS/dalpha_c . lam.
-__global__ void __launch_bounds__(kCellThreads)
+__global__ void __launch_bounds__(kCellThreads, PIP_ADJ_CELL_MINB)
 cell_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *__restrict__ lam,
                 const double *acc, double *out, const double *dtp, double fac,
                 const double *__restrict__ gx, const unsigned long long *__restrict__ mx,

@@ -556,7 +556,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
 template <int NVM>
 __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, DevCtrl *ctrl,
                                                   int slot) {
-  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
+  const double gm = p.gm;
   double dtc = 10.0, rhoc = 0.0, grc = 0.0;
   const long long nc = p.nc;
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
@@ -691,7 +691,6 @@ __global__ void flux_kernel(const KParams p, const double *__restrict__ U, doubl
 // with the exponential form S receives the U0 increments (-/+ dt_coll*dS).
 template <int NVM>
 __global__ void source_kernel(const KParams p, double *U, double *S, double dt_coll) {
-  const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
   const long long nc = p.nc;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc;
        q += (long long)gridDim.x * blockDim.x) {
