@@ -21,6 +21,12 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
 * cpu_baseline: the CPU restatement on all host cores, bounded sample of the same workload.
 * --impl reference: the reference's own algorithm on host cores (the reference is Fortran +
   MPI + HDF5 and cannot be built on this image; its CPU restatement runs instead).
+* adjoint: the discrete adjoint of the two-fluid linear wave-damping run (512x256, 500 FP64
+  steps, checkpoints every 25 steps): device time of the plain FP64 forward (pip_run), of
+  the checkpointing forward and of the backward (recomputation included), and their ratios.
+* ensemble: 512 seeded 1D two-fluid shock tubes (nx log-uniform in [256, 8192], alpha_c
+  log-uniform in [0.1, 1e4]) advanced to t = 0.1 in one persistent launch (FP32-mixed):
+  sum over runs of interior cells x steps / device time.
 """
 from __future__ import annotations
 
@@ -248,6 +254,78 @@ def e2e_run(s, Uh, Um, steps, warmup, dist):
     return e2e_s, Uh.nbytes + Um.nbytes
 
 
+def measure_adjoint(nsteps=500, K=25):
+    """C5: two-fluid linear wave damping 512x256, alpha_c = 10, loss = L2 misfit of the final
+    ion vy and neutral density against a forward run with alpha_c = 20 from another seed."""
+    import torch
+    from pip_b200 import capi, ics
+    from pip_b200.adjoint import AdjointRun, pip_run, wave_damping_state
+    s, _, _ = ics.wave_damping(512, 256, col=10.0)
+    X, Y = ics._grid(s)
+
+    def pert(seed):
+        dv = ics.velocity_modes(X, Y, s.end[0] - s.start[0], s.end[1] - s.start[1], seed, 1.0e-4, 8)
+        return [torch.from_numpy(d).cuda() for d in dv]
+    r = AdjointRun(s, nsteps, checkpoint_every=K)
+    UT = r.forward(wave_damping_state(s, *pert(5151)), 20.0)
+    tvy = (UT[2, 2:-2, 2:-2] / UT[0, 2:-2, 2:-2]).clone()
+    trn = UT[8, 2:-2, 2:-2].clone()
+    U0 = wave_damping_state(s, *pert(5150))
+    fwd, bwd = [], []
+    for _ in range(3):
+        U0g = U0.clone().requires_grad_(True)
+        ac = torch.tensor(10.0, dtype=torch.float64, device="cuda", requires_grad=True)
+        UN = pip_run(U0g, ac, r)
+        loss = (((UN[2, 2:-2, 2:-2] / UN[0, 2:-2, 2:-2]) - tvy) ** 2).sum() + \
+            ((UN[8, 2:-2, 2:-2] - trn) ** 2).sum()
+        loss.backward()
+        fwd.append(r.forward_ms)
+        bwd.append(r.backward_ms)
+    plain = []
+    with capi.Context(s) as c:
+        Uc = U0.cpu().numpy()
+        for _ in range(3):
+            c.upload(Uc[8:].copy(), Uc[:8].copy())
+            st, t, n, ms = c.run_timed(nsteps=nsteps)
+            plain.append(ms)
+    r.close()
+    f, b, p0 = min(fwd[1:]), min(bwd[1:]), min(plain[1:])
+    return {"workload": "2D two-fluid linear wave damping 512x256 (+2 ghosts), periodic, rho=1 "
+                        "(50% ions), p=0.6, B0=1 x, alpha_c=10, velocity modes |k|<=8 amp 1e-4 "
+                        "(seed 5150); loss: L2 misfit of final ion vy and neutral density vs "
+                        "alpha_c=20, seed 5151",
+            "steps": nsteps, "checkpoint_every": K, "dtype": "f64",
+            "forward_ms": p0, "checkpointed_forward_ms": f, "backward_ms": b,
+            "backward_over_forward": b / p0, "gradient_over_forward": (f + b) / p0,
+            "target_backward_over_forward": 4.0, "loss": float(loss.item()),
+            "dloss_dcol": float(ac.grad.item()),
+            "how": "device time (CUDA events in the library) of pip_run over 500 steps, of "
+                   "pip_adj_forward (same kernels + checkpoint copies) and of pip_adj_backward "
+                   "(recompute of each 25-step segment + reverse sweep); best of 2 after one warm-up"}
+
+
+def measure_ensemble(n_runs=512, t_end=0.1):
+    from pip_b200.ensemble import Ensemble, shock_tube_ensemble
+    mem = shock_tube_ensemble(n_runs, 4242)
+    with Ensemble(mem) as e:
+        threads, ctas, _ = e.tune(t_probe=0.002)
+        for r, (s, Uh, Um) in enumerate(mem):
+            e.upload(r, Uh, Um)
+        ms = e.run(t_end=t_end)
+        updates = 0
+        bad = 0
+        for r in range(len(mem)):
+            _, _, t, n, st = e.member(r, state=False)
+            updates += n * mem[r][0].ix0
+            bad += st != 0
+    return {"workload": "%d seeded 1D two-fluid shock tubes, nx log-uniform [256, 8192], "
+                        "alpha_c log-uniform [0.1, 1e4], to t=%g, FP32-mixed" % (n_runs, t_end),
+            "value": updates / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
+            "cell_updates": updates, "runs_failed": bad, "threads": threads,
+            "ctas_per_sm": ctas, "how": "one persistent launch (CUDA graph), configuration "
+                                        "chosen by the autotuner on a t=0.002 probe"}
+
+
 def rel_l1_interior(a, b, m):
     import numpy as np
     out = []
@@ -268,6 +346,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N_GRID, help="grid size (default 1024)")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -326,6 +406,8 @@ def main():
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_sample()
         cpu.pop("s_per_step", None)
+    adjoint = None if args.no_adjoint else measure_adjoint()
+    ensemble = None if args.no_ensemble else measure_ensemble()
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
@@ -361,6 +443,8 @@ def main():
                      "peak_kind": peak_kind, "ms_stage1": mix["ms1"], "ms_stage2": mix["ms2"],
                      "step_achieved_gbs": MIXED_BYTES_PER_CELL_STEP * cells / (mix["msstep"] * 1e-3) / 1e9},
         "cpu_baseline": cpu,
+        "adjoint": adjoint,
+        "ensemble": ensemble,
         "e2e": e2e,
         "gpu_launches": mix["launches"],
         "clocks": mix["clocks"],
