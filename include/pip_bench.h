@@ -27,8 +27,13 @@ int pip_run_timed(pip_ctx *ctx, int64_t nsteps, double t_end, double *time_out,
 int pip_bench_stage_ms(pip_ctx *ctx, int nsteps, float *ms_stage1, float *ms_stage2,
                        float *ms_step);
 
-/* Number of kernels pip_run launches for nsteps steps (1 cfl pass + 2 per step). */
+/* Number of kernels pip_run launches for nsteps steps (1 cfl pass + 2 per step; runs with
+ * conduction add the BiCGstab kernels, see pip_conduction_iterations). */
 int64_t pip_kernels_per_run(pip_ctx *ctx, int64_t nsteps);
+
+/* BiCGstab iterations (inner iterations for the mixed form) of the last pip_run, pip_step
+ * or pip_conduction of a flag_heat = 1 context. */
+int64_t pip_conduction_iterations(pip_ctx *ctx);
 
 #ifdef __cplusplus
 }

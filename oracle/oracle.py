@@ -60,6 +60,8 @@ def lib():
         L.orc_run.argtypes = [vp, ctypes.c_long, d, dp, P(ctypes.c_long), dp, ctypes.c_long]
         L.orc_run.restype = ctypes.c_int
         L.orc_has_nan.argtypes = [vp]
+        L.orc_conduction.argtypes = [vp, d, P(ctypes.c_int), dp]
+        L.orc_conduction.restype = ctypes.c_int
         L.orc_has_nan.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -146,6 +148,13 @@ class Oracle:
         S_m = np.zeros(self.shape_m)
         lib().orc_source(self.h, float(dt_coll), _ptr(S_h), _ptr(S_m))
         return S_h, S_m
+
+    def conduction(self, dt: float):
+        """HC(U_m,nvar_m,1) over dt; returns (status, iterations, relative residual)."""
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        st = lib().orc_conduction(self.h, float(dt), ctypes.byref(it), ctypes.byref(rr))
+        return st, it.value, rr.value
 
     def fill_ghosts(self) -> None:
         lib().orc_bnd(self.h)

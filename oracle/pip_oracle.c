@@ -828,6 +828,233 @@ static void add_flux_rk(orc_ctx *c, const double *F, const double *U0, double *U
   }
 }
 
+/* ---------------------------------------------------------------- implicit conduction */
+
+/* Stencil of the 9-point matrix (initialize_HC, HC_rot.f90:41-46, hc_split=2): entries
+ * 0..8 couple cell (i,j) with (i,j), (i-1,j), (i+1,j), (i,j-1), (i,j+1), (i-1,j-1),
+ * (i+1,j-1), (i-1,j+1), (i+1,j+1). */
+#define HC_EPSI 1.0e-5               /* HC_rot.f90:17 */
+
+/* matrix(i,j,:) . v over the 9-point stencil, summed left to right as the Fortran does. */
+static double hc_apply(const orc_ctx *c, const double *mat, const double *v, size_t q) {
+  const size_t nc = c->nc;
+  const long ix = c->ix;
+  return mat[q] * v[q] + mat[q + nc] * v[q - 1] + mat[q + 2 * nc] * v[q + 1] +
+         mat[q + 3 * nc] * v[q - ix] + mat[q + 4 * nc] * v[q + ix] +
+         mat[q + 5 * nc] * v[q - 1 - ix] + mat[q + 6 * nc] * v[q + 1 - ix] +
+         mat[q + 7 * nc] * v[q - 1 + ix] + mat[q + 8 * nc] * v[q + 1 + ix];
+}
+
+/* set_matrix_source_MHD2D9 (HC_rot.f90:643-739) for the interior cells (dxc = dx and
+ * dyc = dy for s_order = 2, Model_rot.f90:430-431), then set_matrix_boundary
+ * (HC_rot.f90:468-529) on all four sides: with one rank per direction every neighbour is
+ * -1 (set_mpi_neighbor, MPI_rot.f90:123), so the stencil entries outside the domain are
+ * folded onto the boundary row (x-, x+, y-, y+ in that order). */
+static void hc_matrix(const orc_ctx *c, const double *ro, const double *te, const double *bx,
+                      const double *by, const double *bz, double dt, double *mat) {
+  const pip_params *p = &c->p;
+  const size_t nc = c->nc;
+  const int ix = c->ix, jx = c->jx;
+  const int is = p->margin[0], ie = ix - p->margin[0] - 1;
+  const int js = p->margin[1], je = jx - p->margin[1] - 1;
+  const double gm = p->gm, kapper = p->kapper;
+  for (int j = js; j <= je; ++j)
+    for (int i = is; i <= ie; ++i) {
+      const size_t q = (size_t)j * ix + i;
+      const double eta = kapper * dt * (gm - 1.0) / ro[q] * gm;
+      const double bxl = (bx[q - 1] + bx[q]) / 2.0, bxr = (bx[q + 1] + bx[q]) / 2.0;
+      const double bxd = (bx[q - ix] + bx[q]) / 2.0, bxu = (bx[q + ix] + bx[q]) / 2.0;
+      const double byl = (by[q - 1] + by[q]) / 2.0, byr = (by[q + 1] + by[q]) / 2.0;
+      const double byd = (by[q - ix] + by[q]) / 2.0, byu = (by[q + ix] + by[q]) / 2.0;
+      const double bzl = (bz[q - 1] + bz[q]) / 2.0, bzr = (bz[q + 1] + bz[q]) / 2.0;
+      const double bzd = (bz[q - ix] + bz[q]) / 2.0, bzu = (bz[q + ix] + bz[q]) / 2.0;
+      const double nxl = bxl / (fmx(sqrt(bxl * bxl + byl * byl + bzl * bzl), HC_EPSI));
+      const double nxr = bxr / (fmx(sqrt(bxr * bxr + byr * byr + bzr * bzr), HC_EPSI));
+      const double nxd = bxd / (fmx(sqrt(bxd * bxd + byd * byd + bzd * bzd), HC_EPSI));
+      const double nxu = bxu / (fmx(sqrt(bxu * bxu + byu * byu + bzu * bzu), HC_EPSI));
+      const double nyl = byl / (fmx(sqrt(bxl * bxl + byl * byl + bzl * bzl), HC_EPSI));
+      const double nyr = byr / (fmx(sqrt(bxr * bxr + byr * byr + bzr * bzr), HC_EPSI));
+      const double nyd = byd / (fmx(sqrt(bxd * bxd + byd * byd + bzd * bzd), HC_EPSI));
+      const double nyu = byu / (fmx(sqrt(bxu * bxu + byu * byu + bzu * bzu), HC_EPSI));
+      const double te_xm = 0.5 * (te[q] + te[q - 1]), te_xp = 0.5 * (te[q] + te[q + 1]);
+      const double te_ym = 0.5 * (te[q] + te[q - ix]), te_yp = 0.5 * (te[q] + te[q + ix]);
+      const double te_xm25 = te_xm * te_xm * sqrt(te_xm), te_xp25 = te_xp * te_xp * sqrt(te_xp);
+      const double te_ym25 = te_ym * te_ym * sqrt(te_ym), te_yp25 = te_yp * te_yp * sqrt(te_yp);
+      const double dxc = c->dx[i], dyc = c->dy[j];
+      const double bxxl = -(eta * te_xm25 * nxl * nxl / dxc / c->dx[i - 1]);
+      const double bxxr = -(eta * te_xp25 * nxr * nxr / dxc / c->dx[i]);
+      const double byyd = -(eta * te_ym25 * nyd * nyd / dyc / c->dy[j - 1]);
+      const double byyu = -(eta * te_yp25 * nyu * nyu / dyc / c->dy[j]);
+      const double bxyl = -(eta / 4.0 / dxc / dyc * nxl * nyl * te_xm25);
+      const double bxyr = -(eta / 4.0 / dxc / dyc * nxr * nyr * te_xp25);
+      const double byxd = -(eta / 4.0 / dxc / dyc * nyd * nxd * te_ym25);
+      const double byxu = -(eta / 4.0 / dxc / dyc * nyu * nxu * te_yp25);
+      double *m = mat + q;
+      m[nc] = bxxl - (byxu - byxd);
+      m[2 * nc] = bxxr + (byxu - byxd);
+      m[3 * nc] = byyd - (bxyr - bxyl);
+      m[4 * nc] = byyu + (bxyr - bxyl);
+      m[5 * nc] = bxyl + byxd;
+      m[6 * nc] = -(bxyr + byxd);
+      m[7 * nc] = -(bxyl + byxu);
+      m[8 * nc] = bxyr + byxu;
+      m[0] = 1.0 - (m[nc] + m[2 * nc] + m[3 * nc] + m[4 * nc]);
+    }
+  /* set_matrix_boundary, hc_split = 2 (entries 1..9 of the Fortran are 0..8 here) */
+#define M(n, qq) mat[(size_t)(n) * nc + (qq)]
+  for (int j = js; j <= je; ++j) {       /* x-minus */
+    const size_t q = (size_t)j * ix + is;
+    M(0, q) = M(1, q) + M(0, q); M(1, q) = 0.0;
+    M(3, q) = M(3, q) + M(5, q); M(5, q) = 0.0;
+    M(4, q) = M(4, q) + M(7, q); M(7, q) = 0.0;
+  }
+  for (int j = js; j <= je; ++j) {       /* x-plus */
+    const size_t q = (size_t)j * ix + ie;
+    M(0, q) = M(2, q) + M(0, q); M(2, q) = 0.0;
+    M(3, q) = M(3, q) + M(6, q); M(6, q) = 0.0;
+    M(4, q) = M(4, q) + M(8, q); M(8, q) = 0.0;
+  }
+  for (int i = is; i <= ie; ++i) {       /* y-minus */
+    const size_t q = (size_t)js * ix + i;
+    M(0, q) = M(3, q) + M(0, q); M(3, q) = 0.0;
+    M(1, q) = M(5, q) + M(1, q); M(5, q) = 0.0;
+    M(2, q) = M(6, q) + M(2, q); M(6, q) = 0.0;
+  }
+  for (int i = is; i <= ie; ++i) {       /* y-plus */
+    const size_t q = (size_t)je * ix + i;
+    M(0, q) = M(4, q) + M(0, q); M(4, q) = 0.0;
+    M(1, q) = M(1, q) + M(7, q); M(7, q) = 0.0;
+    M(2, q) = M(2, q) + M(8, q); M(8, q) = 0.0;
+  }
+#undef M
+}
+
+/* BiCGstab (HC_rot.f90:187-299, hc_split = 2): the residual is recomputed from te every
+ * iteration; stops when sqrt(sum r^2 / sum b^2) <= hc_error or after hc_max+1 iterations.
+ * Sums run in the Fortran array order.  Entries of the Krylov vectors outside the interior
+ * are zero (the folded matrix multiplies them by exact zeros). */
+static int hc_bicgstab(const orc_ctx *c, const double *mat, double *te, const double *src,
+                       int *count_out, double *relres_out) {
+  const pip_params *p = &c->p;
+  const size_t nc = c->nc;
+  const int ix = c->ix, jx = c->jx;
+  const int is = p->margin[0], ie = ix - p->margin[0] - 1;
+  const int js = p->margin[1], je = jx - p->margin[1] - 1;
+  double *r = calloc(nc, sizeof(double)), *r0 = calloc(nc, sizeof(double));
+  double *pk = calloc(nc, sizeof(double)), *apk = calloc(nc, sizeof(double));
+  double *tkp = calloc(nc, sizeof(double));
+  double total_resi = 0.0, total_source = 0.0;
+  for (int j = js; j <= je; ++j)
+    for (int i = is; i <= ie; ++i) {
+      const size_t q = (size_t)j * ix + i;
+      double v = src[q];
+      v = v - mat[q] * te[q];
+      v = v - mat[q + nc] * te[q - 1];
+      v = v - mat[q + 2 * nc] * te[q + 1];
+      v = v - mat[q + 3 * nc] * te[q - ix];
+      v = v - mat[q + 4 * nc] * te[q + ix];
+      v = v - mat[q + 5 * nc] * te[q - 1 - ix];
+      v = v - mat[q + 6 * nc] * te[q + 1 - ix];
+      v = v - mat[q + 7 * nc] * te[q - 1 + ix];
+      v = v - mat[q + 8 * nc] * te[q + 1 + ix];
+      r[q] = v;
+      total_resi += v * v;
+      total_source += src[q] * src[q];
+      r0[q] = v;
+      pk[q] = v;
+    }
+  int count = 0;
+  const double error = p->hc_error;
+  while (sqrt(total_resi / total_source) > error && count <= p->hc_max) {
+    double alphau = 0.0, alphad = 0.0;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        apk[q] = hc_apply(c, mat, pk, q);
+        alphau = alphau + (r[q] * r0[q]);
+        alphad = alphad + (r0[q] * apk[q]);
+      }
+    const double alpha = alphau / alphad;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        tkp[q] = r[q] - alpha * apk[q];
+      }
+    double omegau = 0.0, omegad = 0.0;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        const double atk = hc_apply(c, mat, tkp, q);
+        omegau = omegau + tkp[q] * atk;
+        omegad = omegad + atk * atk;
+      }
+    const double omega = omegau / omegad;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        te[q] = te[q] + alpha * pk[q] + omega * tkp[q];
+      }
+    double betau = 0.0;
+    total_resi = 0.0;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        r[q] = src[q] - hc_apply(c, mat, te, q);
+        betau = betau + r0[q] * r[q];
+        total_resi = total_resi + r[q] * r[q];
+      }
+    const double beta = betau / alphau * alpha / omega;
+    for (int j = js; j <= je; ++j)
+      for (int i = is; i <= ie; ++i) {
+        const size_t q = (size_t)j * ix + i;
+        pk[q] = r[q] + beta * (pk[q] - omega * apk[q]);
+      }
+    count = count + 1;
+  }
+  const double relres = sqrt(total_resi / total_source);
+  free(r); free(r0); free(pk); free(apk); free(tkp);
+  if (count_out) *count_out = count;
+  if (relres_out) *relres_out = relres;
+  return relres <= error ? PIP_OK : PIP_ERR_ITER;
+}
+
+/* HC(U_m, nvar_m, 1) (HC_rot.f90:67-140) on one rank: cq2pv_mhd (rewriting U_m), te =
+ * gm*(pr/ro), the matrix (source = te), BiCGstab, pr = (te*ro)/gm, pv2cq_mhd
+ * (Scheme_rot.f90:43-79, flag_b_stg = 0).  Called by post_step (Solver_rot.f90:296-303)
+ * when flag_heat = 1 with the implicit integration. */
+int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres) {
+  const pip_params *p = &c->p;
+  const size_t nc = c->nc;
+  const double gm = p->gm;
+  double *w = malloc(sizeof(double) * nc * 8);
+  double *ro = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc, *pr = w + 4 * nc;
+  double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
+  cq2pv_mhd(c, c->U_m, ro, vx, vy, vz, pr, bx, by, bz);
+  double *te = malloc(sizeof(double) * nc), *src = malloc(sizeof(double) * nc);
+  for (size_t q = 0; q < nc; ++q) {
+    te[q] = gm * (pr[q] / ro[q]);
+    src[q] = te[q];
+  }
+  double *mat = calloc(9 * nc, sizeof(double));
+  hc_matrix(c, ro, te, bx, by, bz, dt, mat);
+  const int st = hc_bicgstab(c, mat, te, src, iters, relres);
+  double *U = c->U_m;
+  for (size_t q = 0; q < nc; ++q) {
+    pr[q] = (te[q] * ro[q]) / gm;
+    U[q] = ro[q];
+    U[q + nc] = ro[q] * vx[q];
+    U[q + 2 * nc] = ro[q] * vy[q];
+    U[q + 3 * nc] = ro[q] * vz[q];
+    U[q + 4 * nc] = pr[q] / (gm - 1.0) + 0.5 * ro[q] * (vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q]) +
+                    0.5 * (bx[q] * bx[q] + by[q] * by[q] + bz[q] * bz[q]);
+    U[q + 5 * nc] = bx[q];
+    U[q + 6 * nc] = by[q];
+    U[q + 7 * nc] = bz[q];
+  }
+  free(w); free(te); free(src); free(mat);
+  return st;
+}
+
 /* run_solver, Solver_rot.f90:42-81 with set_flux :124, set_source :162, time_integral
  * :179-277 (flag_time=0), add_source :498-503, divb_cleaning_Dedner_source
  * (Scheme_rot.f90:546-554) and PIPbnd after each stage and at the end. */
@@ -862,6 +1089,8 @@ void orc_run_solver(orc_ctx *c, double dt) {
     }
     orc_bnd(c);
   }
+  /* post_step (Solver_rot.f90:296-303): implicit conduction of the ions */
+  if (p->flag_heat == 1) orc_conduction(c, dt, NULL, NULL);
   orc_bnd(c);
   free(U_h0); free(U_m0); free(F_h); free(F_m); free(S_h); free(S_m);
 }
@@ -904,6 +1133,7 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   *status = PIP_ERR_PARAM;
   if (!p || p->ndim < 1 || p->ndim > 2 || p->kx != 1 || p->nvar_h != 5) return NULL;
   if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return NULL;
+  if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0))) return NULL;
   orc_ctx *c = calloc(1, sizeof(orc_ctx));
   c->p = *p;
   c->ix = p->ix; c->jx = p->jx; c->kx = p->kx;

@@ -48,6 +48,9 @@ void orc_bnd(orc_ctx *c);
  * receives up to max_hist per-step dt values. */
 int orc_run(orc_ctx *c, long nsteps, double t_end, double *time_out, long *steps_done,
             double *dt_hist, long max_hist);
+/* HC(U_m,nvar_m,1) (HC_rot.f90:67-140), 9-point matrix + BiCGstab on one rank, over dt;
+ * returns PIP_OK or PIP_ERR_ITER; iters/relres may be NULL. */
+int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres);
 /* stop_sim's NaN scan (IO_rot.f90:641-668) over both species. */
 int orc_has_nan(const orc_ctx *c);
 

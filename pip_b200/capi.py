@@ -34,7 +34,7 @@ EXPORTS = (
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc",
     # include/pip_bench.h
-    "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run",
+    "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
     "pip_ensemble_create", "pip_ensemble_destroy", "pip_ensemble_upload", "pip_ensemble_run",
     "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
@@ -95,6 +95,8 @@ def lib(path: Optional[str] = None):
     L.pip_run_timed.argtypes = [vp, ctypes.c_int64, d, dp, P(ctypes.c_int64), P(ctypes.c_float)]
     L.pip_bench_stage_ms.argtypes = [vp, i, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)]
     L.pip_kernels_per_run.argtypes = [vp, ctypes.c_int64]
+    L.pip_conduction_iterations.argtypes = [vp]
+    L.pip_conduction_iterations.restype = ctypes.c_int64
     # batched ensembles (include/pip_ensemble.h)
     L.pip_ensemble_create.argtypes = [P(PipParams), i, P(vp)]
     L.pip_ensemble_destroy.argtypes = [vp]
@@ -210,6 +212,20 @@ class Context:
         if check and st not in (PIP_OK, PIP_ERR_NAN, PIP_ERR_DT):
             raise PipError(st, "pip_run")
         return st, t.value, n.value
+
+    def conduction(self, dt: float) -> Tuple[int, int, float]:
+        """HC(U_m,nvar_m,1) over dt (flag_heat = 1 contexts): (status, iterations, relative
+        residual); status PIP_OK or PIP_ERR_ITER."""
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        st = lib().pip_conduction(self.h, float(dt), ctypes.byref(it), ctypes.byref(rr))
+        if st not in (PIP_OK, PIP_ERR_ITER):
+            raise PipError(st, "pip_conduction")
+        return st, it.value, rr.value
+
+    @property
+    def conduction_iterations(self) -> int:
+        return int(lib().pip_conduction_iterations(self.h))
 
     @property
     def time(self) -> float:

@@ -37,6 +37,9 @@ struct pip_ctx {
   int *d_flag = nullptr;
   DevCtrl *ctrl = nullptr;
   DevCtrl *h_ctrl = nullptr;          // pinned mirror
+  pip::HcEngine *hc = nullptr;        // implicit conduction (flag_heat = 1)
+  double *d_dt = nullptr;             // host dt of pip_step / pip_conduction on the device
+  int hc_iters = 0;                   // BiCGstab iterations of the last run
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   bool uploaded = false;
@@ -134,7 +137,10 @@ int validate(const pip_params *p) {
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
   if (p->precision != PIP_FP64 && p->precision != PIP_MIXED) return PIP_ERR_PARAM;
-  if (p->flag_heat != 0) return PIP_ERR_PARAM;
+  if (p->flag_heat != 0 && p->flag_heat != 1) return PIP_ERR_PARAM;
+  if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0) ||
+                            !(p->kapper >= 0.0)))
+    return PIP_ERR_PARAM;
   const int m0 = p->margin[0], m1 = p->margin[1];
   if (m0 < 2 || m0 > pip::kMaxMargin || p->margin[2] != 0) return PIP_ERR_PARAM;
   if (p->ndim == 1 && (m1 != 0 || p->jx != 1)) return PIP_ERR_PARAM;
@@ -185,6 +191,7 @@ void build_kparams(pip_ctx *c) {
   k.decay[0] = std::exp(-0.5 * p.safety * p.db_clean);
   k.decay[1] = std::exp(-1.0 * p.safety * p.db_clean);
   k.dz0 = c->dz[0];
+  k.hc_kapper = p.kapper;
   for (int s = 0; s < 2; ++s) {
     const int fx = s, fy = 2 + s;
     k.typex[s] = bnd_type(p.flag_bnd[fx]);
@@ -254,6 +261,7 @@ int pip::kparams_from_params(const pip_params *p, KParams *k) {
   k->decay[0] = std::exp(-0.5 * p->safety * p->db_clean);
   k->decay[1] = std::exp(-1.0 * p->safety * p->db_clean);
   k->dz0 = p->dz[0];
+  k->hc_kapper = p->kapper;
   for (int s = 0; s < 2; ++s) {
     k->typex[s] = bnd_type(p->flag_bnd[s]);
     for (int l = 0; l < pip::kMaxMargin; ++l)
@@ -337,6 +345,17 @@ cudaError_t to_fp64(pip_ctx *c) {
 cudaError_t from_fp64(pip_ctx *c) {
   if (!c->mixed) return cudaSuccess;
   return pip::mixed_split(c->A, c->Ahi, c->Alo, c->kp.nc * c->nplanes(), c->stream);
+}
+
+// post_step's implicit conduction (Solver_rot.f90:296-303) on the context state with the dt
+// at dtp (device) and the ghost fill that follows it in run_solver (:78).
+int conduct(pip_ctx *c, const double *dtp, int *iters, double *relres, int *status) {
+  CK(to_fp64(c));
+  CK(pip::hc_run(c->hc, c->kp, c->A, dtp, c->p.hc_error, c->p.hc_max, c->stream, iters, relres,
+                 status));
+  CK(c->L->ghosts(c->kp, c->A, c->stream));
+  CK(from_fp64(c));
+  return PIP_OK;
 }
 
 // K steps of [stage 1, stage 2] as launched by pip_run.
@@ -440,6 +459,9 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
     return fail(e);
   c->kp.dx = c->d_dx;
   c->kp.dy = c->d_dy;
+  if ((e = cudaMalloc(&c->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
+  if (p->flag_heat == 1 && (e = pip::hc_create(c->kp, c->mixed, &c->hc)) != cudaSuccess)
+    return fail(e);
   if (c->mixed) {
     std::vector<double> r(c->dx.size()), ry(c->dy.size());
     for (size_t i = 0; i < r.size(); ++i) r[i] = 1.0 / c->dx[i];
@@ -474,6 +496,8 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->scratch);
   cudaFree(c->ctrl);
   cudaFree(c->d_flag);
+  cudaFree(c->d_dt);
+  pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -534,6 +558,13 @@ int pip_step(pip_ctx *c, double dt) {
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_stage(c, 1, 0, 0));
   CK(do_stage(c, 2, 0, 0));
+  if (c->hc) {
+    CK(cudaMemcpyAsync(c->d_dt, &c->h_ctrl->dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int it = 0, st = 0;
+    const int r = conduct(c, c->d_dt, &it, nullptr, &st);
+    if (r != PIP_OK) return r;
+    c->hc_iters = it;
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->last_dt = dt;
   return PIP_OK;
@@ -571,6 +602,32 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
+  if (c->hc) {
+    // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
+    // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
+    // BiCGstab's convergence checks anyway, so no graph
+    long long n = 0;
+    int total_it = 0;
+    for (;;) {
+      CK(do_stage(c, 1, 1, 0));
+      CK(do_stage(c, 2, 1, 0));
+      int it = 0, hst = 0;
+      const int r = conduct(c, &c->ctrl->dt, &it, nullptr, &hst);
+      if (r != PIP_OK) return r;
+      total_it += it;
+      if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+      if (h.nan_flag || h.status || h.step != n + 1) break;
+      CK(do_cfl(c, (int)(n & 1)));          // the cfl after run_solver (main.f90:47)
+      if (h.done) break;
+      CK(do_cfl(c, (int)((n + 1) & 1)));    // the next step's cfl (main.f90:36)
+      ++n;
+    }
+    c->hc_iters = total_it;
+    if (device_ms) {
+      CK(cudaEventRecord(ev1, c->stream));
+      CK(cudaEventSynchronize(ev1));
+    }
+  } else {
   const int K = 32;
   int st = PIP_OK;
   if (nsteps > 0 && !(t_end > 0.0)) {
@@ -594,6 +651,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
       CK(cudaEventRecord(ev1, c->stream));
       CK(cudaEventSynchronize(ev1));
     }
+  }
   }
   if (device_ms) {
     CK(cudaEventElapsedTime(device_ms, ev0, ev1));
@@ -665,6 +723,8 @@ int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
   return 1 + 2 * (nsteps > 0 ? nsteps : 0);
 }
 
+int64_t pip_conduction_iterations(pip_ctx *c) { return c ? c->hc_iters : 0; }
+
 int pip_set_time(pip_ctx *c, double t) {
   if (!c) return PIP_ERR_NULL;
   c->time = t;
@@ -733,11 +793,25 @@ int pip_status(pip_ctx *c, int *stop_flag, int *nan_flag) {
 }
 
 int pip_conduction(pip_ctx *c, double dt, int *iters, double *relres) {
-  (void)dt;
   if (!c) return PIP_ERR_NULL;
   if (iters) *iters = 0;
   if (relres) *relres = 0.0;
-  return PIP_ERR_PARAM;  // flag_heat contexts are rejected at creation
+  if (!c->hc) return PIP_ERR_PARAM;      // context created without flag_heat = 1
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  double *hdt = &c->h_ctrl->dt;
+  *hdt = dt;
+  CK(cudaMemcpyAsync(c->d_dt, hdt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int it = 0, st = 0;
+  double rr = 0.0;
+  const int r = conduct(c, c->d_dt, &it, &rr, &st);
+  if (r != PIP_OK) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  c->hc_iters = it;
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+  return st == 0 ? PIP_OK : PIP_ERR_ITER;
 }
 
 int pip_last_cuda_error(void) { return g_last_cuda_error; }

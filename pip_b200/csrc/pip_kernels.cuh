@@ -30,6 +30,7 @@ struct KParams {
   double ir_chi, ir_ion, ir_rec;
   double decay[2];   // Dedner psi factor exp(-(dt_sub/dt)*safety*db_clean) per stage
   double dz0;        // dz(1)
+  double hc_kapper;  // Spitzer coefficient of the implicit conduction (kapper)
   const double *dx, *dy;
   const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]
@@ -69,6 +70,16 @@ const Launchers &launchers_exact();
 
 struct pip_params;
 namespace pip {
+
+// Implicit conduction of the ions (pip_conduction.cu): buffers for one grid; mixed = FP32
+// inner BiCGstab with FP64 iterative refinement.  hc_run works on the FP64 state U (ion
+// planes first) with dt read from the device; the ghost cells of U are left for the caller
+// to fill.  status: 0 or PIP_ERR_ITER.
+struct HcEngine;
+cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out);
+void hc_destroy(HcEngine *e);
+cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, double tol,
+                   int hc_max, cudaStream_t s, int *iters, double *relres, int *status);
 
 // Records a CUDA error code for pip_last_cuda_error (pip_capi.cu).
 void record_cuda_error(int code);

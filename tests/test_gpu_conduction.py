@@ -1,0 +1,106 @@
+"""Implicit anisotropic conduction of the ions (HC(U_m,nvar_m,1) with the 9-point matrix
+and BiCGstab, include/pip_gpu.h pip_conduction) against the oracle, alone and inside whole
+runs with ionisation/recombination, plus the FP32-inner / FP64-refinement form."""
+import numpy as np
+import pytest
+
+from generic_state import generic_state
+from helpers import interior, rel_l1
+from oracle import oracle as O
+from pip_b200 import capi, ics
+from pip_b200.params import PIP_FP64, PIP_MIXED
+
+pytestmark = pytest.mark.gpu
+
+
+def kh_case(nx=48, ny=24, kapper=1.0, tol=1.0e-12, seed=3, **kw):
+    s, _, _ = ics.kelvin_helmholtz(nx, ny, flag_heat=1, kapper=kapper, hc_error=tol,
+                                   hc_max=2000, **kw)
+    Uh, Um = generic_state(s, seed)
+    o = O.Oracle(s, Uh, Um)
+    o.prologue()
+    Uh0, Um0 = o.state()
+    return s, o, Uh0, Um0
+
+
+@pytest.mark.parametrize("kapper", [0.1, 1.0, 10.0])
+def test_conduction_matches_oracle(gpu_lib, kapper):
+    s, o, Uh0, Um0 = kh_case(kapper=kapper)
+    dt, _ = o.cfl()
+    h0, m0 = o.state()
+    st_o, it_o, rr_o = o.conduction(dt)
+    o.fill_ghosts()
+    oh, om = o.state()
+    o.close()
+    with capi.Context(s) as c:
+        c.upload(h0, m0)
+        st, it, rr = c.conduction(dt)
+        c.pipbnd()
+        gh, gm = c.download()
+    assert st_o == 0 and st == 0 and rr <= 1e-12
+    # BiCGstab's iteration count depends on rounding (the GPU sums in another order)
+    assert abs(it - it_o) <= max(3, 0.1 * it_o), (it, it_o)
+    assert rel_l1(interior(gm, s), interior(om, s)).max() <= 1e-10
+    assert np.array_equal(interior(gh, s), interior(oh, s))
+
+
+@pytest.mark.parametrize("bnd", [[1, 1, 2, 2, 1, 1], [10, 10, 10, 10, 1, 1]])
+def test_run_with_conduction_and_ir_matches_oracle(gpu_lib, bnd):
+    s, o, Uh0, Um0 = kh_case(kapper=1.0, flag_bnd=bnd)
+    st_o, t_o, n_o, hist = o.run(nsteps=15, max_hist=15)
+    oh, om = o.state()
+    o.close()
+    with capi.Context(s) as c:
+        c.upload(Uh0, Um0)
+        st, t, n = c.run(nsteps=15)
+        gh, gm = c.download()
+        iters = c.conduction_iterations
+    assert st_o == 0 and st == 0 and n == 15 and iters > 0
+    assert abs(t - t_o) <= 1e-12 * t_o
+    assert max(rel_l1(interior(gh, s), interior(oh, s)).max(),
+               rel_l1(interior(gm, s), interior(om, s)).max()) <= 1e-10
+
+
+def test_mixed_refinement_reaches_fp64_residual(gpu_lib):
+    """FP32 BiCGstab on the correction, FP64 residual and update: same solution as the FP64
+    solve within the residual target."""
+    s, o, Uh0, Um0 = kh_case(kapper=3.0, tol=1.0e-10)
+    dt, _ = o.cfl()
+    h0, m0 = o.state()
+    o.close()
+    out = {}
+    for prec in (PIP_FP64, PIP_MIXED):
+        with capi.Context(s.overrides(precision=prec)) as c:
+            c.upload(h0, m0)
+            st, it, rr = c.conduction(dt)
+            out[prec] = (st, it, rr, c.download())
+    st64, it64, rr64, (h64, m64) = out[PIP_FP64]
+    stmx, itmx, rrmx, (hmx, mmx) = out[PIP_MIXED]
+    assert st64 == 0 and stmx == 0 and rr64 <= 1e-10 and rrmx <= 1e-10
+    # the mixed context stores its state as an FP32 pair (~48 bits): compare the ion energy
+    err = rel_l1(interior(mmx, s), interior(m64, s))[4]
+    print("mixed vs fp64 ion energy", err, "iterations", it64, itmx)
+    assert err <= 1e-8
+
+
+def test_iteration_limit_is_reported(gpu_lib):
+    s, o, Uh0, Um0 = kh_case(kapper=10.0, tol=1.0e-14)
+    dt, _ = o.cfl()
+    h0, m0 = o.state()
+    o.close()
+    with capi.Context(s.overrides(hc_max=3)) as c:
+        c.upload(h0, m0)
+        st, it, rr = c.conduction(dt)
+        assert st == capi.PIP_ERR_ITER and it == 4 and rr > 1e-14
+        st2, _, _ = c.run(nsteps=2)            # the run goes on, as the reference's does
+        assert st2 == 0
+
+
+def test_conduction_rejects_unsupported(gpu_lib):
+    s, _, _ = ics.brio_wu(64, flag_heat=1, kapper=1.0)
+    with pytest.raises(capi.PipError):
+        capi.Context(s)
+    s2, _, _ = ics.orszag_tang(32)
+    with capi.Context(s2) as c:
+        with pytest.raises(capi.PipError):
+            c.conduction(1e-3)
