@@ -27,6 +27,10 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
 * ensemble: 512 seeded 1D two-fluid shock tubes (nx log-uniform in [256, 8192], alpha_c
   log-uniform in [0.1, 1e4]) advanced to t = 0.1 in one persistent launch (FP32-mixed):
   sum over runs of interior cells x steps / device time.
+* conduction: the 2048x1024 partially ionised Kelvin-Helmholtz run with ionisation/
+  recombination and implicit anisotropic conduction (BiCGstab to 1e-10), 1000 steps, plain
+  FP64 and FP32-mixed (FP32 inner solve with FP64 iterative refinement): ms per step,
+  iterations per step, solver time and GB/s per iteration, mixed-vs-FP64 L1.
 """
 from __future__ import annotations
 
@@ -326,6 +330,59 @@ def measure_ensemble(n_runs=512, t_end=0.1):
                                         "chosen by the autotuner on a t=0.002 probe"}
 
 
+# C3 BiCGstab iteration (three kernels): algorithmic bytes per interior cell -- 5 face-factor
+# planes per matrix application; k1 reads p, Ap, r, r0 and writes p', Ap'; k2 reads r, Ap'
+# and writes t; k3 reads x, p', t, b, r0 and writes x', r.
+HC_BYTES_PER_CELL_ITER = {"f64": 8 * (3 * 5 + 6 + 3 + 7), "f32": 4 * (3 * 5 + 6 + 3 + 7)}
+
+
+def measure_conduction(nsteps=1000, kapper=0.01):
+    """C3: 2D partially ionised Kelvin-Helmholtz 2048x1024 with ionisation/recombination and
+    implicit anisotropic conduction (BiCGstab to 1e-10), plain FP64 and FP32-mixed (FP32
+    inner solve, FP64 refinement); the same runs without conduction give the cost of the
+    solver alone."""
+    from pip_b200 import capi, ics
+    from pip_b200.params import PIP_FP64, PIP_MIXED
+    out = {}
+    states = {}
+    for name, prec in (("fp64", PIP_FP64), ("mixed", PIP_MIXED)):
+        res = {}
+        for heat in (1, 0):
+            s, Uh, Um = ics.kelvin_helmholtz(2048, 1024, flag_heat=heat, kapper=kapper,
+                                             hc_error=1e-10, hc_max=5000, precision=prec)
+            with capi.Context(s) as c:
+                c.upload(Uh, Um)
+                c.prologue()
+                st, t, n, ms = c.run_timed(nsteps=nsteps)
+                if st != 0 or n != nsteps:
+                    raise RuntimeError("C3 %s run ended with status %d after %d steps" % (name, st, n))
+                it = c.conduction_iterations if heat else 0
+                if heat:
+                    states[name] = c.download()
+            res[heat] = (ms, it)
+        (ms_h, it), (ms_0, _) = res[1], res[0]
+        us_it = (ms_h - ms_0) * 1e3 / max(it, 1)
+        b = HC_BYTES_PER_CELL_ITER["f64" if prec == PIP_FP64 else "f32"]
+        out[name] = {"ms_per_step": ms_h / nsteps, "ms_per_step_without_conduction": ms_0 / nsteps,
+                     "cell_updates_per_s": 2048 * 1024 * nsteps / (ms_h * 1e-3),
+                     "bicgstab_iterations": it, "iterations_per_step": it / nsteps,
+                     "us_per_iteration": us_it,
+                     "iteration_gbs": b * 2048 * 1024 / (us_it * 1e-6) / 1e9,
+                     "algorithmic_bytes_per_cell_iteration": b}
+    l1 = rel_l1_interior(states["mixed"], states["fp64"], 3)
+    out.update({
+        "workload": "2D partially ionised Kelvin-Helmholtz 2048x1024 (+3 ghosts), periodic x, "
+                    "reflecting y, IR power law chi=5, kapper=%g (kappa_par ~ T^2.5 along B), "
+                    "BiCGstab to relative residual 1e-10, %d steps" % (kapper, nsteps),
+        "mixed_over_fp64": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+        "l1_mixed_vs_fp64_max": float(l1[:13].max()),
+        "l1_mixed_vs_fp64": dict(zip(L1_NAMES[:13], [float(x) for x in l1[:13]])),
+        "how": "device time (CUDA events in the library) of pip_run over %d steps; the solver "
+               "time per iteration is (time with conduction - time without) / iterations, and "
+               "its GB/s counts the algorithmic bytes of the three BiCGstab kernels" % nsteps})
+    return out
+
+
 def rel_l1_interior(a, b, m):
     import numpy as np
     out = []
@@ -348,6 +405,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_GRID, help="grid size (default 1024)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-conduction", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -408,6 +466,7 @@ def main():
         cpu.pop("s_per_step", None)
     adjoint = None if args.no_adjoint else measure_adjoint()
     ensemble = None if args.no_ensemble else measure_ensemble()
+    conduction = None if args.no_conduction else measure_conduction()
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
@@ -445,6 +504,7 @@ def main():
         "cpu_baseline": cpu,
         "adjoint": adjoint,
         "ensemble": ensemble,
+        "conduction": conduction,
         "e2e": e2e,
         "gpu_launches": mix["launches"],
         "clocks": mix["clocks"],

@@ -4,27 +4,41 @@
 // (:468-529), BiCGstab (:187-299, hc_split = 2) and the conversion back (pv2cq_mhd,
 // Scheme_rot.f90:43-79).
 //
+// The matrix is held as face factors rather than nine planes: eta = kapper dt (gm-1) gm / ro
+// per cell, te^2.5 nx nx and te^2.5 nx ny per x-face, te^2.5 ny ny and te^2.5 ny nx per
+// y-face (nx, ny the components of the unit field vector at the face), and per column /
+// row the grid factors 1/(dxc dx), 1/dxc, ...; each kernel rebuilds the nine entries of its
+// row (the reference's combinations and boundary folds) in registers.  That is 5 planes
+// read per matrix application instead of 9; the entries differ from the reference's
+// left-to-right products (eta*te25*n*n/dxc/dx) by rounding only.
+//
 // BiCGstab keeps the reference's structure (the residual is recomputed from the iterate
-// every iteration, so the stopping test sees the true residual).  One iteration is five
+// every iteration, so the stopping test sees the true residual).  One iteration is three
 // kernels over the interior cells:
-//   k0  p  = r + beta (p - omega Ap)                      (from the second iteration)
-//   k1  Ap = A p;             sums (r,r0), (r0,Ap)   -> alpha
-//   k2  t  = r - alpha Ap;    At = A t (t at the neighbours formed on the fly);
-//                             sums (t,At), (At,At)   -> omega
-//   k3  x  = x + alpha p + omega t
-//   k4  r  = b - A x;         sums (r0,r), (r,r)     -> beta, relative residual, stop flag
-// Scalars are reduced by the last block of each kernel to finish (fixed order:
-// deterministic) into a device block; every kernel returns at once when the stop flag is
-// set, so the host launches iterations in groups and reads the flag between groups.
-// Vectors and matrix are templated: FP64 for the plain path; FP32 for the inner solve of
-// the mixed path, whose FP64 outer loop (iterative refinement) recomputes the residual in
-// FP64 and corrects x in FP64 until the FP64 relative residual reaches the target.
+//   k1  p' = r + beta (p - omega Ap)  (p' = p in the first iteration); Ap' = A p';
+//                                                    sums (r,r0), (r0,Ap')  -> alpha
+//   k2  t  = r - alpha Ap';  At = A t;               sums (t,At), (At,At)   -> omega
+//   k3  x' = x + alpha p' + omega t;  r = b - A x';  sums (r0,r), (r,r)     -> beta,
+//       relative residual, stop flag
+// A block owns 128 columns and a range of rows; the inputs of each row are staged into
+// shared memory by bulk async copies several rows ahead, and each thread keeps the 3x3
+// neighbourhood of the vector the matrix is applied to (p', t or x', formed from its inputs
+// once per point) in registers as it walks down its column.  p, Ap and x are
+// double-buffered (iteration i reads buffer i&1 and writes (i+1)&1), so no kernel reads
+// what it writes.  Scalars are reduced by the last block of each kernel to finish (fixed
+// order: deterministic) into a device block; every kernel returns at once when the stop
+// flag is set, so the host launches iterations in groups and reads the flag between
+// groups.  Vectors and matrix are templated: FP64 for the plain path; FP32 (FP32 products
+// and sums, FP64 dot products) for the inner solve of the mixed path, whose FP64 outer
+// loop (iterative refinement) recomputes the residual in FP64 and corrects x in FP64 until
+// the FP64 relative residual reaches the target.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <initializer_list>
 #include <new>
-#include <vector>
 
 #include "pip_kernels.cuh"
 #include "pip_physics.cuh"
@@ -32,8 +46,12 @@
 namespace pip {
 namespace hc {
 
-constexpr int NT = 256;
-constexpr double kEpsi = 1.0e-5;   // HC_rot.f90:17
+constexpr int NT = 256;             // one-thread-per-cell kernels
+constexpr int SX = 128;             // BiCGstab kernels: interior columns (threads) per block
+constexpr int NS = 4;               // pipeline stages (rows staged ahead)
+constexpr int SLOT = 136;           // elements per staged row segment (SX + 2 + alignment)
+constexpr int kWaitLimit = 1 << 22; // polls of an mbarrier before a block gives up
+constexpr double kEpsi = 1.0e-5;    // HC_rot.f90:17
 
 struct Scal {
   double rr, bb;                  // sum r^2, sum b^2
@@ -41,7 +59,7 @@ struct Scal {
   double omegau, omegad, omega;
   double betau, beta;
   double relres, tol;
-  int count, hc_max, done, pad;
+  int count, hc_max, done, fault;
   unsigned int blocks_done;
 };
 
@@ -53,22 +71,87 @@ __device__ __forceinline__ bool interior_cell(const KParams &p, long long t, int
   return true;
 }
 
-// matrix(i,j,:) . v over the stencil (0: (i,j), 1: i-1, 2: i+1, 3: j-1, 4: j+1, 5: (i-1,j-1),
-// 6: (i+1,j-1), 7: (i-1,j+1), 8: (i+1,j+1)), summed left to right.
+// Face-factor planes of the matrix.
+constexpr int NPL = 5;   // 0 eta (cell), 1 fxx, 2 fxy (x-face i-1/2), 3 fyy, 4 fyx (y-face j-1/2)
+
+// The face factors of one row: eta of the cell, (fxx, fxy) of its left (l) and right (r)
+// x-faces, (fyy, fyx) of its lower (d) and upper (u) y-faces, and the grid factors
+// 1/(dx_i dx_{i-1}), 1/(dx_i dx_i), 1/dx_i of its column and the same in y of its row.
 template <typename T>
-__device__ __forceinline__ double apply9(const T *__restrict__ m, const T *__restrict__ v,
-                                         long long q, long long nc, long long ix) {
-  return (double)m[q] * (double)v[q] + (double)m[q + nc] * (double)v[q - 1] +
-         (double)m[q + 2 * nc] * (double)v[q + 1] + (double)m[q + 3 * nc] * (double)v[q - ix] +
-         (double)m[q + 4 * nc] * (double)v[q + ix] + (double)m[q + 5 * nc] * (double)v[q - 1 - ix] +
-         (double)m[q + 6 * nc] * (double)v[q + 1 - ix] + (double)m[q + 7 * nc] * (double)v[q - 1 + ix] +
-         (double)m[q + 8 * nc] * (double)v[q + 1 + ix];
+struct RowFactors {
+  T eta, fxxl, fxxr, fxyl, fxyr, fyyd, fyyu, fyxd, fyxu;
+  T cxl, cxr, idx, cyd, cyu, idy;
+};
+
+// The nine entries of row (i,j), in the reference's neighbour order 0 (i,j), 1 (i-1,j),
+// 2 (i+1,j), 3 (i,j-1), 4 (i,j+1), 5 (i-1,j-1), 6 (i+1,j-1), 7 (i-1,j+1), 8 (i+1,j+1),
+// with set_matrix_boundary's folds on all four sides (HC_rot.f90:468-529; one rank per
+// direction, so every side folds: MPI_rot.f90:123).
+template <typename T>
+__device__ __forceinline__ void entries(const KParams &p, const RowFactors<T> &f, int i, int j,
+                                        T (&c)[9]) {
+  const T eta = f.eta;
+  const T exy = eta * (T(0.25) * f.idx * f.idy);
+  const T bxxl = -(eta * f.fxxl * f.cxl);
+  const T bxxr = -(eta * f.fxxr * f.cxr);
+  const T byyd = -(eta * f.fyyd * f.cyd);
+  const T byyu = -(eta * f.fyyu * f.cyu);
+  const T bxyl = -(exy * f.fxyl);
+  const T bxyr = -(exy * f.fxyr);
+  const T byxd = -(exy * f.fyxd);
+  const T byxu = -(exy * f.fyxu);
+  c[1] = bxxl - (byxu - byxd);
+  c[2] = bxxr + (byxu - byxd);
+  c[3] = byyd - (bxyr - bxyl);
+  c[4] = byyu + (bxyr - bxyl);
+  c[5] = bxyl + byxd;
+  c[6] = -(bxyr + byxd);
+  c[7] = -(bxyl + byxu);
+  c[8] = bxyr + byxu;
+  c[0] = T(1) - (c[1] + c[2] + c[3] + c[4]);
+  if (i == p.m0) {                 // x-minus
+    c[0] = c[1] + c[0]; c[1] = T(0);
+    c[3] = c[3] + c[5]; c[5] = T(0);
+    c[4] = c[4] + c[7]; c[7] = T(0);
+  }
+  if (i == p.m0 + p.nx - 1) {      // x-plus
+    c[0] = c[2] + c[0]; c[2] = T(0);
+    c[3] = c[3] + c[6]; c[6] = T(0);
+    c[4] = c[4] + c[8]; c[8] = T(0);
+  }
+  if (j == p.m1) {                 // y-minus
+    c[0] = c[3] + c[0]; c[3] = T(0);
+    c[1] = c[5] + c[1]; c[5] = T(0);
+    c[2] = c[6] + c[2]; c[6] = T(0);
+  }
+  if (j == p.m1 + p.ny - 1) {      // y-plus
+    c[0] = c[4] + c[0]; c[4] = T(0);
+    c[1] = c[1] + c[7]; c[7] = T(0);
+    c[2] = c[2] + c[8]; c[8] = T(0);
+  }
 }
 
-// Block sums of up to 2 values into part[k*nb + block]; returns true in thread 0 of the last
+// w is the 3x3 neighbourhood [dj+1][di+1] of a vector; sum_n c_n * w_n, n = 0..8 left to
+// right, in T.
+template <typename T>
+__device__ __forceinline__ T stencil(const T (&c)[9], const T (&w)[3][3]) {
+  T s = c[0] * w[1][1];
+  s = s + c[1] * w[1][0];
+  s = s + c[2] * w[1][2];
+  s = s + c[3] * w[0][1];
+  s = s + c[4] * w[2][1];
+  s = s + c[5] * w[0][0];
+  s = s + c[6] * w[0][2];
+  s = s + c[7] * w[2][0];
+  s = s + c[8] * w[2][2];
+  return s;
+}
+
+// Block sums of 2 values into part[k*nb + block]; returns true in thread 0 of the last
 // block to finish, which then holds the totals (summed in block order) in tot[].
+template <int NTB>
 __device__ bool reduce2(double a, double b, double *part, unsigned int *counter, double (&tot)[2]) {
-  __shared__ double s[2][NT / 32];
+  __shared__ double s[2][NTB / 32];
   __shared__ bool s_last;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -84,7 +167,7 @@ __device__ bool reduce2(double a, double b, double *part, unsigned int *counter,
   const unsigned int nb = gridDim.x;
   if (threadIdx.x == 0) {
     double x = 0.0, y = 0.0;
-    for (int k = 0; k < NT / 32; ++k) {
+    for (int k = 0; k < NTB / 32; ++k) {
       x += s[0][k];
       y += s[1][k];
     }
@@ -95,18 +178,18 @@ __device__ bool reduce2(double a, double b, double *part, unsigned int *counter,
   }
   __syncthreads();
   if (!s_last) return false;
-  // the last block: totals in block order (each thread a strided slice, then warp order)
+  // the last block: totals in block order (each thread a strided slice, then a tree)
   __threadfence();
   double x = 0.0, y = 0.0;
-  for (unsigned int k = threadIdx.x; k < nb; k += NT) {
+  for (unsigned int k = threadIdx.x; k < nb; k += NTB) {
     x += part[k];
     y += part[nb + k];
   }
-  __shared__ double s2[2][NT];
+  __shared__ double s2[2][NTB];
   s2[0][threadIdx.x] = x;
   s2[1][threadIdx.x] = y;
   __syncthreads();
-  for (int h = NT / 2; h > 0; h >>= 1) {
+  for (int h = NTB / 2; h > 0; h >>= 1) {
     if ((int)threadIdx.x < h) {
       s2[0][threadIdx.x] += s2[0][threadIdx.x + h];
       s2[1][threadIdx.x] += s2[1][threadIdx.x + h];
@@ -141,227 +224,405 @@ __global__ void setup_kernel(const KParams p, double *U, double *te, double *b, 
   }
 }
 
-// set_matrix_source_MHD2D9 for the interior cells (dxc = dx, dyc = dy) and
-// set_matrix_boundary on all four sides (one rank per direction: every neighbour is -1,
-// MPI_rot.f90:123), folded per cell in the order x-, x+, y-, y+.  Writes the FP64 matrix
-// and, when m32 is given, its FP32 copy.
+// The face factors of set_matrix_source_MHD2D9 (HC_rot.f90:643-739, dxc = dx, dyc = dy):
+// thread (i,j) over i = m0..m0+nx, j = m1..m1+ny writes the x-face i-1/2 of row j (j
+// interior), the y-face j-1/2 of column i (i interior) and eta of cell (i,j) (interior).
+// The face quantities of the reference (bxl, al, nxl, te_xm, ...) are symmetric in the two
+// cells of the face, so each face is computed once.  Writes the FP64 planes and, when m32
+// is given, their FP32 copy.
 __global__ void matrix_kernel(const KParams p, const double *__restrict__ U, const double *__restrict__ te,
                               const double *dtp, double *m64, float *m32) {
-  int i, j;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (!interior_cell(p, t, i, j)) return;
+  const long long w = p.nx + 1;
+  if (t >= w * (p.ny + 1)) return;
+  const int i = p.m0 + (int)(t % w), j = p.m1 + (int)(t / w);
+  const bool row_in = j < p.m1 + p.ny, col_in = i < p.m0 + p.nx;
   const long long nc = p.nc, ix = p.ix;
   const long long q = (long long)j * ix + i;
-  const double *ro = U, *bx = U + 5 * nc, *by = U + 6 * nc, *bz = U + 7 * nc;
-  const double gm = p.gm, dt = *dtp;
-  const double eta = p.hc_kapper * dt * (gm - 1.0) / ro[q] * gm;
-  const double bxl = (bx[q - 1] + bx[q]) / 2.0, bxr = (bx[q + 1] + bx[q]) / 2.0;
-  const double bxd = (bx[q - ix] + bx[q]) / 2.0, bxu = (bx[q + ix] + bx[q]) / 2.0;
-  const double byl = (by[q - 1] + by[q]) / 2.0, byr = (by[q + 1] + by[q]) / 2.0;
-  const double byd = (by[q - ix] + by[q]) / 2.0, byu = (by[q + ix] + by[q]) / 2.0;
-  const double bzl = (bz[q - 1] + bz[q]) / 2.0, bzr = (bz[q + 1] + bz[q]) / 2.0;
-  const double bzd = (bz[q - ix] + bz[q]) / 2.0, bzu = (bz[q + ix] + bz[q]) / 2.0;
-  const double al = fmax(sqrt(bxl * bxl + byl * byl + bzl * bzl), kEpsi);
-  const double ar = fmax(sqrt(bxr * bxr + byr * byr + bzr * bzr), kEpsi);
-  const double ad = fmax(sqrt(bxd * bxd + byd * byd + bzd * bzd), kEpsi);
-  const double au = fmax(sqrt(bxu * bxu + byu * byu + bzu * bzu), kEpsi);
-  const double nxl = bxl / al, nxr = bxr / ar, nxd = bxd / ad, nxu = bxu / au;
-  const double nyl = byl / al, nyr = byr / ar, nyd = byd / ad, nyu = byu / au;
-  const double te_xm = 0.5 * (te[q] + te[q - 1]), te_xp = 0.5 * (te[q] + te[q + 1]);
-  const double te_ym = 0.5 * (te[q] + te[q - ix]), te_yp = 0.5 * (te[q] + te[q + ix]);
-  const double te_xm25 = te_xm * te_xm * sqrt(te_xm), te_xp25 = te_xp * te_xp * sqrt(te_xp);
-  const double te_ym25 = te_ym * te_ym * sqrt(te_ym), te_yp25 = te_yp * te_yp * sqrt(te_yp);
-  const double dxc = p.dx[i], dyc = p.dy[j];
-  const double bxxl = -(eta * te_xm25 * nxl * nxl / dxc / p.dx[i - 1]);
-  const double bxxr = -(eta * te_xp25 * nxr * nxr / dxc / p.dx[i]);
-  const double byyd = -(eta * te_ym25 * nyd * nyd / dyc / p.dy[j - 1]);
-  const double byyu = -(eta * te_yp25 * nyu * nyu / dyc / p.dy[j]);
-  const double bxyl = -(eta / 4.0 / dxc / dyc * nxl * nyl * te_xm25);
-  const double bxyr = -(eta / 4.0 / dxc / dyc * nxr * nyr * te_xp25);
-  const double byxd = -(eta / 4.0 / dxc / dyc * nyd * nxd * te_ym25);
-  const double byxu = -(eta / 4.0 / dxc / dyc * nyu * nxu * te_yp25);
-  double m[9];
-  m[1] = bxxl - (byxu - byxd);
-  m[2] = bxxr + (byxu - byxd);
-  m[3] = byyd - (bxyr - bxyl);
-  m[4] = byyu + (bxyr - bxyl);
-  m[5] = bxyl + byxd;
-  m[6] = -(bxyr + byxd);
-  m[7] = -(bxyl + byxu);
-  m[8] = bxyr + byxu;
-  m[0] = 1.0 - (m[1] + m[2] + m[3] + m[4]);
-  if (i == p.m0) {                 // x-minus
-    m[0] = m[1] + m[0]; m[1] = 0.0;
-    m[3] = m[3] + m[5]; m[5] = 0.0;
-    m[4] = m[4] + m[7]; m[7] = 0.0;
+  const double *bx = U + 5 * nc, *by = U + 6 * nc, *bz = U + 7 * nc;
+  double f[NPL] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int have = 0;
+  auto face = [&](long long o, double &fnn, double &fnt, bool x_face) {
+    const double b1 = (bx[o] + bx[q]) / 2.0, b2 = (by[o] + by[q]) / 2.0, b3 = (bz[o] + bz[q]) / 2.0;
+    const double a = fmax(sqrt(b1 * b1 + b2 * b2 + b3 * b3), kEpsi);
+    const double n1 = b1 / a, n2 = b2 / a;
+    const double tm = 0.5 * (te[q] + te[o]);
+    const double t25 = tm * tm * sqrt(tm);
+    if (x_face) {
+      fnn = t25 * n1 * n1;
+      fnt = n1 * n2 * t25;
+    } else {
+      fnn = t25 * n2 * n2;
+      fnt = n2 * n1 * t25;
+    }
+  };
+  if (row_in) {
+    face(q - 1, f[1], f[2], true);
+    have |= 6;
   }
-  if (i == p.m0 + p.nx - 1) {      // x-plus
-    m[0] = m[2] + m[0]; m[2] = 0.0;
-    m[3] = m[3] + m[6]; m[6] = 0.0;
-    m[4] = m[4] + m[8]; m[8] = 0.0;
+  if (col_in) {
+    face(q - ix, f[3], f[4], false);
+    have |= 24;
   }
-  if (j == p.m1) {                 // y-minus
-    m[0] = m[3] + m[0]; m[3] = 0.0;
-    m[1] = m[5] + m[1]; m[5] = 0.0;
-    m[2] = m[6] + m[2]; m[6] = 0.0;
-  }
-  if (j == p.m1 + p.ny - 1) {      // y-plus
-    m[0] = m[4] + m[0]; m[4] = 0.0;
-    m[1] = m[1] + m[7]; m[7] = 0.0;
-    m[2] = m[2] + m[8]; m[8] = 0.0;
+  if (row_in && col_in) {
+    const double gm = p.gm, dt = *dtp;
+    f[0] = p.hc_kapper * dt * (gm - 1.0) / U[q] * gm;
+    have |= 1;
   }
 #pragma unroll
-  for (int n = 0; n < 9; ++n) m64[q + n * nc] = m[n];
-  if (m32) {
+  for (int n = 0; n < NPL; ++n) {
+    if (!(have >> n & 1)) continue;
+    m64[q + n * nc] = f[n];
+    if (m32) m32[q + n * nc] = (float)f[n];
+  }
+}
+
+// Grid factors per column (1/(dx_i dx_{i-1}), 1/(dx_i dx_i), 1/dx_i: three arrays of ix)
+// and per row (the same in y: three arrays of jx, after the column ones).
+__global__ void geometry_kernel(const KParams p, double *g64, float *g32) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool col = t < p.ix;
+  if (!col && t >= p.ix + p.jx) return;
+  const int k = col ? t : t - p.ix;
+  const int n = col ? p.ix : p.jx;
+  const double *d = col ? p.dx : p.dy;
+  const long long base = col ? 0 : 3LL * p.ix;
+  double v[3] = {0.0, 0.0, 0.0};
+  if (k >= 1) {
+    v[0] = 1.0 / (d[k] * d[k - 1]);
+    v[1] = 1.0 / (d[k] * d[k]);
+    v[2] = 1.0 / d[k];
+  }
+  for (int c = 0; c < 3; ++c) {
+    g64[base + (long long)c * n + k] = v[c];
+    if (g32) g32[base + (long long)c * n + k] = (float)v[c];
+  }
+}
+
+// ---- shared-memory staging by bulk async copies (the TMA engine) on mbarriers ----
+
+__device__ __forceinline__ uint32_t smem_addr(const void *ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Bounded wait on phase `parity` of bar; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int k = 0; k < kWaitLimit; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// The four BiCGstab kernels share one body.  A block owns SX interior columns starting at
+// i0 and a contiguous range of rows [ja, jb); the rows of a column block are divided evenly
+// among its blocks (one wave over the SMs).  For each row j the inputs are staged, NS rows
+// ahead, as row segments copied into shared memory (one bulk copy per segment, one
+// mbarrier per stage):
+//   window vectors (row j+1, columns i0-1 .. i0+SX)   -- the vector A is applied to is
+//                                                        formed from these at each point
+//   own vectors    (row j, columns i0 .. i0+SX-1)
+//   eta (row j), fxx and fxy (row j, columns i0 .. i0+SX: both x-faces of every cell),
+//   fyy and fyx (rows j and j+1: both y-faces).
+// Window rows ja-1 and ja come from plain loads before the pipeline starts.  A segment is
+// copied from its start rounded down to 16 bytes, its length rounded up to 16 bytes and cut
+// at the end of its allocation (conduction runs with at least two ghost rows, so the cut
+// never reaches a value that is used).
+enum Kind { KINIT = 0, K1 = 1, K2 = 2, K3 = 3 };
+template <int KIND> struct KindShape;
+template <> struct KindShape<KINIT> { static constexpr int nw = 1, no = 1; };  // x | b
+template <> struct KindShape<K1> { static constexpr int nw = 3, no = 2; };     // p, Ap, r | r, r0
+template <> struct KindShape<K2> { static constexpr int nw = 2, no = 0; };     // r, Ap' |
+template <> struct KindShape<K3> { static constexpr int nw = 3, no = 2; };     // x, p', t | b, r0
+constexpr int kMatCopies = 7;
+
+template <int KIND>
+__host__ __device__ constexpr int n_copies() {
+  return KindShape<KIND>::nw + KindShape<KIND>::no + kMatCopies;
+}
+
+template <typename T, int KIND>
+__host__ __device__ constexpr size_t stage_smem() {
+  return (size_t)NS * n_copies<KIND>() * SLOT * sizeof(T) + NS * sizeof(unsigned long long);
+}
+
+template <typename T>
+struct BicgArgs {
+  const T *m, *g;            // face-factor planes (NPL*nc) and grid factors
+  const T *w[3];             // window vectors
+  const T *o[2];             // own vectors
+  T *out[3];                 // INIT: r, r0, p;  K1: p', Ap';  K2: t;  K3: x', r
+  double *part;
+  Scal *sc;
+  int ncb, nrb;              // column blocks, row ranges per column block
+};
+
+// Copy c of a row: its source plane, row offset, first column offset (from i0), number of
+// elements and the end of the allocation it lies in.
+template <typename T, int KIND>
+__device__ __forceinline__ void copy_desc(const BicgArgs<T> &a, long long nc, int c, const T *&base,
+                                          int &dj, int &di, int &n, const T *&lim) {
+  constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
+  if (c < NW) {
+    base = a.w[c]; dj = 1; di = -1; n = SX + 2; lim = a.w[c] + nc;
+  } else if (c < NW + NO) {
+    base = a.o[c - NW]; dj = 0; di = 0; n = SX; lim = a.o[c - NW] + nc;
+  } else {
+    const int k = c - NW - NO;     // eta, fxx, fxy, fyy(j), fyy(j+1), fyx(j), fyx(j+1)
+    const int plane = k == 0 ? 0 : (k <= 2 ? k : (k <= 4 ? 3 : 4));
+    base = a.m + plane * nc;
+    dj = (k == 4 || k == 6) ? 1 : 0;
+    di = 0;
+    n = (k == 1 || k == 2) ? SX + 1 : SX;
+    lim = a.m + NPL * nc;
+  }
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArgs<T> a) {
+  constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
+  constexpr int NCP = n_copies<KIND>();
+  Scal *sc = a.sc;
+  if (sc->done) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T *buf = reinterpret_cast<T *>(smem);
+  unsigned long long *bar =
+      reinterpret_cast<unsigned long long *>(smem + (size_t)NS * NCP * SLOT * sizeof(T));
+
+  const int t = threadIdx.x;
+  const int cb = blockIdx.x % a.ncb, rb = blockIdx.x / a.ncb;
+  const int i0 = p.m0 + cb * SX, i = i0 + t;
+  const bool active = i < p.m0 + p.nx;
+  const int ja = p.m1 + (int)((long long)p.ny * rb / a.nrb);
+  const int jb = p.m1 + (int)((long long)p.ny * (rb + 1) / a.nrb);
+  const int nrows = jb - ja;
+  const long long ix = p.ix, nc = p.nc;
+
+  // Warp 0 stages rows: lane c < NCP owns copy c (its source address at row ja, the length
+  // and the allocation end), so a row's copies are set up in parallel.  The first element of
+  // copy c inside its staged segment goes to off[stage][c] for the consumers.
+  __shared__ int off[NS][NCP];
+  const int lane = t & 31;
+  uintptr_t c_addr = 0, c_cap = 0;
+  uint32_t c_len = 0;
+  if (t < 32 && lane < NCP) {
+    const T *base, *lim;
+    int dj, di, n;
+    copy_desc<T, KIND>(a, nc, lane, base, dj, di, n, lim);
+    c_addr = (uintptr_t)(base + ((long long)(ja + dj) * ix + i0 + di));
+    c_len = (uint32_t)(n * sizeof(T));
+    c_cap = (uintptr_t)lim & ~(uintptr_t)15;
+  }
+  const uintptr_t row_bytes = (uintptr_t)ix * sizeof(T);
+  auto issue = [&](int r) {       // warp 0: stage row ja + r
+    const int st = r % NS;
+    const uint32_t bs = smem_addr(&bar[st]);
+    uintptr_t a0 = 0;
+    uint32_t bytes = 0;
+    if (lane < NCP) {
+      const uintptr_t ad = c_addr + (uintptr_t)r * row_bytes;
+      a0 = ad & ~(uintptr_t)15;
+      uintptr_t end = (ad + c_len + 15) & ~(uintptr_t)15;
+      if (end > c_cap) end = c_cap;
+      bytes = (uint32_t)(end - a0);
+      off[st][lane] = (int)((ad - a0) / sizeof(T));
+    }
+    uint32_t total = bytes;
 #pragma unroll
-    for (int n = 0; n < 9; ++n) m32[q + n * nc] = (float)m[n];
-  }
-}
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    if (lane == 0) mbar_expect_tx(bs, total);
+    __syncwarp();
+    if (lane < NCP)
+      bulk_load(smem_addr(buf + ((size_t)st * NCP + lane) * SLOT), (const void *)a0, bytes, bs);
+  };
 
-// r = b - A x (term by term, as the reference's initial residual), r0 = r, p = r;
-// totals (r,r), (b,b); the stop test of the loop head.
-template <typename T>
-__global__ void __launch_bounds__(NT) init_kernel(const KParams p, const T *__restrict__ m,
-                                                   const T *__restrict__ x, const T *__restrict__ b,
-                                                   T *r, T *r0, T *pv, double *part, Scal *sc) {
-  int i, j;
-  double rr = 0.0, bb = 0.0;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (interior_cell(p, t, i, j)) {
-    const long long nc = p.nc, ix = p.ix;
-    const long long q = (long long)j * ix + i;
-    double v = (double)b[q];
-    v = v - (double)m[q] * (double)x[q];
-    v = v - (double)m[q + nc] * (double)x[q - 1];
-    v = v - (double)m[q + 2 * nc] * (double)x[q + 1];
-    v = v - (double)m[q + 3 * nc] * (double)x[q - ix];
-    v = v - (double)m[q + 4 * nc] * (double)x[q + ix];
-    v = v - (double)m[q + 5 * nc] * (double)x[q - 1 - ix];
-    v = v - (double)m[q + 6 * nc] * (double)x[q + 1 - ix];
-    v = v - (double)m[q + 7 * nc] * (double)x[q - 1 + ix];
-    v = v - (double)m[q + 8 * nc] * (double)x[q + 1 + ix];
-    const T vt = (T)v;
-    r[q] = vt;
-    r0[q] = vt;
-    pv[q] = vt;
-    rr = (double)vt * (double)vt;
-    bb = (double)b[q] * (double)b[q];
+  if (t == 0) {
+    for (int st = 0; st < NS; ++st) mbar_init(smem_addr(&bar[st]), 1u);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (t < 32)
+    for (int r = 0; r < NS && r < nrows; ++r) issue(r);
+  __syncthreads();                // off[][] of the first stages
+
+  // scalars of the update formed at each point
+  T s1 = T(0), s2 = T(0);
+  bool first = false;
+  if (KIND == K1) {
+    first = sc->count == 0;
+    s1 = (T)sc->beta;
+    s2 = (T)sc->omega;
+  } else if (KIND == K2) {
+    s1 = (T)sc->alpha;
+  } else if (KIND == K3) {
+    s1 = (T)sc->alpha;
+    s2 = (T)sc->omega;
+  }
+  auto form = [&](const T (&v)[3]) -> T {
+    if (KIND == KINIT) return v[0];
+    if (KIND == K1) return first ? v[0] : v[2] + s1 * (v[0] - s2 * v[1]);
+    if (KIND == K2) return v[0] - s1 * v[1];
+    return v[0] + s1 * v[1] + s2 * v[2];
+  };
+
+  T w[3][3];
+  RowFactors<T> f;
+  if (active && nrows > 0) {
+#pragma unroll
+    for (int dr = 0; dr < 2; ++dr)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const long long k = (long long)(ja - 1 + dr) * ix + i - 1 + d;
+        T v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = c < NW ? a.w[c][k] : T(0);
+        w[dr][d] = form(v);
+      }
+    f.cxl = a.g[i];
+    f.cxr = a.g[ix + i];
+    f.idx = a.g[2 * ix + i];
+  }
+  const T *gy = a.g + 3 * ix;
+  double acc0 = 0.0, acc1 = 0.0;
+  bool fault = false;
+  int r = 0;
+  for (; r < nrows; ++r) {
+    const int st = r % NS, j = ja + r;
+    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((r / NS) & 1));
+    if (__syncthreads_or(!ok)) {
+      fault = true;
+      break;
+    }
+    const T *sb = buf + (size_t)st * NCP * SLOT;
+    if (active) {
+      const long long q = (long long)j * ix + i;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        T v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = c < NW ? sb[c * SLOT + off[st][c] + t + d] : T(0);
+        w[2][d] = form(v);
+      }
+      T own[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+        own[c] = c < NO ? sb[(NW + c) * SLOT + off[st][NW + c] + t] : T(0);
+      constexpr int mc = NW + NO;
+      f.eta = sb[mc * SLOT + off[st][mc] + t];
+      f.fxxl = sb[(mc + 1) * SLOT + off[st][mc + 1] + t];
+      f.fxxr = sb[(mc + 1) * SLOT + off[st][mc + 1] + t + 1];
+      f.fxyl = sb[(mc + 2) * SLOT + off[st][mc + 2] + t];
+      f.fxyr = sb[(mc + 2) * SLOT + off[st][mc + 2] + t + 1];
+      f.fyyd = sb[(mc + 3) * SLOT + off[st][mc + 3] + t];
+      f.fyyu = sb[(mc + 4) * SLOT + off[st][mc + 4] + t];
+      f.fyxd = sb[(mc + 5) * SLOT + off[st][mc + 5] + t];
+      f.fyxu = sb[(mc + 6) * SLOT + off[st][mc + 6] + t];
+      f.cyd = gy[j];
+      f.cyu = gy[p.jx + j];
+      f.idy = gy[2 * p.jx + j];
+      T c[9];
+      entries(p, f, i, j, c);
+      if (KIND == KINIT) {
+        // r = b - A x term by term, as the reference's initial residual
+        const T bq = own[0];
+        T v = bq;
+        v = v - c[0] * w[1][1];
+        v = v - c[1] * w[1][0];
+        v = v - c[2] * w[1][2];
+        v = v - c[3] * w[0][1];
+        v = v - c[4] * w[2][1];
+        v = v - c[5] * w[0][0];
+        v = v - c[6] * w[0][2];
+        v = v - c[7] * w[2][0];
+        v = v - c[8] * w[2][2];
+        a.out[0][q] = v;
+        a.out[1][q] = v;
+        a.out[2][q] = v;
+        acc0 += (double)v * (double)v;
+        acc1 += (double)bq * (double)bq;
+      } else if (KIND == K1) {
+        a.out[0][q] = w[1][1];
+        const T av = stencil(c, w);
+        a.out[1][q] = av;
+        const double r0q = (double)own[1];
+        acc0 += (double)own[0] * r0q;
+        acc1 += r0q * (double)av;
+      } else if (KIND == K2) {
+        a.out[0][q] = w[1][1];
+        const T at = stencil(c, w);
+        acc0 += (double)w[1][1] * (double)at;
+        acc1 += (double)at * (double)at;
+      } else {
+        a.out[0][q] = w[1][1];
+        const T v = own[0] - stencil(c, w);
+        a.out[1][q] = v;
+        acc0 += (double)own[1] * (double)v;
+        acc1 += (double)v * (double)v;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        w[0][d] = w[1][d];
+        w[1][d] = w[2][d];
+      }
+    }
+    __syncthreads();              // stage st is free again
+    if (t < 32 && r + NS < nrows) issue(r + NS);
+  }
+  if (fault) {
+    // a staged row never arrived: flag it, let the copies still in flight land (bounded),
+    // and leave the scalars alone (the host reads the flag and stops)
+    if (t == 0) {
+      atomicExch(&sc->fault, 1);
+      for (int k = r; k < nrows && k < r + NS; ++k)
+        mbar_wait(smem_addr(&bar[k % NS]), (uint32_t)((k / NS) & 1));
+    }
+    return;
   }
   double tot[2];
-  if (reduce2(rr, bb, part, &sc->blocks_done, tot)) {
-    sc->rr = tot[0];
-    sc->bb = tot[1];
-    sc->count = 0;
-    sc->relres = tot[1] > 0.0 ? sqrt(tot[0] / tot[1]) : 0.0;
-    sc->done = !(sc->relres > sc->tol && sc->count <= sc->hc_max);
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NT) k0_kernel(const KParams p, const T *__restrict__ r, T *pv,
-                                                 const T *__restrict__ ap, const Scal *sc) {
-  if (sc->done || sc->count == 0) return;
-  int i, j;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (!interior_cell(p, t, i, j)) return;
-  const long long q = (long long)j * p.ix + i;
-  const double beta = sc->beta, omega = sc->omega;
-  pv[q] = (T)((double)r[q] + beta * ((double)pv[q] - omega * (double)ap[q]));
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NT) k1_kernel(const KParams p, const T *__restrict__ m,
-                                                 const T *__restrict__ pv, const T *__restrict__ r,
-                                                 const T *__restrict__ r0, T *ap, double *part, Scal *sc) {
-  if (sc->done) return;
-  int i, j;
-  double au = 0.0, ad = 0.0;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (interior_cell(p, t, i, j)) {
-    const long long q = (long long)j * p.ix + i;
-    const T a = (T)apply9(m, pv, q, p.nc, p.ix);
-    ap[q] = a;
-    au = (double)r[q] * (double)r0[q];
-    ad = (double)r0[q] * (double)a;
-  }
-  double tot[2];
-  if (reduce2(au, ad, part, &sc->blocks_done, tot)) {
-    sc->alphau = tot[0];
-    sc->alphad = tot[1];
-    sc->alpha = tot[0] / tot[1];
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NT) k2_kernel(const KParams p, const T *__restrict__ m,
-                                                 const T *__restrict__ r, const T *__restrict__ ap,
-                                                 T *tv, double *part, Scal *sc) {
-  if (sc->done) return;
-  int i, j;
-  double ou = 0.0, od = 0.0;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (interior_cell(p, t, i, j)) {
-    const long long nc = p.nc, ix = p.ix;
-    const long long q = (long long)j * ix + i;
-    const double alpha = sc->alpha;
-    // t = r - alpha Ap at the cell and its neighbours (outside the interior the matrix
-    // entries are zero and Ap, r are zero)
-    auto tt = [&](long long k) { return (T)((double)r[k] - alpha * (double)ap[k]); };
-    const T t0 = tt(q);
-    tv[q] = t0;
-    const double at = (double)m[q] * (double)t0 + (double)m[q + nc] * (double)tt(q - 1) +
-                      (double)m[q + 2 * nc] * (double)tt(q + 1) + (double)m[q + 3 * nc] * (double)tt(q - ix) +
-                      (double)m[q + 4 * nc] * (double)tt(q + ix) +
-                      (double)m[q + 5 * nc] * (double)tt(q - 1 - ix) +
-                      (double)m[q + 6 * nc] * (double)tt(q + 1 - ix) +
-                      (double)m[q + 7 * nc] * (double)tt(q - 1 + ix) +
-                      (double)m[q + 8 * nc] * (double)tt(q + 1 + ix);
-    const double atr = (double)(T)at;
-    ou = (double)t0 * atr;
-    od = atr * atr;
-  }
-  double tot[2];
-  if (reduce2(ou, od, part, &sc->blocks_done, tot)) {
-    sc->omegau = tot[0];
-    sc->omegad = tot[1];
-    sc->omega = tot[0] / tot[1];
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NT) k3_kernel(const KParams p, T *x, const T *__restrict__ pv,
-                                                 const T *__restrict__ tv, const Scal *sc) {
-  if (sc->done) return;
-  int i, j;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (!interior_cell(p, t, i, j)) return;
-  const long long q = (long long)j * p.ix + i;
-  x[q] = (T)((double)x[q] + sc->alpha * (double)pv[q] + sc->omega * (double)tv[q]);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NT) k4_kernel(const KParams p, const T *__restrict__ m,
-                                                 const T *__restrict__ x, const T *__restrict__ b,
-                                                 const T *__restrict__ r0, T *r, double *part, Scal *sc) {
-  if (sc->done) return;
-  int i, j;
-  double bu = 0.0, rr = 0.0;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (interior_cell(p, t, i, j)) {
-    const long long q = (long long)j * p.ix + i;
-    const T v = (T)((double)b[q] - apply9(m, x, q, p.nc, p.ix));
-    r[q] = v;
-    bu = (double)r0[q] * (double)v;
-    rr = (double)v * (double)v;
-  }
-  double tot[2];
-  if (reduce2(bu, rr, part, &sc->blocks_done, tot)) {
-    sc->betau = tot[0];
-    sc->rr = tot[1];
-    sc->beta = tot[0] / sc->alphau * sc->alpha / sc->omega;
-    sc->count = sc->count + 1;
-    sc->relres = sqrt(tot[1] / sc->bb);
-    sc->done = !(sc->relres > sc->tol && sc->count <= sc->hc_max);
+  if (reduce2<SX>(acc0, acc1, a.part, &sc->blocks_done, tot)) {
+    if (KIND == KINIT) {
+      sc->rr = tot[0];
+      sc->bb = tot[1];
+      sc->count = 0;
+      sc->relres = tot[1] > 0.0 ? sqrt(tot[0] / tot[1]) : 0.0;
+      sc->done = !(sc->relres > sc->tol && sc->count <= sc->hc_max);
+    } else if (KIND == K1) {
+      sc->alphau = tot[0];
+      sc->alphad = tot[1];
+      sc->alpha = tot[0] / tot[1];
+    } else if (KIND == K2) {
+      sc->omegau = tot[0];
+      sc->omegad = tot[1];
+      sc->omega = tot[0] / tot[1];
+    } else {
+      sc->betau = tot[0];
+      sc->rr = tot[1];
+      sc->beta = tot[0] / sc->alphau * sc->alpha / sc->omega;
+      sc->count = sc->count + 1;
+      sc->relres = sqrt(tot[1] / sc->bb);
+      sc->done = !(sc->relres > sc->tol && sc->count <= sc->hc_max);
+    }
   }
 }
 
@@ -398,20 +659,81 @@ __global__ void set_scal_kernel(Scal *sc, double tol, int hc_max) {
   sc->tol = tol;
   sc->hc_max = hc_max;
   sc->done = 0;
+  sc->fault = 0;
   sc->count = 0;
   sc->blocks_done = 0u;
+}
+
+// One wave of BiCGstab blocks: ncb column blocks x nrb row ranges.
+struct Grid {
+  int ncb = 1, nrb = 1, nb = 1;
+};
+
+template <typename T, int KIND>
+cudaError_t kind_blocks(int *bps) {
+  const size_t smem = stage_smem<T, KIND>();
+  cudaError_t err = cudaFuncSetAttribute(bicg_kernel<T, KIND>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int n = 0;
+  if (err == cudaSuccess)
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bicg_kernel<T, KIND>, SX, smem);
+  if (err == cudaSuccess) *bps = std::min(*bps, std::max(n, 1));
+  return err;
+}
+
+// The grid of the four kernels of precision T: as many row ranges per column block as fill
+// every SM at the occupancy of the most demanding kernel.
+template <typename T>
+cudaError_t make_grid(const KParams &k, int sms, Grid *g) {
+  int bps = 1 << 20;
+  cudaError_t err = kind_blocks<T, KINIT>(&bps);
+  if (err == cudaSuccess) err = kind_blocks<T, K1>(&bps);
+  if (err == cudaSuccess) err = kind_blocks<T, K2>(&bps);
+  if (err == cudaSuccess) err = kind_blocks<T, K3>(&bps);
+  if (err != cudaSuccess) return err;
+  g->ncb = (k.nx + SX - 1) / SX;
+  g->nrb = std::max(1, std::min(k.ny, sms * bps / g->ncb));
+  g->nb = g->ncb * g->nrb;
+  return cudaSuccess;
+}
+
+template <typename T, int KIND>
+void launch(const Grid &g, const KParams &k, BicgArgs<T> a, cudaStream_t s) {
+  a.ncb = g.ncb;
+  a.nrb = g.nrb;
+  bicg_kernel<T, KIND><<<g.nb, SX, stage_smem<T, KIND>(), s>>>(k, a);
+}
+
+template <typename T>
+BicgArgs<T> make_args(const T *m, const T *g, std::initializer_list<const T *> w,
+                      std::initializer_list<const T *> o, std::initializer_list<T *> out,
+                      double *part, Scal *sc) {
+  BicgArgs<T> a{};
+  a.m = m;
+  a.g = g;
+  int n = 0;
+  for (const T *v : w) a.w[n++] = v;
+  n = 0;
+  for (const T *v : o) a.o[n++] = v;
+  n = 0;
+  for (T *v : out) a.out[n++] = v;
+  a.part = part;
+  a.sc = sc;
+  return a;
 }
 
 }  // namespace hc
 
 struct HcEngine {
   long long nc = 0;
-  int nb = 0;                       // blocks over the interior
+  hc::Grid grid64, grid32;          // BiCGstab grids of the FP64 and FP32 kernels
   bool mixed = false;
-  double *m64 = nullptr, *te = nullptr, *b = nullptr, *kin = nullptr, *mag = nullptr;
-  double *r = nullptr, *r0 = nullptr, *p = nullptr, *ap = nullptr, *t = nullptr;
-  float *m32 = nullptr, *d = nullptr, *b32 = nullptr, *r32 = nullptr, *r032 = nullptr,
-        *p32 = nullptr, *ap32 = nullptr, *t32 = nullptr;
+  double *m64 = nullptr, *g64 = nullptr, *b = nullptr, *kin = nullptr, *mag = nullptr;
+  double *x[2] = {nullptr, nullptr}, *p[2] = {nullptr, nullptr}, *ap[2] = {nullptr, nullptr};
+  double *r = nullptr, *r0 = nullptr, *t = nullptr;
+  float *m32 = nullptr, *g32 = nullptr, *b32 = nullptr, *r32 = nullptr, *r032 = nullptr,
+        *t32 = nullptr;
+  float *x32[2] = {nullptr, nullptr}, *p32[2] = {nullptr, nullptr}, *ap32[2] = {nullptr, nullptr};
   double *part = nullptr;
   hc::Scal *sc = nullptr, *sc32 = nullptr;
   hc::Scal *h_sc = nullptr;         // pinned
@@ -419,9 +741,10 @@ struct HcEngine {
 
 void hc_destroy(HcEngine *e) {
   if (!e) return;
-  void *bufs[] = {e->m64, e->te, e->b, e->kin, e->mag, e->r, e->r0, e->p, e->ap, e->t,
-                  e->m32, e->d, e->b32, e->r32, e->r032, e->p32, e->ap32, e->t32,
-                  e->part, e->sc, e->sc32};
+  void *bufs[] = {e->m64, e->g64, e->b, e->kin, e->mag, e->x[0], e->x[1], e->p[0], e->p[1],
+                  e->ap[0], e->ap[1], e->r, e->r0, e->t, e->m32, e->g32, e->b32, e->r32,
+                  e->r032, e->t32, e->x32[0], e->x32[1], e->p32[0], e->p32[1], e->ap32[0],
+                  e->ap32[1], e->part, e->sc, e->sc32};
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (e->h_sc) cudaFreeHost(e->h_sc);
@@ -430,14 +753,23 @@ void hc_destroy(HcEngine *e) {
 
 cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out) {
   *out = nullptr;
+  // the staged row segments reach up to two ghost rows past the interior
+  if (k.m0 < 2 || k.m1 < 2) return cudaErrorInvalidValue;
   HcEngine *e = new (std::nothrow) HcEngine();
   if (!e) return cudaErrorMemoryAllocation;
   e->nc = k.nc;
   e->mixed = mixed;
-  const long long n = (long long)k.nx * k.ny;
-  e->nb = (int)((n + hc::NT - 1) / hc::NT);
+  int dev = 0, sms = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (err == cudaSuccess) err = hc::make_grid<double>(k, sms, &e->grid64);
+  if (err == cudaSuccess && mixed) err = hc::make_grid<float>(k, sms, &e->grid32);
+  if (err != cudaSuccess) {
+    delete e;
+    return err;
+  }
   const size_t dv = sizeof(double) * (size_t)k.nc, fv = sizeof(float) * (size_t)k.nc;
-  cudaError_t err = cudaSuccess;
+  const size_t ng = 3 * ((size_t)k.ix + (size_t)k.jx);
   auto md = [&](double **p, size_t bytes) {
     if (err == cudaSuccess) err = cudaMalloc(p, bytes);
     if (err == cudaSuccess) err = cudaMemset(*p, 0, bytes);
@@ -446,15 +778,22 @@ cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out) {
     if (err == cudaSuccess) err = cudaMalloc(p, bytes);
     if (err == cudaSuccess) err = cudaMemset(*p, 0, bytes);
   };
-  md(&e->m64, 9 * dv);
-  md(&e->te, dv); md(&e->b, dv); md(&e->kin, dv); md(&e->mag, dv);
-  md(&e->r, dv); md(&e->r0, dv); md(&e->p, dv); md(&e->ap, dv); md(&e->t, dv);
-  if (mixed) {
-    mf(&e->m32, 9 * fv);
-    mf(&e->d, fv); mf(&e->b32, fv); mf(&e->r32, fv); mf(&e->r032, fv);
-    mf(&e->p32, fv); mf(&e->ap32, fv); mf(&e->t32, fv);
+  md(&e->m64, hc::NPL * dv);
+  md(&e->g64, sizeof(double) * ng);
+  md(&e->b, dv); md(&e->kin, dv); md(&e->mag, dv);
+  for (int h = 0; h < 2; ++h) {
+    md(&e->x[h], dv); md(&e->p[h], dv); md(&e->ap[h], dv);
   }
-  md(&e->part, sizeof(double) * 2 * (size_t)e->nb);
+  md(&e->r, dv); md(&e->r0, dv); md(&e->t, dv);
+  if (mixed) {
+    mf(&e->m32, hc::NPL * fv);
+    mf(&e->g32, sizeof(float) * ng);
+    mf(&e->b32, fv); mf(&e->r32, fv); mf(&e->r032, fv); mf(&e->t32, fv);
+    for (int h = 0; h < 2; ++h) {
+      mf(&e->x32[h], fv); mf(&e->p32[h], fv); mf(&e->ap32[h], fv);
+    }
+  }
+  md(&e->part, sizeof(double) * 2 * (size_t)std::max(e->grid64.nb, e->grid32.nb));
   if (err == cudaSuccess) err = cudaMalloc(&e->sc, sizeof(hc::Scal));
   if (err == cudaSuccess) err = cudaMemset(e->sc, 0, sizeof(hc::Scal));
   if (err == cudaSuccess) err = cudaMalloc(&e->sc32, sizeof(hc::Scal));
@@ -470,33 +809,49 @@ cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out) {
 
 namespace {
 
-// BiCGstab on the interior cells until the stop flag of sc is set; the host reads the flag
-// every `group` iterations.  Returns the scalars block (count, relres) in *h.
+// BiCGstab on the interior cells from x[0] until the stop flag of sc is set; the host reads
+// the flag every `group` iterations.  On return h holds the scalars; the iterate is in
+// x[h->count & 1].
 template <typename T>
-cudaError_t bicgstab(HcEngine *e, const KParams &k, const T *m, T *x, const T *b, T *r, T *r0, T *pv,
-                     T *ap, T *tv, hc::Scal *sc, double tol, int hc_max, cudaStream_t s,
-                     hc::Scal *h) {
+cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T *m, const T *g,
+                     T *const (&x)[2], const T *b, T *r, T *r0, T *const (&pv)[2],
+                     T *const (&ap)[2], T *tv, hc::Scal *sc, double tol, int hc_max,
+                     cudaStream_t s, hc::Scal *h) {
   using namespace hc;
-  const int nb = e->nb;
   set_scal_kernel<<<1, 1, 0, s>>>(sc, tol, hc_max);
-  init_kernel<T><<<nb, NT, 0, s>>>(k, m, x, b, r, r0, pv, e->part, sc);
+  launch<T, KINIT>(gr, k, make_args<T>(m, g, {x[0]}, {b}, {r, r0, pv[0]}, e->part, sc), s);
   const int group = 4;
   for (int it = 0; it <= hc_max; it += group) {
-    for (int g = 0; g < group; ++g) {
-      k0_kernel<T><<<nb, NT, 0, s>>>(k, r, pv, ap, sc);
-      k1_kernel<T><<<nb, NT, 0, s>>>(k, m, pv, r, r0, ap, e->part, sc);
-      k2_kernel<T><<<nb, NT, 0, s>>>(k, m, r, ap, tv, e->part, sc);
-      k3_kernel<T><<<nb, NT, 0, s>>>(k, x, pv, tv, sc);
-      k4_kernel<T><<<nb, NT, 0, s>>>(k, m, x, b, r0, r, e->part, sc);
+    for (int u = 0; u < group; ++u) {
+      const int a = (it + u) & 1, z = a ^ 1;
+      launch<T, K1>(gr, k, make_args<T>(m, g, {pv[a], ap[a], r}, {r, r0}, {pv[z], ap[z]}, e->part, sc), s);
+      launch<T, K2>(gr, k, make_args<T>(m, g, {r, ap[z]}, {}, {tv}, e->part, sc), s);
+      launch<T, K3>(gr, k, make_args<T>(m, g, {x[a], pv[z], tv}, {b, r0}, {x[z], r}, e->part, sc), s);
     }
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     err = cudaMemcpyAsync(h, sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) return err;
+    if (h->fault) return cudaErrorLaunchTimeout;
     if (h->done) break;
   }
   return cudaSuccess;
+}
+
+// The FP64 residual r = b - A x[0] (r0 = p = r as well) and its scalars into h.
+cudaError_t residual64(HcEngine *e, const KParams &k, double tol, cudaStream_t s, hc::Scal *h) {
+  using namespace hc;
+  set_scal_kernel<<<1, 1, 0, s>>>(e->sc, tol, 0);
+  launch<double, KINIT>(e->grid64, k,
+                        make_args<double>(e->m64, e->g64, {e->x[0]}, {e->b}, {e->r, e->r0, e->p[0]},
+                                          e->part, e->sc),
+                        s);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaMemcpyAsync(h, e->sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err == cudaSuccess && h->fault) err = cudaErrorLaunchTimeout;
+  return err;
 }
 
 }  // namespace
@@ -506,46 +861,50 @@ cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, 
   using namespace hc;
   const long long nc = k.nc;
   const int gu = (int)std::min<long long>((nc + 255) / 256, 148 * 8);
-  setup_kernel<<<gu, 256, 0, s>>>(k, U, e->te, e->b, e->kin, e->mag);
-  matrix_kernel<<<e->nb, NT, 0, s>>>(k, U, e->te, dtp, e->m64, e->mixed ? e->m32 : nullptr);
+  const int gi = (int)(((long long)k.nx * k.ny + NT - 1) / NT);
+  const int gf = (int)(((long long)(k.nx + 1) * (k.ny + 1) + NT - 1) / NT);
+  setup_kernel<<<gu, 256, 0, s>>>(k, U, e->x[0], e->b, e->kin, e->mag);
+  matrix_kernel<<<gf, NT, 0, s>>>(k, U, e->x[0], dtp, e->m64, e->mixed ? e->m32 : nullptr);
+  geometry_kernel<<<(k.ix + k.jx + NT - 1) / NT, NT, 0, s>>>(k, e->g64, e->mixed ? e->g32 : nullptr);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   int total = 0;
   Scal *h = e->h_sc;
+  const double *xf = e->x[0];
   if (!e->mixed) {
-    err = bicgstab<double>(e, k, e->m64, e->te, e->b, e->r, e->r0, e->p, e->ap, e->t, e->sc, tol,
-                           hc_max, s, h);
+    err = bicgstab<double>(e, e->grid64, k, e->m64, e->g64, e->x, e->b, e->r, e->r0, e->p, e->ap,
+                           e->t, e->sc, tol, hc_max, s, h);
     if (err != cudaSuccess) return err;
     total = h->count;
+    xf = e->x[h->count & 1];
   } else {
     // iterative refinement: FP64 residual of the FP64 matrix, FP32 BiCGstab on the
-    // correction, FP64 update; at most hc_max inner iterations in total
+    // correction, FP64 update of x[0]; at most hc_max inner iterations in total
     const double inner_tol = 1.0e-4;
+    bool fp64_scalars = false;      // h holds the FP64 residual of the current x[0]
     for (int outer = 0; outer < 32; ++outer) {
-      set_scal_kernel<<<1, 1, 0, s>>>(e->sc, tol, 0);
-      init_kernel<double><<<e->nb, NT, 0, s>>>(k, e->m64, e->te, e->b, e->r, e->r0, e->p, e->part,
-                                               e->sc);
-      err = cudaMemcpyAsync(h, e->sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
-      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      err = residual64(e, k, tol, s, h);
       if (err != cudaSuccess) return err;
+      fp64_scalars = true;
       if (!(h->relres > tol) || total > hc_max) break;
-      cast_kernel<<<e->nb, NT, 0, s>>>(k, e->r, e->b32);
-      cudaMemsetAsync(e->d, 0, sizeof(float) * (size_t)nc, s);
-      err = bicgstab<float>(e, k, e->m32, e->d, e->b32, e->r32, e->r032, e->p32, e->ap32, e->t32,
-                            e->sc32, inner_tol, std::max(1, hc_max - total), s, h);
+      cast_kernel<<<gi, NT, 0, s>>>(k, e->r, e->b32);
+      err = cudaMemsetAsync(e->x32[0], 0, sizeof(float) * (size_t)nc, s);
       if (err != cudaSuccess) return err;
+      err = bicgstab<float>(e, e->grid32, k, e->m32, e->g32, e->x32, e->b32, e->r32, e->r032,
+                            e->p32, e->ap32, e->t32, e->sc32, inner_tol,
+                            std::max(1, hc_max - total), s, h);
+      if (err != cudaSuccess) return err;
+      fp64_scalars = false;
       total += h->count;
-      correct_kernel<<<e->nb, NT, 0, s>>>(k, e->te, e->d);
+      correct_kernel<<<gi, NT, 0, s>>>(k, e->x[0], e->x32[h->count & 1]);
     }
-    // the FP64 residual of the final iterate
-    set_scal_kernel<<<1, 1, 0, s>>>(e->sc, tol, 0);
-    init_kernel<double><<<e->nb, NT, 0, s>>>(k, e->m64, e->te, e->b, e->r, e->r0, e->p, e->part,
-                                             e->sc);
-    err = cudaMemcpyAsync(h, e->sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    if (err != cudaSuccess) return err;
+    if (!fp64_scalars) {
+      // the FP64 residual of the final iterate
+      err = residual64(e, k, tol, s, h);
+      if (err != cudaSuccess) return err;
+    }
   }
-  writeback_kernel<<<e->nb, NT, 0, s>>>(k, U, e->te, e->kin, e->mag);
+  writeback_kernel<<<gi, NT, 0, s>>>(k, U, xf, e->kin, e->mag);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   if (iters) *iters = total;
