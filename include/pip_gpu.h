@@ -204,6 +204,41 @@ int pip_status(pip_ctx *ctx, int *stop_flag, int *nan_flag);
  * final relative residual. */
 int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
 
+/*
+ * Domain decomposition over ranks (one context per rank and device, each holding its own
+ * block with ghost cells, as the Fortran code does after set_mpi, MPI_rot.f90:11-41).
+ *
+ * pip_set_neighbors replaces set_mpi_neighbor (MPI_rot.f90:90-126): neighbor[f] for faces
+ * f = 0 (x-), 1 (x+), 2 (y-), 3 (y+) is the rank owning the block across the face, or -1
+ * where the face is a physical boundary (faces beyond ndim must be -1).  Faces with a
+ * neighbour get their ghost layers only from the halo exchange: the stage kernels and
+ * pip_fill_ghosts apply flag_bnd to the other faces, as MHDbnd/HDbnd skip faces whose
+ * neighbor is not -1 (Boundary_rot.f90:80-90).  With a neighbour on any face, pip_step and
+ * pip_run return PIP_ERR_STATE (the exchange must come between the stages: step with
+ * pip_stage), and implicit conduction (flag_heat = 1) is not supported (PIP_ERR_PARAM).
+ *
+ * pip_stage runs one RK stage of run_solver (Solver_rot.f90:59-71) with the given dt and
+ * Dedner speed cmax: stage 1 then stage 2, each followed by PIPbnd's exchange
+ * (pip_halo_pack / pip_halo_unpack on every face with a neighbour).  dt is the global one
+ * (cfl's MPI_Allreduce MIN of the ranks' pip_cfl values, Scheme_rot.f90:201-202) and cmax
+ * the maximum over ranks of safety*min(dx,dy,dz)/dt (:207-209).
+ *
+ * pip_halo_pack / pip_halo_unpack are the two halves of mpi_bnd (MPI_rot.f90:128-339):
+ * pack copies the margin interior layers next to face f (all planes of the state the last
+ * stage wrote, ghost cells of the other direction included) into `send`; unpack writes a
+ * message received from the neighbour across face f into the ghost layers of face f.  A
+ * message packed at face f is unpacked by the neighbour at the opposite face (f ^ 1).
+ * send and recv are DEVICE buffers of at least pip_halo_bytes(ctx, f) bytes; *bytes gets
+ * the message length, which the receiver passes to unpack (FP64 form: margin x extent x
+ * (nvar_m + 5) doubles; FP32-mixed form after stage 1: half of that).  Both calls return
+ * when the copy is complete.
+ */
+int pip_set_neighbors(pip_ctx *ctx, const int neighbor[4]);
+int pip_stage(pip_ctx *ctx, int stage, double dt, double cmax);
+int64_t pip_halo_bytes(pip_ctx *ctx, int face);
+int pip_halo_pack(pip_ctx *ctx, int face, void *send, int64_t *bytes);
+int pip_halo_unpack(pip_ctx *ctx, int face, const void *recv, int64_t bytes);
+
 /* Last CUDA error code seen by any context (cudaError_t as int), 0 if none. */
 int pip_last_cuda_error(void);
 

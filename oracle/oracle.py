@@ -54,6 +54,8 @@ def lib():
         L.orc_set_cmax.argtypes = [vp, d]
         L.orc_cfl.argtypes = [vp, dp, dp]
         L.orc_run_solver.argtypes = [vp, d]
+        L.orc_stage.argtypes = [vp, ctypes.c_int, d]
+        L.orc_set_neighbors.argtypes = [vp, P(ctypes.c_int)]
         L.orc_flux.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_source.argtypes = [vp, d, dp, dp]
         L.orc_bnd.argtypes = [vp]
@@ -136,6 +138,15 @@ class Oracle:
 
     def run_solver(self, dt: float) -> None:
         lib().orc_run_solver(self.h, float(dt))
+
+    def stage(self, istep: int, dt: float) -> None:
+        """One stage of run_solver with the stage's PIPbnd (physical faces only)."""
+        lib().orc_stage(self.h, int(istep), float(dt))
+
+    def set_neighbors(self, neighbor) -> None:
+        """set_mpi_neighbor: faces with a neighbouring rank are left to the halo exchange."""
+        nb = (ctypes.c_int * 4)(*[int(v) for v in neighbor])
+        lib().orc_set_neighbors(self.h, nb)
 
     def flux(self, direction: int):
         F_h = np.zeros(self.shape_h)

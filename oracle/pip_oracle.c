@@ -33,6 +33,9 @@ struct orc_ctx {
   double *gm_ion, *gm_rec;           /* IR rates (PIP_IR_POWERLAW) */
   int sym_m[6][9], sym_h[6][5];      /* set_sym_mhd / set_sym_hd */
   double cmax, time, last_dt;
+  int neighbor[6];                   /* set_mpi_neighbor: rank across each face, -1 physical */
+  double *U_h0, *U_m0;               /* run_solver's U0 between orc_stage calls */
+  double stage_dt;
 };
 
 static int g_threads = 1;
@@ -188,12 +191,21 @@ static int bnd_type(int code) {
   return code;
 }
 
-/* PIPbnd, Boundary_rot.f90:34-52 (one rank: mpi_bnd exchanges nothing). */
+/* PIPbnd, Boundary_rot.f90:34-52, without its mpi_bnd: MHDbnd/HDbnd on the faces whose
+ * neighbor is -1 (:80-90); the faces with a neighbouring rank are left to the caller's
+ * halo exchange. */
 void orc_bnd(orc_ctx *c) {
   for (int f = 0; f < 2 * c->p.ndim; ++f)
-    boundary_control(c, c->U_m, c->nm, f / 2 + 1, f % 2, c->sym_m[f], bnd_type(c->p.flag_bnd[f]));
+    if (c->neighbor[f] == -1)
+      boundary_control(c, c->U_m, c->nm, f / 2 + 1, f % 2, c->sym_m[f], bnd_type(c->p.flag_bnd[f]));
   for (int f = 0; f < 2 * c->p.ndim; ++f)
-    boundary_control(c, c->U_h, c->nh, f / 2 + 1, f % 2, c->sym_h[f], bnd_type(c->p.flag_bnd[f]));
+    if (c->neighbor[f] == -1)
+      boundary_control(c, c->U_h, c->nh, f / 2 + 1, f % 2, c->sym_h[f], bnd_type(c->p.flag_bnd[f]));
+}
+
+/* set_mpi_neighbor (MPI_rot.f90:90-126) for faces x-, x+, y-, y+. */
+void orc_set_neighbors(orc_ctx *c, const int nb[4]) {
+  for (int f = 0; f < 4; ++f) c->neighbor[f] = nb[f];
 }
 
 /* ---------------------------------------------------------------- conversions */
@@ -1055,44 +1067,52 @@ int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres) {
   return st;
 }
 
-/* run_solver, Solver_rot.f90:42-81 with set_flux :124, set_source :162, time_integral
- * :179-277 (flag_time=0), add_source :498-503, divb_cleaning_Dedner_source
- * (Scheme_rot.f90:546-554) and PIPbnd after each stage and at the end. */
-void orc_run_solver(orc_ctx *c, double dt) {
+/* One stage of run_solver, Solver_rot.f90:59-71 with set_flux :124, set_source :162,
+ * time_integral :179-277 (flag_time=0), add_source :498-503, divb_cleaning_Dedner_source
+ * (Scheme_rot.f90:546-554) and PIPbnd after the stage.  Stage 1 keeps U0 for stage 2. */
+void orc_stage(orc_ctx *c, int istep, double dt) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
   int nh = c->nh, nm = c->nm, t_order = p->t_order;
-  double *U_h0 = malloc(sizeof(double) * nc * nh), *U_m0 = malloc(sizeof(double) * nc * nm);
-  memcpy(U_h0, c->U_h, sizeof(double) * nc * nh);
-  memcpy(U_m0, c->U_m, sizeof(double) * nc * nm);
+  if (istep == 1) {
+    if (!c->U_h0) c->U_h0 = malloc(sizeof(double) * nc * nh);
+    if (!c->U_m0) c->U_m0 = malloc(sizeof(double) * nc * nm);
+    memcpy(c->U_h0, c->U_h, sizeof(double) * nc * nh);
+    memcpy(c->U_m0, c->U_m, sizeof(double) * nc * nm);
+    c->stage_dt = dt;
+  }
+  double *U_h0 = c->U_h0, *U_m0 = c->U_m0;
   double *F_h = calloc(nc * nh * 3, sizeof(double)), *F_m = calloc(nc * nm * 3, sizeof(double));
   double *S_h = malloc(sizeof(double) * nc * nh), *S_m = malloc(sizeof(double) * nc * nm);
   double dt_coll[2] = {dt * 0.5, dt * 0.5};
-  for (int istep = 1; istep <= t_order; ++istep) {
-    double dt_coll_i = dt_coll[t_order - istep];
-    for (int dir = 1; dir <= p->ndim; ++dir)
-      flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
-    memset(S_h, 0, sizeof(double) * nc * nh);
-    memset(S_m, 0, sizeof(double) * nc * nm);
-    source_pip(c, U_h0, U_m0, dt_coll_i, S_h, S_m);
-    double dt_sub = dt / (double)(t_order - istep + 1);
-    for (int dir = 1; dir <= p->ndim; ++dir)
-      add_flux_rk(c, F_h + (size_t)(dir - 1) * nc * nh, U_h0, c->U_h, nh, dt_sub, dir);
-    for (size_t q = 0; q < nc * nh; ++q) c->U_h[q] = c->U_h[q] + S_h[q] * dt_sub;
-    for (int dir = 1; dir <= p->ndim; ++dir)
-      add_flux_rk(c, F_m + (size_t)(dir - 1) * nc * nm, U_m0, c->U_m, nm, dt_sub, dir);
-    for (size_t q = 0; q < nc * nm; ++q) c->U_m[q] = c->U_m[q] + S_m[q] * dt_sub;
-    if (p->flag_divb == 1) {
-      double fac = exp(-dt_sub / dt * p->safety * p->db_clean);
-      double *ps = c->U_m + 8 * nc;
-      for (size_t q = 0; q < nc; ++q) ps[q] = ps[q] * fac;
-    }
-    orc_bnd(c);
+  double dt_coll_i = dt_coll[t_order - istep];
+  for (int dir = 1; dir <= p->ndim; ++dir)
+    flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
+  memset(S_h, 0, sizeof(double) * nc * nh);
+  memset(S_m, 0, sizeof(double) * nc * nm);
+  source_pip(c, U_h0, U_m0, dt_coll_i, S_h, S_m);
+  double dt_sub = dt / (double)(t_order - istep + 1);
+  for (int dir = 1; dir <= p->ndim; ++dir)
+    add_flux_rk(c, F_h + (size_t)(dir - 1) * nc * nh, U_h0, c->U_h, nh, dt_sub, dir);
+  for (size_t q = 0; q < nc * nh; ++q) c->U_h[q] = c->U_h[q] + S_h[q] * dt_sub;
+  for (int dir = 1; dir <= p->ndim; ++dir)
+    add_flux_rk(c, F_m + (size_t)(dir - 1) * nc * nm, U_m0, c->U_m, nm, dt_sub, dir);
+  for (size_t q = 0; q < nc * nm; ++q) c->U_m[q] = c->U_m[q] + S_m[q] * dt_sub;
+  if (p->flag_divb == 1) {
+    double fac = exp(-dt_sub / dt * p->safety * p->db_clean);
+    double *ps = c->U_m + 8 * nc;
+    for (size_t q = 0; q < nc; ++q) ps[q] = ps[q] * fac;
   }
-  /* post_step (Solver_rot.f90:296-303): implicit conduction of the ions */
-  if (p->flag_heat == 1) orc_conduction(c, dt, NULL, NULL);
   orc_bnd(c);
-  free(U_h0); free(U_m0); free(F_h); free(F_m); free(S_h); free(S_m);
+  free(F_h); free(F_m); free(S_h); free(S_m);
+}
+
+/* run_solver, Solver_rot.f90:42-81: t_order stages, then post_step's implicit conduction
+ * of the ions (:296-303) and the closing PIPbnd. */
+void orc_run_solver(orc_ctx *c, double dt) {
+  for (int istep = 1; istep <= c->p.t_order; ++istep) orc_stage(c, istep, dt);
+  if (c->p.flag_heat == 1) orc_conduction(c, dt, NULL, NULL);
+  orc_bnd(c);
 }
 
 int orc_has_nan(const orc_ctx *c) {
@@ -1136,6 +1156,7 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0))) return NULL;
   orc_ctx *c = calloc(1, sizeof(orc_ctx));
   c->p = *p;
+  for (int f = 0; f < 6; ++f) c->neighbor[f] = -1;
   c->ix = p->ix; c->jx = p->jx; c->kx = p->kx;
   c->nh = p->nvar_h; c->nm = p->nvar_m;
   c->nc = (size_t)c->ix * c->jx * c->kx;
@@ -1159,6 +1180,7 @@ void orc_destroy(orc_ctx *c) {
   if (!c) return;
   free(c->dx); free(c->dy); free(c->dz);
   free(c->U_h); free(c->U_m); free(c->gm_ion); free(c->gm_rec);
+  free(c->U_h0); free(c->U_m0);
   free(c);
 }
 

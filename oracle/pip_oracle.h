@@ -38,6 +38,11 @@ void orc_set_cmax(orc_ctx *c, double cmax);
 void orc_cfl(orc_ctx *c, double *dt, double *cmax);
 /* Solver_rot.f90:42-81 with the given dt and the stored cmax. */
 void orc_run_solver(orc_ctx *c, double dt);
+/* One stage (1 or 2) of run_solver with the closing PIPbnd of the stage. */
+void orc_stage(orc_ctx *c, int istep, double dt);
+/* set_mpi_neighbor: faces x-, x+, y-, y+ with a neighbouring rank (>= 0) are skipped by
+ * the boundary fill and left to the caller's halo exchange. */
+void orc_set_neighbors(orc_ctx *c, const int nb[4]);
 /* Solver_rot.f90:124-159 for one direction (1-based), F arrays (ix,jx,kx,nvar). */
 void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m);
 /* PIP_rot.f90:1309-1429; returns S (explicit) or the U0 increments (exponential form). */

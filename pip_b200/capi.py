@@ -32,7 +32,8 @@ EXPORTS = (
     "pip_ctx_create", "pip_ctx_destroy", "pip_upload", "pip_download", "pip_cfl", "pip_step",
     "pip_run", "pip_set_time", "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts",
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
-    "pip_step_noalloc",
+    "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
+    "pip_halo_unpack",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -87,6 +88,12 @@ def lib(path: Optional[str] = None):
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
     L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
+    L.pip_set_neighbors.argtypes = [vp, P(i)]
+    L.pip_stage.argtypes = [vp, i, d, d]
+    L.pip_halo_bytes.argtypes = [vp, i]
+    L.pip_halo_bytes.restype = ctypes.c_int64
+    L.pip_halo_pack.argtypes = [vp, i, vp, P(ctypes.c_int64)]
+    L.pip_halo_unpack.argtypes = [vp, i, vp, ctypes.c_int64]
     L.pip_step_noalloc.restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
@@ -252,6 +259,31 @@ class Context:
 
     def pipbnd(self) -> None:
         _check(lib().pip_fill_ghosts(self.h), "pip_fill_ghosts")
+
+    # ------------------------------------------------------------------ domain decomposition
+    def set_neighbors(self, neighbor) -> None:
+        """set_mpi_neighbor (MPI_rot.f90:90-126): rank across faces x-, x+, y-, y+ or -1."""
+        nb = (ctypes.c_int * 4)(*[int(v) for v in neighbor])
+        _check(lib().pip_set_neighbors(self.h, nb), "pip_set_neighbors")
+
+    def stage(self, stage: int, dt: float, cmax: float) -> None:
+        """One RK stage of run_solver (Solver_rot.f90:59-71)."""
+        _check(lib().pip_stage(self.h, int(stage), float(dt), float(cmax)), "pip_stage")
+
+    def halo_bytes(self, face: int) -> int:
+        return int(lib().pip_halo_bytes(self.h, int(face)))
+
+    def halo_pack(self, face: int, send_ptr: int) -> int:
+        """mpi_bnd's send side of face f into device memory at send_ptr; returns bytes."""
+        n = ctypes.c_int64()
+        _check(lib().pip_halo_pack(self.h, int(face), ctypes.c_void_p(send_ptr), ctypes.byref(n)),
+               "pip_halo_pack")
+        return n.value
+
+    def halo_unpack(self, face: int, recv_ptr: int, nbytes: int) -> None:
+        """mpi_bnd's receive side: the message at recv_ptr into the ghost layers of face f."""
+        _check(lib().pip_halo_unpack(self.h, int(face), ctypes.c_void_p(recv_ptr), int(nbytes)),
+               "pip_halo_unpack")
 
     def status(self) -> Tuple[int, int]:
         stop = ctypes.c_int()

@@ -42,6 +42,9 @@ struct pip_ctx {
   int hc_iters = 0;                   // BiCGstab iterations of the last run
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  int neighbor[4] = {-1, -1, -1, -1};  // set_mpi_neighbor: rank across each face, -1 physical
+  bool exchanged = false;             // some face is filled by the halo exchange
+  int last_stage = 0;                 // RK stage that wrote the state last (1: the U1 array)
   bool uploaded = false;
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
@@ -512,6 +515,7 @@ int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
   CK(from_fp64(c));
   CK(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
+  c->last_stage = 0;
   return PIP_OK;
 }
 
@@ -545,7 +549,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
 
 int pip_step(pip_ctx *c, double dt) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
   if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   DevCtrl &h = *c->h_ctrl;
@@ -567,14 +571,16 @@ int pip_step(pip_ctx *c, double dt) {
   }
   CK(cudaStreamSynchronize(c->stream));
   c->last_dt = dt;
+  c->last_stage = 2;
   return PIP_OK;
 }
 
 static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
                     int64_t *steps_done, float *device_ms) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
   if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
+  c->last_stage = 2;
   if (set_device(c)) return PIP_ERR_CUDA;
   if ((t_end > 0.0 && c->time >= t_end)) {
     if (time_out) *time_out = c->time;
@@ -812,6 +818,123 @@ int pip_conduction(pip_ctx *c, double dt, int *iters, double *relres) {
   if (iters) *iters = it;
   if (relres) *relres = rr;
   return st == 0 ? PIP_OK : PIP_ERR_ITER;
+}
+
+int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
+  if (!c || !neighbor) return PIP_ERR_NULL;
+  bool any = false;
+  for (int f = 0; f < 4; ++f) {
+    if (neighbor[f] < -1) return PIP_ERR_PARAM;
+    if (f >= 2 * c->kp.ndim && neighbor[f] != -1) return PIP_ERR_PARAM;
+    any = any || neighbor[f] >= 0;
+  }
+  // the conduction matrix folds every side of the block (one rank per direction)
+  if (any && c->hc) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_steps = 0;
+  }
+  build_kparams(c);                  // physical boundaries of every face ...
+  for (int f = 0; f < 4; ++f) {      // ... then the exchanged faces get no ghost source
+    c->neighbor[f] = neighbor[f];
+    if (neighbor[f] < 0) continue;
+    int *g = f < 2 ? c->kp.gx[f] : c->kp.gy[f - 2];
+    for (int l = 0; l < pip::kMaxMargin; ++l) g[l] = -1;
+    (f < 2 ? c->kp.typex[f] : c->kp.typey[f - 2]) = 0;
+  }
+  c->kp.dx = c->d_dx;
+  c->kp.dy = c->d_dy;
+  c->kp.rdx = c->d_rdx;
+  c->kp.rdy = c->d_rdy;
+  c->exchanged = any;
+  return PIP_OK;
+}
+
+int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (stage != 1 && stage != 2) return PIP_ERR_PARAM;
+  if (!(dt > 0.0) || !std::isfinite(dt) || !std::isfinite(cmax)) return PIP_ERR_PARAM;
+  if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  if (stage == 1) {
+    DevCtrl &h = *c->h_ctrl;
+    h.dt = dt;
+    h.cmax = cmax;
+    h.done = 0;
+    h.nan_flag = 0;
+    h.status = 0;
+    h.blocks_done = 0;
+    if (push_ctrl(c)) return PIP_ERR_CUDA;
+    c->cmax = cmax;
+  }
+  CK(do_stage(c, stage, 0, 0));
+  if (stage == 2 && c->hc) {
+    CK(cudaMemcpyAsync(c->d_dt, &c->h_ctrl->dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int it = 0, st = 0;
+    const int r = conduct(c, c->d_dt, &it, nullptr, &st);
+    if (r != PIP_OK) return r;
+    c->hc_iters = it;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_stage = stage;
+  if (stage == 2) c->last_dt = dt;
+  return PIP_OK;
+}
+
+namespace {
+// The arrays the last stage wrote: stage 1 -> U1 (B, or Bf in the mixed form), otherwise
+// the state (A, or the FP32 pair Ahi/Alo).
+void halo_arrays(pip_ctx *c, void **a0, void **a1, int *eb) {
+  *a1 = nullptr;
+  if (c->last_stage == 1) {
+    *a0 = c->mixed ? (void *)c->Bf : (void *)c->B;
+    *eb = c->mixed ? 4 : 8;
+  } else if (c->mixed) {
+    *a0 = c->Ahi;
+    *a1 = c->Alo;
+    *eb = 4;
+  } else {
+    *a0 = c->A;
+    *eb = 8;
+  }
+}
+}  // namespace
+
+int64_t pip_halo_bytes(pip_ctx *c, int face) {
+  if (!c || face < 0 || face >= 2 * c->kp.ndim) return 0;
+  return (int64_t)pip::halo_elems(c->kp, face) * 8;
+}
+
+int pip_halo_pack(pip_ctx *c, int face, void *send, int64_t *bytes) {
+  if (!c || !send) return PIP_ERR_NULL;
+  if (face < 0 || face >= 2 * c->kp.ndim) return PIP_ERR_PARAM;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  void *a0, *a1;
+  int eb;
+  halo_arrays(c, &a0, &a1, &eb);
+  CK(pip::halo_pack(c->kp, face, a0, a1, eb, send, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (bytes) *bytes = (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1);
+  return PIP_OK;
+}
+
+int pip_halo_unpack(pip_ctx *c, int face, const void *recv, int64_t bytes) {
+  if (!c || !recv) return PIP_ERR_NULL;
+  if (face < 0 || face >= 2 * c->kp.ndim) return PIP_ERR_PARAM;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  void *a0, *a1;
+  int eb;
+  halo_arrays(c, &a0, &a1, &eb);
+  if (bytes != (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(pip::halo_unpack(c->kp, face, a0, a1, eb, recv, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
 }
 
 int pip_last_cuda_error(void) { return g_last_cuda_error; }

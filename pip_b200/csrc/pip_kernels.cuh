@@ -81,6 +81,14 @@ void hc_destroy(HcEngine *e);
 cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, double tol,
                    int hc_max, cudaStream_t s, int *iters, double *relres, int *status);
 
+// Halo messages of mpi_bnd (pip_halo.cu): elements per array of face f's message, and the
+// copies between the state arrays (a1 may be null) and a message buffer.
+long long halo_elems(const KParams &p, int face);
+cudaError_t halo_pack(const KParams &p, int face, const void *a0, const void *a1, int elem_bytes,
+                      void *buf, cudaStream_t s);
+cudaError_t halo_unpack(const KParams &p, int face, void *a0, void *a1, int elem_bytes,
+                        const void *buf, cudaStream_t s);
+
 // Records a CUDA error code for pip_last_cuda_error (pip_capi.cu).
 void record_cuda_error(int code);
 

@@ -588,7 +588,8 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
 
 // PIPbnd (Boundary_rot.f90:34-125): x ghost columns for every row, then (2D) y ghost rows
 // for every column; boundary_control types 1 (periodic), 2 (mirror with sign table) and
-// 10 (copy of the first interior layer).
+// 10 (copy of the first interior layer).  Faces with a neighbouring rank (source -1) are
+// left to the halo exchange, as MHDbnd/HDbnd skip faces whose neighbor is not -1.
 __global__ void ghosts_x_kernel(const KParams p, double *U, int nplanes) {
   const long long nc = p.nc;
   const int ng = 2 * p.m0;
@@ -598,6 +599,7 @@ __global__ void ghosts_x_kernel(const KParams p, double *U, int nplanes) {
     const int side = g / p.m0, l = g % p.m0;
     const int dst = side == 0 ? l : p.ix - p.m0 + l;
     const int src = p.gx[side][l];
+    if (src < 0) continue;         // face filled by the halo exchange
     for (int n = 0; n < nplanes; ++n) {
       const double v = U[(long long)j * p.ix + src + n * nc];
       U[(long long)j * p.ix + dst + n * nc] = p.typex[side] == 10 ? v : (double)p.symx[side][n] * v;
@@ -614,6 +616,7 @@ __global__ void ghosts_y_kernel(const KParams p, double *U, int nplanes) {
     const int side = g / p.m1, l = g % p.m1;
     const int dst = side == 0 ? l : p.jx - p.m1 + l;
     const int src = p.gy[side][l];
+    if (src < 0) continue;         // face filled by the halo exchange
     for (int n = 0; n < nplanes; ++n) {
       const double v = U[(long long)src * p.ix + i + n * nc];
       U[(long long)dst * p.ix + i + n * nc] = p.typey[side] == 10 ? v : (double)p.symy[side][n] * v;

@@ -1,0 +1,304 @@
+"""Spatial domain decomposition of the two-fluid step over ranks (the MPI layer of PIP,
+MPI_rot.f90, rebuilt for one process per GPU).
+
+The reference splits the grid into blocks (``set_mpi_pos``, MPI_rot.f90:43-88; the 1D split
+``flag_mpi_split = 1`` puts every rank along x), gives each rank its own block with ghost
+cells (``set_mpi``, :11-41), its own coordinates (``set_coordinate``'s MPI branch,
+Model_rot.f90:410-417), its neighbours (``set_mpi_neighbor``, :90-126), fills the ghost
+layers between blocks after every RK stage (``mpi_bnd`` inside ``PIPbnd``,
+Boundary_rot.f90:34-52; two ``MPI_Sendrecv`` per direction, :128-339) and reduces dt (MIN)
+and cmax (MAX) over ranks in ``cfl`` (Scheme_rot.f90:200-210).
+
+Here a 2D grid is split along y (rows stay whole, so a y message is a run of contiguous
+rows) and a 1D grid along x.  Each rank's block is a ``Context`` told its neighbours
+(``pip_set_neighbors``); a step is driven from the host:
+
+    cfl on every block -> MIN over ranks -> dt;  cmax = MAX over ranks of safety*min(d)/dt
+    stage 1 -> halo exchange -> stage 2 -> halo exchange -> cfl (the rewrite of main.f90:47)
+
+The exchange has the reference's two phases per direction: every block sends its upper
+interior layers to the neighbour above and receives its lower ghost layers from the
+neighbour below, then the reverse.  Messages are packed and unpacked on the device
+(``pip_halo_pack`` / ``pip_halo_unpack``) and moved by ``torch.distributed`` point-to-point
+(NCCL over NVLink between GPUs), or, for several blocks held by one process, by a device
+copy.
+
+Blocks are engines with the methods ``cfl() -> (dt, cmax)``, ``stage(k, dt, cmax)``,
+``halo_bytes(face)``, ``message_bytes(face)``, ``buffer(nbytes)``,
+``pack(face, buf) -> nbytes``, ``unpack(face, buf, nbytes)``, ``has_nan() -> bool``,
+``download()`` and ``close()``; ``DeviceBlock`` is the one on a GPU context.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .params import Settings
+
+FACE_NAMES = ("x-", "x+", "y-", "y+")
+
+
+# ---------------------------------------------------------------------- the split
+def split_axis(s: Settings) -> int:
+    """0 (x) for 1D grids, 1 (y) for 2D grids."""
+    return 0 if s.ndim == 1 else 1
+
+
+@dataclasses.dataclass
+class Block:
+    """One rank's part of the grid."""
+    rank: int
+    world: int
+    settings: Settings            # the rank's own grid (interior cells of the block)
+    neighbor: Tuple[int, int, int, int]
+    lo: int                       # first global interior index along the split axis
+    n: int                        # interior cells along the split axis
+
+    @property
+    def sg(self) -> float:
+        """safety*min(dx, dy, dz) of the block (the numerator of cfl's cmax)."""
+        _, _, _, dx, dy, dz = self.settings.coordinates()
+        return self.settings.safety * min(dx.min(), dy.min(), dz.min())
+
+
+def block_of(s: Settings, world: int, rank: int) -> Block:
+    """set_mpi / set_mpi_pos / set_mpi_neighbor / set_coordinate for rank ``rank`` of
+    ``world`` blocks along the split axis."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank %d of %d" % (rank, world))
+    ax = split_axis(s)
+    total = s.ix0 if ax == 0 else s.jx0
+    if total % world:
+        raise ValueError("%d cells along %s do not divide into %d blocks"
+                         % (total, "xy"[ax], world))
+    n = total // world
+    # set_coordinate's MPI branch (Model_rot.f90:410-417)
+    start, end = list(s.start), list(s.end)
+    length = end[ax] - start[ax]
+    ds = 1.0 / world
+    start[ax] = start[ax] + ds * rank * length
+    end[ax] = start[ax] + ds * length
+    kw = {"ix0": n} if ax == 0 else {"jx0": n}
+    local = s.overrides(start=tuple(start), end=tuple(end), **kw)
+    # set_mpi_neighbor (MPI_rot.f90:90-126): periodic faces wrap around the ranks
+    nb = [-1, -1, -1, -1]
+    if world > 1:
+        lo_face, hi_face = 2 * ax, 2 * ax + 1
+        nb[lo_face] = rank - 1
+        nb[hi_face] = rank + 1
+        if rank == 0:
+            nb[lo_face] = world - 1 if s.flag_bnd[lo_face] == 1 else -1
+        if rank == world - 1:
+            nb[hi_face] = 0 if s.flag_bnd[hi_face] == 1 else -1
+    return Block(rank, world, local, tuple(nb), rank * n, n)
+
+
+def scatter(s: Settings, U: np.ndarray, world: int, rank: int) -> np.ndarray:
+    """The rank's block of a global state (planes, jx, ix) with ghosts: its interior plus
+    margin layers on each side along the split axis, taken from the global array (the
+    neighbours' interior cells, or the global ghost cells at the ends)."""
+    b = block_of(s, world, rank)
+    ax = split_axis(s)
+    m = s.margin[ax]
+    sl = slice(b.lo, b.lo + b.n + 2 * m)
+    return np.ascontiguousarray(U[:, :, sl] if ax == 0 else U[:, sl, :])
+
+
+def gather(s: Settings, parts: Sequence[np.ndarray]) -> np.ndarray:
+    """The global state from every rank's block (rank order): interiors side by side, the
+    global ghost layers from the first and last blocks."""
+    world = len(parts)
+    ax = split_axis(s)
+    m = s.margin[ax]
+    out = []
+    for r, p in enumerate(parts):
+        n = (p.shape[2] if ax == 0 else p.shape[1]) - 2 * m
+        a = m if r > 0 else 0
+        e = m + n + (m if r == world - 1 else 0)
+        out.append(p[:, :, a:e] if ax == 0 else p[:, a:e, :])
+    return np.ascontiguousarray(np.concatenate(out, axis=2 if ax == 0 else 1))
+
+
+# ---------------------------------------------------------------------- transports
+class TorchComm:
+    """Reductions and point-to-point messages between processes through
+    ``torch.distributed`` (NCCL for device buffers, gloo for host buffers)."""
+
+    def __init__(self, device=None, group=None):
+        import torch
+        import torch.distributed as dist
+        self.dist = dist
+        self.torch = torch
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.device = device if device is not None else "cpu"
+
+    def allreduce(self, value: float, op: str) -> float:
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN if op == "min" else self.dist.ReduceOp.MAX,
+                             group=self.group)
+        return float(t.item())
+
+    def exchange(self, sends, recvs) -> None:
+        """sends: [(src_rank, dst_rank, tensor)], recvs: [(dst_rank, src_rank, tensor)] for
+        this process's blocks; at most one message per ordered pair of ranks.  The sends and
+        receives go out as one batch (one NCCL group), so two ranks that send to each other
+        do not wait on each other's receive."""
+        P2POp = self.dist.P2POp
+        ops = [P2POp(self.dist.irecv, t, src, self.group) for _, src, t in recvs]
+        ops += [P2POp(self.dist.isend, t, dst, self.group) for _, dst, t in sends]
+        for q in self.dist.batch_isend_irecv(ops):
+            q.wait()
+        if self.torch.cuda.is_available():
+            self.torch.cuda.synchronize()
+
+
+class LocalComm:
+    """Every block in this process (several GPU contexts on one device, or host engines):
+    reductions over the blocks and messages as device/host copies."""
+
+    def allreduce(self, value: float, op: str) -> float:
+        return value
+
+    def exchange(self, sends, recvs) -> None:
+        box = {(src, dst): t for src, dst, t in sends}
+        for dst, src, t in recvs:
+            t.copy_(box[(src, dst)])
+
+
+# ---------------------------------------------------------------------- engines
+class DeviceBlock:
+    """A rank's block on a GPU context (``pip_set_neighbors`` + ``pip_stage`` +
+    ``pip_halo_pack/unpack``)."""
+
+    def __init__(self, block: Block, U_h: np.ndarray, U_m: np.ndarray, device: int = 0):
+        import torch
+        from .capi import Context
+        self.torch = torch
+        self.block = block
+        self.ctx = Context(block.settings)
+        self.ctx.set_neighbors(block.neighbor)
+        self.ctx.upload(U_h, U_m)
+        self.device = torch.device("cuda", device)
+        self.mixed = block.settings.precision != 0
+        self.last_stage = 0
+
+    def cfl(self) -> Tuple[float, float]:
+        return self.ctx.cfl()
+
+    def stage(self, k: int, dt: float, cmax: float) -> None:
+        self.ctx.stage(k, dt, cmax)
+        self.last_stage = k
+
+    def message_bytes(self, face: int) -> int:
+        """Length of the message of face f for the state the last stage wrote: the FP32-mixed
+        form's stage-1 array holds one FP32 value per cell, every other state 8 bytes."""
+        n = self.ctx.halo_bytes(face)
+        return n // 2 if (self.mixed and self.last_stage == 1) else n
+
+    def buffer(self, nbytes: int):
+        return self.torch.empty(nbytes, dtype=self.torch.uint8, device=self.device)
+
+    def halo_bytes(self, face: int) -> int:
+        return self.ctx.halo_bytes(face)
+
+    def pack(self, face: int, buf) -> int:
+        return self.ctx.halo_pack(face, buf.data_ptr())
+
+    def unpack(self, face: int, buf, nbytes: int) -> None:
+        self.ctx.halo_unpack(face, buf.data_ptr(), nbytes)
+
+    def has_nan(self) -> bool:
+        return bool(self.ctx.status()[1])
+
+    def download(self) -> Tuple[np.ndarray, np.ndarray]:
+        return self.ctx.download()
+
+    def close(self) -> None:
+        self.ctx.close()
+
+
+# ---------------------------------------------------------------------- the driver
+class DecomposedRun:
+    """The time loop of main.f90:31-68 over decomposed blocks.  ``engines`` are the blocks
+    this process holds (one per process with ``TorchComm``, all of them with
+    ``LocalComm``)."""
+
+    def __init__(self, engines: Sequence, comm, divb: bool):
+        self.engines = list(engines)
+        self.comm = comm
+        self.divb = divb
+        self.time = 0.0
+        self.steps = 0
+        self.dt_history: List[float] = []
+        self._send: Dict[Tuple[int, int], object] = {}
+        self._recv: Dict[Tuple[int, int], object] = {}
+        for e in self.engines:
+            for f in range(4):
+                if e.block.neighbor[f] >= 0:
+                    n = e.halo_bytes(f)
+                    self._send[(e.block.rank, f)] = e.buffer(n)
+                    self._recv[(e.block.rank, f)] = e.buffer(n)
+
+    def halo(self) -> None:
+        """mpi_bnd (MPI_rot.f90:128-339): per split direction, phase 1 sends the upper
+        interior layers up and fills the lower ghost layers from below; phase 2 the
+        reverse."""
+        for d in (0, 1):
+            for send_face in (2 * d + 1, 2 * d):
+                recv_face = send_face ^ 1
+                sends, recvs = [], []
+                for e in self.engines:
+                    r = e.block.rank
+                    if e.block.neighbor[send_face] >= 0:
+                        buf = self._send[(r, send_face)]
+                        n = e.pack(send_face, buf)
+                        sends.append((r, e.block.neighbor[send_face], buf[:n]))
+                    if e.block.neighbor[recv_face] >= 0:
+                        n = e.message_bytes(recv_face)
+                        recvs.append((r, e.block.neighbor[recv_face], self._recv[(r, recv_face)][:n]))
+                if not sends and not recvs:
+                    continue
+                self.comm.exchange(sends, recvs)
+                for e in self.engines:
+                    r = e.block.rank
+                    if e.block.neighbor[recv_face] >= 0:
+                        e.unpack(recv_face, self._recv[(r, recv_face)], e.message_bytes(recv_face))
+
+    def step(self) -> float:
+        """cfl; run_solver with PIPbnd's exchange after each stage; cfl (main.f90:36-47)."""
+        dt = min(e.cfl()[0] for e in self.engines)
+        dt = self.comm.allreduce(dt, "min")
+        cmax = 0.0
+        if self.divb:
+            cmax = self.comm.allreduce(max(e.block.sg / dt for e in self.engines), "max")
+        for k in (1, 2):
+            for e in self.engines:
+                e.stage(k, dt, cmax)
+            self.halo()
+        for e in self.engines:
+            e.cfl()
+        self.time += dt
+        self.steps += 1
+        self.dt_history.append(dt)
+        return dt
+
+    def run(self, nsteps: int, check_every: int = 1) -> int:
+        """nsteps steps with stop_sim's checks (IO_rot.f90:625-674) every check_every steps:
+        returns 0, 3 (NaN) or 4 (dt <= 1e-12), the same on every rank."""
+        for n in range(nsteps):
+            dt = self.step()
+            if dt <= 1.0e-12:
+                return 4
+            if (n + 1) % check_every == 0 or n == nsteps - 1:
+                bad = max(float(e.has_nan()) for e in self.engines)
+                if self.comm.allreduce(bad, "max") > 0.0:
+                    return 3
+        return 0
+
+    def close(self) -> None:
+        for e in self.engines:
+            e.close()

@@ -1,0 +1,20 @@
+"""Small seeded cases for the decomposition tests: periodic 2D with Dedner cleaning
+(Orszag-Tang), 2D with reflecting walls at the ends of the split axis and ionisation/
+recombination (Kelvin-Helmholtz), and 1D with outflow ends (Brio-Wu)."""
+from generic_state import generic_state
+from pip_b200 import ics
+
+
+def make_case(case):
+    if case == "ot":
+        s, Uh, Um = ics.orszag_tang(16)
+    elif case == "kh":
+        s, Uh, Um = ics.kelvin_helmholtz(16, 16)
+    elif case == "bw":
+        s, Uh, Um = ics.brio_wu(64)
+    elif case == "ot_generic":
+        s, _, _ = ics.orszag_tang(16)
+        Uh, Um = generic_state(s, 11)
+    else:
+        raise ValueError(case)
+    return s, Uh, Um

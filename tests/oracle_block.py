@@ -1,0 +1,77 @@
+"""A block of a decomposed run on the oracle (CPU): the engine protocol of
+pip_b200.decomp (cfl, stage, halo_bytes, message_bytes, buffer, pack, unpack, has_nan,
+download, close) with the oracle's orc_stage and its neighbour-aware PIPbnd, and mpi_bnd's
+layer slices (MPI_rot.f90:128-339) done on the host arrays.  Message layout: ion planes
+then neutral planes, layer, position along the face -- the layout of pip_halo_pack."""
+import numpy as np
+import torch
+
+from oracle import oracle as O
+
+
+class OracleBlock:
+    def __init__(self, block, U_h, U_m):
+        self.block = block
+        self.s = block.settings
+        self.o = O.Oracle(self.s, U_h, U_m)
+        self.o.set_neighbors(block.neighbor)
+        ix, jx, _ = self.s.shape
+        self.n = (ix, jx)
+        self.m = self.s.margin
+
+    def cfl(self):
+        return self.o.cfl()
+
+    def stage(self, k, dt, cmax):
+        self.o.cmax = cmax
+        self.o.stage(k, dt)
+
+    def _layers(self, face, pack):
+        d = face // 2
+        m = self.m[d]
+        n = self.n[d]
+        lower = face % 2 == 0
+        first = (m if lower else n - 2 * m) if pack else (0 if lower else n - m)
+        return d, slice(first, first + m)
+
+    def halo_bytes(self, face):
+        d = face // 2
+        ix, jx = self.n
+        return 8 * (self.s.nvar_m + 5) * self.m[d] * (jx if d == 0 else ix)
+
+    def message_bytes(self, face):
+        return self.halo_bytes(face)
+
+    def buffer(self, nbytes):
+        return torch.empty(nbytes, dtype=torch.uint8)
+
+    def pack(self, face, buf):
+        U_h, U_m = self.o.state()
+        U = np.concatenate([U_m, U_h], axis=0)
+        d, sl = self._layers(face, True)
+        msg = U[:, sl, :] if d == 1 else U[:, :, sl].transpose(0, 2, 1)
+        raw = np.ascontiguousarray(msg).view(np.uint8).reshape(-1)
+        buf[: raw.size] = torch.from_numpy(raw)
+        return raw.size
+
+    def unpack(self, face, buf, nbytes):
+        U_h, U_m = self.o.state()
+        U = np.concatenate([U_m, U_h], axis=0)
+        d, sl = self._layers(face, False)
+        ix, jx = self.n
+        msg = buf[:nbytes].numpy().view(np.float64)
+        if d == 1:
+            U[:, sl, :] = msg.reshape(U.shape[0], -1, ix)
+        else:
+            U[:, :, sl] = msg.reshape(U.shape[0], -1, jx).transpose(0, 2, 1)
+        nm = self.s.nvar_m
+        self.o.set_state(U[nm:], U[:nm])
+
+    def has_nan(self):
+        return self.o.has_nan()
+
+    def download(self):
+        return self.o.state()
+
+    def close(self):
+        self.o.close()

@@ -1,0 +1,122 @@
+"""Domain decomposition on the device: blocks on GPU contexts (pip_set_neighbors,
+pip_stage, pip_halo_pack / pip_halo_unpack) stepped by pip_b200.decomp.  The run here has
+every block in one process on one GPU (the host sequences the blocks' launches; nothing
+on the device waits for another block), exchanging halos by device copies; the same
+driver over torch.distributed/NCCL moves the same buffers between GPUs.  Checked against
+the single-block run of the same driver (bitwise: the per-cell arithmetic does not depend
+on the split), against pip_run, and against the single-domain oracle."""
+import numpy as np
+import pytest
+import torch
+
+from decomp_cases import make_case
+from helpers import interior, rel_l1
+from oracle import oracle as O
+from pip_b200 import capi, decomp, ics
+from pip_b200.params import PIP_MIXED
+
+pytestmark = pytest.mark.gpu
+
+
+def device_run(s, Uh, Um, world, nsteps):
+    engines = [decomp.DeviceBlock(decomp.block_of(s, world, r), decomp.scatter(s, Uh, world, r),
+                                  decomp.scatter(s, Um, world, r)) for r in range(world)]
+    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
+    st = run.run(nsteps)
+    states = [e.download() for e in engines]
+    run.close()
+    return (st, run.dt_history, decomp.gather(s, [a for a, _ in states]),
+            decomp.gather(s, [b for _, b in states]))
+
+
+def test_halo_pack_unpack_layout(gpu_lib):
+    s, Uh, Um = make_case("ot_generic")
+    b = decomp.block_of(s, 2, 0)
+    uh, um = decomp.scatter(s, Uh, 2, 0), decomp.scatter(s, Um, 2, 0)
+    U = np.concatenate([um, uh], axis=0)
+    ix, jx, _ = b.settings.shape
+    m = b.settings.margin[1]
+    with capi.Context(b.settings) as c:
+        c.set_neighbors(b.neighbor)
+        c.upload(uh, um)
+        assert c.halo_bytes(2) == 8 * U.shape[0] * m * ix
+        buf = torch.empty(c.halo_bytes(2), dtype=torch.uint8, device="cuda")
+        for face, rows in ((2, slice(m, 2 * m)), (3, slice(jx - 2 * m, jx - m))):
+            n = c.halo_pack(face, buf.data_ptr())
+            got = buf[:n].cpu().numpy().view(np.float64).reshape(U.shape[0], m, ix)
+            assert np.array_equal(got, U[:, rows, :])
+        bufx = torch.empty(c.halo_bytes(0), dtype=torch.uint8, device="cuda")
+        n = c.halo_pack(1, bufx.data_ptr())
+        got = bufx[:n].cpu().numpy().view(np.float64).reshape(U.shape[0], m, jx)
+        assert np.array_equal(got, U[:, :, ix - 2 * m: ix - m].transpose(0, 2, 1))
+        # a message into the lower ghost rows, nothing else touched
+        msg = np.arange(U.shape[0] * m * ix, dtype=np.float64)
+        t = torch.from_numpy(msg).cuda().view(torch.uint8)
+        c.halo_unpack(2, t.data_ptr(), t.numel())
+        gh, gm = c.download()
+        G = np.concatenate([gm, gh], axis=0)
+        assert np.array_equal(G[:, :m, :], msg.reshape(U.shape[0], m, ix))
+        assert np.array_equal(G[:, m:, :], U[:, m:, :])
+
+
+@pytest.mark.parametrize("case,world", [("ot", 2), ("ot", 4), ("ot_generic", 2), ("kh", 4),
+                                        ("bw", 4)])
+def test_blocks_match_single_block(gpu_lib, case, world):
+    nsteps = 8
+    s, Uh, Um = make_case(case)
+    st1, dt1, h1, m1 = device_run(s, Uh, Um, 1, nsteps)
+    stn, dtn, hn, mn = device_run(s, Uh, Um, world, nsteps)
+    assert st1 == 0 and stn == 0
+    assert dtn == dt1
+    assert np.array_equal(hn, h1) and np.array_equal(mn, m1)
+    # the single block through pip_stage is the step of pip_run
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        st, t, n = c.run(nsteps=nsteps)
+        rh, rm = c.download()
+    assert st == 0 and n == nsteps
+    assert abs(t - sum(dt1)) <= 1e-14 * t
+    assert max(rel_l1(interior(h1, s), interior(rh, s)).max(),
+               rel_l1(interior(m1, s), interior(rm, s)).max()) <= 1e-12
+    # and the oracle's single-domain run
+    o = O.Oracle(s, Uh, Um)
+    st_o, t_o, n_o, hist = o.run(nsteps=nsteps, max_hist=nsteps)
+    oh, om = o.state()
+    o.close()
+    np.testing.assert_allclose(np.array(dtn), hist, rtol=1e-10, atol=0)
+    assert max(rel_l1(interior(hn, s), interior(oh, s)).max(),
+               rel_l1(interior(mn, s), interior(om, s)).max()) <= 1e-10
+
+
+def test_mixed_blocks_match_single_block(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(32, precision=PIP_MIXED)
+    st1, dt1, h1, m1 = device_run(s, Uh, Um, 1, 6)
+    st2, dt2, h2, m2 = device_run(s, Uh, Um, 4, 6)
+    assert st1 == 0 and st2 == 0 and dt1 == dt2
+    assert np.array_equal(h2, h1) and np.array_equal(m2, m1)
+
+
+def test_decomposition_rejects(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(16)
+    b = decomp.block_of(s, 2, 0)
+    with capi.Context(b.settings) as c:
+        c.set_neighbors(b.neighbor)
+        c.upload(decomp.scatter(s, Uh, 2, 0), decomp.scatter(s, Um, 2, 0))
+        with pytest.raises(capi.PipError) as e:
+            c.run_solver(1e-4)                       # pip_step cannot exchange mid-step
+        assert e.value.code == capi.PIP_ERR_STATE
+        with pytest.raises(capi.PipError) as e:
+            c.run(nsteps=1)
+        assert e.value.code == capi.PIP_ERR_STATE
+        with pytest.raises(capi.PipError) as e:
+            c.stage(2, 1e-4, 0.0)                    # stage 2 before stage 1
+        assert e.value.code == capi.PIP_ERR_STATE
+        with pytest.raises(capi.PipError) as e:
+            c.set_neighbors([0, -1, -1, -1])         # x is not split, but accepted ...
+            c.set_neighbors([-2, -1, -1, -1])        # ... a rank below -1 is not
+        assert e.value.code == capi.PIP_ERR_PARAM
+    s3, _, _ = ics.kelvin_helmholtz(16, 16, flag_heat=1, kapper=0.1)
+    with capi.Context(s3) as c:
+        with pytest.raises(capi.PipError) as e:
+            c.set_neighbors([-1, -1, 1, 1])          # conduction folds every side
+        assert e.value.code == capi.PIP_ERR_PARAM
