@@ -13,6 +13,11 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
   state arrays exceed the 126 MB L2, so no flush between steps).  The plain FP64 path is
   timed the same way ("fp64"), and the relative L1 error of the mixed state against the
   FP64 state after the same steps is reported per variable.
+* N > 1 GPUs (torchrun, one rank per GPU; or --decompose with one GPU): the y-slab domain
+  decomposition of pip_b200.decomp, weak-scaled -- the Orszag-Tang pattern repeated in y
+  over [0,1] x [0,N] with one 1024x1024 slab per GPU, a halo exchange (NCCL point-to-point)
+  after each RK stage, dt MIN and cmax MAX over ranks; device time between CUDA events
+  around the step loop, max over ranks; value = N x 1024^2 x steps / time.
 * e2e: the same metric through the public C ABI with pinned host buffers:
   pip_upload + pip_run + pip_download, copies inside the timed region.
 * roofline: the stage-2 kernel (the heavier of the two per-step kernels) against the
@@ -196,7 +201,13 @@ def run_reference(args):
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": n, "warmup": 1, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": cells, "precision": "fp64",
+        "config": {"workload": (WORKLOAD if not decomposed else
+                                "Orszag-Tang pattern repeated in y: %dx%d cells over [0,1]x[0,%d] "
+                                "(periodic), one %dx%d y-slab per GPU, halo exchange of 2 ghost "
+                                "rows x 14 planes after each RK stage (NCCL point-to-point), dt MIN "
+                                "and cmax MAX over ranks; physics as the 1024x1024 run"
+                                % (n, n * world, world, n, n)),
+                   "cells": cells * world, "precision": "fp64",
                    "parallelism": "host OpenMP, %d threads" % threads},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": "%d of the requested %d steps (time budget %.0f s)"
@@ -233,6 +244,89 @@ def measure(n, precision, steps, warmup, dist, local):
     ctx.close()
     return dict(ms=ms, state=state, launches=launches, clocks=clk.summary(), ms1=ms1, ms2=ms2,
                 msstep=msstep, settings=s, U=(Uh, Um))
+
+
+def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
+    """Weak-scaled decomposition: the Orszag-Tang pattern repeated in y over [0,1] x
+    [0,world], 1024 x (1024*world) cells, one 1024x1024 y-slab per rank (pip_b200.decomp:
+    cfl -> MIN/MAX over ranks, stage, halo exchange, stage, halo exchange, cfl).  Device
+    time between CUDA events on the current stream around the step loop (every call of the
+    loop completes before the next starts), max over ranks by the caller."""
+    import torch
+    from pip_b200 import decomp, ics
+    from pip_b200.params import Settings
+    sg = ics.orszag_tang(8, precision=precision)[0].overrides(
+        ix0=n, jx0=n * world, end=(1.0, float(world), 1.0))
+    b = decomp.block_of(sg, world, rank)
+    _, Uh, Um = ics.orszag_tang(n, precision=precision, start=b.settings.start, end=b.settings.end)
+    eng = decomp.DeviceBlock(b, Uh, Um, device=local)
+    comm = decomp.TorchComm(device=torch.device("cuda", local)) if dist else decomp.LocalComm()
+    run = decomp.DecomposedRun([eng], comm, divb=sg.divb == 1)
+    # the prologue's cfl and ghost fill (physical faces, then the exchanged ones)
+    eng.ctx.cfl()
+    eng.ctx.pipbnd()
+    run.halo()
+    if run.run(warmup) != 0:
+        raise RuntimeError("decomposed warm-up stopped")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        st = run.run(steps, check_every=steps)
+        e1.record()
+        torch.cuda.synchronize()
+    if st != 0:
+        raise RuntimeError("decomposed run stopped with status %d" % st)
+    ms = e0.elapsed_time(e1)
+    state = eng.download()
+    s_blk = b.settings
+    # per step: 2 cfl + 2 stage kernels and, per stage, a pack and an unpack per phase
+    halo_faces = sum(1 for v in b.neighbor if v >= 0)
+    launches = steps * (4 + 2 * 2 * halo_faces)
+    run.close()
+    # the stage kernels' own durations on an undecomposed block of the same size
+    from pip_b200 import capi
+    with capi.Context(s_blk) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        ms1, ms2, msstep = c.stage_ms(min(200, steps))
+    return dict(ms=ms, state=state, launches=launches, clocks=clk.summary(), ms1=ms1, ms2=ms2,
+                msstep=msstep, settings=s_blk, U=(Uh, Um), world_cells=n * n * world)
+
+
+def e2e_decomposed(n, precision, steps, warmup, dist, local, world, rank):
+    """The decomposed run through the public API from pinned host arrays: pip_upload of the
+    rank's block, the decomposed steps, pip_download; wall clock, max over ranks by the
+    caller."""
+    import torch
+    from pip_b200 import decomp, ics
+    sg = ics.orszag_tang(8, precision=precision)[0].overrides(
+        ix0=n, jx0=n * world, end=(1.0, float(world), 1.0))
+    b = decomp.block_of(sg, world, rank)
+    _, Uh, Um = ics.orszag_tang(n, precision=precision, start=b.settings.start, end=b.settings.end)
+    pin = lambda a: torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+    ph, pm, oh, om = pin(Uh), pin(Um), pin(Uh), pin(Um)
+    ph[...] = Uh
+    pm[...] = Um
+    eng = decomp.DeviceBlock(b, ph, pm, device=local)
+    comm = decomp.TorchComm(device=torch.device("cuda", local)) if dist else decomp.LocalComm()
+    run = decomp.DecomposedRun([eng], comm, divb=sg.divb == 1)
+    run.run(warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.ctx.upload(ph, pm)
+    st = run.run(steps, check_every=steps)
+    eng.ctx.download(oh, om)
+    e2e_s = time.perf_counter() - t0
+    run.close()
+    if st != 0:
+        raise RuntimeError("decomposed e2e run stopped with status %d" % st)
+    return e2e_s, Uh.nbytes + Um.nbytes
 
 
 def e2e_run(s, Uh, Um, steps, warmup, dist):
@@ -406,6 +500,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-conduction", action="store_true")
+    ap.add_argument("--decompose", action="store_true",
+                    help="run the domain-decomposed step also with one GPU (always with N > 1)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -438,8 +534,13 @@ def main():
     build.build()
     n = args.n
     cells = n * n
-    f64 = measure(n, PIP_FP64, args.steps, args.warmup, dist, local)
-    mix = measure(n, PIP_MIXED, args.steps, args.warmup, dist, local)
+    decomposed = world > 1 or args.decompose
+    if decomposed:
+        f64 = measure_decomposed(n, PIP_FP64, args.steps, args.warmup, dist, local, world, rank)
+        mix = measure_decomposed(n, PIP_MIXED, args.steps, args.warmup, dist, local, world, rank)
+    else:
+        f64 = measure(n, PIP_FP64, args.steps, args.warmup, dist, local)
+        mix = measure(n, PIP_MIXED, args.steps, args.warmup, dist, local)
     l1 = rel_l1_interior(mix["state"], f64["state"], 2)
     ms64 = max_over_ranks(f64["ms"])
     msmx = max_over_ranks(mix["ms"])
@@ -448,14 +549,21 @@ def main():
     peak, peak_kind = measured_peaks()
     a64 = FP64_BYTES_PER_CELL_STAGE2 * cells / (f64["ms2"] * 1e-3) / 1e9
     amx = MIXED_BYTES_PER_CELL_STAGE2 * cells / (mix["ms2"] * 1e-3) / 1e9
-    e2e_s, state_bytes = e2e_run(mix["settings"], mix["U"][0], mix["U"][1], args.steps,
-                                 args.warmup, dist)
+    if decomposed:
+        e2e_s, state_bytes = e2e_decomposed(n, PIP_MIXED, args.steps, args.warmup, dist, local,
+                                            world, rank)
+        how = ("FP32-mixed, decomposed: pip_upload of each rank's block (pinned FP64 host "
+               "arrays) + %d steps of cfl/allreduce/stage/halo/stage/halo/cfl + pip_download, "
+               "wall clock, max over ranks" % args.steps)
+    else:
+        e2e_s, state_bytes = e2e_run(mix["settings"], mix["U"][0], mix["U"][1], args.steps,
+                                     args.warmup, dist)
+        how = ("FP32-mixed: pip_upload (pinned FP64 host arrays) + pip_run(%d steps) + "
+               "pip_download, wall clock around the synchronous C ABI calls" % args.steps)
     e2e_s = max_over_ranks(e2e_s)
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": state_bytes / args.steps,
-           "how": "FP32-mixed: pip_upload (pinned FP64 host arrays) + pip_run(%d steps) + "
-                  "pip_download, wall clock around the synchronous C ABI calls" % args.steps}
+           "d2h_bytes_per_step": state_bytes / args.steps, "how": how}
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -471,12 +579,19 @@ def main():
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64-mixed", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": cells,
+        "config": {"workload": (WORKLOAD if not decomposed else
+                                "Orszag-Tang pattern repeated in y: %dx%d cells over [0,1]x[0,%d] "
+                                "(periodic), one %dx%d y-slab per GPU, halo exchange of 2 ghost "
+                                "rows x 14 planes after each RK stage (NCCL point-to-point), dt MIN "
+                                "and cmax MAX over ranks; physics as the 1024x1024 run"
+                                % (n, n * world, world, n, n)),
+                   "cells": cells * world,
                    "precision": "FP32-mixed (FP32 fluxes/state, FP64 source and compensated "
                                 "RK accumulation)",
                    "l2": "inputs larger than L2 (FP64 state 2 x %.0f MB, mixed 3 x %.0f MB vs "
                          "126 MB L2)" % (state_bytes / 1e6, state_bytes / 2e6),
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+                   "parallelism": ("y-slab domain decomposition over %d GPU(s)" % world
+                                   if decomposed else "single GPU")},
         "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
                  "roofline": {"bound": "hbm", "achieved": a64, "peak": peak, "unit": "GB/s",
                               "frac": a64 / peak,

@@ -230,11 +230,18 @@ int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
  * message packed at face f is unpacked by the neighbour at the opposite face (f ^ 1).
  * send and recv are DEVICE buffers of at least pip_halo_bytes(ctx, f) bytes; *bytes gets
  * the message length, which the receiver passes to unpack (FP64 form: margin x extent x
- * (nvar_m + 5) doubles; FP32-mixed form after stage 1: half of that).  Both calls return
- * when the copy is complete.
+ * (nvar_m + 5) doubles; FP32-mixed form after stage 1: half of that).
+ *
+ * pip_stage, pip_halo_pack and pip_halo_unpack queue their work on the context's stream
+ * (pip_ctx_stream) and return without waiting for it, so a step needs no host round trip
+ * between its stages: issue the message transfer on the same stream (NCCL send/recv on
+ * that stream, or a copy queued there), or wait for the stream before touching the buffers
+ * from elsewhere.  Errors of queued work surface at the next call that waits (pip_cfl,
+ * pip_download, pip_status).
  */
 int pip_set_neighbors(pip_ctx *ctx, const int neighbor[4]);
 int pip_stage(pip_ctx *ctx, int stage, double dt, double cmax);
+int pip_ctx_stream(pip_ctx *ctx, void **stream);
 int64_t pip_halo_bytes(pip_ctx *ctx, int face);
 int pip_halo_pack(pip_ctx *ctx, int face, void *send, int64_t *bytes);
 int pip_halo_unpack(pip_ctx *ctx, int face, const void *recv, int64_t bytes);

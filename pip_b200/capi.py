@@ -33,7 +33,7 @@ EXPORTS = (
     "pip_run", "pip_set_time", "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts",
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
-    "pip_halo_unpack",
+    "pip_halo_unpack", "pip_ctx_stream",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -94,6 +94,7 @@ def lib(path: Optional[str] = None):
     L.pip_halo_bytes.restype = ctypes.c_int64
     L.pip_halo_pack.argtypes = [vp, i, vp, P(ctypes.c_int64)]
     L.pip_halo_unpack.argtypes = [vp, i, vp, ctypes.c_int64]
+    L.pip_ctx_stream.argtypes = [vp, P(vp)]
     L.pip_step_noalloc.restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
@@ -270,18 +271,27 @@ class Context:
         """One RK stage of run_solver (Solver_rot.f90:59-71)."""
         _check(lib().pip_stage(self.h, int(stage), float(dt), float(cmax)), "pip_stage")
 
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t (pip_ctx_stream), as an integer handle."""
+        h = ctypes.c_void_p()
+        _check(lib().pip_ctx_stream(self.h, ctypes.byref(h)), "pip_ctx_stream")
+        return int(h.value or 0)
+
     def halo_bytes(self, face: int) -> int:
         return int(lib().pip_halo_bytes(self.h, int(face)))
 
     def halo_pack(self, face: int, send_ptr: int) -> int:
-        """mpi_bnd's send side of face f into device memory at send_ptr; returns bytes."""
+        """mpi_bnd's send side of face f into device memory at send_ptr (queued on the
+        context stream); returns the message length in bytes."""
         n = ctypes.c_int64()
         _check(lib().pip_halo_pack(self.h, int(face), ctypes.c_void_p(send_ptr), ctypes.byref(n)),
                "pip_halo_pack")
         return n.value
 
     def halo_unpack(self, face: int, recv_ptr: int, nbytes: int) -> None:
-        """mpi_bnd's receive side: the message at recv_ptr into the ghost layers of face f."""
+        """mpi_bnd's receive side: the message at recv_ptr into the ghost layers of face f
+        (queued on the context stream)."""
         _check(lib().pip_halo_unpack(self.h, int(face), ctypes.c_void_p(recv_ptr), int(nbytes)),
                "pip_halo_unpack")
 

@@ -317,6 +317,17 @@ int sync_ctrl_to_host(pip_ctx *c) {
   return PIP_OK;
 }
 
+// The control fields a host-stepped stage reads, set on the device from launch arguments
+// (no pinned host buffer that a later call could rewrite before the copy runs).
+__global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
+  ctrl->dt = dt;
+  ctrl->cmax = cmax;
+  ctrl->done = 0;
+  ctrl->nan_flag = 0;
+  ctrl->status = 0;
+  ctrl->blocks_done = 0;
+}
+
 int push_ctrl(pip_ctx *c) {
   CK(cudaMemcpyAsync(c->ctrl, c->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice, c->stream));
   return PIP_OK;
@@ -861,27 +872,27 @@ int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
   if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (stage == 1) {
-    DevCtrl &h = *c->h_ctrl;
-    h.dt = dt;
-    h.cmax = cmax;
-    h.done = 0;
-    h.nan_flag = 0;
-    h.status = 0;
-    h.blocks_done = 0;
-    if (push_ctrl(c)) return PIP_ERR_CUDA;
+    stage_ctrl_kernel<<<1, 1, 0, c->stream>>>(c->ctrl, dt, cmax);
+    CK(cudaGetLastError());
     c->cmax = cmax;
   }
   CK(do_stage(c, stage, 0, 0));
   if (stage == 2 && c->hc) {
-    CK(cudaMemcpyAsync(c->d_dt, &c->h_ctrl->dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_dt, &c->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     int it = 0, st = 0;
     const int r = conduct(c, c->d_dt, &it, nullptr, &st);
     if (r != PIP_OK) return r;
     c->hc_iters = it;
   }
-  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
   c->last_stage = stage;
   if (stage == 2) c->last_dt = dt;
+  return PIP_OK;
+}
+
+int pip_ctx_stream(pip_ctx *c, void **stream) {
+  if (!c || !stream) return PIP_ERR_NULL;
+  *stream = (void *)c->stream;
   return PIP_OK;
 }
 
@@ -918,7 +929,6 @@ int pip_halo_pack(pip_ctx *c, int face, void *send, int64_t *bytes) {
   int eb;
   halo_arrays(c, &a0, &a1, &eb);
   CK(pip::halo_pack(c->kp, face, a0, a1, eb, send, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   if (bytes) *bytes = (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1);
   return PIP_OK;
 }
@@ -933,7 +943,6 @@ int pip_halo_unpack(pip_ctx *c, int face, const void *recv, int64_t bytes) {
   if (bytes != (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(pip::halo_unpack(c->kp, face, a0, a1, eb, recv, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   return PIP_OK;
 }
 

@@ -25,8 +25,12 @@ copy.
 
 Blocks are engines with the methods ``cfl() -> (dt, cmax)``, ``stage(k, dt, cmax)``,
 ``halo_bytes(face)``, ``message_bytes(face)``, ``buffer(nbytes)``,
-``pack(face, buf) -> nbytes``, ``unpack(face, buf, nbytes)``, ``has_nan() -> bool``,
-``download()`` and ``close()``; ``DeviceBlock`` is the one on a GPU context.
+``pack(face, buf) -> nbytes``, ``unpack(face, buf, nbytes)``, ``stream()`` (a context
+manager ordering the transfers with the block's own work), ``has_nan() -> bool``,
+``download()`` and ``close()``; ``DeviceBlock`` is the one on a GPU context.  A device
+block's stages, packing and unpacking are queued on its context's stream and the NCCL
+transfers are issued on that stream, so a step waits on the host only in its two cfl
+calls.
 """
 from __future__ import annotations
 
@@ -150,10 +154,10 @@ class TorchComm:
         P2POp = self.dist.P2POp
         ops = [P2POp(self.dist.irecv, t, src, self.group) for _, src, t in recvs]
         ops += [P2POp(self.dist.isend, t, dst, self.group) for _, dst, t in sends]
+        # with NCCL the transfer starts after the current stream's work (the packing) and
+        # wait() makes the current stream wait for it (no host block)
         for q in self.dist.batch_isend_irecv(ops):
             q.wait()
-        if self.torch.cuda.is_available():
-            self.torch.cuda.synchronize()
 
 
 class LocalComm:
@@ -165,8 +169,14 @@ class LocalComm:
 
     def exchange(self, sends, recvs) -> None:
         box = {(src, dst): t for src, dst, t in sends}
+        sync = any(t.is_cuda for _, _, t in recvs)
+        if sync:       # the blocks' streams differ: packing done before the copies ...
+            import torch
+            torch.cuda.synchronize()
         for dst, src, t in recvs:
             t.copy_(box[(src, dst)])
+        if sync:       # ... and the copies before the unpacking
+            torch.cuda.synchronize()
 
 
 # ---------------------------------------------------------------------- engines
@@ -185,6 +195,7 @@ class DeviceBlock:
         self.device = torch.device("cuda", device)
         self.mixed = block.settings.precision != 0
         self.last_stage = 0
+        self._stream = torch.cuda.ExternalStream(self.ctx.stream, device=self.device)
 
     def cfl(self) -> Tuple[float, float]:
         return self.ctx.cfl()
@@ -210,6 +221,11 @@ class DeviceBlock:
 
     def unpack(self, face: int, buf, nbytes: int) -> None:
         self.ctx.halo_unpack(face, buf.data_ptr(), nbytes)
+
+    def stream(self):
+        """Context manager that makes torch work (the NCCL transfers) run in order with the
+        context's stream."""
+        return self.torch.cuda.stream(self._stream)
 
     def has_nan(self) -> bool:
         return bool(self.ctx.status()[1])
@@ -262,7 +278,11 @@ class DecomposedRun:
                         recvs.append((r, e.block.neighbor[recv_face], self._recv[(r, recv_face)][:n]))
                 if not sends and not recvs:
                     continue
-                self.comm.exchange(sends, recvs)
+                if len(self.engines) == 1:
+                    with self.engines[0].stream():
+                        self.comm.exchange(sends, recvs)
+                else:
+                    self.comm.exchange(sends, recvs)
                 for e in self.engines:
                     r = e.block.rank
                     if e.block.neighbor[recv_face] >= 0:

@@ -67,6 +67,10 @@ class OracleBlock:
         nm = self.s.nvar_m
         self.o.set_state(U[nm:], U[:nm])
 
+    def stream(self):
+        import contextlib
+        return contextlib.nullcontext()
+
     def has_nan(self):
         return self.o.has_nan()
 

@@ -43,15 +43,18 @@ def test_halo_pack_unpack_layout(gpu_lib):
         buf = torch.empty(c.halo_bytes(2), dtype=torch.uint8, device="cuda")
         for face, rows in ((2, slice(m, 2 * m)), (3, slice(jx - 2 * m, jx - m))):
             n = c.halo_pack(face, buf.data_ptr())
+            torch.cuda.synchronize()                 # the pack is queued on the context stream
             got = buf[:n].cpu().numpy().view(np.float64).reshape(U.shape[0], m, ix)
             assert np.array_equal(got, U[:, rows, :])
         bufx = torch.empty(c.halo_bytes(0), dtype=torch.uint8, device="cuda")
         n = c.halo_pack(1, bufx.data_ptr())
+        torch.cuda.synchronize()
         got = bufx[:n].cpu().numpy().view(np.float64).reshape(U.shape[0], m, jx)
         assert np.array_equal(got, U[:, :, ix - 2 * m: ix - m].transpose(0, 2, 1))
         # a message into the lower ghost rows, nothing else touched
         msg = np.arange(U.shape[0] * m * ix, dtype=np.float64)
         t = torch.from_numpy(msg).cuda().view(torch.uint8)
+        torch.cuda.synchronize()                     # the message is in place before unpacking
         c.halo_unpack(2, t.data_ptr(), t.numel())
         gh, gm = c.download()
         G = np.concatenate([gm, gh], axis=0)
