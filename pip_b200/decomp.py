@@ -140,6 +140,9 @@ class TorchComm:
         self.world = dist.get_world_size(group)
         self.device = device if device is not None else "cpu"
 
+    def barrier(self) -> None:
+        self.dist.barrier(group=self.group)
+
     def allreduce(self, value: float, op: str) -> float:
         t = self.torch.tensor([value], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN if op == "min" else self.dist.ReduceOp.MAX,
@@ -164,8 +167,13 @@ class LocalComm:
     """Every block in this process (several GPU contexts on one device, or host engines):
     reductions over the blocks and messages as device/host copies."""
 
+    rank = 0
+
     def allreduce(self, value: float, op: str) -> float:
         return value
+
+    def barrier(self) -> None:
+        pass
 
     def exchange(self, sends, recvs) -> None:
         box = {(src, dst): t for src, dst, t in sends}
@@ -318,6 +326,18 @@ class DecomposedRun:
                 if self.comm.allreduce(bad, "max") > 0.0:
                     return 3
         return 0
+
+    def write_output(self, outdir: str, nout: int, s_global) -> None:
+        """output() of the decomposed state (IO_rot.f90:39-105): rank 0 creates the file of
+        the global grid, then every rank writes its block's hyperslab (pip_b200.output)."""
+        from . import output
+        if self.comm.rank == 0:
+            output.create_output(outdir, nout, s_global, self.time)
+        self.comm.barrier()
+        for e in self.engines:
+            U_h, U_m = e.download()
+            output.write_output_block(outdir, nout, s_global, e.block, U_h, U_m)
+        self.comm.barrier()
 
     def close(self) -> None:
         for e in self.engines:

@@ -14,7 +14,7 @@ import decomp_worker
 from decomp_cases import make_case
 from oracle import oracle as O
 from oracle_block import OracleBlock
-from pip_b200 import decomp, ics
+from pip_b200 import decomp, ics, output
 
 
 def single_domain(case, nsteps):
@@ -109,3 +109,21 @@ def test_two_gloo_ranks_match_single_domain(case):
     gh = decomp.gather(s, [g[3] for g in got])
     gm = decomp.gather(s, [g[4] for g in got])
     assert np.array_equal(gh, uh) and np.array_equal(gm, um)
+
+
+def test_decomposed_output_is_the_single_domain_output(tmp_path):
+    """Each block writes its hyperslab of output 1 after 4 steps; the file is the one the
+    single-domain run writes."""
+    s, Uh, Um = make_case("kh")
+    o = O.Oracle(s, Uh, Um)
+    o.run(nsteps=4)
+    oh, om = o.state()
+    ref = output.write_output(str(tmp_path / "one"), 1, s, o.time, oh, om)
+    o.close()
+    engines = [OracleBlock(decomp.block_of(s, 4, r), decomp.scatter(s, Uh, 4, r),
+                           decomp.scatter(s, Um, 4, r)) for r in range(4)]
+    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=False)
+    assert run.run(4) == 0
+    run.write_output(str(tmp_path / "blocks"), 1, s)
+    run.close()
+    assert open(ref, "rb").read() == open(str(tmp_path / "blocks" / "t0001.bin"), "rb").read()
