@@ -16,8 +16,9 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
 * N > 1 GPUs (torchrun, one rank per GPU; or --decompose with one GPU): the y-slab domain
   decomposition of pip_b200.decomp, weak-scaled -- the Orszag-Tang pattern repeated in y
   over [0,1] x [0,N] with one 1024x1024 slab per GPU, a halo exchange (NCCL point-to-point)
-  after each RK stage, dt MIN and cmax MAX over ranks; device time between CUDA events
-  around the step loop, max over ranks; value = N x 1024^2 x steps / time.
+  after each RK stage, the cfl candidates (dt MIN, rho/IR-rate MAX) reduced over ranks on
+  the device between steps; device time between CUDA events around the step loop, max over
+  ranks; value = N x 1024^2 x steps / time.
 * e2e: the same metric through the public C ABI with pinned host buffers:
   pip_upload + pip_run + pip_download, copies inside the timed region.
 * roofline: the stage-2 kernel (the heavier of the two per-step kernels) against the
@@ -266,7 +267,7 @@ def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     eng.ctx.cfl()
     eng.ctx.pipbnd()
     run.halo()
-    if run.run(warmup) != 0:
+    if run.run_device(warmup) != 0:
         raise RuntimeError("decomposed warm-up stopped")
     if dist:
         dist.barrier()
@@ -275,7 +276,7 @@ def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record()
-        st = run.run(steps, check_every=steps)
+        st = run.run_device(steps, check_every=0)
         e1.record()
         torch.cuda.synchronize()
     if st != 0:
@@ -283,9 +284,10 @@ def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     ms = e0.elapsed_time(e1)
     state = eng.download()
     s_blk = b.settings
-    # per step: 2 cfl + 2 stage kernels and, per stage, a pack and an unpack per phase
+    # per step: 2 stage kernels and, per stage, a pack and an unpack per exchanged face
+    # (the cfl is fused into stage 2); one cfl kernel opens the run
     halo_faces = sum(1 for v in b.neighbor if v >= 0)
-    launches = steps * (4 + 2 * 2 * halo_faces)
+    launches = 1 + steps * (2 + 2 * 2 * halo_faces)
     run.close()
     # the stage kernels' own durations on an undecomposed block of the same size
     from pip_b200 import capi
@@ -314,13 +316,13 @@ def e2e_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     eng = decomp.DeviceBlock(b, ph, pm, device=local)
     comm = decomp.TorchComm(device=torch.device("cuda", local)) if dist else decomp.LocalComm()
     run = decomp.DecomposedRun([eng], comm, divb=sg.divb == 1)
-    run.run(warmup)
+    run.run_device(warmup)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     eng.ctx.upload(ph, pm)
-    st = run.run(steps, check_every=steps)
+    st = run.run_device(steps, check_every=0)
     eng.ctx.download(oh, om)
     e2e_s = time.perf_counter() - t0
     run.close()
@@ -553,8 +555,8 @@ def main():
         e2e_s, state_bytes = e2e_decomposed(n, PIP_MIXED, args.steps, args.warmup, dist, local,
                                             world, rank)
         how = ("FP32-mixed, decomposed: pip_upload of each rank's block (pinned FP64 host "
-               "arrays) + %d steps of cfl/allreduce/stage/halo/stage/halo/cfl + pip_download, "
-               "wall clock, max over ranks" % args.steps)
+               "arrays) + %d device-driven steps (stage, halo, stage, halo, cfl-candidate "
+               "allreduce) + pip_download, wall clock, max over ranks" % args.steps)
     else:
         e2e_s, state_bytes = e2e_run(mix["settings"], mix["U"][0], mix["U"][1], args.steps,
                                      args.warmup, dist)

@@ -242,6 +242,36 @@ int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
 int pip_set_neighbors(pip_ctx *ctx, const int neighbor[4]);
 int pip_stage(pip_ctx *ctx, int stage, double dt, double cmax);
 int pip_ctx_stream(pip_ctx *ctx, void **stream);
+
+/*
+ * Device-driven stepping of a decomposed run: the time loop of pip_run (main.f90:31-68)
+ * with dt, cmax, time and the stop flags on the device, and the ranks' cfl reductions done
+ * by the caller on device memory between steps -- no host round trip per step.
+ *
+ *   pip_set_cmax_scale(ctx, s)  once: s = MAX over ranks of safety*min(dx,dy,dz) (cfl's
+ *                               cmax allreduce, Scheme_rot.f90:207-209, taken out of dt)
+ *   pip_dev_begin(ctx, nsteps, t_end)   state as pip_run starts it; queues the first cfl
+ *   reduce the candidates (below), then per step:
+ *     pip_dev_stage(ctx, 1); exchange; pip_dev_stage(ctx, 2); exchange; reduce
+ *   pip_dev_poll(ctx, &done, &time, &steps)   waits for the queued work and reports
+ *
+ * pip_dev_begin waits for the first cfl; pip_dev_stage queues on the context stream and
+ * returns at once.  Stage 1 takes dt = min(dt_cfl, col_lim/rho_max, ir_lim/max(gr_max,
+ * 1e-5)) from the reduced candidates and cmax = s/dt; stage 2 writes the next step's
+ * candidates from its updated cells (the cfl after run_solver and the next step's cfl,
+ * fused).  pip_dev_candidates gives their device addresses: dt_min is 2 int64 to reduce
+ * with MIN, rho_gr_max 4 int64 to reduce with MAX (positive doubles as bit patterns, which
+ * order like the doubles; both slots of each, as they lie in memory).  Every rank must
+ * issue the same calls; a rank whose state stops (NaN, dt floor, last step) keeps
+ * exchanging and reducing while its kernels do nothing, so the collectives stay matched.
+ * pip_dev_poll returns PIP_ERR_NAN / PIP_ERR_DT like pip_run; *done is 1 once the loop has
+ * ended.  Not with flag_heat = 1 (PIP_ERR_PARAM).
+ */
+int pip_set_cmax_scale(pip_ctx *ctx, double safety_min_d);
+int pip_dev_begin(pip_ctx *ctx, int64_t nsteps, double t_end);
+int pip_dev_stage(pip_ctx *ctx, int stage);
+int pip_dev_candidates(pip_ctx *ctx, void **dt_min, void **rho_gr_max);
+int pip_dev_poll(pip_ctx *ctx, int *done, double *time, int64_t *steps);
 int64_t pip_halo_bytes(pip_ctx *ctx, int face);
 int pip_halo_pack(pip_ctx *ctx, int face, void *send, int64_t *bytes);
 int pip_halo_unpack(pip_ctx *ctx, int face, const void *recv, int64_t bytes);

@@ -33,7 +33,8 @@ EXPORTS = (
     "pip_run", "pip_set_time", "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts",
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
-    "pip_halo_unpack", "pip_ctx_stream",
+    "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
+    "pip_dev_candidates", "pip_dev_poll",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -95,6 +96,11 @@ def lib(path: Optional[str] = None):
     L.pip_halo_pack.argtypes = [vp, i, vp, P(ctypes.c_int64)]
     L.pip_halo_unpack.argtypes = [vp, i, vp, ctypes.c_int64]
     L.pip_ctx_stream.argtypes = [vp, P(vp)]
+    L.pip_set_cmax_scale.argtypes = [vp, d]
+    L.pip_dev_begin.argtypes = [vp, ctypes.c_int64, d]
+    L.pip_dev_stage.argtypes = [vp, i]
+    L.pip_dev_candidates.argtypes = [vp, P(vp), P(vp)]
+    L.pip_dev_poll.argtypes = [vp, P(i), dp, P(ctypes.c_int64)]
     L.pip_step_noalloc.restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
@@ -277,6 +283,32 @@ class Context:
         h = ctypes.c_void_p()
         _check(lib().pip_ctx_stream(self.h, ctypes.byref(h)), "pip_ctx_stream")
         return int(h.value or 0)
+
+    def set_cmax_scale(self, sg: float) -> None:
+        _check(lib().pip_set_cmax_scale(self.h, float(sg)), "pip_set_cmax_scale")
+
+    def dev_begin(self, nsteps: int = 0, t_end: float = 0.0) -> None:
+        _check(lib().pip_dev_begin(self.h, int(nsteps), float(t_end)), "pip_dev_begin")
+
+    def dev_stage(self, stage: int) -> None:
+        _check(lib().pip_dev_stage(self.h, int(stage)), "pip_dev_stage")
+
+    def dev_candidates(self) -> Tuple[int, int]:
+        """Device addresses of the cfl candidates: (2 int64 to MIN, 4 int64 to MAX)."""
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().pip_dev_candidates(self.h, ctypes.byref(a), ctypes.byref(b)),
+               "pip_dev_candidates")
+        return int(a.value), int(b.value)
+
+    def dev_poll(self) -> Tuple[int, int, float, int]:
+        """(status, done, time, steps) of the device-driven loop, after waiting for it."""
+        done = ctypes.c_int()
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        st = lib().pip_dev_poll(self.h, ctypes.byref(done), ctypes.byref(t), ctypes.byref(n))
+        if st not in (PIP_OK, PIP_ERR_NAN, PIP_ERR_DT):
+            raise PipError(st, "pip_dev_poll")
+        return st, done.value, t.value, n.value
 
     def halo_bytes(self, face: int) -> int:
         return int(lib().pip_halo_bytes(self.h, int(face)))

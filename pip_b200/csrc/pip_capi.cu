@@ -45,6 +45,7 @@ struct pip_ctx {
   int neighbor[4] = {-1, -1, -1, -1};  // set_mpi_neighbor: rank across each face, -1 physical
   bool exchanged = false;             // some face is filled by the halo exchange
   int last_stage = 0;                 // RK stage that wrote the state last (1: the U1 array)
+  bool dev_loop = false;              // pip_dev_begin has set up the device-driven loop
   bool uploaded = false;
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
@@ -519,6 +520,7 @@ void pip_ctx_destroy(pip_ctx *c) {
 
 int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
   if (!c || !U_h || !U_m) return PIP_ERR_NULL;
+  c->dev_loop = false;
   if (set_device(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(cudaMemcpyAsync(c->A, U_m, pb * c->kp.nvm, cudaMemcpyHostToDevice, c->stream));
@@ -592,6 +594,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
   if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
   c->last_stage = 2;
+  c->dev_loop = false;
   if (set_device(c)) return PIP_ERR_CUDA;
   if ((t_end > 0.0 && c->time >= t_end)) {
     if (time_out) *time_out = c->time;
@@ -887,6 +890,78 @@ int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
   CK(cudaGetLastError());
   c->last_stage = stage;
   if (stage == 2) c->last_dt = dt;
+  return PIP_OK;
+}
+
+int pip_set_cmax_scale(pip_ctx *c, double safety_min_d) {
+  if (!c) return PIP_ERR_NULL;
+  if (!(safety_min_d > 0.0) || !std::isfinite(safety_min_d)) return PIP_ERR_PARAM;
+  c->kp.sg_all = safety_min_d;
+  if (c->graph) {
+    if (set_device(c)) return PIP_ERR_CUDA;
+    CK(cudaStreamSynchronize(c->stream));
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_steps = 0;
+  }
+  return PIP_OK;
+}
+
+int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded || c->hc) return c->hc ? PIP_ERR_PARAM : PIP_ERR_STATE;
+  if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaStreamSynchronize(c->stream));   // nothing queued still reads the pinned block
+  DevCtrl &h = *c->h_ctrl;
+  std::memset(&h, 0, sizeof(DevCtrl));
+  h.time = c->time;
+  h.t_end = t_end > 0.0 ? t_end : 0.0;
+  h.nsteps = nsteps > 0 ? nsteps : 0;
+  h.cmax = c->cmax;
+  reset_slot(h, 0);
+  reset_slot(h, 1);
+  if (push_ctrl(c)) return PIP_ERR_CUDA;
+  CK(do_cfl(c, 0));                         // the first step's cfl candidates (main.f90:36)
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_stage = 0;
+  c->dev_loop = true;
+  return PIP_OK;
+}
+
+int pip_dev_stage(pip_ctx *c, int stage) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->dev_loop) return PIP_ERR_STATE;
+  if (stage != 1 && stage != 2) return PIP_ERR_PARAM;
+  if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(stage == 1 ? do_stage(c, 1, 1, 0) : do_stage(c, 2, 1, -1));
+  c->last_stage = stage;
+  return PIP_OK;
+}
+
+int pip_dev_candidates(pip_ctx *c, void **dt_min, void **rho_gr_max) {
+  if (!c || !dt_min || !rho_gr_max) return PIP_ERR_NULL;
+  *dt_min = (void *)&c->ctrl->red_dt[0];
+  *rho_gr_max = (void *)&c->ctrl->red_rho[0];
+  return PIP_OK;
+}
+
+int pip_dev_poll(pip_ctx *c, int *done, double *time, int64_t *steps) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->dev_loop) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+  const DevCtrl &h = *c->h_ctrl;
+  c->time = h.time;
+  c->dt = h.dt;
+  c->last_dt = h.dt;
+  c->cmax = h.cmax;
+  if (done) *done = (h.done || h.nan_flag) ? 1 : 0;
+  if (time) *time = h.time;
+  if (steps) *steps = h.step;
+  if (h.nan_flag) return PIP_ERR_NAN;
+  if (h.status) return h.status;
   return PIP_OK;
 }
 

@@ -21,10 +21,19 @@
 namespace pip {
 namespace mixed {
 
+// 2D tile height and CTAs per SM of the stage kernels (compile-time tuning constants).
+#ifndef PIP_MIXED_TY
+#define PIP_MIXED_TY 7
+#endif
+#ifndef PIP_MIXED_MINB
+#define PIP_MIXED_MINB 3
+#endif
+
 constexpr int kH = 2;
 template <int NDIM> struct Tile;
 template <> struct Tile<2> {
-  static constexpr int TX = 32, TY = 7, NT = 256;  // 487 faces = two rounds of 256 threads
+  // TY = 7: 487 faces = two rounds of 256 threads
+  static constexpr int TX = 32, TY = PIP_MIXED_TY, NT = (TX * TY + 255) / 256 * 256;
 };
 template <> struct Tile<1> {
   static constexpr int TX = 128, TY = 1, NT = 128;
@@ -77,7 +86,7 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
 // One RK stage (see the FP64 stage_kernel for the structure).  Stage 1: Us = A.hi,
 // U0 = A.hi, output B (FP32).  Stage 2: Us = B, U0 = A.hi + A.lo, output A (hi, lo).
 template <int NDIM, int NVM, int STAGE>
-__global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 3 : 4)
+__global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? PIP_MIXED_MINB : 4)
 stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
              float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;

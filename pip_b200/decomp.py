@@ -11,10 +11,14 @@ and cmax (MAX) over ranks in ``cfl`` (Scheme_rot.f90:200-210).
 
 Here a 2D grid is split along y (rows stay whole, so a y message is a run of contiguous
 rows) and a 1D grid along x.  Each rank's block is a ``Context`` told its neighbours
-(``pip_set_neighbors``); a step is driven from the host:
+(``pip_set_neighbors``).  A step is either driven from the host (``run``):
 
     cfl on every block -> MIN over ranks -> dt;  cmax = MAX over ranks of safety*min(d)/dt
     stage 1 -> halo exchange -> stage 2 -> halo exchange -> cfl (the rewrite of main.f90:47)
+
+or queued on the device (``run_device``, pip_dev_*): stage 1 takes dt and cmax from the cfl
+candidates, stage 2 computes the next step's candidates, and the MIN/MAX over ranks is an
+allreduce of those device words between the steps, so nothing waits on the host.
 
 The exchange has the reference's two phases per direction: every block sends its upper
 interior layers to the neighbour above and receives its lower ghost layers from the
@@ -149,6 +153,13 @@ class TorchComm:
                              group=self.group)
         return float(t.item())
 
+    def reduce_candidates(self, pairs) -> None:
+        """cfl's MIN/MAX allreduces on device memory: pairs = [(t_min, t_max)] of this
+        process's blocks (one), reduced in place over the ranks on the current stream."""
+        for t_min, t_max in pairs:
+            self.dist.all_reduce(t_min, op=self.dist.ReduceOp.MIN, group=self.group)
+            self.dist.all_reduce(t_max, op=self.dist.ReduceOp.MAX, group=self.group)
+
     def exchange(self, sends, recvs) -> None:
         """sends: [(src_rank, dst_rank, tensor)], recvs: [(dst_rank, src_rank, tensor)] for
         this process's blocks; at most one message per ordered pair of ranks.  The sends and
@@ -175,6 +186,18 @@ class LocalComm:
     def barrier(self) -> None:
         pass
 
+    def reduce_candidates(self, pairs) -> None:
+        if len(pairs) < 2:     # one block: the reduction is the identity
+            return
+        import torch
+        torch.cuda.synchronize()
+        lo = torch.stack([a for a, _ in pairs]).min(dim=0).values
+        hi = torch.stack([b for _, b in pairs]).max(dim=0).values
+        for a, b in pairs:
+            a.copy_(lo)
+            b.copy_(hi)
+        torch.cuda.synchronize()
+
     def exchange(self, sends, recvs) -> None:
         box = {(src, dst): t for src, dst, t in sends}
         sync = any(t.is_cuda for _, _, t in recvs)
@@ -188,6 +211,19 @@ class LocalComm:
 
 
 # ---------------------------------------------------------------------- engines
+class _DeviceArray:
+    """A device address as a CUDA-array-interface object (a zero-copy torch view)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False),
+                                         "version": 3, "strides": None, "stream": None}
+
+
+def _device_int64(ptr: int, n: int, device):
+    import torch
+    return torch.as_tensor(_DeviceArray(ptr, n), device=device)
+
+
 class DeviceBlock:
     """A rank's block on a GPU context (``pip_set_neighbors`` + ``pip_stage`` +
     ``pip_halo_pack/unpack``)."""
@@ -211,6 +247,15 @@ class DeviceBlock:
     def stage(self, k: int, dt: float, cmax: float) -> None:
         self.ctx.stage(k, dt, cmax)
         self.last_stage = k
+
+    def dev_stage(self, k: int) -> None:
+        self.ctx.dev_stage(k)
+        self.last_stage = k
+
+    def candidates(self):
+        """int64 views of the device cfl candidates: (2 to MIN, 4 to MAX)."""
+        a, b = self.ctx.dev_candidates()
+        return _device_int64(a, 2, self.device), _device_int64(b, 4, self.device)
 
     def message_bytes(self, face: int) -> int:
         """Length of the message of face f for the state the last stage wrote: the FP32-mixed
@@ -313,6 +358,48 @@ class DecomposedRun:
         self.steps += 1
         self.dt_history.append(dt)
         return dt
+
+    def run_device(self, nsteps: int, check_every: int = 64) -> int:
+        """nsteps steps with dt, cmax and time on the device (pip_dev_*): per step stage 1,
+        exchange, stage 2 (with the next step's cfl candidates), exchange, MIN/MAX of the
+        candidates over ranks -- all queued on the block streams, no host wait; the host
+        checks the stop flags every check_every steps.  Returns 0, 3 (NaN) or 4 (dt floor),
+        the same on every rank."""
+        if not getattr(self, "_scaled", False):
+            sg = self.comm.allreduce(max(e.block.sg for e in self.engines), "max")
+            for e in self.engines:
+                e.ctx.set_cmax_scale(sg)
+            self._scaled = True
+        pairs = [e.candidates() for e in self.engines]
+
+        def reduce():
+            if len(self.engines) == 1:
+                with self.engines[0].stream():
+                    self.comm.reduce_candidates(pairs)
+            else:
+                self.comm.reduce_candidates(pairs)
+
+        for e in self.engines:
+            e.ctx.dev_begin(nsteps=nsteps)
+        reduce()
+        for n in range(nsteps):
+            for e in self.engines:
+                e.dev_stage(1)
+            self.halo()
+            for e in self.engines:
+                e.dev_stage(2)
+            self.halo()
+            reduce()
+            if check_every and (n + 1) % check_every == 0 and n + 1 < nsteps:
+                stop = max(float(e.ctx.dev_poll()[1]) for e in self.engines)
+                if self.comm.allreduce(stop, "max") > 0.0:
+                    break
+        polls = [e.ctx.dev_poll() for e in self.engines]
+        code = max(float(st) for st, _, _, _ in polls)
+        code = int(self.comm.allreduce(code, "max"))
+        self.time = polls[0][2]
+        self.steps = polls[0][3]
+        return code
 
     def run(self, nsteps: int, check_every: int = 1) -> int:
         """nsteps steps with stop_sim's checks (IO_rot.f90:625-674) every check_every steps:

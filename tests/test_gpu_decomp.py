@@ -123,3 +123,42 @@ def test_decomposition_rejects(gpu_lib):
         with pytest.raises(capi.PipError) as e:
             c.set_neighbors([-1, -1, 1, 1])          # conduction folds every side
         assert e.value.code == capi.PIP_ERR_PARAM
+
+
+def device_loop_run(s, Uh, Um, world, nsteps):
+    engines = [decomp.DeviceBlock(decomp.block_of(s, world, r), decomp.scatter(s, Uh, world, r),
+                                  decomp.scatter(s, Um, world, r)) for r in range(world)]
+    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
+    st = run.run_device(nsteps, check_every=4)
+    states = [e.download() for e in engines]
+    run.close()
+    return (st, run.time, run.steps, decomp.gather(s, [a for a, _ in states]),
+            decomp.gather(s, [b for _, b in states]))
+
+
+@pytest.mark.parametrize("case,world", [("ot", 2), ("ot", 4), ("ot_generic", 4), ("kh", 4),
+                                        ("bw", 4)])
+def test_device_loop_blocks_match_pip_run(gpu_lib, case, world):
+    """pip_dev_*: dt, cmax and time stay on the device, the candidates are reduced over the
+    blocks between steps; the result is pip_run's on the whole grid, bitwise."""
+    nsteps = 10
+    s, Uh, Um = make_case(case)
+    st, t, n, hn, mn = device_loop_run(s, Uh, Um, world, nsteps)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        st1, t1, n1 = c.run(nsteps=nsteps)
+        rh, rm = c.download()
+    assert st == 0 and st1 == 0 and n == n1 == nsteps
+    assert t == t1
+    assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
+
+
+def test_device_loop_mixed_matches_pip_run(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(32, precision=PIP_MIXED)
+    st, t, n, hn, mn = device_loop_run(s, Uh, Um, 4, 9)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        st1, t1, n1 = c.run(nsteps=9)
+        rh, rm = c.download()
+    assert st == 0 and n == 9 and t == t1
+    assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
