@@ -63,6 +63,10 @@ FP64_BYTES_PER_CELL_STAGE2 = 3 * 14 * 8
 # mixed: stage 1 R hi + W U1 (4+4 B); stage 2 R U1, hi, lo + W hi, lo (5 x 4 B), per plane
 MIXED_BYTES_PER_CELL_STEP = 14 * (8 + 20)
 MIXED_BYTES_PER_CELL_STAGE2 = 14 * 20
+# FP64 pipe busy time per step of the FP64 stage kernels on OT 1024^2, from the committed
+# ncu capture (profiles/stage_kernel_fp64_ot1024.md: pipe-active fraction x duration,
+# stage 1 0.3278 x 470 us + stage 2 0.3028 x 530.1 us): the compute floor of the FP64 path
+FP64_PIPE_US_PER_STEP = 0.3278 * 470.0 + 0.3028 * 530.1
 L1_NAMES = ["ro_n", "mx_n", "my_n", "mz_n", "en_n", "ro_p", "mx_p", "my_p", "mz_p", "en_p",
             "bx", "by", "bz", "ps"]
 
@@ -599,7 +603,15 @@ def main():
                               "frac": a64 / peak,
                               "traffic": ncu_traffic("stage2_fp64_ot1024"),
                               "algorithmic_bytes_per_cell": FP64_BYTES_PER_CELL_STAGE2,
-                              "ms_stage1": f64["ms1"], "ms_stage2": f64["ms2"]},
+                              "ms_stage1": f64["ms1"], "ms_stage2": f64["ms2"],
+                              "fp64_pipe": {
+                                  "floor_us_per_step": FP64_PIPE_US_PER_STEP,
+                                  "frac": FP64_PIPE_US_PER_STEP / (f64["ms"] / args.steps * 1e3),
+                                  "hbm_floor_us_per_step": FP64_BYTES_PER_CELL_STEP * cells
+                                  / (peak * 1e9) * 1e6,
+                                  "note": "the FP64 pipe, not HBM, bounds the FP64 stage kernels: "
+                                          "its busy time per step (ncu) exceeds the HBM floor "
+                                          "~3.5x, so HBM frac cannot pass ~0.29"}},
                  "gpu_launches": f64["launches"], "clocks": f64["clocks"]},
         "mixed_over_fp64": vmx / v64,
         "l1_mixed_vs_fp64": {
