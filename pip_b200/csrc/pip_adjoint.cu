@@ -456,18 +456,23 @@ __global__ void fold_kernel(const KParams p, double *lam, const int *cells, int 
     if (ntx == 0 && nty == 0) continue;
     const long long nc = p.nc;
     const long long q = (long long)gj * p.ix + gi;
+    // gather every plane's ghost cotangents first, then add them to the cell: the ghost
+    // cells read here are never fold targets, so the loads need not wait for the stores
+    double add[NV];
+#pragma unroll
     for (int n = 0; n < NV; ++n) {
-      double add = 0.0;
+      add[n] = 0.0;
       for (int a = 0; a < ntx; ++a) {
         const double g = (double)p.symx[sx[a]][n];
-        add += g * lam[(long long)gj * p.ix + tx[a] + n * nc];
+        add[n] += g * lam[(long long)gj * p.ix + tx[a] + n * nc];
         for (int b = 0; b < nty; ++b)
-          add += (double)p.symy[sy[b]][n] * g * lam[(long long)ty[b] * p.ix + tx[a] + n * nc];
+          add[n] += (double)p.symy[sy[b]][n] * g * lam[(long long)ty[b] * p.ix + tx[a] + n * nc];
       }
       for (int b = 0; b < nty; ++b)
-        add += (double)p.symy[sy[b]][n] * lam[(long long)ty[b] * p.ix + gi + n * nc];
-      lam[q + n * nc] += add;
+        add[n] += (double)p.symy[sy[b]][n] * lam[(long long)ty[b] * p.ix + gi + n * nc];
     }
+#pragma unroll
+    for (int n = 0; n < NV; ++n) lam[q + n * nc] += add[n];
   }
 }
 
@@ -609,8 +614,10 @@ struct pip_adj {
   size_t state_elems = 0;
   double *A = nullptr, *B = nullptr;
   std::vector<double *> ckpt;   // nseg_max states
-  std::vector<double *> segz;   // K-1 states (z_1 .. z_K-1 of a segment)
-  std::vector<double *> segu;   // K states (U1 of each step of a segment)
+  std::vector<double *> segz[2];  // two sets of K-1 states (z_1 .. z_K-1 of a segment)
+  std::vector<double *> segu[2];  // two sets of K states (U1 of each step of a segment)
+  cudaStream_t stream2 = nullptr;  // recomputation of the next segment during a reverse sweep
+  cudaEvent_t ev_start = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
   double *La = nullptr, *Lb = nullptr;
   double *dt_hist = nullptr;
   double *d_dx = nullptr, *d_dy = nullptr;
@@ -716,13 +723,24 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
   a->ckpt.assign(a->nseg_max, nullptr);
   for (auto &x : a->ckpt)
     if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
-  a->segz.assign(a->K > 1 ? a->K - 1 : 0, nullptr);
-  for (auto &x : a->segz)
-    if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
-  a->segu.assign(a->K, nullptr);
-  for (auto &x : a->segu) {
-    if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemset(x, 0, sb)) != cudaSuccess) return fail(e);
+  // the second set lets the recomputation of segment s-1 run beside the reverse sweep of s
+  for (int set = 0; set < (a->nseg_max > 1 ? 2 : 1); ++set) {
+    a->segz[set].assign(a->K > 1 ? a->K - 1 : 0, nullptr);
+    for (auto &x : a->segz[set])
+      if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
+    a->segu[set].assign(a->K, nullptr);
+    for (auto &x : a->segu[set]) {
+      if ((e = cudaMalloc(&x, sb)) != cudaSuccess) return fail(e);
+      if ((e = cudaMemset(x, 0, sb)) != cudaSuccess) return fail(e);
+    }
+  }
+  if ((e = cudaStreamCreateWithFlags(&a->stream2, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&a->ev_start, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  for (int set = 0; set < 2; ++set) {
+    if ((e = cudaEventCreateWithFlags(&a->ev_rec[set], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(e);
+    if ((e = cudaEventCreateWithFlags(&a->ev_rev[set], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(e);
   }
   if ((e = cudaMalloc(&a->dt_hist, sizeof(double) * max_steps)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->d_dx, sizeof(double) * p->ix)) != cudaSuccess) return fail(e);
@@ -776,10 +794,17 @@ void pip_adj_destroy(pip_adj *a) {
     if (b) cudaFree(b);
   for (double *b : a->ckpt)
     if (b) cudaFree(b);
-  for (double *b : a->segz)
-    if (b) cudaFree(b);
-  for (double *b : a->segu)
-    if (b) cudaFree(b);
+  if (a->stream2) cudaStreamSynchronize(a->stream2);
+  for (int set = 0; set < 2; ++set) {
+    for (double *b : a->segz[set])
+      if (b) cudaFree(b);
+    for (double *b : a->segu[set])
+      if (b) cudaFree(b);
+    if (a->ev_rec[set]) cudaEventDestroy(a->ev_rec[set]);
+    if (a->ev_rev[set]) cudaEventDestroy(a->ev_rev[set]);
+  }
+  if (a->ev_start) cudaEventDestroy(a->ev_start);
+  if (a->stream2) cudaStreamDestroy(a->stream2);
   if (a->cand) cudaFree(a->cand);
   if (a->d_fold) cudaFree(a->d_fold);
   if (a->mx) cudaFree(a->mx);
@@ -866,31 +891,49 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
   const int64_t N = a->steps;
   const int nseg = (int)((N + a->K - 1) / a->K);
   const int gf = grid_fold(a->nfold);
-  for (int s = nseg - 1; s >= 0; --s) {
+  // Segment s is recomputed from its checkpoint into buffer set s % 2 on stream2 while the
+  // reverse sweep of segment s + 1 runs on stream: the recomputation waits for the sweep
+  // that last used its set (segment s + 2), the sweep of s for the recomputation of s.
+  auto zp = [&](int s, int j) -> double * { return j == 0 ? a->ckpt[s] : a->segz[s % 2][j - 1]; };
+  auto recompute = [&](int s) -> int {
     const int64_t n0 = (int64_t)s * a->K;
     const int len = (int)std::min<int64_t>(a->K, N - n0);
-    auto zp = [&](int j) -> double * { return j == 0 ? a->ckpt[s] : a->segz[j - 1]; };
-    // recompute z_n, U1_n of the segment with the recorded dt
+    if (s + 2 < nseg) ACK(cudaStreamWaitEvent(a->stream2, a->ev_rev[s % 2], 0));
+    // z_n, U1_n of the segment with the recorded dt
     for (int j = 0; j < len; ++j) {
       ACK(cudaMemcpyAsync(&a->ctrl->dt, a->dt_hist + n0 + j, sizeof(double), cudaMemcpyDeviceToDevice,
-                          a->stream));
-      ACK(a->L->stage(kp, 1, zp(j), zp(j), a->segu[j], a->ctrl, 0, 0, a->stream));
-      if (j + 1 < len) ACK(a->L->stage(kp, 2, a->segu[j], zp(j), zp(j + 1), a->ctrl, 0, 2, a->stream));
+                          a->stream2));
+      ACK(a->L->stage(kp, 1, zp(s, j), zp(s, j), a->segu[s % 2][j], a->ctrl, 0, 0, a->stream2));
+      if (j + 1 < len)
+        ACK(a->L->stage(kp, 2, a->segu[s % 2][j], zp(s, j), zp(s, j + 1), a->ctrl, 0, 2, a->stream2));
     }
+    ACK(cudaEventRecord(a->ev_rec[s % 2], a->stream2));
+    return PIP_OK;
+  };
+  ACK(cudaEventRecord(a->ev_start, a->stream));
+  ACK(cudaStreamWaitEvent(a->stream2, a->ev_start, 0));
+  int rst = recompute(nseg - 1);
+  if (rst != PIP_OK) return rst;
+  for (int s = nseg - 1; s >= 0; --s) {
+    if (s > 0 && (rst = recompute(s - 1)) != PIP_OK) return rst;
+    const int64_t n0 = (int64_t)s * a->K;
+    const int len = (int)std::min<int64_t>(a->K, N - n0);
+    ACK(cudaStreamWaitEvent(a->stream, a->ev_rec[s % 2], 0));
     // reverse sweep
     for (int j = len - 1; j >= 0; --j) {
       const double *dtp = a->dt_hist + n0 + j;
       pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->La, a->d_fold, a->nfold);
       ACK(cudaGetLastError());
-      ACK(launch_vjp(a, 2, a->segu[j], a->La, nullptr, a->Lb, dtp));
+      ACK(launch_vjp(a, 2, a->segu[s % 2][j], a->La, nullptr, a->Lb, dtp));
       pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->Lb, a->d_fold, a->nfold);
       ACK(cudaGetLastError());
-      ACK(launch_vjp(a, 1, zp(j), a->Lb, a->La, a->La, dtp));
+      ACK(launch_vjp(a, 1, zp(s, j), a->Lb, a->La, a->La, dtp));
       pip::adjk::finalize_kernel<<<1, 256, 0, a->stream>>>(kp, a->nb, a->nbc, a->p1dot, a->p1dac, a->p2dot,
-                                                            a->p2dac, a->cand, dtp, zp(j), a->La,
+                                                            a->p2dac, a->cand, dtp, zp(s, j), a->La,
                                                             a->dcol, nullptr);
       ACK(cudaGetLastError());
     }
+    ACK(cudaEventRecord(a->ev_rev[s % 2], a->stream));
   }
   ACK(cudaMemcpyAsync(g0, a->La, sb, cudaMemcpyDeviceToDevice, a->stream));
   if (device_ms) ACK(cudaEventRecord(e1, a->stream));
