@@ -21,9 +21,9 @@
 //   k3  x' = x + alpha p' + omega t;  r = b - A x';  sums (r0,r), (r,r)     -> beta,
 //       relative residual, stop flag
 // A block owns 128 columns and a range of rows; the inputs of each row are staged into
-// shared memory by bulk async copies several rows ahead, and each thread keeps the 3x3
-// neighbourhood of the vector the matrix is applied to (p', t or x', formed from its inputs
-// once per point) in registers as it walks down its column.  p, Ap and x are
+// shared memory by bulk async copies rows ahead (two stages of two rows), and each thread
+// keeps the 3x3 neighbourhood of the vector the matrix is applied to (p', t or x', formed
+// from its inputs once per point) in registers as it walks down its column.  p, Ap and x are
 // double-buffered (iteration i reads buffer i&1 and writes (i+1)&1), so no kernel reads
 // what it writes.  Scalars are reduced by the last block of each kernel to finish (fixed
 // order: deterministic) into a device block; every kernel returns at once when the stop
@@ -48,7 +48,15 @@ namespace hc {
 
 constexpr int NT = 256;             // one-thread-per-cell kernels
 constexpr int SX = 128;             // BiCGstab kernels: interior columns (threads) per block
-constexpr int NS = 4;               // pipeline stages (rows staged ahead)
+// Pipeline of the BiCGstab kernels: NS stages of RS rows each (compile-time tuning).
+#ifndef PIP_HC_STAGES
+#define PIP_HC_STAGES 2
+#endif
+#ifndef PIP_HC_ROWS
+#define PIP_HC_ROWS 2
+#endif
+constexpr int NS = PIP_HC_STAGES;   // pipeline stages (row groups staged ahead)
+constexpr int RS = PIP_HC_ROWS;     // rows per stage: one wait and one block barrier per group
 constexpr int SLOT = 136;           // elements per staged row segment (SX + 2 + alignment)
 constexpr int kWaitLimit = 1 << 22; // polls of an mbarrier before a block gives up
 constexpr double kEpsi = 1.0e-5;    // HC_rot.f90:17
@@ -336,9 +344,9 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
 
 // The four BiCGstab kernels share one body.  A block owns SX interior columns starting at
 // i0 and a contiguous range of rows [ja, jb); the rows of a column block are divided evenly
-// among its blocks (one wave over the SMs).  For each row j the inputs are staged, NS rows
+// among its blocks (one wave over the SMs).  Rows are staged in groups of RS, NS groups
 // ahead, as row segments copied into shared memory (one bulk copy per segment, one
-// mbarrier per stage):
+// mbarrier per stage; the block waits and synchronises once per group).  For row j:
 //   window vectors (row j+1, columns i0-1 .. i0+SX)   -- the vector A is applied to is
 //                                                        formed from these at each point
 //   own vectors    (row j, columns i0 .. i0+SX-1)
@@ -363,7 +371,7 @@ __host__ __device__ constexpr int n_copies() {
 
 template <typename T, int KIND>
 __host__ __device__ constexpr size_t stage_smem() {
-  return (size_t)NS * n_copies<KIND>() * SLOT * sizeof(T) + NS * sizeof(unsigned long long);
+  return (size_t)NS * RS * n_copies<KIND>() * SLOT * sizeof(T) + NS * sizeof(unsigned long long);
 }
 
 template <typename T>
@@ -407,7 +415,8 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   extern __shared__ __align__(128) unsigned char smem[];
   T *buf = reinterpret_cast<T *>(smem);
   unsigned long long *bar =
-      reinterpret_cast<unsigned long long *>(smem + (size_t)NS * NCP * SLOT * sizeof(T));
+      reinterpret_cast<unsigned long long *>(smem + (size_t)NS * RS * NCP * SLOT * sizeof(T));
+  static_assert(RS * NCP <= 32, "one lane of warp 0 per staged copy");
 
   const int t = threadIdx.x;
   const int cb = blockIdx.x % a.ncb, rb = blockIdx.x / a.ncb;
@@ -418,43 +427,47 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   const int nrows = jb - ja;
   const long long ix = p.ix, nc = p.nc;
 
-  // Warp 0 stages rows: lane c < NCP owns copy c (its source address at row ja, the length
-  // and the allocation end), so a row's copies are set up in parallel.  The first element of
-  // copy c inside its staged segment goes to off[stage][c] for the consumers.
-  __shared__ int off[NS][NCP];
+  // Warp 0 stages row groups: lane rr*NCP + c owns copy c of row rr of a group (its source
+  // address at row ja + rr, the length and the allocation end), so a group's copies are set
+  // up in parallel.  The first element of that copy inside its staged segment goes to
+  // off[stage][rr][c] for the consumers.
+  __shared__ int off[NS][RS][NCP];
   const int lane = t & 31;
+  const int lrow = lane / NCP, lcopy = lane % NCP;
   uintptr_t c_addr = 0, c_cap = 0;
   uint32_t c_len = 0;
-  if (t < 32 && lane < NCP) {
+  if (t < 32 && lane < RS * NCP) {
     const T *base, *lim;
     int dj, di, n;
-    copy_desc<T, KIND>(a, nc, lane, base, dj, di, n, lim);
-    c_addr = (uintptr_t)(base + ((long long)(ja + dj) * ix + i0 + di));
+    copy_desc<T, KIND>(a, nc, lcopy, base, dj, di, n, lim);
+    c_addr = (uintptr_t)(base + ((long long)(ja + lrow + dj) * ix + i0 + di));
     c_len = (uint32_t)(n * sizeof(T));
     c_cap = (uintptr_t)lim & ~(uintptr_t)15;
   }
   const uintptr_t row_bytes = (uintptr_t)ix * sizeof(T);
-  auto issue = [&](int r) {       // warp 0: stage row ja + r
-    const int st = r % NS;
+  auto issue = [&](int g) {       // warp 0: stage rows ja + g*RS .. of group g
+    const int st = g % NS;
     const uint32_t bs = smem_addr(&bar[st]);
     uintptr_t a0 = 0;
     uint32_t bytes = 0;
-    if (lane < NCP) {
-      const uintptr_t ad = c_addr + (uintptr_t)r * row_bytes;
+    if (lane < RS * NCP && g * RS + lrow < nrows) {
+      const uintptr_t ad = c_addr + (uintptr_t)(g * RS) * row_bytes;
       a0 = ad & ~(uintptr_t)15;
       uintptr_t end = (ad + c_len + 15) & ~(uintptr_t)15;
       if (end > c_cap) end = c_cap;
       bytes = (uint32_t)(end - a0);
-      off[st][lane] = (int)((ad - a0) / sizeof(T));
+      off[st][lrow][lcopy] = (int)((ad - a0) / sizeof(T));
     }
     uint32_t total = bytes;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
     if (lane == 0) mbar_expect_tx(bs, total);
     __syncwarp();
-    if (lane < NCP)
-      bulk_load(smem_addr(buf + ((size_t)st * NCP + lane) * SLOT), (const void *)a0, bytes, bs);
+    if (bytes)
+      bulk_load(smem_addr(buf + ((size_t)(st * RS + lrow) * NCP + lcopy) * SLOT), (const void *)a0,
+                bytes, bs);
   };
+  const int ngroups = (nrows + RS - 1) / RS;
 
   if (t == 0) {
     for (int st = 0; st < NS; ++st) mbar_init(smem_addr(&bar[st]), 1u);
@@ -463,8 +476,8 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   }
   __syncthreads();
   if (t < 32)
-    for (int r = 0; r < NS && r < nrows; ++r) issue(r);
-  __syncthreads();                // off[][] of the first stages
+    for (int g = 0; g < NS && g < ngroups; ++g) issue(g);
+  __syncthreads();                // off[][][] of the first stages
 
   // scalars of the update formed at each point
   T s1 = T(0), s2 = T(0);
@@ -506,38 +519,43 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   const T *gy = a.g + 3 * ix;
   double acc0 = 0.0, acc1 = 0.0;
   bool fault = false;
-  int r = 0;
-  for (; r < nrows; ++r) {
-    const int st = r % NS, j = ja + r;
-    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((r / NS) & 1));
+  int g = 0;
+  for (; g < ngroups; ++g) {
+    const int st = g % NS;
+    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((g / NS) & 1));
     if (__syncthreads_or(!ok)) {
       fault = true;
       break;
     }
-    const T *sb = buf + (size_t)st * NCP * SLOT;
+#pragma unroll
+    for (int rr = 0; rr < RS; ++rr) {
+    const int r = g * RS + rr, j = ja + r;
+    if (r >= nrows) break;
+    const T *sb = buf + (size_t)(st * RS + rr) * NCP * SLOT;
+    const int *of = off[st][rr];
     if (active) {
       const long long q = (long long)j * ix + i;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         T v[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = c < NW ? sb[c * SLOT + off[st][c] + t + d] : T(0);
+        for (int c = 0; c < 3; ++c) v[c] = c < NW ? sb[c * SLOT + of[c] + t + d] : T(0);
         w[2][d] = form(v);
       }
       T own[2];
 #pragma unroll
       for (int c = 0; c < 2; ++c)
-        own[c] = c < NO ? sb[(NW + c) * SLOT + off[st][NW + c] + t] : T(0);
+        own[c] = c < NO ? sb[(NW + c) * SLOT + of[NW + c] + t] : T(0);
       constexpr int mc = NW + NO;
-      f.eta = sb[mc * SLOT + off[st][mc] + t];
-      f.fxxl = sb[(mc + 1) * SLOT + off[st][mc + 1] + t];
-      f.fxxr = sb[(mc + 1) * SLOT + off[st][mc + 1] + t + 1];
-      f.fxyl = sb[(mc + 2) * SLOT + off[st][mc + 2] + t];
-      f.fxyr = sb[(mc + 2) * SLOT + off[st][mc + 2] + t + 1];
-      f.fyyd = sb[(mc + 3) * SLOT + off[st][mc + 3] + t];
-      f.fyyu = sb[(mc + 4) * SLOT + off[st][mc + 4] + t];
-      f.fyxd = sb[(mc + 5) * SLOT + off[st][mc + 5] + t];
-      f.fyxu = sb[(mc + 6) * SLOT + off[st][mc + 6] + t];
+      f.eta = sb[mc * SLOT + of[mc] + t];
+      f.fxxl = sb[(mc + 1) * SLOT + of[mc + 1] + t];
+      f.fxxr = sb[(mc + 1) * SLOT + of[mc + 1] + t + 1];
+      f.fxyl = sb[(mc + 2) * SLOT + of[mc + 2] + t];
+      f.fxyr = sb[(mc + 2) * SLOT + of[mc + 2] + t + 1];
+      f.fyyd = sb[(mc + 3) * SLOT + of[mc + 3] + t];
+      f.fyyu = sb[(mc + 4) * SLOT + of[mc + 4] + t];
+      f.fyxd = sb[(mc + 5) * SLOT + of[mc + 5] + t];
+      f.fyxu = sb[(mc + 6) * SLOT + of[mc + 6] + t];
       f.cyd = gy[j];
       f.cyu = gy[p.jx + j];
       f.idy = gy[2 * p.jx + j];
@@ -586,15 +604,16 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
         w[1][d] = w[2][d];
       }
     }
+    }
     __syncthreads();              // stage st is free again
-    if (t < 32 && r + NS < nrows) issue(r + NS);
+    if (t < 32 && g + NS < ngroups) issue(g + NS);
   }
   if (fault) {
-    // a staged row never arrived: flag it, let the copies still in flight land (bounded),
+    // a staged group never arrived: flag it, let the copies still in flight land (bounded),
     // and leave the scalars alone (the host reads the flag and stops)
     if (t == 0) {
       atomicExch(&sc->fault, 1);
-      for (int k = r; k < nrows && k < r + NS; ++k)
+      for (int k = g; k < ngroups && k < g + NS; ++k)
         mbar_wait(smem_addr(&bar[k % NS]), (uint32_t)((k / NS) & 1));
     }
     return;
