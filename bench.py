@@ -65,8 +65,8 @@ MIXED_BYTES_PER_CELL_STEP = 14 * (8 + 20)
 MIXED_BYTES_PER_CELL_STAGE2 = 14 * 20
 # FP64 pipe busy time per step of the FP64 stage kernels on OT 1024^2, from the committed
 # ncu capture (profiles/stage_kernel_fp64_ot1024.md: pipe-active fraction x duration,
-# stage 1 0.3278 x 470 us + stage 2 0.3028 x 530.1 us): the compute floor of the FP64 path
-FP64_PIPE_US_PER_STEP = 0.3278 * 470.0 + 0.3028 * 530.1
+# stage 1 0.4188 x 278.5 us + stage 2 0.3919 x 303.3 us): the compute floor of the FP64 path
+FP64_PIPE_US_PER_STEP = 0.4188 * 278.5 + 0.3919 * 303.3
 L1_NAMES = ["ro_n", "mx_n", "my_n", "mz_n", "en_n", "ro_p", "mx_p", "my_p", "mz_p", "en_p",
             "bx", "by", "bz", "ps"]
 
@@ -611,7 +611,7 @@ def main():
                                   / (peak * 1e9) * 1e6,
                                   "note": "the FP64 pipe, not HBM, bounds the FP64 stage kernels: "
                                           "its busy time per step (ncu) exceeds the HBM floor "
-                                          "~3.5x, so HBM frac cannot pass ~0.29"}},
+                                          "~2.6x, so HBM frac cannot pass ~0.38"}},
                  "gpu_launches": f64["launches"], "clocks": f64["clocks"]},
         "mixed_over_fp64": vmx / v64,
         "l1_mixed_vs_fp64": {
