@@ -28,3 +28,34 @@ def rank_main(rank, world, port, case, nsteps, q):
         dist.destroy_process_group()
     except Exception as e:   # reported to the parent, which fails the test
         q.put((rank, "error", repr(e), None, None))
+
+
+def reduce_main(rank, world, port, q):
+    """cfl-candidate reduction of the device-driven loop over a gloo group: each rank holds
+    its candidates as int64 bit patterns of positive doubles (dt words to MIN, rho/IR-rate
+    words to MAX); the reduced words must be the bit patterns of the doubles' MIN/MAX."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    for p in (here, os.path.dirname(here)):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from pip_b200 import decomp
+    try:
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                                world_size=world, timeout=datetime.timedelta(seconds=60))
+        comm = decomp.TorchComm("cpu")
+        rng = np.random.default_rng(100 + rank)
+        dt = rng.uniform(1e-5, 1e-2, 2)
+        mx = rng.uniform(0.0, 1e4, 4)
+        t_min = torch.from_numpy(dt.view(np.int64).copy())
+        t_max = torch.from_numpy(mx.view(np.int64).copy())
+        comm.reduce_candidates([(t_min, t_max)])
+        comm.barrier()
+        q.put((rank, dt, mx, t_min.numpy().view(np.float64).copy(),
+               t_max.numpy().view(np.float64).copy()))
+        dist.destroy_process_group()
+    except Exception as e:
+        q.put((rank, "error", repr(e), None, None))

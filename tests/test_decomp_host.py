@@ -127,3 +127,26 @@ def test_decomposed_output_is_the_single_domain_output(tmp_path):
     run.write_output(str(tmp_path / "blocks"), 1, s)
     run.close()
     assert open(ref, "rb").read() == open(str(tmp_path / "blocks" / "t0001.bin"), "rb").read()
+
+
+def test_candidate_reduction_over_two_gloo_ranks():
+    """The device-driven loop's reduction (TorchComm.reduce_candidates): MIN of the dt words
+    and MAX of the rho/IR-rate words as int64 bit patterns equal the doubles' MIN/MAX."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=decomp_worker.reduce_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        got = sorted((q.get(timeout=120) for _ in procs), key=lambda x: x[0])
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(not isinstance(g[1], str) for g in got), got
+    want_min = np.minimum(got[0][1], got[1][1])
+    want_max = np.maximum(got[0][2], got[1][2])
+    for g in got:
+        assert np.array_equal(g[3], want_min) and np.array_equal(g[4], want_max)
