@@ -22,8 +22,11 @@ namespace pip {
 namespace mixed {
 
 // 2D tile height and CTAs per SM of the stage kernels (compile-time tuning constants).
+#ifndef PIP_MIXED_TX
+#define PIP_MIXED_TX 16
+#endif
 #ifndef PIP_MIXED_TY
-#define PIP_MIXED_TY 7
+#define PIP_MIXED_TY 14
 #endif
 #ifndef PIP_MIXED_MINB
 #define PIP_MIXED_MINB 3
@@ -32,8 +35,9 @@ namespace mixed {
 constexpr int kH = 2;
 template <int NDIM> struct Tile;
 template <> struct Tile<2> {
-  // TY = 7: 487 faces = two rounds of 256 threads
-  static constexpr int TX = 32, TY = PIP_MIXED_TY, NT = (TX * TY + 255) / 256 * 256;
+  // 16x14 cells: 17x14 x faces + 16x15 y faces = 478 faces, two rounds of 256 threads;
+  // primitives for 20x18 - 16 = 344 cells (1.54 per updated cell; 1.70 with 32x7)
+  static constexpr int TX = PIP_MIXED_TX, TY = PIP_MIXED_TY, NT = (TX * TY + 255) / 256 * 256;
 };
 template <> struct Tile<1> {
   static constexpr int TX = 128, TY = 1, NT = 128;

@@ -17,9 +17,16 @@ namespace PIP_FLAVOUR {
 constexpr int kH = 2;  // stencil half-width of minmod MUSCL
 
 template <int NDIM> struct Tile;
-// 32x7 cells: 33x7 x faces + 32x8 y faces = 487 faces = two rounds of 256 threads.
+// 2D tile (compile-time tuning constants; 32x7 cells: 33x7 x faces + 32x8 y faces = 487
+// faces = two rounds of 256 threads).
+#ifndef PIP_FP64_TX
+#define PIP_FP64_TX 32
+#endif
+#ifndef PIP_FP64_TY
+#define PIP_FP64_TY 7
+#endif
 template <> struct Tile<2> {
-  static constexpr int TX = 32, TY = 7, NT = 256;
+  static constexpr int TX = PIP_FP64_TX, TY = PIP_FP64_TY, NT = (TX * TY + 255) / 256 * 256;
 };
 template <> struct Tile<1> {
   static constexpr int TX = 128, TY = 1, NT = 128;
