@@ -179,9 +179,21 @@ def cpu_sample(target_s: float = 15.0, threads: int = 0):
                       % (steps, threads), "s_per_step": one}
 
 
+def workload_text(n, world, decomposed):
+    """The workload of the bench line: the single-GPU Orszag-Tang run, or its weak-scaled
+    decomposition over `world` GPUs."""
+    if not decomposed:
+        return WORKLOAD
+    return ("Orszag-Tang pattern repeated in y: %dx%d cells over [0,1]x[0,%d] (periodic), one "
+            "%dx%d y-slab per GPU, halo exchange of 2 ghost rows x 14 planes after each RK "
+            "stage (NCCL point-to-point), dt MIN and cmax MAX over ranks; physics as the "
+            "1024x1024 run" % (n, n * world, world, n, n))
+
+
 def run_reference(args):
     """--impl reference: the reference algorithm on host cores (CPU restatement)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     budget = float(os.environ.get("PIP_REF_BUDGET_S", "90"))
@@ -206,14 +218,11 @@ def run_reference(args):
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": n, "warmup": 1, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": (WORKLOAD if not decomposed else
-                                "Orszag-Tang pattern repeated in y: %dx%d cells over [0,1]x[0,%d] "
-                                "(periodic), one %dx%d y-slab per GPU, halo exchange of 2 ghost "
-                                "rows x 14 planes after each RK stage (NCCL point-to-point), dt MIN "
-                                "and cmax MAX over ranks; physics as the 1024x1024 run"
-                                % (n, n * world, world, n, n)),
+        "config": {"workload": workload_text(N_GRID, world, world > 1 or args.decompose),
                    "cells": cells * world, "precision": "fp64",
-                   "parallelism": "host OpenMP, %d threads" % threads},
+                   "parallelism": "host OpenMP, %d threads" % threads,
+                   "host_sample": "one %dx%d block on the host cores (the per-cell rate of the "
+                                  "workload)" % (N_GRID, N_GRID)},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": "%d of the requested %d steps (time budget %.0f s)"
                                    % (n, args.steps, budget)},
@@ -585,12 +594,7 @@ def main():
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64-mixed", "data": "synthetic",
-        "config": {"workload": (WORKLOAD if not decomposed else
-                                "Orszag-Tang pattern repeated in y: %dx%d cells over [0,1]x[0,%d] "
-                                "(periodic), one %dx%d y-slab per GPU, halo exchange of 2 ghost "
-                                "rows x 14 planes after each RK stage (NCCL point-to-point), dt MIN "
-                                "and cmax MAX over ranks; physics as the 1024x1024 run"
-                                % (n, n * world, world, n, n)),
+        "config": {"workload": workload_text(n, world, decomposed),
                    "cells": cells * world,
                    "precision": "FP32-mixed (FP32 fluxes/state, FP64 source and compensated "
                                 "RK accumulation)",
