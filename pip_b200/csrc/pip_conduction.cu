@@ -899,10 +899,10 @@ cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, 
   } else {
     // iterative refinement: FP64 residual of the FP64 matrix, FP32 BiCGstab on the
     // correction, FP64 update of x[0]; at most hc_max inner iterations in total.  A loose
-    // inner tolerance wins: each refinement restarts BiCGstab where it converges fastest,
-    // while a tight FP32 solve stagnates near FP32 precision (KH 2048x1024, kapper 0.01:
-    // 21.6 inner iterations per step at 3e-3, 23.4 at 1e-3, 35.5 at 1e-4, 29 at 1e-6;
-    // 23 at 1e-2, where the refinements themselves add up).
+    // inner tolerance: each refinement restarts BiCGstab where it converges fastest, while
+    // a tight FP32 solve stagnates near FP32 precision (KH 2048x1024, kapper 0.01, first 60
+    // steps: 21.6 inner iterations per step at 3e-3, 23.4 at 1e-3, 35.5 at 1e-4, 29 at
+    // 1e-6, 23 at 1e-2; over 1000 steps 18.4 at 3e-3 against 19.3 at 1e-4).
 #ifndef PIP_HC_INNER_TOL
 #define PIP_HC_INNER_TOL 3.0e-3
 #endif
