@@ -58,7 +58,8 @@ enum pip_ir_law {
  * (Model_rot.f90:39-333) and set_coordinate (Model_rot.f90:394-458) have run.
  * Supported subset (anything else returns PIP_ERR_PARAM):
  *   flag_eqs=PIP (two-fluid), flag_sch=0, flag_hll=2, s_order=2, t_order=2, flag_time=0,
- *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col=1 (constant col),
+ *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col 1..7 (2..7 with
+ *   precision PIP_FP64 only),
  *   flag_pip_imp 0/1, flag_ir 0 or PIP_IR_POWERLAW with flag_ir_type 1 or 2,
  *   flag_bnd in {1,2,3,4,5,6,7,10,11}, no resistivity/viscosity/gravity/ambipolar.
  */
@@ -75,7 +76,10 @@ typedef struct pip_params {
   int32_t t_order;         /* 2: midpoint RK2 */
   int32_t flag_time;       /* 0: standard RK (Solver_rot.f90:203-220) */
   int32_t flag_divb;       /* 1: Dedner 9-wave cleaning */
-  int32_t flag_col;        /* 1: alpha_c = col everywhere (set_collisional col_type 0) */
+  int32_t flag_col;        /* 1: alpha_c = col everywhere (set_collisional col_type 0);
+                              2..7: col_type 1..6, alpha_c per cell from both species'
+                              temperatures (and drift) at the start of every RK stage
+                              (PIP_rot.f90:44-97, set_coefficients Solver_rot.f90:95-122) */
   int32_t flag_pip_imp;    /* 0: explicit collision source; 1: exponential form */
   int32_t flag_ir;         /* pip_ir_law */
   int32_t flag_ir_type;    /* IR energy exchange: 1 Khomenko, 2 Singh (PIP_rot.f90:1399-1411) */
@@ -98,7 +102,8 @@ typedef struct pip_params {
   double ir_rec_coef;      /* recombination rate coefficient */
   double kapper;           /* Spitzer coefficient: kappa_par = kapper*T^2.5 */
   double hc_error;         /* BiCGstab relative residual target */
-  double reserved_d[7];
+  double beta;             /* plasma beta of set_collisional col_type 1, 3, 5 (> 0 there) */
+  double reserved_d[6];
   const double *dx;        /* ix cell widths (dsc(:,1)) */
   const double *dy;        /* jx cell widths (dsc(:,2)); 1D: one entry, the reference sets 100 */
   const double *dz;        /* kx cell widths (dsc(:,3)); one entry, the reference sets 100 */
@@ -187,6 +192,21 @@ int pip_flux(pip_ctx *ctx, int dir, double *F_h, double *F_m);
  * flag_pip_imp=1 it returns the increments the exponential form adds to U0
  * (-dt_coll*dS for the neutrals, +dt_coll*dS for the ions). */
 int pip_source(pip_ctx *ctx, double dt_coll, double *S_h, double *S_m);
+
+/* set_coefficients(U_h,U_m,1) (Solver_rot.f90:95-122), collision part: with flag_col
+ * 2..7, set_collisional (PIP_rot.f90:44-97) rewrites both energies through the floored
+ * pressure (get_Te_MHD/get_Te_HD, Scheme_rot.f90:83-128) and sets alpha_c per cell from
+ * the temperatures and the drift; pip_source then uses that field.  No-op for flag_col 1.
+ * pip_step, pip_run and pip_stage make the field themselves at the start of every stage.
+ * After pip_upload the first call that needs the field (pip_cfl, pip_step, pip_run,
+ * pip_stage, pip_flux, pip_source, pip_dev_begin, pip_get_alpha_c) runs this first, as
+ * the prologue's set_coefficients(U_h,U_m,0) (Initial_rot.f90:140) does. */
+int pip_coefficients(pip_ctx *ctx);
+
+/* alpha_c per cell (ix*jx doubles, Fortran order; the globalvar `ac` array that output()
+ * saves as "ac", IO_rot.f90:235): the field of the last set_collisional, or col
+ * everywhere for flag_col 1. */
+int pip_get_alpha_c(pip_ctx *ctx, double *ac);
 
 /* PIPbnd(U_h,U_m,0) (Boundary_rot.f90:34-52) on the device state; with one rank the
  * MPI halo exchange (MPI_rot.f90:128-339) reduces to this ghost fill. */

@@ -65,6 +65,9 @@ def lib():
         L.orc_conduction.argtypes = [vp, d, P(ctypes.c_int), dp]
         L.orc_conduction.restype = ctypes.c_int
         L.orc_has_nan.restype = ctypes.c_int
+        L.orc_coefficients.argtypes = [vp]
+        L.orc_alpha_c.argtypes = [vp, dp]
+        L.orc_alpha_c.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -169,6 +172,16 @@ class Oracle:
 
     def fill_ghosts(self) -> None:
         lib().orc_bnd(self.h)
+
+    def coefficients(self) -> None:
+        """set_coefficients' collision part: flag_col 2..7 rewrites the energies, sets alpha_c."""
+        lib().orc_coefficients(self.h)
+
+    def alpha_c(self) -> np.ndarray:
+        """alpha_c of every cell, shaped like one plane of the state."""
+        a = np.empty(self.shape_h[1:])
+        lib().orc_alpha_c(self.h, _ptr(a))
+        return a
 
     def prologue(self) -> None:
         """The prologue's cfl and ghost fill (Initial_rot.f90:152-160)."""

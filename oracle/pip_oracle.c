@@ -23,6 +23,7 @@
 #define HLLG_FACTOR 1.001            /* HLL_rot.f90:702 */
 #define MU_P 0.5                     /* initialize_collisional, PIP_rot.f90:35 */
 #define MU_N 1.0                     /* PIP_rot.f90:36 */
+#define PI_REF 3.1415926535897932    /* Parameters.f90:2 */
 
 struct orc_ctx {
   pip_params p;
@@ -36,7 +37,12 @@ struct orc_ctx {
   int neighbor[6];                   /* set_mpi_neighbor: rank across each face, -1 physical */
   double *U_h0, *U_m0;               /* run_solver's U0 between orc_stage calls */
   double stage_dt;
+  int col_type;                      /* initialize_collisional: flag_col 2..7 -> 1..6 */
+  double *ac;                        /* alpha_c per cell (globalvar ac) for col_type >= 1 */
+  int ac_valid;                      /* set by the first set_collisional */
 };
+
+static void ensure_ac(orc_ctx *c);
 
 static int g_threads = 1;
 
@@ -613,6 +619,7 @@ static void flux_dir(orc_ctx *c, int dir, double *F_h, double *F_m) {
 }
 
 void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m) {
+  ensure_ac(c);
   memset(F_h, 0, sizeof(double) * c->nc * c->nh);
   memset(F_m, 0, sizeof(double) * c->nc * c->nm);
   flux_dir(c, dir, F_h, F_m);
@@ -641,13 +648,80 @@ static void set_ir_rates(orc_ctx *c) {
   }
 }
 
+/* alpha_c of set_collisional's col_type 1..6 (PIP_rot.f90:53-95) for one cell from the two
+ * temperatures and the drift, with the Fortran operation order (left to right). */
+static double alpha_c_cell(int type, double col, double beta, double gm, double te_h, double te_m,
+                           double vdx, double vdy, double vdz) {
+  double T = te_h + te_m;
+  double a = col * sqrt(T / 2.0);
+  if (type == 1) return a / sqrt(beta / 2.0 * gm);
+  if (type == 2) return a;
+  double v2 = vdx * vdx + vdy * vdy + vdz * vdz;     /* sum(vd**2,dim=4) */
+  a = a * sqrt(1.0 + 9.0 * PI_REF / 64.0 * gm / 2.0 * v2 / T);
+  if (type == 3) return a / sqrt(beta / 2.0 * gm);
+  if (type == 4) return a;
+  if (type == 5)
+    return a / sqrt(beta / 2.0 * gm) * pow((beta / 2.0 * gm) / T / 2.0 + gm * PI_REF / 16.0 * v2, 0.125);
+  return a / pow(T / 2.0 + gm * PI_REF / 16.0 * v2, 0.125);
+}
+
+/* set_collisional for col_type >= 1 (PIP_rot.f90:44-97): get_Te_MHD and get_Te_HD
+ * (Scheme_rot.f90:83-128) rewrite both energies through the floored pressure and give
+ * Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro; get_vel_diff (:988-999) gives the drift; alpha_c of
+ * every cell, ghosts included, goes to c->ac.  The floor `if(minval(pr).le.pr_lim)
+ * pr=max(pr,pr_lim)` is the per-cell max. */
+static void set_collisional(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  double gm = p->gm, pr_lim = p->pr_lim, col = p->col, beta = p->beta;
+  int type = c->col_type;
+  double *Um = c->U_m, *Uh = c->U_h;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double m1 = Um[q], m2 = Um[q + nc], m3 = Um[q + 2 * nc], m4 = Um[q + 3 * nc];
+    double m6 = Um[q + 5 * nc], m7 = Um[q + 6 * nc], m8 = Um[q + 7 * nc];
+    double prm = (gm - 1.0) * (Um[q + 4 * nc] -
+                               0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 + m7 * m7 + m8 * m8));
+    prm = fmx(prm, pr_lim);
+    Um[q + 4 * nc] = prm / (gm - 1.0) + 0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 +
+                                               m7 * m7 + m8 * m8);
+    double te_m = 0.5 * gm * (prm / m1);
+    double h1 = Uh[q], h2 = Uh[q + nc], h3 = Uh[q + 2 * nc], h4 = Uh[q + 3 * nc];
+    double prh = (gm - 1.0) * (Uh[q + 4 * nc] - 0.5 * (h2 * h2 + h3 * h3 + h4 * h4) / h1);
+    prh = fmx(prh, pr_lim);
+    Uh[q + 4 * nc] = prh / (gm - 1.0) + 0.5 * ((h2 * h2 + h3 * h3 + h4 * h4) / h1);
+    double te_h = gm * (prh / h1);
+    c->ac[q] = alpha_c_cell(type, col, beta, gm, te_h, te_m, h2 / h1 - m2 / m1, h3 / h1 - m3 / m1,
+                            h4 / h1 - m4 / m1);
+  }
+  c->ac_valid = 1;
+}
+
+/* The alpha_c field of the last set_collisional, made by set_coefficients(U_h,U_m,0)
+ * (Initial_rot.f90:140) on the state as it stands when nothing has made one yet. */
+static void ensure_ac(orc_ctx *c) {
+  if (c->col_type >= 1 && !c->ac_valid) set_collisional(c);
+}
+
+void orc_coefficients(orc_ctx *c) {
+  if (c->col_type >= 1) set_collisional(c);
+}
+
+int orc_alpha_c(orc_ctx *c, double *ac) {
+  size_t nc = c->nc;
+  ensure_ac(c);
+  for (size_t q = 0; q < nc; ++q) ac[q] = c->col_type >= 1 ? c->ac[q] : c->p.col;
+  return 0;
+}
+
 /* source_PIP, PIP_rot.f90:1309-1429 (explicit and exponential collision forms plus the
  * IR block with flag_IR_type 1 or 2).  out_h/out_m receive S (explicit form) or the U0
  * increments of the exponential form, plus the IR rates in S. */
 static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, double *S_h,
                        double *S_m) {
   size_t nc = c->nc;
-  double gm = c->p.gm, ac = c->p.col;
+  double gm = c->p.gm;
+  const double *acf = c->col_type >= 1 ? c->ac : NULL;
   double *w = malloc(sizeof(double) * nc * 13);
   double *nde = w, *nvx = w + nc, *nvy = w + 2 * nc, *nvz = w + 3 * nc, *npr = w + 4 * nc;
   double *de = w + 5 * nc, *vx = w + 6 * nc, *vy = w + 7 * nc, *vz = w + 8 * nc, *pr = w + 9 * nc;
@@ -657,6 +731,7 @@ static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, d
   int imp = c->p.flag_pip_imp == 1;
 #pragma omp parallel for schedule(static)
   for (size_t q = 0; q < nc; ++q) {
+    double ac = acf ? acf[q] : c->p.col;
     double te = pr[q] / de[q] * gm * MU_P;
     double nte = npr[q] / nde[q] * gm * MU_N;
     double ds[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -719,6 +794,7 @@ static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, d
 
 void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m) {
   size_t nc = c->nc;
+  ensure_ac(c);
   memset(S_h, 0, sizeof(double) * nc * c->nh);
   memset(S_m, 0, sizeof(double) * nc * c->nm);
   if (c->p.flag_pip_imp == 1) {
@@ -737,6 +813,8 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
   double gm = p->gm, safety = p->safety, ac = p->col;
+  ensure_ac(c);
+  const double *acf = c->col_type >= 1 ? c->ac : NULL;
   double *w = malloc(sizeof(double) * nc * 8);
   double *de = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc, *pr = w + 4 * nc;
   double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
@@ -779,8 +857,9 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   double mm = -INFINITY, mh = -INFINITY;
 #pragma omp parallel for reduction(max : mm, mh) schedule(static)
   for (size_t q = 0; q < nc; ++q) {
-    mm = fmx(mm, c->U_m[q] * ac);
-    mh = fmx(mh, c->U_h[q] * ac);
+    double a = acf ? acf[q] : ac;
+    mm = fmx(mm, c->U_m[q] * a);
+    mh = fmx(mh, c->U_h[q] * a);
   }
   if (p->flag_pip_imp == 1) dttemp = fmn(dttemp, p->pip_imp_factor / fmx(mm, mh));
   else dttemp = fmn(dttemp, fmn(safety, 0.3) / fmx(mm, mh));
@@ -1075,6 +1154,7 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   size_t nc = c->nc;
   int nh = c->nh, nm = c->nm, t_order = p->t_order;
   if (istep == 1) {
+    ensure_ac(c);
     if (!c->U_h0) c->U_h0 = malloc(sizeof(double) * nc * nh);
     if (!c->U_m0) c->U_m0 = malloc(sizeof(double) * nc * nm);
     memcpy(c->U_h0, c->U_h, sizeof(double) * nc * nh);
@@ -1086,6 +1166,8 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   double *S_h = malloc(sizeof(double) * nc * nh), *S_m = malloc(sizeof(double) * nc * nm);
   double dt_coll[2] = {dt * 0.5, dt * 0.5};
   double dt_coll_i = dt_coll[t_order - istep];
+  /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_col >= 2 recomputes alpha_c */
+  if (c->col_type >= 1) set_collisional(c);
   for (int dir = 1; dir <= p->ndim; ++dir)
     flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
   memset(S_h, 0, sizeof(double) * nc * nh);
@@ -1154,6 +1236,7 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   if (!p || p->ndim < 1 || p->ndim > 2 || p->kx != 1 || p->nvar_h != 5) return NULL;
   if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return NULL;
   if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0))) return NULL;
+  if (p->flag_col < 1 || p->flag_col > 7) return NULL;
   orc_ctx *c = calloc(1, sizeof(orc_ctx));
   c->p = *p;
   for (int f = 0; f < 6; ++f) c->neighbor[f] = -1;
@@ -1170,6 +1253,8 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   c->U_m = calloc(c->nc * c->nm, sizeof(double));
   c->gm_ion = calloc(c->nc, sizeof(double));
   c->gm_rec = calloc(c->nc, sizeof(double));
+  c->col_type = p->flag_col >= 2 ? p->flag_col - 1 : 0;   /* PIP_rot.f90:21-26 */
+  if (c->col_type >= 1) c->ac = calloc(c->nc, sizeof(double));
   set_sym_mhd(c);
   set_sym_hd(c);
   *status = PIP_OK;
@@ -1181,6 +1266,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->dx); free(c->dy); free(c->dz);
   free(c->U_h); free(c->U_m); free(c->gm_ion); free(c->gm_rec);
   free(c->U_h0); free(c->U_m0);
+  free(c->ac);
   free(c);
 }
 

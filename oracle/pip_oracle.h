@@ -47,6 +47,13 @@ void orc_set_neighbors(orc_ctx *c, const int nb[4]);
 void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m);
 /* PIP_rot.f90:1309-1429; returns S (explicit) or the U0 increments (exponential form). */
 void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m);
+/* set_coefficients (Solver_rot.f90:95-122) for the collision coefficient: with flag_col
+ * 2..7, set_collisional (PIP_rot.f90:44-97) rewrites both energies and sets alpha_c per
+ * cell; a no-op for flag_col 1. */
+void orc_coefficients(orc_ctx *c);
+/* alpha_c of every cell (col for flag_col 1), made from the current state when no
+ * set_collisional has run yet (Initial_rot.f90:140). */
+int orc_alpha_c(orc_ctx *c, double *ac);
 /* Boundary_rot.f90:34-52. */
 void orc_bnd(orc_ctx *c);
 /* main.f90:31-68 loop; returns 0, PIP_ERR_NAN or PIP_ERR_DT.  dt_hist (may be NULL)

@@ -34,7 +34,7 @@ EXPORTS = (
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
-    "pip_dev_candidates", "pip_dev_poll",
+    "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -86,6 +86,8 @@ def lib(path: Optional[str] = None):
     L.pip_flux.argtypes = [vp, i, dp, dp]
     L.pip_source.argtypes = [vp, d, dp, dp]
     L.pip_fill_ghosts.argtypes = [vp]
+    L.pip_coefficients.argtypes = [vp]
+    L.pip_get_alpha_c.argtypes = [vp, dp]
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
     L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
@@ -135,7 +137,8 @@ def lib(path: Optional[str] = None):
     L.pip_kernels_per_run.restype = ctypes.c_int64
     for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",
                  "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts", "pip_status",
-                 "pip_conduction", "pip_last_cuda_error", "pip_run_timed", "pip_bench_stage_ms"):
+                 "pip_conduction", "pip_last_cuda_error", "pip_run_timed", "pip_bench_stage_ms",
+                 "pip_coefficients", "pip_get_alpha_c"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -266,6 +269,16 @@ class Context:
 
     def pipbnd(self) -> None:
         _check(lib().pip_fill_ghosts(self.h), "pip_fill_ghosts")
+
+    def coefficients(self) -> None:
+        """set_coefficients' collision part (flag_col 2..7: energies rewritten, alpha_c set)."""
+        _check(lib().pip_coefficients(self.h), "pip_coefficients")
+
+    def alpha_c(self) -> np.ndarray:
+        """alpha_c of every cell, shaped like one plane of the state."""
+        a = np.empty(self.shape_h[1:])
+        _check(lib().pip_get_alpha_c(self.h, _ptr(a)), "pip_get_alpha_c")
+        return a
 
     # ------------------------------------------------------------------ domain decomposition
     def set_neighbors(self, neighbor) -> None:

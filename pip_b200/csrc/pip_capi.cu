@@ -47,6 +47,9 @@ struct pip_ctx {
   int last_stage = 0;                 // RK stage that wrote the state last (1: the U1 array)
   bool dev_loop = false;              // pip_dev_begin has set up the device-driven loop
   bool uploaded = false;
+  double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
+  bool ac_valid = false;              // acf holds the last set_collisional's field
+  bool ac_fresh = false;              // ... made over every cell, no stage since
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
   size_t plane_bytes() const { return sizeof(double) * (size_t)kp.nc; }
@@ -136,7 +139,12 @@ int validate(const pip_params *p) {
   if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return PIP_ERR_PARAM;
   if (p->flag_sch != 0 || p->flag_hll != 2 || p->s_order != 2 || p->t_order != 2 || p->flag_time != 0)
     return PIP_ERR_PARAM;
-  if (p->flag_col != 1) return PIP_ERR_PARAM;
+  // flag_col 1: constant alpha_c; 2..7: set_collisional col_type 1..6 (PIP_rot.f90:21-26),
+  // per-cell alpha_c in the FP64 form, beta > 0 where alpha_c divides by sqrt(beta*gm/2)
+  if (p->flag_col < 1 || p->flag_col > 7) return PIP_ERR_PARAM;
+  if (p->flag_col >= 2 && p->precision != PIP_FP64) return PIP_ERR_PARAM;
+  if ((p->flag_col == 2 || p->flag_col == 4 || p->flag_col == 6) && !(p->beta > 0.0))
+    return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
@@ -196,6 +204,9 @@ void build_kparams(pip_ctx *c) {
   k.decay[1] = std::exp(-1.0 * p.safety * p.db_clean);
   k.dz0 = c->dz[0];
   k.hc_kapper = p.kapper;
+  k.col_type = p.flag_col >= 2 ? p.flag_col - 1 : 0;
+  k.ac_b2g = p.beta / 2.0 * p.gm;
+  k.ac_sb = std::sqrt(k.ac_b2g);
   for (int s = 0; s < 2; ++s) {
     const int fx = s, fy = 2 + s;
     k.typex[s] = bnd_type(p.flag_bnd[fx]);
@@ -232,6 +243,8 @@ void pip::record_cuda_error(int code) { g_last_cuda_error = code; }
 int pip::kparams_from_params(const pip_params *p, KParams *k) {
   const int st = validate(p);
   if (st != PIP_OK) return st;
+  // the per-cell alpha_c field lives in a context
+  if (p->flag_col != 1) return PIP_ERR_PARAM;
   *k = KParams{};
   k->ndim = p->ndim;
   k->ix = p->ix;
@@ -329,6 +342,17 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
   ctrl->blocks_done = 0;
 }
 
+// The alpha_c field for a state that no set_collisional has seen since its upload:
+// set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140) rewrites the energies
+// and sets alpha_c before the first cfl and the first stage.
+int ensure_ac(pip_ctx *c) {
+  if (!c->kp.col_type || c->ac_valid) return PIP_OK;
+  CK(c->L->coefficients(c->kp, c->A, c->stream));
+  c->ac_valid = true;
+  c->ac_fresh = true;
+  return PIP_OK;
+}
+
 int push_ctrl(pip_ctx *c) {
   CK(cudaMemcpyAsync(c->ctrl, c->h_ctrl, sizeof(DevCtrl), cudaMemcpyHostToDevice, c->stream));
   return PIP_OK;
@@ -336,6 +360,7 @@ int push_ctrl(pip_ctx *c) {
 
 // One RK stage of the context's precision form.
 cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
+  if (stage == 2) c->ac_fresh = false;
   if (c->mixed) {
     if (stage == 1)
       return pip::mixed_stage(c->kp, 1, c->Ahi, c->Ahi, nullptr, c->Bf, nullptr, c->ctrl, dt_mode,
@@ -349,7 +374,9 @@ cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
 
 cudaError_t do_cfl(pip_ctx *c, int slot) {
   if (c->mixed) return pip::mixed_cfl(c->kp, c->Ahi, c->Alo, c->ctrl, slot, c->stream);
-  return c->L->cfl(c->kp, c->A, c->ctrl, slot, c->stream);
+  KParams k = c->kp;
+  k.ac_all = c->ac_fresh ? 1 : 0;
+  return c->L->cfl(k, c->A, c->ctrl, slot, c->stream);
 }
 
 // The mixed form keeps its state in (hi, lo); these move it through the FP64 array A.
@@ -475,6 +502,11 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   c->kp.dx = c->d_dx;
   c->kp.dy = c->d_dy;
   if ((e = cudaMalloc(&c->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
+  if (c->kp.col_type) {
+    if ((e = cudaMalloc(&c->acf, c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->acf, 0, c->plane_bytes())) != cudaSuccess) return fail(e);
+    c->kp.acf = c->acf;
+  }
   if (p->flag_heat == 1 && (e = pip::hc_create(c->kp, c->mixed, &c->hc)) != cudaSuccess)
     return fail(e);
   if (c->mixed) {
@@ -512,6 +544,7 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->ctrl);
   cudaFree(c->d_flag);
   cudaFree(c->d_dt);
+  cudaFree(c->acf);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -528,6 +561,7 @@ int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
   CK(from_fp64(c));
   CK(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
+  c->ac_valid = false;
   c->last_stage = 0;
   return PIP_OK;
 }
@@ -548,6 +582,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
+  if (ensure_ac(c)) return PIP_ERR_CUDA;
   reset_slot(*c->h_ctrl, 0);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
@@ -565,6 +600,7 @@ int pip_step(pip_ctx *c, double dt) {
   if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
   if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
+  if (ensure_ac(c)) return PIP_ERR_CUDA;
   DevCtrl &h = *c->h_ctrl;
   h.dt = dt;
   h.cmax = c->cmax;
@@ -596,6 +632,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   c->last_stage = 2;
   c->dev_loop = false;
   if (set_device(c)) return PIP_ERR_CUDA;
+  if (ensure_ac(c)) return PIP_ERR_CUDA;
   if ((t_end > 0.0 && c->time >= t_end)) {
     if (time_out) *time_out = c->time;
     if (steps_done) *steps_done = 0;
@@ -622,6 +659,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
+  c->ac_fresh = false;                      // the stages below (a graph may hold them)
   if (c->hc) {
     // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
     // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
@@ -710,6 +748,7 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
   h.nsteps = nsteps;
   reset_slot(h, 0);
   reset_slot(h, 1);
+  if (ensure_ac(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
   std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
@@ -739,8 +778,8 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
 }
 
 int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
-  (void)c;
-  return 1 + 2 * (nsteps > 0 ? nsteps : 0);
+  const int64_t init = c && c->kp.col_type && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
+  return init + 1 + 2 * (nsteps > 0 ? nsteps : 0);
 }
 
 int64_t pip_conduction_iterations(pip_ctx *c) { return c ? c->hc_iters : 0; }
@@ -762,7 +801,7 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
   if (!c->uploaded) return PIP_ERR_STATE;
   if (dir < 1 || dir > c->kp.ndim) return PIP_ERR_PARAM;
   if (c->mixed) return PIP_ERR_STATE;  // unit-level entry points are FP64 only
-  if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
+  if (set_device(c) || ensure_scratch(c) || ensure_ac(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(cudaMemsetAsync(c->scratch, 0, pb * c->nplanes(), c->stream));
   CK(c->L->flux(c->kp, c->A, c->scratch, dir, c->cmax, c->stream));
@@ -776,12 +815,37 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
 int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
   if (!c || !S_h || !S_m) return PIP_ERR_NULL;
   if (!c->uploaded || c->mixed) return PIP_ERR_STATE;
-  if (set_device(c) || ensure_scratch(c)) return PIP_ERR_CUDA;
+  if (set_device(c) || ensure_scratch(c) || ensure_ac(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(c->L->source(c->kp, c->A, c->scratch, dt_coll, c->stream));
   CK(cudaMemcpyAsync(S_m, c->scratch, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(S_h, c->scratch + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost,
                      c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_coefficients(pip_ctx *c) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->kp.col_type) return PIP_OK;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(c->L->coefficients(c->kp, c->A, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ac_valid = true;
+  c->ac_fresh = true;
+  return PIP_OK;
+}
+
+int pip_get_alpha_c(pip_ctx *c, double *ac) {
+  if (!c || !ac) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->kp.col_type) {
+    for (long long q = 0; q < c->kp.nc; ++q) ac[q] = c->p.col;
+    return PIP_OK;
+  }
+  if (set_device(c) || ensure_ac(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(ac, c->acf, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PIP_OK;
 }
@@ -875,6 +939,7 @@ int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
   if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (stage == 1) {
+    if (ensure_ac(c)) return PIP_ERR_CUDA;
     stage_ctrl_kernel<<<1, 1, 0, c->stream>>>(c->ctrl, dt, cmax);
     CK(cudaGetLastError());
     c->cmax = cmax;
@@ -921,6 +986,7 @@ int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
   h.cmax = c->cmax;
   reset_slot(h, 0);
   reset_slot(h, 1);
+  if (ensure_ac(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));                         // the first step's cfl candidates (main.f90:36)
   CK(cudaStreamSynchronize(c->stream));

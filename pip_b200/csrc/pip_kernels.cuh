@@ -31,6 +31,12 @@ struct KParams {
   double decay[2];   // Dedner psi factor exp(-(dt_sub/dt)*safety*db_clean) per stage
   double dz0;        // dz(1)
   double hc_kapper;  // Spitzer coefficient of the implicit conduction (kapper)
+  int col_type;      // set_collisional col_type: 0 constant alpha_c, 1..6 per cell (FP64 form)
+  double ac_b2g;     // beta/2*gm of col_type 1, 3, 5
+  double ac_sb;      // sqrt(beta/2*gm)
+  double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
+  int ac_all;        // acf made over every cell since the last stage: the cfl counts the ghosts
+                     // of exchanged faces too (else the neighbouring block counts them)
   const double *dx, *dy;
   const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]
@@ -61,6 +67,7 @@ struct Launchers {
                       cudaStream_t s);
   cudaError_t (*source)(const KParams &p, double *U, double *S, double dt_coll, cudaStream_t s);
   cudaError_t (*nan_scan)(const KParams &p, const double *U, int *flag, cudaStream_t s);
+  cudaError_t (*coefficients)(const KParams &p, double *U, cudaStream_t s);
 };
 
 const Launchers &launchers_fast();

@@ -99,13 +99,59 @@ __device__ __forceinline__ void ir_rates(const double (&u)[NVM], const KParams &
   gi = p.ir_ion * rs * exp(-p.ir_chi / te);
 }
 
+constexpr double kPiRef = 3.1415926535897932;  // pi of Parameters.f90:2
+
+// get_Te_MHD and get_Te_HD (Scheme_rot.f90:83-128) on one cell: the pressures with the
+// floor (`if(minval(pr).le.pr_lim) pr=max(pr,pr_lim)` is the per-cell max), the energies
+// um[4], uh[4] rewritten from them, and the temperatures Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro.
+template <int NVM>
+__device__ __forceinline__ void get_te(double (&um)[NVM], double (&uh)[5], const KParams &p,
+                                       double &te_m, double &te_h) {
+  const double gm = p.gm;
+  double pr = (gm - 1.0) * (um[4] - 0.5 * ((um[1] * um[1] + um[2] * um[2] + um[3] * um[3]) / um[0] +
+                                           um[5] * um[5] + um[6] * um[6] + um[7] * um[7]));
+  pr = fmax(pr, p.pr_lim);
+  um[4] = pr / (gm - 1.0) + 0.5 * ((um[1] * um[1] + um[2] * um[2] + um[3] * um[3]) / um[0] +
+                                   um[5] * um[5] + um[6] * um[6] + um[7] * um[7]);
+  te_m = 0.5 * gm * (pr / um[0]);
+  double ph = (gm - 1.0) * (uh[4] - 0.5 * (uh[1] * uh[1] + uh[2] * uh[2] + uh[3] * uh[3]) / uh[0]);
+  ph = fmax(ph, p.pr_lim);
+  uh[4] = ph / (gm - 1.0) + 0.5 * ((uh[1] * uh[1] + uh[2] * uh[2] + uh[3] * uh[3]) / uh[0]);
+  te_h = gm * (ph / uh[0]);
+}
+
+// set_collisional for col_type 1..6 (PIP_rot.f90:44-97) on one cell: rewrites the energies
+// (get_te) and returns alpha_c from Te_h + Te_m and the drift of get_vel_diff
+// (Scheme_rot.f90:988-999), in the Fortran operation order.
+template <int NVM>
+__device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double (&uh)[5],
+                                                       const KParams &p) {
+  double te_m, te_h;
+  get_te<NVM>(um, uh, p, te_m, te_h);
+  const double gm = p.gm, T = te_h + te_m;
+  double a = p.ac * sqrt(T / 2.0);
+  const int type = p.col_type;
+  if (type == 1) return a / p.ac_sb;
+  if (type == 2) return a;
+  const double vdx = uh[1] / uh[0] - um[1] / um[0];
+  const double vdy = uh[2] / uh[0] - um[2] / um[0];
+  const double vdz = uh[3] / uh[0] - um[3] / um[0];
+  const double v2 = vdx * vdx + vdy * vdy + vdz * vdz;
+  a = a * sqrt(1.0 + 9.0 * kPiRef / 64.0 * gm / 2.0 * v2 / T);
+  if (type == 3) return a / p.ac_sb;
+  if (type == 4) return a;
+  if (type == 5) return a / p.ac_sb * pow(p.ac_b2g / T / 2.0 + gm * kPiRef / 16.0 * v2, 0.125);
+  return a / pow(T / 2.0 + gm * kPiRef / 16.0 * v2, 0.125);
+}
+
 // Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
-// rewritten states um/uh and their primitives.
+// rewritten states um/uh, their primitives and the cell's alpha_c.
 template <int NVM>
 __device__ __forceinline__ void collision_ds(const double (&um)[NVM], const double (&uh)[5],
                                              const Prim<double> &qm, const Prim<double> &qh,
-                                             const KParams &p, double dt_coll, double (&ds)[5]) {
-  const double gm = p.gm, ac = p.ac;
+                                             const KParams &p, double ac, double dt_coll,
+                                             double (&ds)[5]) {
+  const double gm = p.gm;
   const double te = qm.pr / qm.de * gm * kMuP;
   const double nte = qh.pr / qh.de * gm * kMuN;
   ds[0] = 0.0;
@@ -177,7 +223,8 @@ __device__ __forceinline__ bool near_boundary(const KParams &p, int gi, int gj) 
 }
 
 template <int NDIM>
-__device__ __forceinline__ void write_ghosts(const KParams &p, int gi, int gj, double *U, int nplanes) {
+__device__ __forceinline__ void write_ghosts(const KParams &p, int gi, int gj, double *U, int nplanes,
+                                             bool unsigned_plane = false) {
   const long long nc = p.nc;
   const long long q = (long long)gj * p.ix + gi;
   int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
@@ -199,13 +246,18 @@ __device__ __forceinline__ void write_ghosts(const KParams &p, int gi, int gj, d
   for (int n = 0; n < nplanes; ++n) {
     const double v = U[q + n * nc];
     for (int a = 0; a < ntx; ++a) {
+      if (unsigned_plane) {
+        U[(long long)gj * p.ix + tx[a] + n * nc] = v;
+        for (int b = 0; b < nty; ++b) U[(long long)ty[b] * p.ix + tx[a] + n * nc] = v;
+        continue;
+      }
       const double g = (double)p.symx[sx[a]][n];
       U[(long long)gj * p.ix + tx[a] + n * nc] = g * v;
       for (int b = 0; b < nty; ++b)
         U[(long long)ty[b] * p.ix + tx[a] + n * nc] = (double)p.symy[sy[b]][n] * (g * v);
     }
     for (int b = 0; b < nty; ++b)
-      U[(long long)ty[b] * p.ix + gi + n * nc] = (double)p.symy[sy[b]][n] * v;
+      U[(long long)ty[b] * p.ix + gi + n * nc] = unsigned_plane ? v : (double)p.symy[sy[b]][n] * v;
   }
 }
 
@@ -259,8 +311,9 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
 // (time_integral) and the ghost fill (PIPbnd).  STAGE 2 optionally fuses the two cfl
 // calls that follow run_solver and open the next step (main.f90:47 and :36): epi = 1
 // applies one cq2pv rewrite; epi = 2 applies two and reduces the next dt; epi = -1 takes
-// 1 or 2 from the control block's last-step flag.
-template <int NDIM, int NVM, int STAGE>
+// 1 or 2 from the control block's last-step flag.  VC: alpha_c per cell (col_type >= 1),
+// a separate instance so that the constant-alpha_c kernels keep their register budget.
+template <int NDIM, int NVM, int STAGE, bool VC>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
 stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
              DevCtrl *ctrl, int dt_mode, int epi) {
@@ -337,6 +390,11 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     if (gi >= p.ix || gj >= p.jx) continue;
     double um[NVM], uh[5], vm[NVM], vh[5];
     load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
+    if (VC) {
+      // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux
+      double te_m, te_h;
+      get_te<NVM>(um, uh, p, te_m, te_h);
+    }
     u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
     u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
 #pragma unroll
@@ -433,6 +491,9 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     } else {
       load_cell<NVM>(Us, q, nc, s_m, s_h);
     }
+    // alpha_c of the stage (set_coefficients at the stage start; U0 keeps its energies)
+    double ac_s = p.ac;
+    if (VC) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
     double gr = 0.0, gion = 0.0;
     if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
 
@@ -443,9 +504,11 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       for (int n = 0; n < NVM; ++n) r_m[n] = a_m[n];
 #pragma unroll
       for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
+      double ac_r = p.ac;
+      if (VC) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
       const Prim<double> qh = rt_hd(r_h, p);
       const Prim<double> qm = rt_mhd<NVM>(r_m, p);
-      collision_ds<NVM>(r_m, r_h, qm, qh, p, dt_coll, ds);
+      collision_ds<NVM>(r_m, r_h, qm, qh, p, ac_r, dt_coll, ds);
 #pragma unroll
       for (int n = 0; n < 5; ++n) {
         a_h[n] = a_h[n] - dt_coll * ds[n];
@@ -458,7 +521,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       const Prim<double> qh = rt_hd(s_h, p);
       const Prim<double> qm = rt_mhd<NVM>(s_m, p);
       double ds[5];
-      collision_ds<NVM>(s_m, s_h, qm, qh, p, dt_coll, ds);
+      collision_ds<NVM>(s_m, s_h, qm, qh, p, ac_s, dt_coll, ds);
       if (p.imp) {
 #pragma unroll
         for (int n = 0; n < 5; ++n) {
@@ -517,7 +580,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       const double sg = p.safety * gmin;
       dtc = fmin(cfl_mhd_cell<double>(qm, n_m[5], n_m[6], n_m[7], gm, sg),
                  cfl_hd_cell<double>(qh, gm, sg));
-      rhoc = fmax(n_m[0] * p.ac, n_h[0] * p.ac);
+      rhoc = fmax(n_m[0] * ac_s, n_h[0] * ac_s);
       if (p.ir) {
         double g1, g2;
         ir_rates<NVM>(n_m, p, g1, g2);
@@ -531,6 +594,11 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
     if (bad) atomicOr(&ctrl->nan_flag, 1);
     store_cell<NDIM, NVM>(Uo, p, gi, gj, n_m, n_h);
+    if (STAGE == 2 && VC) {
+      // the alpha_c field that the next cfl reads (cfl_pn_col, Scheme_rot.f90:305-313)
+      p.acf[q] = ac_s;
+      if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
+    }
   }
   if (STAGE == 2 && s_epi == 2) {
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
@@ -555,6 +623,12 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       }
     }
   }
+}
+
+// A ghost cell of a face whose layers come from the halo exchange (source -1).
+__device__ __forceinline__ bool exchanged_ghost(const KParams &p, int i, int j) {
+  if ((i < p.m0 && p.gx[0][0] < 0) || (i >= p.ix - p.m0 && p.gx[1][0] < 0)) return true;
+  return p.ndim == 2 && ((j < p.m1 && p.gy[0][0] < 0) || (j >= p.jx - p.m1 && p.gy[1][0] < 0));
 }
 
 // cfl (Scheme_rot.f90:183-213) as a standalone pass over every cell: cq2pv rewrite of
@@ -583,7 +657,15 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
       dtc = fmin(dtc, fmin(cfl_mhd_cell<double>(qm, um[5], um[6], um[7], gm, sg),
                            cfl_hd_cell<double>(qh, gm, sg)));
     }
-    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (!p.col_type) {
+      rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    } else if (p.ac_all || !exchanged_ghost(p, i, j)) {
+      // after a stage, the ghosts of faces filled by the halo exchange are the neighbour's
+      // interior cells, counted there; every other ghost equals its source cell's rho and
+      // alpha_c
+      const double a = p.acf[q];
+      rhoc = fmax(rhoc, fmax(um[0] * a, uh[0] * a));
+    }
     if (p.ir) {
       double g1, g2;
       ir_rates<NVM>(um, p, g1, g2);
@@ -711,7 +793,7 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
     const Prim<double> qh = rt_hd(uh, p);
     const Prim<double> qm = rt_mhd<NVM>(um, p);
     double ds[5], sm[5], sh[5];
-    collision_ds<NVM>(um, uh, qm, qh, p, dt_coll, ds);
+    collision_ds<NVM>(um, uh, qm, qh, p, p.col_type ? p.acf[q] : p.ac, dt_coll, ds);
     for (int n = 0; n < 5; ++n) {
       if (p.imp) {
         sh[n] = 0.0 - dt_coll * ds[n];
@@ -738,6 +820,21 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
   }
 }
 
+// set_collisional over every cell (set_coefficients, Solver_rot.f90:95-122, col_type >= 1):
+// both energies rewritten in place, alpha_c into p.acf.
+template <int NVM>
+__global__ void coefficients_kernel(const KParams p, double *U) {
+  const long long nc = p.nc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nc;
+       q += (long long)gridDim.x * blockDim.x) {
+    double um[NVM], uh[5];
+    load_cell<NVM>(U, q, nc, um, uh);
+    p.acf[q] = set_collisional_cell<NVM>(um, uh, p);
+    U[q + 4 * nc] = um[4];
+    U[q + (NVM + 4) * nc] = uh[4];
+  }
+}
+
 __global__ void nan_kernel(const double *__restrict__ U, long long n, int *flag) {
   int bad = 0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -758,7 +855,11 @@ constexpr size_t stage_smem_bytes() {
 
 template <int NDIM, int NVM, int STAGE>
 static cudaError_t set_stage_attr() {
-  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE>,
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stage_smem_bytes<NDIM, NVM>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE, true>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)stage_smem_bytes<NDIM, NVM>());
 }
@@ -781,7 +882,10 @@ static cudaError_t launch_stage_t(const KParams &p, const double *Us, const doub
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   const size_t shm = stage_smem_bytes<NDIM, NVM>();
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
-  stage_kernel<NDIM, NVM, STAGE><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
+  if (p.col_type)
+    stage_kernel<NDIM, NVM, STAGE, true><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
+  else
+    stage_kernel<NDIM, NVM, STAGE, false><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
   return cudaGetLastError();
 }
 
@@ -835,6 +939,13 @@ static cudaError_t launch_source(const KParams &p, double *U, double *S, double 
   return cudaGetLastError();
 }
 
+static cudaError_t launch_coefficients(const KParams &p, double *U, cudaStream_t s) {
+  if (!p.col_type) return cudaSuccess;
+  if (p.nvm == 9) coefficients_kernel<9><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
+  else coefficients_kernel<8><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
+  return cudaGetLastError();
+}
+
 static cudaError_t launch_nan(const KParams &p, const double *U, int *flag, cudaStream_t s) {
   const long long n = p.nc * (p.nvm + 5);
   nan_kernel<<<grid_for(n, 256), 256, 0, s>>>(U, n, flag);
@@ -847,7 +958,7 @@ const Launchers &PIP_LAUNCHERS() {
   static const Launchers L = {PIP_FLAVOUR::prepare,       PIP_FLAVOUR::launch_stage,
                               PIP_FLAVOUR::launch_cfl,    PIP_FLAVOUR::launch_ghosts,
                               PIP_FLAVOUR::launch_flux,   PIP_FLAVOUR::launch_source,
-                              PIP_FLAVOUR::launch_nan};
+                              PIP_FLAVOUR::launch_nan,    PIP_FLAVOUR::launch_coefficients};
   return L;
 }
 

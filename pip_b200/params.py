@@ -66,7 +66,8 @@ class PipParams(ctypes.Structure):
         ("ir_rec_coef", ctypes.c_double),
         ("kapper", ctypes.c_double),
         ("hc_error", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 7),
+        ("beta", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 6),
         ("dx", ctypes.POINTER(ctypes.c_double)),
         ("dy", ctypes.POINTER(ctypes.c_double)),
         ("dz", ctypes.POINTER(ctypes.c_double)),
@@ -113,6 +114,7 @@ class Settings:
     n_fraction: float = 0.5
     col: float = 100.0
     flag_col: int = 1
+    beta: float = 0.1
     flag_pip_imp: int = 0
     pip_imp_factor: float = 10.0
     flag_ir: int = 0
@@ -220,8 +222,12 @@ class Settings:
             bad.append("only flag_sch=0, flag_hll=2 (HLLD/HLLC) is supported")
         if self.s_order != 2 or self.t_order != 2 or self.flag_time != 0:
             bad.append("only s_order=2, t_order=2, flag_time=0 is supported")
-        if self.flag_col != 1:
-            bad.append("only flag_col=1 (constant alpha_c) is supported")
+        if self.flag_col not in range(1, 8):
+            bad.append("flag_col must be 1..7 (set_collisional col_type 0..6)")
+        elif self.flag_col >= 2 and self.precision != PIP_FP64:
+            bad.append("flag_col 2..7 (alpha_c per cell) needs precision PIP_FP64")
+        elif self.flag_col in (2, 4, 6) and not self.beta > 0.0:
+            bad.append("flag_col %d divides by sqrt(beta*gm/2): beta must be > 0" % self.flag_col)
         if self.flag_resi or self.flag_amb or self.flag_visc or self.flag_grav:
             bad.append("resistivity, ambipolar, viscosity and gravity are not supported")
         if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW):
@@ -279,6 +285,7 @@ class Settings:
         p.ir_rec_coef = self.ir_rec_coef
         p.kapper = self.kapper
         p.hc_error = self.hc_error
+        p.beta = self.beta
         dptr = ctypes.POINTER(ctypes.c_double)
         p.dx = dx.ctypes.data_as(dptr)
         p.dy = dy.ctypes.data_as(dptr)
@@ -300,7 +307,7 @@ class Settings:
         reals = {"gm_d": "gm_d", "gm_n": "gm_n", "safety": "safety", "db_clean": "db_clean",
                  "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
                  "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",
-                 "kapper": "kapper", "tend": "tend"}
+                 "kapper": "kapper", "tend": "tend", "beta": "beta"}
         bnd = {"flag_bnd_x_l": 0, "flag_bnd_x_r": 1, "flag_bnd_y_l": 2, "flag_bnd_y_r": 3,
                "flag_bnd_z_l": 4, "flag_bnd_z_r": 5}
         for raw in text.splitlines():

@@ -54,8 +54,9 @@ def _create(s, **field):
 
 @pytest.mark.parametrize("field", [
     dict(abi_version=PIP_ABI_VERSION + 1), dict(ndim=3), dict(flag_sch=1), dict(flag_hll=0),
-    dict(s_order=1), dict(t_order=4), dict(flag_time=1), dict(flag_col=3), dict(nvar_m=9),
-    dict(flag_ir=4), dict(precision=7), dict(flag_pip_imp=2),
+    dict(s_order=1), dict(t_order=4), dict(flag_time=1), dict(flag_col=0), dict(flag_col=8),
+    dict(flag_col=3, precision=1), dict(flag_col=2, beta=0.0), dict(flag_col=6, beta=-1.0),
+    dict(nvar_m=9), dict(flag_ir=4), dict(precision=7), dict(flag_pip_imp=2),
 ])
 def test_rejects_unsupported_parameters(lib, field):
     s, _, _ = ics.brio_wu(64)
