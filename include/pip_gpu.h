@@ -208,6 +208,11 @@ int pip_coefficients(pip_ctx *ctx);
  * everywhere for flag_col 1. */
 int pip_get_alpha_c(pip_ctx *ctx, double *ac);
 
+/* Restart's read of the "ac" dataset (reread_variables, IO_rot.f90:570-572): sets the
+ * field the first cfl after a pip_upload uses instead of making one from the state.
+ * No-op for flag_col 1. */
+int pip_set_alpha_c(pip_ctx *ctx, const double *ac);
+
 /* PIPbnd(U_h,U_m,0) (Boundary_rot.f90:34-52) on the device state; with one rank the
  * MPI halo exchange (MPI_rot.f90:128-339) reduces to this ghost fill. */
 int pip_fill_ghosts(pip_ctx *ctx);

@@ -49,7 +49,6 @@ struct pip_ctx {
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
   bool ac_valid = false;              // acf holds the last set_collisional's field
-  bool ac_fresh = false;              // ... made over every cell, no stage since
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
   size_t plane_bytes() const { return sizeof(double) * (size_t)kp.nc; }
@@ -349,7 +348,6 @@ int ensure_ac(pip_ctx *c) {
   if (!c->kp.col_type || c->ac_valid) return PIP_OK;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   c->ac_valid = true;
-  c->ac_fresh = true;
   return PIP_OK;
 }
 
@@ -360,7 +358,6 @@ int push_ctrl(pip_ctx *c) {
 
 // One RK stage of the context's precision form.
 cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
-  if (stage == 2) c->ac_fresh = false;
   if (c->mixed) {
     if (stage == 1)
       return pip::mixed_stage(c->kp, 1, c->Ahi, c->Ahi, nullptr, c->Bf, nullptr, c->ctrl, dt_mode,
@@ -374,9 +371,7 @@ cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
 
 cudaError_t do_cfl(pip_ctx *c, int slot) {
   if (c->mixed) return pip::mixed_cfl(c->kp, c->Ahi, c->Alo, c->ctrl, slot, c->stream);
-  KParams k = c->kp;
-  k.ac_all = c->ac_fresh ? 1 : 0;
-  return c->L->cfl(k, c->A, c->ctrl, slot, c->stream);
+  return c->L->cfl(c->kp, c->A, c->ctrl, slot, c->stream);
 }
 
 // The mixed form keeps its state in (hi, lo); these move it through the FP64 array A.
@@ -659,7 +654,6 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
-  c->ac_fresh = false;                      // the stages below (a graph may hold them)
   if (c->hc) {
     // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
     // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
@@ -833,7 +827,6 @@ int pip_coefficients(pip_ctx *c) {
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->ac_valid = true;
-  c->ac_fresh = true;
   return PIP_OK;
 }
 
@@ -847,6 +840,17 @@ int pip_get_alpha_c(pip_ctx *c, double *ac) {
   if (set_device(c) || ensure_ac(c)) return PIP_ERR_CUDA;
   CK(cudaMemcpyAsync(ac, c->acf, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_set_alpha_c(pip_ctx *c, const double *ac) {
+  if (!c || !ac) return PIP_ERR_NULL;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->kp.col_type) return PIP_OK;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(c->acf, ac, c->plane_bytes(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ac_valid = true;
   return PIP_OK;
 }
 

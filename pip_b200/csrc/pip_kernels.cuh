@@ -35,8 +35,6 @@ struct KParams {
   double ac_b2g;     // beta/2*gm of col_type 1, 3, 5
   double ac_sb;      // sqrt(beta/2*gm)
   double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
-  int ac_all;        // acf made over every cell since the last stage: the cfl counts the ghosts
-                     // of exchanged faces too (else the neighbouring block counts them)
   const double *dx, *dy;
   const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]

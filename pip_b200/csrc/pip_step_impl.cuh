@@ -101,23 +101,34 @@ __device__ __forceinline__ void ir_rates(const double (&u)[NVM], const KParams &
 
 constexpr double kPiRef = 3.1415926535897932;  // pi of Parameters.f90:2
 
+// Explicitly rounded operations: the alpha_c field is computed at several call sites (the
+// stage kernels' cells, the exchanged ghost cells, the whole-grid pass), and FMA
+// contraction would round each site differently in the contracted build.
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+
 // get_Te_MHD and get_Te_HD (Scheme_rot.f90:83-128) on one cell: the pressures with the
 // floor (`if(minval(pr).le.pr_lim) pr=max(pr,pr_lim)` is the per-cell max), the energies
 // um[4], uh[4] rewritten from them, and the temperatures Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro.
 template <int NVM>
 __device__ __forceinline__ void get_te(double (&um)[NVM], double (&uh)[5], const KParams &p,
                                        double &te_m, double &te_h) {
-  const double gm = p.gm;
-  double pr = (gm - 1.0) * (um[4] - 0.5 * ((um[1] * um[1] + um[2] * um[2] + um[3] * um[3]) / um[0] +
-                                           um[5] * um[5] + um[6] * um[6] + um[7] * um[7]));
+  const double gm = p.gm, g1 = rsub(gm, 1.0);
+  // (m.m)/ro + bx^2 + by^2 + bz^2, summed left to right
+  const double mm = radd(radd(rmul(um[1], um[1]), rmul(um[2], um[2])), rmul(um[3], um[3]));
+  const double em = radd(radd(radd(rdiv(mm, um[0]), rmul(um[5], um[5])), rmul(um[6], um[6])),
+                         rmul(um[7], um[7]));
+  double pr = rmul(g1, rsub(um[4], rmul(0.5, em)));
   pr = fmax(pr, p.pr_lim);
-  um[4] = pr / (gm - 1.0) + 0.5 * ((um[1] * um[1] + um[2] * um[2] + um[3] * um[3]) / um[0] +
-                                   um[5] * um[5] + um[6] * um[6] + um[7] * um[7]);
-  te_m = 0.5 * gm * (pr / um[0]);
-  double ph = (gm - 1.0) * (uh[4] - 0.5 * (uh[1] * uh[1] + uh[2] * uh[2] + uh[3] * uh[3]) / uh[0]);
+  um[4] = radd(rdiv(pr, g1), rmul(0.5, em));
+  te_m = rmul(rmul(0.5, gm), rdiv(pr, um[0]));
+  const double mh = radd(radd(rmul(uh[1], uh[1]), rmul(uh[2], uh[2])), rmul(uh[3], uh[3]));
+  double ph = rmul(g1, rsub(uh[4], rdiv(rmul(0.5, mh), uh[0])));   // 0.5*(m.m)/ro
   ph = fmax(ph, p.pr_lim);
-  uh[4] = ph / (gm - 1.0) + 0.5 * ((uh[1] * uh[1] + uh[2] * uh[2] + uh[3] * uh[3]) / uh[0]);
-  te_h = gm * (ph / uh[0]);
+  uh[4] = radd(rdiv(ph, g1), rmul(0.5, rdiv(mh, uh[0])));           // 0.5*((m.m)/ro)
+  te_h = rmul(gm, rdiv(ph, uh[0]));
 }
 
 // set_collisional for col_type 1..6 (PIP_rot.f90:44-97) on one cell: rewrites the energies
@@ -128,20 +139,23 @@ __device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double
                                                        const KParams &p) {
   double te_m, te_h;
   get_te<NVM>(um, uh, p, te_m, te_h);
-  const double gm = p.gm, T = te_h + te_m;
-  double a = p.ac * sqrt(T / 2.0);
+  const double gm = p.gm, T = radd(te_h, te_m);
+  double a = rmul(p.ac, __dsqrt_rn(rdiv(T, 2.0)));
   const int type = p.col_type;
-  if (type == 1) return a / p.ac_sb;
+  if (type == 1) return rdiv(a, p.ac_sb);
   if (type == 2) return a;
-  const double vdx = uh[1] / uh[0] - um[1] / um[0];
-  const double vdy = uh[2] / uh[0] - um[2] / um[0];
-  const double vdz = uh[3] / uh[0] - um[3] / um[0];
-  const double v2 = vdx * vdx + vdy * vdy + vdz * vdz;
-  a = a * sqrt(1.0 + 9.0 * kPiRef / 64.0 * gm / 2.0 * v2 / T);
-  if (type == 3) return a / p.ac_sb;
+  const double vdx = rsub(rdiv(uh[1], uh[0]), rdiv(um[1], um[0]));
+  const double vdy = rsub(rdiv(uh[2], uh[0]), rdiv(um[2], um[0]));
+  const double vdz = rsub(rdiv(uh[3], uh[0]), rdiv(um[3], um[0]));
+  const double v2 = radd(radd(rmul(vdx, vdx), rmul(vdy, vdy)), rmul(vdz, vdz));
+  // 9*pi/64*gm/2*v2/T, left to right
+  const double k = rdiv(rmul(rdiv(rmul(rdiv(rmul(9.0, kPiRef), 64.0), gm), 2.0), v2), T);
+  a = rmul(a, __dsqrt_rn(radd(1.0, k)));
+  if (type == 3) return rdiv(a, p.ac_sb);
   if (type == 4) return a;
-  if (type == 5) return a / p.ac_sb * pow(p.ac_b2g / T / 2.0 + gm * kPiRef / 16.0 * v2, 0.125);
-  return a / pow(T / 2.0 + gm * kPiRef / 16.0 * v2, 0.125);
+  const double w = rmul(rdiv(rmul(gm, kPiRef), 16.0), v2);          // gm*pi/16*v2
+  if (type == 5) return rmul(rdiv(a, p.ac_sb), pow(radd(rdiv(rdiv(p.ac_b2g, T), 2.0), w), 0.125));
+  return rdiv(a, pow(radd(rdiv(T, 2.0), w), 0.125));
 }
 
 // Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
@@ -302,6 +316,36 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
     atomicMin(&ctrl->red_dt[slot], dbits(dtc));
     atomicMax(&ctrl->red_rho[slot], dbits(rho));
     atomicMax(&ctrl->red_gr[slot], dbits(gr));
+  }
+}
+
+// alpha_c of the ghost cells that the halo exchange filled (faces whose source is -1),
+// from the stage-2 input state there, as set_collisional computes it on every cell after
+// mpi_bnd.  The tiles along such a face take its ghost layers over their columns (rows in
+// 1D), the edge tiles also the corner cells; the ranges of the tiles are disjoint.
+template <int NDIM, int NVM, int TX, int TY, int NT>
+__device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ Us, int i0, int j0,
+                                   int tid) {
+  const bool first_x = blockIdx.x == 0, last_x = blockIdx.x == gridDim.x - 1;
+  const bool first_y = blockIdx.y == 0, last_y = blockIdx.y == gridDim.y - 1;
+  const bool lo_x = first_x && p.gx[0][0] < 0, hi_x = last_x && p.gx[1][0] < 0;
+  const bool lo_y = NDIM == 2 && first_y && p.gy[0][0] < 0;
+  const bool hi_y = NDIM == 2 && last_y && p.gy[1][0] < 0;
+  if (!(lo_x || hi_x || lo_y || hi_y)) return;
+  const int ca = first_x ? 0 : i0;
+  const int cb = last_x ? p.ix : i0 + TX;
+  const int ra = NDIM == 2 ? (first_y ? 0 : j0) : 0;
+  const int rb = NDIM == 2 ? (last_y ? p.jx : j0 + TY) : 1;
+  const int w = cb - ca, n = w * (rb - ra);
+  for (int t = tid; t < n; t += NT) {
+    const int i = ca + t % w, j = ra + t / w;
+    const bool ghost = (lo_x && i < p.m0) || (hi_x && i >= p.ix - p.m0) ||
+                       (lo_y && j < p.m1) || (hi_y && j >= p.jx - p.m1);
+    if (!ghost) continue;
+    const long long q = (long long)j * p.ix + i;
+    double um[NVM], uh[5];
+    load_cell<NVM>(Us, q, p.nc, um, uh);
+    p.acf[q] = set_collisional_cell<NVM>(um, uh, p);
   }
 }
 
@@ -600,6 +644,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
     }
   }
+  if (STAGE == 2 && VC) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
   if (STAGE == 2 && s_epi == 2) {
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   }
@@ -623,12 +668,6 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       }
     }
   }
-}
-
-// A ghost cell of a face whose layers come from the halo exchange (source -1).
-__device__ __forceinline__ bool exchanged_ghost(const KParams &p, int i, int j) {
-  if ((i < p.m0 && p.gx[0][0] < 0) || (i >= p.ix - p.m0 && p.gx[1][0] < 0)) return true;
-  return p.ndim == 2 && ((j < p.m1 && p.gy[0][0] < 0) || (j >= p.jx - p.m1 && p.gy[1][0] < 0));
 }
 
 // cfl (Scheme_rot.f90:183-213) as a standalone pass over every cell: cq2pv rewrite of
@@ -659,10 +698,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
     }
     if (!p.col_type) {
       rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
-    } else if (p.ac_all || !exchanged_ghost(p, i, j)) {
-      // after a stage, the ghosts of faces filled by the halo exchange are the neighbour's
-      // interior cells, counted there; every other ghost equals its source cell's rho and
-      // alpha_c
+    } else {
       const double a = p.acf[q];
       rhoc = fmax(rhoc, fmax(um[0] * a, uh[0] * a));
     }

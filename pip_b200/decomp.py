@@ -286,6 +286,9 @@ class DeviceBlock:
     def download(self) -> Tuple[np.ndarray, np.ndarray]:
         return self.ctx.download()
 
+    def alpha_c(self) -> np.ndarray:
+        return self.ctx.alpha_c()
+
     def close(self) -> None:
         self.ctx.close()
 
@@ -423,7 +426,8 @@ class DecomposedRun:
         self.comm.barrier()
         for e in self.engines:
             U_h, U_m = e.download()
-            output.write_output_block(outdir, nout, s_global, e.block, U_h, U_m)
+            ac = e.alpha_c() if s_global.flag_col >= 2 else None
+            output.write_output_block(outdir, nout, s_global, e.block, U_h, U_m, ac)
         self.comm.barrier()
 
     def close(self) -> None:

@@ -8,7 +8,10 @@ ionisation/recombination rates ``ion rec`` when flag_ir >= 1, then ``ro_n mx_n m
 en_n`` (names from ``set_initial_out`` :362-374).  Every 3D dataset is FP64 of the global
 dimensions with ghost cells, Fortran order (x fastest); each rank writes a hyperslab
 (``create_write_dataspaces`` :127-164): its interior, plus its ghost layers on the sides
-where it touches the global boundary.  ``config.txt`` (``mk_config`` :377-402) records the
+where it touches the global boundary.  With alpha_c per cell (flag_col 2..7) the file opens
+its variables with ``ac``, the field of the last set_collisional, as ``def_varfiles``
+(:231-259) writes it before the state at every output; ``restart`` reads it back
+(``reread_variables`` :570-572).  ``config.txt`` (``mk_config`` :377-402) records the
 setting lines, the equation flags, variable counts, grid, margins, gamma and flag_bnd, and
 ``restart`` (:405-459) reads them back with the state of output ``flag_restart``.
 
@@ -43,8 +46,9 @@ def file_stem(outdir: str, nout: int) -> str:
 
 
 def variables(s: Settings) -> Tuple[str, ...]:
-    """The 3D datasets of save_varfiles, in order."""
-    names = list(VAR_M[: s.nvar_m])
+    """The 3D datasets of def_varfiles and save_varfiles, in order."""
+    names = ["ac"] if s.flag_col >= 2 else []
+    names += list(VAR_M[: s.nvar_m])
     if s.flag_ir != PIP_IR_NONE:
         names += ["ion", "rec"]
     return tuple(names) + VAR_H
@@ -100,8 +104,13 @@ def _create(stem: str, s: Settings, global_shape, time: float, grid) -> Dict[str
     return where
 
 
-def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray):
-    planes = {VAR_M[n]: U_m[n] for n in range(s.nvar_m)}
+def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np.ndarray]):
+    planes = {}
+    if s.flag_col >= 2:
+        if ac is None:
+            raise ValueError("flag_col %d writes the alpha_c field: pass ac" % s.flag_col)
+        planes["ac"] = np.asarray(ac).reshape(U_h.shape[1:])
+    planes.update({VAR_M[n]: U_m[n] for n in range(s.nvar_m)})
     if s.flag_ir != PIP_IR_NONE:
         planes["ion"], planes["rec"] = ir_rates(s, U_m)
     for n, name in enumerate(VAR_H):
@@ -110,14 +119,15 @@ def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray):
 
 
 def write_output(outdir: str, nout: int, s: Settings, time: float, U_h: np.ndarray,
-                 U_m: np.ndarray) -> str:
-    """output() of a whole state (global arrays with ghosts, layout (planes, jx, ix))."""
+                 U_m: np.ndarray, ac: Optional[np.ndarray] = None) -> str:
+    """output() of a whole state (global arrays with ghosts, layout (planes, jx, ix)); ac is
+    the alpha_c field (pip_get_alpha_c), needed with flag_col 2..7."""
     os.makedirs(outdir, exist_ok=True)
     stem = file_stem(outdir, nout)
     x, y, z, dx, dy, dz = s.coordinates()
     where = _create(stem, s, s.shape, time, (x, y, z, dx, dy, dz))
     mm = np.memmap(stem + ".bin", dtype=np.uint8, mode="r+")
-    for name, plane in _state_planes(s, U_h, U_m).items():
+    for name, plane in _state_planes(s, U_h, U_m, ac).items():
         off, dims = where[name]
         raw = np.ascontiguousarray(plane, dtype="<f8").view(np.uint8).reshape(-1)
         mm[off: off + raw.size] = raw
@@ -136,7 +146,7 @@ def create_output(outdir: str, nout: int, s: Settings, time: float) -> str:
 
 
 def write_output_block(outdir: str, nout: int, s: Settings, block, U_h: np.ndarray,
-                       U_m: np.ndarray) -> None:
+                       U_m: np.ndarray, ac: Optional[np.ndarray] = None) -> None:
     """One rank's hyperslab (create_write_dataspaces, IO_rot.f90:127-164) of a decomposed
     output into the file create_output made: the block's interior rows (1D: columns),
     plus its ghost layers on a side where it touches the global boundary.  s is the global
@@ -151,7 +161,7 @@ def write_output_block(outdir: str, nout: int, s: Settings, block, U_h: np.ndarr
     hi_local = m + block.n + (m if block.rank == block.world - 1 else 0)
     g0 = block.lo + lo_local                 # first global index written
     mm = np.memmap(stem + ".bin", dtype=np.uint8, mode="r+")
-    planes = _state_planes(block.settings, U_h, U_m)
+    planes = _state_planes(block.settings, U_h, U_m, ac)
     for name, off, dims in entries:
         if name not in planes:
             continue
@@ -249,6 +259,16 @@ def restart(outdir: str, nout: int, s: Settings) -> Tuple[float, np.ndarray, np.
     return d["time"], np.ascontiguousarray(U_h), np.ascontiguousarray(U_m)
 
 
+def restart_alpha_c(outdir: str, nout: int, s: Settings) -> Optional[np.ndarray]:
+    """The alpha_c field of output nout (jx, ix) that restart reads with flag_col 2..7
+    (IO_rot.f90:570-572), for pip_set_alpha_c; None for a constant alpha_c."""
+    if s.flag_col < 2:
+        return None
+    d = read_output(file_stem(outdir, nout))
+    ix, jx, _ = s.shape
+    return np.ascontiguousarray(d["ac"][0].reshape(jx, ix))
+
+
 def run_with_output(ctx, s: Settings, outdir: str, dtout: float, tend: float,
                     nout0: int = 0, setting_text: str = "") -> Tuple[int, int, float]:
     """main.f90's loop with output (IO_rot.f90:39-105; get_next_output type 0: output n at
@@ -258,15 +278,16 @@ def run_with_output(ctx, s: Settings, outdir: str, dtout: float, tend: float,
     if nout0 == 0:
         mk_config(outdir, s, setting_text)
     nout = nout0
+    field = (lambda: ctx.alpha_c()) if s.flag_col >= 2 else (lambda: None)
     U_h, U_m = ctx.download()
-    write_output(outdir, nout, s, ctx.time, U_h, U_m)
+    write_output(outdir, nout, s, ctx.time, U_h, U_m, field())
     st = 0
     while ctx.time < tend:
         nxt = min((nout + 1) * dtout, tend)
         st, t, n = ctx.run(t_end=nxt)
         U_h, U_m = ctx.download()
         nout += 1
-        write_output(outdir, nout, s, t, U_h, U_m)
+        write_output(outdir, nout, s, t, U_h, U_m, field())
         if st != 0:
             break
     return st, nout, ctx.time

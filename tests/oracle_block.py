@@ -77,5 +77,8 @@ class OracleBlock:
     def download(self):
         return self.o.state()
 
+    def alpha_c(self):
+        return self.o.alpha_c()
+
     def close(self):
         self.o.close()

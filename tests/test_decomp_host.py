@@ -69,7 +69,8 @@ def local_run(case, world, nsteps):
 
 
 @pytest.mark.parametrize("case,world", [("ot", 2), ("ot", 4), ("ot_generic", 2), ("kh", 2),
-                                        ("kh", 4), ("bw", 2), ("bw", 4)])
+                                        ("kh", 4), ("bw", 2), ("bw", 4), ("ot_col", 4),
+                                        ("kh_col", 2)])
 def test_blocks_in_one_process_match_single_domain(case, world):
     nsteps = 6
     s, uh, um, hist = single_domain(case, nsteps)
@@ -111,18 +112,20 @@ def test_two_gloo_ranks_match_single_domain(case):
     assert np.array_equal(gh, uh) and np.array_equal(gm, um)
 
 
-def test_decomposed_output_is_the_single_domain_output(tmp_path):
+@pytest.mark.parametrize("case", ["kh", "ot_col"])
+def test_decomposed_output_is_the_single_domain_output(tmp_path, case):
     """Each block writes its hyperslab of output 1 after 4 steps; the file is the one the
-    single-domain run writes."""
-    s, Uh, Um = make_case("kh")
+    single-domain run writes (with alpha_c per cell, its field too)."""
+    s, Uh, Um = make_case(case)
     o = O.Oracle(s, Uh, Um)
     o.run(nsteps=4)
     oh, om = o.state()
-    ref = output.write_output(str(tmp_path / "one"), 1, s, o.time, oh, om)
+    ac = o.alpha_c() if s.flag_col >= 2 else None
+    ref = output.write_output(str(tmp_path / "one"), 1, s, o.time, oh, om, ac)
     o.close()
     engines = [OracleBlock(decomp.block_of(s, 4, r), decomp.scatter(s, Uh, 4, r),
                            decomp.scatter(s, Um, 4, r)) for r in range(4)]
-    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=False)
+    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
     assert run.run(4) == 0
     run.write_output(str(tmp_path / "blocks"), 1, s)
     run.close()

@@ -181,15 +181,23 @@ def test_decomposed_runs(gpu_lib, case, world):
         c.upload(Uh, Um)
         st1, t1, n1 = c.run(nsteps=nsteps)
         rh, rm = c.download()
+        ra = c.alpha_c()
     assert st1 == 0 and n1 == nsteps
     engines = _blocks(s, Uh, Um, world)
     run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
     st = run.run_device(nsteps, check_every=4)
     states = [e.download() for e in engines]
+    fields = [e.alpha_c()[None] for e in engines]
     run.close()
     assert st == 0 and run.steps == nsteps and run.time == t1
     assert np.array_equal(decomp.gather(s, [a for a, _ in states]), rh)
     assert np.array_equal(decomp.gather(s, [b for _, b in states]), rm)
+    # the blocks' fields, ghost layers at the global ends included (on a periodic axis those
+    # come from the halo exchange), are the single domain's
+    ga = decomp.gather(s, fields)[0]
+    bad = np.argwhere(ga != ra)
+    assert bad.size == 0, "alpha_c differs at %d cells, e.g. (j, i) %s: %s vs %s" % (
+        len(bad), bad[:8].tolist(), ga[tuple(bad[:8].T)], ra[tuple(bad[:8].T)])
     engines = _blocks(s, Uh, Um, world)
     run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
     st = run.run(nsteps)

@@ -1,7 +1,8 @@
 """Output and restart on the device (pip_b200.output.run_with_output, IO_rot.f90's output
 and restart): a run that writes every dtout, restarted from one of its outputs in a new
 context, reaches the same final state bitwise -- FP64 and FP32-mixed (the mixed state's
-FP32 pair is rebuilt exactly from the FP64 file)."""
+FP32 pair is rebuilt exactly from the FP64 file), and FP64 with alpha_c per cell (the
+field is written with every output and read back)."""
 import numpy as np
 import pytest
 
@@ -11,9 +12,9 @@ from pip_b200.params import PIP_FP64, PIP_MIXED
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision", [PIP_FP64, PIP_MIXED])
-def test_restart_continues_the_run(gpu_lib, tmp_path, precision):
-    s, Uh, Um = ics.kelvin_helmholtz(64, 32, precision=precision)
+@pytest.mark.parametrize("precision,flag_col", [(PIP_FP64, 1), (PIP_MIXED, 1), (PIP_FP64, 5)])
+def test_restart_continues_the_run(gpu_lib, tmp_path, precision, flag_col):
+    s, Uh, Um = ics.kelvin_helmholtz(64, 32, precision=precision, flag_col=flag_col)
     dtout, tend = 0.01, 0.04
     out = str(tmp_path / "run")
     with capi.Context(s) as c:
@@ -31,6 +32,8 @@ def test_restart_continues_the_run(gpu_lib, tmp_path, precision):
     out2 = str(tmp_path / "restarted")
     with capi.Context(s) as c:
         c.upload(h2, m2)
+        if flag_col >= 2:                            # reread_variables' "ac"
+            c.set_alpha_c(output.restart_alpha_c(out, 2, s))
         c.time = t2
         st, last, t = output.run_with_output(c, s, out2, dtout, tend, nout0=2)
     again = output.read_output(output.file_stem(out2, 4))

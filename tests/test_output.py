@@ -54,6 +54,28 @@ def test_rank_hyperslabs_make_the_global_file(tmp_path, case, world):
     assert open(ref[:-4] + ".idx").read() == open(output.file_stem(out, 1) + ".idx").read()
 
 
+def test_alpha_c_dataset(tmp_path):
+    """flag_col 2..7: def_varfiles' "ac" opens the variables; restart reads it back; the
+    ranks' hyperslabs of it make the single writer's file."""
+    s, Uh, Um = ics.orszag_tang(16, flag_col=5)
+    ac = np.random.default_rng(2).random(Uh.shape[1:]) + 1.0
+    with pytest.raises(ValueError, match="ac"):
+        output.write_output(str(tmp_path / "x"), 0, s, 0.0, Uh, Um)
+    ref = output.write_output(str(tmp_path / "one"), 2, s, 0.5, Uh, Um, ac)
+    names = [ln.split()[0] for ln in open(ref[:-4] + ".idx")]
+    assert names[7:9] == ["ac", "ro_p"]
+    assert np.array_equal(output.read_output(ref)["ac"][0], ac)
+    assert np.array_equal(output.restart_alpha_c(str(tmp_path / "one"), 2, s), ac)
+    assert output.restart_alpha_c(str(tmp_path / "one"), 2, s.overrides(flag_col=1)) is None
+    out = str(tmp_path / "ranks")
+    output.create_output(out, 2, s, 0.5)
+    for r in range(4):
+        b = decomp.block_of(s, 4, r)
+        output.write_output_block(out, 2, s, b, decomp.scatter(s, Uh, 4, r),
+                                  decomp.scatter(s, Um, 4, r), decomp.scatter(s, ac[None], 4, r)[0])
+    assert open(ref, "rb").read() == open(output.file_stem(out, 2) + ".bin", "rb").read()
+
+
 def test_config_and_restart(tmp_path):
     s, Uh, Um = ics.orszag_tang(16)
     text = "2.0d0          :gm_d;\n1.0d-8         :ro_lim;\n# no key here\n"
