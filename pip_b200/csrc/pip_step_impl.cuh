@@ -112,23 +112,43 @@ __device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a,
 // get_Te_MHD and get_Te_HD (Scheme_rot.f90:83-128) on one cell: the pressures with the
 // floor (`if(minval(pr).le.pr_lim) pr=max(pr,pr_lim)` is the per-cell max), the energies
 // um[4], uh[4] rewritten from them, and the temperatures Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro.
+// The FMA build multiplies by 1/ro and 1/(gm-1) (returned in rm, rh for the drift); the
+// FMA-free build divides as the Fortran does.  Divisions by 2, 16 and 64 below are exact
+// multiplications by their reciprocals.
 template <int NVM>
 __device__ __forceinline__ void get_te(double (&um)[NVM], double (&uh)[5], const KParams &p,
-                                       double &te_m, double &te_h) {
+                                       double &te_m, double &te_h, double &rm, double &rh) {
   const double gm = p.gm, g1 = rsub(gm, 1.0);
   // (m.m)/ro + bx^2 + by^2 + bz^2, summed left to right
   const double mm = radd(radd(rmul(um[1], um[1]), rmul(um[2], um[2])), rmul(um[3], um[3]));
-  const double em = radd(radd(radd(rdiv(mm, um[0]), rmul(um[5], um[5])), rmul(um[6], um[6])),
+  const double mh = radd(radd(rmul(uh[1], uh[1]), rmul(uh[2], uh[2])), rmul(uh[3], uh[3]));
+#if PIP_RCP
+  rm = rdiv(1.0, um[0]);
+  rh = rdiv(1.0, uh[0]);
+  const double km = rmul(mm, rm), kh = rmul(mh, rh);
+#else
+  rm = rh = 0.0;
+  const double km = rdiv(mm, um[0]), kh = rdiv(mh, uh[0]);
+#endif
+  const double em = radd(radd(radd(km, rmul(um[5], um[5])), rmul(um[6], um[6])),
                          rmul(um[7], um[7]));
   double pr = rmul(g1, rsub(um[4], rmul(0.5, em)));
   pr = fmax(pr, p.pr_lim);
+#if PIP_RCP
+  um[4] = radd(rmul(pr, p.igm1), rmul(0.5, em));
+  te_m = rmul(rmul(0.5, gm), rmul(pr, rm));
+  double ph = rmul(g1, rsub(uh[4], rmul(rmul(0.5, mh), rh)));
+  ph = fmax(ph, p.pr_lim);
+  uh[4] = radd(rmul(ph, p.igm1), rmul(0.5, kh));
+  te_h = rmul(gm, rmul(ph, rh));
+#else
   um[4] = radd(rdiv(pr, g1), rmul(0.5, em));
   te_m = rmul(rmul(0.5, gm), rdiv(pr, um[0]));
-  const double mh = radd(radd(rmul(uh[1], uh[1]), rmul(uh[2], uh[2])), rmul(uh[3], uh[3]));
   double ph = rmul(g1, rsub(uh[4], rdiv(rmul(0.5, mh), uh[0])));   // 0.5*(m.m)/ro
   ph = fmax(ph, p.pr_lim);
-  uh[4] = radd(rdiv(ph, g1), rmul(0.5, rdiv(mh, uh[0])));           // 0.5*((m.m)/ro)
+  uh[4] = radd(rdiv(ph, g1), rmul(0.5, kh));                        // 0.5*((m.m)/ro)
   te_h = rmul(gm, rdiv(ph, uh[0]));
+#endif
 }
 
 // set_collisional for col_type 1..6 (PIP_rot.f90:44-97) on one cell: rewrites the energies
@@ -137,25 +157,32 @@ __device__ __forceinline__ void get_te(double (&um)[NVM], double (&uh)[5], const
 template <int NVM>
 __device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double (&uh)[5],
                                                        const KParams &p) {
-  double te_m, te_h;
-  get_te<NVM>(um, uh, p, te_m, te_h);
+  double te_m, te_h, rm, rh;
+  get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
   const double gm = p.gm, T = radd(te_h, te_m);
-  double a = rmul(p.ac, __dsqrt_rn(rdiv(T, 2.0)));
+  double a = rmul(p.ac, __dsqrt_rn(rmul(T, 0.5)));
   const int type = p.col_type;
   if (type == 1) return rdiv(a, p.ac_sb);
   if (type == 2) return a;
+#if PIP_RCP
+  const double vdx = rsub(rmul(uh[1], rh), rmul(um[1], rm));
+  const double vdy = rsub(rmul(uh[2], rh), rmul(um[2], rm));
+  const double vdz = rsub(rmul(uh[3], rh), rmul(um[3], rm));
+#else
   const double vdx = rsub(rdiv(uh[1], uh[0]), rdiv(um[1], um[0]));
   const double vdy = rsub(rdiv(uh[2], uh[0]), rdiv(um[2], um[0]));
   const double vdz = rsub(rdiv(uh[3], uh[0]), rdiv(um[3], um[0]));
+#endif
   const double v2 = radd(radd(rmul(vdx, vdx), rmul(vdy, vdy)), rmul(vdz, vdz));
   // 9*pi/64*gm/2*v2/T, left to right
-  const double k = rdiv(rmul(rdiv(rmul(rdiv(rmul(9.0, kPiRef), 64.0), gm), 2.0), v2), T);
+  const double k = rdiv(rmul(rmul(rmul(rmul(rmul(9.0, kPiRef), 0.015625), gm), 0.5), v2), T);
   a = rmul(a, __dsqrt_rn(radd(1.0, k)));
   if (type == 3) return rdiv(a, p.ac_sb);
   if (type == 4) return a;
-  const double w = rmul(rdiv(rmul(gm, kPiRef), 16.0), v2);          // gm*pi/16*v2
-  if (type == 5) return rmul(rdiv(a, p.ac_sb), pow(radd(rdiv(rdiv(p.ac_b2g, T), 2.0), w), 0.125));
-  return rdiv(a, pow(radd(rdiv(T, 2.0), w), 0.125));
+  const double w = rmul(rmul(rmul(gm, kPiRef), 0.0625), v2);       // gm*pi/16*v2
+  if (type == 5)
+    return rmul(rdiv(a, p.ac_sb), pow(radd(rmul(rdiv(p.ac_b2g, T), 0.5), w), 0.125));
+  return rdiv(a, pow(radd(rmul(T, 0.5), w), 0.125));
 }
 
 // Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
@@ -436,8 +463,8 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
     if (VC) {
       // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux
-      double te_m, te_h;
-      get_te<NVM>(um, uh, p, te_m, te_h);
+      double te_m, te_h, rm, rh;
+      get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
     }
     u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
     u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
