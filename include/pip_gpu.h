@@ -61,7 +61,8 @@ enum pip_ir_law {
  *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col 1..7 (2..7 with
  *   precision PIP_FP64 only),
  *   flag_pip_imp 0/1, flag_ir 0 or PIP_IR_POWERLAW with flag_ir_type 1 or 2,
- *   flag_bnd in {1,2,3,4,5,6,7,10,11}, no resistivity/viscosity/gravity/ambipolar.
+ *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0/1 (a fixed eta field; FP64 form, not
+ *   with flag_heat), no viscosity/gravity/ambipolar diffusion.
  */
 typedef struct pip_params {
   int32_t abi_version;     /* must equal PIP_ABI_VERSION */
@@ -89,7 +90,11 @@ typedef struct pip_params {
   int32_t precision;       /* pip_precision */
   int32_t fp_exact;        /* 1: FP64 kernels built without FMA contraction (bitwise
                               comparable with an FMA-free CPU build); 0: contracted */
-  int32_t reserved_i[6];
+  int32_t flag_resi;       /* 0, or 1: resistive flux with a fixed eta field (resistive_flux,
+                              Solver_rot.f90:505-638, flag_sch=0 branch; cfl_resi,
+                              Scheme_rot.f90:291-302); eta = eta_0 everywhere unless
+                              pip_set_resistivity gives the field (FP64 form only) */
+  int32_t reserved_i[5];
   double gm;               /* ratio of specific heats: gm_d/gm_n */
   double safety;           /* CFL number */
   double ro_lim, pr_lim;   /* density and pressure floors */
@@ -103,7 +108,8 @@ typedef struct pip_params {
   double kapper;           /* Spitzer coefficient: kappa_par = kapper*T^2.5 */
   double hc_error;         /* BiCGstab relative residual target */
   double beta;             /* plasma beta of set_collisional col_type 1, 3, 5 (> 0 there) */
-  double reserved_d[6];
+  double eta_0;            /* uniform resistivity (set_resistivity resi_type 0) */
+  double reserved_d[5];
   const double *dx;        /* ix cell widths (dsc(:,1)) */
   const double *dy;        /* jx cell widths (dsc(:,2)); 1D: one entry, the reference sets 100 */
   const double *dz;        /* kx cell widths (dsc(:,3)); one entry, the reference sets 100 */
@@ -212,6 +218,11 @@ int pip_get_alpha_c(pip_ctx *ctx, double *ac);
  * field the first cfl after a pip_upload uses instead of making one from the state.
  * No-op for flag_col 1. */
 int pip_set_alpha_c(pip_ctx *ctx, const double *ac);
+
+/* set_resistivity (Res_rot.f90:16-60) for flag_resi 1: the eta field (ix*jx doubles,
+ * Fortran order, ghosts included) that resistive_flux and cfl_resi use from the next call
+ * on; eta_0 everywhere until called.  PIP_ERR_PARAM without flag_resi 1. */
+int pip_set_resistivity(pip_ctx *ctx, const double *eta);
 
 /* PIPbnd(U_h,U_m,0) (Boundary_rot.f90:34-52) on the device state; with one rank the
  * MPI halo exchange (MPI_rot.f90:128-339) reduces to this ghost fill. */

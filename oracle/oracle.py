@@ -66,6 +66,7 @@ def lib():
         L.orc_conduction.restype = ctypes.c_int
         L.orc_has_nan.restype = ctypes.c_int
         L.orc_coefficients.argtypes = [vp]
+        L.orc_set_resistivity.argtypes = [vp, dp]
         L.orc_alpha_c.argtypes = [vp, dp]
         L.orc_alpha_c.restype = ctypes.c_int
         _lib = L
@@ -176,6 +177,11 @@ class Oracle:
     def coefficients(self) -> None:
         """set_coefficients' collision part: flag_col 2..7 rewrites the energies, sets alpha_c."""
         lib().orc_coefficients(self.h)
+
+    def set_resistivity(self, eta: np.ndarray) -> None:
+        """The eta field (jx, ix) of flag_resi 1 (eta_0 everywhere until set)."""
+        e = np.ascontiguousarray(eta, dtype=np.float64).reshape(self.shape_h[1:])
+        lib().orc_set_resistivity(self.h, _ptr(e))
 
     def alpha_c(self) -> np.ndarray:
         """alpha_c of every cell, shaped like one plane of the state."""

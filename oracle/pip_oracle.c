@@ -40,6 +40,8 @@ struct orc_ctx {
   int col_type;                      /* initialize_collisional: flag_col 2..7 -> 1..6 */
   double *ac;                        /* alpha_c per cell (globalvar ac) for col_type >= 1 */
   int ac_valid;                      /* set by the first set_collisional */
+  int resi;                          /* flag_resi 1: resistive flux with the eta field */
+  double *eta;                       /* globalvar eta (set_resistivity), nc values */
 };
 
 static void ensure_ac(orc_ctx *c);
@@ -603,7 +605,76 @@ static void set_fluxes(const orc_ctx *c, double *F, const double *VL, const doub
       }
 }
 
-/* hlld_fluxes_ideal / hllc_fluxes_ideal for one direction (HLL_rot.f90:94-121). */
+/* get_rotation (Util_rot.f90:148-236), s_order 2 branch, of B = U_m(:,:,:,6:8): the
+ * central-difference curl on cells 2..ix-1 (2..jx-1), zero elsewhere. */
+static void get_rotation(const orc_ctx *c, double *R) {
+  size_t nc = c->nc;
+  const double *bx = c->U_m + 5 * nc, *by = c->U_m + 6 * nc, *bz = c->U_m + 7 * nc;
+  int ix = c->ix, jx = c->jx;
+  memset(R, 0, sizeof(double) * 3 * nc);
+  double *R1 = R, *R2 = R + nc, *R3 = R + 2 * nc;
+  if (c->p.ndim == 1) {
+    for (int j = 0; j < jx; ++j)
+      for (int i = 1; i < ix - 1; ++i) {
+        size_t q = AT(c, i, j, 0);
+        R2[q] = -(bz[q + 1] - bz[q - 1]) / (2.0 * c->dx[i]);
+        R3[q] = (by[q + 1] - by[q - 1]) / (2.0 * c->dx[i]);
+      }
+    return;
+  }
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j < jx - 1; ++j)
+    for (int i = 1; i < ix - 1; ++i) {
+      size_t q = AT(c, i, j, 0), s = (size_t)ix;
+      R1[q] = (bz[q + s] - bz[q - s]) / (2.0 * c->dy[j]);
+      R2[q] = -(bz[q + 1] - bz[q - 1]) / (2.0 * c->dx[i]);
+      R3[q] = ((by[q + 1] - by[q - 1]) / (2.0 * c->dx[i]) - (bx[q + s] - bx[q - s]) / (2.0 * c->dy[j]));
+    }
+}
+
+/* resistive_flux (Solver_rot.f90:505-638), flag_sch=0 branch, for direction dir: E =
+ * eta*curl B at the cells, averaged onto the faces 1..ix-1 (1..jx-1) and added to the
+ * energy and induction fluxes. */
+static void resistive_flux(orc_ctx *c, int dir, double *F) {
+  size_t nc = c->nc;
+  int ix = c->ix, jx = c->jx;
+  double *w = malloc(sizeof(double) * 6 * nc);
+  double *cur = w, *ex = w + 3 * nc, *ey = w + 4 * nc, *ez = w + 5 * nc;
+  get_rotation(c, cur);
+  for (size_t q = 0; q < nc; ++q) {
+    ex[q] = cur[q] * c->eta[q];
+    ey[q] = cur[q + nc] * c->eta[q];
+    ez[q] = cur[q + 2 * nc] * c->eta[q];
+  }
+  const double *bx = c->U_m + 5 * nc, *by = c->U_m + 6 * nc, *bz = c->U_m + 7 * nc;
+  if (dir == 1) {
+    for (int j = 0; j < jx; ++j)
+      for (int i = 0; i < ix - 1; ++i) {
+        size_t q = AT(c, i, j, 0), r = q + 1;
+        F[q + 4 * nc] = F[q + 4 * nc] +
+                        0.25 * ((ey[r] + ey[q]) * (bz[q] + bz[r]) - (ez[q] + ez[r]) * (by[q] + by[r]));
+        F[q + 6 * nc] = F[q + 6 * nc] - 0.5 * (ez[q] + ez[r]);
+        F[q + 7 * nc] = F[q + 7 * nc] + 0.5 * (ey[q] + ey[r]);
+      }
+  } else if (dir == 2) {
+    for (int j = 0; j < jx - 1; ++j)
+      for (int i = 0; i < ix; ++i) {
+        size_t q = AT(c, i, j, 0), r = q + (size_t)ix;
+        F[q + 4 * nc] = F[q + 4 * nc] +
+                        0.25 * ((ez[r] + ez[q]) * (bx[q] + bx[r]) - (ex[q] + ex[r]) * (bz[q] + bz[r]));
+        F[q + 5 * nc] = F[q + 5 * nc] + 0.5 * (ez[q] + ez[r]);
+        F[q + 7 * nc] = F[q + 7 * nc] - 0.5 * (ex[q] + ex[r]);
+      }
+  }
+  free(w);
+}
+
+void orc_set_resistivity(orc_ctx *c, const double *eta) {
+  if (c->eta) memcpy(c->eta, eta, sizeof(double) * c->nc);
+}
+
+/* hlld_fluxes_ideal / hllc_fluxes_ideal for one direction (HLL_rot.f90:94-121), then
+ * set_flux's resistive_flux (Solver_rot.f90:155-156). */
 static void flux_dir(orc_ctx *c, int dir, double *F_h, double *F_m) {
   size_t nc = c->nc;
   double *V = malloc(sizeof(double) * nc * 9);
@@ -612,6 +683,7 @@ static void flux_dir(orc_ctx *c, int dir, double *F_h, double *F_m) {
   u2v_mhd(c, c->U_m, V);
   get_side(c, V, VL, VR, dir, c->nm);
   set_fluxes(c, F_m, VL, VR, dir, 1);
+  if (c->resi) resistive_flux(c, dir, F_m);
   u2v_hd(c, c->U_h, V);
   get_side(c, V, VL, VR, dir, c->nh);
   set_fluxes(c, F_h, VL, VR, dir, 0);
@@ -873,6 +945,19 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
       gi = fmx(gi, c->gm_ion[q]);
     }
     dttemp = fmn(dttemp, fmn(safety, 0.1) / fmx(fmx(gr, gi), 1.0e-5));
+  }
+
+  /* cfl_resi (Scheme_rot.f90:291-302) */
+  if (c->resi) {
+    double etmin = 1.0e-8, dr = dttemp;
+#pragma omp parallel for collapse(2) reduction(min : dr) schedule(static)
+    for (int k = m2; k < c->kx - m2; ++k)
+      for (int j = m1; j < c->jx - m1; ++j)
+        for (int i = m0; i < c->ix - m0; ++i) {
+          double gmin = fmn(fmn(c->dx[i], c->dy[j]), c->dz[k]);
+          dr = fmn(dr, safety * (gmin * gmin) / fmx(c->eta[AT(c, i, j, k)], etmin));
+        }
+    dttemp = dr;
   }
 
   /* cmax for Dedner cleaning */
@@ -1237,6 +1322,7 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return NULL;
   if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0))) return NULL;
   if (p->flag_col < 1 || p->flag_col > 7) return NULL;
+  if (p->flag_resi != 0 && p->flag_resi != 1) return NULL;
   orc_ctx *c = calloc(1, sizeof(orc_ctx));
   c->p = *p;
   for (int f = 0; f < 6; ++f) c->neighbor[f] = -1;
@@ -1254,6 +1340,11 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   c->gm_ion = calloc(c->nc, sizeof(double));
   c->gm_rec = calloc(c->nc, sizeof(double));
   c->col_type = p->flag_col >= 2 ? p->flag_col - 1 : 0;   /* PIP_rot.f90:21-26 */
+  c->resi = p->flag_resi == 1;
+  if (c->resi) {
+    c->eta = malloc(sizeof(double) * c->nc);
+    for (size_t q = 0; q < c->nc; ++q) c->eta[q] = p->eta_0;   /* set_resistivity type 0 */
+  }
   if (c->col_type >= 1) c->ac = calloc(c->nc, sizeof(double));
   set_sym_mhd(c);
   set_sym_hd(c);
@@ -1267,6 +1358,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->U_h); free(c->U_m); free(c->gm_ion); free(c->gm_rec);
   free(c->U_h0); free(c->U_m0);
   free(c->ac);
+  free(c->eta);
   free(c);
 }
 

@@ -54,6 +54,9 @@ void orc_coefficients(orc_ctx *c);
 /* alpha_c of every cell (col for flag_col 1), made from the current state when no
  * set_collisional has run yet (Initial_rot.f90:140). */
 int orc_alpha_c(orc_ctx *c, double *ac);
+/* The eta field of set_resistivity (Res_rot.f90:16-60) for flag_resi 1 (nc values);
+ * eta_0 everywhere until called. */
+void orc_set_resistivity(orc_ctx *c, const double *eta);
 /* Boundary_rot.f90:34-52. */
 void orc_bnd(orc_ctx *c);
 /* main.f90:31-68 loop; returns 0, PIP_ERR_NAN or PIP_ERR_DT.  dt_hist (may be NULL)

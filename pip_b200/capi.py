@@ -35,7 +35,7 @@ EXPORTS = (
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
-    "pip_set_alpha_c",
+    "pip_set_alpha_c", "pip_set_resistivity",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -90,6 +90,7 @@ def lib(path: Optional[str] = None):
     L.pip_coefficients.argtypes = [vp]
     L.pip_get_alpha_c.argtypes = [vp, dp]
     L.pip_set_alpha_c.argtypes = [vp, dp]
+    L.pip_set_resistivity.argtypes = [vp, dp]
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
     L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
@@ -140,7 +141,8 @@ def lib(path: Optional[str] = None):
     for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",
                  "pip_get_time", "pip_flux", "pip_source", "pip_fill_ghosts", "pip_status",
                  "pip_conduction", "pip_last_cuda_error", "pip_run_timed", "pip_bench_stage_ms",
-                 "pip_coefficients", "pip_get_alpha_c", "pip_set_alpha_c"):
+                 "pip_coefficients", "pip_get_alpha_c", "pip_set_alpha_c",
+                 "pip_set_resistivity"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -281,6 +283,11 @@ class Context:
         a = np.empty(self.shape_h[1:])
         _check(lib().pip_get_alpha_c(self.h, _ptr(a)), "pip_get_alpha_c")
         return a
+
+    def set_resistivity(self, eta: np.ndarray) -> None:
+        """The eta field (jx, ix) of flag_resi 1 (set_resistivity; eta_0 everywhere until set)."""
+        e = np.ascontiguousarray(eta, dtype=np.float64).reshape(self.shape_h[1:])
+        _check(lib().pip_set_resistivity(self.h, _ptr(e)), "pip_set_resistivity")
 
     def set_alpha_c(self, ac: np.ndarray) -> None:
         """The field of a restart output (its "ac" dataset) for the next cfl."""

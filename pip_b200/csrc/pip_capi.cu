@@ -48,6 +48,7 @@ struct pip_ctx {
   bool dev_loop = false;              // pip_dev_begin has set up the device-driven loop
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
+  double *etaf = nullptr;             // eta per cell (flag_resi 1)
   bool ac_valid = false;              // acf holds the last set_collisional's field
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
@@ -144,6 +145,9 @@ int validate(const pip_params *p) {
   if (p->flag_col >= 2 && p->precision != PIP_FP64) return PIP_ERR_PARAM;
   if ((p->flag_col == 2 || p->flag_col == 4 || p->flag_col == 6) && !(p->beta > 0.0))
     return PIP_ERR_PARAM;
+  // flag_resi 1: a fixed eta field (FP64 form); with conduction the margin would be 4
+  if (p->flag_resi != 0 && p->flag_resi != 1) return PIP_ERR_PARAM;
+  if (p->flag_resi == 1 && (p->precision != PIP_FP64 || p->flag_heat != 0)) return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
@@ -204,6 +208,8 @@ void build_kparams(pip_ctx *c) {
   k.dz0 = c->dz[0];
   k.hc_kapper = p.kapper;
   k.col_type = p.flag_col >= 2 ? p.flag_col - 1 : 0;
+  k.resi = p.flag_resi;
+  k.resi_dt = INFINITY;
   k.ac_b2g = p.beta / 2.0 * p.gm;
   k.ac_sb = std::sqrt(k.ac_b2g);
   for (int s = 0; s < 2; ++s) {
@@ -242,9 +248,10 @@ void pip::record_cuda_error(int code) { g_last_cuda_error = code; }
 int pip::kparams_from_params(const pip_params *p, KParams *k) {
   const int st = validate(p);
   if (st != PIP_OK) return st;
-  // the per-cell alpha_c field lives in a context
-  if (p->flag_col != 1) return PIP_ERR_PARAM;
+  // the per-cell alpha_c and eta fields live in a context
+  if (p->flag_col != 1 || p->flag_resi != 0) return PIP_ERR_PARAM;
   *k = KParams{};
+  k->resi_dt = INFINITY;
   k->ndim = p->ndim;
   k->ix = p->ix;
   k->jx = p->jx;
@@ -317,11 +324,26 @@ double finalize_dt_host(const KParams &k, const DevCtrl &c, int slot) {
   return dt;
 }
 
-void reset_slot(DevCtrl &h, int slot) {
-  const double ten = 10.0;
-  std::memcpy(&h.red_dt[slot], &ten, sizeof(double));
+// A reduction slot before a cfl: the min-CFL candidate starts at cfl_mhd's 10.0 and
+// cfl_resi's bound (min is exact and commutative, so the order of the terms is free).
+void reset_slot(DevCtrl &h, int slot, const KParams &k) {
+  const double seed = std::fmin(10.0, k.resi_dt);
+  std::memcpy(&h.red_dt[slot], &seed, sizeof(double));
   h.red_rho[slot] = 0ull;
   h.red_gr[slot] = 0ull;
+}
+
+// cfl_resi (Scheme_rot.f90:291-302) for a fixed eta field: the minimum over the interior
+// cells of safety*gmin**2/max(eta,1e-8), gmin = min(dx(i),dy(j),dz(1)).
+double resi_bound(const pip_ctx *c, const double *eta) {
+  const KParams &k = c->kp;
+  double dt = INFINITY;
+  for (int j = k.m1; j < k.jx - k.m1; ++j)
+    for (int i = k.m0; i < k.ix - k.m0; ++i) {
+      const double gmin = std::fmin(std::fmin(c->dx[i], c->dy[j]), c->dz[0]);
+      dt = std::fmin(dt, c->p.safety * (gmin * gmin) / std::fmax(eta[(size_t)j * k.ix + i], 1.0e-8));
+    }
+  return dt;
 }
 
 int sync_ctrl_to_host(pip_ctx *c) {
@@ -497,6 +519,15 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   c->kp.dx = c->d_dx;
   c->kp.dy = c->d_dy;
   if ((e = cudaMalloc(&c->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
+  if (c->kp.resi) {
+    // set_resistivity type 0 until pip_set_resistivity gives another field
+    std::vector<double> eta((size_t)c->kp.nc, p->eta_0);
+    if ((e = cudaMalloc(&c->etaf, c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(c->etaf, eta.data(), c->plane_bytes(), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(e);
+    c->kp.etaf = c->etaf;
+    c->kp.resi_dt = resi_bound(c, eta.data());
+  }
   if (c->kp.col_type) {
     if ((e = cudaMalloc(&c->acf, c->plane_bytes())) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(c->acf, 0, c->plane_bytes())) != cudaSuccess) return fail(e);
@@ -540,6 +571,7 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->d_flag);
   cudaFree(c->d_dt);
   cudaFree(c->acf);
+  cudaFree(c->etaf);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -578,7 +610,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
   if (!c->uploaded) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (ensure_ac(c)) return PIP_ERR_CUDA;
-  reset_slot(*c->h_ctrl, 0);
+  reset_slot(*c->h_ctrl, 0, c->kp);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
   if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
@@ -639,8 +671,8 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   h.t_end = t_end > 0.0 ? t_end : 0.0;
   h.nsteps = nsteps > 0 ? nsteps : 0;
   h.cmax = c->cmax;
-  reset_slot(h, 0);
-  reset_slot(h, 1);
+  reset_slot(h, 0, c->kp);
+  reset_slot(h, 1, c->kp);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (device_ms) {
@@ -740,8 +772,8 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
   std::memset(&h, 0, sizeof(DevCtrl));
   h.time = c->time;
   h.nsteps = nsteps;
-  reset_slot(h, 0);
-  reset_slot(h, 1);
+  reset_slot(h, 0, c->kp);
+  reset_slot(h, 1, c->kp);
   if (ensure_ac(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
@@ -851,6 +883,21 @@ int pip_set_alpha_c(pip_ctx *c, const double *ac) {
   CK(cudaMemcpyAsync(c->acf, ac, c->plane_bytes(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->ac_valid = true;
+  return PIP_OK;
+}
+
+int pip_set_resistivity(pip_ctx *c, const double *eta) {
+  if (!c || !eta) return PIP_ERR_NULL;
+  if (!c->kp.resi) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaStreamSynchronize(c->stream));      // no queued kernel still reads the field
+  CK(cudaMemcpy(c->etaf, eta, c->plane_bytes(), cudaMemcpyHostToDevice));
+  c->kp.resi_dt = resi_bound(c, eta);
+  if (c->graph) {                             // the graph holds the old kernel parameters
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_steps = 0;
+  }
   return PIP_OK;
 }
 
@@ -988,8 +1035,8 @@ int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
   h.t_end = t_end > 0.0 ? t_end : 0.0;
   h.nsteps = nsteps > 0 ? nsteps : 0;
   h.cmax = c->cmax;
-  reset_slot(h, 0);
-  reset_slot(h, 1);
+  reset_slot(h, 0, c->kp);
+  reset_slot(h, 1, c->kp);
   if (ensure_ac(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));                         // the first step's cfl candidates (main.f90:36)

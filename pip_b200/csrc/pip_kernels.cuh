@@ -35,6 +35,10 @@ struct KParams {
   double ac_b2g;     // beta/2*gm of col_type 1, 3, 5
   double ac_sb;      // sqrt(beta/2*gm)
   double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
+  int resi;          // flag_resi 1: resistive flux (eta field etaf), FP64 form
+  const double *etaf;  // eta per cell, nc values
+  double resi_dt;    // cfl_resi's bound min(safety*gmin^2/max(eta,1e-8)) over the interior
+                     // cells (+inf without resistivity); seeds the min-CFL reduction slot
   const double *dx, *dy;
   const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]

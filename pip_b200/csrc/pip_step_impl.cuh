@@ -346,6 +346,53 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
   }
 }
 
+// E = eta*curl B of one cell (get_rotation's s_order-2 branch, Util_rot.f90:148-236, and
+// resistive_flux's ex, ey, ez, Solver_rot.f90:597-599) from the field planes bx, by, bz
+// with row stride sy; gi, gj the cell's global indices (never on the outermost layer).
+template <int NDIM>
+__device__ __forceinline__ void cell_e(const double *bx, const double *by, const double *bz,
+                                       long long c, long long sy, const KParams &p, int gi, int gj,
+                                       double &ex, double &ey, double &ez) {
+  const double eta = p.etaf[(long long)gj * p.ix + gi];
+  const double dx2 = 2.0 * p.dx[gi];
+  double r1 = 0.0, r3;
+  const double r2 = -((bz[c + 1] - bz[c - 1]) / dx2);
+  if (NDIM == 2) {
+    const double dy2 = 2.0 * p.dy[gj];
+    r1 = (bz[c + sy] - bz[c - sy]) / dy2;
+    r3 = (by[c + 1] - by[c - 1]) / dx2 - (bx[c + sy] - bx[c - sy]) / dy2;
+  } else {
+    r3 = (by[c + 1] - by[c - 1]) / dx2;
+  }
+  ex = r1 * eta;
+  ey = r2 * eta;
+  ez = r3 * eta;
+}
+
+// resistive_flux's face terms (Solver_rot.f90:601-636, flag_sch=0 branch) added to the MHD
+// flux F (stride nf) of the face between cells c0 and c1 = c0 + (x: 1, y: sy).
+template <int NDIM>
+__device__ __forceinline__ void add_resistive(double *F, long long nf, long long fo, bool ydir,
+                                              const double *bx, const double *by, const double *bz,
+                                              long long c0, long long sy, const KParams &p,
+                                              int gi, int gj) {
+  double ex0, ey0, ez0, ex1, ey1, ez1;
+  const long long c1 = ydir ? c0 + sy : c0 + 1;
+  cell_e<NDIM>(bx, by, bz, c0, sy, p, gi, gj, ex0, ey0, ez0);
+  cell_e<NDIM>(bx, by, bz, c1, sy, p, ydir ? gi : gi + 1, ydir ? gj + 1 : gj, ex1, ey1, ez1);
+  if (!ydir) {
+    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ey1 + ey0) * (bz[c0] + bz[c1]) -
+                                              (ez0 + ez1) * (by[c0] + by[c1]));
+    F[6 * nf + fo] = F[6 * nf + fo] - 0.5 * (ez0 + ez1);
+    F[7 * nf + fo] = F[7 * nf + fo] + 0.5 * (ey0 + ey1);
+  } else {
+    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ez1 + ez0) * (bx[c0] + bx[c1]) -
+                                              (ex0 + ex1) * (bz[c0] + bz[c1]));
+    F[5 * nf + fo] = F[5 * nf + fo] + 0.5 * (ez0 + ez1);
+    F[7 * nf + fo] = F[7 * nf + fo] - 0.5 * (ex0 + ex1);
+  }
+}
+
 // alpha_c of the ghost cells that the halo exchange filled (faces whose source is -1),
 // from the stage-2 input state there, as set_collisional computes it on every cell after
 // mpi_bnd.  The tiles along such a face take its ghost layers over their columns (rows in
@@ -382,9 +429,10 @@ __device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ 
 // (time_integral) and the ghost fill (PIPbnd).  STAGE 2 optionally fuses the two cfl
 // calls that follow run_solver and open the next step (main.f90:47 and :36): epi = 1
 // applies one cq2pv rewrite; epi = 2 applies two and reduces the next dt; epi = -1 takes
-// 1 or 2 from the control block's last-step flag.  VC: alpha_c per cell (col_type >= 1),
-// a separate instance so that the constant-alpha_c kernels keep their register budget.
-template <int NDIM, int NVM, int STAGE, bool VC>
+// 1 or 2 from the control block's last-step flag.  EXT: the instance for alpha_c per cell
+// (col_type >= 1) and resistivity, separate so that the plain kernels keep their register
+// budget.
+template <int NDIM, int NVM, int STAGE, bool EXT>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
 stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
              DevCtrl *ctrl, int dt_mode, int epi) {
@@ -443,7 +491,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     ctrl->last = ((ctrl->t_end > 0.0 && tn >= ctrl->t_end) ||
                   (ctrl->nsteps > 0 && st + 1 >= ctrl->nsteps)) ? 1 : 0;
     const int ns = (int)((st + 1) & 1);
-    ctrl->red_dt[ns] = dbits(10.0);
+    ctrl->red_dt[ns] = dbits(fmin(10.0, p.resi_dt));  // cfl_mhd's start, cfl_resi's bound
     ctrl->red_rho[ns] = 0ull;
     ctrl->red_gr[ns] = 0ull;
   }
@@ -456,12 +504,14 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   // ---- 1. stage state of the tile and its halo -> primitives in shared memory
   for (int idx = tid; idx < RR; idx += NT) {
     const int ri = idx % RX, rj = idx / RX;
-    if (NDIM == 2 && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
+    // the corners only for the curl of B next to the tile's corner faces (resistivity)
+    if (NDIM == 2 && !(EXT && p.resi) && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH))
+      continue;
     const int gi = i0 - kH + ri, gj = NDIM == 2 ? j0 - kH + rj : 0;
     if (gi >= p.ix || gj >= p.jx) continue;
     double um[NVM], uh[5], vm[NVM], vh[5];
     load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
-    if (VC) {
+    if (EXT && p.col_type) {
       // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux
       double te_m, te_h, rm, rh;
       get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
@@ -519,6 +569,9 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
         const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         Fout[dst * nf + fo] = fx[n];
       }
+      if (EXT && p.resi)
+        add_resistive<NDIM>(Fout, nf, fo, perm_y != 0, sV + 5 * RR, sV + 6 * RR, sV + 7 * RR, a, RX,
+                            p, i0 - kH + a % RX, NDIM == 2 ? j0 - kH + a / RX : 0);
     }
     {
       double vl[5], vr[5], fx[5];
@@ -564,7 +617,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     }
     // alpha_c of the stage (set_coefficients at the stage start; U0 keeps its energies)
     double ac_s = p.ac;
-    if (VC) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
+    if (EXT && p.col_type) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
     double gr = 0.0, gion = 0.0;
     if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
 
@@ -576,7 +629,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
 #pragma unroll
       for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
       double ac_r = p.ac;
-      if (VC) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
+      if (EXT && p.col_type) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
       const Prim<double> qh = rt_hd(r_h, p);
       const Prim<double> qm = rt_mhd<NVM>(r_m, p);
       collision_ds<NVM>(r_m, r_h, qm, qh, p, ac_r, dt_coll, ds);
@@ -665,13 +718,13 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
     if (bad) atomicOr(&ctrl->nan_flag, 1);
     store_cell<NDIM, NVM>(Uo, p, gi, gj, n_m, n_h);
-    if (STAGE == 2 && VC) {
+    if (STAGE == 2 && EXT && p.col_type) {
       // the alpha_c field that the next cfl reads (cfl_pn_col, Scheme_rot.f90:305-313)
       p.acf[q] = ac_s;
       if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
     }
   }
-  if (STAGE == 2 && VC) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
+  if (STAGE == 2 && EXT && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
   if (STAGE == 2 && s_epi == 2) {
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   }
@@ -823,6 +876,12 @@ __global__ void flux_kernel(const KParams p, const double *__restrict__ U, doubl
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         F[qa + dst * nc] = fx[n];
       }
+      if (p.resi) {
+        if (p.ndim == 2)
+          add_resistive<2>(F, nc, qa, py, U + 5 * nc, U + 6 * nc, U + 7 * nc, qa, p.ix, p, i, j);
+        else
+          add_resistive<1>(F, nc, qa, false, U + 5 * nc, U + 6 * nc, U + 7 * nc, qa, p.ix, p, i, j);
+      }
     }
     {
       double vl[5], vr[5], fx[5];
@@ -945,7 +1004,7 @@ static cudaError_t launch_stage_t(const KParams &p, const double *Us, const doub
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   const size_t shm = stage_smem_bytes<NDIM, NVM>();
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
-  if (p.col_type)
+  if (p.col_type || p.resi)
     stage_kernel<NDIM, NVM, STAGE, true><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
   else
     stage_kernel<NDIM, NVM, STAGE, false><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);

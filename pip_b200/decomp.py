@@ -228,7 +228,9 @@ class DeviceBlock:
     """A rank's block on a GPU context (``pip_set_neighbors`` + ``pip_stage`` +
     ``pip_halo_pack/unpack``)."""
 
-    def __init__(self, block: Block, U_h: np.ndarray, U_m: np.ndarray, device: int = 0):
+    def __init__(self, block: Block, U_h: np.ndarray, U_m: np.ndarray, device: int = 0,
+                 eta: Optional[np.ndarray] = None):
+        """eta: the block's part of a fixed resistivity field (flag_resi), if not uniform."""
         import torch
         from .capi import Context
         self.torch = torch
@@ -236,6 +238,8 @@ class DeviceBlock:
         self.ctx = Context(block.settings)
         self.ctx.set_neighbors(block.neighbor)
         self.ctx.upload(U_h, U_m)
+        if eta is not None:
+            self.ctx.set_resistivity(eta)
         self.device = torch.device("cuda", device)
         self.mixed = block.settings.precision != 0
         self.last_stage = 0

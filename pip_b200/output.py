@@ -9,9 +9,9 @@ en_n`` (names from ``set_initial_out`` :362-374).  Every 3D dataset is FP64 of t
 dimensions with ghost cells, Fortran order (x fastest); each rank writes a hyperslab
 (``create_write_dataspaces`` :127-164): its interior, plus its ghost layers on the sides
 where it touches the global boundary.  With alpha_c per cell (flag_col 2..7) the file opens
-its variables with ``ac``, the field of the last set_collisional, as ``def_varfiles``
-(:231-259) writes it before the state at every output; ``restart`` reads it back
-(``reread_variables`` :570-572).  ``config.txt`` (``mk_config`` :377-402) records the
+its variables with ``ac``, the field of the last set_collisional, and with resistivity
+(flag_resi) with ``et``, the eta field, as ``def_varfiles`` (:231-259) writes them before
+the state at every output; restart reads them back (``reread_variables`` :566-572).  ``config.txt`` (``mk_config`` :377-402) records the
 setting lines, the equation flags, variable counts, grid, margins, gamma and flag_bnd, and
 ``restart`` (:405-459) reads them back with the state of output ``flag_restart``.
 
@@ -48,6 +48,8 @@ def file_stem(outdir: str, nout: int) -> str:
 def variables(s: Settings) -> Tuple[str, ...]:
     """The 3D datasets of def_varfiles and save_varfiles, in order."""
     names = ["ac"] if s.flag_col >= 2 else []
+    if s.flag_resi:
+        names.append("et")
     names += list(VAR_M[: s.nvar_m])
     if s.flag_ir != PIP_IR_NONE:
         names += ["ion", "rec"]
@@ -104,12 +106,15 @@ def _create(stem: str, s: Settings, global_shape, time: float, grid) -> Dict[str
     return where
 
 
-def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np.ndarray]):
+def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np.ndarray],
+                  eta: Optional[np.ndarray] = None):
     planes = {}
     if s.flag_col >= 2:
         if ac is None:
             raise ValueError("flag_col %d writes the alpha_c field: pass ac" % s.flag_col)
         planes["ac"] = np.asarray(ac).reshape(U_h.shape[1:])
+    if s.flag_resi:
+        planes["et"] = (s.eta_field() if eta is None else np.asarray(eta)).reshape(U_h.shape[1:])
     planes.update({VAR_M[n]: U_m[n] for n in range(s.nvar_m)})
     if s.flag_ir != PIP_IR_NONE:
         planes["ion"], planes["rec"] = ir_rates(s, U_m)
@@ -119,15 +124,17 @@ def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np
 
 
 def write_output(outdir: str, nout: int, s: Settings, time: float, U_h: np.ndarray,
-                 U_m: np.ndarray, ac: Optional[np.ndarray] = None) -> str:
+                 U_m: np.ndarray, ac: Optional[np.ndarray] = None,
+                 eta: Optional[np.ndarray] = None) -> str:
     """output() of a whole state (global arrays with ghosts, layout (planes, jx, ix)); ac is
-    the alpha_c field (pip_get_alpha_c), needed with flag_col 2..7."""
+    the alpha_c field (pip_get_alpha_c), needed with flag_col 2..7; eta the resistivity
+    field (default: the settings' set_resistivity field)."""
     os.makedirs(outdir, exist_ok=True)
     stem = file_stem(outdir, nout)
     x, y, z, dx, dy, dz = s.coordinates()
     where = _create(stem, s, s.shape, time, (x, y, z, dx, dy, dz))
     mm = np.memmap(stem + ".bin", dtype=np.uint8, mode="r+")
-    for name, plane in _state_planes(s, U_h, U_m, ac).items():
+    for name, plane in _state_planes(s, U_h, U_m, ac, eta).items():
         off, dims = where[name]
         raw = np.ascontiguousarray(plane, dtype="<f8").view(np.uint8).reshape(-1)
         mm[off: off + raw.size] = raw
@@ -146,7 +153,8 @@ def create_output(outdir: str, nout: int, s: Settings, time: float) -> str:
 
 
 def write_output_block(outdir: str, nout: int, s: Settings, block, U_h: np.ndarray,
-                       U_m: np.ndarray, ac: Optional[np.ndarray] = None) -> None:
+                       U_m: np.ndarray, ac: Optional[np.ndarray] = None,
+                       eta: Optional[np.ndarray] = None) -> None:
     """One rank's hyperslab (create_write_dataspaces, IO_rot.f90:127-164) of a decomposed
     output into the file create_output made: the block's interior rows (1D: columns),
     plus its ghost layers on a side where it touches the global boundary.  s is the global
@@ -161,7 +169,10 @@ def write_output_block(outdir: str, nout: int, s: Settings, block, U_h: np.ndarr
     hi_local = m + block.n + (m if block.rank == block.world - 1 else 0)
     g0 = block.lo + lo_local                 # first global index written
     mm = np.memmap(stem + ".bin", dtype=np.uint8, mode="r+")
-    planes = _state_planes(block.settings, U_h, U_m, ac)
+    if s.flag_resi and eta is None:                  # the block's part of the global field
+        from .decomp import scatter
+        eta = scatter(s, s.eta_field()[None], block.world, block.rank)[0]
+    planes = _state_planes(block.settings, U_h, U_m, ac, eta)
     for name, off, dims in entries:
         if name not in planes:
             continue
@@ -257,6 +268,16 @@ def restart(outdir: str, nout: int, s: Settings) -> Tuple[float, np.ndarray, np.
     U_m = np.stack([d[VAR_M[n]][0] for n in range(s.nvar_m)]).reshape(s.nvar_m, jx, ix)
     U_h = np.stack([d[v][0] for v in VAR_H]).reshape(5, jx, ix)
     return d["time"], np.ascontiguousarray(U_h), np.ascontiguousarray(U_m)
+
+
+def restart_resistivity(outdir: str, nout: int, s: Settings) -> Optional[np.ndarray]:
+    """The eta field of output nout (jx, ix) that restart reads with flag_resi (IO_rot.f90:
+    566-568), for pip_set_resistivity; None without resistivity."""
+    if not s.flag_resi:
+        return None
+    d = read_output(file_stem(outdir, nout))
+    ix, jx, _ = s.shape
+    return np.ascontiguousarray(d["et"][0].reshape(jx, ix))
 
 
 def restart_alpha_c(outdir: str, nout: int, s: Settings) -> Optional[np.ndarray]:

@@ -52,7 +52,8 @@ class PipParams(ctypes.Structure):
         ("flag_bnd", ctypes.c_int32 * 6),
         ("precision", ctypes.c_int32),
         ("fp_exact", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 6),
+        ("flag_resi", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 5),
         ("gm", ctypes.c_double),
         ("safety", ctypes.c_double),
         ("ro_lim", ctypes.c_double),
@@ -67,7 +68,8 @@ class PipParams(ctypes.Structure):
         ("kapper", ctypes.c_double),
         ("hc_error", ctypes.c_double),
         ("beta", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 6),
+        ("eta_0", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 5),
         ("dx", ctypes.POINTER(ctypes.c_double)),
         ("dy", ctypes.POINTER(ctypes.c_double)),
         ("dz", ctypes.POINTER(ctypes.c_double)),
@@ -127,7 +129,9 @@ class Settings:
     kapper: float = 0.0
     hc_max: int = 500
     hc_error: float = 1.0e-10
-    flag_resi: int = 0
+    flag_resi: int = 0          # 10*resi_type + 1 (Res_rot.f90:8-15): 1 uniform, 11 localised
+    eta_0: float = 0.0
+    debug_parameter: float = 0.0
     flag_amb: int = 0
     flag_visc: int = 0
     flag_grav: int = 0
@@ -210,6 +214,17 @@ class Settings:
             out.append(c)
         return out[0], out[1], out[2], dx, dy, dz
 
+    def eta_field(self) -> np.ndarray:
+        """set_resistivity's eta (Res_rot.f90:16-60) as (jx, ix): resi_type 0 eta_0
+        everywhere, resi_type 1 eta_0*exp(-((x/0.8)**2 + ((y-debug_parameter)/0.8)**2))."""
+        x, y, _, _, _, _ = self.coordinates()
+        ix, jx, _ = self.shape
+        if (self.flag_resi // 10) % 10 == 1:
+            ax = x / 0.8
+            ay = (y - self.debug_parameter) / 0.8
+            return self.eta_0 * np.exp(-(ax[None, :] * ax[None, :] + ay[:, None] * ay[:, None]))
+        return np.full((jx, ix), float(self.eta_0))
+
     # ---------------------------------------------------------------- checks
     def validate(self) -> None:
         """Raise ValueError for settings outside the supported two-fluid path."""
@@ -228,8 +243,13 @@ class Settings:
             bad.append("flag_col 2..7 (alpha_c per cell) needs precision PIP_FP64")
         elif self.flag_col in (2, 4, 6) and not self.beta > 0.0:
             bad.append("flag_col %d divides by sqrt(beta*gm/2): beta must be > 0" % self.flag_col)
-        if self.flag_resi or self.flag_amb or self.flag_visc or self.flag_grav:
-            bad.append("resistivity, ambipolar, viscosity and gravity are not supported")
+        if self.flag_resi not in (0, 1, 11):
+            bad.append("flag_resi must be 0, 1 (uniform eta_0) or 11 (localised eta), "
+                       "a fixed eta field")
+        elif self.flag_resi and (self.precision != PIP_FP64 or self.flag_heat):
+            bad.append("resistivity needs precision PIP_FP64 and no conduction")
+        if self.flag_amb or self.flag_visc or self.flag_grav:
+            bad.append("ambipolar diffusion, viscosity and gravity are not supported")
         if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW):
             bad.append("flag_ir must be 0 or %d" % PIP_IR_POWERLAW)
         if self.flag_ir and self.flag_ir_type not in (1, 2):
@@ -286,6 +306,8 @@ class Settings:
         p.kapper = self.kapper
         p.hc_error = self.hc_error
         p.beta = self.beta
+        p.flag_resi = self.flag_resi % 10
+        p.eta_0 = self.eta_0
         dptr = ctypes.POINTER(ctypes.c_double)
         p.dx = dx.ctypes.data_as(dptr)
         p.dy = dy.ctypes.data_as(dptr)
@@ -307,7 +329,8 @@ class Settings:
         reals = {"gm_d": "gm_d", "gm_n": "gm_n", "safety": "safety", "db_clean": "db_clean",
                  "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
                  "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",
-                 "kapper": "kapper", "tend": "tend", "beta": "beta"}
+                 "kapper": "kapper", "tend": "tend", "beta": "beta", "eta_0": "eta_0",
+                 "debug_parameter": "debug_parameter"}
         bnd = {"flag_bnd_x_l": 0, "flag_bnd_x_r": 1, "flag_bnd_y_l": 2, "flag_bnd_y_r": 3,
                "flag_bnd_z_l": 4, "flag_bnd_z_r": 5}
         for raw in text.splitlines():

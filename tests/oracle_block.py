@@ -10,11 +10,13 @@ from oracle import oracle as O
 
 
 class OracleBlock:
-    def __init__(self, block, U_h, U_m):
+    def __init__(self, block, U_h, U_m, eta=None):
         self.block = block
         self.s = block.settings
         self.o = O.Oracle(self.s, U_h, U_m)
         self.o.set_neighbors(block.neighbor)
+        if eta is not None:
+            self.o.set_resistivity(eta)
         ix, jx, _ = self.s.shape
         self.n = (ix, jx)
         self.m = self.s.margin
