@@ -37,9 +37,10 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
   recombination and implicit anisotropic conduction (BiCGstab to 1e-10), 1000 steps, plain
   FP64 and FP32-mixed (FP32 inner solve with FP64 iterative refinement): ms per step,
   iterations per step, solver time and GB/s per iteration, mixed-vs-FP64 L1.
-* alpha_c_per_cell: the FP64 OT step with flag_col=5 (set_collisional col_type 4: alpha_c
-  from both temperatures and the drift, recomputed at every RK stage), 500 steps, and its
-  cost over the constant-alpha_c FP64 step.
+* alpha_c_per_cell, resistivity: the FP64 OT step with flag_col=5 (set_collisional
+  col_type 4: alpha_c from both temperatures and the drift, recomputed at every RK stage),
+  and with flag_resi=1, eta_0=1e-4 (resistive_flux on every face; margin 3), 500 steps
+  each, and their cost over the plain FP64 step.
 """
 from __future__ import annotations
 
@@ -370,14 +371,13 @@ def e2e_run(s, Uh, Um, steps, warmup, dist):
     return e2e_s, Uh.nbytes + Um.nbytes
 
 
-def measure_alpha_c(n, steps, ms_constant, flag_col=5):
-    """The FP64 step with alpha_c per cell (set_collisional col_type flag_col-1 at every RK
-    stage: temperatures and drift of both species, energy rewrite) on the same OT n x n,
-    against the constant-alpha_c step measured before (ms_constant per step)."""
+def measure_variant(n, steps, ms_plain, what, **overrides):
+    """The FP64 step of the OT n x n workload with extra physics (overrides of the
+    settings), against the plain FP64 step measured before (ms_plain per step)."""
     import torch
     from pip_b200 import capi, ics
     from pip_b200.params import PIP_FP64
-    s, Uh, Um = ics.orszag_tang(n, precision=PIP_FP64, flag_col=flag_col)
+    s, Uh, Um = ics.orszag_tang(n, precision=PIP_FP64, **overrides)
     ctx = capi.Context(s)
     ctx.upload(Uh, Um)
     ctx.prologue()
@@ -388,12 +388,11 @@ def measure_alpha_c(n, steps, ms_constant, flag_col=5):
     ms1, ms2, _ = ctx.stage_ms(min(200, steps))
     ctx.close()
     if st != 0 or nstep != steps:
-        raise RuntimeError("alpha_c run ended with status %d after %d steps" % (st, nstep))
-    return {"workload": "OT %dx%d FP64, flag_col=%d (col_type %d)" % (n, n, flag_col,
-                                                                   flag_col - 1),
-            "steps": steps, "ms_per_step": ms / steps, "value": n * n * steps / (ms * 1e-3),
-            "unit": UNIT, "ms_stage1": ms1, "ms_stage2": ms2,
-            "over_constant_alpha_c": (ms / steps) / ms_constant, "gpu_launches": launches}
+        raise RuntimeError("%s run ended with status %d after %d steps" % (what, st, nstep))
+    return {"workload": "OT %dx%d FP64, %s" % (n, n, what), "steps": steps,
+            "ms_per_step": ms / steps, "value": n * n * steps / (ms * 1e-3), "unit": UNIT,
+            "ms_stage1": ms1, "ms_stage2": ms2, "over_plain_fp64": (ms / steps) / ms_plain,
+            "gpu_launches": launches}
 
 
 def measure_adjoint(nsteps=500, K=25):
@@ -544,7 +543,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-conduction", action="store_true")
-    ap.add_argument("--no-alpha-c", action="store_true")
+    ap.add_argument("--no-extra-physics", action="store_true")
     ap.add_argument("--decompose", action="store_true",
                     help="run the domain-decomposed step also with one GPU (always with N > 1)")
     args = ap.parse_args()
@@ -620,7 +619,13 @@ def main():
     adjoint = None if args.no_adjoint else measure_adjoint()
     ensemble = None if args.no_ensemble else measure_ensemble()
     conduction = None if args.no_conduction else measure_conduction()
-    alpha_c = None if args.no_alpha_c else measure_alpha_c(n, 500, ms64 / args.steps)
+    alpha_c = resistivity = None
+    if not args.no_extra_physics:
+        alpha_c = measure_variant(n, 500, ms64 / args.steps,
+                                  "flag_col=5 (set_collisional col_type 4)", flag_col=5)
+        resistivity = measure_variant(n, 500, ms64 / args.steps,
+                                      "flag_resi=1, eta_0=1e-4 (resistive_flux)",
+                                      flag_resi=1, eta_0=1.0e-4)
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
@@ -670,6 +675,7 @@ def main():
         "ensemble": ensemble,
         "conduction": conduction,
         "alpha_c_per_cell": alpha_c,
+        "resistivity": resistivity,
         "e2e": e2e,
         "gpu_launches": mix["launches"],
         "clocks": mix["clocks"],

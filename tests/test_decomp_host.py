@@ -70,7 +70,7 @@ def local_run(case, world, nsteps):
 
 @pytest.mark.parametrize("case,world", [("ot", 2), ("ot", 4), ("ot_generic", 2), ("kh", 2),
                                         ("kh", 4), ("bw", 2), ("bw", 4), ("ot_col", 4),
-                                        ("kh_col", 2)])
+                                        ("kh_col", 2), ("ot_resi", 4)])
 def test_blocks_in_one_process_match_single_domain(case, world):
     nsteps = 6
     s, uh, um, hist = single_domain(case, nsteps)
@@ -86,7 +86,7 @@ def _free_port():
         return k.getsockname()[1]
 
 
-@pytest.mark.parametrize("case", ["ot", "kh", "bw"])
+@pytest.mark.parametrize("case", ["ot", "kh", "bw", "ot_resi"])
 def test_two_gloo_ranks_match_single_domain(case):
     nsteps = 5
     s, uh, um, hist = single_domain(case, nsteps)
