@@ -112,3 +112,27 @@ def test_conduction_rejects_unsupported(gpu_lib):
     with capi.Context(s2) as c:
         with pytest.raises(capi.PipError):
             c.conduction(1e-3)
+
+
+def test_run_with_conduction_and_alpha_c_per_cell(gpu_lib):
+    """Conduction after the stages with alpha_c per cell (set_collisional col_type 4)."""
+    s, _, _ = ics.kelvin_helmholtz(48, 24, flag_heat=1, kapper=1.0, hc_error=1.0e-12,
+                                   hc_max=2000, flag_col=5)
+    Uh, Um = generic_state(s, 3)
+    o = O.Oracle(s, Uh, Um)
+    o.prologue()
+    st_o, t_o, n_o, _ = o.run(nsteps=12)
+    oh, om = o.state()
+    ac_o = o.alpha_c()
+    o.close()
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        st, t, n = c.run(nsteps=12)
+        gh, gm = c.download()
+        ac_g = c.alpha_c()
+    assert st_o == 0 and st == 0 and n == n_o == 12
+    assert abs(t - t_o) <= 1e-12 * t_o
+    assert max(rel_l1(interior(gh, s), interior(oh, s)).max(),
+               rel_l1(interior(gm, s), interior(om, s)).max()) <= 1e-10
+    assert np.abs(ac_g - ac_o).sum() <= 1e-10 * np.abs(ac_o).sum()
