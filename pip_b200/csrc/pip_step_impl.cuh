@@ -354,9 +354,21 @@ __device__ __forceinline__ void cell_e(const double *bx, const double *by, const
                                        long long c, long long sy, const KParams &p, int gi, int gj,
                                        double &ex, double &ey, double &ez) {
   const double eta = p.etaf[(long long)gj * p.ix + gi];
+  double r1 = 0.0, r2, r3;
+#if PIP_RCP
+  // the FMA build multiplies by 1/(2 dx), 1/(2 dy)
+  const double rx = 1.0 / (2.0 * p.dx[gi]);
+  r2 = -((bz[c + 1] - bz[c - 1]) * rx);
+  if (NDIM == 2) {
+    const double ry = 1.0 / (2.0 * p.dy[gj]);
+    r1 = (bz[c + sy] - bz[c - sy]) * ry;
+    r3 = (by[c + 1] - by[c - 1]) * rx - (bx[c + sy] - bx[c - sy]) * ry;
+  } else {
+    r3 = (by[c + 1] - by[c - 1]) * rx;
+  }
+#else
   const double dx2 = 2.0 * p.dx[gi];
-  double r1 = 0.0, r3;
-  const double r2 = -((bz[c + 1] - bz[c - 1]) / dx2);
+  r2 = -((bz[c + 1] - bz[c - 1]) / dx2);
   if (NDIM == 2) {
     const double dy2 = 2.0 * p.dy[gj];
     r1 = (bz[c + sy] - bz[c - sy]) / dy2;
@@ -364,13 +376,32 @@ __device__ __forceinline__ void cell_e(const double *bx, const double *by, const
   } else {
     r3 = (by[c + 1] - by[c - 1]) / dx2;
   }
+#endif
   ex = r1 * eta;
   ey = r2 * eta;
   ez = r3 * eta;
 }
 
 // resistive_flux's face terms (Solver_rot.f90:601-636, flag_sch=0 branch) added to the MHD
-// flux F (stride nf) of the face between cells c0 and c1 = c0 + (x: 1, y: sy).
+// flux F (stride nf) of a face from E of its two cells (0: left/lower, 1: right/upper) and
+// B there.
+__device__ __forceinline__ void face_terms(double *F, long long nf, long long fo, bool ydir,
+                                           double ex0, double ey0, double ez0, double ex1,
+                                           double ey1, double ez1, double bx0, double bx1,
+                                           double by0, double by1, double bz0, double bz1) {
+  if (!ydir) {
+    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ey1 + ey0) * (bz0 + bz1) - (ez0 + ez1) * (by0 + by1));
+    F[6 * nf + fo] = F[6 * nf + fo] - 0.5 * (ez0 + ez1);
+    F[7 * nf + fo] = F[7 * nf + fo] + 0.5 * (ey0 + ey1);
+  } else {
+    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ez1 + ez0) * (bx0 + bx1) - (ex0 + ex1) * (bz0 + bz1));
+    F[5 * nf + fo] = F[5 * nf + fo] + 0.5 * (ez0 + ez1);
+    F[7 * nf + fo] = F[7 * nf + fo] - 0.5 * (ex0 + ex1);
+  }
+}
+
+// The face terms of the face between cells c0 and c1 = c0 + (x: 1, y: sy) of the field
+// planes, E computed at both cells (the unit-level flux kernel).
 template <int NDIM>
 __device__ __forceinline__ void add_resistive(double *F, long long nf, long long fo, bool ydir,
                                               const double *bx, const double *by, const double *bz,
@@ -380,17 +411,8 @@ __device__ __forceinline__ void add_resistive(double *F, long long nf, long long
   const long long c1 = ydir ? c0 + sy : c0 + 1;
   cell_e<NDIM>(bx, by, bz, c0, sy, p, gi, gj, ex0, ey0, ez0);
   cell_e<NDIM>(bx, by, bz, c1, sy, p, ydir ? gi : gi + 1, ydir ? gj + 1 : gj, ex1, ey1, ez1);
-  if (!ydir) {
-    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ey1 + ey0) * (bz[c0] + bz[c1]) -
-                                              (ez0 + ez1) * (by[c0] + by[c1]));
-    F[6 * nf + fo] = F[6 * nf + fo] - 0.5 * (ez0 + ez1);
-    F[7 * nf + fo] = F[7 * nf + fo] + 0.5 * (ey0 + ey1);
-  } else {
-    F[4 * nf + fo] = F[4 * nf + fo] + 0.25 * ((ez1 + ez0) * (bx[c0] + bx[c1]) -
-                                              (ex0 + ex1) * (bz[c0] + bz[c1]));
-    F[5 * nf + fo] = F[5 * nf + fo] + 0.5 * (ez0 + ez1);
-    F[7 * nf + fo] = F[7 * nf + fo] - 0.5 * (ex0 + ex1);
-  }
+  face_terms(F, nf, fo, ydir, ex0, ey0, ez0, ex1, ey1, ez1, bx[c0], bx[c1], by[c0], by[c1], bz[c0],
+             bz[c1]);
 }
 
 // alpha_c of the ghost cells that the halo exchange filled (faces whose source is -1),
@@ -429,10 +451,10 @@ __device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ 
 // (time_integral) and the ghost fill (PIPbnd).  STAGE 2 optionally fuses the two cfl
 // calls that follow run_solver and open the next step (main.f90:47 and :36): epi = 1
 // applies one cq2pv rewrite; epi = 2 applies two and reduces the next dt; epi = -1 takes
-// 1 or 2 from the control block's last-step flag.  EXT: the instance for alpha_c per cell
-// (col_type >= 1) and resistivity, separate so that the plain kernels keep their register
-// budget.
-template <int NDIM, int NVM, int STAGE, bool EXT>
+// 1 or 2 from the control block's last-step flag.  X selects the extra physics of the
+// instance: bit 0 alpha_c per cell (col_type >= 1), bit 1 resistivity; each combination is
+// its own instance so that the others keep their register budget.
+template <int NDIM, int NVM, int STAGE, int X>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
 stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
              DevCtrl *ctrl, int dt_mode, int epi) {
@@ -440,10 +462,13 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   constexpr int NV = NVM + 5;
   constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
+  constexpr int EW = TX + 2, EH = NDIM == 2 ? TY + 2 : 1, EN = EW * EH;
   extern __shared__ double smem[];
   double *sV = smem;
   double *sFx = sV + NV * RR;
   double *sFy = sFx + NV * NFX;
+  constexpr bool COL = (X & 1) != 0, RES = (X & 2) != 0;
+  double *sE = sFy + NV * NFY;  // RES only: E of the tile's cells and one ring
   __shared__ double s_dt, s_cmax;
   __shared__ long long s_step;
   __shared__ int s_exit, s_epi;
@@ -505,13 +530,13 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   for (int idx = tid; idx < RR; idx += NT) {
     const int ri = idx % RX, rj = idx / RX;
     // the corners only for the curl of B next to the tile's corner faces (resistivity)
-    if (NDIM == 2 && !(EXT && p.resi) && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH))
+    if (NDIM == 2 && !RES && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH))
       continue;
     const int gi = i0 - kH + ri, gj = NDIM == 2 ? j0 - kH + rj : 0;
     if (gi >= p.ix || gj >= p.jx) continue;
     double um[NVM], uh[5], vm[NVM], vh[5];
     load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
-    if (EXT && p.col_type) {
+    if (COL) {
       // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux
       double te_m, te_h, rm, rh;
       get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
@@ -524,6 +549,21 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
   }
   __syncthreads();
+  if (RES) {
+    // E = eta*curl B once per cell of the tile and its first ring (each enters four faces)
+    for (int idx = tid; idx < EN; idx += NT) {
+      const int er = idx % EW, ej = idx / EW;
+      const int gi = i0 - 1 + er, gj = NDIM == 2 ? j0 - 1 + ej : 0;
+      if (gi > p.ix - 2 || (NDIM == 2 && gj > p.jx - 2)) continue;
+      const int c = (NDIM == 2 ? (ej + kH - 1) * RX : 0) + er + kH - 1;
+      double ex, ey, ez;
+      cell_e<NDIM>(sV + 5 * RR, sV + 6 * RR, sV + 7 * RR, c, RX, p, gi, gj, ex, ey, ez);
+      sE[idx] = ex;
+      sE[EN + idx] = ey;
+      sE[2 * EN + idx] = ez;
+    }
+    __syncthreads();
+  }
 
   // ---- 2. face fluxes (set_flux): x faces then y faces of the tile
   const int iend = p.m0 + p.nx, jend = NDIM == 2 ? p.m1 + p.ny : 1;
@@ -569,9 +609,6 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
         const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         Fout[dst * nf + fo] = fx[n];
       }
-      if (EXT && p.resi)
-        add_resistive<NDIM>(Fout, nf, fo, perm_y != 0, sV + 5 * RR, sV + 6 * RR, sV + 7 * RR, a, RX,
-                            p, i0 - kH + a % RX, NDIM == 2 ? j0 - kH + a / RX : 0);
     }
     {
       double vl[5], vr[5], fx[5];
@@ -591,6 +628,40 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
         const int dst = perm_y ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;
         Fout[(NVM + dst) * nf + fo] = fx[n];
       }
+    }
+  }
+  if (RES) {
+    // resistive_flux's terms, added by the thread that wrote the face's flux (same faces
+    // per thread as above), in a loop of their own to keep the Riemann solvers' registers
+    for (int f = tid; f < NFX + NFY; f += NT) {
+      int a, s, nf, fo, e0, e1;
+      double *Fout;
+      const bool ydir = f >= NFX;
+      if (!ydir) {
+        const int fi = f % (TX + 1), fj = f / (TX + 1);
+        if (i0 + fi - 1 >= iend || (NDIM == 2 && j0 + fj >= jend)) continue;
+        a = (NDIM == 2 ? (fj + kH) * RX : 0) + fi + kH - 1;
+        s = 1;
+        Fout = sFx;
+        fo = f;
+        nf = NFX;
+        e0 = (NDIM == 2 ? (fj + 1) * EW : 0) + fi;
+        e1 = e0 + 1;
+      } else {
+        const int g = f - NFX, fi = g % TX, fj = g / TX;
+        if (i0 + fi >= iend || j0 + fj - 1 >= jend) continue;
+        a = (fj + kH - 1) * RX + fi + kH;
+        s = RX;
+        Fout = sFy;
+        fo = g;
+        nf = NFY;
+        e0 = fj * EW + fi + 1;
+        e1 = e0 + EW;
+      }
+      const int a1 = a + s;
+      const double *bx = sV + 5 * RR, *by = sV + 6 * RR, *bz = sV + 7 * RR;
+      face_terms(Fout, nf, fo, ydir, sE[e0], sE[EN + e0], sE[2 * EN + e0], sE[e1], sE[EN + e1],
+                 sE[2 * EN + e1], bx[a], bx[a1], by[a], by[a1], bz[a], bz[a1]);
     }
   }
   __syncthreads();
@@ -617,7 +688,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     }
     // alpha_c of the stage (set_coefficients at the stage start; U0 keeps its energies)
     double ac_s = p.ac;
-    if (EXT && p.col_type) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
+    if (COL) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
     double gr = 0.0, gion = 0.0;
     if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
 
@@ -629,7 +700,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
 #pragma unroll
       for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
       double ac_r = p.ac;
-      if (EXT && p.col_type) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
+      if (COL) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
       const Prim<double> qh = rt_hd(r_h, p);
       const Prim<double> qm = rt_mhd<NVM>(r_m, p);
       collision_ds<NVM>(r_m, r_h, qm, qh, p, ac_r, dt_coll, ds);
@@ -718,13 +789,13 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
     if (bad) atomicOr(&ctrl->nan_flag, 1);
     store_cell<NDIM, NVM>(Uo, p, gi, gj, n_m, n_h);
-    if (STAGE == 2 && EXT && p.col_type) {
+    if (STAGE == 2 && COL) {
       // the alpha_c field that the next cfl reads (cfl_pn_col, Scheme_rot.f90:305-313)
       p.acf[q] = ac_s;
       if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
     }
   }
-  if (STAGE == 2 && EXT && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
+  if (STAGE == 2 && COL) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
   if (STAGE == 2 && s_epi == 2) {
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   }
@@ -967,23 +1038,29 @@ __global__ void nan_kernel(const double *__restrict__ U, long long n, int *flag)
 
 // ---------------------------------------------------------------- host launchers
 
-template <int NDIM, int NVM>
+template <int NDIM, int NVM, int X>
 constexpr size_t stage_smem_bytes() {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY;
   constexpr int RR = (TX + 2 * kH) * (NDIM == 2 ? TY + 2 * kH : 1);
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
-  return sizeof(double) * (NVM + 5) * (RR + NFX + NFY);
+  constexpr int EN = (TX + 2) * (NDIM == 2 ? TY + 2 : 1);
+  return sizeof(double) * ((NVM + 5) * (RR + NFX + NFY) + ((X & 2) ? 3 * EN : 0));
+}
+
+template <int NDIM, int NVM, int STAGE, int X>
+static cudaError_t set_stage_attr_x() {
+  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE, X>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)stage_smem_bytes<NDIM, NVM, X>());
 }
 
 template <int NDIM, int NVM, int STAGE>
 static cudaError_t set_stage_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_smem_bytes<NDIM, NVM>());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<NDIM, NVM, STAGE, true>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)stage_smem_bytes<NDIM, NVM>());
+  cudaError_t e;
+  if ((e = set_stage_attr_x<NDIM, NVM, STAGE, 0>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr_x<NDIM, NVM, STAGE, 1>()) != cudaSuccess) return e;
+  if ((e = set_stage_attr_x<NDIM, NVM, STAGE, 2>()) != cudaSuccess) return e;
+  return set_stage_attr_x<NDIM, NVM, STAGE, 3>();
 }
 
 // Raises the dynamic shared-memory limit of every stage-kernel instance on the current
@@ -1002,12 +1079,25 @@ template <int NDIM, int NVM, int STAGE>
 static cudaError_t launch_stage_t(const KParams &p, const double *Us, const double *U0, double *Uo,
                                   DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
-  const size_t shm = stage_smem_bytes<NDIM, NVM>();
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
-  if (p.col_type || p.resi)
-    stage_kernel<NDIM, NVM, STAGE, true><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
-  else
-    stage_kernel<NDIM, NVM, STAGE, false><<<grid, NT, shm, s>>>(p, Us, U0, Uo, ctrl, dt_mode, epi);
+  switch ((p.col_type ? 1 : 0) | (p.resi ? 2 : 0)) {
+    case 0:
+      stage_kernel<NDIM, NVM, STAGE, 0><<<grid, NT, stage_smem_bytes<NDIM, NVM, 0>(), s>>>(
+          p, Us, U0, Uo, ctrl, dt_mode, epi);
+      break;
+    case 1:
+      stage_kernel<NDIM, NVM, STAGE, 1><<<grid, NT, stage_smem_bytes<NDIM, NVM, 1>(), s>>>(
+          p, Us, U0, Uo, ctrl, dt_mode, epi);
+      break;
+    case 2:
+      stage_kernel<NDIM, NVM, STAGE, 2><<<grid, NT, stage_smem_bytes<NDIM, NVM, 2>(), s>>>(
+          p, Us, U0, Uo, ctrl, dt_mode, epi);
+      break;
+    default:
+      stage_kernel<NDIM, NVM, STAGE, 3><<<grid, NT, stage_smem_bytes<NDIM, NVM, 3>(), s>>>(
+          p, Us, U0, Uo, ctrl, dt_mode, epi);
+      break;
+  }
   return cudaGetLastError();
 }
 
