@@ -46,6 +46,14 @@ enum pip_precision {
 /* Ionisation/recombination laws accepted in pip_params.flag_ir. */
 enum pip_ir_law {
   PIP_IR_NONE = 0,
+  /* set_IR type 2 (PIP_rot.f90:148-170): Popescu et al. 2019 empirical rates with the
+   * electron temperature T_norm/1.1604e4 eV and n_norm; recomputed with set_coefficients at
+   * every RK stage (Solver_rot.f90:111) and before each cfl (main.f90:32-34,44-46), each time
+   * after get_Te's energy rewrite (Scheme_rot.f90:83-128). */
+  PIP_IR_POPESCU = 2,
+  /* set_IR type 3 (PIP_rot.f90:173-228): the type-2 rates scaled to the ionisation
+   * equilibrium of T_norm (f_n, f_p, tfac from flag_col's parity and beta); same calls. */
+  PIP_IR_POPESCU_EQ = 3,
   /* Gm_ion = ir_ion_coef*T^-1/2*exp(-ir_chi/T), Gm_rec = ir_rec_coef*T^-1/2 with
    * T = gm*p_i/(2 rho_i) (get_Te_MHD, Scheme_rot.f90:104-110); the rates are frozen at
    * the start of each step as set_IR is (main.f90:32-34).  This law is new: none of
@@ -109,7 +117,9 @@ typedef struct pip_params {
   double hc_error;         /* BiCGstab relative residual target */
   double beta;             /* plasma beta of set_collisional col_type 1, 3, 5 (> 0 there) */
   double eta_0;            /* uniform resistivity (set_resistivity resi_type 0) */
-  double reserved_d[5];
+  double t_norm, n_norm;   /* T0 (K) and n0 of the normalisation (setting keys T_norm, n_norm;
+                              set_IR types 2 and 3) */
+  double reserved_d[3];
   const double *dx;        /* ix cell widths (dsc(:,1)) */
   const double *dy;        /* jx cell widths (dsc(:,2)); 1D: one entry, the reference sets 100 */
   const double *dz;        /* kx cell widths (dsc(:,3)); one entry, the reference sets 100 */

@@ -67,6 +67,7 @@ def lib():
         L.orc_has_nan.restype = ctypes.c_int
         L.orc_coefficients.argtypes = [vp]
         L.orc_set_resistivity.argtypes = [vp, dp]
+        L.orc_ir_rates.argtypes = [vp, dp, dp]
         L.orc_alpha_c.argtypes = [vp, dp]
         L.orc_alpha_c.restype = ctypes.c_int
         _lib = L
@@ -182,6 +183,13 @@ class Oracle:
         """The eta field (jx, ix) of flag_resi 1 (eta_0 everywhere until set)."""
         e = np.ascontiguousarray(eta, dtype=np.float64).reshape(self.shape_h[1:])
         lib().orc_set_resistivity(self.h, _ptr(e))
+
+    def ir_rates(self):
+        """(Gm_ion, Gm_rec) of the last set_IR, each shaped like one plane."""
+        ion = np.empty(self.shape_h[1:])
+        rec = np.empty(self.shape_h[1:])
+        lib().orc_ir_rates(self.h, _ptr(ion), _ptr(rec))
+        return ion, rec
 
     def alpha_c(self) -> np.ndarray:
         """alpha_c of every cell, shaped like one plane of the state."""

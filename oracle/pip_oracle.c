@@ -39,7 +39,7 @@ struct orc_ctx {
   double stage_dt;
   int col_type;                      /* initialize_collisional: flag_col 2..7 -> 1..6 */
   double *ac;                        /* alpha_c per cell (globalvar ac) for col_type >= 1 */
-  int ac_valid;                      /* set by the first set_collisional */
+  int init_done;                     /* set_coefficients(U_h,U_m,0) has run */
   int resi;                          /* flag_resi 1: resistive flux with the eta field */
   double *eta;                       /* globalvar eta (set_resistivity), nc values */
 };
@@ -742,41 +742,104 @@ static double alpha_c_cell(int type, double col, double beta, double gm, double 
  * Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro; get_vel_diff (:988-999) gives the drift; alpha_c of
  * every cell, ghosts included, goes to c->ac.  The floor `if(minval(pr).le.pr_lim)
  * pr=max(pr,pr_lim)` is the per-cell max. */
+/* get_Te_MHD and get_Te_HD (Scheme_rot.f90:83-128) on cell q: both energies rewritten
+ * through the floored pressure; Te_m = 0.5*gm*pr/ro, Te_h = gm*pr/ro. */
+static void get_te_cell(orc_ctx *c, size_t q, double *te_m, double *te_h) {
+  size_t nc = c->nc;
+  double gm = c->p.gm, pr_lim = c->p.pr_lim;
+  double *Um = c->U_m, *Uh = c->U_h;
+  double m1 = Um[q], m2 = Um[q + nc], m3 = Um[q + 2 * nc], m4 = Um[q + 3 * nc];
+  double m6 = Um[q + 5 * nc], m7 = Um[q + 6 * nc], m8 = Um[q + 7 * nc];
+  double prm = (gm - 1.0) * (Um[q + 4 * nc] -
+                             0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 + m7 * m7 + m8 * m8));
+  prm = fmx(prm, pr_lim);
+  Um[q + 4 * nc] = prm / (gm - 1.0) + 0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 +
+                                             m7 * m7 + m8 * m8);
+  *te_m = 0.5 * gm * (prm / m1);
+  double h1 = Uh[q], h2 = Uh[q + nc], h3 = Uh[q + 2 * nc], h4 = Uh[q + 3 * nc];
+  double prh = (gm - 1.0) * (Uh[q + 4 * nc] - 0.5 * (h2 * h2 + h3 * h3 + h4 * h4) / h1);
+  prh = fmx(prh, pr_lim);
+  Uh[q + 4 * nc] = prh / (gm - 1.0) + 0.5 * ((h2 * h2 + h3 * h3 + h4 * h4) / h1);
+  *te_h = gm * (prh / h1);
+}
+
 static void set_collisional(orc_ctx *c) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
-  double gm = p->gm, pr_lim = p->pr_lim, col = p->col, beta = p->beta;
+  double gm = p->gm, col = p->col, beta = p->beta;
   int type = c->col_type;
-  double *Um = c->U_m, *Uh = c->U_h;
+  const double *Um = c->U_m, *Uh = c->U_h;
 #pragma omp parallel for schedule(static)
   for (size_t q = 0; q < nc; ++q) {
+    double te_m, te_h;
+    get_te_cell(c, q, &te_m, &te_h);
     double m1 = Um[q], m2 = Um[q + nc], m3 = Um[q + 2 * nc], m4 = Um[q + 3 * nc];
-    double m6 = Um[q + 5 * nc], m7 = Um[q + 6 * nc], m8 = Um[q + 7 * nc];
-    double prm = (gm - 1.0) * (Um[q + 4 * nc] -
-                               0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 + m7 * m7 + m8 * m8));
-    prm = fmx(prm, pr_lim);
-    Um[q + 4 * nc] = prm / (gm - 1.0) + 0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 +
-                                               m7 * m7 + m8 * m8);
-    double te_m = 0.5 * gm * (prm / m1);
     double h1 = Uh[q], h2 = Uh[q + nc], h3 = Uh[q + 2 * nc], h4 = Uh[q + 3 * nc];
-    double prh = (gm - 1.0) * (Uh[q + 4 * nc] - 0.5 * (h2 * h2 + h3 * h3 + h4 * h4) / h1);
-    prh = fmx(prh, pr_lim);
-    Uh[q + 4 * nc] = prh / (gm - 1.0) + 0.5 * ((h2 * h2 + h3 * h3 + h4 * h4) / h1);
-    double te_h = gm * (prh / h1);
     c->ac[q] = alpha_c_cell(type, col, beta, gm, te_h, te_m, h2 / h1 - m2 / m1, h3 / h1 - m3 / m1,
                             h4 / h1 - m4 / m1);
   }
-  c->ac_valid = 1;
 }
 
-/* The alpha_c field of the last set_collisional, made by set_coefficients(U_h,U_m,0)
- * (Initial_rot.f90:140) on the state as it stands when nothing has made one yet. */
+/* set_IR types 2 and 3 (PIP_rot.f90:148-228): get_Te_HD and get_Te_MHD rewrite both energies,
+ * then the Popescu et al. 2019 rates from the ion temperature Te_p and density, with the
+ * electron temperature Te_0 = T_norm/1.1604e4 eV.  The single-precision literals of the
+ * Fortran (1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) are rounded to float first, as there. */
+static void set_ir_popescu(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  double t_ir = p->t_ir, n6 = p->n_norm * (double)1.0e6f;
+  double Te_0 = p->t_norm / (double)1.1604e4f;
+  double c26 = (double)2.6e-19f, c291 = (double)2.91e-14f;
+  int law = p->flag_ir;
+  double rec2 = c26 * n6 / sqrt(Te_0) * t_ir;            /* type 2 rec_fac */
+  double rec3 = c26 * n6 / sqrt(Te_0);                   /* type 3 rec_fac */
+  double ioneq = (c26 / sqrt(Te_0)) /
+                 (c291 / (0.232 + 13.6 / Te_0) * pow(13.6 / Te_0, 0.39) * exp(-13.6 / Te_0));
+  double f_n = ioneq / (ioneq + 1.0), f_p = 1.0 - f_n, f_p_p = 2.0 * f_p / (f_n + 2.0 * f_p);
+  double tfac = (p->flag_col % 2 == 1) ? 0.5 * f_p_p / f_p
+                                       : p->beta / 2.0 * f_p_p * 5.0 / 6.0 / f_p;
+  const double *Um = c->U_m;
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < nc; ++q) {
+    double te_p, te_n;
+    get_te_cell(c, q, &te_p, &te_n);
+    double ro = Um[q];
+    if (law == PIP_IR_POPESCU) {
+      double a = 13.6 / Te_0 / te_p;
+      c->gm_rec[q] = ro / sqrt(te_p) * rec2;
+      c->gm_ion[q] = (n6 * ro) * c291 * exp(-13.6 / Te_0 / te_p) * pow(a, 0.39) / (0.232 + a) * t_ir;
+    } else {
+      double b = 13.6 / Te_0 / te_p * tfac;
+      c->gm_rec[q] = ro / sqrt(te_p) * t_ir / f_p * sqrt(tfac);
+      double g = c291 * n6 * ro * exp(-13.6 / Te_0 / te_p * tfac) * pow(b, 0.39);
+      c->gm_ion[q] = g / (0.232 + b) / rec3 / f_p * t_ir;
+    }
+  }
+}
+
+static int ir_per_stage(const orc_ctx *c) {
+  return c->p.flag_ir == PIP_IR_POPESCU || c->p.flag_ir == PIP_IR_POPESCU_EQ;
+}
+
+/* set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140), on the state as it
+ * stands, before the first call that reads the state: set_collisional (alpha_c per cell)
+ * and set_IR (the Popescu laws), each with get_Te's energy rewrite. */
 static void ensure_ac(orc_ctx *c) {
-  if (c->col_type >= 1 && !c->ac_valid) set_collisional(c);
+  if (c->init_done) return;
+  if (c->col_type >= 1) set_collisional(c);
+  if (ir_per_stage(c)) set_ir_popescu(c);
+  c->init_done = 1;
+}
+
+void orc_ir_rates(const orc_ctx *c, double *gm_ion, double *gm_rec) {
+  memcpy(gm_ion, c->gm_ion, sizeof(double) * c->nc);
+  memcpy(gm_rec, c->gm_rec, sizeof(double) * c->nc);
 }
 
 void orc_coefficients(orc_ctx *c) {
   if (c->col_type >= 1) set_collisional(c);
+  if (ir_per_stage(c)) set_ir_popescu(c);
+  c->init_done = 1;
 }
 
 int orc_alpha_c(orc_ctx *c, double *ac) {
@@ -869,6 +932,8 @@ void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m) {
   ensure_ac(c);
   memset(S_h, 0, sizeof(double) * nc * c->nh);
   memset(S_m, 0, sizeof(double) * nc * c->nm);
+  /* the Popescu rates of the state as given (set_IR before set_source) */
+  if (ir_per_stage(c)) set_ir_popescu(c);
   if (c->p.flag_pip_imp == 1) {
     /* report the U0 increments: run the form on zero U0 copies */
     source_pip(c, S_h, S_m, dt_coll, S_h, S_m);
@@ -892,10 +957,12 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
   int m0 = p->margin[0], m1 = p->margin[1], m2 = p->margin[2];
 
+  /* set_IR of the time loop before each cfl (main.f90:32-34,44-46), Popescu laws */
+  if (ir_per_stage(c)) set_ir_popescu(c);
   /* cfl_mhd */
   cq2pv_mhd(c, c->U_m, de, vx, vy, vz, pr, bx, by, bz);
   /* set_IR for the rates the following run_solver uses: from the rewritten ion state */
-  if (p->flag_ir != PIP_IR_NONE) set_ir_rates(c);
+  if (p->flag_ir == PIP_IR_POWERLAW) set_ir_rates(c);
   double dt_min = 10.0;
 #pragma omp parallel for collapse(2) reduction(min : dt_min) schedule(static)
   for (int k = m2; k < c->kx - m2; ++k)
@@ -1251,8 +1318,10 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   double *S_h = malloc(sizeof(double) * nc * nh), *S_m = malloc(sizeof(double) * nc * nm);
   double dt_coll[2] = {dt * 0.5, dt * 0.5};
   double dt_coll_i = dt_coll[t_order - istep];
-  /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_col >= 2 recomputes alpha_c */
+  /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_col >= 2 recomputes alpha_c,
+   * flag_IR >= 2 the rates (after it, :108-112) */
   if (c->col_type >= 1) set_collisional(c);
+  if (ir_per_stage(c)) set_ir_popescu(c);
   for (int dir = 1; dir <= p->ndim; ++dir)
     flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
   memset(S_h, 0, sizeof(double) * nc * nh);

@@ -47,10 +47,12 @@ void orc_set_neighbors(orc_ctx *c, const int nb[4]);
 void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m);
 /* PIP_rot.f90:1309-1429; returns S (explicit) or the U0 increments (exponential form). */
 void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m);
-/* set_coefficients (Solver_rot.f90:95-122) for the collision coefficient: with flag_col
- * 2..7, set_collisional (PIP_rot.f90:44-97) rewrites both energies and sets alpha_c per
- * cell; a no-op for flag_col 1. */
+/* set_coefficients (Solver_rot.f90:95-122): with flag_col 2..7, set_collisional
+ * (PIP_rot.f90:44-97) rewrites both energies and sets alpha_c per cell; with set_IR types 2
+ * and 3, set_IR (PIP_rot.f90:127-228) rewrites them again and sets the rates. */
 void orc_coefficients(orc_ctx *c);
+/* Gm_ion and Gm_rec of the last set_IR (nc values each). */
+void orc_ir_rates(const orc_ctx *c, double *gm_ion, double *gm_rec);
 /* alpha_c of every cell (col for flag_col 1), made from the current state when no
  * set_collisional has run yet (Initial_rot.f90:140). */
 int orc_alpha_c(orc_ctx *c, double *ac);

@@ -149,7 +149,12 @@ int validate(const pip_params *p) {
   if (p->flag_resi != 0 && p->flag_resi != 1) return PIP_ERR_PARAM;
   if (p->flag_resi == 1 && (p->precision != PIP_FP64 || p->flag_heat != 0)) return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
-  if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
+  if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW && p->flag_ir != PIP_IR_POPESCU &&
+      p->flag_ir != PIP_IR_POPESCU_EQ)
+    return PIP_ERR_PARAM;
+  if ((p->flag_ir == PIP_IR_POPESCU || p->flag_ir == PIP_IR_POPESCU_EQ) &&
+      (p->precision != PIP_FP64 || !(p->t_norm > 0.0) || !(p->n_norm > 0.0)))
+    return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
   if (p->precision != PIP_FP64 && p->precision != PIP_MIXED) return PIP_ERR_PARAM;
   if (p->flag_heat != 0 && p->flag_heat != 1) return PIP_ERR_PARAM;
@@ -169,6 +174,33 @@ int validate(const pip_params *p) {
   return PIP_OK;
 }
 
+// Constants of set_IR types 2 and 3 (PIP_rot.f90:148-228), with the Fortran's
+// single-precision literals (1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) rounded to float first.
+void popescu_constants(const pip_params &p, KParams &k) {
+  k.irs = (p.flag_ir == PIP_IR_POPESCU || p.flag_ir == PIP_IR_POPESCU_EQ) ? p.flag_ir : 0;
+  if (!k.irs) return;
+  const double te0 = p.t_norm / (double)1.1604e4f;
+  const double n6 = p.n_norm * (double)1.0e6f;
+  const double c26 = (double)2.6e-19f, c291 = (double)2.91e-14f;
+  k.ir_c136 = 13.6 / te0;
+  k.ir_n6 = n6;
+  k.ir_c291 = c291;
+  k.ir_c291n6 = c291 * n6;
+  k.ir_tir = p.t_ir;
+  if (k.irs == PIP_IR_POPESCU) {
+    k.ir_recfac = c26 * n6 / std::sqrt(te0) * p.t_ir;
+    return;
+  }
+  k.ir_recfac = c26 * n6 / std::sqrt(te0);
+  const double ioneq = (c26 / std::sqrt(te0)) /
+                       (c291 / (0.232 + 13.6 / te0) * std::pow(13.6 / te0, 0.39) * std::exp(-13.6 / te0));
+  const double f_n = ioneq / (ioneq + 1.0), f_p = 1.0 - f_n;
+  const double f_p_p = 2.0 * f_p / (f_n + 2.0 * f_p);
+  k.ir_fp = f_p;
+  k.ir_tfac = (p.flag_col % 2 == 1) ? 0.5 * f_p_p / f_p : p.beta / 2.0 * f_p_p * 5.0 / 6.0 / f_p;
+  k.ir_sqtfac = std::sqrt(k.ir_tfac);
+}
+
 void build_kparams(pip_ctx *c) {
   const pip_params &p = c->p;
   KParams &k = c->kp;
@@ -181,8 +213,9 @@ void build_kparams(pip_ctx *c) {
   k.ny = p.ndim == 2 ? p.jx - 2 * k.m1 : 1;
   k.nvm = p.nvar_m;
   k.imp = p.flag_pip_imp;
-  k.ir = p.flag_ir == PIP_IR_POWERLAW;
+  k.ir = p.flag_ir != PIP_IR_NONE;
   k.ir_type = p.flag_ir_type;
+  popescu_constants(p, k);
   k.nc = (long long)p.ix * p.jx;
   k.gm = p.gm;
   k.igm1 = 1.0 / (p.gm - 1.0);
@@ -248,8 +281,9 @@ void pip::record_cuda_error(int code) { g_last_cuda_error = code; }
 int pip::kparams_from_params(const pip_params *p, KParams *k) {
   const int st = validate(p);
   if (st != PIP_OK) return st;
-  // the per-cell alpha_c and eta fields live in a context
+  // the per-cell alpha_c and eta fields and the per-stage rates live in a context
   if (p->flag_col != 1 || p->flag_resi != 0) return PIP_ERR_PARAM;
+  if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW) return PIP_ERR_PARAM;
   *k = KParams{};
   k->resi_dt = INFINITY;
   k->ndim = p->ndim;
@@ -261,7 +295,7 @@ int pip::kparams_from_params(const pip_params *p, KParams *k) {
   k->ny = p->ndim == 2 ? p->jx - 2 * k->m1 : 1;
   k->nvm = p->nvar_m;
   k->imp = p->flag_pip_imp;
-  k->ir = p->flag_ir == PIP_IR_POWERLAW;
+  k->ir = p->flag_ir != PIP_IR_NONE;
   k->ir_type = p->flag_ir_type;
   k->nc = (long long)p->ix * p->jx;
   k->gm = p->gm;
@@ -367,7 +401,7 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
 // set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140) rewrites the energies
 // and sets alpha_c before the first cfl and the first stage.
 int ensure_ac(pip_ctx *c) {
-  if (!c->kp.col_type || c->ac_valid) return PIP_OK;
+  if ((!c->kp.col_type && !c->kp.irs) || c->ac_valid) return PIP_OK;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   c->ac_valid = true;
   return PIP_OK;
@@ -804,7 +838,7 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
 }
 
 int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
-  const int64_t init = c && c->kp.col_type && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
+  const int64_t init = c && (c->kp.col_type || c->kp.irs) && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
   return init + 1 + 2 * (nsteps > 0 ? nsteps : 0);
 }
 
@@ -854,7 +888,7 @@ int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
 int pip_coefficients(pip_ctx *c) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
-  if (!c->kp.col_type) return PIP_OK;
+  if (!c->kp.col_type && !c->kp.irs) return PIP_OK;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   CK(cudaStreamSynchronize(c->stream));

@@ -18,7 +18,8 @@ struct KParams {
   int m0, m1;        // ghost layers in x and y
   int nvm;           // ion planes (8 or 9); neutral planes follow
   int imp;           // exponential collision form
-  int ir;            // PIP_IR_POWERLAW active
+  int ir;            // an ionisation/recombination law is active (IR source and cfl bound)
+  int irs;           // 2 or 3: set_IR's Popescu law, rates from every stage's state (FP64 form)
   int ir_type;       // IR energy form 1 or 2
   long long nc;      // ix*jx
   double gm, ro_lim, pr_lim, ac, safety;
@@ -34,6 +35,8 @@ struct KParams {
   int col_type;      // set_collisional col_type: 0 constant alpha_c, 1..6 per cell (FP64 form)
   double ac_b2g;     // beta/2*gm of col_type 1, 3, 5
   double ac_sb;      // sqrt(beta/2*gm)
+  double ir_c136, ir_n6, ir_c291, ir_c291n6;  // 13.6/Te_0, n_norm*1e6, 2.91e-14, their product
+  double ir_recfac, ir_fp, ir_tfac, ir_sqtfac, ir_tir;  // rec_fac, f_p, tfac, sqrt(tfac), t_ir
   double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
   int resi;          // flag_resi 1: resistive flux (eta field etaf), FP64 form
   const double *etaf;  // eta per cell, nc values

@@ -185,6 +185,33 @@ __device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double
   return rdiv(a, pow(radd(rmul(T, 0.5), w), 0.125));
 }
 
+// set_IR types 2 and 3 (PIP_rot.f90:148-228) for one cell from the ion density ro and the
+// temperature te of get_Te_MHD, in the Fortran operation order (constants from the host).
+__device__ __forceinline__ void popescu_rates(const KParams &p, double ro, double te, double &gr,
+                                              double &gi) {
+  if (p.irs == 2) {
+    const double a = rdiv(p.ir_c136, te);
+    gr = rmul(rdiv(ro, __dsqrt_rn(te)), p.ir_recfac);
+    gi = rmul(rdiv(rmul(rmul(rmul(rmul(p.ir_n6, ro), p.ir_c291), exp(-a)), pow(a, 0.39)),
+                   radd(0.232, a)),
+              p.ir_tir);
+  } else {
+    const double b = rmul(rdiv(p.ir_c136, te), p.ir_tfac);
+    gr = rmul(rdiv(rmul(rdiv(ro, __dsqrt_rn(te)), p.ir_tir), p.ir_fp), p.ir_sqtfac);
+    const double g = rmul(rmul(rmul(p.ir_c291n6, ro), exp(-b)), pow(b, 0.39));
+    gi = rmul(rdiv(rdiv(rdiv(g, radd(0.232, b)), p.ir_recfac), p.ir_fp), p.ir_tir);
+  }
+}
+
+// set_IR of a Popescu law on one cell: get_Te's energy rewrite, then the rates.
+template <int NVM>
+__device__ __forceinline__ void set_ir_cell(double (&um)[NVM], double (&uh)[5], const KParams &p,
+                                            double &gr, double &gi) {
+  double te_m, te_h, rm, rh;
+  get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+  popescu_rates(p, um[0], te_m, gr, gi);
+}
+
 // Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
 // rewritten states um/uh, their primitives and the cell's alpha_c.
 template <int NVM>
@@ -452,8 +479,9 @@ __device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ 
 // calls that follow run_solver and open the next step (main.f90:47 and :36): epi = 1
 // applies one cq2pv rewrite; epi = 2 applies two and reduces the next dt; epi = -1 takes
 // 1 or 2 from the control block's last-step flag.  X selects the extra physics of the
-// instance: bit 0 alpha_c per cell (col_type >= 1), bit 1 resistivity; each combination is
-// its own instance so that the others keep their register budget.
+// instance: bit 0 set_coefficients at every stage (alpha_c per cell, col_type >= 1, and/or
+// the Popescu IR rates), bit 1 resistivity; each combination is its own instance so that
+// the others keep their register budget.
 template <int NDIM, int NVM, int STAGE, int X>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
 stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
@@ -537,9 +565,11 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     double um[NVM], uh[5], vm[NVM], vh[5];
     load_cell<NVM>(Us, (long long)gj * p.ix + gi, nc, um, uh);
     if (COL) {
-      // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux
+      // set_coefficients (Solver_rot.f90:62) rewrites the energies before set_flux: in
+      // set_collisional and again in set_IR
       double te_m, te_h, rm, rh;
-      get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+      if (p.col_type) get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+      if (p.irs) get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
     }
     u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
     u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
@@ -688,9 +718,10 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     }
     // alpha_c of the stage (set_coefficients at the stage start; U0 keeps its energies)
     double ac_s = p.ac;
-    if (COL) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
+    if (COL && p.col_type) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
     double gr = 0.0, gion = 0.0;
-    if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
+    if (COL && p.irs) set_ir_cell<NVM>(s_m, s_h, p, gr, gion);  // set_IR of the stage
+    else if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
 
     // exponential form: U0 carries the collision increments of the earlier stages
     if (p.imp && STAGE == 2) {
@@ -700,7 +731,11 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
 #pragma unroll
       for (int n = 0; n < 5; ++n) r_h[n] = a_h[n];
       double ac_r = p.ac;
-      if (COL) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
+      if (COL && p.col_type) ac_r = set_collisional_cell<NVM>(r_m, r_h, p);
+      if (COL && p.irs) {
+        double g1, g2;
+        set_ir_cell<NVM>(r_m, r_h, p, g1, g2);
+      }
       const Prim<double> qh = rt_hd(r_h, p);
       const Prim<double> qm = rt_mhd<NVM>(r_m, p);
       collision_ds<NVM>(r_m, r_h, qm, qh, p, ac_r, dt_coll, ds);
@@ -763,12 +798,21 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     // fused cfl rewrites (and the next step's CFL terms)
     const int ep = STAGE == 1 ? 0 : s_epi;  // stage 1 is never followed by a cfl
     if (ep >= 1) {
+      if (COL && p.irs) {  // the time loop's set_IR before the cfl (main.f90:44-46)
+        double g1, g2;
+        set_ir_cell<NVM>(n_m, n_h, p, g1, g2);
+      }
       const Prim<double> qm = rt_mhd<NVM>(n_m, p);
       const Prim<double> qh = rt_hd(n_h, p);
       (void)qm;
       (void)qh;
     }
     if (ep == 2) {
+      if (COL && p.irs) {  // the next step's set_IR (main.f90:32-34): cfl_pip_ir's rates
+        double g1, g2;
+        set_ir_cell<NVM>(n_m, n_h, p, g1, g2);
+        grc = fmax(g1, g2);
+      }
       const Prim<double> qm = rt_mhd<NVM>(n_m, p);
       const Prim<double> qh = rt_hd(n_h, p);
       const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
@@ -776,7 +820,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       dtc = fmin(cfl_mhd_cell<double>(qm, n_m[5], n_m[6], n_m[7], gm, sg),
                  cfl_hd_cell<double>(qh, gm, sg));
       rhoc = fmax(n_m[0] * ac_s, n_h[0] * ac_s);
-      if (p.ir) {
+      if (p.ir && !p.irs) {
         double g1, g2;
         ir_rates<NVM>(n_m, p, g1, g2);
         grc = fmax(g1, g2);
@@ -789,13 +833,13 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) bad |= !isfinite(n_h[n]);
     if (bad) atomicOr(&ctrl->nan_flag, 1);
     store_cell<NDIM, NVM>(Uo, p, gi, gj, n_m, n_h);
-    if (STAGE == 2 && COL) {
+    if (STAGE == 2 && COL && p.col_type) {
       // the alpha_c field that the next cfl reads (cfl_pn_col, Scheme_rot.f90:305-313)
       p.acf[q] = ac_s;
       if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
     }
   }
-  if (STAGE == 2 && COL) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
+  if (STAGE == 2 && COL && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
   if (STAGE == 2 && s_epi == 2) {
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   }
@@ -833,6 +877,8 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
+    double gp1 = 0.0, gp2 = 0.0;
+    if (p.irs) set_ir_cell<NVM>(um, uh, p, gp1, gp2);  // the time loop's set_IR before cfl
     const Prim<double> qm = rt_mhd<NVM>(um, p);
     const Prim<double> qh = rt_hd(uh, p);
 #pragma unroll
@@ -853,7 +899,9 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
       const double a = p.acf[q];
       rhoc = fmax(rhoc, fmax(um[0] * a, uh[0] * a));
     }
-    if (p.ir) {
+    if (p.irs) {
+      grc = fmax(grc, fmax(gp1, gp2));
+    } else if (p.ir) {
       double g1, g2;
       ir_rates<NVM>(um, p, g1, g2);
       grc = fmax(grc, fmax(g1, g2));
@@ -982,7 +1030,8 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
     double gr = 0.0, gion = 0.0;
-    if (p.ir) ir_rates<NVM>(um, p, gr, gion);
+    if (p.irs) set_ir_cell<NVM>(um, uh, p, gr, gion);  // the rates of the state as given
+    else if (p.ir) ir_rates<NVM>(um, p, gr, gion);
     const Prim<double> qh = rt_hd(uh, p);
     const Prim<double> qm = rt_mhd<NVM>(um, p);
     double ds[5], sm[5], sh[5];
@@ -1022,7 +1071,11 @@ __global__ void coefficients_kernel(const KParams p, double *U) {
        q += (long long)gridDim.x * blockDim.x) {
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
-    p.acf[q] = set_collisional_cell<NVM>(um, uh, p);
+    if (p.col_type) p.acf[q] = set_collisional_cell<NVM>(um, uh, p);
+    if (p.irs) {
+      double g1, g2;
+      set_ir_cell<NVM>(um, uh, p, g1, g2);
+    }
     U[q + 4 * nc] = um[4];
     U[q + (NVM + 4) * nc] = uh[4];
   }
@@ -1080,7 +1133,7 @@ static cudaError_t launch_stage_t(const KParams &p, const double *Us, const doub
                                   DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
-  switch ((p.col_type ? 1 : 0) | (p.resi ? 2 : 0)) {
+  switch ((p.col_type || p.irs ? 1 : 0) | (p.resi ? 2 : 0)) {
     case 0:
       stage_kernel<NDIM, NVM, STAGE, 0><<<grid, NT, stage_smem_bytes<NDIM, NVM, 0>(), s>>>(
           p, Us, U0, Uo, ctrl, dt_mode, epi);
@@ -1152,7 +1205,7 @@ static cudaError_t launch_source(const KParams &p, double *U, double *S, double 
 }
 
 static cudaError_t launch_coefficients(const KParams &p, double *U, cudaStream_t s) {
-  if (!p.col_type) return cudaSuccess;
+  if (!p.col_type && !p.irs) return cudaSuccess;
   if (p.nvm == 9) coefficients_kernel<9><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   else coefficients_kernel<8><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   return cudaGetLastError();

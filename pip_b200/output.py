@@ -34,7 +34,7 @@ from typing import Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
-from .params import PIP_IR_NONE, Settings
+from .params import PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, Settings
 
 VAR_M = ("ro_p", "mx_p", "my_p", "mz_p", "en_p", "bx", "by", "bz", "ps")
 VAR_H = ("ro_n", "mx_n", "my_n", "mz_n", "en_n")
@@ -73,14 +73,35 @@ def layout(s: Settings, global_shape: Tuple[int, int, int]):
 
 
 def ir_rates(s: Settings, U_m: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
-    """Gm_ion, Gm_rec of PIP_IR_POWERLAW from the ion state (the rates the step uses: the
-    pressure of get_Pr_MHD with its floor, the temperature of get_Te_MHD)."""
+    """Gm_ion, Gm_rec from the ion state: the temperature of get_Te_MHD (get_Pr_MHD's
+    pressure with its floor), then PIP_IR_POWERLAW or set_IR type 2 or 3 (PIP_rot.f90:148-228;
+    the Fortran's single-precision literals rounded to float)."""
     gm = s.gm
     u = U_m
     pr = (gm - 1.0) * (u[4] - 0.5 * ((u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] +
                                      u[5] * u[5] + u[6] * u[6] + u[7] * u[7]))
     pr = np.maximum(pr, s.pr_lim)
     te = 0.5 * gm * (pr / u[0])
+    if s.flag_ir in (PIP_IR_POPESCU, PIP_IR_POPESCU_EQ):
+        f32 = lambda x: float(np.float32(x))
+        te0 = s.t_norm / f32(1.1604e4)
+        n6 = s.n_norm * f32(1.0e6)
+        c26, c291 = f32(2.6e-19), f32(2.91e-14)
+        if s.flag_ir == PIP_IR_POPESCU:
+            a = 13.6 / te0 / te
+            rec = u[0] / np.sqrt(te) * (c26 * n6 / np.sqrt(te0) * s.t_ir)
+            ion = (n6 * u[0]) * c291 * np.exp(-a) * a ** 0.39 / (0.232 + a) * s.t_ir
+            return ion, rec
+        ioneq = (c26 / np.sqrt(te0)) / (c291 / (0.232 + 13.6 / te0) * (13.6 / te0) ** 0.39 *
+                                         np.exp(-13.6 / te0))
+        f_n = ioneq / (ioneq + 1.0)
+        f_p = 1.0 - f_n
+        f_p_p = 2.0 * f_p / (f_n + 2.0 * f_p)
+        tfac = 0.5 * f_p_p / f_p if s.flag_col % 2 == 1 else s.beta / 2.0 * f_p_p * 5.0 / 6.0 / f_p
+        b = 13.6 / te0 / te * tfac
+        rec = u[0] / np.sqrt(te) * s.t_ir / f_p * np.sqrt(tfac)
+        ion = c291 * n6 * u[0] * np.exp(-b) * b ** 0.39 / (0.232 + b) / (c26 * n6 / np.sqrt(te0)) / f_p * s.t_ir
+        return ion, rec
     rs = 1.0 / np.sqrt(te)
     return s.ir_ion_coef * rs * np.exp(-s.ir_chi / te), s.ir_rec_coef * rs
 

@@ -18,6 +18,8 @@ PIP_ABI_VERSION = 1
 PIP_FP64 = 0
 PIP_MIXED = 1
 PIP_IR_NONE = 0
+PIP_IR_POPESCU = 2              # set_IR type 2 (PIP_rot.f90:148-170)
+PIP_IR_POPESCU_EQ = 3           # set_IR type 3 (PIP_rot.f90:173-228)
 PIP_IR_POWERLAW = 5
 
 # boundary codes the C ABI accepts (boundary_control types 1, 2 and 10, and the codes
@@ -69,7 +71,9 @@ class PipParams(ctypes.Structure):
         ("hc_error", ctypes.c_double),
         ("beta", ctypes.c_double),
         ("eta_0", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 5),
+        ("t_norm", ctypes.c_double),
+        ("n_norm", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 3),
         ("dx", ctypes.POINTER(ctypes.c_double)),
         ("dy", ctypes.POINTER(ctypes.c_double)),
         ("dz", ctypes.POINTER(ctypes.c_double)),
@@ -131,6 +135,8 @@ class Settings:
     hc_error: float = 1.0e-10
     flag_resi: int = 0          # 10*resi_type + 1 (Res_rot.f90:8-15): 1 uniform, 11 localised
     eta_0: float = 0.0
+    t_norm: float = 0.0         # setting key T_norm (K)
+    n_norm: float = 0.0         # setting key n_norm
     debug_parameter: float = 0.0
     flag_amb: int = 0
     flag_visc: int = 0
@@ -250,8 +256,13 @@ class Settings:
             bad.append("resistivity needs precision PIP_FP64 and no conduction")
         if self.flag_amb or self.flag_visc or self.flag_grav:
             bad.append("ambipolar diffusion, viscosity and gravity are not supported")
-        if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW):
-            bad.append("flag_ir must be 0 or %d" % PIP_IR_POWERLAW)
+        if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_IR_POWERLAW):
+            bad.append("flag_ir must be 0, 2, 3 (set_IR types 2, 3) or %d" % PIP_IR_POWERLAW)
+        elif self.flag_ir in (PIP_IR_POPESCU, PIP_IR_POPESCU_EQ):
+            if not (self.t_norm > 0.0 and self.n_norm > 0.0):
+                bad.append("set_IR types 2 and 3 need T_norm > 0 and n_norm > 0")
+            if self.precision != PIP_FP64:
+                bad.append("set_IR types 2 and 3 need precision PIP_FP64")
         if self.flag_ir and self.flag_ir_type not in (1, 2):
             bad.append("flag_ir_type must be 1 or 2")
         for f in range(2 * self.ndim):
@@ -308,6 +319,8 @@ class Settings:
         p.beta = self.beta
         p.flag_resi = self.flag_resi % 10
         p.eta_0 = self.eta_0
+        p.t_norm = self.t_norm
+        p.n_norm = self.n_norm
         dptr = ctypes.POINTER(ctypes.c_double)
         p.dx = dx.ctypes.data_as(dptr)
         p.dy = dy.ctypes.data_as(dptr)
@@ -330,7 +343,7 @@ class Settings:
                  "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
                  "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",
                  "kapper": "kapper", "tend": "tend", "beta": "beta", "eta_0": "eta_0",
-                 "debug_parameter": "debug_parameter"}
+                 "debug_parameter": "debug_parameter", "T_norm": "t_norm", "n_norm": "n_norm"}
         bnd = {"flag_bnd_x_l": 0, "flag_bnd_x_r": 1, "flag_bnd_y_l": 2, "flag_bnd_y_r": 3,
                "flag_bnd_z_l": 4, "flag_bnd_z_r": 5}
         for raw in text.splitlines():

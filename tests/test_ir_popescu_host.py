@@ -1,0 +1,118 @@
+"""set_IR types 2 and 3 (Popescu et al. 2019 rates, PIP_rot.f90:148-228) in the oracle, on
+the CPU: the rates after set_coefficients against a vectorised restatement written from the
+Fortran (its single-precision literals rounded to float), the energy rewrite of get_Te, the
+cfl bound and a decomposed run."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle_block import OracleBlock
+from pip_b200 import decomp, ics, output
+from pip_b200.params import PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_MIXED, Settings
+
+
+def case(law, **kw):
+    return ics.kelvin_helmholtz(32, 16, flag_ir=law, t_norm=1.5e4, n_norm=1.0e11, t_ir=10.0, **kw)
+
+
+def literal_rates(s, U_m):
+    """Gm_ion, Gm_rec of set_IR type 2 or 3 after get_Te_MHD, whole-array, Fortran order."""
+    gm = s.gm
+    m2 = U_m[1] * U_m[1] + U_m[2] * U_m[2] + U_m[3] * U_m[3]
+    pr = (gm - 1.0) * (U_m[4] - 0.5 * ((m2 / U_m[0] + U_m[5] * U_m[5]) + U_m[6] * U_m[6]
+                                       + U_m[7] * U_m[7]))
+    if pr.min() <= s.pr_lim:
+        pr = np.maximum(pr, s.pr_lim)
+    Te_p = 0.5 * gm * (pr / U_m[0])
+    T0, n0, t_ir = s.t_norm, s.n_norm, s.t_ir
+    r = lambda x: float(np.float32(x))                  # a REAL*4 literal
+    Te_0 = T0 / r(1.1604e4)
+    if s.flag_ir == PIP_IR_POPESCU:
+        rec_fac = r(2.6e-19) * (n0 * r(1.0e6)) / np.sqrt(Te_0) * t_ir
+        Gm_rec = U_m[0] / np.sqrt(Te_p) * rec_fac
+        Gm_ion = ((n0 * r(1.0e6) * U_m[0]) * r(2.91e-14) * np.exp(-13.6 / Te_0 / Te_p)
+                  * (13.6 / Te_0 / Te_p) ** 0.39 / (0.232 + 13.6 / Te_0 / Te_p) * t_ir)
+        return Gm_ion, Gm_rec
+    rec_fac = r(2.6e-19) * (n0 * r(1.0e6)) / np.sqrt(Te_0)
+    ioneq = (r(2.6e-19) / np.sqrt(Te_0)) / (r(2.91e-14) / (0.232 + 13.6 / Te_0)
+                                             * (13.6 / Te_0) ** 0.39 * np.exp(-13.6 / Te_0))
+    f_n = ioneq / (ioneq + 1.0)
+    f_p = 1.0 - f_n
+    f_p_p = 2.0 * f_p / (f_n + 2.0 * f_p)
+    if s.flag_col % 2 == 1:
+        tfac = 0.5 * f_p_p / f_p
+    else:
+        tfac = s.beta / 2.0 * f_p_p * 5.0 / 6.0 / f_p
+    Gm_rec = U_m[0] / np.sqrt(Te_p) * t_ir / f_p * np.sqrt(tfac)
+    Gm_ion = (r(2.91e-14) * (n0 * r(1.0e6)) * U_m[0] * np.exp(-13.6 / Te_0 / Te_p * tfac)
+              * (13.6 / Te_0 / Te_p * tfac) ** 0.39)
+    Gm_ion = Gm_ion / (0.232 + 13.6 / Te_0 / Te_p * tfac) / rec_fac / f_p * t_ir
+    return Gm_ion, Gm_rec
+
+
+@pytest.mark.parametrize("law,flag_col", [(PIP_IR_POPESCU, 1), (PIP_IR_POPESCU_EQ, 1),
+                                          (PIP_IR_POPESCU_EQ, 4)])
+def test_rates_match_the_literal_restatement(law, flag_col):
+    s, Uh, Um = case(law, flag_col=flag_col)
+    o = O.Oracle(s, Uh, Um)
+    try:
+        o.coefficients()
+        ion, rec = o.ir_rates()
+        oh, om = o.state()
+    finally:
+        o.close()
+    want_ion, want_rec = literal_rates(s, Um)
+    assert np.all(rec > 0.0) and np.all(ion > 0.0)
+    # exp and x**0.39 of numpy against libm: a few ulp
+    np.testing.assert_allclose(rec, want_rec, rtol=1e-15, atol=0.0)
+    np.testing.assert_allclose(ion, want_ion, rtol=1e-14, atol=0.0)
+    # the output writer's rates are these (from the state the rates were taken from)
+    w_ion, w_rec = output.ir_rates(s, om)
+    np.testing.assert_allclose(w_rec, rec, rtol=1e-15, atol=0.0)
+    np.testing.assert_allclose(w_ion, ion, rtol=1e-14, atol=0.0)
+    # get_Te rewrote the energies only
+    np.testing.assert_array_equal(om[[0, 1, 2, 3, 5, 6, 7]], Um[[0, 1, 2, 3, 5, 6, 7]])
+    np.testing.assert_allclose(om[4], Um[4], rtol=1e-14)
+
+
+def test_cfl_bound_and_run():
+    s, Uh, Um = case(PIP_IR_POPESCU_EQ)
+    o = O.Oracle(s, Uh, Um)
+    try:
+        dt, _ = o.cfl()
+        ion, rec = o.ir_rates()
+        bound = min(s.safety, 0.1) / max(ion.max(), rec.max(), 1e-5)
+        assert dt <= bound * (1 + 1e-15)
+        st, t, n, _ = o.run(nsteps=20)
+        assert st == 0 and n == 20 and not o.has_nan()
+    finally:
+        o.close()
+
+
+@pytest.mark.parametrize("law", [PIP_IR_POPESCU, PIP_IR_POPESCU_EQ])
+def test_blocks_match_single_domain(law):
+    s, Uh, Um = case(law, flag_col=5)
+    o = O.Oracle(s, Uh, Um)
+    st, t, n, hist = o.run(nsteps=5, max_hist=5)
+    oh, om = o.state()
+    o.close()
+    engines = [OracleBlock(decomp.block_of(s, 2, r), decomp.scatter(s, Uh, 2, r),
+                           decomp.scatter(s, Um, 2, r)) for r in range(2)]
+    run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
+    assert run.run(5) == 0
+    states = [e.download() for e in engines]
+    run.close()
+    assert np.array_equal(np.array(run.dt_history), hist)
+    assert np.array_equal(decomp.gather(s, [a for a, _ in states]), oh)
+    assert np.array_equal(decomp.gather(s, [b for _, b in states]), om)
+
+
+def test_settings():
+    with pytest.raises(ValueError, match="T_norm"):
+        Settings(flag_ir=3).validate()
+    with pytest.raises(ValueError, match="PIP_FP64"):
+        Settings(flag_ir=2, t_norm=1e4, n_norm=1e11, precision=PIP_MIXED).validate()
+    s = Settings.from_setting_text("3:flag_IR;\n1.5d4:T_norm;\n1d11:n_norm;\n")
+    assert (s.flag_ir, s.t_norm, s.n_norm) == (3, 1.5e4, 1e11)
+    p, _ = s.to_params()
+    assert p.t_norm == 1.5e4 and p.n_norm == 1e11
