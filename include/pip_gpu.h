@@ -68,7 +68,8 @@ enum pip_ir_law {
  *   flag_eqs=PIP (two-fluid), flag_sch=0, flag_hll=2, s_order=2, t_order=2, flag_time=0,
  *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col 1..7 (2..7 with
  *   precision PIP_FP64 only),
- *   flag_pip_imp 0/1, flag_ir 0 or PIP_IR_POWERLAW with flag_ir_type 1 or 2,
+ *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ (FP64 form; T_norm and
+ *   n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type 1 or 2,
  *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0/1 (a fixed eta field; FP64 form, not
  *   with flag_heat), no viscosity/gravity/ambipolar diffusion.
  */
