@@ -46,6 +46,10 @@ enum pip_precision {
 /* Ionisation/recombination laws accepted in pip_params.flag_ir. */
 enum pip_ir_law {
   PIP_IR_NONE = 0,
+  /* set_IR type 1 (PIP_rot.f90:135-149, marked work in progress there): rates from T_norm,
+   * n_norm and t_ir; computed by the time loop's set_IR before each cfl (main.f90:32-34,44-46)
+   * and at the prologue, after get_Te's energy rewrite, and frozen over the step. */
+  PIP_IR_JEFFERY = 1,
   /* set_IR type 2 (PIP_rot.f90:148-170): Popescu et al. 2019 empirical rates with the
    * electron temperature T_norm/1.1604e4 eV and n_norm; recomputed with set_coefficients at
    * every RK stage (Solver_rot.f90:111) and before each cfl (main.f90:32-34,44-46), each time
@@ -68,8 +72,8 @@ enum pip_ir_law {
  *   flag_eqs=PIP (two-fluid), flag_sch=0, flag_hll=2, s_order=2, t_order=2, flag_time=0,
  *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col 1..7 (2..7 with
  *   precision PIP_FP64 only),
- *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ (FP64 form; T_norm and
- *   n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type 1 or 2,
+ *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ (FP64
+ *   form; T_norm and n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type 1 or 2,
  *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0/1 (a fixed eta field; FP64 form, not
  *   with flag_heat), no viscosity/gravity/ambipolar diffusion.
  */

@@ -780,13 +780,32 @@ static void set_collisional(orc_ctx *c) {
   }
 }
 
-/* set_IR types 2 and 3 (PIP_rot.f90:148-228): get_Te_HD and get_Te_MHD rewrite both energies,
- * then the Popescu et al. 2019 rates from the ion temperature Te_p and density, with the
- * electron temperature Te_0 = T_norm/1.1604e4 eV.  The single-precision literals of the
- * Fortran (1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) are rounded to float first, as there. */
+/* set_IR types 1, 2 and 3 (PIP_rot.f90:134-228): get_Te_HD and get_Te_MHD rewrite both
+ * energies, then the rates from the ion temperature Te_p and density.  Type 1 (the Jeffery
+ * formulation, :135-149) from T_norm and n_norm; types 2 and 3 the Popescu et al. 2019 rates
+ * with the electron temperature Te_0 = T_norm/1.1604e4 eV.  The single-precision literals of
+ * the Fortran (2.7, 5.6e-16, 1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) are rounded to float first,
+ * as there. */
 static void set_ir_popescu(orc_ctx *c) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
+  if (p->flag_ir == PIP_IR_JEFFERY) {
+    double T0 = p->t_norm, n0 = p->n_norm;
+    double factor = exp(-13.2 / (T0 / 11605.0));
+    double factor2 = (double)2.7f * pow(13.2 * 11605.0, -2.0) * pow(T0, 1.0 / 2.0) * n0;
+    double factor3 = (double)5.6e-16f * pow(13.2 * 11605.0, -2.0) * pow(T0, -1.0) * pow(n0, 2.0);
+    double rec_fac = factor2 / factor3, ion_fac = factor3 / p->t_ir;
+    const double *Um1 = c->U_m;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < nc; ++q) {
+      double te_p, te_n;
+      get_te_cell(c, q, &te_p, &te_n);
+      double ro = Um1[q];
+      c->gm_rec[q] = pow(te_p, -0.5) * (ro * ro) * rec_fac * ion_fac;
+      c->gm_ion[q] = pow(te_p, 0.5) * ro * pow(factor, 1.0 / te_p) * ion_fac;
+    }
+    return;
+  }
   double t_ir = p->t_ir, n6 = p->n_norm * (double)1.0e6f;
   double Te_0 = p->t_norm / (double)1.1604e4f;
   double c26 = (double)2.6e-19f, c291 = (double)2.91e-14f;
@@ -821,13 +840,18 @@ static int ir_per_stage(const orc_ctx *c) {
   return c->p.flag_ir == PIP_IR_POPESCU || c->p.flag_ir == PIP_IR_POPESCU_EQ;
 }
 
+/* set_IR types 1-3: called by the time loop before each cfl and at the prologue */
+static int ir_loop(const orc_ctx *c) {
+  return ir_per_stage(c) || c->p.flag_ir == PIP_IR_JEFFERY;
+}
+
 /* set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140), on the state as it
  * stands, before the first call that reads the state: set_collisional (alpha_c per cell)
  * and set_IR (the Popescu laws), each with get_Te's energy rewrite. */
 static void ensure_ac(orc_ctx *c) {
   if (c->init_done) return;
   if (c->col_type >= 1) set_collisional(c);
-  if (ir_per_stage(c)) set_ir_popescu(c);
+  if (ir_loop(c)) set_ir_popescu(c);
   c->init_done = 1;
 }
 
@@ -838,7 +862,7 @@ void orc_ir_rates(const orc_ctx *c, double *gm_ion, double *gm_rec) {
 
 void orc_coefficients(orc_ctx *c) {
   if (c->col_type >= 1) set_collisional(c);
-  if (ir_per_stage(c)) set_ir_popescu(c);
+  if (ir_loop(c)) set_ir_popescu(c);
   c->init_done = 1;
 }
 
@@ -957,8 +981,8 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
   int m0 = p->margin[0], m1 = p->margin[1], m2 = p->margin[2];
 
-  /* set_IR of the time loop before each cfl (main.f90:32-34,44-46), Popescu laws */
-  if (ir_per_stage(c)) set_ir_popescu(c);
+  /* set_IR of the time loop before each cfl (main.f90:32-34,44-46), set_IR types 1-3 */
+  if (ir_loop(c)) set_ir_popescu(c);
   /* cfl_mhd */
   cq2pv_mhd(c, c->U_m, de, vx, vy, vz, pr, bx, by, bz);
   /* set_IR for the rates the following run_solver uses: from the rewritten ion state */

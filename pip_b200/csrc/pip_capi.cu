@@ -50,6 +50,7 @@ struct pip_ctx {
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
   double *etaf = nullptr;             // eta per cell (flag_resi 1)
   bool ac_valid = false;              // acf holds the last set_collisional's field
+  double *irg = nullptr;              // set_IR type 1's rates (2 planes)
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
   size_t plane_bytes() const { return sizeof(double) * (size_t)kp.nc; }
@@ -150,9 +151,10 @@ int validate(const pip_params *p) {
   if (p->flag_resi == 1 && (p->precision != PIP_FP64 || p->flag_heat != 0)) return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW && p->flag_ir != PIP_IR_POPESCU &&
-      p->flag_ir != PIP_IR_POPESCU_EQ)
+      p->flag_ir != PIP_IR_POPESCU_EQ && p->flag_ir != PIP_IR_JEFFERY)
     return PIP_ERR_PARAM;
-  if ((p->flag_ir == PIP_IR_POPESCU || p->flag_ir == PIP_IR_POPESCU_EQ) &&
+  if ((p->flag_ir == PIP_IR_POPESCU || p->flag_ir == PIP_IR_POPESCU_EQ ||
+       p->flag_ir == PIP_IR_JEFFERY) &&
       (p->precision != PIP_FP64 || !(p->t_norm > 0.0) || !(p->n_norm > 0.0)))
     return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
@@ -178,6 +180,19 @@ int validate(const pip_params *p) {
 // single-precision literals (1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) rounded to float first.
 void popescu_constants(const pip_params &p, KParams &k) {
   k.irs = (p.flag_ir == PIP_IR_POPESCU || p.flag_ir == PIP_IR_POPESCU_EQ) ? p.flag_ir : 0;
+  k.irf = p.flag_ir == PIP_IR_JEFFERY ? 1 : 0;
+  k.irl = k.irs || k.irf ? 1 : 0;
+  if (k.irf) {
+    // set_IR type 1 (PIP_rot.f90:135-149)
+    const double T0 = p.t_norm, n0 = p.n_norm;
+    k.ir_factor = std::exp(-13.2 / (T0 / 11605.0));
+    const double f2 = (double)2.7f * std::pow(13.2 * 11605.0, -2.0) * std::pow(T0, 1.0 / 2.0) * n0;
+    const double f3 = (double)5.6e-16f * std::pow(13.2 * 11605.0, -2.0) * std::pow(T0, -1.0) *
+                      std::pow(n0, 2.0);
+    k.ir_recfac = f2 / f3;
+    k.ir_ionfac = f3 / p.t_ir;
+    return;
+  }
   if (!k.irs) return;
   const double te0 = p.t_norm / (double)1.1604e4f;
   const double n6 = p.n_norm * (double)1.0e6f;
@@ -401,7 +416,7 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
 // set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140) rewrites the energies
 // and sets alpha_c before the first cfl and the first stage.
 int ensure_ac(pip_ctx *c) {
-  if ((!c->kp.col_type && !c->kp.irs) || c->ac_valid) return PIP_OK;
+  if ((!c->kp.col_type && !c->kp.irl) || c->ac_valid) return PIP_OK;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   c->ac_valid = true;
   return PIP_OK;
@@ -562,6 +577,11 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
     c->kp.etaf = c->etaf;
     c->kp.resi_dt = resi_bound(c, eta.data());
   }
+  if (c->kp.irf) {
+    if ((e = cudaMalloc(&c->irg, 2 * c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->irg, 0, 2 * c->plane_bytes())) != cudaSuccess) return fail(e);
+    c->kp.irg = c->irg;
+  }
   if (c->kp.col_type) {
     if ((e = cudaMalloc(&c->acf, c->plane_bytes())) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(c->acf, 0, c->plane_bytes())) != cudaSuccess) return fail(e);
@@ -606,6 +626,7 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->d_dt);
   cudaFree(c->acf);
   cudaFree(c->etaf);
+  cudaFree(c->irg);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -838,7 +859,7 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
 }
 
 int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
-  const int64_t init = c && (c->kp.col_type || c->kp.irs) && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
+  const int64_t init = c && (c->kp.col_type || c->kp.irl) && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
   return init + 1 + 2 * (nsteps > 0 ? nsteps : 0);
 }
 
@@ -888,7 +909,7 @@ int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
 int pip_coefficients(pip_ctx *c) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
-  if (!c->kp.col_type && !c->kp.irs) return PIP_OK;
+  if (!c->kp.col_type && !c->kp.irl) return PIP_OK;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   CK(cudaStreamSynchronize(c->stream));

@@ -20,6 +20,8 @@ struct KParams {
   int imp;           // exponential collision form
   int ir;            // an ionisation/recombination law is active (IR source and cfl bound)
   int irs;           // 2 or 3: set_IR's Popescu law, rates from every stage's state (FP64 form)
+  int irl;           // 1, 2 or 3: set_IR runs before each cfl (with get_Te's energy rewrite)
+  int irf;           // 1: set_IR type 1, rates frozen in irg between the time loop's set_IR calls
   int ir_type;       // IR energy form 1 or 2
   long long nc;      // ix*jx
   double gm, ro_lim, pr_lim, ac, safety;
@@ -37,6 +39,8 @@ struct KParams {
   double ac_sb;      // sqrt(beta/2*gm)
   double ir_c136, ir_n6, ir_c291, ir_c291n6;  // 13.6/Te_0, n_norm*1e6, 2.91e-14, their product
   double ir_recfac, ir_fp, ir_tfac, ir_sqtfac, ir_tir;  // rec_fac, f_p, tfac, sqrt(tfac), t_ir
+  double ir_factor, ir_ionfac;  // set_IR type 1: factor = exp(-13.2/(T0/11605)), ion_fac
+  double *irg;       // type 1: Gm_ion (nc values) then Gm_rec (nc values) of the last set_IR
   double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
   int resi;          // flag_resi 1: resistive flux (eta field etaf), FP64 form
   const double *etaf;  // eta per cell, nc values

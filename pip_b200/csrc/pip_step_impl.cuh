@@ -185,11 +185,14 @@ __device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double
   return rdiv(a, pow(radd(rmul(T, 0.5), w), 0.125));
 }
 
-// set_IR types 2 and 3 (PIP_rot.f90:148-228) for one cell from the ion density ro and the
+// set_IR types 1, 2 and 3 (PIP_rot.f90:134-228) for one cell from the ion density ro and the
 // temperature te of get_Te_MHD, in the Fortran operation order (constants from the host).
 __device__ __forceinline__ void popescu_rates(const KParams &p, double ro, double te, double &gr,
                                               double &gi) {
-  if (p.irs == 2) {
+  if (p.irf) {
+    gr = rmul(rmul(rmul(pow(te, -0.5), rmul(ro, ro)), p.ir_recfac), p.ir_ionfac);
+    gi = rmul(rmul(rmul(pow(te, 0.5), ro), pow(p.ir_factor, rdiv(1.0, te))), p.ir_ionfac);
+  } else if (p.irs == 2) {
     const double a = rdiv(p.ir_c136, te);
     gr = rmul(rdiv(ro, __dsqrt_rn(te)), p.ir_recfac);
     gi = rmul(rdiv(rmul(rmul(rmul(rmul(p.ir_n6, ro), p.ir_c291), exp(-a)), pow(a, 0.39)),
@@ -203,7 +206,7 @@ __device__ __forceinline__ void popescu_rates(const KParams &p, double ro, doubl
   }
 }
 
-// set_IR of a Popescu law on one cell: get_Te's energy rewrite, then the rates.
+// set_IR of types 1-3 on one cell: get_Te's energy rewrite, then the rates.
 template <int NVM>
 __device__ __forceinline__ void set_ir_cell(double (&um)[NVM], double (&uh)[5], const KParams &p,
                                             double &gr, double &gi) {
@@ -720,8 +723,14 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     double ac_s = p.ac;
     if (COL && p.col_type) ac_s = set_collisional_cell<NVM>(s_m, s_h, p);
     double gr = 0.0, gion = 0.0;
-    if (COL && p.irs) set_ir_cell<NVM>(s_m, s_h, p, gr, gion);  // set_IR of the stage
-    else if (p.ir) ir_rates<NVM>(a_m, p, gr, gion);
+    if (COL && p.irs) {
+      set_ir_cell<NVM>(s_m, s_h, p, gr, gion);  // set_IR of the stage
+    } else if (COL && p.irf) {
+      gion = p.irg[q];                          // the time loop's last set_IR
+      gr = p.irg[nc + q];
+    } else if (p.ir) {
+      ir_rates<NVM>(a_m, p, gr, gion);
+    }
 
     // exponential form: U0 carries the collision increments of the earlier stages
     if (p.imp && STAGE == 2) {
@@ -798,7 +807,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     // fused cfl rewrites (and the next step's CFL terms)
     const int ep = STAGE == 1 ? 0 : s_epi;  // stage 1 is never followed by a cfl
     if (ep >= 1) {
-      if (COL && p.irs) {  // the time loop's set_IR before the cfl (main.f90:44-46)
+      if (COL && p.irl) {  // the time loop's set_IR before the cfl (main.f90:44-46)
         double g1, g2;
         set_ir_cell<NVM>(n_m, n_h, p, g1, g2);
       }
@@ -808,10 +817,14 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       (void)qh;
     }
     if (ep == 2) {
-      if (COL && p.irs) {  // the next step's set_IR (main.f90:32-34): cfl_pip_ir's rates
+      if (COL && p.irl) {  // the next step's set_IR (main.f90:32-34): cfl_pip_ir's rates
         double g1, g2;
         set_ir_cell<NVM>(n_m, n_h, p, g1, g2);
         grc = fmax(g1, g2);
+        if (p.irf) {       // type 1: the rates of the next step's stages
+          p.irg[q] = g2;
+          p.irg[nc + q] = g1;
+        }
       }
       const Prim<double> qm = rt_mhd<NVM>(n_m, p);
       const Prim<double> qh = rt_hd(n_h, p);
@@ -820,7 +833,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       dtc = fmin(cfl_mhd_cell<double>(qm, n_m[5], n_m[6], n_m[7], gm, sg),
                  cfl_hd_cell<double>(qh, gm, sg));
       rhoc = fmax(n_m[0] * ac_s, n_h[0] * ac_s);
-      if (p.ir && !p.irs) {
+      if (p.ir && !p.irl) {
         double g1, g2;
         ir_rates<NVM>(n_m, p, g1, g2);
         grc = fmax(g1, g2);
@@ -878,7 +891,13 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
     double gp1 = 0.0, gp2 = 0.0;
-    if (p.irs) set_ir_cell<NVM>(um, uh, p, gp1, gp2);  // the time loop's set_IR before cfl
+    if (p.irl) {                                        // the time loop's set_IR before cfl
+      set_ir_cell<NVM>(um, uh, p, gp1, gp2);
+      if (p.irf) {
+        p.irg[q] = gp2;
+        p.irg[nc + q] = gp1;
+      }
+    }
     const Prim<double> qm = rt_mhd<NVM>(um, p);
     const Prim<double> qh = rt_hd(uh, p);
 #pragma unroll
@@ -899,7 +918,7 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
       const double a = p.acf[q];
       rhoc = fmax(rhoc, fmax(um[0] * a, uh[0] * a));
     }
-    if (p.irs) {
+    if (p.irl) {
       grc = fmax(grc, fmax(gp1, gp2));
     } else if (p.ir) {
       double g1, g2;
@@ -1030,8 +1049,14 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
     double gr = 0.0, gion = 0.0;
-    if (p.irs) set_ir_cell<NVM>(um, uh, p, gr, gion);  // the rates of the state as given
-    else if (p.ir) ir_rates<NVM>(um, p, gr, gion);
+    if (p.irs) {
+      set_ir_cell<NVM>(um, uh, p, gr, gion);  // the rates of the state as given
+    } else if (p.irf) {
+      gion = p.irg[q];                        // the last set_IR's
+      gr = p.irg[nc + q];
+    } else if (p.ir) {
+      ir_rates<NVM>(um, p, gr, gion);
+    }
     const Prim<double> qh = rt_hd(uh, p);
     const Prim<double> qm = rt_mhd<NVM>(um, p);
     double ds[5], sm[5], sh[5];
@@ -1072,9 +1097,13 @@ __global__ void coefficients_kernel(const KParams p, double *U) {
     double um[NVM], uh[5];
     load_cell<NVM>(U, q, nc, um, uh);
     if (p.col_type) p.acf[q] = set_collisional_cell<NVM>(um, uh, p);
-    if (p.irs) {
+    if (p.irl) {
       double g1, g2;
       set_ir_cell<NVM>(um, uh, p, g1, g2);
+      if (p.irf) {
+        p.irg[q] = g2;
+        p.irg[nc + q] = g1;
+      }
     }
     U[q + 4 * nc] = um[4];
     U[q + (NVM + 4) * nc] = uh[4];
@@ -1133,7 +1162,7 @@ static cudaError_t launch_stage_t(const KParams &p, const double *Us, const doub
                                   DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
-  switch ((p.col_type || p.irs ? 1 : 0) | (p.resi ? 2 : 0)) {
+  switch ((p.col_type || p.irl ? 1 : 0) | (p.resi ? 2 : 0)) {
     case 0:
       stage_kernel<NDIM, NVM, STAGE, 0><<<grid, NT, stage_smem_bytes<NDIM, NVM, 0>(), s>>>(
           p, Us, U0, Uo, ctrl, dt_mode, epi);
@@ -1205,7 +1234,7 @@ static cudaError_t launch_source(const KParams &p, double *U, double *S, double 
 }
 
 static cudaError_t launch_coefficients(const KParams &p, double *U, cudaStream_t s) {
-  if (!p.col_type && !p.irs) return cudaSuccess;
+  if (!p.col_type && !p.irl) return cudaSuccess;
   if (p.nvm == 9) coefficients_kernel<9><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   else coefficients_kernel<8><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   return cudaGetLastError();

@@ -34,7 +34,7 @@ from typing import Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
-from .params import PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, Settings
+from .params import PIP_IR_JEFFERY, PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, Settings
 
 VAR_M = ("ro_p", "mx_p", "my_p", "mz_p", "en_p", "bx", "by", "bz", "ps")
 VAR_H = ("ro_n", "mx_n", "my_n", "mz_n", "en_n")
@@ -74,14 +74,23 @@ def layout(s: Settings, global_shape: Tuple[int, int, int]):
 
 def ir_rates(s: Settings, U_m: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """Gm_ion, Gm_rec from the ion state: the temperature of get_Te_MHD (get_Pr_MHD's
-    pressure with its floor), then PIP_IR_POWERLAW or set_IR type 2 or 3 (PIP_rot.f90:148-228;
-    the Fortran's single-precision literals rounded to float)."""
+    pressure with its floor), then PIP_IR_POWERLAW or set_IR type 1, 2 or 3
+    (PIP_rot.f90:134-228; the Fortran's single-precision literals rounded to float)."""
     gm = s.gm
     u = U_m
     pr = (gm - 1.0) * (u[4] - 0.5 * ((u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] +
                                      u[5] * u[5] + u[6] * u[6] + u[7] * u[7]))
     pr = np.maximum(pr, s.pr_lim)
     te = 0.5 * gm * (pr / u[0])
+    if s.flag_ir == PIP_IR_JEFFERY:
+        T0, n0 = s.t_norm, s.n_norm
+        f32 = lambda x: float(np.float32(x))
+        factor = np.exp(-13.2 / (T0 / 11605.0))
+        f2 = f32(2.7) * (13.2 * 11605.0) ** -2.0 * T0 ** 0.5 * n0
+        f3 = f32(5.6e-16) * (13.2 * 11605.0) ** -2.0 * T0 ** -1.0 * n0 ** 2.0
+        rec = te ** -0.5 * (u[0] * u[0]) * (f2 / f3) * (f3 / s.t_ir)
+        ion = te ** 0.5 * u[0] * factor ** (1.0 / te) * (f3 / s.t_ir)
+        return ion, rec
     if s.flag_ir in (PIP_IR_POPESCU, PIP_IR_POPESCU_EQ):
         f32 = lambda x: float(np.float32(x))
         te0 = s.t_norm / f32(1.1604e4)

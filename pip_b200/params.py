@@ -18,6 +18,7 @@ PIP_ABI_VERSION = 1
 PIP_FP64 = 0
 PIP_MIXED = 1
 PIP_IR_NONE = 0
+PIP_IR_JEFFERY = 1              # set_IR type 1 (PIP_rot.f90:135-149)
 PIP_IR_POPESCU = 2              # set_IR type 2 (PIP_rot.f90:148-170)
 PIP_IR_POPESCU_EQ = 3           # set_IR type 3 (PIP_rot.f90:173-228)
 PIP_IR_POWERLAW = 5
@@ -256,13 +257,14 @@ class Settings:
             bad.append("resistivity needs precision PIP_FP64 and no conduction")
         if self.flag_amb or self.flag_visc or self.flag_grav:
             bad.append("ambipolar diffusion, viscosity and gravity are not supported")
-        if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_IR_POWERLAW):
-            bad.append("flag_ir must be 0, 2, 3 (set_IR types 2, 3) or %d" % PIP_IR_POWERLAW)
-        elif self.flag_ir in (PIP_IR_POPESCU, PIP_IR_POPESCU_EQ):
+        set_ir_laws = (PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ)
+        if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW) + set_ir_laws:
+            bad.append("flag_ir must be 0, 1, 2, 3 (set_IR types 1-3) or %d" % PIP_IR_POWERLAW)
+        elif self.flag_ir in set_ir_laws:
             if not (self.t_norm > 0.0 and self.n_norm > 0.0):
-                bad.append("set_IR types 2 and 3 need T_norm > 0 and n_norm > 0")
+                bad.append("set_IR types 1-3 need T_norm > 0 and n_norm > 0")
             if self.precision != PIP_FP64:
-                bad.append("set_IR types 2 and 3 need precision PIP_FP64")
+                bad.append("set_IR types 1-3 need precision PIP_FP64")
         if self.flag_ir and self.flag_ir_type not in (1, 2):
             bad.append("flag_ir_type must be 1 or 2")
         for f in range(2 * self.ndim):

@@ -1,5 +1,6 @@
-"""set_IR types 2 and 3 (Popescu et al. 2019 rates) on the device, through the C ABI,
-against the oracle: the rates come from every stage's state and before each cfl, after
+"""set_IR types 1-3 on the device, through the C ABI, against the oracle: types 2 and 3
+(Popescu et al. 2019) take the rates from every stage's state and before each cfl, type 1
+(Jeffery) from the time loop's set_IR before each cfl, frozen over the step; each after
 get_Te's energy rewrite.  exp() and x**0.39 enter, so the runs are held to the drop-in
 tolerance of 1e-10 relative L1 per variable; the decomposed device loop equals the single
 domain bit for bit."""
@@ -12,7 +13,7 @@ import torch
 from helpers import rel_l1
 from oracle import oracle as O
 from pip_b200 import capi, decomp, ics
-from pip_b200.params import PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_MIXED
+from pip_b200.params import PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_MIXED
 
 pytestmark = pytest.mark.gpu
 
@@ -40,22 +41,44 @@ def compare(s, Uh, Um, nsteps):
     assert err <= TOL, "relative L1 %.3e > %.1e" % (err, TOL)
 
 
-@pytest.mark.parametrize("law,ir_type", [(PIP_IR_POPESCU, 1), (PIP_IR_POPESCU_EQ, 1),
-                                         (PIP_IR_POPESCU_EQ, 2)])
+@pytest.mark.parametrize("law,ir_type", [(PIP_IR_JEFFERY, 1), (PIP_IR_POPESCU, 1),
+                                         (PIP_IR_POPESCU_EQ, 1), (PIP_IR_POPESCU_EQ, 2)])
 @pytest.mark.parametrize("exact", [1, 0])
 def test_kelvin_helmholtz(gpu_lib, law, ir_type, exact):
     s, Uh, Um = case(law, flag_ir_type=ir_type, fp_exact=exact)
     compare(s, Uh, Um, 15)
 
 
-def test_with_alpha_c_per_cell_and_exponential_form(gpu_lib):
-    s, Uh, Um = case(PIP_IR_POPESCU_EQ, flag_col=4, flag_pip_imp=1, fp_exact=1)
+@pytest.mark.parametrize("law", [PIP_IR_JEFFERY, PIP_IR_POPESCU_EQ])
+def test_with_alpha_c_per_cell_and_exponential_form(gpu_lib, law):
+    s, Uh, Um = case(law, flag_col=4, flag_pip_imp=1, fp_exact=1)
     compare(s, Uh, Um, 12)
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_decomposed_device_loop(gpu_lib, world):
-    s, Uh, Um = case(PIP_IR_POPESCU_EQ, nx=32, ny=32, flag_col=5)
+def test_drop_in_call_sequence(gpu_lib):
+    """Type 1 through main.f90's calls one by one (cfl, run_solver, cfl) equals pip_run."""
+    s, Uh, Um = case(PIP_IR_JEFFERY, fp_exact=1)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        for _ in range(6):
+            dt, _ = c.cfl()
+            c.run_solver(dt)
+            c.cfl()
+        a = c.download()
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        c.run(nsteps=6)
+        b = c.download()
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("law,world", [(PIP_IR_POPESCU_EQ, 2), (PIP_IR_POPESCU_EQ, 4),
+                                       (PIP_IR_JEFFERY, 4)])
+def test_decomposed_device_loop(gpu_lib, law, world):
+    s, Uh, Um = case(law, nx=32, ny=32, flag_col=5)
     with capi.Context(s) as c:
         c.upload(Uh, Um)
         st1, t1, n1 = c.run(nsteps=8)

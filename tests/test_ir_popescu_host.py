@@ -1,14 +1,15 @@
-"""set_IR types 2 and 3 (Popescu et al. 2019 rates, PIP_rot.f90:148-228) in the oracle, on
-the CPU: the rates after set_coefficients against a vectorised restatement written from the
-Fortran (its single-precision literals rounded to float), the energy rewrite of get_Te, the
-cfl bound and a decomposed run."""
+"""set_IR types 1-3 (PIP_rot.f90:134-228: the Jeffery formulation and the Popescu et al.
+2019 rates) in the oracle, on the CPU: the rates after set_coefficients against a vectorised
+restatement written from the Fortran (its single-precision literals rounded to float), the
+energy rewrite of get_Te, the cfl bound and a decomposed run."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from oracle_block import OracleBlock
 from pip_b200 import decomp, ics, output
-from pip_b200.params import PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_MIXED, Settings
+from pip_b200.params import (PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_MIXED,
+                             Settings)
 
 
 def case(law, **kw):
@@ -16,7 +17,7 @@ def case(law, **kw):
 
 
 def literal_rates(s, U_m):
-    """Gm_ion, Gm_rec of set_IR type 2 or 3 after get_Te_MHD, whole-array, Fortran order."""
+    """Gm_ion, Gm_rec of set_IR type 1, 2 or 3 after get_Te_MHD, whole-array, Fortran order."""
     gm = s.gm
     m2 = U_m[1] * U_m[1] + U_m[2] * U_m[2] + U_m[3] * U_m[3]
     pr = (gm - 1.0) * (U_m[4] - 0.5 * ((m2 / U_m[0] + U_m[5] * U_m[5]) + U_m[6] * U_m[6]
@@ -26,6 +27,15 @@ def literal_rates(s, U_m):
     Te_p = 0.5 * gm * (pr / U_m[0])
     T0, n0, t_ir = s.t_norm, s.n_norm, s.t_ir
     r = lambda x: float(np.float32(x))                  # a REAL*4 literal
+    if s.flag_ir == PIP_IR_JEFFERY:
+        factor = np.exp(-13.2 / (T0 / 11605.0))
+        factor2 = r(2.7) * (13.2 * 11605.0) ** -2.0 * T0 ** (1.0 / 2.0) * n0
+        factor3 = r(5.6e-16) * (13.2 * 11605.0) ** -2.0 * T0 ** -1.0 * n0 ** 2.0
+        rec_fac = factor2 / factor3
+        ion_fac = factor3 / t_ir
+        Gm_rec = Te_p ** -0.5 * U_m[0] ** 2.0 * rec_fac * ion_fac
+        Gm_ion = Te_p ** 0.5 * U_m[0] * factor ** (1.0 / Te_p) * ion_fac
+        return Gm_ion, Gm_rec
     Te_0 = T0 / r(1.1604e4)
     if s.flag_ir == PIP_IR_POPESCU:
         rec_fac = r(2.6e-19) * (n0 * r(1.0e6)) / np.sqrt(Te_0) * t_ir
@@ -50,8 +60,8 @@ def literal_rates(s, U_m):
     return Gm_ion, Gm_rec
 
 
-@pytest.mark.parametrize("law,flag_col", [(PIP_IR_POPESCU, 1), (PIP_IR_POPESCU_EQ, 1),
-                                          (PIP_IR_POPESCU_EQ, 4)])
+@pytest.mark.parametrize("law,flag_col", [(PIP_IR_JEFFERY, 1), (PIP_IR_POPESCU, 1),
+                                          (PIP_IR_POPESCU_EQ, 1), (PIP_IR_POPESCU_EQ, 4)])
 def test_rates_match_the_literal_restatement(law, flag_col):
     s, Uh, Um = case(law, flag_col=flag_col)
     o = O.Oracle(s, Uh, Um)
@@ -75,8 +85,9 @@ def test_rates_match_the_literal_restatement(law, flag_col):
     np.testing.assert_allclose(om[4], Um[4], rtol=1e-14)
 
 
-def test_cfl_bound_and_run():
-    s, Uh, Um = case(PIP_IR_POPESCU_EQ)
+@pytest.mark.parametrize("law", [PIP_IR_JEFFERY, PIP_IR_POPESCU_EQ])
+def test_cfl_bound_and_run(law):
+    s, Uh, Um = case(law)
     o = O.Oracle(s, Uh, Um)
     try:
         dt, _ = o.cfl()
@@ -89,7 +100,7 @@ def test_cfl_bound_and_run():
         o.close()
 
 
-@pytest.mark.parametrize("law", [PIP_IR_POPESCU, PIP_IR_POPESCU_EQ])
+@pytest.mark.parametrize("law", [PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ])
 def test_blocks_match_single_domain(law):
     s, Uh, Um = case(law, flag_col=5)
     o = O.Oracle(s, Uh, Um)
