@@ -89,9 +89,11 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
 
 // One RK stage (see the FP64 stage_kernel for the structure).  Stage 1: Us = A.hi,
 // U0 = A.hi, output B (FP32).  Stage 2: Us = B, U0 = A.hi + A.lo, output A (hi, lo).
+// The parameter block is __grid_constant__: the out-of-line ghost writer takes its address,
+// which would otherwise copy the whole block to every thread's stack.
 template <int NDIM, int NVM, int STAGE>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? PIP_MIXED_MINB : 4)
-stage_kernel(const KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
+stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
              float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   constexpr int NV = NVM + 5;
