@@ -75,7 +75,9 @@ def layout(s: Settings, global_shape: Tuple[int, int, int]):
 def ir_rates(s: Settings, U_m: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """Gm_ion, Gm_rec from the ion state: the temperature of get_Te_MHD (get_Pr_MHD's
     pressure with its floor), then PIP_IR_POWERLAW or set_IR type 1, 2 or 3
-    (PIP_rot.f90:134-228; the Fortran's single-precision literals rounded to float)."""
+    (PIP_rot.f90:134-228; the Fortran's single-precision literals rounded to float).  The
+    rates are recomputed from the state as written; the run's last set_IR took them from
+    the state before the cfl's rewrite, so they agree to round-off."""
     gm = s.gm
     u = U_m
     pr = (gm - 1.0) * (u[4] - 0.5 * ((u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] +

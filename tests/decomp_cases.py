@@ -1,7 +1,8 @@
 """Small seeded cases for the decomposition tests: periodic 2D with Dedner cleaning
 (Orszag-Tang), 2D with reflecting walls at the ends of the split axis and ionisation/
 recombination (Kelvin-Helmholtz), and 1D with outflow ends (Brio-Wu); the ``_col`` cases
-use alpha_c per cell (set_collisional), ``ot_resi`` adds a uniform resistivity."""
+use alpha_c per cell (set_collisional), ``ot_resi`` adds a uniform resistivity, ``kh_ir1``
+and ``kh_ir3`` use set_IR types 1 and 3."""
 from generic_state import generic_state
 from pip_b200 import ics
 
@@ -17,6 +18,11 @@ def make_case(case):
         s, Uh, Um = ics.orszag_tang(16, flag_col=6)   # alpha_c per cell, col_type 5
     elif case == "kh_col":
         s, Uh, Um = ics.kelvin_helmholtz(16, 16, flag_col=4)
+    elif case == "kh_ir1":
+        s, Uh, Um = ics.kelvin_helmholtz(16, 16, flag_ir=1, t_norm=1.5e4, n_norm=1.0e11, t_ir=10.0)
+    elif case == "kh_ir3":
+        s, Uh, Um = ics.kelvin_helmholtz(16, 16, flag_ir=3, t_norm=1.5e4, n_norm=1.0e11, t_ir=10.0,
+                                         flag_col=5)
     elif case == "ot_resi":
         s, Uh, Um = ics.orszag_tang(16, flag_resi=1, eta_0=2e-3, flag_col=3)
     elif case == "ot_generic":

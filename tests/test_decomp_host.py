@@ -86,7 +86,7 @@ def _free_port():
         return k.getsockname()[1]
 
 
-@pytest.mark.parametrize("case", ["ot", "kh", "bw", "ot_resi"])
+@pytest.mark.parametrize("case", ["ot", "kh", "bw", "ot_resi", "kh_ir1", "kh_ir3"])
 def test_two_gloo_ranks_match_single_domain(case):
     nsteps = 5
     s, uh, um, hist = single_domain(case, nsteps)
