@@ -44,7 +44,7 @@ struct orc_ctx {
   double *eta;                       /* globalvar eta (set_resistivity), nc values */
 };
 
-static void ensure_ac(orc_ctx *c);
+static void ensure_coefficients(orc_ctx *c);
 
 static int g_threads = 1;
 
@@ -691,7 +691,7 @@ static void flux_dir(orc_ctx *c, int dir, double *F_h, double *F_m) {
 }
 
 void orc_flux(orc_ctx *c, int dir, double *F_h, double *F_m) {
-  ensure_ac(c);
+  ensure_coefficients(c);
   memset(F_h, 0, sizeof(double) * c->nc * c->nh);
   memset(F_m, 0, sizeof(double) * c->nc * c->nm);
   flux_dir(c, dir, F_h, F_m);
@@ -786,7 +786,7 @@ static void set_collisional(orc_ctx *c) {
  * with the electron temperature Te_0 = T_norm/1.1604e4 eV.  The single-precision literals of
  * the Fortran (2.7, 5.6e-16, 1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) are rounded to float first,
  * as there. */
-static void set_ir_popescu(orc_ctx *c) {
+static void set_ir_law(orc_ctx *c) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
   if (p->flag_ir == PIP_IR_JEFFERY) {
@@ -848,10 +848,10 @@ static int ir_loop(const orc_ctx *c) {
 /* set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140), on the state as it
  * stands, before the first call that reads the state: set_collisional (alpha_c per cell)
  * and set_IR (the Popescu laws), each with get_Te's energy rewrite. */
-static void ensure_ac(orc_ctx *c) {
+static void ensure_coefficients(orc_ctx *c) {
   if (c->init_done) return;
   if (c->col_type >= 1) set_collisional(c);
-  if (ir_loop(c)) set_ir_popescu(c);
+  if (ir_loop(c)) set_ir_law(c);
   c->init_done = 1;
 }
 
@@ -862,13 +862,13 @@ void orc_ir_rates(const orc_ctx *c, double *gm_ion, double *gm_rec) {
 
 void orc_coefficients(orc_ctx *c) {
   if (c->col_type >= 1) set_collisional(c);
-  if (ir_loop(c)) set_ir_popescu(c);
+  if (ir_loop(c)) set_ir_law(c);
   c->init_done = 1;
 }
 
 int orc_alpha_c(orc_ctx *c, double *ac) {
   size_t nc = c->nc;
-  ensure_ac(c);
+  ensure_coefficients(c);
   for (size_t q = 0; q < nc; ++q) ac[q] = c->col_type >= 1 ? c->ac[q] : c->p.col;
   return 0;
 }
@@ -953,11 +953,11 @@ static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, d
 
 void orc_source(orc_ctx *c, double dt_coll, double *S_h, double *S_m) {
   size_t nc = c->nc;
-  ensure_ac(c);
+  ensure_coefficients(c);
   memset(S_h, 0, sizeof(double) * nc * c->nh);
   memset(S_m, 0, sizeof(double) * nc * c->nm);
   /* the Popescu rates of the state as given (set_IR before set_source) */
-  if (ir_per_stage(c)) set_ir_popescu(c);
+  if (ir_per_stage(c)) set_ir_law(c);
   if (c->p.flag_pip_imp == 1) {
     /* report the U0 increments: run the form on zero U0 copies */
     source_pip(c, S_h, S_m, dt_coll, S_h, S_m);
@@ -974,7 +974,7 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
   double gm = p->gm, safety = p->safety, ac = p->col;
-  ensure_ac(c);
+  ensure_coefficients(c);
   const double *acf = c->col_type >= 1 ? c->ac : NULL;
   double *w = malloc(sizeof(double) * nc * 8);
   double *de = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc, *pr = w + 4 * nc;
@@ -982,7 +982,7 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   int m0 = p->margin[0], m1 = p->margin[1], m2 = p->margin[2];
 
   /* set_IR of the time loop before each cfl (main.f90:32-34,44-46), set_IR types 1-3 */
-  if (ir_loop(c)) set_ir_popescu(c);
+  if (ir_loop(c)) set_ir_law(c);
   /* cfl_mhd */
   cq2pv_mhd(c, c->U_m, de, vx, vy, vz, pr, bx, by, bz);
   /* set_IR for the rates the following run_solver uses: from the rewritten ion state */
@@ -1330,7 +1330,7 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   size_t nc = c->nc;
   int nh = c->nh, nm = c->nm, t_order = p->t_order;
   if (istep == 1) {
-    ensure_ac(c);
+    ensure_coefficients(c);
     if (!c->U_h0) c->U_h0 = malloc(sizeof(double) * nc * nh);
     if (!c->U_m0) c->U_m0 = malloc(sizeof(double) * nc * nm);
     memcpy(c->U_h0, c->U_h, sizeof(double) * nc * nh);
@@ -1345,7 +1345,7 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_col >= 2 recomputes alpha_c,
    * flag_IR >= 2 the rates (after it, :108-112) */
   if (c->col_type >= 1) set_collisional(c);
-  if (ir_per_stage(c)) set_ir_popescu(c);
+  if (ir_per_stage(c)) set_ir_law(c);
   for (int dir = 1; dir <= p->ndim; ++dir)
     flux_dir(c, dir, F_h + (size_t)(dir - 1) * nc * nh, F_m + (size_t)(dir - 1) * nc * nm);
   memset(S_h, 0, sizeof(double) * nc * nh);

@@ -49,7 +49,7 @@ struct pip_ctx {
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
   double *etaf = nullptr;             // eta per cell (flag_resi 1)
-  bool ac_valid = false;              // acf holds the last set_collisional's field
+  bool coef_valid = false;            // set_coefficients(U_h,U_m,0) has run on this state
   double *irg = nullptr;              // set_IR type 1's rates (2 planes)
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
@@ -176,9 +176,10 @@ int validate(const pip_params *p) {
   return PIP_OK;
 }
 
-// Constants of set_IR types 2 and 3 (PIP_rot.f90:148-228), with the Fortran's
-// single-precision literals (1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) rounded to float first.
-void popescu_constants(const pip_params &p, KParams &k) {
+// Constants of set_IR types 1-3 (PIP_rot.f90:134-228), with the Fortran's
+// single-precision literals (2.7, 5.6e-16, 1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) rounded to
+// float first.
+void ir_law_constants(const pip_params &p, KParams &k) {
   k.irs = (p.flag_ir == PIP_IR_POPESCU || p.flag_ir == PIP_IR_POPESCU_EQ) ? p.flag_ir : 0;
   k.irf = p.flag_ir == PIP_IR_JEFFERY ? 1 : 0;
   k.irl = k.irs || k.irf ? 1 : 0;
@@ -230,7 +231,7 @@ void build_kparams(pip_ctx *c) {
   k.imp = p.flag_pip_imp;
   k.ir = p.flag_ir != PIP_IR_NONE;
   k.ir_type = p.flag_ir_type;
-  popescu_constants(p, k);
+  ir_law_constants(p, k);
   k.nc = (long long)p.ix * p.jx;
   k.gm = p.gm;
   k.igm1 = 1.0 / (p.gm - 1.0);
@@ -412,13 +413,13 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
   ctrl->blocks_done = 0;
 }
 
-// The alpha_c field for a state that no set_collisional has seen since its upload:
-// set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140) rewrites the energies
-// and sets alpha_c before the first cfl and the first stage.
-int ensure_ac(pip_ctx *c) {
-  if ((!c->kp.col_type && !c->kp.irl) || c->ac_valid) return PIP_OK;
+// set_coefficients(U_h,U_m,0) of the prologue (Initial_rot.f90:140) for a state uploaded
+// since the last one: set_collisional (alpha_c per cell) and set_IR (types 1-3) rewrite the
+// energies and set their fields before the first cfl and the first stage.
+int ensure_coefficients(pip_ctx *c) {
+  if ((!c->kp.col_type && !c->kp.irl) || c->coef_valid) return PIP_OK;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
-  c->ac_valid = true;
+  c->coef_valid = true;
   return PIP_OK;
 }
 
@@ -643,7 +644,7 @@ int pip_upload(pip_ctx *c, const double *U_h, const double *U_m) {
   CK(from_fp64(c));
   CK(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
-  c->ac_valid = false;
+  c->coef_valid = false;
   c->last_stage = 0;
   return PIP_OK;
 }
@@ -664,7 +665,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
-  if (ensure_ac(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   reset_slot(*c->h_ctrl, 0, c->kp);
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
@@ -682,7 +683,7 @@ int pip_step(pip_ctx *c, double dt) {
   if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
   if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
-  if (ensure_ac(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   DevCtrl &h = *c->h_ctrl;
   h.dt = dt;
   h.cmax = c->cmax;
@@ -714,7 +715,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   c->last_stage = 2;
   c->dev_loop = false;
   if (set_device(c)) return PIP_ERR_CUDA;
-  if (ensure_ac(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   if ((t_end > 0.0 && c->time >= t_end)) {
     if (time_out) *time_out = c->time;
     if (steps_done) *steps_done = 0;
@@ -829,7 +830,7 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
   h.nsteps = nsteps;
   reset_slot(h, 0, c->kp);
   reset_slot(h, 1, c->kp);
-  if (ensure_ac(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
   std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
@@ -859,7 +860,7 @@ int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *ms
 }
 
 int64_t pip_kernels_per_run(pip_ctx *c, int64_t nsteps) {
-  const int64_t init = c && (c->kp.col_type || c->kp.irl) && !c->ac_valid ? 1 : 0;  // set_coefficients(0)
+  const int64_t init = c && (c->kp.col_type || c->kp.irl) && !c->coef_valid ? 1 : 0;  // set_coefficients(0)
   return init + 1 + 2 * (nsteps > 0 ? nsteps : 0);
 }
 
@@ -882,7 +883,7 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
   if (!c->uploaded) return PIP_ERR_STATE;
   if (dir < 1 || dir > c->kp.ndim) return PIP_ERR_PARAM;
   if (c->mixed) return PIP_ERR_STATE;  // unit-level entry points are FP64 only
-  if (set_device(c) || ensure_scratch(c) || ensure_ac(c)) return PIP_ERR_CUDA;
+  if (set_device(c) || ensure_scratch(c) || ensure_coefficients(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(cudaMemsetAsync(c->scratch, 0, pb * c->nplanes(), c->stream));
   CK(c->L->flux(c->kp, c->A, c->scratch, dir, c->cmax, c->stream));
@@ -896,7 +897,7 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
 int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
   if (!c || !S_h || !S_m) return PIP_ERR_NULL;
   if (!c->uploaded || c->mixed) return PIP_ERR_STATE;
-  if (set_device(c) || ensure_scratch(c) || ensure_ac(c)) return PIP_ERR_CUDA;
+  if (set_device(c) || ensure_scratch(c) || ensure_coefficients(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
   CK(c->L->source(c->kp, c->A, c->scratch, dt_coll, c->stream));
   CK(cudaMemcpyAsync(S_m, c->scratch, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
@@ -913,7 +914,7 @@ int pip_coefficients(pip_ctx *c) {
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  c->ac_valid = true;
+  c->coef_valid = true;
   return PIP_OK;
 }
 
@@ -924,7 +925,7 @@ int pip_get_alpha_c(pip_ctx *c, double *ac) {
     for (long long q = 0; q < c->kp.nc; ++q) ac[q] = c->p.col;
     return PIP_OK;
   }
-  if (set_device(c) || ensure_ac(c)) return PIP_ERR_CUDA;
+  if (set_device(c) || ensure_coefficients(c)) return PIP_ERR_CUDA;
   CK(cudaMemcpyAsync(ac, c->acf, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PIP_OK;
@@ -937,7 +938,7 @@ int pip_set_alpha_c(pip_ctx *c, const double *ac) {
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(cudaMemcpyAsync(c->acf, ac, c->plane_bytes(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  c->ac_valid = true;
+  c->coef_valid = true;
   return PIP_OK;
 }
 
@@ -1045,7 +1046,7 @@ int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
   if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (stage == 1) {
-    if (ensure_ac(c)) return PIP_ERR_CUDA;
+    if (ensure_coefficients(c)) return PIP_ERR_CUDA;
     stage_ctrl_kernel<<<1, 1, 0, c->stream>>>(c->ctrl, dt, cmax);
     CK(cudaGetLastError());
     c->cmax = cmax;
@@ -1092,7 +1093,7 @@ int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
   h.cmax = c->cmax;
   reset_slot(h, 0, c->kp);
   reset_slot(h, 1, c->kp);
-  if (ensure_ac(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));                         // the first step's cfl candidates (main.f90:36)
   CK(cudaStreamSynchronize(c->stream));

@@ -187,7 +187,7 @@ __device__ __forceinline__ double set_collisional_cell(double (&um)[NVM], double
 
 // set_IR types 1, 2 and 3 (PIP_rot.f90:134-228) for one cell from the ion density ro and the
 // temperature te of get_Te_MHD, in the Fortran operation order (constants from the host).
-__device__ __forceinline__ void popescu_rates(const KParams &p, double ro, double te, double &gr,
+__device__ __forceinline__ void ir_law_rates(const KParams &p, double ro, double te, double &gr,
                                               double &gi) {
   if (p.irf) {
     gr = rmul(rmul(rmul(pow(te, -0.5), rmul(ro, ro)), p.ir_recfac), p.ir_ionfac);
@@ -212,7 +212,7 @@ __device__ __forceinline__ void set_ir_cell(double (&um)[NVM], double (&uh)[5], 
                                             double &gr, double &gi) {
   double te_m, te_h, rm, rh;
   get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
-  popescu_rates(p, um[0], te_m, gr, gi);
+  ir_law_rates(p, um[0], te_m, gr, gi);
 }
 
 // Collisional exchange dS of source_PIP (PIP_rot.f90:1333-1368) for one cell from the
@@ -1087,8 +1087,9 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
   }
 }
 
-// set_collisional over every cell (set_coefficients, Solver_rot.f90:95-122, col_type >= 1):
-// both energies rewritten in place, alpha_c into p.acf.
+// set_coefficients over every cell (Solver_rot.f90:95-122): set_collisional (col_type >= 1,
+// alpha_c into p.acf) and set_IR (types 1-3; type 1's rates into p.irg), each rewriting
+// both energies in place.
 template <int NVM>
 __global__ void coefficients_kernel(const KParams p, double *U) {
   const long long nc = p.nc;
