@@ -127,3 +127,34 @@ def test_settings():
     assert (s.flag_ir, s.t_norm, s.n_norm) == (3, 1.5e4, 1e11)
     p, _ = s.to_params()
     assert p.t_norm == 1.5e4 and p.n_norm == 1e11
+
+
+def test_type3_equilibrium_has_no_mass_exchange():
+    """set_IR type 3 is scaled to the ionisation equilibrium of T_norm: at the ion
+    temperature tfac (code units) and rho_n/rho_i = ioneq the ionisation and recombination
+    mass rates cancel (source_PIP's IR block, PIP_rot.f90:1370-1376)."""
+    s, _, _ = case(PIP_IR_POPESCU_EQ)
+    f32 = lambda x: float(np.float32(x))
+    Te_0 = s.t_norm / f32(1.1604e4)
+    ioneq = (f32(2.6e-19) / np.sqrt(Te_0)) / (f32(2.91e-14) / (0.232 + 13.6 / Te_0)
+                                               * (13.6 / Te_0) ** 0.39 * np.exp(-13.6 / Te_0))
+    f_n = ioneq / (ioneq + 1.0)
+    f_p = 1.0 - f_n
+    tfac = 0.5 * (2.0 * f_p / (f_n + 2.0 * f_p)) / f_p          # flag_col 1
+    ix, jx, _ = s.shape
+    ro_i = 0.3
+    ro_n = ioneq * ro_i
+    p_i = tfac * ro_i / (0.5 * s.gm)                          # Te_p = 0.5*gm*p/ro = tfac
+    zero = np.zeros((jx, ix))
+    Uh = ics.pv2cq_hd(s, ro_n + zero, zero, zero, zero, 0.4 + zero)
+    Um = ics.pv2cq_mhd(s, ro_i + zero, zero, zero, zero, p_i + zero, 0.1 + zero, zero, zero)
+    o = O.Oracle(s.overrides(col=0.0), Uh, Um)
+    try:
+        o.coefficients()
+        ion, rec = o.ir_rates()
+        S_h, S_m = o.source(1e-3)
+    finally:
+        o.close()
+    scale = rec * ro_i
+    assert np.all(np.abs(S_m[0]) <= 1e-12 * scale)      # rec*ro_i - ion*ro_n = 0
+    np.testing.assert_allclose(ion * ro_n, rec * ro_i, rtol=1e-12)
