@@ -76,3 +76,30 @@ def test_null_arguments(lib):
     assert capi.lib().pip_ctx_create(None, ctypes.byref(h)) == capi.PIP_ERR_NULL
     assert capi.lib().pip_upload(None, None, None) == capi.PIP_ERR_NULL
     assert capi.lib().pip_run(None, 1, 0.0, None, None) == capi.PIP_ERR_NULL
+
+
+def test_parameter_block_layout_matches_the_header(tmp_path):
+    """The ctypes pip_params has the C struct's size and field offsets (include/pip_gpu.h,
+    compiled by the host C compiler), so a Fortran or Python caller and the library agree
+    on every field."""
+    from pip_b200.params import PipParams
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    names = [f[0] for f in PipParams._fields_]
+    src = ["#include <stdio.h>", "#include <stddef.h>",
+           '#include "%s"' % os.path.join(ROOT, "include", "pip_gpu.h"),
+           "int main(void) {", '  printf("size %zu\\n", sizeof(pip_params));']
+    src += ['  printf("%s %%zu\\n", offsetof(pip_params, %s));' % (n, n) for n in names]
+    src += ["  return 0;", "}"]
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-o", str(exe), str(c)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], check=True,
+                                                       capture_output=True, text=True).stdout.splitlines())
+    assert int(out["size"]) == ctypes.sizeof(PipParams)
+    for n in names:
+        assert int(out[n]) == getattr(PipParams, n).offset, n
