@@ -1,7 +1,7 @@
 """ctypes binding of the C ABI (include/pip_gpu.h) in pip_b200/libpipgpu.so.
 
 This is the reference-facing surface in Python form: the same calls the Fortran driver
-makes through ISO_C_BINDING.  There is no CPU fallback: if the CUDA
+makes through an ISO_C_BINDING interface module.  There is no CPU fallback: if the CUDA
 library is missing or no GPU is visible the calls raise.
 """
 from __future__ import annotations
