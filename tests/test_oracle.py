@@ -49,6 +49,27 @@ def test_periodic_conservation():
         assert abs(after - before) <= 1e-13 * scale, name
 
 
+@pytest.mark.parametrize("extra", [
+    dict(flag_col=5),
+    dict(flag_col=7, flag_resi=1, eta_0=2e-3),
+    dict(flag_col=4, flag_ir=3, t_norm=1.5e4, n_norm=1.0e11, t_ir=10.0),
+    dict(flag_ir=1, t_norm=1.5e4, n_norm=1.0e11, t_ir=10.0, flag_resi=1, eta_0=1e-3),
+])
+def test_periodic_conservation_with_extra_physics(extra):
+    """The same invariants with alpha_c per cell, resistivity and the set_IR laws: their
+    sources are antisymmetric between the species and the resistive terms are fluxes."""
+    s, Uh, Um = ics.orszag_tang(40, **extra)
+    st, t, n, Uh2, Um2, _ = O.run_case(s, Uh, Um, nsteps=40, threads=4)
+    assert st == 0
+    m = s.margin[0]
+    sl = (slice(m, -m), slice(m, -m))
+    for k, name in ((0, "mass"), (1, "mx"), (2, "my"), (4, "energy")):
+        before = Uh[k][sl].sum() + Um[k][sl].sum()
+        after = Uh2[k][sl].sum() + Um2[k][sl].sum()
+        scale = np.abs(Uh[k][sl]).sum() + np.abs(Um[k][sl]).sum()
+        assert abs(after - before) <= 1e-13 * scale, name
+
+
 def test_directional_symmetry():
     """A 1D tube along x equals the same tube along y of a 2D grid with (vx,vy), (bx,by)
     swapped, bit for bit (the reference's debug_direction check, shock_tube.f90:64-123)."""
