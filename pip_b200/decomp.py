@@ -230,7 +230,10 @@ class DeviceBlock:
 
     def __init__(self, block: Block, U_h: np.ndarray, U_m: np.ndarray, device: int = 0,
                  eta: Optional[np.ndarray] = None):
-        """eta: the block's part of a fixed resistivity field (flag_resi), if not uniform."""
+        """eta: the block's part of a fixed resistivity field (flag_resi).  By default a
+        localised field (resi_type 1) is made from the block's own coordinates, as each
+        rank's set_resistivity does (Res_rot.f90:29-35); pass the scattered global field to
+        match a single-domain run bit for bit."""
         import torch
         from .capi import Context
         self.torch = torch
@@ -238,6 +241,8 @@ class DeviceBlock:
         self.ctx = Context(block.settings)
         self.ctx.set_neighbors(block.neighbor)
         self.ctx.upload(U_h, U_m)
+        if eta is None and block.settings.flag_resi and (block.settings.flag_resi // 10) % 10:
+            eta = block.settings.eta_field()
         if eta is not None:
             self.ctx.set_resistivity(eta)
         self.device = torch.device("cuda", device)
