@@ -166,7 +166,8 @@ int pip_step(pip_ctx *ctx, double dt);
  * For callers that cannot call cudaMalloc: a host code whose device memory is owned by
  * someone else (an OpenACC or CUDA Fortran data region, a fixed-size memory pool of the
  * application) or that must not allocate on its stepping path.  Same computation as
- * pip_step with the FP64 kernels, on a state the caller already holds on the device:
+ * pip_step with the FP64 kernels (the two RK stages with their ghost fill), on a state the
+ * caller already holds on the device:
  * U_dev is the device image of U_m followed by U_h (nvar_m + 5 planes of ix*jx doubles,
  * Fortran order, ghosts included), updated in place.  dt and cmax are what cfl returned
  * (pip_cfl, or the caller's own).  The work is queued on `stream` (a cudaStream_t; NULL for
@@ -175,8 +176,11 @@ int pip_step(pip_ctx *ctx, double dt);
  * The U1 stage buffer, the control block and device copies of dx/dy live in one
  * file-scope device array of PIP_NOALLOC_SCRATCH_BYTES that every GPU loading this
  * library holds until the process exits.  Limits: ix*jx <= PIP_NOALLOC_MAX_CELLS and
- * ix, jx <= PIP_NOALLOC_MAX_AXIS; larger grids, the mixed precision form and any
- * parameter pip_ctx_create would reject return PIP_ERR_PARAM.  The first call on each
+ * ix, jx <= PIP_NOALLOC_MAX_AXIS; larger grids, the mixed precision form, implicit
+ * conduction (flag_heat = 1: pip_step's BiCGstab after the stages needs a context's
+ * buffers), per-cell alpha_c (flag_col >= 2), resistivity, set_IR types 1-3 and any
+ * parameter pip_ctx_create would reject return PIP_ERR_PARAM before any GPU work.  The
+ * call reads p->dx and p->dy (host arrays) while it runs.  The first call on each
  * device looks up that array's device address and sets the kernels' shared-memory limit;
  * make that first call before any stream capture.  All calls share the one array and it
  * keeps the previous call's contents (the control block is rewritten by every call), so
@@ -254,6 +258,17 @@ int pip_status(pip_ctx *ctx, int *stop_flag, int *nan_flag);
  * hc_error.  iters and relres (either may be NULL) receive the iteration count and the
  * final relative residual. */
 int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
+
+/* Diagnostic; no counterpart in the reference.  The BiCGstab kernels stage their rows with
+ * bulk async copies and wait for each on an mbarrier a bounded number of polls; a block
+ * whose wait runs out flags the solve, waits (bounded by the default limit) for its copies
+ * still in flight and returns, the remaining kernels of the solve return at once, and
+ * pip_conduction / pip_step / pip_run return PIP_ERR_CUDA with pip_last_cuda_error() =
+ * cudaErrorLaunchTimeout (702); the context stays usable (upload a state and go on).
+ * This sets the number of polls from the next solve on (polls < 0: the default, 2^22);
+ * 0 makes every wait run out at once, which exercises that path.  PIP_ERR_PARAM without
+ * flag_heat = 1. */
+int pip_set_hc_wait_limit(pip_ctx *ctx, int polls);
 
 /*
  * Domain decomposition over ranks (one context per rank and device, each holding its own

@@ -8,7 +8,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <cstring>
 #include <mutex>
 
 #include "../../include/pip_gpu.h"
@@ -28,6 +27,20 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void *g_scratch_addr[kMaxDevices];  // device address of the scratch array, per device
 
+// A failed CUDA call: keep its code for pip_last_cuda_error, as the context calls do.
+int cuda_fail(cudaError_t e) {
+  pip::record_cuda_error((int)e);
+  return PIP_ERR_CUDA;
+}
+
+// The whole control block starts from zero on every call, with this call's dt and cmax;
+// both come in as launch arguments, so no host buffer has to outlive the call.
+__global__ void noalloc_ctrl_kernel(pip::DevCtrl *ctrl, double dt, double cmax) {
+  *ctrl = pip::DevCtrl{};
+  ctrl->dt = dt;
+  ctrl->cmax = cmax;
+}
+
 }  // namespace
 
 // [control block | dx | dy | U1 (14 planes of up to PIP_NOALLOC_MAX_CELLS doubles)]
@@ -39,24 +52,28 @@ extern "C" int pip_step_noalloc(const pip_params *p, double *U_dev, double dt, d
   pip::KParams k;
   const int st = pip::kparams_from_params(p, &k);
   if (st != PIP_OK) return st;
-  if (p->precision != PIP_FP64) return PIP_ERR_PARAM;
+  // the FP64 kernels only; and no implicit conduction, whose BiCGstab needs buffers of
+  // its own: pip_step runs HC after the two stages, which this entry point does not
+  if (p->precision != PIP_FP64 || p->flag_heat != 0) return PIP_ERR_PARAM;
   if (k.nc > PIP_NOALLOC_MAX_CELLS || p->ix > PIP_NOALLOC_MAX_AXIS || p->jx > PIP_NOALLOC_MAX_AXIS)
     return PIP_ERR_PARAM;
   if (!(dt > 0.0) || !std::isfinite(dt) || !std::isfinite(cmax)) return PIP_ERR_PARAM;
   const pip::Launchers &L = p->fp_exact ? pip::launchers_exact() : pip::launchers_fast();
 
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PIP_ERR_CUDA;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e);
+  if (dev < 0 || dev >= kMaxDevices) return PIP_ERR_CUDA;
   void *base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_addr[dev]) {
       void *ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return PIP_ERR_CUDA;
+      if ((e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch)) != cudaSuccess) return cuda_fail(e);
+      if (!ptr) return PIP_ERR_CUDA;
       // both FP64 flavours, so a later call with the other fp_exact also finds its limit set
-      if (pip::launchers_fast().prepare() != cudaSuccess ||
-          pip::launchers_exact().prepare() != cudaSuccess)
-        return PIP_ERR_CUDA;
+      if ((e = pip::launchers_fast().prepare()) != cudaSuccess) return cuda_fail(e);
+      if ((e = pip::launchers_exact().prepare()) != cudaSuccess) return cuda_fail(e);
       g_scratch_addr[dev] = ptr;
     }
     base = g_scratch_addr[dev];
@@ -69,17 +86,14 @@ extern "C" int pip_step_noalloc(const pip_params *p, double *U_dev, double dt, d
   k.dx = ddx;
   k.dy = ddy;
 
-  // the control block starts from zero on every call, with this call's dt and cmax
-  pip::DevCtrl h;
-  std::memset(&h, 0, sizeof h);
-  h.dt = dt;
-  h.cmax = cmax;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (cudaMemcpyAsync(ctrl, &h, sizeof h, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(ddx, p->dx, sizeof(double) * p->ix, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(ddy, p->dy, sizeof(double) * p->jx, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return PIP_ERR_CUDA;
-  if (L.stage(k, 1, U_dev, U_dev, U1, ctrl, 0, 0, s) != cudaSuccess) return PIP_ERR_CUDA;
-  if (L.stage(k, 2, U1, U_dev, U_dev, ctrl, 0, 0, s) != cudaSuccess) return PIP_ERR_CUDA;
+  noalloc_ctrl_kernel<<<1, 1, 0, s>>>(ctrl, dt, cmax);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaMemcpyAsync(ddx, p->dx, sizeof(double) * p->ix, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e);
+  if ((e = cudaMemcpyAsync(ddy, p->dy, sizeof(double) * p->jx, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e);
+  if ((e = L.stage(k, 1, U_dev, U_dev, U1, ctrl, 0, 0, s)) != cudaSuccess) return cuda_fail(e);
+  if ((e = L.stage(k, 2, U1, U_dev, U_dev, ctrl, 0, 0, s)) != cudaSuccess) return cuda_fail(e);
   return PIP_OK;
 }
