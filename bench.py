@@ -101,7 +101,8 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "utilization.gpu")
 
     def __init__(self, device_index: int):
         self.dev = device_index
@@ -136,24 +137,32 @@ class ClockSampler:
                 self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        """Median SM clock over the samples taken under load (GPU utilisation >= 50 %; all
+        samples if none is), the maximum clock and every throttle reason seen active."""
+        sm, busy, mx, reasons = [], [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
+                f = float(parts[1])
                 mx = float(parts[2])
             except ValueError:
                 continue
+            sm.append(f)
+            try:
+                if len(parts) > 9 and float(parts[9]) >= 50.0:
+                    busy.append(f)
+            except ValueError:
+                pass
             for n, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(busy or sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm), "samples_under_load": len(busy)}
 
 
 def cpu_sample(target_s: float = 15.0, threads: int = 0):
@@ -209,9 +218,12 @@ def run_reference(args):
     s, Uh, Um = ics.orszag_tang(N_GRID)
     o = O.Oracle(s, Uh, Um)
     o.prologue()
+    # the same untimed warm-up steps as the GPU arm, then as many of the requested steps as
+    # the time budget allows
+    warmup = max(1, args.warmup)
     t0 = time.perf_counter()
-    o.run(nsteps=max(1, min(args.warmup, 1)))
-    warm = time.perf_counter() - t0
+    o.run(nsteps=warmup)
+    warm = (time.perf_counter() - t0) / warmup
     steps = max(1, min(args.steps, int(budget / max(warm, 1e-3))))
     t0 = time.perf_counter()
     st, _, n, _ = o.run(nsteps=steps)
@@ -221,7 +233,7 @@ def run_reference(args):
     val = cells * n / dt
     line = {
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": n, "warmup": 1, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+        "steps": n, "warmup": warmup, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_text(N_GRID, world, world > 1 or args.decompose),
                    "cells": cells * world, "precision": "fp64",
@@ -239,12 +251,13 @@ def run_reference(args):
     return 0
 
 
-def measure(n, precision, steps, warmup, dist, local):
+def measure(n, precision, steps, warmup, dist, local, exact=0):
     """Device-resident timing of one precision form on OT n x n: returns timings, the
-    state after warmup+steps steps and per-kernel durations."""
+    state after warmup+steps steps and per-kernel durations.  exact=1: the FP64 kernels
+    built without FMA contraction."""
     import torch
     from pip_b200 import capi, ics
-    s, Uh, Um = ics.orszag_tang(n, precision=precision)
+    s, Uh, Um = ics.orszag_tang(n, precision=precision, fp_exact=exact)
     ctx = capi.Context(s)
     ctx.upload(Uh, Um)
     ctx.prologue()
@@ -447,7 +460,7 @@ def measure_adjoint(nsteps=500, K=25):
 
 
 def measure_ensemble(n_runs=512, t_end=0.1):
-    from pip_b200.ensemble import Ensemble, shock_tube_ensemble
+    from pip_b200.ensemble import Ensemble, fp64_single_run_errors, shock_tube_ensemble
     mem = shock_tube_ensemble(n_runs, 4242)
     with Ensemble(mem) as e:
         threads, ctas, _ = e.tune(t_probe=0.002)
@@ -456,16 +469,35 @@ def measure_ensemble(n_runs=512, t_end=0.1):
         ms = e.run(t_end=t_end)
         updates = 0
         bad = 0
+        results = []
         for r in range(len(mem)):
-            _, _, t, n, st = e.member(r, state=False)
-            updates += n * mem[r][0].ix0
-            bad += st != 0
+            res = e.member(r)
+            updates += res[3] * mem[r][0].ix0
+            bad += res[4] != 0
+            results.append(res)
+    # every member against its own single-run FP64 solve (same start, same steps)
+    t0 = time.time()
+    errs = fp64_single_run_errors(mem, results)
+    worst = max(range(len(mem)), key=lambda r: float(errs[r][0].max()))
+    l1_all = [float(x[0].max()) for x in errs]
+    m = mem[worst][0]
     return {"workload": "%d seeded 1D two-fluid shock tubes, nx log-uniform [256, 8192], "
                         "alpha_c log-uniform [0.1, 1e4], to t=%g, FP32-mixed" % (n_runs, t_end),
             "value": updates / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
             "cell_updates": updates, "runs_failed": bad, "threads": threads,
-            "ctas_per_sm": ctas, "how": "one persistent launch (CUDA graph), configuration "
-                                        "chosen by the autotuner on a t=0.002 probe"}
+            "ctas_per_sm": ctas,
+            "vs_fp64_single_runs": {
+                "members_checked": len(errs), "max_rel_l1": max(l1_all),
+                "median_rel_l1": float(statistics.median(l1_all)),
+                "members_above_1e-5": sum(x > 1e-5 for x in l1_all),
+                "max_rel_time_diff": max(float(x[1]) for x in errs),
+                "worst_member": {"index": worst, "nx": m.ix0, "alpha_c": m.col},
+                "check_s": time.time() - t0,
+                "how": "each member's 13 fields against a plain FP64 single run (pip_run) from "
+                       "the same initial state over the same number of steps; relative L1 "
+                       "per variable over the interior cells, max over variables"},
+            "how": "one persistent launch (CUDA graph), configuration "
+                   "chosen by the autotuner on a t=0.002 probe"}
 
 
 # C3 BiCGstab iteration (three kernels): algorithmic bytes per interior cell -- 5 face-factor
@@ -507,7 +539,20 @@ def measure_conduction(nsteps=1000, kapper=0.01):
                      "us_per_iteration": us_it,
                      "iteration_gbs": b * 2048 * 1024 / (us_it * 1e-6) / 1e9,
                      "algorithmic_bytes_per_cell_iteration": b}
+    # the rounding-only spread: the FP64 path built without FMA contraction against the FMA
+    # build, same run; the mixed-vs-FP64 figures above are read against it
+    s, Uh, Um = ics.kelvin_helmholtz(2048, 1024, flag_heat=1, kapper=kapper, hc_error=1e-10,
+                                     hc_max=5000, fp_exact=1)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        st, t, n, _ = c.run_timed(nsteps=nsteps)
+        if st != 0 or n != nsteps:
+            raise RuntimeError("C3 FMA-free run ended with status %d after %d steps" % (st, n))
+        states["fp64_exact"] = c.download()
+    spread = rel_l1_interior(states["fp64_exact"], states["fp64"], 3)
     l1 = rel_l1_interior(states["mixed"], states["fp64"], 3)
+    out["l1_fp64_fma_vs_fma_free"] = dict(zip(L1_NAMES[:13], [float(x) for x in spread[:13]]))
     out.update({
         "workload": "2D partially ionised Kelvin-Helmholtz 2048x1024 (+3 ghosts), periodic x, "
                     "reflecting y, IR power law chi=5, kapper=%g (kappa_par ~ T^2.5 along B), "
@@ -519,6 +564,20 @@ def measure_conduction(nsteps=1000, kapper=0.01):
                "time per iteration is (time with conduction - time without) / iterations, and "
                "its GB/s counts the algorithmic bytes of the three BiCGstab kernels" % nsteps})
     return out
+
+
+def compact(x, top=True):
+    """The printed line: the descriptive strings ("how", "note", the sub-records'
+    "workload") dropped -- the module docstring describes each record -- and floats rounded
+    to 4 significant digits, so the whole line stays short."""
+    if isinstance(x, dict):
+        return {k: compact(v, False) for k, v in x.items()
+                if k not in ("how", "note") and not (k == "workload" and not top)}
+    if isinstance(x, list):
+        return [compact(v, False) for v in x]
+    if isinstance(x, float):
+        return float("%.4g" % x)
+    return x
 
 
 def rel_l1_interior(a, b, m):
@@ -547,6 +606,8 @@ def main():
     ap.add_argument("--no-extra-physics", action="store_true")
     ap.add_argument("--decompose", action="store_true",
                     help="run the domain-decomposed step also with one GPU (always with N > 1)")
+    ap.add_argument("--detail", default=None,
+                    help="also write the full record (descriptions, unrounded) to this file")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -580,12 +641,18 @@ def main():
     n = args.n
     cells = n * n
     decomposed = world > 1 or args.decompose
+    # clocks over the whole measurement (every timed region below lies inside it)
+    whole = ClockSampler(local).__enter__()
     if decomposed:
         f64 = measure_decomposed(n, PIP_FP64, args.steps, args.warmup, dist, local, world, rank)
         mix = measure_decomposed(n, PIP_MIXED, args.steps, args.warmup, dist, local, world, rank)
     else:
         f64 = measure(n, PIP_FP64, args.steps, args.warmup, dist, local)
         mix = measure(n, PIP_MIXED, args.steps, args.warmup, dist, local)
+    # the FMA-free FP64 flavour: bit for bit the oracle's arithmetic, so it meets the
+    # drop-in bar on all 14 fields (the FMA build's psi differs by ~1e-8)
+    f64x = None if decomposed else measure(n, PIP_FP64, args.steps, args.warmup, dist, local,
+                                           exact=1)
     l1 = rel_l1_interior(mix["state"], f64["state"], 2)
     ms64 = max_over_ranks(f64["ms"])
     msmx = max_over_ranks(mix["ms"])
@@ -610,6 +677,7 @@ def main():
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps, "how": how}
     if rank != 0:
+        whole.__exit__()
         if dist:
             dist.destroy_process_group()
         return 0
@@ -634,6 +702,7 @@ def main():
         ionisation = variant("flag_ir=3 (set_IR type 3 at every stage), T_norm=1.5e4, "
                              "n_norm=1e11, t_IR=10", flag_ir=3, t_norm=1.5e4, n_norm=1.0e11,
                              t_ir=10.0)
+    whole.__exit__()
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": msmx / args.steps, "higher_is_better": True,
@@ -661,17 +730,23 @@ def main():
                                           "its busy time per step (ncu) exceeds the HBM floor "
                                           "~2.6x, so HBM frac cannot pass ~0.38"}},
                  "gpu_launches": f64["launches"], "clocks": f64["clocks"]},
+        "fp64_fma_free": None if f64x is None else {
+            "value": cells * args.steps / (f64x["ms"] * 1e-3),
+            "ms_per_step": f64x["ms"] / args.steps, "ms_stage1": f64x["ms1"],
+            "ms_stage2": f64x["ms2"]},
         "mixed_over_fp64": vmx / v64,
+        "mixed_over_fp64_fma_free": None if f64x is None else f64x["ms"] / mix["ms"],
         "l1_mixed_vs_fp64": {
             "max_physical": float(max(l1[:5].max(), l1[5:13].max())),
             "psi": float(l1[13]),
             "bar": 1e-5,
-            "pass": bool(max(l1[:5].max(), l1[5:13].max()) <= 1e-5),
+            "pass": bool(l1.max() <= 1e-5),
+            "pass_physical": bool(max(l1[:5].max(), l1[5:13].max()) <= 1e-5),
             "per_variable": dict(zip(L1_NAMES, [float(x) for x in l1])),
             "after_steps": args.warmup + args.steps,
-            "note": "13 physical fields (8 MHD + 5 hydro); psi is the Dedner potential, driven "
-                    "by div B, a truncation-level difference of B, so FP32 flux rounding in B "
-                    "dominates it"},
+            "note": "pass is over all 14 stored fields; pass_physical over the 13 physical "
+                    "fields (8 MHD + 5 hydro) without the Dedner potential psi, which "
+                    "amplifies white noise in B ~1e7-fold (tests/psi_sensitivity.py)"},
         "roofline": {"bound": "hbm", "achieved": amx, "peak": peak, "unit": "GB/s",
                      "frac": amx / peak, "traffic": ncu_traffic("stage2_mixed_ot1024"),
                      "kernel": "mixed stage_kernel<2,9,2> (stage 2: fluxes+source+update+cfl)",
@@ -687,9 +762,12 @@ def main():
         "ionisation_recombination": ionisation,
         "e2e": e2e,
         "gpu_launches": mix["launches"],
-        "clocks": mix["clocks"],
+        "clocks": whole.summary(),
     }
-    print(json.dumps(line), flush=True)
+    if args.detail:
+        with open(args.detail, "w") as f:
+            json.dump(line, f, indent=1)
+    print(json.dumps(compact(line)), flush=True)
     if dist:
         dist.destroy_process_group()
     return 0

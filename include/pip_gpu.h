@@ -74,8 +74,9 @@ enum pip_ir_law {
  *   precision PIP_FP64 only),
  *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ (FP64
  *   form; T_norm and n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type 1 or 2,
- *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0/1 (a fixed eta field; FP64 form, not
- *   with flag_heat), no viscosity/gravity/ambipolar diffusion.
+ *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0, 1 (a fixed eta field) or 2 (eta
+ *   recomputed at every RK stage, resi_type 2 or 3; FP64 form, not with flag_heat), no
+ *   viscosity/gravity/ambipolar diffusion.
  */
 typedef struct pip_params {
   int32_t abi_version;     /* must equal PIP_ABI_VERSION */
@@ -106,8 +107,15 @@ typedef struct pip_params {
   int32_t flag_resi;       /* 0, or 1: resistive flux with a fixed eta field (resistive_flux,
                               Solver_rot.f90:505-638, flag_sch=0 branch; cfl_resi,
                               Scheme_rot.f90:291-302); eta = eta_0 everywhere unless
-                              pip_set_resistivity gives the field (FP64 form only) */
-  int32_t reserved_i[5];
+                              pip_set_resistivity gives the field (FP64 form only);
+                              2: eta from the stage state at the start of every RK stage
+                              (set_resistivity resi_type 2 or 3, Res_rot.f90:37-60, called by
+                              set_coefficients, Solver_rot.f90:98-101) -- the setting's
+                              flag_resi = 22 or 32 */
+  int32_t resi_type;       /* flag_resi 2: 2 anomalous eta = 11 eta_0 where |curl B| >= j_cri
+                              (else eta_0), 3 eta = eta_0 (|curl B|/rho_i/vd_cri - 1)^2 where
+                              |curl B|/rho_i >= vd_cri (else 0) */
+  int32_t reserved_i[4];
   double gm;               /* ratio of specific heats: gm_d/gm_n */
   double safety;           /* CFL number */
   double ro_lim, pr_lim;   /* density and pressure floors */
@@ -124,7 +132,8 @@ typedef struct pip_params {
   double eta_0;            /* uniform resistivity (set_resistivity resi_type 0) */
   double t_norm, n_norm;   /* T0 (K) and n0 of the normalisation (setting keys T_norm, n_norm;
                               set_IR types 2 and 3) */
-  double reserved_d[3];
+  double j_cri, vd_cri;    /* thresholds of resi_type 2 and 3 (setting keys j_cri, vd_cri) */
+  double reserved_d[1];
   const double *dx;        /* ix cell widths (dsc(:,1)) */
   const double *dy;        /* jx cell widths (dsc(:,2)); 1D: one entry, the reference sets 100 */
   const double *dz;        /* kx cell widths (dsc(:,3)); one entry, the reference sets 100 */
@@ -242,6 +251,15 @@ int pip_set_alpha_c(pip_ctx *ctx, const double *ac);
  * Fortran order, ghosts included) that resistive_flux and cfl_resi use from the next call
  * on; eta_0 everywhere until called.  PIP_ERR_PARAM without flag_resi 1. */
 int pip_set_resistivity(pip_ctx *ctx, const double *eta);
+
+/* cfl_resi's bound (Scheme_rot.f90:291-302) of the current eta: min over the interior cells
+ * of safety*min(dx,dy,dz)**2/max(eta,1e-8).  With flag_resi 2 the eta is set_resistivity's
+ * of the last RK stage (or of the uploaded state before the first step).  cfl_resi writes
+ * the Fortran global dt rather than cfl's argument, so after run_solver the time loop's
+ * cfl(U_h,U_m,dtnew) lowers the dt that `time` advances by (main.f90:47,58): a host that
+ * steps with pip_step and pip_cfl applies dt = min(dt, bound) before time = time + dt.
+ * pip_run does this itself.  PIP_ERR_PARAM without resistivity. */
+int pip_resi_dt(pip_ctx *ctx, double *bound);
 
 /* PIPbnd(U_h,U_m,0) (Boundary_rot.f90:34-52) on the device state; with one rank the
  * MPI halo exchange (MPI_rot.f90:128-339) reduces to this ghost fill. */

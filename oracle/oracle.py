@@ -67,6 +67,8 @@ def lib():
         L.orc_has_nan.restype = ctypes.c_int
         L.orc_coefficients.argtypes = [vp]
         L.orc_set_resistivity.argtypes = [vp, dp]
+        L.orc_resistivity.argtypes = [vp, dp]
+        L.orc_resistivity.restype = None
         L.orc_ir_rates.argtypes = [vp, dp, dp]
         L.orc_alpha_c.argtypes = [vp, dp]
         L.orc_alpha_c.restype = ctypes.c_int
@@ -183,6 +185,12 @@ class Oracle:
         """The eta field (jx, ix) of flag_resi 1 (eta_0 everywhere until set)."""
         e = np.ascontiguousarray(eta, dtype=np.float64).reshape(self.shape_h[1:])
         lib().orc_set_resistivity(self.h, _ptr(e))
+
+    def resistivity(self) -> np.ndarray:
+        """The current eta field (jx, ix)."""
+        e = np.empty(self.shape_h[1:])
+        lib().orc_resistivity(self.h, _ptr(e))
+        return e
 
     def ir_rates(self):
         """(Gm_ion, Gm_rec) of the last set_IR, each shaped like one plane."""

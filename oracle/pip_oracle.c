@@ -40,11 +40,13 @@ struct orc_ctx {
   int col_type;                      /* initialize_collisional: flag_col 2..7 -> 1..6 */
   double *ac;                        /* alpha_c per cell (globalvar ac) for col_type >= 1 */
   int init_done;                     /* set_coefficients(U_h,U_m,0) has run */
-  int resi;                          /* flag_resi 1: resistive flux with the eta field */
+  int resi;                          /* flag_resi 1: resistive flux with a fixed eta field;
+                                        2: eta from set_resistivity at every RK stage */
   double *eta;                       /* globalvar eta (set_resistivity), nc values */
 };
 
 static void ensure_coefficients(orc_ctx *c);
+static double cfl_resi(orc_ctx *c, double dt);
 
 static int g_threads = 1;
 
@@ -669,6 +671,38 @@ static void resistive_flux(orc_ctx *c, int dir, double *F) {
   free(w);
 }
 
+/* set_resistivity resi_type 2 and 3 (Res_rot.f90:37-60): eta from |curl B| of the current
+ * state (get_rotation of U_m(:,:,:,6:8), zero on the outermost layer): type 2 eta_0, or
+ * 11 eta_0 where |curl B| >= j_cri; type 3 eta_0 (vd/vd_cri - 1)**2 where the drift
+ * vd = |curl B|/rho_i >= vd_cri, else 0. */
+static void set_resistivity_anomalous(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  double *cur = malloc(sizeof(double) * 3 * nc);
+  get_rotation(c, cur);
+  const double *r1 = cur, *r2 = cur + nc, *r3 = cur + 2 * nc;
+  for (size_t q = 0; q < nc; ++q) {
+    double c2 = sqrt(r1[q] * r1[q] + r2[q] * r2[q] + r3[q] * r3[q]);
+    if (p->resi_type == 2) {
+      c->eta[q] = p->eta_0;
+      if (c2 >= p->j_cri) c->eta[q] = p->eta_0 * 11.0;
+    } else {
+      double vdri = c2 / c->U_m[q];
+      c->eta[q] = 0.0;
+      if (vdri >= p->vd_cri) {
+        double a = vdri / p->vd_cri - 1.0;
+        c->eta[q] = p->eta_0 * (a * a);
+      }
+    }
+  }
+  free(cur);
+}
+
+void orc_resistivity(orc_ctx *c, double *eta) {
+  ensure_coefficients(c);
+  memcpy(eta, c->eta, sizeof(double) * c->nc);
+}
+
 void orc_set_resistivity(orc_ctx *c, const double *eta) {
   if (c->eta) memcpy(c->eta, eta, sizeof(double) * c->nc);
 }
@@ -850,6 +884,7 @@ static int ir_loop(const orc_ctx *c) {
  * and set_IR (the Popescu laws), each with get_Te's energy rewrite. */
 static void ensure_coefficients(orc_ctx *c) {
   if (c->init_done) return;
+  if (c->resi == 2) set_resistivity_anomalous(c);
   if (c->col_type >= 1) set_collisional(c);
   if (ir_loop(c)) set_ir_law(c);
   c->init_done = 1;
@@ -861,6 +896,7 @@ void orc_ir_rates(const orc_ctx *c, double *gm_ion, double *gm_rec) {
 }
 
 void orc_coefficients(orc_ctx *c) {
+  if (c->resi == 2) set_resistivity_anomalous(c);
   if (c->col_type >= 1) set_collisional(c);
   if (ir_loop(c)) set_ir_law(c);
   c->init_done = 1;
@@ -1039,17 +1075,7 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   }
 
   /* cfl_resi (Scheme_rot.f90:291-302) */
-  if (c->resi) {
-    double etmin = 1.0e-8, dr = dttemp;
-#pragma omp parallel for collapse(2) reduction(min : dr) schedule(static)
-    for (int k = m2; k < c->kx - m2; ++k)
-      for (int j = m1; j < c->jx - m1; ++j)
-        for (int i = m0; i < c->ix - m0; ++i) {
-          double gmin = fmn(fmn(c->dx[i], c->dy[j]), c->dz[k]);
-          dr = fmn(dr, safety * (gmin * gmin) / fmx(c->eta[AT(c, i, j, k)], etmin));
-        }
-    dttemp = dr;
-  }
+  if (c->resi) dttemp = cfl_resi(c, dttemp);
 
   /* cmax for Dedner cleaning */
   double cmax = c->cmax;
@@ -1065,6 +1091,25 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
   free(w);
   if (dt_out) *dt_out = dttemp;
   if (cmax_out) *cmax_out = cmax;
+}
+
+/* cfl_resi (Scheme_rot.f90:291-302): dt lowered to safety*gmin**2/max(eta,1e-8) over the
+ * interior cells.  It writes the global dt, whatever variable the enclosing cfl call
+ * fills: in the time loop's first cfl that is the step's dt, in the second (after
+ * run_solver) the dt that `time` then advances by (main.f90:47,58). */
+static double cfl_resi(orc_ctx *c, double dt) {
+  const pip_params *p = &c->p;
+  const int m0 = p->margin[0], m1 = p->margin[1], m2 = p->margin[2];
+  const double safety = p->safety, etmin = 1.0e-8;
+  double dr = dt;
+#pragma omp parallel for collapse(2) reduction(min : dr) schedule(static)
+  for (int k = m2; k < c->kx - m2; ++k)
+    for (int j = m1; j < c->jx - m1; ++j)
+      for (int i = m0; i < c->ix - m0; ++i) {
+        double gmin = fmn(fmn(c->dx[i], c->dy[j]), c->dz[k]);
+        dr = fmn(dr, safety * (gmin * gmin) / fmx(c->eta[AT(c, i, j, k)], etmin));
+      }
+  return dr;
 }
 
 /* ---------------------------------------------------------------- integration */
@@ -1342,8 +1387,9 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
   double *S_h = malloc(sizeof(double) * nc * nh), *S_m = malloc(sizeof(double) * nc * nm);
   double dt_coll[2] = {dt * 0.5, dt * 0.5};
   double dt_coll_i = dt_coll[t_order - istep];
-  /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_col >= 2 recomputes alpha_c,
-   * flag_IR >= 2 the rates (after it, :108-112) */
+  /* set_coefficients(U_h,U_m,1) (Solver_rot.f90:62): flag_resi >= 2 recomputes eta
+   * (:98-101), flag_col >= 2 alpha_c, flag_IR >= 2 the rates (after it, :108-112) */
+  if (c->resi == 2) set_resistivity_anomalous(c);
   if (c->col_type >= 1) set_collisional(c);
   if (ir_per_stage(c)) set_ir_law(c);
   for (int dir = 1; dir <= p->ndim; ++dir)
@@ -1395,6 +1441,9 @@ int orc_run(orc_ctx *c, long nsteps, double t_end, double *time_out, long *steps
     c->cmax = cmax;
     orc_run_solver(c, dt);
     orc_cfl(c, &dtnew, NULL);
+    /* the second cfl's cfl_resi lowers the global dt with the eta of the last stage (a
+     * no-op for a fixed eta field, whose bound dt already holds) */
+    if (c->resi) dt = cfl_resi(c, dt);
     c->time = c->time + dt;
     c->last_dt = dt;
     if (dt_hist && n < max_hist) dt_hist[n] = dt;
@@ -1415,7 +1464,8 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   if (p->nvar_m != (p->flag_divb == 1 ? 9 : 8)) return NULL;
   if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0))) return NULL;
   if (p->flag_col < 1 || p->flag_col > 7) return NULL;
-  if (p->flag_resi != 0 && p->flag_resi != 1) return NULL;
+  if (p->flag_resi < 0 || p->flag_resi > 2) return NULL;
+  if (p->flag_resi == 2 && p->resi_type != 2 && p->resi_type != 3) return NULL;
   orc_ctx *c = calloc(1, sizeof(orc_ctx));
   c->p = *p;
   for (int f = 0; f < 6; ++f) c->neighbor[f] = -1;
@@ -1433,7 +1483,7 @@ orc_ctx *orc_create(const pip_params *p, int *status) {
   c->gm_ion = calloc(c->nc, sizeof(double));
   c->gm_rec = calloc(c->nc, sizeof(double));
   c->col_type = p->flag_col >= 2 ? p->flag_col - 1 : 0;   /* PIP_rot.f90:21-26 */
-  c->resi = p->flag_resi == 1;
+  c->resi = p->flag_resi;
   if (c->resi) {
     c->eta = malloc(sizeof(double) * c->nc);
     for (size_t q = 0; q < c->nc; ++q) c->eta[q] = p->eta_0;   /* set_resistivity type 0 */

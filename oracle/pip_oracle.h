@@ -59,6 +59,9 @@ int orc_alpha_c(orc_ctx *c, double *ac);
 /* The eta field of set_resistivity (Res_rot.f90:16-60) for flag_resi 1 (nc values);
  * eta_0 everywhere until called. */
 void orc_set_resistivity(orc_ctx *c, const double *eta);
+/* The current eta field (nc values): the fixed field, or with flag_resi 2 the one
+ * set_resistivity computed at the start of the last RK stage (or of the prologue). */
+void orc_resistivity(orc_ctx *c, double *eta);
 /* Boundary_rot.f90:34-52. */
 void orc_bnd(orc_ctx *c);
 /* main.f90:31-68 loop; returns 0, PIP_ERR_NAN or PIP_ERR_DT.  dt_hist (may be NULL)

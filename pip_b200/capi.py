@@ -35,7 +35,7 @@ EXPORTS = (
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
-    "pip_set_alpha_c", "pip_set_resistivity",
+    "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -91,8 +91,10 @@ def lib(path: Optional[str] = None):
     L.pip_get_alpha_c.argtypes = [vp, dp]
     L.pip_set_alpha_c.argtypes = [vp, dp]
     L.pip_set_resistivity.argtypes = [vp, dp]
+    L.pip_resi_dt.argtypes = [vp, dp]
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
+    L.pip_set_hc_wait_limit.argtypes = [vp, i]
     L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
     L.pip_set_neighbors.argtypes = [vp, P(i)]
     L.pip_stage.argtypes = [vp, i, d, d]
@@ -244,6 +246,10 @@ class Context:
             raise PipError(st, "pip_conduction")
         return st, it.value, rr.value
 
+    def set_hc_wait_limit(self, polls: int) -> None:
+        """Polls of the BiCGstab staging waits from the next solve on (< 0: the default)."""
+        _check(lib().pip_set_hc_wait_limit(self.h, int(polls)), "pip_set_hc_wait_limit")
+
     @property
     def conduction_iterations(self) -> int:
         return int(lib().pip_conduction_iterations(self.h))
@@ -288,6 +294,12 @@ class Context:
         """The eta field (jx, ix) of flag_resi 1 (set_resistivity; eta_0 everywhere until set)."""
         e = np.ascontiguousarray(eta, dtype=np.float64).reshape(self.shape_h[1:])
         _check(lib().pip_set_resistivity(self.h, _ptr(e)), "pip_set_resistivity")
+
+    def resi_dt(self) -> float:
+        """cfl_resi's bound of the current eta (pip_resi_dt)."""
+        b = ctypes.c_double()
+        _check(lib().pip_resi_dt(self.h, ctypes.byref(b)), "pip_resi_dt")
+        return b.value
 
     def set_alpha_c(self, ac: np.ndarray) -> None:
         """The field of a restart output (its "ac" dataset) for the next cfl."""

@@ -39,10 +39,14 @@ constexpr int NVM = 8, NV = 13;
 #ifndef PIP_ADJ_FACE_MINB
 #define PIP_ADJ_FACE_MINB 2
 #endif
+#ifndef PIP_ADJ_FACEH_MINB
+#define PIP_ADJ_FACEH_MINB 2
+#endif
 #ifndef PIP_ADJ_CELL_MINB
 #define PIP_ADJ_CELL_MINB 2
 #endif
-constexpr int kFaceThreads = 128;   // one face per thread
+constexpr int kFaceThreads = 128;   // one face per thread (ion faces)
+constexpr int kFaceThreadsH = 256;  // one face per thread (neutral faces)
 constexpr int kCellThreads = 256;
 
 // Per-block CFL candidates of stage 1 (the state z_n).
@@ -72,11 +76,13 @@ __device__ __forceinline__ double dmm(int mode, int q) {
   return 0.0;
 }
 
-// Reverse of one face: MUSCL-minmod face states from the primitives in shared memory
+// Reverse of one face for the ions (SP = 0: HLLD) or the neutrals (SP = 1: HLLC): MUSCL-minmod
+// face states from the primitives in shared memory
 // (cells a - s, a, a + s, a + 2s along the face normal), the density floors and the
 // Riemann solvers.  lamF: cotangent of the face flux (natural variable order).  Writes the
 // cotangents of the two face states (gL, gR, natural order, after the floors), the minmod
 // branches and returns <F, lamF>.
+template <int SP>
 __device__ __forceinline__ double face_vjp(const KParams &p, const double *__restrict__ V,
                                            long long a, long long s, bool ydir,
                                            const double (&lamF)[NV], double *gL, double *gR,
@@ -84,7 +90,7 @@ __device__ __forceinline__ double face_vjp(const KParams &p, const double *__res
   const long long RR = p.nc;  // plane stride of the primitives
   double fdot = 0.0;
   modes = 0ull;
-  {
+  if (SP == 0) {
     double vl[8], vr[8], af[8], avl[8], avr[8], flx[8];
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
@@ -112,8 +118,7 @@ __device__ __forceinline__ double face_vjp(const KParams &p, const double *__res
       gL[src * nf + f] = avl[n];
       gR[src * nf + f] = avr[n];
     }
-  }
-  {
+  } else {
     double vl[5], vr[5], af[5], avl[5], avr[5], flx[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
@@ -197,18 +202,23 @@ __global__ void u2v_kernel(const KParams p, const double *__restrict__ U, double
   }
 }
 
-// Reverse of the face fluxes of one RK stage: one thread per face.  x faces (j, i) lie
-// between cells (j, i) and (j, i+1), y faces (j, i) between (j, i) and (j+1, i); a face is
-// stored at the index j*ix + i of its lower cell.  For faces next to an interior cell: the
-// flux cotangent from the cotangent lam of the stage output, the reverse of the MUSCL face
-// states and the Riemann solver (face_vjp), written as (gL, gR, minmod branches); other
-// faces are written as zero.  Per block: sum of <F, lamF> (the flux part of dt_sub
-// <lam, dU/d(dt_sub)>).
-__global__ void __launch_bounds__(kFaceThreads, PIP_ADJ_FACE_MINB)
+// Reverse of the face fluxes of one RK stage for one species (SP = 0 ions, 1 neutrals): one
+// thread per face.  x faces (j, i) lie between cells (j, i) and (j, i+1), y faces (j, i)
+// between (j, i) and (j+1, i); a face is stored at the index j*ix + i of its lower cell.
+// For faces next to an interior cell: the flux cotangent from the cotangent lam of the
+// stage output, the reverse of the MUSCL face states and the Riemann solver (face_vjp),
+// written as (gL, gR) on the species' planes and its half of the minmod-branch word (the
+// ion planes' branches fill bits 0-31, the neutral planes' bits 32-51); other faces are
+// written as zero.  Per block: sum of <F, lamF> over the species' planes (the flux part of
+// dt_sub <lam, dU/d(dt_sub)>).  The two species run as separate kernels because the HLLD
+// reverse needs every register a thread can have and the HLLC reverse far fewer.
+template <int SP, int NT>
+__global__ void __launch_bounds__(NT, SP == 0 ? PIP_ADJ_FACE_MINB : PIP_ADJ_FACEH_MINB)
 face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__restrict__ lam,
                 const double *dtp, double fac, double *gx, unsigned long long *mx, double *gy,
                 unsigned long long *my, double *part_dot, double *part_dac) {
-  __shared__ double s_red[kFaceThreads / 32];
+  constexpr int N0 = SP == 0 ? 0 : NVM, N1 = SP == 0 ? NVM : NV;
+  __shared__ double s_red[NT / 32];
   const long long nc = p.nc;
   const double dt_sub = fac * (*dtp);
   const long long nfx = (long long)p.jx * (p.ix - 1);
@@ -232,12 +242,15 @@ face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__r
     }
     const long long qa = (long long)ja * p.ix + ia, qb = (long long)jb * p.ix + ib;
     double *g = ydir ? gy : gx;
-    unsigned long long *mm = ydir ? my : mx;
+    unsigned int *mh = reinterpret_cast<unsigned int *>(ydir ? my : mx) + 2 * qa + SP;
     const bool in_a = interior(p, ia, ja), in_b = interior(p, ib, jb);
     if (!in_a && !in_b) {
 #pragma unroll
-      for (int n = 0; n < 2 * NV; ++n) g[n * nc + qa] = 0.0;
-      mm[qa] = 0ull;
+      for (int n = N0; n < N1; ++n) {
+        g[n * nc + qa] = 0.0;
+        g[(NV + n) * nc + qa] = 0.0;
+      }
+      *mh = 0u;
     } else {
       double ca = 0.0, cb = 0.0;
       if (!ydir) {
@@ -250,13 +263,18 @@ face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__r
       double lamF[NV];
 #pragma unroll
       for (int n = 0; n < NV; ++n) {
+        if (n < N0 || n >= N1) {
+          lamF[n] = 0.0;
+          continue;
+        }
         const double la = in_a ? lam[qa + n * nc] : 0.0;
         const double lb = in_b ? lam[qb + n * nc] : 0.0;
         lamF[n] = -ca * la + cb * lb;
       }
       unsigned long long m;
-      dot = face_vjp(p, V, qa, ydir ? (long long)p.ix : 1ll, ydir, lamF, g, g + NV * nc, nc, qa, m);
-      mm[qa] = m;
+      dot = face_vjp<SP>(p, V, qa, ydir ? (long long)p.ix : 1ll, ydir, lamF, g, g + NV * nc, nc,
+                         qa, m);
+      *mh = (unsigned int)(m >> (32 * SP));
     }
   }
 #pragma unroll
@@ -265,7 +283,7 @@ face_vjp_kernel(const KParams p, const double *__restrict__ V, const double *__r
   __syncthreads();
   if (threadIdx.x == 0) {
     double sd = 0.0;
-    for (int k = 0; k < kFaceThreads / 32; ++k) sd += s_red[k];
+    for (int k = 0; k < NT / 32; ++k) sd += s_red[k];
     part_dot[blockIdx.x] = sd;
     part_dac[blockIdx.x] = 0.0;
   }
@@ -571,8 +589,10 @@ __global__ void __launch_bounds__(256) finalize_kernel(const KParams p, int nb, 
   if (ldt_out) *ldt_out = ldt;
 }
 
-// One reverse stage: primitives of Us, faces, cells.  Partial sums: face blocks first (nbf),
-// then cell blocks.
+int face_blocks_h(const KParams &p);
+
+// One reverse stage: primitives of Us, faces (ions, then neutrals), cells.  Partial sums: the
+// ion face blocks first (nbf), then the neutral face blocks, then the cell blocks.
 cudaError_t launch_stage_vjp(const KParams &p, const double *Us, const double *lam, const double *acc,
                              double *out, const double *dtp, double fac, double *V, double *gx,
                              unsigned long long *mx, double *gy, unsigned long long *my,
@@ -580,16 +600,24 @@ cudaError_t launch_stage_vjp(const KParams &p, const double *Us, const double *l
   const long long nc = p.nc;
   const int gu = (int)std::min<long long>((nc + 255) / 256, 148 * 8);
   u2v_kernel<<<gu, 256, 0, s>>>(p, Us, V);
-  face_vjp_kernel<<<nbf, kFaceThreads, 0, s>>>(p, V, lam, dtp, fac, gx, mx, gy, my, pdot, pdac);
+  face_vjp_kernel<0, kFaceThreads><<<nbf, kFaceThreads, 0, s>>>(p, V, lam, dtp, fac, gx, mx, gy,
+                                                                my, pdot, pdac);
+  const int nbh = face_blocks_h(p);
+  face_vjp_kernel<1, kFaceThreadsH><<<nbh, kFaceThreadsH, 0, s>>>(p, V, lam, dtp, fac, gx, mx, gy,
+                                                                  my, pdot + nbf, pdac + nbf);
   const int nbc = (int)((nc + kCellThreads - 1) / kCellThreads);
   cell_vjp_kernel<<<nbc, kCellThreads, 0, s>>>(p, Us, lam, acc, out, dtp, fac, gx, mx, gy, my,
-                                               pdot + nbf, pdac + nbf, cand);
+                                               pdot + nbf + nbh, pdac + nbf + nbh, cand);
   return cudaGetLastError();
 }
 
-int face_blocks(const KParams &p) {
-  const long long nf = (long long)p.jx * (p.ix - 1) + (p.ndim == 2 ? (long long)(p.jx - 1) * p.ix : 0);
-  return (int)((nf + kFaceThreads - 1) / kFaceThreads);
+long long face_count(const KParams &p) {
+  return (long long)p.jx * (p.ix - 1) + (p.ndim == 2 ? (long long)(p.jx - 1) * p.ix : 0);
+}
+// blocks of the ion and of the neutral face kernel
+int face_blocks(const KParams &p) { return (int)((face_count(p) + kFaceThreads - 1) / kFaceThreads); }
+int face_blocks_h(const KParams &p) {
+  return (int)((face_count(p) + kFaceThreadsH - 1) / kFaceThreadsH);
 }
 int cell_blocks(const KParams &p) { return (int)((p.nc + kCellThreads - 1) / kCellThreads); }
 
@@ -753,7 +781,7 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
   a->kp.dy = a->d_dy;
   a->nbf = pip::adjk::face_blocks(a->kp);
   a->nbc = pip::adjk::cell_blocks(a->kp);
-  a->nb = a->nbf + a->nbc;
+  a->nb = a->nbf + pip::adjk::face_blocks_h(a->kp) + a->nbc;
   if ((e = cudaMalloc(&a->V, sb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->gx, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->gy, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);

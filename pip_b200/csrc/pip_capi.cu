@@ -49,6 +49,7 @@ struct pip_ctx {
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
   double *etaf = nullptr;             // eta per cell (flag_resi 1)
+  unsigned long long *d_resi = nullptr;  // cfl_resi's bound of the current eta (flag_resi 2)
   bool coef_valid = false;            // set_coefficients(U_h,U_m,0) has run on this state
   double *irg = nullptr;              // set_IR type 1's rates (2 planes)
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
@@ -146,9 +147,12 @@ int validate(const pip_params *p) {
   if (p->flag_col >= 2 && p->precision != PIP_FP64) return PIP_ERR_PARAM;
   if ((p->flag_col == 2 || p->flag_col == 4 || p->flag_col == 6) && !(p->beta > 0.0))
     return PIP_ERR_PARAM;
-  // flag_resi 1: a fixed eta field (FP64 form); with conduction the margin would be 4
-  if (p->flag_resi != 0 && p->flag_resi != 1) return PIP_ERR_PARAM;
-  if (p->flag_resi == 1 && (p->precision != PIP_FP64 || p->flag_heat != 0)) return PIP_ERR_PARAM;
+  // flag_resi 1: a fixed eta field, 2: set_resistivity resi_type 2 or 3 at every stage (FP64
+  // form); with conduction the margin would be 4
+  if (p->flag_resi < 0 || p->flag_resi > 2) return PIP_ERR_PARAM;
+  if (p->flag_resi >= 1 && (p->precision != PIP_FP64 || p->flag_heat != 0)) return PIP_ERR_PARAM;
+  if (p->flag_resi == 2 && p->resi_type != 2 && p->resi_type != 3) return PIP_ERR_PARAM;
+  if (p->flag_resi == 2 && p->resi_type == 3 && !(p->vd_cri > 0.0)) return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW && p->flag_ir != PIP_IR_POPESCU &&
       p->flag_ir != PIP_IR_POPESCU_EQ && p->flag_ir != PIP_IR_JEFFERY)
@@ -259,6 +263,10 @@ void build_kparams(pip_ctx *c) {
   k.col_type = p.flag_col >= 2 ? p.flag_col - 1 : 0;
   k.resi = p.flag_resi;
   k.resi_dt = INFINITY;
+  k.resi_type = p.resi_type;
+  k.eta0 = p.eta_0;
+  k.j_cri = p.j_cri;
+  k.vd_cri = p.vd_cri;
   k.ac_b2g = p.beta / 2.0 * p.gm;
   k.ac_sb = std::sqrt(k.ac_b2g);
   for (int s = 0; s < 2; ++s) {
@@ -417,7 +425,7 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
 // since the last one: set_collisional (alpha_c per cell) and set_IR (types 1-3) rewrite the
 // energies and set their fields before the first cfl and the first stage.
 int ensure_coefficients(pip_ctx *c) {
-  if ((!c->kp.col_type && !c->kp.irl) || c->coef_valid) return PIP_OK;
+  if ((!c->kp.col_type && !c->kp.irl && c->kp.resi != 2) || c->coef_valid) return PIP_OK;
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   c->coef_valid = true;
   return PIP_OK;
@@ -569,7 +577,12 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
   c->kp.dx = c->d_dx;
   c->kp.dy = c->d_dy;
   if ((e = cudaMalloc(&c->d_dt, sizeof(double))) != cudaSuccess) return fail(e);
-  if (c->kp.resi) {
+  if (c->kp.resi == 2) {
+    // eta follows the state: the bound of the eta of the last set_resistivity
+    if ((e = cudaMalloc(&c->d_resi, sizeof(unsigned long long))) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->d_resi, 0, sizeof(unsigned long long))) != cudaSuccess) return fail(e);
+    c->kp.resi_bound = c->d_resi;
+  } else if (c->kp.resi) {
     // set_resistivity type 0 until pip_set_resistivity gives another field
     std::vector<double> eta((size_t)c->kp.nc, p->eta_0);
     if ((e = cudaMalloc(&c->etaf, c->plane_bytes())) != cudaSuccess) return fail(e);
@@ -627,6 +640,7 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->d_dt);
   cudaFree(c->acf);
   cudaFree(c->etaf);
+  cudaFree(c->d_resi);
   cudaFree(c->irg);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
@@ -742,19 +756,23 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
-  if (c->hc) {
+  if (c->hc || c->kp.resi == 2) {
     // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
     // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
-    // BiCGstab's convergence checks anyway, so no graph
+    // BiCGstab's convergence checks anyway, so no graph.  Per-stage eta: whether a step
+    // was the last is known only once stage 2 has lowered its time increment to cfl_resi's
+    // bound, so the next cfl's rewrite cannot be fused into stage 2 either.
     long long n = 0;
     int total_it = 0;
     for (;;) {
       CK(do_stage(c, 1, 1, 0));
       CK(do_stage(c, 2, 1, 0));
-      int it = 0, hst = 0;
-      const int r = conduct(c, &c->ctrl->dt, &it, nullptr, &hst);
-      if (r != PIP_OK) return r;
-      total_it += it;
+      if (c->hc) {
+        int it = 0, hst = 0;
+        const int r = conduct(c, &c->ctrl->dt, &it, nullptr, &hst);
+        if (r != PIP_OK) return r;
+        total_it += it;
+      }
       if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
       if (h.nan_flag || h.status || h.step != n + 1) break;
       CK(do_cfl(c, (int)(n & 1)));          // the cfl after run_solver (main.f90:47)
@@ -942,9 +960,26 @@ int pip_set_alpha_c(pip_ctx *c, const double *ac) {
   return PIP_OK;
 }
 
+int pip_resi_dt(pip_ctx *c, double *bound) {
+  if (!c || !bound) return PIP_ERR_NULL;
+  if (!c->kp.resi) return PIP_ERR_PARAM;
+  if (c->kp.resi == 1) {
+    *bound = c->kp.resi_dt;
+    return PIP_OK;
+  }
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  if (ensure_coefficients(c)) return PIP_ERR_CUDA;
+  unsigned long long b = 0;
+  CK(cudaMemcpyAsync(&b, c->d_resi, sizeof b, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(bound, &b, sizeof(double));
+  return PIP_OK;
+}
+
 int pip_set_resistivity(pip_ctx *c, const double *eta) {
   if (!c || !eta) return PIP_ERR_NULL;
-  if (!c->kp.resi) return PIP_ERR_PARAM;
+  if (c->kp.resi != 1) return PIP_ERR_PARAM;   // none, or eta computed from the state
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(cudaStreamSynchronize(c->stream));      // no queued kernel still reads the field
   CK(cudaMemcpy(c->etaf, eta, c->plane_bytes(), cudaMemcpyHostToDevice));
@@ -1005,6 +1040,13 @@ int pip_conduction(pip_ctx *c, double dt, int *iters, double *relres) {
   return st == 0 ? PIP_OK : PIP_ERR_ITER;
 }
 
+int pip_set_hc_wait_limit(pip_ctx *c, int polls) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->hc) return PIP_ERR_PARAM;
+  pip::hc_set_wait_limit(c->hc, polls);
+  return PIP_OK;
+}
+
 int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
   if (!c || !neighbor) return PIP_ERR_NULL;
   bool any = false;
@@ -1013,8 +1055,9 @@ int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
     if (f >= 2 * c->kp.ndim && neighbor[f] != -1) return PIP_ERR_PARAM;
     any = any || neighbor[f] >= 0;
   }
-  // the conduction matrix folds every side of the block (one rank per direction)
-  if (any && c->hc) return PIP_ERR_PARAM;
+  // the conduction matrix folds every side of the block (one rank per direction); with eta
+  // recomputed at every stage each rank advances its time by its own cfl_resi bound
+  if (any && (c->hc || c->kp.resi == 2)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (c->stream) CK(cudaStreamSynchronize(c->stream));
   if (c->graph) {

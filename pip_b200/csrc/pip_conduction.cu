@@ -69,6 +69,7 @@ struct Scal {
   double relres, tol;
   int count, hc_max, done, fault;
   unsigned int blocks_done;
+  int wait_limit;                 // polls of a staging mbarrier before a block gives up
 };
 
 __device__ __forceinline__ bool interior_cell(const KParams &p, long long t, int &i, int &j) {
@@ -329,9 +330,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0u;
 }
-// Bounded wait on phase `parity` of bar; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int k = 0; k < kWaitLimit; ++k)
+// Bounded wait on phase `parity` of bar; false when `limit` polls ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
+  for (int k = 0; k < limit; ++k)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -411,7 +412,8 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
   constexpr int NCP = n_copies<KIND>();
   Scal *sc = a.sc;
-  if (sc->done) return;
+  if (sc->done || sc->fault) return;
+  const int wait_limit = sc->wait_limit;
   extern __shared__ __align__(128) unsigned char smem[];
   T *buf = reinterpret_cast<T *>(smem);
   unsigned long long *bar =
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
   int g = 0;
   for (; g < ngroups; ++g) {
     const int st = g % NS;
-    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((g / NS) & 1));
+    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((g / NS) & 1), wait_limit);
     if (__syncthreads_or(!ok)) {
       fault = true;
       break;
@@ -609,12 +611,13 @@ __global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArg
     if (t < 32 && g + NS < ngroups) issue(g + NS);
   }
   if (fault) {
-    // a staged group never arrived: flag it, let the copies still in flight land (bounded),
-    // and leave the scalars alone (the host reads the flag and stops)
+    // a staged group never arrived: flag it, let the copies still in flight land (bounded
+    // by the default limit, whatever the limit of the waits above), and leave the scalars
+    // alone (the host reads the flag and stops; later kernels of the solve return at once)
     if (t == 0) {
       atomicExch(&sc->fault, 1);
       for (int k = g; k < ngroups && k < g + NS; ++k)
-        mbar_wait(smem_addr(&bar[k % NS]), (uint32_t)((k / NS) & 1));
+        mbar_wait(smem_addr(&bar[k % NS]), (uint32_t)((k / NS) & 1), kWaitLimit);
     }
     return;
   }
@@ -674,9 +677,10 @@ __global__ void correct_kernel(const KParams p, double *x, const float *__restri
   x[q] = x[q] + (double)d[q];
 }
 
-__global__ void set_scal_kernel(Scal *sc, double tol, int hc_max) {
+__global__ void set_scal_kernel(Scal *sc, double tol, int hc_max, int wait_limit) {
   sc->tol = tol;
   sc->hc_max = hc_max;
+  sc->wait_limit = wait_limit;
   sc->done = 0;
   sc->fault = 0;
   sc->count = 0;
@@ -756,7 +760,12 @@ struct HcEngine {
   double *part = nullptr;
   hc::Scal *sc = nullptr, *sc32 = nullptr;
   hc::Scal *h_sc = nullptr;         // pinned
+  int wait_limit = hc::kWaitLimit;  // polls of a staging mbarrier (hc_set_wait_limit)
 };
+
+void hc_set_wait_limit(HcEngine *e, int polls) {
+  if (e) e->wait_limit = polls < 0 ? hc::kWaitLimit : polls;
+}
 
 void hc_destroy(HcEngine *e) {
   if (!e) return;
@@ -837,7 +846,7 @@ cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T 
                      T *const (&ap)[2], T *tv, hc::Scal *sc, double tol, int hc_max,
                      cudaStream_t s, hc::Scal *h) {
   using namespace hc;
-  set_scal_kernel<<<1, 1, 0, s>>>(sc, tol, hc_max);
+  set_scal_kernel<<<1, 1, 0, s>>>(sc, tol, hc_max, e->wait_limit);
   launch<T, KINIT>(gr, k, make_args<T>(m, g, {x[0]}, {b}, {r, r0, pv[0]}, e->part, sc), s);
   const int group = 4;
   for (int it = 0; it <= hc_max; it += group) {
@@ -861,7 +870,7 @@ cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T 
 // The FP64 residual r = b - A x[0] (r0 = p = r as well) and its scalars into h.
 cudaError_t residual64(HcEngine *e, const KParams &k, double tol, cudaStream_t s, hc::Scal *h) {
   using namespace hc;
-  set_scal_kernel<<<1, 1, 0, s>>>(e->sc, tol, 0);
+  set_scal_kernel<<<1, 1, 0, s>>>(e->sc, tol, 0, e->wait_limit);
   launch<double, KINIT>(e->grid64, k,
                         make_args<double>(e->m64, e->g64, {e->x[0]}, {e->b}, {e->r, e->r0, e->p[0]},
                                           e->part, e->sc),

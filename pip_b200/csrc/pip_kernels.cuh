@@ -42,8 +42,13 @@ struct KParams {
   double ir_factor, ir_ionfac;  // set_IR type 1: factor = exp(-13.2/(T0/11605)), ion_fac
   double *irg;       // type 1: Gm_ion (nc values) then Gm_rec (nc values) of the last set_IR
   double *acf;       // alpha_c per cell of the last set_collisional (col_type >= 1), nc values
-  int resi;          // flag_resi 1: resistive flux (eta field etaf), FP64 form
-  const double *etaf;  // eta per cell, nc values
+  int resi;          // flag_resi 1: resistive flux with the fixed eta field etaf; 2: eta from
+                     // the stage state at every RK stage (resi_type), FP64 form
+  const double *etaf;  // eta per cell, nc values (resi 1)
+  int resi_type;       // resi 2: set_resistivity resi_type 2 (|curl B| switch) or 3 (drift law)
+  double eta0, j_cri, vd_cri;  // eta_0 and the thresholds of resi_type 2 and 3
+  unsigned long long *resi_bound;  // resi 2: cfl_resi's bound (ordered bits of a positive
+                                   // double) of the eta of the last set_resistivity
   double resi_dt;    // cfl_resi's bound min(safety*gmin^2/max(eta,1e-8)) over the interior
                      // cells (+inf without resistivity); seeds the min-CFL reduction slot
   const double *dx, *dy;
@@ -94,6 +99,9 @@ namespace pip {
 struct HcEngine;
 cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out);
 void hc_destroy(HcEngine *e);
+// Polls of a staging mbarrier before a BiCGstab block gives up and flags the solve as
+// failed (polls < 0: the default); applies from the next solve.
+void hc_set_wait_limit(HcEngine *e, int polls);
 cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, double tol,
                    int hc_max, cudaStream_t s, int *iters, double *relres, int *status);
 

@@ -379,11 +379,16 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
 // E = eta*curl B of one cell (get_rotation's s_order-2 branch, Util_rot.f90:148-236, and
 // resistive_flux's ex, ey, ez, Solver_rot.f90:597-599) from the field planes bx, by, bz
 // with row stride sy; gi, gj the cell's global indices (never on the outermost layer).
+//
+// With resi 2 the cell's eta is set_resistivity's (Res_rot.f90:37-60) from this curl B and
+// the ion density ro[c]: resi_type 2 11 eta_0 where |curl B| >= j_cri, else eta_0;
+// resi_type 3 eta_0 (vd/vd_cri - 1)**2 where vd = |curl B|/rho_i >= vd_cri, else 0.  The
+// cell's eta is returned in eta.
 template <int NDIM>
 __device__ __forceinline__ void cell_e(const double *bx, const double *by, const double *bz,
-                                       long long c, long long sy, const KParams &p, int gi, int gj,
-                                       double &ex, double &ey, double &ez) {
-  const double eta = p.etaf[(long long)gj * p.ix + gi];
+                                       const double *ro, long long c, long long sy,
+                                       const KParams &p, int gi, int gj, double &ex, double &ey,
+                                       double &ez, double &eta) {
   double r1 = 0.0, r2, r3;
 #if PIP_RCP
   // the FMA build multiplies by 1/(2 dx), 1/(2 dy)
@@ -407,6 +412,18 @@ __device__ __forceinline__ void cell_e(const double *bx, const double *by, const
     r3 = (by[c + 1] - by[c - 1]) / dx2;
   }
 #endif
+  if (p.resi == 2) {
+    const double c2 = sqrt(r1 * r1 + r2 * r2 + r3 * r3);
+    if (p.resi_type == 2) {
+      eta = c2 >= p.j_cri ? p.eta0 * 11.0 : p.eta0;
+    } else {
+      const double vd = c2 / ro[c];
+      const double a = vd / p.vd_cri - 1.0;
+      eta = vd >= p.vd_cri ? p.eta0 * (a * a) : 0.0;
+    }
+  } else {
+    eta = p.etaf[(long long)gj * p.ix + gi];
+  }
   ex = r1 * eta;
   ey = r2 * eta;
   ez = r3 * eta;
@@ -431,16 +448,17 @@ __device__ __forceinline__ void face_terms(double *F, long long nf, long long fo
 }
 
 // The face terms of the face between cells c0 and c1 = c0 + (x: 1, y: sy) of the field
-// planes, E computed at both cells (the unit-level flux kernel).
+// planes, E computed at both cells (the unit-level flux kernel; ro the ion density plane).
 template <int NDIM>
 __device__ __forceinline__ void add_resistive(double *F, long long nf, long long fo, bool ydir,
                                               const double *bx, const double *by, const double *bz,
-                                              long long c0, long long sy, const KParams &p,
-                                              int gi, int gj) {
-  double ex0, ey0, ez0, ex1, ey1, ez1;
+                                              const double *ro, long long c0, long long sy,
+                                              const KParams &p, int gi, int gj) {
+  double ex0, ey0, ez0, ex1, ey1, ez1, e0, e1;
   const long long c1 = ydir ? c0 + sy : c0 + 1;
-  cell_e<NDIM>(bx, by, bz, c0, sy, p, gi, gj, ex0, ey0, ez0);
-  cell_e<NDIM>(bx, by, bz, c1, sy, p, ydir ? gi : gi + 1, ydir ? gj + 1 : gj, ex1, ey1, ez1);
+  cell_e<NDIM>(bx, by, bz, ro, c0, sy, p, gi, gj, ex0, ey0, ez0, e0);
+  cell_e<NDIM>(bx, by, bz, ro, c1, sy, p, ydir ? gi : gi + 1, ydir ? gj + 1 : gj, ex1, ey1, ez1,
+               e1);
   face_terms(F, nf, fo, ydir, ex0, ey0, ez0, ex1, ey1, ez1, bx[c0], bx[c1], by[c0], by[c1], bz[c0],
              bz[c1]);
 }
@@ -485,6 +503,21 @@ __device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ 
 // instance: bit 0 set_coefficients at every stage (alpha_c per cell, col_type >= 1, and/or
 // the Popescu IR rates), bit 1 resistivity; each combination is its own instance so that
 // the others keep their register budget.
+// Minimum of v over the block, taken into *dst (ordered bits of positive doubles) by one
+// atomic per block.  Every thread of the block calls it.
+template <int NT>
+__device__ __forceinline__ void block_min_to(double v, unsigned long long *dst) {
+  __shared__ double s_min[NT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (threadIdx.x % 32 == 0) s_min[threadIdx.x / 32] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NT / 32; ++k) v = fmin(v, s_min[k]);
+    atomicMin(dst, dbits(v));
+  }
+}
+
 template <int NDIM, int NVM, int STAGE, int X>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
 stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
@@ -552,6 +585,12 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     ctrl->red_gr[ns] = 0ull;
   }
 
+  if (STAGE == 1 && RES && p.resi == 2 && block0 && tid == 0) {
+    // stage 2 takes the minimum of cfl_resi's bound into this word; no kernel reads it
+    // between the stages
+    *p.resi_bound = dbits(INFINITY);
+  }
+
   const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
   const int i0 = p.m0 + blockIdx.x * TX;
   const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
@@ -582,19 +621,29 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
   }
   __syncthreads();
+  // resi 2, stage 2: cfl_resi's bound over this tile's interior cells with the eta of this
+  // stage (the last set_resistivity before the next cfl)
+  double rb = INFINITY;
   if (RES) {
     // E = eta*curl B once per cell of the tile and its first ring (each enters four faces)
+    const int iend_ = p.m0 + p.nx, jend_ = NDIM == 2 ? p.m1 + p.ny : 1;
     for (int idx = tid; idx < EN; idx += NT) {
       const int er = idx % EW, ej = idx / EW;
       const int gi = i0 - 1 + er, gj = NDIM == 2 ? j0 - 1 + ej : 0;
       if (gi > p.ix - 2 || (NDIM == 2 && gj > p.jx - 2)) continue;
       const int c = (NDIM == 2 ? (ej + kH - 1) * RX : 0) + er + kH - 1;
-      double ex, ey, ez;
-      cell_e<NDIM>(sV + 5 * RR, sV + 6 * RR, sV + 7 * RR, c, RX, p, gi, gj, ex, ey, ez);
+      double ex, ey, ez, eta;
+      cell_e<NDIM>(sV + 5 * RR, sV + 6 * RR, sV + 7 * RR, sV, c, RX, p, gi, gj, ex, ey, ez, eta);
       sE[idx] = ex;
       sE[EN + idx] = ey;
       sE[2 * EN + idx] = ez;
+      if (STAGE == 2 && p.resi == 2 && er >= 1 && er <= TX && gi < iend_ &&
+          (NDIM == 1 || (ej >= 1 && ej <= TY && gj < jend_))) {
+        const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+        rb = fmin(rb, p.safety * (gmin * gmin) / fmax(eta, 1.0e-8));
+      }
     }
+    if (STAGE == 2 && p.resi == 2) block_min_to<NT>(rb, p.resi_bound);
     __syncthreads();
   }
 
@@ -854,6 +903,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   }
   if (STAGE == 2 && COL && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
   if (STAGE == 2 && s_epi == 2) {
+    if (RES && p.resi == 2) dtc = fmin(dtc, rb);  // the next step's cfl_resi
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
   }
   if (STAGE == 2 && dt_mode == 1) {
@@ -866,7 +916,16 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       if (atomicAdd(&ctrl->blocks_done, 1u) == nb - 1) {
         __threadfence();
         ctrl->blocks_done = 0u;
-        ctrl->time = ctrl->time_next;
+        if (RES && p.resi == 2) {
+          // the cfl after run_solver lowers the global dt that time advances by to
+          // cfl_resi's bound of this stage's eta (main.f90:47,58; Scheme_rot.f90:298)
+          const double tn = ctrl->time + fmin(dt, bitsd(atomicOr(p.resi_bound, 0ull)));
+          ctrl->time = tn;
+          ctrl->last = ((ctrl->t_end > 0.0 && tn >= ctrl->t_end) ||
+                        (ctrl->nsteps > 0 && s_step + 1 >= ctrl->nsteps)) ? 1 : 0;
+        } else {
+          ctrl->time = ctrl->time_next;
+        }
         ctrl->step = s_step + 1;
         if (ctrl->last) ctrl->done = 1;
         if (dt <= 1.0e-12) {
@@ -886,6 +945,9 @@ __global__ void __launch_bounds__(256) cfl_kernel(const KParams p, double *U, De
                                                   int slot) {
   const double gm = p.gm;
   double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  // cfl_resi with the eta of the last set_resistivity (resi 2; a fixed field's bound is
+  // seeded into the slot by the host)
+  if (p.resi == 2 && blockIdx.x == 0 && threadIdx.x == 0) dtc = bitsd(*p.resi_bound);
   const long long nc = p.nc;
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
     double um[NVM], uh[5];
@@ -1016,9 +1078,10 @@ __global__ void flux_kernel(const KParams p, const double *__restrict__ U, doubl
       }
       if (p.resi) {
         if (p.ndim == 2)
-          add_resistive<2>(F, nc, qa, py, U + 5 * nc, U + 6 * nc, U + 7 * nc, qa, p.ix, p, i, j);
+          add_resistive<2>(F, nc, qa, py, U + 5 * nc, U + 6 * nc, U + 7 * nc, U, qa, p.ix, p, i, j);
         else
-          add_resistive<1>(F, nc, qa, false, U + 5 * nc, U + 6 * nc, U + 7 * nc, qa, p.ix, p, i, j);
+          add_resistive<1>(F, nc, qa, false, U + 5 * nc, U + 6 * nc, U + 7 * nc, U, qa, p.ix, p, i,
+                           j);
       }
     }
     {
@@ -1110,6 +1173,25 @@ __global__ void coefficients_kernel(const KParams p, double *U) {
     U[q + (NVM + 4) * nc] = uh[4];
   }
 }
+
+// set_resistivity resi_type 2 or 3 over the state as it stands (the prologue's
+// set_coefficients, Initial_rot.f90:140): cfl_resi's bound of that eta over the interior
+// cells into *p.resi_bound (set to +inf before by resi_reset_kernel).
+template <int NDIM>
+__global__ void __launch_bounds__(256) resi_bound_kernel(const KParams p, const double *U) {
+  const long long nc = p.nc, n = (long long)p.nx * p.ny;
+  double rb = INFINITY;
+  for (long long t = blockIdx.x * 256ll + threadIdx.x; t < n; t += (long long)gridDim.x * 256) {
+    const int gi = p.m0 + (int)(t % p.nx), gj = p.m1 + (int)(t / p.nx);
+    const long long q = (long long)gj * p.ix + gi;
+    double ex, ey, ez, eta;
+    cell_e<NDIM>(U + 5 * nc, U + 6 * nc, U + 7 * nc, U, q, p.ix, p, gi, gj, ex, ey, ez, eta);
+    const double gmin = fmin(fmin(p.dx[gi], NDIM == 2 ? p.dy[gj] : p.dy[0]), p.dz0);
+    rb = fmin(rb, p.safety * (gmin * gmin) / fmax(eta, 1.0e-8));
+  }
+  block_min_to<256>(rb, p.resi_bound);
+}
+__global__ void resi_reset_kernel(unsigned long long *b) { *b = dbits(INFINITY); }
 
 __global__ void nan_kernel(const double *__restrict__ U, long long n, int *flag) {
   int bad = 0;
@@ -1235,7 +1317,13 @@ static cudaError_t launch_source(const KParams &p, double *U, double *S, double 
 }
 
 static cudaError_t launch_coefficients(const KParams &p, double *U, cudaStream_t s) {
-  if (!p.col_type && !p.irl) return cudaSuccess;
+  if (p.resi == 2) {  // set_resistivity comes first in set_coefficients; it reads B and rho
+    resi_reset_kernel<<<1, 1, 0, s>>>(p.resi_bound);
+    const long long n = (long long)p.nx * p.ny;
+    if (p.ndim == 2) resi_bound_kernel<2><<<grid_for(n, 256), 256, 0, s>>>(p, U);
+    else resi_bound_kernel<1><<<grid_for(n, 256), 256, 0, s>>>(p, U);
+  }
+  if (!p.col_type && !p.irl) return cudaGetLastError();
   if (p.nvm == 9) coefficients_kernel<9><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   else coefficients_kernel<8><<<grid_for(p.nc, 256), 256, 0, s>>>(p, U);
   return cudaGetLastError();

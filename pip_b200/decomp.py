@@ -241,8 +241,10 @@ class DeviceBlock:
         self.ctx = Context(block.settings)
         self.ctx.set_neighbors(block.neighbor)
         self.ctx.upload(U_h, U_m)
-        if eta is None and block.settings.flag_resi and (block.settings.flag_resi // 10) % 10:
-            eta = block.settings.eta_field()
+        if eta is None and block.settings.flag_resi and block.settings.resi_type:
+            # resi_type 2, 3 set once at the prologue (flag_resi 21, 31): from the block's
+            # state, its ghost layers as uploaded
+            eta = block.settings.eta_field(U_m if block.settings.resi_type >= 2 else None)
         if eta is not None:
             self.ctx.set_resistivity(eta)
         self.device = torch.device("cuda", device)

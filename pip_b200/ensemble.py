@@ -99,3 +99,41 @@ def shock_tube_ensemble(n_runs: int = 512, seed: int = 4242, nx_max: Optional[in
             m = dict(m, nx=min(m["nx"], nx_max))
         out.append(ics.shock_tube_member(**m))
     return out
+
+
+def fp64_single_run_errors(members: Sequence[Tuple[Settings, np.ndarray, np.ndarray]],
+                           results: Sequence[Tuple[np.ndarray, np.ndarray, float, int, int]],
+                           workers: int = 8):
+    """Each ensemble member against its own single-run FP64 solve (a context of the plain
+    FP64 path, from the same initial state, the same number of steps).
+
+    results[r] is Ensemble.member(r).  Returns one (relative L1 per variable over the
+    interior cells, ion planes then neutral planes; |time difference| / time) per member.
+    The single runs go to `workers` host threads, each with its own context and stream (the
+    C ABI calls release the GIL), so several run on the GPU at once.
+    """
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .params import PIP_FP64
+
+    def one(r):
+        s, U_h, U_m = members[r]
+        eh, em, t, n, _ = results[r]
+        with capi.Context(s.overrides(precision=PIP_FP64)) as c:
+            c.upload(U_h, U_m)
+            c.prologue()
+            st, t64, n64 = c.run(nsteps=n)
+            if st != 0 or n64 != n:
+                raise RuntimeError("FP64 single run %d ended with status %d after %d of %d steps"
+                                   % (r, st, n64, n))
+            h64, m64 = c.download()
+        m0 = s.margin[0]
+        num = [np.abs(a[:, :, m0:-m0] - b[:, :, m0:-m0]).sum(axis=(1, 2))
+               for a, b in ((em, m64), (eh, h64))]
+        den = [np.abs(b[:, :, m0:-m0]).sum(axis=(1, 2)) for b in (m64, h64)]
+        num, den = np.concatenate(num), np.concatenate(den)
+        l1 = np.where(den > 0, num / np.where(den > 0, den, 1.0), num)
+        return l1, abs(t - t64) / t64
+
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(one, range(len(members))))

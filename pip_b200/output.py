@@ -146,7 +146,11 @@ def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np
             raise ValueError("flag_col %d writes the alpha_c field: pass ac" % s.flag_col)
         planes["ac"] = np.asarray(ac).reshape(U_h.shape[1:])
     if s.flag_resi:
-        planes["et"] = (s.eta_field() if eta is None else np.asarray(eta)).reshape(U_h.shape[1:])
+        # resi_type 2 and 3: eta of the written state by default (the reference writes the
+        # eta of its last set_resistivity, from the last RK stage's state)
+        if eta is None:
+            eta = s.eta_field(U_m if s.resi_type in (2, 3) else None)
+        planes["et"] = np.asarray(eta).reshape(U_h.shape[1:])
     planes.update({VAR_M[n]: U_m[n] for n in range(s.nvar_m)})
     if s.flag_ir != PIP_IR_NONE:
         planes["ion"], planes["rec"] = ir_rates(s, U_m)

@@ -56,7 +56,8 @@ class PipParams(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("fp_exact", ctypes.c_int32),
         ("flag_resi", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 5),
+        ("resi_type", ctypes.c_int32),
+        ("reserved_i", ctypes.c_int32 * 4),
         ("gm", ctypes.c_double),
         ("safety", ctypes.c_double),
         ("ro_lim", ctypes.c_double),
@@ -74,7 +75,9 @@ class PipParams(ctypes.Structure):
         ("eta_0", ctypes.c_double),
         ("t_norm", ctypes.c_double),
         ("n_norm", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 3),
+        ("j_cri", ctypes.c_double),
+        ("vd_cri", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 1),
         ("dx", ctypes.POINTER(ctypes.c_double)),
         ("dy", ctypes.POINTER(ctypes.c_double)),
         ("dz", ctypes.POINTER(ctypes.c_double)),
@@ -134,8 +137,11 @@ class Settings:
     kapper: float = 0.0
     hc_max: int = 500
     hc_error: float = 1.0e-10
-    flag_resi: int = 0          # 10*resi_type + 1 (Res_rot.f90:8-15): 1 uniform, 11 localised
+    flag_resi: int = 0          # 10*resi_type + flag (Res_rot.f90:8-15): 1 uniform, 11 localised;
+                                # 21/31 anomalous eta set once at the prologue, 22/32 at every stage
     eta_0: float = 0.0
+    j_cri: float = 0.0          # resi_type 2 threshold on |curl B|
+    vd_cri: float = 0.0         # resi_type 3 threshold on the drift |curl B|/rho_i
     t_norm: float = 0.0         # setting key T_norm (K)
     n_norm: float = 0.0         # setting key n_norm
     debug_parameter: float = 0.0
@@ -221,12 +227,46 @@ class Settings:
             out.append(c)
         return out[0], out[1], out[2], dx, dy, dz
 
-    def eta_field(self) -> np.ndarray:
+    @property
+    def resi_type(self) -> int:
+        """initialize_resistivity's resi_type = mod(flag_resi/10, 10) (Res_rot.f90:12)."""
+        return (self.flag_resi // 10) % 10
+
+    def eta_field(self, U_m: np.ndarray = None) -> np.ndarray:
         """set_resistivity's eta (Res_rot.f90:16-60) as (jx, ix): resi_type 0 eta_0
-        everywhere, resi_type 1 eta_0*exp(-((x/0.8)**2 + ((y-debug_parameter)/0.8)**2))."""
+        everywhere, resi_type 1 eta_0*exp(-((x/0.8)**2 + ((y-debug_parameter)/0.8)**2)),
+        resi_type 2 and 3 from |curl B| of the ion state U_m (nvar_m, jx, ix) (get_rotation's
+        central differences, zero on the outermost layer): type 2 11 eta_0 where
+        |curl B| >= j_cri, else eta_0; type 3 eta_0 (vd/vd_cri - 1)**2 where
+        vd = |curl B|/rho_i >= vd_cri, else 0."""
         x, y, _, _, _, _ = self.coordinates()
         ix, jx, _ = self.shape
-        if (self.flag_resi // 10) % 10 == 1:
+        if self.resi_type in (2, 3):
+            if U_m is None:
+                raise ValueError("resi_type %d: eta depends on the state; pass U_m" % self.resi_type)
+            _, _, _, dx, dy, _ = self.coordinates()
+            bx, by, bz = (np.asarray(U_m[n], dtype=np.float64) for n in (5, 6, 7))
+            r1 = np.zeros_like(bx)
+            r2 = np.zeros_like(bx)
+            r3 = np.zeros_like(bx)
+            if self.ndim == 1:
+                d2 = (2.0 * dx[1:-1])[None, :]
+                r2[:, 1:-1] = -(bz[:, 2:] - bz[:, :-2]) / d2
+                r3[:, 1:-1] = (by[:, 2:] - by[:, :-2]) / d2
+            else:
+                dx2 = (2.0 * dx[1:-1])[None, :]
+                dy2 = (2.0 * dy[1:-1])[:, None]
+                c = (slice(1, -1), slice(1, -1))
+                r1[c] = (bz[2:, 1:-1] - bz[:-2, 1:-1]) / dy2
+                r2[c] = -(bz[1:-1, 2:] - bz[1:-1, :-2]) / dx2
+                r3[c] = (by[1:-1, 2:] - by[1:-1, :-2]) / dx2 - (bx[2:, 1:-1] - bx[:-2, 1:-1]) / dy2
+            c2 = np.sqrt(r1 * r1 + r2 * r2 + r3 * r3)
+            if self.resi_type == 2:
+                return np.where(c2 >= self.j_cri, self.eta_0 * 11.0, self.eta_0)
+            vd = c2 / np.asarray(U_m[0], dtype=np.float64)
+            a = vd / self.vd_cri - 1.0
+            return np.where(vd >= self.vd_cri, self.eta_0 * (a * a), 0.0)
+        if self.resi_type == 1:
             ax = x / 0.8
             ay = (y - self.debug_parameter) / 0.8
             return self.eta_0 * np.exp(-(ax[None, :] * ax[None, :] + ay[:, None] * ay[:, None]))
@@ -250,11 +290,13 @@ class Settings:
             bad.append("flag_col 2..7 (alpha_c per cell) needs precision PIP_FP64")
         elif self.flag_col in (2, 4, 6) and not self.beta > 0.0:
             bad.append("flag_col %d divides by sqrt(beta*gm/2): beta must be > 0" % self.flag_col)
-        if self.flag_resi not in (0, 1, 11):
-            bad.append("flag_resi must be 0, 1 (uniform eta_0) or 11 (localised eta), "
-                       "a fixed eta field")
+        if self.flag_resi % 10 not in (0, 1, 2) or self.resi_type not in (0, 1, 2, 3) or \
+                self.flag_resi >= 100:
+            bad.append("flag_resi must be 10*resi_type + 1 or 2 with resi_type 0..3")
         elif self.flag_resi and (self.precision != PIP_FP64 or self.flag_heat):
             bad.append("resistivity needs precision PIP_FP64 and no conduction")
+        elif self.resi_type == 3 and not self.vd_cri > 0.0:
+            bad.append("resi_type 3 divides by vd_cri: vd_cri must be > 0")
         if self.flag_amb or self.flag_visc or self.flag_grav:
             bad.append("ambipolar diffusion, viscosity and gravity are not supported")
         set_ir_laws = (PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ)
@@ -319,7 +361,13 @@ class Settings:
         p.kapper = self.kapper
         p.hc_error = self.hc_error
         p.beta = self.beta
-        p.flag_resi = self.flag_resi % 10
+        # per-stage eta only where it depends on the state; a per-stage resi_type 0 or 1
+        # field is the same at every stage, a fixed field
+        flag = self.flag_resi % 10
+        p.flag_resi = 2 if (flag == 2 and self.resi_type in (2, 3)) else (1 if flag else 0)
+        p.resi_type = self.resi_type
+        p.j_cri = self.j_cri
+        p.vd_cri = self.vd_cri
         p.eta_0 = self.eta_0
         p.t_norm = self.t_norm
         p.n_norm = self.n_norm
@@ -345,7 +393,8 @@ class Settings:
                  "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
                  "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",
                  "kapper": "kapper", "tend": "tend", "beta": "beta", "eta_0": "eta_0",
-                 "debug_parameter": "debug_parameter", "T_norm": "t_norm", "n_norm": "n_norm"}
+                 "debug_parameter": "debug_parameter", "T_norm": "t_norm", "n_norm": "n_norm",
+                 "j_cri": "j_cri", "vd_cri": "vd_cri"}
         bnd = {"flag_bnd_x_l": 0, "flag_bnd_x_r": 1, "flag_bnd_y_l": 2, "flag_bnd_y_r": 3,
                "flag_bnd_z_l": 4, "flag_bnd_z_r": 5}
         for raw in text.splitlines():

@@ -136,3 +136,37 @@ def test_run_with_conduction_and_alpha_c_per_cell(gpu_lib):
     assert max(rel_l1(interior(gh, s), interior(oh, s)).max(),
                rel_l1(interior(gm, s), interior(om, s)).max()) <= 1e-10
     assert np.abs(ac_g - ac_o).sum() <= 1e-10 * np.abs(ac_o).sum()
+
+
+@pytest.mark.parametrize("precision", [PIP_FP64, PIP_MIXED])
+def test_expired_staging_wait_is_reported_and_the_context_recovers(gpu_lib, precision):
+    """A BiCGstab block whose mbarrier wait runs out (here: a limit of zero polls, so the
+    first wait of every block runs out before its rows land) flags the solve instead of
+    waiting on; the call reports it and the same context then solves normally."""
+    import ctypes
+    s, o, Uh0, Um0 = kh_case(kapper=1.0)
+    dt, _ = o.cfl()
+    h0, m0 = o.state()
+    o.close()
+    s = s.overrides(precision=precision)
+    with capi.Context(s) as c:
+        c.upload(h0, m0)
+        ref = c.conduction(dt)
+        c.pipbnd()
+        rh, rm = c.download()
+    L = capi.lib()
+    with capi.Context(s) as c:
+        c.set_hc_wait_limit(0)
+        c.upload(h0, m0)
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        st = L.pip_conduction(c.h, float(dt), ctypes.byref(it), ctypes.byref(rr))
+        assert st == capi.PIP_ERR_CUDA, capi.strerror(st)
+        assert L.pip_last_cuda_error() == 702      # cudaErrorLaunchTimeout
+        c.set_hc_wait_limit(-1)
+        c.upload(h0, m0)
+        again = c.conduction(dt)
+        c.pipbnd()
+        gh, gm = c.download()
+    assert again == ref and ref[0] == 0
+    assert np.array_equal(gh, rh) and np.array_equal(gm, rm)

@@ -73,3 +73,38 @@ def test_autotuner_picks_a_valid_configuration(gpu_lib):
             b = f.member(r)
             assert a[r][3] == b[3]
             assert rel_l1(a[r][1], b[1]).max() <= 1e-6
+
+
+# The FP32-mixed form against FP64 on config 4's members, measured over all 512 (bench.py
+# "ensemble"): median 1.2e-6 relative L1, 24 members above 1e-5, the worst 4.4e-5 (large
+# grids with ion fractions of 0.05-0.15, on the small ion density or momentum).  The
+# single-run mixed form gives the same on those members (3-5e-5), so this is the precision
+# form's, not the batching's; members are held to the measured level.
+TOL_C4 = 1e-4
+
+
+def test_config4_members_match_their_fp64_single_runs(gpu_lib):
+    """Config 4 as stated: members of the seeded 512-run ensemble (seed 4242) to t = 0.1,
+    each against its own single-run FP64 solve.  The subset holds the largest grid, the
+    stiffest alpha_c, the largest pressure ratio and the smallest ion fraction of the 512,
+    plus four more drawn with a fixed seed."""
+    from pip_b200.ensemble import fp64_single_run_errors
+    spec = ics.ensemble_members(512, 4242)
+    pick = {max(range(512), key=lambda r: spec[r]["nx"]),
+            max(range(512), key=lambda r: spec[r]["col"]),
+            max(range(512), key=lambda r: spec[r]["pratio"]),
+            min(range(512), key=lambda r: spec[r]["ion_frac"])}
+    pick |= set(int(r) for r in np.random.default_rng(99).choice(512, 4, replace=False))
+    pick = sorted(pick)
+    mem = [ics.shock_tube_member(**spec[r]) for r in pick]
+    with Ensemble(mem) as e:
+        e.run(t_end=0.1)
+        res = [e.member(r) for r in range(len(mem))]
+    for (_, _, t, n, st) in res:
+        assert st == 0 and t >= 0.1
+    errs = fp64_single_run_errors(mem, res)
+    for r, (l1, dt_rel) in zip(pick, errs):
+        assert dt_rel <= 1e-5, (r, dt_rel)
+        print("member %d nx %d alpha_c %.3g: relative L1 %.2e" % (r, spec[r]["nx"], spec[r]["col"],
+                                                                 l1.max()))
+        assert l1.max() <= TOL_C4, (r, spec[r], l1)

@@ -28,10 +28,12 @@ def compare(s, Uh, Um, nsteps=0, t_end=0.0):
     return a, b, err_h, err_m
 
 
-# The Dedner potential psi is driven by div B, a truncation-level difference of B; FP32
-# flux rounding perturbs B by ~1e-7 relative, which is a large relative perturbation of
-# div B, so psi carries ~1e-3 relative L1 against FP64 while the 13 physical fields (8 MHD,
-# 5 hydro) stay at ~1e-7.  psi is held to this looser bound.
+# The Dedner potential psi does not meet the 1e-5 bar in this form, and no form that rounds
+# B to FP32 at every step can: test_psi_amplifies_white_noise_in_b shows the plain FP64
+# path itself moving psi by >1e-4 relative L1 from a one-time 1e-10 perturbation of B.
+# psi is ~1e-4 of |B| in size, and the grid-scale noise FP32 rounding puts into div B at
+# every step drives it.  Measured on OT 1024^2 after 2000 steps: psi 4e-3 while the 13
+# physical fields (8 MHD, 5 hydro) stay at ~5e-7.  psi is held to the measured level.
 TOL_PSI = 1e-2
 
 
@@ -45,6 +47,28 @@ def test_mixed_orszag_tang(gpu_lib):
     assert physical <= TOL_MIXED, (eh, em)
     assert em[8] <= TOL_PSI, em
 
+
+
+def test_psi_amplifies_white_noise_in_b(gpu_lib):
+    """The plain FP64 path alone, OT 1024^2: a one-time white relative perturbation of 1e-10
+    of Bx and By moves psi by more than 1e-4 relative L1 within 10 steps (the 13 physical
+    fields move by less than 1e-9).  The rounding-only change of the FMA-free build keeps
+    psi within 1e-7 over the same steps."""
+    s, Uh, Um = ics.orszag_tang(1024)
+    rng = np.random.default_rng(7)
+    Up = Um.copy()
+    for n in (5, 6):
+        Up[n] *= 1.0 + 1e-10 * rng.uniform(-1.0, 1.0, size=Up[n].shape)
+    a = run(s, Uh, Um, nsteps=10)
+    b = run(s, Uh, Up, nsteps=10)
+    c = run(s.overrides(fp_exact=1), Uh, Um, nsteps=10)
+    em = rel_l1(interior(b[3], s), interior(a[3], s))
+    eh = rel_l1(interior(b[2], s), interior(a[2], s))
+    print("psi after a 1e-10 B perturbation: %.3e; others max %.3e"
+          % (em[8], max(eh.max(), em[:8].max())))
+    assert em[8] > 1e-4
+    assert max(eh.max(), em[:8].max()) < 1e-9
+    assert rel_l1(interior(c[3], s), interior(a[3], s))[8] < 1e-7
 
 
 def test_mixed_brio_wu(gpu_lib):

@@ -62,6 +62,47 @@ def test_orszag_tang_64(gpu_lib, exact):
     assert_match(g, o, TOL_FP64, bitwise=bool(exact))
 
 
+_OT1024 = {}
+
+
+def ot1024_oracle():
+    """The oracle's 20 steps of config 2 at its full size, computed once per session."""
+    if not _OT1024:
+        import os
+        s, Uh, Um = ics.orszag_tang(1024)
+        st, t, n, oh, om, _ = O.run_case(s, Uh, Um, nsteps=20, threads=os.cpu_count() or 8)
+        _OT1024["o"] = (st, t, n, oh, om)
+    return _OT1024["o"]
+
+
+def test_orszag_tang_1024_full_size(gpu_lib):
+    """Config 2 on its stated grid, 1024x1024 (+2 ghosts per side), 20 steps, the FMA-free
+    build: bit for bit."""
+    s, Uh, Um = ics.orszag_tang(1024, fp_exact=1)
+    g = run_gpu(s, Uh, Um, nsteps=20)
+    assert_match(g, ot1024_oracle(), 0.0, bitwise=True)
+
+
+# The Dedner potential psi turns rounding differences into ~1e-8 relative differences within
+# the first steps of this run (psi is ~1e-4 of |B| and driven by the grid-scale part of
+# div B; test_gpu_mixed.py::test_psi_amplifies_white_noise_in_b); the FMA build rounds
+# differently from the FMA-free oracle, so its psi is held to this bound and the 13
+# physical fields to the drop-in bar.  The FMA-free build above meets the bar on all 14.
+TOL_PSI_FMA = 1e-7
+
+
+def test_orszag_tang_1024_full_size_fma(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(1024)
+    g = run_gpu(s, Uh, Um, nsteps=20)
+    o = ot1024_oracle()
+    assert g[0] == o[0] == 0 and g[2] == o[2]
+    assert abs(g[1] - o[1]) <= 1e-12 * o[1]
+    eh, em = rel_l1(g[3], o[3]), rel_l1(g[4], o[4])
+    print("FMA build vs oracle, 13 fields max %.3e, psi %.3e" % (max(eh.max(), em[:8].max()), em[8]))
+    assert max(eh.max(), em[:8].max()) <= TOL_FP64
+    assert em[8] <= TOL_PSI_FMA
+
+
 @pytest.mark.parametrize("nx,ny", [(40, 24), (33, 17), (96, 70)])
 def test_ragged_tiles(gpu_lib, nx, ny):
     """Interior sizes that are not multiples of the 32x8 tile."""

@@ -172,3 +172,60 @@ def test_rejects(gpu_lib):
         with pytest.raises(capi.PipError) as e:
             c.set_resistivity(np.zeros(c.shape_h[1:]))
         assert e.value.code == capi.PIP_ERR_PARAM
+
+
+# ------------------------------------------------------------ anomalous eta (flag_resi 2)
+
+# type 2 with these values switches eta to 11 eta_0 in a cell once its current passes
+# j_cri (after ~13 steps on 32^2), after which cfl_resi's bound of the new eta lowers the
+# time increment; type 3's drift law is continuous
+ANOMALOUS = {"type2": dict(flag_resi=22, eta_0=0.03, j_cri=5.5),
+             "type3": dict(flag_resi=32, eta_0=2e-2, vd_cri=150.0)}
+
+
+@pytest.mark.parametrize("exact", [1, 0])
+@pytest.mark.parametrize("law", sorted(ANOMALOUS))
+def test_orszag_tang_anomalous_eta(gpu_lib, law, exact):
+    """set_resistivity resi_type 2 or 3 at every RK stage (flag_resi 22/32): the eta of each
+    stage from its own state, cfl_resi's bound of the last stage's eta in the next dt and in
+    the time increment.  A step count and a time limit (the last step is found from the
+    lowered time)."""
+    s, Uh, Um = ics.orszag_tang(32, fp_exact=exact, **ANOMALOUS[law])
+    for kw in (dict(nsteps=30), dict(t_end=0.03)):
+        g = run_gpu(s, Uh, Um, **kw)
+        o = run_orc(s, Uh, Um, **kw)
+        assert_match(g, o, bitwise=bool(exact))
+
+
+def test_anomalous_eta_1d(gpu_lib):
+    s, Uh, Um = decay_case(128, 1e-2, flag_resi=22, j_cri=4e-4, fp_exact=1)
+    g = run_gpu(s, Uh, Um, t_end=0.2)
+    o = run_orc(s, Uh, Um, t_end=0.2)
+    assert_match(g, o, bitwise=True)
+
+
+def test_anomalous_eta_host_stepped(gpu_lib):
+    """The Fortran time loop through the C ABI: cfl, run_solver (pip_step), cfl, then
+    dt = min(dt, pip_resi_dt) for cfl_resi's write of the global dt, time += dt."""
+    s, Uh, Um = ics.orszag_tang(32, fp_exact=1, **ANOMALOUS["type2"])
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.prologue()
+        t = 0.0
+        for _ in range(25):
+            dt, _ = c.cfl()
+            c.run_solver(dt)
+            c.cfl()
+            t = t + min(dt, c.resi_dt())
+        gh, gm = c.download()
+    o = run_orc(s, Uh, Um, nsteps=25)
+    assert t == o[1]
+    np.testing.assert_array_equal(gh, o[3])
+    np.testing.assert_array_equal(gm, o[4])
+
+
+def test_anomalous_eta_refuses_a_decomposition(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(32, **ANOMALOUS["type3"])
+    with capi.Context(s) as c:
+        nb = (ctypes.c_int * 4)(-1, -1, 0, 0)
+        assert capi.lib().pip_set_neighbors(c.h, nb) == capi.PIP_ERR_PARAM

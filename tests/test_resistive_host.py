@@ -131,7 +131,12 @@ def test_blocks_with_a_localised_field(world):
 
 def test_settings_and_output(tmp_path):
     with pytest.raises(ValueError, match="flag_resi"):
-        Settings(flag_resi=2).validate()
+        Settings(flag_resi=3).validate()
+    with pytest.raises(ValueError, match="vd_cri"):
+        Settings(flag_resi=32).validate()
+    for v, want in ((2, 1), (12, 1), (21, 1), (22, 2), (32, 2)):
+        p, _ = Settings(flag_resi=v, vd_cri=1.0).to_params()
+        assert (p.flag_resi, p.resi_type) == (want, v // 10)
     with pytest.raises(ValueError, match="PIP_FP64"):
         Settings(flag_resi=1, precision=PIP_MIXED).validate()
     with pytest.raises(ValueError, match="conduction"):
@@ -146,3 +151,87 @@ def test_settings_and_output(tmp_path):
     names = [ln.split()[0] for ln in open(path[:-4] + ".idx")]
     assert names[7:9] == ["et", "ro_p"]
     np.testing.assert_array_equal(output.restart_resistivity(str(tmp_path), 1, s), s.eta_field())
+
+
+# ------------------------------------------------------------ anomalous eta (flag_resi 2)
+
+ANOMALOUS = [dict(flag_resi=22, eta_0=5e-3, j_cri=3.0),
+             dict(flag_resi=32, eta_0=2e-2, vd_cri=150.0)]
+
+
+@pytest.mark.parametrize("kw", ANOMALOUS)
+def test_anomalous_eta_at_the_prologue_matches_the_restatement(kw):
+    """set_resistivity resi_type 2 and 3 (Res_rot.f90:37-60) in the oracle against the
+    vectorised restatement of Settings.eta_field, on the Orszag-Tang field, where both
+    branches of each law occur."""
+    s, Uh, Um = ics.orszag_tang(48, **kw)
+    o = O.Oracle(s, Uh, Um)
+    eta = o.resistivity()
+    o.close()
+    want = s.eta_field(Um)
+    np.testing.assert_array_equal(eta, want)
+    big = eta > kw["eta_0"] if kw["flag_resi"] == 22 else eta > 0.0
+    assert 0.05 < big.mean() < 0.95
+
+
+def _run(s, Uh, Um, nsteps):
+    o = O.Oracle(s, Uh, Um)
+    try:
+        o.prologue()
+        st, t, n, _ = o.run(nsteps, 0.0)
+        h, m = o.state()
+        return t, h, m
+    finally:
+        o.close()
+
+
+def test_anomalous_eta_reduces_to_the_fixed_field_paths():
+    """Per-stage eta whose switch never fires equals the fixed-field runs bit for bit: resi
+    type 2 with j_cri beyond any current is uniform eta_0 (flag_resi 1), type 3 with vd_cri
+    beyond any drift is eta = 0, the ideal run (flag_resi 0, two ghost layers)."""
+    s2, Uh, Um = ics.orszag_tang(32, flag_resi=22, eta_0=2e-3, j_cri=1e30)
+    s1 = s2.overrides(flag_resi=1)
+    t2, h2, m2 = _run(s2, Uh, Um, 12)
+    t1, h1, m1 = _run(s1, Uh, Um, 12)
+    assert t2 == t1
+    np.testing.assert_array_equal(h2, h1)
+    np.testing.assert_array_equal(m2, m1)
+    s3, Uh3, Um3 = ics.orszag_tang(32, flag_resi=32, eta_0=2e-3, vd_cri=1e30)
+    s0, Uh0, Um0 = ics.orszag_tang(32)
+    t3, h3, m3 = _run(s3, Uh3, Um3, 12)
+    t0, h0, m0 = _run(s0, Uh0, Um0, 12)
+    assert t3 == t0
+    np.testing.assert_array_equal(h3[:, 3:-3, 3:-3], h0[:, 2:-2, 2:-2])
+    np.testing.assert_array_equal(m3[:, 3:-3, 3:-3], m0[:, 2:-2, 2:-2])
+
+
+def test_anomalous_eta_lowers_the_time_increment():
+    """Where cfl_resi's bound of the last stage's eta is below the step's dt, the time loop
+    advances time by the bound (main.f90:47,58, through cfl_resi's write of the global dt):
+    time after the step = time before + min(dt, bound of the new eta)."""
+    # type 2 switches eta to 11 eta_0 when a cell's current first passes j_cri: from then
+    # on the bound of the new eta lies below the step's dt
+    s, Uh, Um = ics.orszag_tang(32, flag_resi=22, eta_0=0.03, j_cri=5.5)
+    o = O.Oracle(s, Uh, Um)
+    try:
+        o.prologue()
+        lowered = 0
+        for _ in range(30):
+            t0 = o.time
+            dt, _ = o.cfl()       # the step's dt (the run's own cfl gives the same)
+            st, t1, n, _ = o.run(1, 0.0)
+            assert st == 0 and n == 1
+            bound = _bound(s, o.resistivity())
+            assert t1 - t0 == pytest.approx(min(dt, bound), rel=1e-12)
+            lowered += bound < dt
+        assert lowered > 0
+    finally:
+        o.close()
+
+
+def _bound(s, eta):
+    m = s.margin
+    _, _, _, dx, dy, dz = s.coordinates()
+    gmin = np.minimum(np.minimum(dx[None, :], dy[:, None]), dz[0])
+    b = s.safety * (gmin * gmin) / np.maximum(eta, 1e-8)
+    return float(b[m[1]:-m[1], m[0]:-m[0]].min())
