@@ -31,6 +31,8 @@ struct pip_ctx {
   cudaStream_t stream = nullptr;
   double *A = nullptr, *B = nullptr;  // NV planes each (FP64 form; A stages the mixed form)
   float *Ahi = nullptr, *Alo = nullptr, *Bf = nullptr;  // FP32-mixed form
+  CUtensorMap tm_a, tm_b;             // TMA maps of the mixed stage sources Ahi and Bf
+  bool tma = false;                   // the maps exist (2D grids that meet the TMA rules)
   bool mixed = false;
   double *d_dx = nullptr, *d_dy = nullptr, *d_rdx = nullptr, *d_rdy = nullptr;
   double *scratch = nullptr;          // NV planes for pip_flux / pip_source
@@ -441,9 +443,9 @@ cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
   if (c->mixed) {
     if (stage == 1)
       return pip::mixed_stage(c->kp, 1, c->Ahi, c->Ahi, nullptr, c->Bf, nullptr, c->ctrl, dt_mode,
-                              epi, c->stream);
+                              epi, c->stream, c->tma ? &c->tm_a : nullptr);
     return pip::mixed_stage(c->kp, 2, c->Bf, c->Ahi, c->Alo, c->Ahi, c->Alo, c->ctrl, dt_mode, epi,
-                            c->stream);
+                            c->stream, c->tma ? &c->tm_b : nullptr);
   }
   if (stage == 1) return c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, dt_mode, epi, c->stream);
   return c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, dt_mode, epi, c->stream);
@@ -557,6 +559,9 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
     if ((e = cudaMalloc(&c->Alo, fstate)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&c->Bf, fstate)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(c->Bf, 0, fstate)) != cudaSuccess) return fail(e);
+    // 2D tiles of the stage sources by TMA where the grid meets its alignment rules
+    c->tma = pip::mixed_tile_map(c->kp, c->Ahi, &c->tm_a) &&
+             pip::mixed_tile_map(c->kp, c->Bf, &c->tm_b);
   } else if ((e = cudaMalloc(&c->B, state)) != cudaSuccess) {
     return fail(e);
   }

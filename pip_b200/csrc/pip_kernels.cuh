@@ -1,6 +1,7 @@
 // pip_kernels.cuh -- kernel parameter blocks shared by the FP64 kernels and the C ABI.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -124,7 +125,11 @@ int kparams_from_params(const pip_params *p, KParams *k);
 cudaError_t mixed_prepare();
 cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
                         const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
-                        int epi, cudaStream_t s);
+                        int epi, cudaStream_t s, const CUtensorMap *tm = nullptr);
+// The TMA map of the stage source Us (an array of nvm+5 FP32 planes) for the 2D mixed stage
+// kernels' tiles; false (use per-thread loads) where the grid or the address breaks the
+// TMA's alignment rules.
+bool mixed_tile_map(const KParams &p, const float *Us, CUtensorMap *map);
 cudaError_t mixed_cfl(const KParams &p, float *hi, float *lo, DevCtrl *ctrl, int slot,
                       cudaStream_t s);
 cudaError_t mixed_split(const double *U, float *hi, float *lo, long long n, cudaStream_t s);

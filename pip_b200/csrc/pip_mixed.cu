@@ -14,9 +14,12 @@
 //
 // Compiled with -ftz=true -prec-div=false -prec-sqrt=false: FP32 division and square root
 // are the approximate hardware forms; FP64 arithmetic is unaffected.
+#include <cstring>
+
 #include "pip_kernels.cuh"
 #include "pip_mixed_cell.cuh"
 #include "pip_physics.cuh"
+#include "pip_tma.cuh"
 
 namespace pip {
 namespace mixed {
@@ -90,23 +93,29 @@ __device__ __forceinline__ void block_reduce_cfl(double dtc, double rho, double 
 // One RK stage (see the FP64 stage_kernel for the structure).  Stage 1: Us = A.hi,
 // U0 = A.hi, output B (FP32).  Stage 2: Us = B, U0 = A.hi + A.lo, output A (hi, lo).
 // The parameter block is __grid_constant__: the out-of-line ghost writer takes its address,
-// which would otherwise copy the whole block to every thread's stack.
+// which would otherwise copy the whole block to every thread's stack.  With use_tma (2D),
+// the tile and its halo of all planes of Us arrive by one TMA load (tmap describes Us).
 template <int NDIM, int NVM, int STAGE>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? PIP_MIXED_MINB : 4)
 stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
-             float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi) {
+             float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi,
+             const __grid_constant__ CUtensorMap tmap, int use_tma) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   constexpr int NV = NVM + 5;
   constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
-  extern __shared__ double smd[];
-  // FP64 Dedner fluxes (Bn and psi components, HLL_rot.f90:904-908) of every face: the
-  // psi flux carries ch^2 (BnL+BnR), whose face-to-face difference cancels in FP32
-  double *sD6 = smd;
+  extern __shared__ __align__(128) double smd[];
+  // the tile's primitives first (128-byte aligned: the TMA destination), then the FP64
+  // Dedner fluxes (Bn and psi components, HLL_rot.f90:904-908) of every face -- the psi
+  // flux carries ch^2 (BnL+BnR), whose face-to-face difference cancels in FP32 -- then the
+  // FP32 fluxes
+  float *sV = reinterpret_cast<float *>(smd);
+  double *sD6 = reinterpret_cast<double *>(sV + NV * RR);
   double *sD9 = sD6 + (NVM == 9 ? NFX + NFY : 0);
-  float *sV = reinterpret_cast<float *>(sD9 + (NVM == 9 ? NFX + NFY : 0));
-  float *sFx = sV + NV * RR;
+  float *sFx = reinterpret_cast<float *>(sD9 + (NVM == 9 ? NFX + NFY : 0));
   float *sFy = sFx + NV * NFX;
+  static_assert((NV * RR * sizeof(float)) % sizeof(double) == 0, "Dedner planes alignment");
+  __shared__ __align__(8) unsigned long long s_bar;
   __shared__ double s_dt, s_cmax;
   __shared__ long long s_step;
   __shared__ int s_exit, s_epi;
@@ -159,6 +168,45 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
   const long long nc = p.nc;
 
   // ---- 1. FP32 primitives of the tile and its halo
+  // (the TMA writes shared memory only at 128-byte aligned destinations)
+  if (NDIM == 2 && use_tma && (tma_smem_addr(sV) & 127u) == 0) {
+    // the raw planes by one TMA load into sV (cells outside the array read as zero), then
+    // primitives in place: each thread rewrites its own cells
+    if (tid == 0) {
+      tma_bar_init(&s_bar);
+      tma_bar_expect(&s_bar, (uint32_t)(NV * RR * sizeof(float)));
+      tma_load_tile(sV, &tmap, i0 - kH, j0 - kH, &s_bar);
+    }
+    __syncthreads();
+    const bool ok = tma_bar_wait(&s_bar, kTmaWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      // the tile did not arrive: flag the stage and let the copy land (bounded) before the
+      // CTA's shared memory is released
+      if (tid == 0) {
+        atomicCAS(&ctrl->status, 0, 5);  // PIP_ERR_ITER
+        ctrl->done = 1;
+        tma_bar_wait(&s_bar, kTmaWaitLimit);
+      }
+      return;
+    }
+    for (int idx = tid; idx < RR; idx += NT) {
+      const int ri = idx % RX, rj = idx / RX;
+      if ((ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
+      const int gi = i0 - kH + ri, gj = j0 - kH + rj;
+      if (gi >= p.ix || gj >= p.jx) continue;
+      float um[NVM], uh[5], vm[NVM], vh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) um[n] = sV[n * RR + idx];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uh[n] = sV[(NVM + n) * RR + idx];
+      u2v_mhd<float, NVM>(um, vm, gmf, rolf, prlf);
+      u2v_hd<float>(uh, vh, gmf, rolf, prlf);
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) sV[n * RR + idx] = vm[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+    }
+  } else
   for (int idx = tid; idx < RR; idx += NT) {
     const int ri = idx % RX, rj = idx / RX;
     if (NDIM == 2 && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
@@ -503,11 +551,13 @@ static cudaError_t set_attr() {
 template <int NDIM, int NVM, int STAGE>
 static cudaError_t launch_t(const KParams &p, const float *Us, const float *U0hi, const float *U0lo,
                             float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi,
-                            cudaStream_t s) {
+                            cudaStream_t s, const CUtensorMap *tm) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof none);
   stage_kernel<NDIM, NVM, STAGE><<<grid, NT, smem_bytes<NDIM, NVM>(), s>>>(
-      p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi);
+      p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, tm ? *tm : none, tm ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -530,16 +580,26 @@ cudaError_t mixed_prepare() {
 
 cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
                         const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
-                        int epi, cudaStream_t s) {
+                        int epi, cudaStream_t s, const CUtensorMap *tm) {
   using namespace mixed;
   if (p.ndim == 1)
-    return stage == 1 ? launch_t<1, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
-                      : launch_t<1, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
+    return stage == 1 ? launch_t<1, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr)
+                      : launch_t<1, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr);
   if (p.nvm == 9)
-    return stage == 1 ? launch_t<2, 9, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
-                      : launch_t<2, 9, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
-  return stage == 1 ? launch_t<2, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s)
-                    : launch_t<2, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s);
+    return stage == 1 ? launch_t<2, 9, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm)
+                      : launch_t<2, 9, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm);
+  return stage == 1 ? launch_t<2, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm)
+                    : launch_t<2, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm);
+}
+
+bool mixed_tile_map(const KParams &p, const float *Us, CUtensorMap *map) {
+  using namespace mixed;
+  if (p.ndim != 2) return false;
+  constexpr int TX = Tile<2>::TX, TY = Tile<2>::TY;
+  if (!tma_tile_ok(Us, p.ix, p.jx, p.nvm + 5, (int)sizeof(float), p.m0 - kH, TX, TX + 2 * kH,
+                   TY + 2 * kH))
+    return false;
+  return tma_encode(map, Us, p.ix, p.jx, p.nvm + 5, (int)sizeof(float), TX + 2 * kH, TY + 2 * kH);
 }
 
 cudaError_t mixed_cfl(const KParams &p, float *hi, float *lo, DevCtrl *ctrl, int slot,
