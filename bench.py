@@ -298,7 +298,7 @@ def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     eng.ctx.cfl()
     eng.ctx.pipbnd()
     run.halo()
-    if run.run_device(warmup) != 0:
+    if run.run_device(warmup, overlap=True) != 0:
         raise RuntimeError("decomposed warm-up stopped")
     if dist:
         dist.barrier()
@@ -307,7 +307,7 @@ def measure_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record()
-        st = run.run_device(steps, check_every=0)
+        st = run.run_device(steps, check_every=0, overlap=True)
         e1.record()
         torch.cuda.synchronize()
     if st != 0:
@@ -347,13 +347,13 @@ def e2e_decomposed(n, precision, steps, warmup, dist, local, world, rank):
     eng = decomp.DeviceBlock(b, ph, pm, device=local)
     comm = decomp.TorchComm(device=torch.device("cuda", local)) if dist else decomp.LocalComm()
     run = decomp.DecomposedRun([eng], comm, divb=sg.divb == 1)
-    run.run_device(warmup)
+    run.run_device(warmup, overlap=True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     eng.ctx.upload(ph, pm)
-    st = run.run_device(steps, check_every=0)
+    st = run.run_device(steps, check_every=0, overlap=True)
     eng.ctx.download(oh, om)
     e2e_s = time.perf_counter() - t0
     run.close()

@@ -354,6 +354,21 @@ int pip_ctx_stream(pip_ctx *ctx, void **stream);
 int pip_set_cmax_scale(pip_ctx *ctx, double safety_min_d);
 int pip_dev_begin(pip_ctx *ctx, int64_t nsteps, double t_end);
 int pip_dev_stage(pip_ctx *ctx, int stage);
+
+/* The y exchange overlapped with the stage (2D; no counterpart in the reference, whose
+ * mpi_bnd runs after the whole stage).  A stage is queued in two launches on the context
+ * stream: pip_dev_stage_rows(ctx, k, 1) computes the first and the last row of tiles -- the
+ * cells the exchange sends -- and pip_dev_stage_rows(ctx, k, 2) the rows between them;
+ * together they equal pip_dev_stage(ctx, k) bit for bit.  Between the two calls the caller
+ * records an event on the context stream; the exchange (pack, transfer, unpack) runs on
+ * another stream after that event while the middle rows compute, and the context stream
+ * waits for the exchange before the next stage.  The middle rows neither read nor write
+ * what the exchange reads or writes (it reads the boundary rows' cells, it writes the ghost
+ * rows of the exchanged faces, and the stage reads only its input array).
+ * pip_set_halo_stream(ctx, stream) makes pip_halo_pack / pip_halo_unpack queue on `stream`
+ * (NULL: the context stream again). */
+int pip_dev_stage_rows(pip_ctx *ctx, int stage, int rows);
+int pip_set_halo_stream(pip_ctx *ctx, void *stream);
 int pip_dev_candidates(pip_ctx *ctx, void **dt_min, void **rho_gr_max);
 int pip_dev_poll(pip_ctx *ctx, int *done, double *time, int64_t *steps);
 int64_t pip_halo_bytes(pip_ctx *ctx, int face);

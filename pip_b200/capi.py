@@ -34,6 +34,7 @@ EXPORTS = (
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
+    "pip_dev_stage_rows", "pip_set_halo_stream",
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
     "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
     # include/pip_bench.h
@@ -106,6 +107,8 @@ def lib(path: Optional[str] = None):
     L.pip_set_cmax_scale.argtypes = [vp, d]
     L.pip_dev_begin.argtypes = [vp, ctypes.c_int64, d]
     L.pip_dev_stage.argtypes = [vp, i]
+    L.pip_dev_stage_rows.argtypes = [vp, i, i]
+    L.pip_set_halo_stream.argtypes = [vp, vp]
     L.pip_dev_candidates.argtypes = [vp, P(vp), P(vp)]
     L.pip_dev_poll.argtypes = [vp, P(i), dp, P(ctypes.c_int64)]
     L.pip_step_noalloc.restype = i
@@ -331,6 +334,15 @@ class Context:
 
     def dev_stage(self, stage: int) -> None:
         _check(lib().pip_dev_stage(self.h, int(stage)), "pip_dev_stage")
+
+    def dev_stage_rows(self, stage: int, rows: int) -> None:
+        """Half of a device stage: rows 1 the first and last tile rows, 2 the others."""
+        _check(lib().pip_dev_stage_rows(self.h, int(stage), int(rows)), "pip_dev_stage_rows")
+
+    def set_halo_stream(self, stream: int) -> None:
+        """The stream of pip_halo_pack / pip_halo_unpack (0: the context stream)."""
+        _check(lib().pip_set_halo_stream(self.h, ctypes.c_void_p(stream or None)),
+               "pip_set_halo_stream")
 
     def dev_candidates(self) -> Tuple[int, int]:
         """Device addresses of the cfl candidates: (2 int64 to MIN, 4 int64 to MAX)."""

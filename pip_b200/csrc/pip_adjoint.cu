@@ -875,10 +875,10 @@ int pip_adj_forward(pip_adj *a, const double *U0, double *UN, int64_t nsteps, fl
   for (int64_t n = 0; n < nsteps; ++n) {
     if (n % a->K == 0)
       ACK(cudaMemcpyAsync(a->ckpt[n / a->K], a->A, sb, cudaMemcpyDeviceToDevice, a->stream));
-    ACK(a->L->stage(a->kp, 1, a->A, a->A, a->B, a->ctrl, 1, 0, a->stream));
+    ACK(a->L->stage(a->kp, 1, a->A, a->A, a->B, a->ctrl, 1, 0, a->stream, nullptr, 0));
     ACK(cudaMemcpyAsync(a->dt_hist + n, &a->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice,
                         a->stream));
-    ACK(a->L->stage(a->kp, 2, a->B, a->A, a->A, a->ctrl, 1, -1, a->stream));
+    ACK(a->L->stage(a->kp, 2, a->B, a->A, a->A, a->ctrl, 1, -1, a->stream, nullptr, 0));
   }
   ACK(cudaMemcpyAsync(UN, a->A, sb, cudaMemcpyDeviceToDevice, a->stream));
   if (device_ms) ACK(cudaEventRecord(e1, a->stream));
@@ -931,9 +931,9 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
     for (int j = 0; j < len; ++j) {
       ACK(cudaMemcpyAsync(&a->ctrl->dt, a->dt_hist + n0 + j, sizeof(double), cudaMemcpyDeviceToDevice,
                           a->stream2));
-      ACK(a->L->stage(kp, 1, zp(s, j), zp(s, j), a->segu[s % 2][j], a->ctrl, 0, 0, a->stream2));
+      ACK(a->L->stage(kp, 1, zp(s, j), zp(s, j), a->segu[s % 2][j], a->ctrl, 0, 0, a->stream2, nullptr, 0));
       if (j + 1 < len)
-        ACK(a->L->stage(kp, 2, a->segu[s % 2][j], zp(s, j), zp(s, j + 1), a->ctrl, 0, 2, a->stream2));
+        ACK(a->L->stage(kp, 2, a->segu[s % 2][j], zp(s, j), zp(s, j + 1), a->ctrl, 0, 2, a->stream2, nullptr, 0));
     }
     ACK(cudaEventRecord(a->ev_rec[s % 2], a->stream2));
     return PIP_OK;

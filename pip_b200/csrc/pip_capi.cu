@@ -31,7 +31,7 @@ struct pip_ctx {
   cudaStream_t stream = nullptr;
   double *A = nullptr, *B = nullptr;  // NV planes each (FP64 form; A stages the mixed form)
   float *Ahi = nullptr, *Alo = nullptr, *Bf = nullptr;  // FP32-mixed form
-  CUtensorMap tm_a, tm_b;             // TMA maps of the mixed stage sources Ahi and Bf
+  CUtensorMap tm_a, tm_b;             // TMA maps of the stage sources (A and B, or Ahi and Bf)
   bool tma = false;                   // the maps exist (2D grids that meet the TMA rules)
   bool mixed = false;
   double *d_dx = nullptr, *d_dy = nullptr, *d_rdx = nullptr, *d_rdy = nullptr;
@@ -47,6 +47,8 @@ struct pip_ctx {
   int neighbor[4] = {-1, -1, -1, -1};  // set_mpi_neighbor: rank across each face, -1 physical
   bool exchanged = false;             // some face is filled by the halo exchange
   int last_stage = 0;                 // RK stage that wrote the state last (1: the U1 array)
+  int rows_open = 0;                  // pip_dev_stage_rows: stage whose middle rows are due
+  cudaStream_t halo_stream = nullptr; // pip_set_halo_stream: the stream of pack and unpack
   bool dev_loop = false;              // pip_dev_begin has set up the device-driven loop
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
@@ -438,17 +440,21 @@ int push_ctrl(pip_ctx *c) {
   return PIP_OK;
 }
 
-// One RK stage of the context's precision form.
-cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi) {
+// One RK stage of the context's precision form (rows: every tile row, or the first and
+// last / the middle ones, see Launchers::stage).
+cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi, int rows = 0) {
   if (c->mixed) {
     if (stage == 1)
       return pip::mixed_stage(c->kp, 1, c->Ahi, c->Ahi, nullptr, c->Bf, nullptr, c->ctrl, dt_mode,
-                              epi, c->stream, c->tma ? &c->tm_a : nullptr);
+                              epi, c->stream, c->tma ? &c->tm_a : nullptr, rows);
     return pip::mixed_stage(c->kp, 2, c->Bf, c->Ahi, c->Alo, c->Ahi, c->Alo, c->ctrl, dt_mode, epi,
-                            c->stream, c->tma ? &c->tm_b : nullptr);
+                            c->stream, c->tma ? &c->tm_b : nullptr, rows);
   }
-  if (stage == 1) return c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, dt_mode, epi, c->stream);
-  return c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, dt_mode, epi, c->stream);
+  if (stage == 1)
+    return c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, dt_mode, epi, c->stream,
+                       c->tma ? &c->tm_a : nullptr, rows);
+  return c->L->stage(c->kp, 2, c->B, c->A, c->A, c->ctrl, dt_mode, epi, c->stream,
+                     c->tma ? &c->tm_b : nullptr, rows);
 }
 
 cudaError_t do_cfl(pip_ctx *c, int slot) {
@@ -564,6 +570,8 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
              pip::mixed_tile_map(c->kp, c->Bf, &c->tm_b);
   } else if ((e = cudaMalloc(&c->B, state)) != cudaSuccess) {
     return fail(e);
+  } else {
+    c->tma = c->L->tile_map(c->kp, c->A, &c->tm_a) && c->L->tile_map(c->kp, c->B, &c->tm_b);
   }
   if ((e = cudaMalloc(&c->d_dx, sizeof(double) * p->ix)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&c->d_dy, sizeof(double) * p->jx)) != cudaSuccess) return fail(e);
@@ -1152,12 +1160,35 @@ int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
 
 int pip_dev_stage(pip_ctx *c, int stage) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->dev_loop) return PIP_ERR_STATE;
+  if (!c->dev_loop || c->rows_open) return PIP_ERR_STATE;
   if (stage != 1 && stage != 2) return PIP_ERR_PARAM;
   if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(stage == 1 ? do_stage(c, 1, 1, 0) : do_stage(c, 2, 1, -1));
   c->last_stage = stage;
+  return PIP_OK;
+}
+
+int pip_dev_stage_rows(pip_ctx *c, int stage, int rows) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->dev_loop) return PIP_ERR_STATE;
+  if ((stage != 1 && stage != 2) || (rows != 1 && rows != 2)) return PIP_ERR_PARAM;
+  if (c->kp.ndim != 2) return PIP_ERR_PARAM;
+  if (rows == 1) {
+    if (c->rows_open || (stage == 2 && c->last_stage != 1)) return PIP_ERR_STATE;
+  } else if (c->rows_open != stage) {
+    return PIP_ERR_STATE;
+  }
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(stage == 1 ? do_stage(c, 1, 1, 0, rows) : do_stage(c, 2, 1, -1, rows));
+  c->last_stage = stage;
+  c->rows_open = rows == 1 ? stage : 0;
+  return PIP_OK;
+}
+
+int pip_set_halo_stream(pip_ctx *c, void *stream) {
+  if (!c) return PIP_ERR_NULL;
+  c->halo_stream = static_cast<cudaStream_t>(stream);
   return PIP_OK;
 }
 
@@ -1224,7 +1255,7 @@ int pip_halo_pack(pip_ctx *c, int face, void *send, int64_t *bytes) {
   void *a0, *a1;
   int eb;
   halo_arrays(c, &a0, &a1, &eb);
-  CK(pip::halo_pack(c->kp, face, a0, a1, eb, send, c->stream));
+  CK(pip::halo_pack(c->kp, face, a0, a1, eb, send, c->halo_stream ? c->halo_stream : c->stream));
   if (bytes) *bytes = (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1);
   return PIP_OK;
 }
@@ -1238,7 +1269,8 @@ int pip_halo_unpack(pip_ctx *c, int face, const void *recv, int64_t bytes) {
   halo_arrays(c, &a0, &a1, &eb);
   if (bytes != (int64_t)pip::halo_elems(c->kp, face) * eb * (a1 ? 2 : 1)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
-  CK(pip::halo_unpack(c->kp, face, a0, a1, eb, recv, c->stream));
+  CK(pip::halo_unpack(c->kp, face, a0, a1, eb, recv,
+                      c->halo_stream ? c->halo_stream : c->stream));
   return PIP_OK;
 }
 

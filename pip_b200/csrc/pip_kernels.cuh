@@ -74,8 +74,12 @@ struct DevCtrl {
 // Host launchers (one set per arithmetic flavour: FMA-contracted or FMA-free).
 struct Launchers {
   cudaError_t (*prepare)();
+  // tm: the TMA map of Us for the 2D tiles (tile_map), or null for per-thread loads.  rows
+  // (2D): 0 every tile row; 1 the first and the last tile row (those a y-halo exchange
+  // sends); 2 the rows between them.  A stage launched as 1 then 2 equals one launch of 0.
   cudaError_t (*stage)(const KParams &p, int stage, const double *Us, const double *U0, double *Uo,
-                       DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s);
+                       DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s, const CUtensorMap *tm,
+                       int rows);
   cudaError_t (*cfl)(const KParams &p, double *U, DevCtrl *ctrl, int slot, cudaStream_t s);
   cudaError_t (*ghosts)(const KParams &p, double *U, cudaStream_t s);
   cudaError_t (*flux)(const KParams &p, const double *U, double *F, int dir, double cmax,
@@ -83,6 +87,9 @@ struct Launchers {
   cudaError_t (*source)(const KParams &p, double *U, double *S, double dt_coll, cudaStream_t s);
   cudaError_t (*nan_scan)(const KParams &p, const double *U, int *flag, cudaStream_t s);
   cudaError_t (*coefficients)(const KParams &p, double *U, cudaStream_t s);
+  // the TMA map of a stage source U (nvm+5 FP64 planes) for the 2D stage kernels' tiles;
+  // false where the grid or the address breaks the TMA's alignment rules
+  bool (*tile_map)(const KParams &p, const double *U, CUtensorMap *map);
 };
 
 const Launchers &launchers_fast();
@@ -125,7 +132,8 @@ int kparams_from_params(const pip_params *p, KParams *k);
 cudaError_t mixed_prepare();
 cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
                         const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
-                        int epi, cudaStream_t s, const CUtensorMap *tm = nullptr);
+                        int epi, cudaStream_t s, const CUtensorMap *tm = nullptr,
+                        int rows = 0);
 // The TMA map of the stage source Us (an array of nvm+5 FP32 planes) for the 2D mixed stage
 // kernels' tiles; false (use per-thread loads) where the grid or the address breaks the
 // TMA's alignment rules.

@@ -99,7 +99,7 @@ template <int NDIM, int NVM, int STAGE>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? PIP_MIXED_MINB : 4)
 stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, const float *U0hi, const float *U0lo,
              float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi,
-             const __grid_constant__ CUtensorMap tmap, int use_tma) {
+             const __grid_constant__ CUtensorMap tmap, int use_tma, int rows) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   constexpr int NV = NVM + 5;
   constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
@@ -121,7 +121,11 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
   __shared__ int s_exit, s_epi;
 
   const int tid = threadIdx.x;
-  const bool block0 = blockIdx.x == 0 && blockIdx.y == 0;
+  // tile row: every row (rows 0), the first and the last (1), the rows between them (2)
+  const int nby = NDIM == 2 ? (p.ny + TY - 1) / TY : 1;
+  const int by = NDIM == 1 || rows == 0 ? (int)blockIdx.y
+                 : rows == 1 ? (blockIdx.y == 0 ? 0 : nby - 1) : (int)blockIdx.y + 1;
+  const bool block0 = blockIdx.x == 0 && by == 0;
   if (tid == 0) {
     int ex = STAGE == 1 ? (ctrl->done || ctrl->nan_flag) : ctrl->done;
     double dt, cmax;
@@ -164,7 +168,7 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
   const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
   const float igm1f = (float)p.igm1;
   const int i0 = p.m0 + blockIdx.x * TX;
-  const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
+  const int j0 = NDIM == 2 ? p.m1 + by * TY : 0;
   const long long nc = p.nc;
 
   // ---- 1. FP32 primitives of the tile and its halo
@@ -252,9 +256,11 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
       nf = NFY;
     }
     {
-      float vl[NVM], vr[NVM], fx[NVM];
+      // the HLLD of planes 0-7; with Dedner cleaning the normal-field and psi fluxes are the
+      // FP64 ones below, so the FP32 solver neither reconstructs psi nor stores those two
+      float vl[8], vr[8], fx[8];
 #pragma unroll
-      for (int n = 0; n < NVM; ++n) {
+      for (int n = 0; n < 8; ++n) {
         const int src = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         const float *v = sV + src * RR + a;
         const float v0 = v[-s], v1 = v[0], v2 = v[s], v3 = v[2 * s];
@@ -263,9 +269,10 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
       }
       vl[0] = fmaxf(vl[0], rolf);
       vr[0] = fmaxf(vr[0], rolf);
-      hlld_flux_rcp<float, NVM>(vl, vr, fx, gmf, igm1f, cmaxf);
+      hlld_flux_rcp<float, 8>(vl, vr, fx, gmf, igm1f, cmaxf);
 #pragma unroll
-      for (int n = 0; n < NVM; ++n) {
+      for (int n = 0; n < 8; ++n) {
+        if (NVM == 9 && n == 5) continue;
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n == 5 ? 6 : n == 6 ? 5 : n) : n;
         Fout[dst * nf + fo] = fx[n];
       }
@@ -450,7 +457,7 @@ stage_kernel(const __grid_constant__ KParams p, const float *__restrict__ Us, co
     __syncthreads();
     if (tid == 0) {
       __threadfence();
-      const unsigned int nb = gridDim.x * gridDim.y;
+      const unsigned int nb = gridDim.x * nby;     // every tile of the stage's launches
       if (atomicAdd(&ctrl->blocks_done, 1u) == nb - 1) {
         __threadfence();
         ctrl->blocks_done = 0u;
@@ -551,13 +558,17 @@ static cudaError_t set_attr() {
 template <int NDIM, int NVM, int STAGE>
 static cudaError_t launch_t(const KParams &p, const float *Us, const float *U0hi, const float *U0lo,
                             float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode, int epi,
-                            cudaStream_t s, const CUtensorMap *tm) {
+                            cudaStream_t s, const CUtensorMap *tm, int rows) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
-  dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
+  const int nby = NDIM == 2 ? (p.ny + TY - 1) / TY : 1;
+  if (NDIM == 1) rows = 0;
+  const int gy = rows == 0 ? nby : rows == 1 ? (nby < 2 ? nby : 2) : nby - 2;
+  if (gy <= 0) return cudaSuccess;   // no rows between the first and the last
+  dim3 grid((p.nx + TX - 1) / TX, gy);
   CUtensorMap none;
   std::memset(&none, 0, sizeof none);
   stage_kernel<NDIM, NVM, STAGE><<<grid, NT, smem_bytes<NDIM, NVM>(), s>>>(
-      p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, tm ? *tm : none, tm ? 1 : 0);
+      p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, tm ? *tm : none, tm ? 1 : 0, rows);
   return cudaGetLastError();
 }
 
@@ -580,16 +591,16 @@ cudaError_t mixed_prepare() {
 
 cudaError_t mixed_stage(const KParams &p, int stage, const float *Us, const float *U0hi,
                         const float *U0lo, float *Ohi, float *Olo, DevCtrl *ctrl, int dt_mode,
-                        int epi, cudaStream_t s, const CUtensorMap *tm) {
+                        int epi, cudaStream_t s, const CUtensorMap *tm, int rows) {
   using namespace mixed;
   if (p.ndim == 1)
-    return stage == 1 ? launch_t<1, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr)
-                      : launch_t<1, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr);
+    return stage == 1 ? launch_t<1, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr, 0)
+                      : launch_t<1, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, nullptr, 0);
   if (p.nvm == 9)
-    return stage == 1 ? launch_t<2, 9, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm)
-                      : launch_t<2, 9, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm);
-  return stage == 1 ? launch_t<2, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm)
-                    : launch_t<2, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm);
+    return stage == 1 ? launch_t<2, 9, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm, rows)
+                      : launch_t<2, 9, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm, rows);
+  return stage == 1 ? launch_t<2, 8, 1>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm, rows)
+                    : launch_t<2, 8, 2>(p, Us, U0hi, U0lo, Ohi, Olo, ctrl, dt_mode, epi, s, tm, rows);
 }
 
 bool mixed_tile_map(const KParams &p, const float *Us, CUtensorMap *map) {

@@ -93,7 +93,7 @@ extern "C" int pip_step_noalloc(const pip_params *p, double *U_dev, double dt, d
     return cuda_fail(e);
   if ((e = cudaMemcpyAsync(ddy, p->dy, sizeof(double) * p->jx, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_fail(e);
-  if ((e = L.stage(k, 1, U_dev, U_dev, U1, ctrl, 0, 0, s)) != cudaSuccess) return cuda_fail(e);
-  if ((e = L.stage(k, 2, U1, U_dev, U_dev, ctrl, 0, 0, s)) != cudaSuccess) return cuda_fail(e);
+  if ((e = L.stage(k, 1, U_dev, U_dev, U1, ctrl, 0, 0, s, nullptr, 0)) != cudaSuccess) return cuda_fail(e);
+  if ((e = L.stage(k, 2, U1, U_dev, U_dev, ctrl, 0, 0, s, nullptr, 0)) != cudaSuccess) return cuda_fail(e);
   return PIP_OK;
 }

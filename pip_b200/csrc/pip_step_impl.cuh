@@ -8,8 +8,11 @@
 // arrays: A holds U0 and receives U2 in place, B receives U1.
 #pragma once
 
+#include <cstring>
+
 #include "pip_kernels.cuh"
 #include "pip_physics.cuh"
+#include "pip_tma.cuh"
 
 namespace pip {
 namespace PIP_FLAVOUR {
@@ -469,9 +472,9 @@ __device__ __forceinline__ void add_resistive(double *F, long long nf, long long
 // 1D), the edge tiles also the corner cells; the ranges of the tiles are disjoint.
 template <int NDIM, int NVM, int TX, int TY, int NT>
 __device__ void exchanged_ghost_ac(const KParams &p, const double *__restrict__ Us, int i0, int j0,
-                                   int tid) {
+                                   int tid, int by, int nby) {
   const bool first_x = blockIdx.x == 0, last_x = blockIdx.x == gridDim.x - 1;
-  const bool first_y = blockIdx.y == 0, last_y = blockIdx.y == gridDim.y - 1;
+  const bool first_y = by == 0, last_y = by == nby - 1;
   const bool lo_x = first_x && p.gx[0][0] < 0, hi_x = last_x && p.gx[1][0] < 0;
   const bool lo_y = NDIM == 2 && first_y && p.gy[0][0] < 0;
   const bool hi_y = NDIM == 2 && last_y && p.gy[1][0] < 0;
@@ -520,15 +523,16 @@ __device__ __forceinline__ void block_min_to(double v, unsigned long long *dst) 
 
 template <int NDIM, int NVM, int STAGE, int X>
 __global__ void __launch_bounds__(Tile<NDIM>::NT, NDIM == 2 ? 2 : 4)
-stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, double *Uo,
-             DevCtrl *ctrl, int dt_mode, int epi) {
+stage_kernel(const __grid_constant__ KParams p, const double *__restrict__ Us, const double *U0,
+             double *Uo, DevCtrl *ctrl, int dt_mode, int epi,
+             const __grid_constant__ CUtensorMap tmap, int use_tma, int rows) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
   constexpr int NV = NVM + 5;
   constexpr int RX = TX + 2 * kH, RY = NDIM == 2 ? TY + 2 * kH : 1, RR = RX * RY;
   constexpr int NFX = (TX + 1) * TY, NFY = NDIM == 2 ? TX * (TY + 1) : 0;
   constexpr int EW = TX + 2, EH = NDIM == 2 ? TY + 2 : 1, EN = EW * EH;
-  extern __shared__ double smem[];
-  double *sV = smem;
+  extern __shared__ __align__(128) double smem[];
+  double *sV = smem;                 // first: the TMA destination (128-byte aligned)
   double *sFx = sV + NV * RR;
   double *sFy = sFx + NV * NFX;
   constexpr bool COL = (X & 1) != 0, RES = (X & 2) != 0;
@@ -536,9 +540,15 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
   __shared__ double s_dt, s_cmax;
   __shared__ long long s_step;
   __shared__ int s_exit, s_epi;
+  __shared__ __align__(8) unsigned long long s_bar;
 
   const int tid = threadIdx.x;
-  const bool block0 = blockIdx.x == 0 && blockIdx.y == 0;
+  // tile row of this CTA: every row (rows 0), the first and the last (1: the rows a halo
+  // exchange sends, launched first), or the rows between them (2)
+  const int nby = NDIM == 2 ? (p.ny + TY - 1) / TY : 1;
+  const int by = NDIM == 1 || rows == 0 ? (int)blockIdx.y
+                 : rows == 1 ? (blockIdx.y == 0 ? 0 : nby - 1) : (int)blockIdx.y + 1;
+  const bool block0 = blockIdx.x == 0 && by == 0;
   if (tid == 0) {
     int ex = 0;
     if (STAGE == 1) {
@@ -593,10 +603,53 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
 
   const double gm = p.gm, ro_lim = p.ro_lim, pr_lim = p.pr_lim;
   const int i0 = p.m0 + blockIdx.x * TX;
-  const int j0 = NDIM == 2 ? p.m1 + blockIdx.y * TY : 0;
+  const int j0 = NDIM == 2 ? p.m1 + by * TY : 0;
   const long long nc = p.nc;
 
   // ---- 1. stage state of the tile and its halo -> primitives in shared memory
+  if (NDIM == 2 && use_tma && (tma_smem_addr(sV) & 127u) == 0) {
+    // all planes of the tile and its halo by one TMA load into sV (cells outside the array
+    // read as zero), then the primitives in place, each thread on its own cells
+    if (tid == 0) {
+      tma_bar_init(&s_bar);
+      tma_bar_expect(&s_bar, (uint32_t)(NV * RR * sizeof(double)));
+      tma_load_tile(sV, &tmap, i0 - kH, j0 - kH, &s_bar);
+    }
+    __syncthreads();
+    const bool ok = tma_bar_wait(&s_bar, kTmaWaitLimit);
+    if (__syncthreads_or(!ok)) {
+      // the tile did not arrive: flag the stage and let the copy land (bounded) before the
+      // CTA's shared memory is released
+      if (tid == 0) {
+        atomicCAS(&ctrl->status, 0, 5);  // PIP_ERR_ITER
+        ctrl->done = 1;
+        tma_bar_wait(&s_bar, kTmaWaitLimit);
+      }
+      return;
+    }
+    for (int idx = tid; idx < RR; idx += NT) {
+      const int ri = idx % RX, rj = idx / RX;
+      if (!RES && (ri < kH || ri >= TX + kH) && (rj < kH || rj >= TY + kH)) continue;
+      const int gi = i0 - kH + ri, gj = j0 - kH + rj;
+      if (gi >= p.ix || gj >= p.jx) continue;
+      double um[NVM], uh[5], vm[NVM], vh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) um[n] = sV[n * RR + idx];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) uh[n] = sV[(NVM + n) * RR + idx];
+      if (COL) {
+        double te_m, te_h, rm, rh;
+        if (p.col_type) get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+        if (p.irs) get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+      }
+      u2v_mhd<double, NVM>(um, vm, gm, ro_lim, pr_lim);
+      u2v_hd<double>(uh, vh, gm, ro_lim, pr_lim);
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) sV[n * RR + idx] = vm[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) sV[(NVM + n) * RR + idx] = vh[n];
+    }
+  } else
   for (int idx = tid; idx < RR; idx += NT) {
     const int ri = idx % RX, rj = idx / RX;
     // the corners only for the curl of B next to the tile's corner faces (resistivity)
@@ -901,7 +954,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
       if (near_boundary<NDIM>(p, gi, gj)) write_ghosts<NDIM>(p, gi, gj, p.acf, 1, true);
     }
   }
-  if (STAGE == 2 && COL && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid);
+  if (STAGE == 2 && COL && p.col_type) exchanged_ghost_ac<NDIM, NVM, TX, TY, NT>(p, Us, i0, j0, tid, by, nby);
   if (STAGE == 2 && s_epi == 2) {
     if (RES && p.resi == 2) dtc = fmin(dtc, rb);  // the next step's cfl_resi
     block_reduce_cfl<NT>(dtc, rhoc, grc, ctrl, (int)((s_step + 1) & 1));
@@ -912,7 +965,7 @@ stage_kernel(const KParams p, const double *__restrict__ Us, const double *U0, d
     __syncthreads();
     if (tid == 0) {
       __threadfence();
-      const unsigned int nb = gridDim.x * gridDim.y;
+      const unsigned int nb = gridDim.x * nby;     // every tile of the stage's launches
       if (atomicAdd(&ctrl->blocks_done, 1u) == nb - 1) {
         __threadfence();
         ctrl->blocks_done = 0u;
@@ -1242,41 +1295,60 @@ static cudaError_t prepare() {
 
 template <int NDIM, int NVM, int STAGE>
 static cudaError_t launch_stage_t(const KParams &p, const double *Us, const double *U0, double *Uo,
-                                  DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
+                                  DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s,
+                                  const CUtensorMap *tm, int rows) {
   constexpr int TX = Tile<NDIM>::TX, TY = Tile<NDIM>::TY, NT = Tile<NDIM>::NT;
-  dim3 grid((p.nx + TX - 1) / TX, NDIM == 2 ? (p.ny + TY - 1) / TY : 1);
+  const int nby = NDIM == 2 ? (p.ny + TY - 1) / TY : 1;
+  if (NDIM == 1) rows = 0;
+  const int gy = rows == 0 ? nby : rows == 1 ? (nby < 2 ? nby : 2) : nby - 2;
+  if (gy <= 0) return cudaSuccess;   // no rows between the first and the last
+  dim3 grid((p.nx + TX - 1) / TX, gy);
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof none);
+  const CUtensorMap &map = tm ? *tm : none;
+  const int use = tm ? 1 : 0;
   switch ((p.col_type || p.irl ? 1 : 0) | (p.resi ? 2 : 0)) {
     case 0:
       stage_kernel<NDIM, NVM, STAGE, 0><<<grid, NT, stage_smem_bytes<NDIM, NVM, 0>(), s>>>(
-          p, Us, U0, Uo, ctrl, dt_mode, epi);
+          p, Us, U0, Uo, ctrl, dt_mode, epi, map, use, rows);
       break;
     case 1:
       stage_kernel<NDIM, NVM, STAGE, 1><<<grid, NT, stage_smem_bytes<NDIM, NVM, 1>(), s>>>(
-          p, Us, U0, Uo, ctrl, dt_mode, epi);
+          p, Us, U0, Uo, ctrl, dt_mode, epi, map, use, rows);
       break;
     case 2:
       stage_kernel<NDIM, NVM, STAGE, 2><<<grid, NT, stage_smem_bytes<NDIM, NVM, 2>(), s>>>(
-          p, Us, U0, Uo, ctrl, dt_mode, epi);
+          p, Us, U0, Uo, ctrl, dt_mode, epi, map, use, rows);
       break;
     default:
       stage_kernel<NDIM, NVM, STAGE, 3><<<grid, NT, stage_smem_bytes<NDIM, NVM, 3>(), s>>>(
-          p, Us, U0, Uo, ctrl, dt_mode, epi);
+          p, Us, U0, Uo, ctrl, dt_mode, epi, map, use, rows);
       break;
   }
   return cudaGetLastError();
 }
 
 static cudaError_t launch_stage(const KParams &p, int stage, const double *Us, const double *U0,
-                                double *Uo, DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s) {
+                                double *Uo, DevCtrl *ctrl, int dt_mode, int epi, cudaStream_t s,
+                                const CUtensorMap *tm, int rows) {
   if (p.ndim == 1) {
-    return stage == 1 ? launch_stage_t<1, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
-                      : launch_stage_t<1, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
+    return stage == 1 ? launch_stage_t<1, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, nullptr, 0)
+                      : launch_stage_t<1, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, nullptr, 0);
   }
   if (p.nvm == 9)
-    return stage == 1 ? launch_stage_t<2, 9, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
-                      : launch_stage_t<2, 9, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
-  return stage == 1 ? launch_stage_t<2, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s)
-                    : launch_stage_t<2, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s);
+    return stage == 1 ? launch_stage_t<2, 9, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, tm, rows)
+                      : launch_stage_t<2, 9, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, tm, rows);
+  return stage == 1 ? launch_stage_t<2, 8, 1>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, tm, rows)
+                    : launch_stage_t<2, 8, 2>(p, Us, U0, Uo, ctrl, dt_mode, epi, s, tm, rows);
+}
+
+static bool tile_map(const KParams &p, const double *U, CUtensorMap *map) {
+  if (p.ndim != 2) return false;
+  constexpr int TX = Tile<2>::TX, TY = Tile<2>::TY;
+  if (!tma_tile_ok(U, p.ix, p.jx, p.nvm + 5, (int)sizeof(double), p.m0 - kH, TX, TX + 2 * kH,
+                   TY + 2 * kH))
+    return false;
+  return tma_encode(map, U, p.ix, p.jx, p.nvm + 5, (int)sizeof(double), TX + 2 * kH, TY + 2 * kH);
 }
 
 static int grid_for(long long n, int threads) {
@@ -1341,7 +1413,8 @@ const Launchers &PIP_LAUNCHERS() {
   static const Launchers L = {PIP_FLAVOUR::prepare,       PIP_FLAVOUR::launch_stage,
                               PIP_FLAVOUR::launch_cfl,    PIP_FLAVOUR::launch_ghosts,
                               PIP_FLAVOUR::launch_flux,   PIP_FLAVOUR::launch_source,
-                              PIP_FLAVOUR::launch_nan,    PIP_FLAVOUR::launch_coefficients};
+                              PIP_FLAVOUR::launch_nan,    PIP_FLAVOUR::launch_coefficients,
+                              PIP_FLAVOUR::tile_map};
   return L;
 }
 

@@ -263,6 +263,26 @@ class DeviceBlock:
         self.ctx.dev_stage(k)
         self.last_stage = k
 
+    def dev_stage_rows(self, k: int, rows: int) -> None:
+        """Half of stage k: rows 1 the first and last tile rows (what the y exchange sends),
+        rows 2 the others."""
+        self.ctx.dev_stage_rows(k, rows)
+        self.last_stage = k
+
+    def record(self):
+        """An event on the context stream, after everything queued so far."""
+        ev = self.torch.cuda.Event()
+        ev.record(self._stream)
+        return ev
+
+    def wait(self, ev) -> None:
+        """The context stream waits for ev."""
+        self._stream.wait_event(ev)
+
+    def set_halo_stream(self, stream) -> None:
+        """Queue pack and unpack on `stream` (a torch stream; None: the context stream)."""
+        self.ctx.set_halo_stream(stream.cuda_stream if stream is not None else 0)
+
     def candidates(self):
         """int64 views of the device cfl candidates: (2 to MIN, 4 to MAX)."""
         a, b = self.ctx.dev_candidates()
@@ -326,10 +346,11 @@ class DecomposedRun:
                     self._send[(e.block.rank, f)] = e.buffer(n)
                     self._recv[(e.block.rank, f)] = e.buffer(n)
 
-    def halo(self) -> None:
+    def halo(self, stream=None) -> None:
         """mpi_bnd (MPI_rot.f90:128-339): per split direction, phase 1 sends the upper
         interior layers up and fills the lower ghost layers from below; phase 2 the
-        reverse."""
+        reverse.  With `stream` (a torch stream) the transfers run on it (the engines' pack
+        and unpack must have been pointed at it too)."""
         for d in (0, 1):
             for send_face in (2 * d + 1, 2 * d):
                 recv_face = send_face ^ 1
@@ -345,7 +366,10 @@ class DecomposedRun:
                         recvs.append((r, e.block.neighbor[recv_face], self._recv[(r, recv_face)][:n]))
                 if not sends and not recvs:
                     continue
-                if len(self.engines) == 1:
+                if stream is not None:
+                    with self.engines[0].torch.cuda.stream(stream):
+                        self.comm.exchange(sends, recvs)
+                elif len(self.engines) == 1:
                     with self.engines[0].stream():
                         self.comm.exchange(sends, recvs)
                 else:
@@ -373,12 +397,35 @@ class DecomposedRun:
         self.dt_history.append(dt)
         return dt
 
-    def run_device(self, nsteps: int, check_every: int = 64) -> int:
+    def _stage_overlapped(self, k: int) -> None:
+        """Stage k with its y exchange overlapped: the first and last tile rows, then the
+        exchange on the halo stream while the middle rows compute on the block streams."""
+        for e in self.engines:
+            e.dev_stage_rows(k, 1)
+        hs = self._halo_stream
+        for e in self.engines:
+            hs.wait_event(e.record())
+        self.halo(stream=hs)
+        for e in self.engines:
+            e.dev_stage_rows(k, 2)
+        done = self.engines[0].torch.cuda.Event()
+        done.record(hs)
+        for e in self.engines:
+            e.wait(done)
+
+    def run_device(self, nsteps: int, check_every: int = 64, overlap: bool = False) -> int:
         """nsteps steps with dt, cmax and time on the device (pip_dev_*): per step stage 1,
         exchange, stage 2 (with the next step's cfl candidates), exchange, MIN/MAX of the
         candidates over ranks -- all queued on the block streams, no host wait; the host
-        checks the stop flags every check_every steps.  Returns 0, 3 (NaN) or 4 (dt floor),
-        the same on every rank."""
+        checks the stop flags every check_every steps.  overlap (2D y-split): each exchange
+        runs on a stream of its own while the stage's middle tile rows compute.  Returns 0,
+        3 (NaN) or 4 (dt floor), the same on every rank."""
+        overlap = overlap and all(e.block.settings.ndim == 2 for e in self.engines)
+        if overlap:
+            torch = self.engines[0].torch
+            self._halo_stream = torch.cuda.Stream(device=self.engines[0].device)
+            for e in self.engines:
+                e.set_halo_stream(self._halo_stream)
         if not getattr(self, "_scaled", False):
             sg = self.comm.allreduce(max(e.block.sg for e in self.engines), "max")
             for e in self.engines:
@@ -397,18 +444,25 @@ class DecomposedRun:
             e.ctx.dev_begin(nsteps=nsteps)
         reduce()
         for n in range(nsteps):
-            for e in self.engines:
-                e.dev_stage(1)
-            self.halo()
-            for e in self.engines:
-                e.dev_stage(2)
-            self.halo()
+            if overlap:
+                self._stage_overlapped(1)
+                self._stage_overlapped(2)
+            else:
+                for e in self.engines:
+                    e.dev_stage(1)
+                self.halo()
+                for e in self.engines:
+                    e.dev_stage(2)
+                self.halo()
             reduce()
             if check_every and (n + 1) % check_every == 0 and n + 1 < nsteps:
                 stop = max(float(e.ctx.dev_poll()[1]) for e in self.engines)
                 if self.comm.allreduce(stop, "max") > 0.0:
                     break
         polls = [e.ctx.dev_poll() for e in self.engines]
+        if overlap:
+            for e in self.engines:
+                e.set_halo_stream(None)
         code = max(float(st) for st, _, _, _ in polls)
         code = int(self.comm.allreduce(code, "max"))
         self.time = polls[0][2]

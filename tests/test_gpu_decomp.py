@@ -13,7 +13,7 @@ from decomp_cases import make_case
 from helpers import interior, rel_l1
 from oracle import oracle as O
 from pip_b200 import capi, decomp, ics
-from pip_b200.params import PIP_MIXED
+from pip_b200.params import PIP_FP64, PIP_MIXED
 
 pytestmark = pytest.mark.gpu
 
@@ -125,11 +125,11 @@ def test_decomposition_rejects(gpu_lib):
         assert e.value.code == capi.PIP_ERR_PARAM
 
 
-def device_loop_run(s, Uh, Um, world, nsteps):
+def device_loop_run(s, Uh, Um, world, nsteps, overlap=False):
     engines = [decomp.DeviceBlock(decomp.block_of(s, world, r), decomp.scatter(s, Uh, world, r),
                                   decomp.scatter(s, Um, world, r)) for r in range(world)]
     run = decomp.DecomposedRun(engines, decomp.LocalComm(), divb=s.divb == 1)
-    st = run.run_device(nsteps, check_every=4)
+    st = run.run_device(nsteps, check_every=4, overlap=overlap)
     states = [e.download() for e in engines]
     run.close()
     return (st, run.time, run.steps, decomp.gather(s, [a for a, _ in states]),
@@ -162,3 +162,34 @@ def test_device_loop_mixed_matches_pip_run(gpu_lib):
         rh, rm = c.download()
     assert st == 0 and n == 9 and t == t1
     assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
+
+
+@pytest.mark.parametrize("precision", [PIP_FP64, PIP_MIXED])
+@pytest.mark.parametrize("world", [2, 3])
+def test_device_loop_overlapped_exchange_matches_pip_run(gpu_lib, precision, world):
+    """The y exchange overlapped with each stage: the first and last tile rows first, the
+    exchange on its own stream while the middle rows compute.  Blocks of 48 or 32 rows hold
+    several tile rows, so both launches of a stage do work; bitwise pip_run's result."""
+    s, Uh, Um = ics.orszag_tang(96, precision=precision)
+    st, t, n, hn, mn = device_loop_run(s, Uh, Um, world, 12, overlap=True)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        st1, t1, n1 = c.run(nsteps=12)
+        rh, rm = c.download()
+    assert st == 0 and st1 == 0 and n == n1 == 12 and t == t1
+    assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
+
+
+def test_stage_rows_enforce_their_order(gpu_lib):
+    s, Uh, Um = ics.orszag_tang(32)
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        c.dev_begin(nsteps=2)
+        L = capi.lib()
+        assert L.pip_dev_stage_rows(c.h, 1, 2) == capi.PIP_ERR_STATE     # middle rows first
+        assert L.pip_dev_stage_rows(c.h, 2, 1) == capi.PIP_ERR_STATE     # stage 2 before 1
+        assert L.pip_dev_stage_rows(c.h, 1, 1) == capi.PIP_OK
+        assert L.pip_dev_stage(c.h, 2) == capi.PIP_ERR_STATE             # stage 1 unfinished
+        assert L.pip_dev_stage_rows(c.h, 1, 2) == capi.PIP_OK
+        assert L.pip_dev_stage(c.h, 2) == capi.PIP_OK
+        c.dev_poll()
