@@ -1,12 +1,14 @@
 /*
- * pip_ensemble.h -- batched ensembles of independent 1D two-fluid runs.
+ * pip_ensemble.h -- batched ensembles of independent 1D and 2D two-fluid runs.
  *
  * No counterpart in the reference: PIP runs one simulation per process.  An ensemble holds
- * many 1D runs of different sizes and parameters (each described by its own pip_params,
- * ndim = 1, precision = PIP_MIXED) and advances all of them to an end time in one
+ * many runs of different sizes and parameters (each described by its own pip_params,
+ * ndim = 1 or 2, precision = PIP_MIXED) and advances all of them to an end time in one
  * persistent kernel launch, captured in a CUDA graph: each thread block takes whole runs
- * from a work queue ordered longest first and steps each with its own dt.  Per-run
- * arithmetic is that of the single-run FP32-mixed form.
+ * from a work queue ordered longest first and steps each with its own dt.  A 1D run is
+ * walked in chunks of cells, a 2D run tile by tile (16 x 14 cells) with the single-run
+ * stage kernel's tile step.  Per-run arithmetic is that of the single-run FP32-mixed form.
+ * An ensemble with a 2D run needs at least 256 threads per block.
  */
 #ifndef PIP_ENSEMBLE_H
 #define PIP_ENSEMBLE_H
@@ -39,7 +41,8 @@ int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *de
 int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, double *time,
                         int64_t *steps, int *status);
 
-/* Launch configuration: threads per block (128, 256, 512, 1024) and blocks per SM. */
+/* Launch configuration: threads per block (128, 256, 512, 1024; not 128 when a run is 2D)
+ * and blocks per SM. */
 int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm);
 
 /* Autotuner: times every configuration the device can hold on a probe run to t_probe from

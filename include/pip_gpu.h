@@ -35,7 +35,9 @@ enum pip_status_code {
   PIP_ERR_ITER = 5,    /* an iterative solver or bounded device loop hit its limit */
   PIP_ERR_STATE = 6,   /* call out of order, e.g. a step before any upload */
   PIP_ERR_NOMEM = 7,   /* device allocation failed */
-  PIP_ERR_NULL = 8     /* a required pointer argument was NULL */
+  PIP_ERR_NULL = 8,    /* a required pointer argument was NULL */
+  PIP_ERR_RATE = 9     /* a rate of the 6-level hydrogen model came out negative (where
+                          get_col_ion_coeff stops the run, PIP_rot.f90:546-557,592-601) */
 };
 
 enum pip_precision {
@@ -58,6 +60,11 @@ enum pip_ir_law {
   /* set_IR type 3 (PIP_rot.f90:173-228): the type-2 rates scaled to the ionisation
    * equilibrium of T_norm (f_n, f_p, tfac from flag_col's parity and beta); same calls. */
   PIP_IR_POPESCU_EQ = 3,
+  /* set_IR type 4 (PIP_rot.f90:232-311): the 6-level hydrogen atom (Johnson 1972 collisional
+   * rates, PIP_rot.f90:361-616) with level populations Nexcite advanced after every RK stage
+   * (hydrogen_excitation_update, PIP_rot.f90:1026-1159).  Needs pip_set_nlevel (the
+   * exponential-integral table and the model's settings) and pip_set_nexcite; FP64 form. */
+  PIP_IR_NLEVEL = 4,
   /* Gm_ion = ir_ion_coef*T^-1/2*exp(-ir_chi/T), Gm_rec = ir_rec_coef*T^-1/2 with
    * T = gm*p_i/(2 rho_i) (get_Te_MHD, Scheme_rot.f90:104-110); the rates are frozen at
    * the start of each step as set_IR is (main.f90:32-34).  This law is new: none of
@@ -72,8 +79,9 @@ enum pip_ir_law {
  *   flag_eqs=PIP (two-fluid), flag_sch=0, flag_hll=2, s_order=2, t_order=2, flag_time=0,
  *   ndim 1 or 2 (kx=1), flag_divb 0/1 (forced 0 in 1D), flag_col 1..7 (2..7 with
  *   precision PIP_FP64 only),
- *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ (FP64
- *   form; T_norm and n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type 1 or 2,
+ *   flag_pip_imp 0/1, flag_ir 0, PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ,
+ *   PIP_IR_NLEVEL (FP64 form; T_norm and n_norm > 0) or PIP_IR_POWERLAW, with flag_ir_type
+ *   1 or 2 (or 0, the ionisation-potential form, with PIP_IR_NLEVEL),
  *   flag_bnd in {1,2,3,4,5,6,7,10,11}, flag_resi 0, 1 (a fixed eta field) or 2 (eta
  *   recomputed at every RK stage, resi_type 2 or 3; FP64 form, not with flag_heat), no
  *   viscosity/gravity/ambipolar diffusion.
@@ -97,7 +105,9 @@ typedef struct pip_params {
                               (PIP_rot.f90:44-97, set_coefficients Solver_rot.f90:95-122) */
   int32_t flag_pip_imp;    /* 0: explicit collision source; 1: exponential form */
   int32_t flag_ir;         /* pip_ir_law */
-  int32_t flag_ir_type;    /* IR energy exchange: 1 Khomenko, 2 Singh (PIP_rot.f90:1399-1411) */
+  int32_t flag_ir_type;    /* IR energy exchange: 1 Khomenko, 2 Singh (PIP_rot.f90:1399-1411),
+                              0 with the ionisation potential IRgetionpot (:1381-1397, set_IR
+                              type 4 only) */
   int32_t flag_heat;       /* 0 or 1 (implicit anisotropic conduction of the ions) */
   int32_t hc_max;          /* BiCGstab iteration limit */
   int32_t flag_bnd[6];     /* x_l, x_r, y_l, y_r, z_l, z_r boundary codes */
@@ -289,6 +299,57 @@ int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
 int pip_set_hc_wait_limit(pip_ctx *ctx, int polls);
 
 /*
+ * set_IR type 4 (flag_ir = PIP_IR_NLEVEL): the 6-level hydrogen model.
+ *
+ * The Fortran keeps the model's state in globalvar (Nexcite, colrat, ion_pot, Gm_rec_ref)
+ * and reads expintcalc/colexp.dat once (expintread, PIP_rot.f90:315-357, called by the
+ * initial condition).  Here:
+ *   pip_colexp_table   regenerates that table: colexpintcalc.f90's rows (yn, E0(yn), E1(yn),
+ *                      E2(yn)) for yn = ymin + t*(108-ymin)/nsamps, t = 0..nsamps, as a
+ *                      (4, nsamps+1) column-major array -- the layout expintread fills
+ *                      expinttab with (the reference's file has nsamps = 100000).
+ *   pip_set_nlevel     hands the table and the model's settings to the context; the next
+ *                      prologue-like call (the first pip_cfl / pip_step / pip_run) runs set_IR
+ *                      type 4's fresh-start block (PIP_rot.f90:250-280): Gm_rec_ref from the
+ *                      rates at (T_norm, n_norm) with cell (1,1,1)'s populations, and the
+ *                      initial ion_pot.
+ *   pip_set_nexcite    Nexcite(ix,jx,kx,6): levels 1-5 then the ions, ghosts included, in
+ *   pip_get_nexcite    the state's normalisation (the sum of levels 1-5 is rho_n); the
+ *                      excitation update keeps Nexcite(6) = rho_i and the sum = rho_n.
+ *   pip_get_colrat     colrat(ix,jx,kx,6,6) of the last set_IR.
+ *   pip_get_ion_pot    ion_pot(ix,jx,kx) of the last source_PIP (flag_IR_type 0).
+ *   pip_nlevel_gm_rec_ref  the normalisation rate Gm_rec_ref.
+ * Every RK stage runs set_IR (the rates from the stage state), the stage, then
+ * hydrogen_excitation_update over dt_sub (Solver_rot.f90:218-220); every cfl adds
+ * cfl_pip_ir's and cfl_pip_ir_nexcite's bounds (Scheme_rot.f90:315-335).  pip_run steps on
+ * the host (a launch per kernel), single rank only (pip_set_neighbors and pip_dev_begin return
+ * PIP_ERR_PARAM).  Without pip_set_nlevel those calls return PIP_ERR_STATE.  A negative rate
+ * (where get_col_ion_coeff stops the run) makes pip_run return PIP_ERR_RATE.
+ */
+typedef struct pip_nlevel {
+  int32_t n_levels;        /* nlevels setting: 5 (the hydrogen atom's levels 1-5, then ions) */
+  int32_t flag_rad;        /* 0 or 1: collisional rates only (flag_rad >= 2 adds
+                              get_radrat_fixed's radiative rates, not built: PIP_ERR_PARAM) */
+  int32_t deriv;           /* convective derivative of the excitation update: 1 the two-point
+                              form, 4 the five-point form (derivative, Scheme_rot.f90:692-736,
+                              for s_order 1 and 4), 0 none.  For s_order 2, the scheme of this
+                              path, the reference's derivative sets nothing and the term reads
+                              an uninitialised array, so the form is a setting here. */
+  int32_t reserved;
+  double n0fac;            /* globalvar n0fac, f_p_ini, f_p_p_ini (set by the initial */
+  double f_p_ini;          /* condition, e.g. KHnlev.f90:103-105): electron density */
+  double f_p_p_ini;        /* U_m(1)*n_norm/n0fac, tfac of PIP_rot.f90:240-248 */
+} pip_nlevel;
+
+int pip_colexp_table(int64_t nsamps, double *out);
+int pip_set_nlevel(pip_ctx *ctx, const pip_nlevel *cfg, const double *table, int64_t nrows);
+int pip_set_nexcite(pip_ctx *ctx, const double *nexcite);
+int pip_get_nexcite(pip_ctx *ctx, double *nexcite);
+int pip_get_colrat(pip_ctx *ctx, double *colrat);
+int pip_get_ion_pot(pip_ctx *ctx, double *ion_pot);
+int pip_nlevel_gm_rec_ref(pip_ctx *ctx, double *gm_rec_ref);
+
+/*
  * Domain decomposition over ranks (one context per rank and device, each holding its own
  * block with ghost cells, as the Fortran code does after set_mpi, MPI_rot.f90:11-41).
  *
@@ -356,18 +417,19 @@ int pip_dev_begin(pip_ctx *ctx, int64_t nsteps, double t_end);
 int pip_dev_stage(pip_ctx *ctx, int stage);
 
 /* The y exchange overlapped with the stage (2D; no counterpart in the reference, whose
- * mpi_bnd runs after the whole stage).  A stage is queued in two launches on the context
- * stream: pip_dev_stage_rows(ctx, k, 1) computes the first and the last row of tiles -- the
- * cells the exchange sends -- and pip_dev_stage_rows(ctx, k, 2) the rows between them;
- * together they equal pip_dev_stage(ctx, k) bit for bit.  Between the two calls the caller
- * records an event on the context stream; the exchange (pack, transfer, unpack) runs on
- * another stream after that event while the middle rows compute, and the context stream
- * waits for the exchange before the next stage.  The middle rows neither read nor write
- * what the exchange reads or writes (it reads the boundary rows' cells, it writes the ghost
- * rows of the exchanged faces, and the stage reads only its input array).
+ * mpi_bnd runs after the whole stage).  pip_dev_stage_split(ctx, k, &bs) queues stage k
+ * as two launches: the first and the last row of tiles -- every cell the exchange sends --
+ * on a high-priority stream of the context, returned in bs, and the rows between them on
+ * the context stream, concurrently; the context stream then waits for the boundary rows.
+ * Together they equal pip_dev_stage(ctx, k) bit for bit.  The caller records an event on
+ * bs right after the call and runs the exchange (pack, transfer, unpack) on a stream of its
+ * own after that event while the middle rows compute; the context stream waits for the
+ * exchange before the next stage.  The middle rows neither read nor write what the
+ * exchange reads or writes (it reads the boundary rows' cells, it writes the ghost rows of
+ * the exchanged faces, and a stage reads only its input array).
  * pip_set_halo_stream(ctx, stream) makes pip_halo_pack / pip_halo_unpack queue on `stream`
  * (NULL: the context stream again). */
-int pip_dev_stage_rows(pip_ctx *ctx, int stage, int rows);
+int pip_dev_stage_split(pip_ctx *ctx, int stage, void **boundary_stream);
 int pip_set_halo_stream(pip_ctx *ctx, void *stream);
 int pip_dev_candidates(pip_ctx *ctx, void **dt_min, void **rho_gr_max);
 int pip_dev_poll(pip_ctx *ctx, int *done, double *time, int64_t *steps);

@@ -72,6 +72,18 @@ def lib():
         L.orc_ir_rates.argtypes = [vp, dp, dp]
         L.orc_alpha_c.argtypes = [vp, dp]
         L.orc_alpha_c.restype = ctypes.c_int
+        L.orc_expint_table.argtypes = [ctypes.c_long, dp]
+        L.orc_expint_table.restype = None
+        L.orc_set_nlevel.argtypes = [vp, ctypes.c_int, d, d, d, dp, ctypes.c_long]
+        L.orc_set_nlevel.restype = ctypes.c_int
+        L.orc_set_nexcite.argtypes = [vp, dp]
+        L.orc_get_nexcite.argtypes = [vp, dp]
+        L.orc_get_colrat.argtypes = [vp, dp]
+        L.orc_get_ion_pot.argtypes = [vp, dp]
+        L.orc_gm_rec_ref.argtypes = [vp]
+        L.orc_gm_rec_ref.restype = d
+        L.orc_nlevel_status.argtypes = [vp]
+        L.orc_nlevel_status.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -83,6 +95,13 @@ def _ptr(a: np.ndarray):
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+def expint_table(nsamps: int = 100000) -> np.ndarray:
+    """colexpintcalc.f90's exponential-integral table, shape (nsamps+1, 4): yn, E0, E1, E2."""
+    t = np.empty((nsamps + 1, 4))
+    lib().orc_expint_table(int(nsamps), _ptr(t))
+    return t
 
 
 class Oracle:
@@ -221,6 +240,45 @@ class Oracle:
 
     def has_nan(self) -> bool:
         return bool(lib().orc_has_nan(self.h))
+
+    # ---- set_IR type 4 (the 6-level hydrogen model)
+    def set_nlevel(self, table: np.ndarray, deriv: int = 1, n0fac: float = 1.0,
+                   f_p_ini: float = 1.0, f_p_p_ini: float = 1.0) -> None:
+        """expinttab (rows yn, E0, E1, E2) and the model's settings."""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        st = lib().orc_set_nlevel(self.h, int(deriv), float(n0fac), float(f_p_ini),
+                                  float(f_p_p_ini), _ptr(t), int(t.shape[0]))
+        if st:
+            raise ValueError("orc_set_nlevel rejected the settings (%d)" % st)
+
+    def set_nexcite(self, nex: np.ndarray) -> None:
+        """Nexcite, shape (6, jx, ix): levels 1-5 then the ions."""
+        n = np.ascontiguousarray(nex, dtype=np.float64).reshape((6,) + self.shape_h[1:])
+        lib().orc_set_nexcite(self.h, _ptr(n))
+
+    def nexcite(self) -> np.ndarray:
+        n = np.empty((6,) + self.shape_h[1:])
+        lib().orc_get_nexcite(self.h, _ptr(n))
+        return n
+
+    def colrat(self) -> np.ndarray:
+        """colrat of the last set_IR as [a, b] = colrat(a+1, b+1), shape (6, 6, jx, ix)."""
+        c = np.empty((6, 6) + self.shape_h[1:])
+        lib().orc_get_colrat(self.h, _ptr(c))
+        return np.ascontiguousarray(c.transpose(1, 0, 2, 3))
+
+    def ion_pot(self) -> np.ndarray:
+        a = np.empty(self.shape_h[1:])
+        lib().orc_get_ion_pot(self.h, _ptr(a))
+        return a
+
+    @property
+    def gm_rec_ref(self) -> float:
+        return lib().orc_gm_rec_ref(self.h)
+
+    @property
+    def nlevel_status(self) -> int:
+        return lib().orc_nlevel_status(self.h)
 
 
 def run_case(s: Settings, U_h, U_m, nsteps: int = 0, t_end: Optional[float] = None,

@@ -43,6 +43,22 @@ struct orc_ctx {
   int resi;                          /* flag_resi 1: resistive flux with a fixed eta field;
                                         2: eta from set_resistivity at every RK stage */
   double *eta;                       /* globalvar eta (set_resistivity), nc values */
+  /* set_IR type 4, the 6-level hydrogen model */
+  int nlev_deriv;                    /* convective derivative: 0 none, 1 two-point, 4 five-point */
+  double n0fac, f_p_ini, f_p_p_ini;  /* globalvar normalisation of the model */
+  double *etab;                      /* expinttab (4 x netab, column-major) */
+  long netab;
+  double *nex;                       /* Nexcite (ix,jx,kx,6) */
+  double *colrat;                    /* colrat (ix,jx,kx,6,6) */
+  double *ion_pot;                   /* globalvar ion_pot: the last irgetionpot, nc values */
+  double gm_rec_ref;                 /* Gm_rec_ref */
+  int nlev_init;                     /* the prologue's block of set_IR type 4 has run */
+  int nlev_bad;                      /* a negative rate (the reference stops there) */
+  struct {
+    double gw[6], eion[6], rn[6], bn[6];
+    double xrat[5][5], enn[5][5], rnn[5][5], ann[5][5], bnn[5][5], lgt[5][5];
+    double an0[5], bn0[5], lgi[5];
+  } nk;                              /* get_col_ion_coeff's cell-independent coefficients */
 };
 
 static void ensure_coefficients(orc_ctx *c);
@@ -814,6 +830,407 @@ static void set_collisional(orc_ctx *c) {
   }
 }
 
+/* ---------------------------------------------------------------- 6-level hydrogen model */
+
+/* Literals the Fortran writes without a d0 exponent are default reals: rounded to float
+ * first (kboltz, melec, a0bohr of get_col_ion_coeff, PIP_rot.f90:366-369; 2.18e-18 of
+ * :383; 1.0e14 of :591; 1.e-16 of :1138; Eev of IRgetionpot :1170; 8.6173e-5 of :1224). */
+#define NL_KB ((double)1.38064852e-23f)
+#define NL_ME ((double)9.10938356e-31f)
+#define NL_A0 ((double)5.29e-11f)
+#define NL_EJ ((double)2.18e-18f)
+#define NL_E14 ((double)1.0e14f)
+#define NL_FLOOR ((double)1.e-16f)
+#define NL_EVK ((double)8.6173e-5f)
+#define NL_KBHAT 1.38064852
+#define NL_MEHAT 9.10938356
+#define NL_HHAT 6.62607004
+
+/* colexpintcalc.f90's ionexpfittest: trapezoid sums of exp(-z*t)*t**(-istar) from t = 1 in
+ * steps of 0.001 until a step adds no more than 1e-4 of the first. */
+static double nl_expint_trap(double zhat, double istar) {
+  const double stepsize = 0.001, tol = 0.0001;
+  double a = 1.0, b = a + stepsize;
+  double fa = exp(-zhat * a) * pow(a, -istar), fb = exp(-zhat * b) * pow(b, -istar);
+  double sol0 = 0.5 * (b - a) * (fa + fb), sol = sol0, dif = 1.0;
+  while (dif > tol) {
+    a = b;
+    b = a + stepsize;
+    fa = exp(-zhat * a) * pow(a, -istar);
+    fb = exp(-zhat * b) * pow(b, -istar);
+    double solt = 0.5 * (b - a) * (fa + fb);
+    sol = sol + solt;
+    dif = solt / sol0;
+  }
+  return sol;
+}
+
+/* colexpintcalc.f90 (the generator of expintcalc/colexp.dat, which expintread loads,
+ * PIP_rot.f90:315-333): nsamps+1 rows (yn, E0(yn), E1(yn), E2(yn)) for
+ * yn = ymin + t*(108 - ymin)/nsamps; out is column-major (4, nsamps+1). */
+void orc_expint_table(long nsamps, double *out) {
+  const double ymin = 0.54 / 13.6 * NL_EJ / NL_KB / 100000.0, ymax = 108.0;
+  const double dy = (ymax - ymin) / (double)nsamps;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long t = 0; t <= nsamps; ++t) {
+    double yn = ymin + (double)t * dy;
+    out[4 * t] = yn;
+    out[4 * t + 1] = nl_expint_trap(yn, 0.0);
+    out[4 * t + 2] = nl_expint_trap(yn, 1.0);
+    out[4 * t + 3] = nl_expint_trap(yn, 2.0);
+  }
+}
+
+/* The cell-independent part of get_col_ion_coeff (PIP_rot.f90:378-439, 507-524), in the
+ * Fortran operation order. */
+static void nl_constants(orc_ctx *c) {
+  static const double ev[6] = {13.6, 3.4, 1.51, 0.85, 0.54, 0.0};
+  static const double gw[6] = {2.0, 8.0, 18.0, 32.0, 50.0, 1.0};
+  for (int k = 0; k < 6; ++k) {
+    double n = (double)(k + 1);
+    c->nk.gw[k] = gw[k];
+    c->nk.eion[k] = ev[k] / 13.6 * NL_EJ;
+    c->nk.rn[k] = k == 0 ? 0.45 : 1.94 * pow(n, -1.57);
+    c->nk.bn[k] = k == 0 ? -0.603
+                         : (1.0 / n) * (4.0 - 18.63 / n + 36.24 / (n * n) - 28.09 / (n * n * n));
+  }
+  const double pi = PI_REF;
+  for (int a = 0; a < 5; ++a) {
+    double ri = (double)(a + 1);
+    for (int b = a + 1; b < 5; ++b) {
+      double rj = (double)(b + 1), r = ri / rj;
+      double x = 1.0 - r * r;
+      double g;
+      if (a == 0) g = 1.1330 - 0.4059 / x + 0.07014 / (x * x);
+      else if (a == 1) g = 1.0785 - 0.2319 / x + 0.02947 / (x * x);
+      else
+        g = 0.9935 + 0.2328 / ri - 0.1296 / (ri * ri) -
+            (1.0 / x) * (1.0 / ri) * (0.6282 - 0.5598 / ri + 0.5299 / (ri * ri)) +
+            (1.0 / x) * (1.0 / x) * (1.0 / (ri * ri)) * (0.3887 - 1.181 / ri + 1.470 / (ri * ri));
+      double fnn = 32.0 / 3.0 / sqrt(3.0) / pi * ri / (rj * rj * rj) / (x * x * x) * g;
+      c->nk.xrat[a][b] = x;
+      c->nk.enn[a][b] = c->nk.eion[a] - c->nk.eion[b];
+      c->nk.rnn[a][b] = c->nk.rn[a] * x;
+      c->nk.ann[a][b] = 2.0 * (ri * ri) / x * fnn;
+      c->nk.bnn[a][b] = 4.0 * ((ri * ri) * (ri * ri)) / (rj * rj * rj) / (x * x) *
+                        (1.0 + 4.0 / 3.0 / x + c->nk.bn[a] / (x * x));
+      c->nk.lgt[a][b] = log(2.0 * (ri * ri) / x);
+    }
+    double g1, g2, g3;
+    if (a == 0) { g1 = 1.1330; g2 = -0.4059; g3 = 0.07014; }
+    else if (a == 1) { g1 = 1.0785; g2 = -0.2319; g3 = 0.02947; }
+    else {
+      g1 = 0.9935 + 0.2328 / ri - 0.1296 / (ri * ri);
+      g2 = (-1.0 / ri) * (0.6282 - 0.5598 / ri + 0.5299 / (ri * ri));
+      g3 = (1.0 / ri) * (1.0 / ri) * (0.3887 - 1.181 / ri + 1.470 / (ri * ri));
+    }
+    c->nk.an0[a] = 32.0 / 3.0 / sqrt(3.0) / pi * ri + g1 / 3.0 + g2 / 4.0 + g3 / 5.0;
+    c->nk.bn0[a] = 2.0 / 3.0 * (ri * ri) * (5.0 + c->nk.bn[a]);
+    c->nk.lgi[a] = log(2.0 * (ri * ri));
+  }
+}
+
+/* ionexpfitinterp2 with rad = 0 (PIP_rot.f90:919-946): quadratic interpolation of E_i at z
+ * through table rows xindex..xindex+2.  The reference clamps xindex to 1..n-1 and then reads
+ * row n+1 at the top end, past its table; here xindex stops at n-2. */
+static double nl_interp(const orc_ctx *c, double z, int i) {
+  const double *t = c->etab;
+  long n = c->netab;
+  double xmin = t[0], xmax = t[4 * (n - 1)], xrange = xmax - xmin;
+  double f = floor((z - xmin) / xrange * (double)n);
+  long xi;
+  if (!(f > 0.0)) xi = 1;
+  else if (f >= (double)n) xi = n - 1;
+  else xi = (long)f;
+  if (xi > n - 2) xi = n - 2;
+  const double *r0 = t + 4 * (xi - 1), *r1 = r0 + 4, *r2 = r0 + 8;
+  double x0 = r0[0], x1 = r1[0], x2 = r2[0];
+  double w0 = ((z - x1) * (z - x2)) / ((x0 - x1) * (x0 - x2));
+  double w1 = ((z - x0) * (z - x2)) / ((x1 - x0) * (x1 - x2));
+  double w2 = ((z - x0) * (z - x1)) / ((x2 - x0) * (x2 - x1));
+  return w0 * r0[i + 1] + w1 * r1[i + 1] + w2 * r2[i + 1];
+}
+
+/* get_col_ion_coeff (PIP_rot.f90:361-616) for one cell of electron temperature te [K] and
+ * density ne: colrat (6x6, cr[a*6+b] = colrat(a+1,b+1)) and the unnormalised sums
+ * gi = sum max(Nexcite(ii)*colrat(ii,6),0), gr = sum max(Nexcite(6)*colrat(6,ii),0).
+ * Returns 1 where the reference would stop on a negative rate. */
+static int nl_cell(const orc_ctx *c, double te, double ne, const double *nx, double *cr,
+                   double *gi, double *gr) {
+  const double pi = PI_REF;
+  double colex[5][6];
+  int bad = 0;
+  double s = sqrt(8.0 * NL_KB * te / pi / NL_ME);
+  for (int a = 0; a < 5; ++a) {
+    double ri = (double)(a + 1);
+    for (int b = a + 1; b < 5; ++b) {
+      double yhat = c->nk.enn[a][b] / NL_KB / te;
+      double zhat = c->nk.rnn[a][b] + c->nk.enn[a][b] / NL_KB / te;
+      double E1y = nl_interp(c, yhat, 1), E1z = nl_interp(c, zhat, 1);
+      double E2y = nl_interp(c, yhat, 2), E2z = nl_interp(c, zhat, 2);
+      double ann = c->nk.ann[a][b];
+      colex[a][b] = ne * s * 2.0 * (ri * ri) / c->nk.xrat[a][b] * pi * (NL_A0 * NL_A0) *
+                    (yhat * yhat) *
+                    (ann * ((1.0 / yhat + 0.5) * E1y - (1.0 / zhat + 0.5) * E1z) +
+                     (c->nk.bnn[a][b] - ann * c->nk.lgt[a][b]) * (E2y / yhat - E2z / zhat));
+    }
+    double yn = c->nk.eion[a] / NL_KB / te;
+    double zn = c->nk.rn[a] + c->nk.eion[a] / NL_KB / te;
+    double E1y = nl_interp(c, yn, 1), E1z = nl_interp(c, zn, 1);
+    double E2y = nl_interp(c, yn, 2), E2z = nl_interp(c, zn, 2);
+    double E0y = nl_interp(c, yn, 0), E0z = nl_interp(c, zn, 0);
+    double ziyn = E0y - 2.0 * E1y + E2y, zizn = E0z - 2.0 * E1z + E2z;
+    double an0 = c->nk.an0[a];
+    colex[a][5] = ne * s * 2.0 * (ri * ri) * pi * (NL_A0 * NL_A0) * (yn * yn) *
+                  (an0 * (E1y / yn - E1z / zn) + (c->nk.bn0[a] - an0 * c->nk.lgi[a]) * (ziyn - zizn));
+    if (colex[a][5] < 0.0) bad = 1;
+  }
+  for (int k = 0; k < 36; ++k) cr[k] = 0.0;
+  for (int a = 0; a < 5; ++a) {
+    for (int b = 0; b < 5; ++b) {
+      if (a == b) cr[a * 6 + b] = 0.0;
+      else if (b > a) cr[a * 6 + b] = c->nk.gw[a] / c->nk.gw[b] * colex[a][b];
+      else cr[a * 6 + b] = colex[b][a] * exp(-((c->nk.eion[b] - c->nk.eion[a]) / NL_KB / te));
+    }
+    cr[a * 6 + 5] = colex[a][5] * exp(-((c->nk.eion[5] - c->nk.eion[a]) / NL_KB / te));
+  }
+  for (int a = 0; a < 5; ++a)
+    cr[30 + a] = ne * cr[a * 6 + 5] * c->nk.gw[a] / c->nk.gw[5] / 2.0 *
+                 pow(2.0 * pi * NL_MEHAT * NL_KBHAT * te / NL_HHAT / NL_HHAT * NL_E14, -3.0 / 2.0) *
+                 exp(c->nk.eion[a] / NL_KB / te);
+  for (int k = 0; k < 36; ++k)
+    if (cr[k] < 0.0) bad = 1;
+  double si = 0.0, sr = 0.0;
+  for (int a = 0; a < 5; ++a) {
+    si = si + fmx(nx[a] * cr[a * 6 + 5], 0.0);
+    sr = sr + fmx(nx[5] * cr[30 + a], 0.0);
+  }
+  *gi = si;
+  *gr = sr;
+  return bad;
+}
+
+/* tfac of set_IR type 4 (PIP_rot.f90:240-248); 5.0/3.0 is a default-real quotient there. */
+static double nl_tfac(const orc_ctx *c) {
+  const pip_params *p = &c->p;
+  if (p->flag_col % 2 == 1) return p->t_norm / ((double)(5.0f / 3.0f) * c->f_p_p_ini / c->f_p_ini);
+  return p->beta / 2.0 * c->f_p_p_ini * 5.0 / 6.0 / c->f_p_ini;
+}
+
+/* IRgetionpot (PIP_rot.f90:1162-1235) on cell q from colrat cr and populations nx. */
+static double nl_ionpot(const orc_ctx *c, const double *cr, const double *nx) {
+  static const float eevf[6] = {13.6f, 3.4f, 1.51f, 0.85f, 0.54f, 0.0f};
+  double eev[6];
+  for (int k = 0; k < 6; ++k) eev[k] = (double)eevf[k];
+  double il = 0.0, ig = 0.0;
+  for (int i = 0; i < 5; ++i) {
+    il = il + cr[i * 6 + 5] * eev[i] * nx[i];
+    ig = ig + cr[30 + i] * eev[i] * nx[5];
+    for (int j = 1; j < 5; ++j) {
+      il = il + nx[i] * cr[i * 6 + j] * (eev[i] - eev[j]);
+      ig = ig + nx[j] * (cr[j * 6 + i] * (eev[i] - eev[j]));
+    }
+  }
+  const pip_params *p = &c->p;
+  double en;
+  if (p->flag_col % 2 == 1) en = (il - ig) / p->gm / p->t_norm / NL_EVK;
+  else en = (il - ig) / (p->beta / p->t_norm / 2.0 / NL_EVK);
+  return en / c->gm_rec_ref * p->t_ir;
+}
+
+/* set_IR type 4 (PIP_rot.f90:232-296): get_Te_HD/get_Te_MHD rewrite both energies; on the
+ * first call of a fresh run (the prologue's, :250-280) Gm_rec_ref from the rates at
+ * (T_norm, n_norm) with cell (1,1,1)'s populations and ion_pot from those rates; then
+ * colrat of every cell from Te_p*T0/tfac and U_m(1)*n0/n0fac, and the normalised rates. */
+static void set_ir_nlevel(orc_ctx *c) {
+  const pip_params *p = &c->p;
+  size_t nc = c->nc;
+  if (!c->etab) {
+    c->nlev_bad = 1;   /* no table: orc_set_nlevel was not called */
+    return;
+  }
+  double T0 = p->t_norm, n0 = p->n_norm, tfac = nl_tfac(c);
+  double *te = malloc(sizeof(double) * nc);
+  for (size_t q = 0; q < nc; ++q) {
+    double te_n;
+    get_te_cell(c, q, &te[q], &te_n);
+  }
+  if (!c->nlev_init) {
+    double nx0[6], cr[36], gi, gr;
+    for (int k = 0; k < 6; ++k) nx0[k] = c->nex[k * nc];
+    nl_cell(c, T0, n0, nx0, cr, &gi, &gr);
+    c->gm_rec_ref = gr;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < nc; ++q) {
+      double nx[6];
+      for (int k = 0; k < 6; ++k) nx[k] = c->nex[q + k * nc];
+      c->ion_pot[q] = nl_ionpot(c, cr, nx);
+    }
+    c->nlev_init = 1;
+  }
+  const double *Uh = c->U_h, *Um = c->U_m;
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (size_t q = 0; q < nc; ++q) {
+    double nx[6], cr[36], gi, gr;
+    for (int k = 0; k < 6; ++k) nx[k] = c->nex[q + k * nc];
+    bad |= nl_cell(c, te[q] * T0 / tfac, Um[q] * n0 / c->n0fac, nx, cr, &gi, &gr);
+    for (int k = 0; k < 36; ++k) c->colrat[q + k * nc] = cr[(k % 6) * 6 + k / 6];
+    c->gm_ion[q] = gi / Uh[q] / c->gm_rec_ref * p->t_ir;
+    c->gm_rec[q] = gr / Um[q] / c->gm_rec_ref * p->t_ir;
+  }
+  c->nlev_bad |= bad;
+  free(te);
+}
+
+/* colrat(a+1,b+1) of cell q (the (ix,jx,kx,6,6) array: plane a + 6*b). */
+#define NL_CR(c, q, a, b) ((c)->colrat[(q) + (size_t)((a) + 6 * (b)) * (c)->nc])
+
+/* derivative (Scheme_rot.f90:692-736) of plane v along dir (1 or 2): order 4 (s_order 4's
+ * five-point form) or 1 (s_order 1's two-point form); 0 leaves der at zero.  Cells the
+ * stencil does not reach are zero here (the reference leaves them unset, and its s_order 2
+ * sets no cell at all). */
+static void nl_derivative(const orc_ctx *c, const double *v, double *der, int dir) {
+  int ix = c->ix, jx = c->jx, order = c->nlev_deriv;
+  memset(der, 0, sizeof(double) * c->nc);
+  if (order == 0) return;
+  int w = order == 4 ? 2 : 1;
+  for (int j = 0; j < jx; ++j)
+    for (int i = 0; i < ix; ++i) {
+      size_t q = AT(c, i, j, 0);
+      if (dir == 1) {
+        if (i < w || i >= ix - w) continue;
+        if (order == 4)
+          der[q] = (-v[q + 2] + 8.0 * v[q + 1] - 8.0 * v[q - 1] + v[q - 2]) / (12.0 * c->dx[i]);
+        else
+          der[q] = (v[q + 1] - v[q - 1]) / (2.0 * c->dx[i]);
+      } else {
+        if (j < w || j >= jx - w) continue;
+        size_t s = (size_t)ix;
+        if (order == 4)
+          der[q] = (-v[q + 2 * s] + 8.0 * v[q + s] - 8.0 * v[q - s] + v[q - 2 * s]) /
+                   (12.0 * c->dy[j]);
+        else
+          der[q] = (v[q + s] - v[q - s]) / (2.0 * c->dy[j]);
+      }
+    }
+}
+
+/* The convective term of level ii (0-based) at every cell: d(Nexcite)/dx*vx_n (+ y). */
+static void nl_conv(const orc_ctx *c, int ii, double *conv, double *tmp) {
+  size_t nc = c->nc;
+  const double *Uh = c->U_h, *v = c->nex + ii * nc;
+  nl_derivative(c, v, tmp, 1);
+  for (size_t q = 0; q < nc; ++q) conv[q] = tmp[q] * Uh[q + nc] / Uh[q];
+  if (c->p.ndim > 1) {
+    nl_derivative(c, v, tmp, 2);
+    for (size_t q = 0; q < nc; ++q) conv[q] = conv[q] + tmp[q] * Uh[q + 2 * nc] / Uh[q];
+  }
+}
+
+/* hydrogen_excitation_timestep (Scheme_rot.f90:1002-1049) reduced by cfl_pip_ir_nexcite
+ * (:329-335): max over every cell and levels 1-5 of dNexcite/dt. */
+static double nl_dneut_max(orc_ctx *c) {
+  size_t nc = c->nc;
+  double gref = c->gm_rec_ref, tir = c->p.t_ir;
+  double *conv = malloc(sizeof(double) * nc * 5), *tmp = malloc(sizeof(double) * nc);
+  for (int ii = 0; ii < 5; ++ii) nl_conv(c, ii, conv + ii * nc, tmp);
+  double mx = -INFINITY;
+  for (size_t q = 0; q < nc; ++q) {
+    double nx[6];
+    for (int k = 0; k < 6; ++k) nx[k] = c->nex[q + k * nc];
+    for (int ii = 0; ii < 5; ++ii) {
+      double d = 0.0;
+      for (int jj = 0; jj < 6; ++jj)
+        d = d + nx[jj] * NL_CR(c, q, jj, ii) / gref * tir - nx[ii] * NL_CR(c, q, ii, jj) / gref * tir;
+      mx = fmx(mx, d - conv[q + ii * nc]);
+    }
+  }
+  free(conv);
+  free(tmp);
+  return mx;
+}
+
+/* boundary of one scalar plane (bnd_energy, Boundary_rot.f90:127-162): the type mapping of
+ * MHDbnd, sign +1 (the energy's entry of sym_mhd). */
+static void nl_bnd_plane(orc_ctx *c, double *v) {
+  static const int one[1] = {1};
+  for (int f = 0; f < 2 * c->p.ndim; ++f)
+    if (c->neighbor[f] == -1) boundary_control(c, v, 1, f / 2 + 1, f % 2, one, bnd_type(c->p.flag_bnd[f]));
+}
+
+/* hydrogen_excitation_update (PIP_rot.f90:1026-1159) over dt, after a stage's update of U
+ * (Solver_rot.f90:218-220): the ion population's sum first, then the neutral levels' sums
+ * over the ion and over the other levels, minus the convection by the neutral velocity;
+ * the 1e-16 floor, the ground level absorbing the difference to rho_n, Nexcite(6) = rho_i,
+ * and bnd_energy on every plane. */
+static void hydrogen_excitation_update(orc_ctx *c, double dt) {
+  size_t nc = c->nc;
+  double gref = c->gm_rec_ref, tir = c->p.t_ir;
+  double *conv = malloc(sizeof(double) * nc * 5), *tmp = malloc(sizeof(double) * nc);
+  for (int ii = 0; ii < 5; ++ii) nl_conv(c, ii, conv + ii * nc, tmp);
+  double *N = c->nex;
+  const double *Uh = c->U_h, *Um = c->U_m;
+  for (size_t q = 0; q < nc; ++q) {
+    double nx[6], d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < 6; ++k) nx[k] = N[q + k * nc];
+    for (int jj = 0; jj < 5; ++jj)
+      d[5] = d[5] + nx[jj] * NL_CR(c, q, jj, 5) / gref * tir - nx[5] * NL_CR(c, q, 5, jj) / gref * tir;
+    for (int ii = 0; ii < 5; ++ii)
+      d[ii] = d[ii] + nx[5] * NL_CR(c, q, 5, ii) / gref * tir - nx[ii] * NL_CR(c, q, ii, 5) / gref * tir;
+    for (int ii = 0; ii < 5; ++ii)
+      for (int jj = 0; jj < 5; ++jj)
+        d[ii] = d[ii] + nx[jj] * NL_CR(c, q, jj, ii) / gref * tir - nx[ii] * NL_CR(c, q, ii, jj) / gref * tir;
+    for (int ii = 0; ii < 5; ++ii) {
+      double v = nx[ii] + dt * (d[ii] - conv[q + ii * nc]);
+      nx[ii] = v > NL_FLOOR ? v : NL_FLOOR;
+    }
+    double tot = nx[0] + nx[1] + nx[2] + nx[3] + nx[4] - Uh[q];
+    nx[0] = nx[0] - tot;
+    nx[5] = Um[q];
+    for (int k = 0; k < 6; ++k) N[q + k * nc] = nx[k];
+  }
+  for (int k = 0; k < 6; ++k) nl_bnd_plane(c, N + k * nc);
+  free(conv);
+  free(tmp);
+}
+
+int orc_set_nlevel(orc_ctx *c, int deriv, double n0fac, double f_p_ini, double f_p_p_ini,
+                   const double *table, long nrows) {
+  if (c->p.flag_ir != PIP_IR_NLEVEL || nrows < 3 || (deriv != 0 && deriv != 1 && deriv != 4))
+    return PIP_ERR_PARAM;
+  c->nlev_deriv = deriv;
+  c->n0fac = n0fac;
+  c->f_p_ini = f_p_ini;
+  c->f_p_p_ini = f_p_p_ini;
+  free(c->etab);
+  c->etab = malloc(sizeof(double) * 4 * nrows);
+  memcpy(c->etab, table, sizeof(double) * 4 * nrows);
+  c->netab = nrows;
+  nl_constants(c);
+  if (!c->nex) c->nex = calloc(c->nc * 6, sizeof(double));
+  if (!c->colrat) c->colrat = calloc(c->nc * 36, sizeof(double));
+  if (!c->ion_pot) c->ion_pot = calloc(c->nc, sizeof(double));
+  c->nlev_init = 0;
+  c->init_done = 0;
+  return 0;
+}
+
+void orc_set_nexcite(orc_ctx *c, const double *nex) {
+  memcpy(c->nex, nex, sizeof(double) * c->nc * 6);
+}
+void orc_get_nexcite(const orc_ctx *c, double *nex) {
+  memcpy(nex, c->nex, sizeof(double) * c->nc * 6);
+}
+void orc_get_colrat(const orc_ctx *c, double *colrat) {
+  memcpy(colrat, c->colrat, sizeof(double) * c->nc * 36);
+}
+void orc_get_ion_pot(const orc_ctx *c, double *ion_pot) {
+  memcpy(ion_pot, c->ion_pot, sizeof(double) * c->nc);
+}
+double orc_gm_rec_ref(const orc_ctx *c) { return c->gm_rec_ref; }
+int orc_nlevel_status(const orc_ctx *c) { return c->nlev_bad; }
+
 /* set_IR types 1, 2 and 3 (PIP_rot.f90:134-228): get_Te_HD and get_Te_MHD rewrite both
  * energies, then the rates from the ion temperature Te_p and density.  Type 1 (the Jeffery
  * formulation, :135-149) from T_norm and n_norm; types 2 and 3 the Popescu et al. 2019 rates
@@ -823,6 +1240,10 @@ static void set_collisional(orc_ctx *c) {
 static void set_ir_law(orc_ctx *c) {
   const pip_params *p = &c->p;
   size_t nc = c->nc;
+  if (p->flag_ir == PIP_IR_NLEVEL) {
+    set_ir_nlevel(c);
+    return;
+  }
   if (p->flag_ir == PIP_IR_JEFFERY) {
     double T0 = p->t_norm, n0 = p->n_norm;
     double factor = exp(-13.2 / (T0 / 11605.0));
@@ -871,7 +1292,8 @@ static void set_ir_law(orc_ctx *c) {
 }
 
 static int ir_per_stage(const orc_ctx *c) {
-  return c->p.flag_ir == PIP_IR_POPESCU || c->p.flag_ir == PIP_IR_POPESCU_EQ;
+  return c->p.flag_ir == PIP_IR_POPESCU || c->p.flag_ir == PIP_IR_POPESCU_EQ ||
+         c->p.flag_ir == PIP_IR_NLEVEL;
 }
 
 /* set_IR types 1-3: called by the time loop before each cfl and at the prologue */
@@ -910,7 +1332,7 @@ int orc_alpha_c(orc_ctx *c, double *ac) {
 }
 
 /* source_PIP, PIP_rot.f90:1309-1429 (explicit and exponential collision forms plus the
- * IR block with flag_IR_type 1 or 2).  out_h/out_m receive S (explicit form) or the U0
+ * IR block with flag_IR_type 1 or 2, and 0 with set_IR type 4).  out_h/out_m receive S (explicit form) or the U0
  * increments of the exponential form, plus the IR rates in S. */
 static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, double *S_h,
                        double *S_m) {
@@ -974,13 +1396,21 @@ static void source_pip(orc_ctx *c, double *U_h0, double *U_m0, double dt_coll, d
       ds[3] = gr * de[q] * vz[q] - gi * nde[q] * nvz[q];
       double kin = 0.5 * (gr * de[q] * (vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q]) -
                           gi * nde[q] * (nvx[q] * nvx[q] + nvy[q] * nvy[q] + nvz[q] * nvz[q]));
-      if (c->p.flag_ir_type == 1)
+      if (c->p.flag_ir_type != 2)
         ds[4] = kin - gi * npr[q] / (gm - 1.0) + 0.5 * gr * pr[q] / (gm - 1.0);
       else
         ds[4] = kin - gi * npr[q] / (gm - 1.0) + gr * pr[q] / (gm - 1.0);
       for (int n = 0; n < 5; ++n) {
         S_h[q + n * nc] = S_h[q + n * nc] + ds[n];
         S_m[q + n * nc] = S_m[q + n * nc] - ds[n];
+      }
+      if (c->p.flag_ir_type == 0) {
+        /* the new formulation's ionisation potential (IRgetionpot for type 4; arb_heat 0) */
+        double nx[6], cr[36];
+        for (int k = 0; k < 6; ++k) nx[k] = c->nex[q + k * nc];
+        for (int k = 0; k < 36; ++k) cr[(k % 6) * 6 + k / 6] = c->colrat[q + k * nc];
+        c->ion_pot[q] = nl_ionpot(c, cr, nx);
+        S_m[q + 4 * nc] = S_m[q + 4 * nc] - c->ion_pot[q] + 0.0;
       }
     }
   }
@@ -1072,6 +1502,25 @@ void orc_cfl(orc_ctx *c, double *dt_out, double *cmax_out) {
       gi = fmx(gi, c->gm_ion[q]);
     }
     dttemp = fmn(dttemp, fmn(safety, 0.1) / fmx(fmx(gr, gi), 1.0e-5));
+    if (p->flag_ir_type == 0) {
+      /* get_Pr_MHD (Scheme_rot.f90:112-128, rewriting the ion energy once more), then
+       * ion_pot of the last source_PIP (or of the prologue) over the internal energy */
+      double ipm = -INFINITY;
+      double *Um = c->U_m;
+      for (size_t q = 0; q < nc; ++q) {
+        double m1 = Um[q], m2 = Um[q + nc], m3 = Um[q + 2 * nc], m4 = Um[q + 3 * nc];
+        double m6 = Um[q + 5 * nc], m7 = Um[q + 6 * nc], m8 = Um[q + 7 * nc];
+        double prm = (gm - 1.0) * (Um[q + 4 * nc] -
+                                   0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 + m7 * m7 + m8 * m8));
+        prm = fmx(prm, p->pr_lim);
+        Um[q + 4 * nc] = prm / (gm - 1.0) + 0.5 * ((m2 * m2 + m3 * m3 + m4 * m4) / m1 + m6 * m6 +
+                                                   m7 * m7 + m8 * m8);
+        ipm = fmx(ipm, c->ion_pot[q] / (prm / (gm - 1.0)));
+      }
+      dttemp = fmn(dttemp, safety / fmx(ipm, 1.0e-5));
+    }
+    if (p->flag_ir == PIP_IR_NLEVEL)
+      dttemp = fmn(dttemp, fmn(safety, 0.01) / fmx(nl_dneut_max(c), 1.0e-5));
   }
 
   /* cfl_resi (Scheme_rot.f90:291-302) */
@@ -1409,6 +1858,7 @@ void orc_stage(orc_ctx *c, int istep, double dt) {
     double *ps = c->U_m + 8 * nc;
     for (size_t q = 0; q < nc; ++q) ps[q] = ps[q] * fac;
   }
+  if (p->flag_ir == PIP_IR_NLEVEL) hydrogen_excitation_update(c, dt_sub);
   orc_bnd(c);
   free(F_h); free(F_m); free(S_h); free(S_m);
 }
@@ -1502,6 +1952,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->U_h0); free(c->U_m0);
   free(c->ac);
   free(c->eta);
+  free(c->etab); free(c->nex); free(c->colrat); free(c->ion_pot);
   free(c);
 }
 

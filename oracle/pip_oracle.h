@@ -74,6 +74,24 @@ int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres);
 /* stop_sim's NaN scan (IO_rot.f90:641-668) over both species. */
 int orc_has_nan(const orc_ctx *c);
 
+/* set_IR type 4, the 6-level hydrogen model (PIP_rot.f90:232-311,361-616,874-946,
+ * 1026-1235; Scheme_rot.f90:315-335,692-736,1002-1049).
+ * orc_expint_table: colexpintcalc.f90's table, 4*(nsamps+1) values (yn, E0, E1, E2 per row).
+ * orc_set_nlevel: deriv 0 (no convective term), 1 or 4 (the two- and five-point forms of
+ * derivative); n0fac, f_p_ini, f_p_p_ini of globalvar; table as expintread holds it
+ * (4 x nrows, column-major).  Resets the prologue's block (Gm_rec_ref, ion_pot).
+ * Nexcite is (ix,jx,kx,6), colrat (ix,jx,kx,6,6), both column-major. */
+void orc_expint_table(long nsamps, double *out);
+int orc_set_nlevel(orc_ctx *c, int deriv, double n0fac, double f_p_ini, double f_p_p_ini,
+                   const double *table, long nrows);
+void orc_set_nexcite(orc_ctx *c, const double *nex);
+void orc_get_nexcite(const orc_ctx *c, double *nex);
+void orc_get_colrat(const orc_ctx *c, double *colrat);
+void orc_get_ion_pot(const orc_ctx *c, double *ion_pot);
+double orc_gm_rec_ref(const orc_ctx *c);
+/* 1 once a rate came out negative (where the reference stops). */
+int orc_nlevel_status(const orc_ctx *c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,7 @@ PIP_ERR_ITER = 5
 PIP_ERR_STATE = 6
 PIP_ERR_NOMEM = 7
 PIP_ERR_NULL = 8
+PIP_ERR_RATE = 9
 
 # every extern "C" symbol include/pip_gpu.h declares
 EXPORTS = (
@@ -34,9 +35,11 @@ EXPORTS = (
     "pip_status", "pip_conduction", "pip_last_cuda_error", "pip_strerror",
     "pip_step_noalloc", "pip_set_neighbors", "pip_stage", "pip_halo_bytes", "pip_halo_pack",
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
-    "pip_dev_stage_rows", "pip_set_halo_stream",
+    "pip_dev_stage_split", "pip_set_halo_stream",
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
     "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
+    "pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
+    "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -107,11 +110,21 @@ def lib(path: Optional[str] = None):
     L.pip_set_cmax_scale.argtypes = [vp, d]
     L.pip_dev_begin.argtypes = [vp, ctypes.c_int64, d]
     L.pip_dev_stage.argtypes = [vp, i]
-    L.pip_dev_stage_rows.argtypes = [vp, i, i]
+    L.pip_dev_stage_split.argtypes = [vp, i, P(vp)]
     L.pip_set_halo_stream.argtypes = [vp, vp]
     L.pip_dev_candidates.argtypes = [vp, P(vp), P(vp)]
     L.pip_dev_poll.argtypes = [vp, P(i), dp, P(ctypes.c_int64)]
     L.pip_step_noalloc.restype = i
+    L.pip_colexp_table.argtypes = [ctypes.c_int64, dp]
+    L.pip_set_nlevel.argtypes = [vp, P(PipNlevel), dp, ctypes.c_int64]
+    L.pip_set_nexcite.argtypes = [vp, dp]
+    L.pip_get_nexcite.argtypes = [vp, dp]
+    L.pip_get_colrat.argtypes = [vp, dp]
+    L.pip_get_ion_pot.argtypes = [vp, dp]
+    L.pip_nlevel_gm_rec_ref.argtypes = [vp, dp]
+    for name in ("pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
+                 "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref"):
+        getattr(L, name).restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
     L.pip_strerror.restype = ctypes.c_char_p
@@ -155,6 +168,28 @@ def lib(path: Optional[str] = None):
 
 def strerror(code: int) -> str:
     return lib().pip_strerror(int(code)).decode()
+
+
+class PipNlevel(ctypes.Structure):
+    """ctypes mirror of ``struct pip_nlevel`` (set_IR type 4's settings)."""
+
+    _fields_ = [
+        ("n_levels", ctypes.c_int32),
+        ("flag_rad", ctypes.c_int32),
+        ("deriv", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("n0fac", ctypes.c_double),
+        ("f_p_ini", ctypes.c_double),
+        ("f_p_p_ini", ctypes.c_double),
+    ]
+
+
+def colexp_table(nsamps: int = 100000) -> np.ndarray:
+    """expintcalc/colexp.dat's table as expintread holds it, shape (nsamps+1, 4): rows
+    (yn, E0(yn), E1(yn), E2(yn)) by the algorithm of expintcalc/colexpintcalc.f90."""
+    t = np.empty((int(nsamps) + 1, 4))
+    _check(lib().pip_colexp_table(int(nsamps), _ptr(t)), "pip_colexp_table")
+    return t
 
 
 def _ptr(a: np.ndarray):
@@ -335,9 +370,13 @@ class Context:
     def dev_stage(self, stage: int) -> None:
         _check(lib().pip_dev_stage(self.h, int(stage)), "pip_dev_stage")
 
-    def dev_stage_rows(self, stage: int, rows: int) -> None:
-        """Half of a device stage: rows 1 the first and last tile rows, 2 the others."""
-        _check(lib().pip_dev_stage_rows(self.h, int(stage), int(rows)), "pip_dev_stage_rows")
+    def dev_stage_split(self, stage: int) -> int:
+        """A device stage with its boundary tile rows on a high-priority stream of the
+        context, concurrent with the middle rows; returns that stream (an int handle)."""
+        bs = ctypes.c_void_p()
+        _check(lib().pip_dev_stage_split(self.h, int(stage), ctypes.byref(bs)),
+               "pip_dev_stage_split")
+        return bs.value or 0
 
     def set_halo_stream(self, stream: int) -> None:
         """The stream of pip_halo_pack / pip_halo_unpack (0: the context stream)."""
@@ -383,6 +422,45 @@ class Context:
         nan = ctypes.c_int()
         _check(lib().pip_status(self.h, ctypes.byref(stop), ctypes.byref(nan)), "pip_status")
         return stop.value, nan.value
+
+    # ---- set_IR type 4 (the 6-level hydrogen model)
+    def set_nlevel(self, table: np.ndarray, deriv: int = 1, n0fac: float = 1.0,
+                   f_p_ini: float = 1.0, f_p_p_ini: float = 1.0, n_levels: int = 5,
+                   flag_rad: int = 0) -> None:
+        """The exponential-integral table (rows yn, E0, E1, E2) and the model's settings."""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        if t.ndim != 2 or t.shape[1] != 4:
+            raise ValueError("the table has rows of 4 values (yn, E0, E1, E2)")
+        cfg = PipNlevel(int(n_levels), int(flag_rad), int(deriv), 0, float(n0fac),
+                        float(f_p_ini), float(f_p_p_ini))
+        _check(lib().pip_set_nlevel(self.h, ctypes.byref(cfg), _ptr(t), t.shape[0]),
+               "pip_set_nlevel")
+
+    def set_nexcite(self, nex: np.ndarray) -> None:
+        """Nexcite, shape (6, jx, ix): levels 1-5 then the ions."""
+        n = np.ascontiguousarray(nex, dtype=np.float64).reshape((6,) + self.shape_h[1:])
+        _check(lib().pip_set_nexcite(self.h, _ptr(n)), "pip_set_nexcite")
+
+    def nexcite(self) -> np.ndarray:
+        n = np.empty((6,) + self.shape_h[1:])
+        _check(lib().pip_get_nexcite(self.h, _ptr(n)), "pip_get_nexcite")
+        return n
+
+    def colrat(self) -> np.ndarray:
+        """colrat of the last set_IR as [a, b] = colrat(a+1, b+1), shape (6, 6, jx, ix)."""
+        c = np.empty((6, 6) + self.shape_h[1:])
+        _check(lib().pip_get_colrat(self.h, _ptr(c)), "pip_get_colrat")
+        return np.ascontiguousarray(c.transpose(1, 0, 2, 3))
+
+    def ion_pot(self) -> np.ndarray:
+        a = np.empty(self.shape_h[1:])
+        _check(lib().pip_get_ion_pot(self.h, _ptr(a)), "pip_get_ion_pot")
+        return a
+
+    def gm_rec_ref(self) -> float:
+        v = ctypes.c_double()
+        _check(lib().pip_nlevel_gm_rec_ref(self.h, ctypes.byref(v)), "pip_nlevel_gm_rec_ref")
+        return v.value
 
     def prologue(self) -> None:
         """The prologue's cfl and ghost fill (Initial_rot.f90:152-160)."""

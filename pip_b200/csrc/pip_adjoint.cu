@@ -742,7 +742,12 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
   if ((e = cudaGetDevice(&a->device)) != cudaSuccess) return fail(e);
   if ((e = a->L->prepare()) != cudaSuccess) return fail(e);
   if ((e = pip::adjk::prepare()) != cudaSuccess) return fail(e);
-  if ((e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  // the reverse sweep (stream) is the critical path; the recomputation of the next segment
+  // (stream2) fills the SMs it leaves idle, so it gets the lower priority
+  int prio_lo = 0, prio_hi = 0;
+  if ((e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithPriority(&a->stream, cudaStreamNonBlocking, prio_hi)) != cudaSuccess)
+    return fail(e);
   if ((e = cudaMalloc(&a->A, sb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->B, sb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->La, sb)) != cudaSuccess) return fail(e);
@@ -762,7 +767,8 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
       if ((e = cudaMemset(x, 0, sb)) != cudaSuccess) return fail(e);
     }
   }
-  if ((e = cudaStreamCreateWithFlags(&a->stream2, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithPriority(&a->stream2, cudaStreamNonBlocking, prio_lo)) != cudaSuccess)
+    return fail(e);
   if ((e = cudaEventCreateWithFlags(&a->ev_start, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   for (int set = 0; set < 2; ++set) {
     if ((e = cudaEventCreateWithFlags(&a->ev_rec[set], cudaEventDisableTiming)) != cudaSuccess)

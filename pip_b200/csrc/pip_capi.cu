@@ -47,15 +47,24 @@ struct pip_ctx {
   int neighbor[4] = {-1, -1, -1, -1};  // set_mpi_neighbor: rank across each face, -1 physical
   bool exchanged = false;             // some face is filled by the halo exchange
   int last_stage = 0;                 // RK stage that wrote the state last (1: the U1 array)
-  int rows_open = 0;                  // pip_dev_stage_rows: stage whose middle rows are due
   cudaStream_t halo_stream = nullptr; // pip_set_halo_stream: the stream of pack and unpack
+  cudaStream_t rows_stream = nullptr; // pip_dev_stage_split: high-priority stream of the
+  cudaEvent_t rows_ev[2] = {nullptr, nullptr};  // boundary rows, and its two events
   bool dev_loop = false;              // pip_dev_begin has set up the device-driven loop
   bool uploaded = false;
   double *acf = nullptr;              // alpha_c per cell (flag_col 2..7)
   double *etaf = nullptr;             // eta per cell (flag_resi 1)
   unsigned long long *d_resi = nullptr;  // cfl_resi's bound of the current eta (flag_resi 2)
   bool coef_valid = false;            // set_coefficients(U_h,U_m,0) has run on this state
-  double *irg = nullptr;              // set_IR type 1's rates (2 planes)
+  double *irg = nullptr;              // set_IR type 1's or type 4's rates (2 planes)
+  // set_IR type 4: Nexcite (two sets of 6 planes, nl_cur the current), colrat (36 planes),
+  // ion_pot, the table, the coefficients, the reference rates (37 values)
+  double *nl_nex[2] = {nullptr, nullptr};
+  int nl_cur = 0;
+  double *nl_cr = nullptr, *nl_ip = nullptr, *nl_tab = nullptr, *nl_ref = nullptr;
+  pip::NlevConst *nl_k = nullptr;
+  bool nl_ready = false;              // pip_set_nlevel has run
+  bool nl_init = false;               // the fresh-start block (Gm_rec_ref, ion_pot) has run
   double dt = 0.0, cmax = 0.0, time = 0.0, last_dt = 1.0;
   int nplanes() const { return kp.nvm + 5; }
   size_t plane_bytes() const { return sizeof(double) * (size_t)kp.nc; }
@@ -159,13 +168,18 @@ int validate(const pip_params *p) {
   if (p->flag_resi == 2 && p->resi_type == 3 && !(p->vd_cri > 0.0)) return PIP_ERR_PARAM;
   if (p->flag_pip_imp != 0 && p->flag_pip_imp != 1) return PIP_ERR_PARAM;
   if (p->flag_ir != PIP_IR_NONE && p->flag_ir != PIP_IR_POWERLAW && p->flag_ir != PIP_IR_POPESCU &&
-      p->flag_ir != PIP_IR_POPESCU_EQ && p->flag_ir != PIP_IR_JEFFERY)
+      p->flag_ir != PIP_IR_POPESCU_EQ && p->flag_ir != PIP_IR_JEFFERY && p->flag_ir != PIP_IR_NLEVEL)
     return PIP_ERR_PARAM;
   if ((p->flag_ir == PIP_IR_POPESCU || p->flag_ir == PIP_IR_POPESCU_EQ ||
-       p->flag_ir == PIP_IR_JEFFERY) &&
+       p->flag_ir == PIP_IR_JEFFERY || p->flag_ir == PIP_IR_NLEVEL) &&
       (p->precision != PIP_FP64 || !(p->t_norm > 0.0) || !(p->n_norm > 0.0)))
     return PIP_ERR_PARAM;
-  if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2) return PIP_ERR_PARAM;
+  // flag_IR_type 0 (source_PIP's ionisation potential) exists for set_IR type 4 only: for the
+  // other types the reference reads ion_pot and arb_heat before any call allocates them
+  if (p->flag_ir != PIP_IR_NONE && p->flag_ir_type != 1 && p->flag_ir_type != 2 &&
+      !(p->flag_ir == PIP_IR_NLEVEL && p->flag_ir_type == 0))
+    return PIP_ERR_PARAM;
+  if (p->flag_ir == PIP_IR_NLEVEL && p->flag_col % 2 == 0 && !(p->beta > 0.0)) return PIP_ERR_PARAM;
   if (p->precision != PIP_FP64 && p->precision != PIP_MIXED) return PIP_ERR_PARAM;
   if (p->flag_heat != 0 && p->flag_heat != 1) return PIP_ERR_PARAM;
   if (p->flag_heat == 1 && (p->ndim != 2 || p->hc_max < 0 || !(p->hc_error > 0.0) ||
@@ -188,9 +202,23 @@ int validate(const pip_params *p) {
 // single-precision literals (2.7, 5.6e-16, 1.1604e4, 2.6e-19, 2.91e-14, 1.0e6) rounded to
 // float first.
 void ir_law_constants(const pip_params &p, KParams &k) {
-  k.irs = (p.flag_ir == PIP_IR_POPESCU || p.flag_ir == PIP_IR_POPESCU_EQ) ? p.flag_ir : 0;
+  k.irs = (p.flag_ir == PIP_IR_POPESCU || p.flag_ir == PIP_IR_POPESCU_EQ ||
+           p.flag_ir == PIP_IR_NLEVEL) ? p.flag_ir : 0;
   k.irf = p.flag_ir == PIP_IR_JEFFERY ? 1 : 0;
   k.irl = k.irs || k.irf ? 1 : 0;
+  k.irn = p.flag_ir == PIP_IR_NLEVEL ? 1 : 0;
+  if (k.irn) {
+    // set_IR type 4 and IRgetionpot (PIP_rot.f90:232-296,1222-1233); tfac, the table and the
+    // populations come with pip_set_nlevel
+    k.nl_T0 = p.t_norm;
+    k.nl_n0 = p.n_norm;
+    k.nl_tir = p.t_ir;
+    k.nl_odd = p.flag_col % 2 == 1 ? 1 : 0;
+    k.nl_en_even = p.beta / p.t_norm / 2.0 / (double)8.6173e-5f;
+    k.nl_lim = std::min(p.safety, 0.01);
+    k.nl_gref = 1.0;
+    return;
+  }
   if (k.irf) {
     // set_IR type 1 (PIP_rot.f90:135-149)
     const double T0 = p.t_norm, n0 = p.n_norm;
@@ -383,6 +411,13 @@ double finalize_dt_host(const KParams &k, const DevCtrl &c, int slot) {
   std::memcpy(&gr, &c.red_gr[slot], sizeof(double));
   dt = std::fmin(dt, k.col_lim / rho);
   if (k.ir) dt = std::fmin(dt, k.ir_lim / std::fmax(gr, 1.0e-5));
+  if (k.irn) {
+    double ip, nx;
+    std::memcpy(&ip, &c.red_ip[slot], sizeof(double));
+    std::memcpy(&nx, &c.red_nx[slot], sizeof(double));
+    if (k.ir_type == 0) dt = std::fmin(dt, k.safety / ip);
+    dt = std::fmin(dt, k.nl_lim / nx);
+  }
   return dt;
 }
 
@@ -393,6 +428,8 @@ void reset_slot(DevCtrl &h, int slot, const KParams &k) {
   std::memcpy(&h.red_dt[slot], &seed, sizeof(double));
   h.red_rho[slot] = 0ull;
   h.red_gr[slot] = 0ull;
+  h.red_ip[slot] = 0ull;
+  h.red_nx[slot] = 0ull;
 }
 
 // cfl_resi (Scheme_rot.f90:291-302) for a fixed eta field: the minimum over the interior
@@ -430,9 +467,35 @@ __global__ void stage_ctrl_kernel(DevCtrl *ctrl, double dt, double cmax) {
 // energies and set their fields before the first cfl and the first stage.
 int ensure_coefficients(pip_ctx *c) {
   if ((!c->kp.col_type && !c->kp.irl && c->kp.resi != 2) || c->coef_valid) return PIP_OK;
+  if (c->kp.irn) {
+    // set_IR type 4 inside set_coefficients: on a fresh start first its reference block
+    // (Gm_rec_ref, the initial ion_pot), then the rates of the state; before the energy
+    // rewrites of coefficients_kernel, whose sequence the rates kernel repeats on its copies
+    int ipmode = 0;
+    if (!c->nl_init) {
+      CK(c->L->nlev_ref(c->kp, c->nl_ref, c->stream));
+      double gref = 0.0;
+      CK(cudaMemcpyAsync(&gref, c->nl_ref + 36, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      c->kp.nl_gref = gref;
+      c->nl_init = true;
+      ipmode = c->kp.ir_type == 0 ? 2 : 0;
+    }
+    CK(c->L->nlev_rates(c->kp, c->A, c->kp.col_type ? 1 : 0, ipmode, c->nl_ref, c->ctrl, c->stream));
+  }
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   c->coef_valid = true;
   return PIP_OK;
+}
+
+// set_IR type 4 needs pip_set_nlevel first.
+bool nl_missing(const pip_ctx *c) { return c->kp.irn && !c->nl_ready; }
+
+// Nexcite's update target becomes the current set.
+void nl_swap(pip_ctx *c) {
+  c->nl_cur ^= 1;
+  c->kp.nl_nex = c->nl_nex[c->nl_cur];
+  c->kp.nl_nex2 = c->nl_nex[c->nl_cur ^ 1];
 }
 
 int push_ctrl(pip_ctx *c) {
@@ -450,6 +513,21 @@ cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi, int rows = 0) 
     return pip::mixed_stage(c->kp, 2, c->Bf, c->Ahi, c->Alo, c->Ahi, c->Alo, c->ctrl, dt_mode, epi,
                             c->stream, c->tma ? &c->tm_b : nullptr, rows);
   }
+  if (c->kp.irn) {
+    // set_IR type 4 of the stage (set_coefficients, after set_collisional's rewrite), the
+    // stage, then hydrogen_excitation_update on the updated state (Solver_rot.f90:218-220)
+    const double *Us = stage == 1 ? c->A : c->B;
+    double *Uo = stage == 1 ? c->B : c->A;
+    cudaError_t e = c->L->nlev_rates(c->kp, Us, c->kp.col_type ? 1 : 0, c->kp.ir_type == 0 ? 1 : 0,
+                                     nullptr, c->ctrl, c->stream);
+    if (e != cudaSuccess) return e;
+    e = c->L->stage(c->kp, stage, Us, c->A, Uo, c->ctrl, dt_mode, epi, c->stream,
+                    c->tma ? (stage == 1 ? &c->tm_a : &c->tm_b) : nullptr, rows);
+    if (e != cudaSuccess) return e;
+    e = c->L->nlev_update(c->kp, Uo, c->ctrl, stage, c->stream);
+    if (e == cudaSuccess) nl_swap(c);
+    return e;
+  }
   if (stage == 1)
     return c->L->stage(c->kp, 1, c->A, c->A, c->B, c->ctrl, dt_mode, epi, c->stream,
                        c->tma ? &c->tm_a : nullptr, rows);
@@ -459,6 +537,13 @@ cudaError_t do_stage(pip_ctx *c, int stage, int dt_mode, int epi, int rows = 0) 
 
 cudaError_t do_cfl(pip_ctx *c, int slot) {
   if (c->mixed) return pip::mixed_cfl(c->kp, c->Ahi, c->Alo, c->ctrl, slot, c->stream);
+  if (c->kp.irn) {
+    // the time loop's set_IR before the cfl, the cfl, then its type-4 terms
+    cudaError_t e = c->L->nlev_rates(c->kp, c->A, 0, 0, nullptr, c->ctrl, c->stream);
+    if (e != cudaSuccess) return e;
+    if ((e = c->L->cfl(c->kp, c->A, c->ctrl, slot, c->stream)) != cudaSuccess) return e;
+    return c->L->nlev_cfl(c->kp, c->A, c->ctrl, slot, c->stream);
+  }
   return c->L->cfl(c->kp, c->A, c->ctrl, slot, c->stream);
 }
 
@@ -604,7 +689,24 @@ int pip_ctx_create(const pip_params *p, pip_ctx **out) {
     c->kp.etaf = c->etaf;
     c->kp.resi_dt = resi_bound(c, eta.data());
   }
-  if (c->kp.irf) {
+  if (c->kp.irn) {
+    for (int k = 0; k < 2; ++k) {
+      if ((e = cudaMalloc(&c->nl_nex[k], 6 * c->plane_bytes())) != cudaSuccess) return fail(e);
+      if ((e = cudaMemset(c->nl_nex[k], 0, 6 * c->plane_bytes())) != cudaSuccess) return fail(e);
+    }
+    if ((e = cudaMalloc(&c->nl_cr, 36 * c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->nl_cr, 0, 36 * c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->nl_ip, c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(c->nl_ip, 0, c->plane_bytes())) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->nl_ref, 37 * sizeof(double))) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&c->nl_k, sizeof(pip::NlevConst))) != cudaSuccess) return fail(e);
+    c->kp.nl_nex = c->nl_nex[0];
+    c->kp.nl_nex2 = c->nl_nex[1];
+    c->kp.nl_cr = c->nl_cr;
+    c->kp.nl_ip = c->nl_ip;
+    c->kp.nl_k = c->nl_k;
+  }
+  if (c->kp.irf || c->kp.irn) {
     if ((e = cudaMalloc(&c->irg, 2 * c->plane_bytes())) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(c->irg, 0, 2 * c->plane_bytes())) != cudaSuccess) return fail(e);
     c->kp.irg = c->irg;
@@ -654,7 +756,17 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->acf);
   cudaFree(c->etaf);
   cudaFree(c->d_resi);
+  if (c->rows_stream) cudaStreamDestroy(c->rows_stream);
+  for (cudaEvent_t ev : c->rows_ev)
+    if (ev) cudaEventDestroy(ev);
   cudaFree(c->irg);
+  cudaFree(c->nl_nex[0]);
+  cudaFree(c->nl_nex[1]);
+  cudaFree(c->nl_cr);
+  cudaFree(c->nl_ip);
+  cudaFree(c->nl_tab);
+  cudaFree(c->nl_ref);
+  cudaFree(c->nl_k);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -690,13 +802,15 @@ int pip_download(pip_ctx *c, double *U_h, double *U_m) {
 
 int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->uploaded || nl_missing(c)) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (ensure_coefficients(c)) return PIP_ERR_CUDA;
   reset_slot(*c->h_ctrl, 0, c->kp);
+  c->h_ctrl->status = 0;
   if (push_ctrl(c)) return PIP_ERR_CUDA;
   CK(do_cfl(c, 0));
   if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+  if (c->h_ctrl->status) return c->h_ctrl->status;
   const double d = finalize_dt_host(c->kp, *c->h_ctrl, 0);
   c->dt = d;
   if (c->p.flag_divb >= 1) c->cmax = c->kp.sg_all / d;
@@ -707,7 +821,7 @@ int pip_cfl(pip_ctx *c, double *dt, double *cmax) {
 
 int pip_step(pip_ctx *c, double dt) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
+  if (!c->uploaded || c->exchanged || nl_missing(c)) return PIP_ERR_STATE;
   if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (ensure_coefficients(c)) return PIP_ERR_CUDA;
@@ -731,13 +845,17 @@ int pip_step(pip_ctx *c, double dt) {
   CK(cudaStreamSynchronize(c->stream));
   c->last_dt = dt;
   c->last_stage = 2;
+  if (c->kp.irn) {   // a negative rate of the 6-level model
+    if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+    if (h.status) return h.status;
+  }
   return PIP_OK;
 }
 
 static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
                     int64_t *steps_done, float *device_ms) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded || c->exchanged) return PIP_ERR_STATE;
+  if (!c->uploaded || c->exchanged || nl_missing(c)) return PIP_ERR_STATE;
   if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
   c->last_stage = 2;
   c->dev_loop = false;
@@ -769,12 +887,14 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
-  if (c->hc || c->kp.resi == 2) {
+  if (c->hc || c->kp.resi == 2 || c->kp.irn) {
     // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
     // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
     // BiCGstab's convergence checks anyway, so no graph.  Per-stage eta: whether a step
     // was the last is known only once stage 2 has lowered its time increment to cfl_resi's
-    // bound, so the next cfl's rewrite cannot be fused into stage 2 either.
+    // bound, so the next cfl's rewrite cannot be fused into stage 2 either.  set_IR type 4:
+    // the rates, excitation-update and cfl kernels of the 6-level model sit between the
+    // stages and the cfl calls.
     long long n = 0;
     int total_it = 0;
     for (;;) {
@@ -853,7 +973,7 @@ int pip_run_timed(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
 int pip_bench_stage_ms(pip_ctx *c, int nsteps, float *ms1, float *ms2, float *msstep) {
   if (!c || !ms1 || !ms2 || !msstep) return PIP_ERR_NULL;
   if (!c->uploaded) return PIP_ERR_STATE;
-  if (nsteps <= 0) return PIP_ERR_PARAM;
+  if (nsteps <= 0 || c->kp.irn) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   DevCtrl &h = *c->h_ctrl;
   std::memset(&h, 0, sizeof(DevCtrl));
@@ -927,9 +1047,12 @@ int pip_flux(pip_ctx *c, int dir, double *F_h, double *F_m) {
 
 int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
   if (!c || !S_h || !S_m) return PIP_ERR_NULL;
-  if (!c->uploaded || c->mixed) return PIP_ERR_STATE;
+  if (!c->uploaded || c->mixed || nl_missing(c)) return PIP_ERR_STATE;
   if (set_device(c) || ensure_scratch(c) || ensure_coefficients(c)) return PIP_ERR_CUDA;
   const size_t pb = c->plane_bytes();
+  // set_IR type 4: the rates (and ion_pot) of the state as given, as for types 2 and 3
+  if (c->kp.irn)
+    CK(c->L->nlev_rates(c->kp, c->A, 0, c->kp.ir_type == 0 ? 1 : 0, nullptr, c->ctrl, c->stream));
   CK(c->L->source(c->kp, c->A, c->scratch, dt_coll, c->stream));
   CK(cudaMemcpyAsync(S_m, c->scratch, pb * c->kp.nvm, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(S_h, c->scratch + (size_t)c->kp.nvm * c->kp.nc, pb * 5, cudaMemcpyDeviceToHost,
@@ -940,9 +1063,15 @@ int pip_source(pip_ctx *c, double dt_coll, double *S_h, double *S_m) {
 
 int pip_coefficients(pip_ctx *c) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!c->uploaded || nl_missing(c)) return PIP_ERR_STATE;
   if (!c->kp.col_type && !c->kp.irl) return PIP_OK;
   if (set_device(c)) return PIP_ERR_CUDA;
+  if (c->kp.irn) {   // set_IR type 4's rates come before the rewrites
+    c->coef_valid = false;
+    if (ensure_coefficients(c)) return PIP_ERR_CUDA;
+    CK(cudaStreamSynchronize(c->stream));
+    return PIP_OK;
+  }
   CK(c->L->coefficients(c->kp, c->A, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->coef_valid = true;
@@ -1070,7 +1199,7 @@ int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
   }
   // the conduction matrix folds every side of the block (one rank per direction); with eta
   // recomputed at every stage each rank advances its time by its own cfl_resi bound
-  if (any && (c->hc || c->kp.resi == 2)) return PIP_ERR_PARAM;
+  if (any && (c->hc || c->kp.resi == 2 || c->kp.irn)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (c->stream) CK(cudaStreamSynchronize(c->stream));
   if (c->graph) {
@@ -1138,6 +1267,7 @@ int pip_set_cmax_scale(pip_ctx *c, double safety_min_d) {
 int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
   if (!c) return PIP_ERR_NULL;
   if (!c->uploaded || c->hc) return c->hc ? PIP_ERR_PARAM : PIP_ERR_STATE;
+  if (c->kp.irn) return PIP_ERR_PARAM;   // set_IR type 4 steps on the host (pip_run)
   if (nsteps <= 0 && !(t_end > 0.0)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(cudaStreamSynchronize(c->stream));   // nothing queued still reads the pinned block
@@ -1160,7 +1290,7 @@ int pip_dev_begin(pip_ctx *c, int64_t nsteps, double t_end) {
 
 int pip_dev_stage(pip_ctx *c, int stage) {
   if (!c) return PIP_ERR_NULL;
-  if (!c->dev_loop || c->rows_open) return PIP_ERR_STATE;
+  if (!c->dev_loop) return PIP_ERR_STATE;
   if (stage != 1 && stage != 2) return PIP_ERR_PARAM;
   if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
@@ -1169,20 +1299,35 @@ int pip_dev_stage(pip_ctx *c, int stage) {
   return PIP_OK;
 }
 
-int pip_dev_stage_rows(pip_ctx *c, int stage, int rows) {
-  if (!c) return PIP_ERR_NULL;
+int pip_dev_stage_split(pip_ctx *c, int stage, void **boundary_stream) {
+  if (!c || !boundary_stream) return PIP_ERR_NULL;
   if (!c->dev_loop) return PIP_ERR_STATE;
-  if ((stage != 1 && stage != 2) || (rows != 1 && rows != 2)) return PIP_ERR_PARAM;
+  if (stage != 1 && stage != 2) return PIP_ERR_PARAM;
   if (c->kp.ndim != 2) return PIP_ERR_PARAM;
-  if (rows == 1) {
-    if (c->rows_open || (stage == 2 && c->last_stage != 1)) return PIP_ERR_STATE;
-  } else if (c->rows_open != stage) {
-    return PIP_ERR_STATE;
-  }
+  if (stage == 2 && c->last_stage != 1) return PIP_ERR_STATE;
   if (set_device(c)) return PIP_ERR_CUDA;
-  CK(stage == 1 ? do_stage(c, 1, 1, 0, rows) : do_stage(c, 2, 1, -1, rows));
+  if (!c->rows_stream) {
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&c->rows_stream, cudaStreamNonBlocking, hi));
+    CK(cudaEventCreateWithFlags(&c->rows_ev[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->rows_ev[1], cudaEventDisableTiming));
+  }
+  // the boundary rows on the high-priority stream, concurrent with the middle rows on the
+  // context stream; the context stream then waits for them
+  const int epi = stage == 1 ? 0 : -1;
+  cudaStream_t s0 = c->stream;
+  CK(cudaEventRecord(c->rows_ev[0], s0));
+  CK(cudaStreamWaitEvent(c->rows_stream, c->rows_ev[0], 0));
+  c->stream = c->rows_stream;
+  cudaError_t e = do_stage(c, stage, 1, epi, 1);
+  c->stream = s0;
+  CK(e);
+  CK(cudaEventRecord(c->rows_ev[1], c->rows_stream));
+  CK(do_stage(c, stage, 1, epi, 2));
+  CK(cudaStreamWaitEvent(s0, c->rows_ev[1], 0));
   c->last_stage = stage;
-  c->rows_open = rows == 1 ? stage : 0;
+  *boundary_stream = (void *)c->rows_stream;
   return PIP_OK;
 }
 
@@ -1274,6 +1419,85 @@ int pip_halo_unpack(pip_ctx *c, int face, const void *recv, int64_t bytes) {
   return PIP_OK;
 }
 
+int pip_set_nlevel(pip_ctx *c, const pip_nlevel *cfg, const double *table, int64_t nrows) {
+  if (!c || !cfg || !table) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (cfg->n_levels != 5 || cfg->flag_rad < 0 || cfg->flag_rad > 1) return PIP_ERR_PARAM;
+  if (cfg->deriv != 0 && cfg->deriv != 1 && cfg->deriv != 4) return PIP_ERR_PARAM;
+  if (nrows < 3 || !(cfg->n0fac != 0.0) || !(cfg->f_p_ini != 0.0) || !std::isfinite(cfg->f_p_p_ini))
+    return PIP_ERR_PARAM;
+  for (int64_t r = 0; r + 1 < nrows; ++r)
+    if (!(table[4 * (r + 1)] > table[4 * r])) return PIP_ERR_PARAM;   // abscissae increase
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->nl_tab);
+  c->nl_tab = nullptr;
+  CK(cudaMalloc(&c->nl_tab, sizeof(double) * 4 * (size_t)nrows));
+  CK(cudaMemcpy(c->nl_tab, table, sizeof(double) * 4 * (size_t)nrows, cudaMemcpyHostToDevice));
+  pip::NlevConst k;
+  pip::nlev_constants(&k);
+  CK(cudaMemcpy(c->nl_k, &k, sizeof k, cudaMemcpyHostToDevice));
+  KParams &kp = c->kp;
+  kp.nl_tab = c->nl_tab;
+  kp.nl_ntab = nrows;
+  kp.nl_xmin = table[0];
+  kp.nl_xrange = table[4 * (nrows - 1)] - table[0];
+  kp.nl_deriv = cfg->deriv;
+  kp.nl_n0fac = cfg->n0fac;
+  // tfac of set_IR type 4 (PIP_rot.f90:240-248); 5.0/3.0 is a default-real quotient there
+  kp.nl_tfac = c->p.flag_col % 2 == 1
+                   ? c->p.t_norm / ((double)(5.0f / 3.0f) * cfg->f_p_p_ini / cfg->f_p_ini)
+                   : c->p.beta / 2.0 * cfg->f_p_p_ini * 5.0 / 6.0 / cfg->f_p_ini;
+  c->nl_ready = true;
+  c->nl_init = false;
+  c->coef_valid = false;
+  return PIP_OK;
+}
+
+int pip_set_nexcite(pip_ctx *c, const double *nexcite) {
+  if (!c || !nexcite) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(c->kp.nl_nex, nexcite, 6 * c->plane_bytes(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_get_nexcite(pip_ctx *c, double *nexcite) {
+  if (!c || !nexcite) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(nexcite, c->kp.nl_nex, 6 * c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_get_colrat(pip_ctx *c, double *colrat) {
+  if (!c || !colrat) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(colrat, c->nl_cr, 36 * c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_get_ion_pot(pip_ctx *c, double *ion_pot) {
+  if (!c || !ion_pot) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(ion_pot, c->nl_ip, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_nlevel_gm_rec_ref(pip_ctx *c, double *gm_rec_ref) {
+  if (!c || !gm_rec_ref) return PIP_ERR_NULL;
+  if (!c->kp.irn) return PIP_ERR_PARAM;
+  if (!c->nl_init) return PIP_ERR_STATE;
+  *gm_rec_ref = c->kp.nl_gref;
+  return PIP_OK;
+}
+
 int pip_last_cuda_error(void) { return g_last_cuda_error; }
 
 const char *pip_strerror(int code) {
@@ -1287,6 +1511,7 @@ const char *pip_strerror(int code) {
     case PIP_ERR_STATE: return "call out of order";
     case PIP_ERR_NOMEM: return "device allocation failed";
     case PIP_ERR_NULL: return "NULL argument";
+    case PIP_ERR_RATE: return "negative rate of the 6-level hydrogen model";
     default: return "unknown status";
   }
 }

@@ -25,12 +25,15 @@
 #include "../../include/pip_gpu.h"
 #include "pip_kernels.cuh"
 #include "pip_mixed_cell.cuh"
+#include "pip_mixed_tile.cuh"
 #include "pip_physics.cuh"
 
 namespace pip {
 namespace ens {
 
 constexpr int NVM = 8, NV = 13, kH = 2;
+// 2D members: the mixed stage kernels' 16x14 tiles, walked by one CTA
+constexpr int TX2 = 16, TY2 = 14;
 
 struct Member {
   long long off;      // first float of the member's planes in hi/lo/U1
@@ -268,8 +271,119 @@ __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *
   }
 }
 
-// Persistent ensemble kernel: CTAs take runs from the queue until it is empty.
-template <int NT>
+// Shared memory of a 2D member's tile step (the mixed stage kernel's layout).
+template <int NVM2>
+constexpr size_t smem_2d() {
+  constexpr int RR = (TX2 + 2 * kH) * (TY2 + 2 * kH);
+  constexpr int NFX = (TX2 + 1) * TY2, NFY = TX2 * (TY2 + 1);
+  return sizeof(float) * (NVM2 + 5) * (RR + NFX + NFY) +
+         (NVM2 == 9 ? 2 * sizeof(double) * (NFX + NFY) : 0);
+}
+
+// A 2D member (ion planes NVM2 = 8, or 9 with Dedner cleaning) advanced by one CTA to the
+// end time: its cfl, then per step stage 1 over every tile and stage 2 over every tile
+// (mixed::tile_stage, the single-run mixed kernels' arithmetic), the CTA synchronised
+// between tiles and stages.
+template <int NT, int NVM2>
+__device__ void run_member_2d(const KParams &p, float *Ahi, float *Alo, float *B, RunState &rs,
+                              double t_end, long long max_steps, float *smem, double *s_red) {
+  constexpr int NV2 = NVM2 + 5;
+  constexpr int RR = (TX2 + 2 * kH) * (TY2 + 2 * kH);
+  constexpr int NFX = (TX2 + 1) * TY2, NFY = TX2 * (TY2 + 1);
+  float *sV = smem;
+  double *sD6 = reinterpret_cast<double *>(sV + NV2 * RR);
+  double *sD9 = sD6 + (NVM2 == 9 ? NFX + NFY : 0);
+  float *sFx = reinterpret_cast<float *>(sD9 + (NVM2 == 9 ? NFX + NFY : 0));
+  float *sFy = sFx + NV2 * NFX;
+  const int tid = threadIdx.x;
+  const long long nc = p.nc;
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  // cfl of the first step: floors of every cell and the CFL terms (the mixed cfl kernel's
+  // arithmetic)
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  for (long long q = tid; q < nc; q += NT) {
+    double um[NVM2], uh[5];
+#pragma unroll
+    for (int n = 0; n < NVM2; ++n) um[n] = (double)Ahi[q + n * nc] + (double)Alo[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n)
+      uh[n] = (double)Ahi[q + (NVM2 + n) * nc] + (double)Alo[q + (NVM2 + n) * nc];
+    mixed::floors_mhd<NVM2>(um, p);
+    mixed::floors_hd(uh, p);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      float h = (float)um[n];
+      Ahi[q + n * nc] = h;
+      Alo[q + n * nc] = (float)(um[n] - (double)h);
+      h = (float)uh[n];
+      Ahi[q + (NVM2 + n) * nc] = h;
+      Alo[q + (NVM2 + n) * nc] = (float)(uh[n] - (double)h);
+    }
+    const int i = (int)(q % p.ix), j = (int)(q / p.ix);
+    if (i >= p.m0 && i < p.ix - p.m0 && j >= p.m1 && j < p.jx - p.m1) {
+      float fm[NVM2], fh[5];
+#pragma unroll
+      for (int n = 0; n < NVM2; ++n) fm[n] = (float)um[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
+      const Prim<float> qm = cq2pv_mhd<float, NVM2>(fm, gmf, rolf, prlf);
+      const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
+      const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[j]), p.dz0));
+      dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
+                                    cfl_hd_cell<float>(qh, gmf, sg)));
+    }
+    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (p.ir) {
+      double g1, g2;
+      mixed::ir_rates<NVM2>(um, p, g1, g2);
+      grc = fmax(grc, fmax(g1, g2));
+    }
+  }
+  block_minmax<NT>(dtc, rhoc, grc, s_red);
+  double dt = finalize_dt(p, dtc, rhoc, grc);
+  const int ntx = (p.nx + TX2 - 1) / TX2, nty = (p.ny + TY2 - 1) / TY2, ntiles = ntx * nty;
+  bool bad = false;
+  for (;;) {
+    const double tn = rs.time + dt;
+    const bool last = (t_end > 0.0 && tn >= t_end) || (max_steps > 0 && rs.steps + 1 >= max_steps);
+    const double cmax = p.sg_all / dt;
+    double d1 = 10.0, r1 = 0.0, g1 = 0.0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int i0 = p.m0 + (t % ntx) * TX2, j0 = p.m1 + (t / ntx) * TY2;
+      mixed::tile_stage<2, NVM2, 1, TX2, TY2, NT, kH>(p, Ahi, Ahi, Alo, B, nullptr, i0, j0, dt, cmax,
+                                                     0, false, sV, sD6, sD9, sFx, sFy, d1, r1, g1,
+                                                     bad);
+      __syncthreads();   // the next tile reuses the shared memory
+    }
+    double d2 = 10.0, r2 = 0.0, g2 = 0.0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int i0 = p.m0 + (t % ntx) * TX2, j0 = p.m1 + (t / ntx) * TY2;
+      mixed::tile_stage<2, NVM2, 2, TX2, TY2, NT, kH>(p, B, Ahi, Alo, Ahi, Alo, i0, j0, dt, cmax,
+                                                     last ? 1 : 2, false, sV, sD6, sD9, sFx, sFy,
+                                                     d2, r2, g2, bad);
+      __syncthreads();
+    }
+    rs.time = tn;
+    rs.steps += 1;
+    rs.dt = dt;
+    if (__syncthreads_or(bad)) {
+      rs.status = 3;  // PIP_ERR_NAN
+      break;
+    }
+    if (dt <= 1.0e-12) {
+      rs.status = 4;  // PIP_ERR_DT
+      break;
+    }
+    if (last) break;
+    block_minmax<NT>(d2, r2, g2, s_red);
+    dt = finalize_dt(p, d2, r2, g2);
+  }
+}
+
+// Persistent ensemble kernel: CTAs take runs from the queue until it is empty.  HAS2D: the
+// instance that can also step 2D members (its larger register footprint stays out of
+// ensembles of 1D members only).
+template <int NT, bool HAS2D>
 __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const KParams *kps,
                                                       const int *order, int nmem, float *hi,
                                                       float *lo, float *U1, RunState *st,
@@ -296,6 +410,16 @@ __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const K
     float *Ahi = hi + mem[r].off, *Alo = lo + mem[r].off, *B = U1 + mem[r].off;
     RunState rs = st[r];
     if (rs.status != 0 || (t_end > 0.0 && rs.time >= t_end)) {
+      __syncthreads();
+      continue;
+    }
+    if (HAS2D && p.ndim == 2) {
+      // (the host allows 2D members only with NT >= TX2 * TY2 threads)
+      if (NT >= TX2 * TY2) {
+        if (p.nvm == 9) run_member_2d<NT, 9>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
+        else run_member_2d<NT, 8>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
+      }
+      if (tid == 0) st[r] = rs;
       __syncthreads();
       continue;
     }
@@ -371,15 +495,24 @@ __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const K
   }
 }
 
-constexpr size_t smem_bytes(int nt) { return sizeof(float) * NV * ((nt - 1 + 2 * kH) + nt); }
+// dynamic shared memory of a launch: the 1D chunk layout, and the 2D tile layout when the
+// ensemble holds 2D members
+constexpr size_t smem_1d(int nt) { return sizeof(float) * NV * ((nt - 1 + 2 * kH) + nt); }
+constexpr size_t smem_bytes(int nt, bool has2d) {
+  return has2d && smem_2d<9>() > smem_1d(nt) ? smem_2d<9>() : smem_1d(nt);
+}
 
-cudaError_t launch(int nt, int grid, cudaStream_t s, const Member *mem, const KParams *kps,
-                   const int *order, int nmem, float *hi, float *lo, float *U1, RunState *st,
-                   unsigned *queue, double t_end, long long max_steps) {
-#define PIP_ENS_CASE(NTV)                                                                       \
-  case NTV:                                                                                     \
-    ensemble_kernel<NTV><<<grid, NTV, smem_bytes(NTV), s>>>(mem, kps, order, nmem, hi, lo, U1, \
-                                                            st, queue, t_end, max_steps);       \
+cudaError_t launch(int nt, bool has2d, int grid, cudaStream_t s, const Member *mem,
+                   const KParams *kps, const int *order, int nmem, float *hi, float *lo,
+                   float *U1, RunState *st, unsigned *queue, double t_end, long long max_steps) {
+#define PIP_ENS_CASE(NTV)                                                                      \
+  case NTV:                                                                                    \
+    if (has2d)                                                                                 \
+      ensemble_kernel<NTV, true><<<grid, NTV, smem_bytes(NTV, true), s>>>(                     \
+          mem, kps, order, nmem, hi, lo, U1, st, queue, t_end, max_steps);                     \
+    else                                                                                       \
+      ensemble_kernel<NTV, false><<<grid, NTV, smem_bytes(NTV, false), s>>>(                   \
+          mem, kps, order, nmem, hi, lo, U1, st, queue, t_end, max_steps);                     \
     break;
   switch (nt) {
     PIP_ENS_CASE(128)
@@ -392,26 +525,39 @@ cudaError_t launch(int nt, int grid, cudaStream_t s, const Member *mem, const KP
   return cudaGetLastError();
 }
 
-cudaError_t prepare() {
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(ensemble_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes(512))) != cudaSuccess)
-    return e;
-  return cudaFuncSetAttribute(ensemble_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem_bytes(1024));
+template <int NT, bool HAS2D>
+cudaError_t set_smem() {
+  return cudaFuncSetAttribute(ensemble_kernel<NT, HAS2D>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes(NT, HAS2D));
 }
 
-int max_ctas_per_sm(int nt) {
+cudaError_t prepare() {
+  cudaError_t e;
+  if ((e = set_smem<128, false>()) != cudaSuccess || (e = set_smem<256, false>()) != cudaSuccess ||
+      (e = set_smem<512, false>()) != cudaSuccess || (e = set_smem<1024, false>()) != cudaSuccess ||
+      (e = set_smem<256, true>()) != cudaSuccess || (e = set_smem<512, true>()) != cudaSuccess ||
+      (e = set_smem<1024, true>()) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
+template <int NT, bool HAS2D>
+int occupancy() {
   int n = 0;
-  cudaError_t e = cudaSuccess;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &n, ensemble_kernel<NT, HAS2D>, NT, smem_bytes(NT, HAS2D));
+  return e == cudaSuccess ? n : 0;
+}
+
+int max_ctas_per_sm(int nt, bool has2d) {
   switch (nt) {
-    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<128>, 128, smem_bytes(128)); break;
-    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<256>, 256, smem_bytes(256)); break;
-    case 512: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<512>, 512, smem_bytes(512)); break;
-    case 1024: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_kernel<1024>, 1024, smem_bytes(1024)); break;
+    case 128: return has2d ? 0 : occupancy<128, false>();
+    case 256: return has2d ? occupancy<256, true>() : occupancy<256, false>();
+    case 512: return has2d ? occupancy<512, true>() : occupancy<512, false>();
+    case 1024: return has2d ? occupancy<1024, true>() : occupancy<1024, false>();
     default: return 0;
   }
-  return e == cudaSuccess ? n : 0;
 }
 
 }  // namespace ens
@@ -441,6 +587,7 @@ struct pip_ensemble {
   RunState *d_st = nullptr;
   unsigned *d_queue = nullptr;
   int threads = 256, ctas_per_sm = 2;
+  bool has2d = false;                             // some member is 2D
   cudaGraphExec_t graph = nullptr;
   double graph_t_end = -1.0;
   long long graph_steps = -1;
@@ -472,7 +619,7 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
   std::vector<double> dxtab;
   for (int r = 0; r < n; ++r) {
     const pip_params &p = members[r];
-    if (p.ndim != 1 || p.precision != PIP_MIXED) {
+    if ((p.ndim != 1 && p.ndim != 2) || p.precision != PIP_MIXED) {
       delete e;
       return PIP_ERR_PARAM;
     }
@@ -483,18 +630,25 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
     }
     e->mem[r].off = off;
     e->mem[r].kp = r;
-    off += (long long)pip::ens::NV * p.ix;
-    // dx, 1/dx and dy of this member, pointed at after the upload of the table
+    const long long nc = (long long)p.ix * p.jx;
+    off += (long long)(p.nvar_m + 5) * nc;
+    // dx, 1/dx, dy (and in 2D 1/dy) of this member, pointed at after the upload of the table
+    const int ny = p.ndim == 2 ? p.jx : 1;
     for (int i = 0; i < p.ix; ++i) dxtab.push_back(p.dx[i]);
     for (int i = 0; i < p.ix; ++i) dxtab.push_back(1.0 / p.dx[i]);
-    dxtab.push_back(p.dy[0]);
+    for (int j = 0; j < ny; ++j) dxtab.push_back(p.dy[j]);
+    if (p.ndim == 2)
+      for (int j = 0; j < ny; ++j) dxtab.push_back(1.0 / p.dy[j]);
     e->kp[r].dx = reinterpret_cast<const double *>(dxoff);
     e->kp[r].rdx = reinterpret_cast<const double *>(dxoff + p.ix);
     e->kp[r].dy = reinterpret_cast<const double *>(dxoff + 2 * p.ix);
-    e->kp[r].rdy = nullptr;
-    dxoff += 2 * p.ix + 1;
-    e->cost[r] = (long long)p.ix * p.ix;
+    e->kp[r].rdy = p.ndim == 2 ? reinterpret_cast<const double *>(dxoff + 2 * p.ix + ny) : nullptr;
+    dxoff += 2 * p.ix + (p.ndim == 2 ? 2 * ny : 1);
+    // cells x steps: the steps go as the finest width
+    e->cost[r] = nc * std::max(p.ix, p.ndim == 2 ? p.jx : 0);
+    if (p.ndim == 2) e->has2d = true;
   }
+  if (e->has2d) e->threads = std::max(e->threads, 256);
   e->total_floats = off;
   auto fail = [&](cudaError_t c) {
     pip::record_cuda_error((int)c);
@@ -522,6 +676,7 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
     e->kp[r].dx = e->d_dx + reinterpret_cast<long long>(e->kp[r].dx);
     e->kp[r].rdx = e->d_dx + reinterpret_cast<long long>(e->kp[r].rdx);
     e->kp[r].dy = e->d_dx + reinterpret_cast<long long>(e->kp[r].dy);
+    if (e->kp[r].rdy) e->kp[r].rdy = e->d_dx + reinterpret_cast<long long>(e->kp[r].rdy);
   }
   if ((c = cudaMalloc(&e->d_kp, sizeof(pip::KParams) * n)) != cudaSuccess) return fail(c);
   if ((c = cudaMemcpy(e->d_kp, e->kp.data(), sizeof(pip::KParams) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -539,9 +694,10 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
   if ((c = cudaMalloc(&e->d_st, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
   if ((c = cudaMemset(e->d_st, 0, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
   if ((c = cudaMalloc(&e->d_queue, sizeof(unsigned))) != cudaSuccess) return fail(c);
-  int maxix = 0;
-  for (int r = 0; r < n; ++r) maxix = std::max(maxix, members[r].ix);
-  if ((c = cudaMalloc(&e->stage64, sizeof(double) * pip::ens::NV * maxix)) != cudaSuccess) return fail(c);
+  long long maxst = 0;
+  for (int r = 0; r < n; ++r)
+    maxst = std::max(maxst, (long long)(members[r].nvar_m + 5) * members[r].ix * members[r].jx);
+  if ((c = cudaMalloc(&e->stage64, sizeof(double) * maxst)) != cudaSuccess) return fail(c);
   *out = e;
   return PIP_OK;
 }
@@ -573,10 +729,10 @@ int pip_ensemble_upload(pip_ensemble *e, int member, const double *U_h, const do
   EK(cudaSetDevice(e->device));
   const pip::KParams &k = e->kp[member];
   const size_t pb = sizeof(double) * (size_t)k.nc;
-  EK(cudaMemcpyAsync(e->stage64, U_m, pb * 8, cudaMemcpyHostToDevice, e->stream));
-  EK(cudaMemcpyAsync(e->stage64 + 8 * k.nc, U_h, pb * 5, cudaMemcpyHostToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->stage64, U_m, pb * k.nvm, cudaMemcpyHostToDevice, e->stream));
+  EK(cudaMemcpyAsync(e->stage64 + k.nvm * k.nc, U_h, pb * 5, cudaMemcpyHostToDevice, e->stream));
   EK(pip::mixed_split(e->stage64, e->hi + e->mem[member].off, e->lo + e->mem[member].off,
-                      pip::ens::NV * k.nc, e->stream));
+                      (k.nvm + 5) * k.nc, e->stream));
   RunState z;
   std::memset(&z, 0, sizeof z);
   EK(cudaMemcpyAsync(e->d_st + member, &z, sizeof z, cudaMemcpyHostToDevice, e->stream));
@@ -595,9 +751,9 @@ int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, d
   EK(cudaMemcpyAsync(&rs, e->d_st + member, sizeof rs, cudaMemcpyDeviceToHost, e->stream));
   if (U_h && U_m) {
     EK(pip::mixed_join(e->hi + e->mem[member].off, e->lo + e->mem[member].off, e->stage64,
-                       pip::ens::NV * k.nc, e->stream));
-    EK(cudaMemcpyAsync(U_m, e->stage64, pb * 8, cudaMemcpyDeviceToHost, e->stream));
-    EK(cudaMemcpyAsync(U_h, e->stage64 + 8 * k.nc, pb * 5, cudaMemcpyDeviceToHost, e->stream));
+                       (k.nvm + 5) * k.nc, e->stream));
+    EK(cudaMemcpyAsync(U_m, e->stage64, pb * k.nvm, cudaMemcpyDeviceToHost, e->stream));
+    EK(cudaMemcpyAsync(U_h, e->stage64 + k.nvm * k.nc, pb * 5, cudaMemcpyDeviceToHost, e->stream));
   }
   EK(cudaStreamSynchronize(e->stream));
   if (time) *time = rs.time;
@@ -609,7 +765,8 @@ int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, d
 int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm) {
   if (!e) return PIP_ERR_NULL;
   if (threads != 128 && threads != 256 && threads != 512 && threads != 1024) return PIP_ERR_PARAM;
-  const int mx = pip::ens::max_ctas_per_sm(threads);
+  if (e->has2d && threads < 256) return PIP_ERR_PARAM;   // a 2D tile needs 224 threads
+  const int mx = pip::ens::max_ctas_per_sm(threads, e->has2d);
   if (ctas_per_sm < 1 || ctas_per_sm > mx) return PIP_ERR_PARAM;
   e->threads = threads;
   e->ctas_per_sm = ctas_per_sm;
@@ -618,7 +775,8 @@ int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm) {
 
 static int ens_enqueue(pip_ensemble *e, double t_end, long long max_steps) {
   EK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), e->stream));
-  EK(pip::ens::launch(e->threads, e->sms * e->ctas_per_sm, e->stream, e->d_mem, e->d_kp, e->d_order,
+  EK(pip::ens::launch(e->threads, e->has2d, e->sms * e->ctas_per_sm, e->stream, e->d_mem, e->d_kp,
+                      e->d_order,
                       e->n, e->hi, e->lo, e->U1, e->d_st, e->d_queue, t_end, max_steps));
   return PIP_OK;
 }
@@ -684,7 +842,8 @@ int pip_ensemble_tune(pip_ensemble *e, double t_probe, int *threads, int *ctas_p
   int bt = e->threads, bc = e->ctas_per_sm;
   const int cand_t[4] = {128, 256, 512, 1024};
   for (int ti = 0; ti < 4; ++ti) {
-    const int mx = std::min(pip::ens::max_ctas_per_sm(cand_t[ti]), 8);
+    if (e->has2d && cand_t[ti] < 256) continue;
+    const int mx = std::min(pip::ens::max_ctas_per_sm(cand_t[ti], e->has2d), 8);
     for (int cps = 1; cps <= mx; ++cps) {
       e->threads = cand_t[ti];
       e->ctas_per_sm = cps;

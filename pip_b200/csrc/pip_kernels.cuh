@@ -11,6 +11,16 @@ namespace pip {
 constexpr int kMaxMargin = 3;
 constexpr int kMaxPlanes = 14;   // 9 ion + 5 neutral
 
+// Cell-independent coefficients of the 6-level hydrogen model's collisional rates
+// (get_col_ion_coeff, PIP_rot.f90:378-439,507-524), built on the host in the Fortran
+// operation order; index a, b = level - 1, entries with a < b used.
+struct NlevConst {
+  double gw[6], eion[6], rn[6];
+  double xrat[5][5], enn[5][5], rnn[5][5], ann[5][5], bnn[5][5], lgt[5][5];
+  double an0[5], bn0[5], lgi[5];
+  double eev[6];     // IRgetionpot's level energies (eV, default-real literals)
+};
+
 // Scalars and tables of one simulation, passed by value to every kernel.
 struct KParams {
   int ndim;          // 1 or 2
@@ -23,7 +33,8 @@ struct KParams {
   int irs;           // 2 or 3: set_IR's Popescu law, rates from every stage's state (FP64 form)
   int irl;           // 1, 2 or 3: set_IR runs before each cfl (with get_Te's energy rewrite)
   int irf;           // 1: set_IR type 1, rates frozen in irg between the time loop's set_IR calls
-  int ir_type;       // IR energy form 1 or 2
+  int ir_type;       // IR energy form 0 (with the ionisation potential, set_IR type 4), 1 or 2
+  int irn;           // set_IR type 4: the 6-level hydrogen model (FP64 form; irs = 4 as well)
   long long nc;      // ix*jx
   double gm, ro_lim, pr_lim, ac, safety;
   double igm1;       // 1/(gm-1)
@@ -52,6 +63,20 @@ struct KParams {
                                    // double) of the eta of the last set_resistivity
   double resi_dt;    // cfl_resi's bound min(safety*gmin^2/max(eta,1e-8)) over the interior
                      // cells (+inf without resistivity); seeds the min-CFL reduction slot
+  // set_IR type 4 (irn): exponential-integral table rows (yn, E0, E1, E2), its first
+  // abscissa and range, the model's coefficients, level populations (6 planes: current and
+  // the excitation update's target), colrat (36 planes, plane a + 6*b = colrat(a+1,b+1)),
+  // ion_pot, and the normalisation of set_IR type 4 / IRgetionpot
+  const double *nl_tab;
+  long long nl_ntab;
+  double nl_xmin, nl_xrange;
+  const NlevConst *nl_k;
+  double *nl_nex, *nl_nex2, *nl_cr, *nl_ip;
+  int nl_deriv;      // convective derivative: 0 none, 1 two-point, 4 five-point
+  int nl_odd;        // mod(flag_col,2) == 1
+  double nl_T0, nl_tfac, nl_n0, nl_n0fac, nl_gref, nl_tir;
+  double nl_en_even; // beta/T0/2/8.6173e-5 (even flag_col)
+  double nl_lim;     // min(safety,0.01) of cfl_pip_ir_nexcite
   const double *dx, *dy;
   const double *rdx, *rdy;   // 1/dx, 1/dy (FP32-mixed form only; null otherwise)
   // boundary maps: ghost layer q of side s (0 lower, 1 upper) copies interior index g?[s][q]
@@ -67,6 +92,8 @@ struct DevCtrl {
   unsigned long long red_dt[2];   // min CFL candidate (positive doubles as ordered bits)
   unsigned long long red_rho[2];  // max rho*alpha_c
   unsigned long long red_gr[2];   // max IR rate
+  unsigned long long red_ip[2];   // set_IR type 4, flag_IR_type 0: max(ion_pot/e_int, 1e-5)
+  unsigned long long red_nx[2];   // set_IR type 4: max(dNexcite/dt, 1e-5)
   int last, done, nan_flag, status;
   unsigned int blocks_done;       // last-block-done counter of the stage-2 kernel
 };
@@ -90,6 +117,20 @@ struct Launchers {
   // the TMA map of a stage source U (nvm+5 FP64 planes) for the 2D stage kernels' tiles;
   // false where the grid or the address breaks the TMA's alignment rules
   bool (*tile_map)(const KParams &p, const double *U, CUtensorMap *map);
+  // set_IR type 4.  nlev_ref: colrat at (T_norm, n_norm) with cell (1,1,1)'s populations
+  // into out[0..35] (out[a*6+b] = colrat(a+1,b+1)) and that cell's recombination sum
+  // (Gm_rec_ref) into out[36].  nlev_rates: set_IR over every cell of U (colrw: a
+  // set_collisional rewrite comes first; ipmode 0 no ion_pot, 1 ion_pot from the new colrat,
+  // 2 from crref), writing colrat, the rates into irg and ion_pot; status 9 into ctrl on a
+  // negative rate.  nlev_update: hydrogen_excitation_update after stage `stage` (dt from
+  // ctrl), nl_nex -> nl_nex2 with its ghosts.  nlev_cfl: cfl_pip_ir's type-4 terms and
+  // cfl_pip_ir_nexcite into slot `slot`.
+  cudaError_t (*nlev_ref)(const KParams &p, double *out, cudaStream_t s);
+  cudaError_t (*nlev_rates)(const KParams &p, const double *U, int colrw, int ipmode,
+                            const double *crref, DevCtrl *ctrl, cudaStream_t s);
+  cudaError_t (*nlev_update)(const KParams &p, const double *U, const DevCtrl *ctrl, int stage,
+                             cudaStream_t s);
+  cudaError_t (*nlev_cfl)(const KParams &p, double *U, DevCtrl *ctrl, int slot, cudaStream_t s);
 };
 
 const Launchers &launchers_fast();
@@ -123,6 +164,9 @@ cudaError_t halo_unpack(const KParams &p, int face, void *a0, void *a1, int elem
 
 // Records a CUDA error code for pip_last_cuda_error (pip_capi.cu).
 void record_cuda_error(int code);
+
+// The 6-level model's cell-independent coefficients (pip_nlevel.cu).
+void nlev_constants(NlevConst *k);
 
 // Validates a parameter block and fills the kernel parameters without allocating
 // (pip_capi.cu); dx and dy of the result are left null.

@@ -84,6 +84,12 @@ __device__ __forceinline__ double finalize_dt(const KParams &p, const DevCtrl *c
   double rho = bitsd(c->red_rho[slot]);
   dt = fmin(dt, p.col_lim / rho);
   if (p.ir) dt = fmin(dt, p.ir_lim / fmax(bitsd(c->red_gr[slot]), 1.0e-5));
+  if (p.irn) {
+    // cfl_pip_ir's ion_pot term (flag_IR_type 0) and cfl_pip_ir_nexcite; the slots hold
+    // the maxima already raised to 1e-5
+    if (p.ir_type == 0) dt = fmin(dt, p.safety / bitsd(c->red_ip[slot]));
+    dt = fmin(dt, p.nl_lim / bitsd(c->red_nx[slot]));
+  }
   return dt;
 }
 
@@ -215,6 +221,11 @@ __device__ __forceinline__ void set_ir_cell(double (&um)[NVM], double (&uh)[5], 
                                             double &gr, double &gi) {
   double te_m, te_h, rm, rh;
   get_te<NVM>(um, uh, p, te_m, te_h, rm, rh);
+  if (p.irn) {   // type 4: the rates come from nlev_rates_kernel (irg)
+    gr = 0.0;
+    gi = 0.0;
+    return;
+  }
   ir_law_rates(p, um[0], te_m, gr, gi);
 }
 
@@ -260,7 +271,8 @@ __device__ __forceinline__ void collision_ds(const double (&um)[NVM], const doub
   }
 }
 
-// IR exchange of source_PIP (PIP_rot.f90:1370-1411, flag_IR_type 1 or 2).
+// IR exchange of source_PIP (PIP_rot.f90:1370-1411, flag_IR_type 0, 1 or 2; 0 has type 1's
+// energy term, its ionisation potential is added by the caller).
 __device__ __forceinline__ void ir_ds(const Prim<double> &qm, const Prim<double> &qh, double gr,
                                       double gi, const KParams &p, double (&ds)[5]) {
   const double gm = p.gm;
@@ -270,7 +282,7 @@ __device__ __forceinline__ void ir_ds(const Prim<double> &qm, const Prim<double>
   ds[3] = gr * qm.de * qm.vz - gi * qh.de * qh.vz;
   const double kin = 0.5 * (gr * qm.de * (qm.vx * qm.vx + qm.vy * qm.vy + qm.vz * qm.vz) -
                             gi * qh.de * (qh.vx * qh.vx + qh.vy * qh.vy + qh.vz * qh.vz));
-  if (p.ir_type == 1)
+  if (p.ir_type != 2)
     ds[4] = kin - gi * qh.pr / (gm - 1.0) + 0.5 * gr * qm.pr / (gm - 1.0);
   else
     ds[4] = kin - gi * qh.pr / (gm - 1.0) + gr * qm.pr / (gm - 1.0);
@@ -593,6 +605,8 @@ stage_kernel(const __grid_constant__ KParams p, const double *__restrict__ Us, c
     ctrl->red_dt[ns] = dbits(fmin(10.0, p.resi_dt));  // cfl_mhd's start, cfl_resi's bound
     ctrl->red_rho[ns] = 0ull;
     ctrl->red_gr[ns] = 0ull;
+    ctrl->red_ip[ns] = 0ull;
+    ctrl->red_nx[ns] = 0ull;
   }
 
   if (STAGE == 1 && RES && p.resi == 2 && block0 && tid == 0) {
@@ -616,16 +630,13 @@ stage_kernel(const __grid_constant__ KParams p, const double *__restrict__ Us, c
       tma_load_tile(sV, &tmap, i0 - kH, j0 - kH, &s_bar);
     }
     __syncthreads();
-    const bool ok = tma_bar_wait(&s_bar, kTmaWaitLimit);
-    if (__syncthreads_or(!ok)) {
-      // the tile did not arrive: flag the stage and let the copy land (bounded) before the
-      // CTA's shared memory is released
-      if (tid == 0) {
-        atomicCAS(&ctrl->status, 0, 5);  // PIP_ERR_ITER
-        ctrl->done = 1;
-        tma_bar_wait(&s_bar, kTmaWaitLimit);
-      }
-      return;
+    if (!tma_bar_wait(&s_bar, kTmaWaitLimit)) {
+      // the tile did not arrive: flag the stage (the run stops with PIP_ERR_ITER; this
+      // tile's results are void) and let the copy land (bounded) before going on, so that
+      // no copy is in flight when the CTA's shared memory is released
+      atomicCAS(&ctrl->status, 0, 5);
+      ctrl->done = 1;
+      tma_bar_wait(&s_bar, kTmaWaitLimit);
     }
     for (int idx = tid; idx < RR; idx += NT) {
       const int ri = idx % RX, rj = idx / RX;
@@ -827,6 +838,10 @@ stage_kernel(const __grid_constant__ KParams p, const double *__restrict__ Us, c
     double gr = 0.0, gion = 0.0;
     if (COL && p.irs) {
       set_ir_cell<NVM>(s_m, s_h, p, gr, gion);  // set_IR of the stage
+      if (p.irn) {                              // type 4: nlev_rates_kernel's rates
+        gion = p.irg[q];
+        gr = p.irg[nc + q];
+      }
     } else if (COL && p.irf) {
       gion = p.irg[q];                          // the time loop's last set_IR
       gr = p.irg[nc + q];
@@ -885,6 +900,8 @@ stage_kernel(const __grid_constant__ KParams p, const double *__restrict__ Us, c
           S_h[n] = S_h[n] + ds[n];
           S_m[n] = S_m[n] - ds[n];
         }
+        // flag_IR_type 0: S_m(5) - ion_pot + arb_heat (0), PIP_rot.f90:1397
+        if (p.irn && p.ir_type == 0) S_m[4] = S_m[4] - p.nl_ip[q] + 0.0;
       }
     }
     // time_integral: add_flux_rk (x, then y) and add_source, per species
@@ -1167,6 +1184,10 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
     double gr = 0.0, gion = 0.0;
     if (p.irs) {
       set_ir_cell<NVM>(um, uh, p, gr, gion);  // the rates of the state as given
+      if (p.irn) {
+        gion = p.irg[q];
+        gr = p.irg[nc + q];
+      }
     } else if (p.irf) {
       gion = p.irg[q];                        // the last set_IR's
       gr = p.irg[nc + q];
@@ -1192,6 +1213,7 @@ __global__ void source_kernel(const KParams p, double *U, double *S, double dt_c
         sh[n] = sh[n] + ds[n];
         sm[n] = sm[n] - ds[n];
       }
+      if (p.irn && p.ir_type == 0) sm[4] = sm[4] - p.nl_ip[q] + 0.0;
     }
     for (int n = 0; n < 5; ++n) {
       U[q + n * nc] = um[n];
@@ -1253,6 +1275,8 @@ __global__ void nan_kernel(const double *__restrict__ U, long long n, int *flag)
     bad |= !isfinite(U[t]);
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
+
+#include "pip_nlevel_impl.cuh"
 
 // ---------------------------------------------------------------- host launchers
 
@@ -1401,6 +1425,37 @@ static cudaError_t launch_coefficients(const KParams &p, double *U, cudaStream_t
   return cudaGetLastError();
 }
 
+static cudaError_t launch_nlev_ref(const KParams &p, double *out, cudaStream_t s) {
+  nlev_ref_kernel<<<1, 32, 0, s>>>(p, out);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_nlev_rates(const KParams &p, const double *U, int colrw, int ipmode,
+                                     const double *crref, DevCtrl *ctrl, cudaStream_t s) {
+  const int g = grid_for(p.nc, 128);
+  if (p.nvm == 9) nlev_rates_kernel<9><<<g, 128, 0, s>>>(p, U, colrw, ipmode, crref, ctrl);
+  else nlev_rates_kernel<8><<<g, 128, 0, s>>>(p, U, colrw, ipmode, crref, ctrl);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_nlev_update(const KParams &p, const double *U, const DevCtrl *ctrl,
+                                      int stage, cudaStream_t s) {
+  const int g = grid_for((long long)p.nx * p.ny, 128);
+  if (p.ndim == 1) nlev_update_kernel<1, 8><<<g, 128, 0, s>>>(p, U, ctrl, stage);
+  else if (p.nvm == 9) nlev_update_kernel<2, 9><<<g, 128, 0, s>>>(p, U, ctrl, stage);
+  else nlev_update_kernel<2, 8><<<g, 128, 0, s>>>(p, U, ctrl, stage);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_nlev_cfl(const KParams &p, double *U, DevCtrl *ctrl, int slot,
+                                   cudaStream_t s) {
+  const int g = grid_for(p.nc, 256);
+  if (p.ndim == 1) nlev_cfl_kernel<1, 8><<<g, 256, 0, s>>>(p, U, ctrl, slot);
+  else if (p.nvm == 9) nlev_cfl_kernel<2, 9><<<g, 256, 0, s>>>(p, U, ctrl, slot);
+  else nlev_cfl_kernel<2, 8><<<g, 256, 0, s>>>(p, U, ctrl, slot);
+  return cudaGetLastError();
+}
+
 static cudaError_t launch_nan(const KParams &p, const double *U, int *flag, cudaStream_t s) {
   const long long n = p.nc * (p.nvm + 5);
   nan_kernel<<<grid_for(n, 256), 256, 0, s>>>(U, n, flag);
@@ -1414,7 +1469,9 @@ const Launchers &PIP_LAUNCHERS() {
                               PIP_FLAVOUR::launch_cfl,    PIP_FLAVOUR::launch_ghosts,
                               PIP_FLAVOUR::launch_flux,   PIP_FLAVOUR::launch_source,
                               PIP_FLAVOUR::launch_nan,    PIP_FLAVOUR::launch_coefficients,
-                              PIP_FLAVOUR::tile_map};
+                              PIP_FLAVOUR::tile_map,      PIP_FLAVOUR::launch_nlev_ref,
+                              PIP_FLAVOUR::launch_nlev_rates, PIP_FLAVOUR::launch_nlev_update,
+                              PIP_FLAVOUR::launch_nlev_cfl};
   return L;
 }
 

@@ -251,6 +251,7 @@ class DeviceBlock:
         self.mixed = block.settings.precision != 0
         self.last_stage = 0
         self._stream = torch.cuda.ExternalStream(self.ctx.stream, device=self.device)
+        self._side = {}
 
     def cfl(self) -> Tuple[float, float]:
         return self.ctx.cfl()
@@ -263,16 +264,16 @@ class DeviceBlock:
         self.ctx.dev_stage(k)
         self.last_stage = k
 
-    def dev_stage_rows(self, k: int, rows: int) -> None:
-        """Half of stage k: rows 1 the first and last tile rows (what the y exchange sends),
-        rows 2 the others."""
-        self.ctx.dev_stage_rows(k, rows)
+    def dev_stage_split(self, k: int):
+        """Stage k with its first and last tile rows (what the y exchange sends) on a
+        high-priority stream, concurrent with the middle rows; returns an event that fires
+        when the boundary rows are done."""
+        bs = self.ctx.dev_stage_split(k)
         self.last_stage = k
-
-    def record(self):
-        """An event on the context stream, after everything queued so far."""
+        if bs not in self._side:
+            self._side[bs] = self.torch.cuda.ExternalStream(bs, device=self.device)
         ev = self.torch.cuda.Event()
-        ev.record(self._stream)
+        ev.record(self._side[bs])
         return ev
 
     def wait(self, ev) -> None:
@@ -398,16 +399,13 @@ class DecomposedRun:
         return dt
 
     def _stage_overlapped(self, k: int) -> None:
-        """Stage k with its y exchange overlapped: the first and last tile rows, then the
-        exchange on the halo stream while the middle rows compute on the block streams."""
-        for e in self.engines:
-            e.dev_stage_rows(k, 1)
+        """Stage k with its y exchange overlapped: the first and last tile rows on a
+        high-priority stream, then the exchange on the halo stream while the middle rows
+        compute on the block streams."""
         hs = self._halo_stream
         for e in self.engines:
-            hs.wait_event(e.record())
+            hs.wait_event(e.dev_stage_split(k))
         self.halo(stream=hs)
-        for e in self.engines:
-            e.dev_stage_rows(k, 2)
         done = self.engines[0].torch.cuda.Event()
         done.record(hs)
         for e in self.engines:

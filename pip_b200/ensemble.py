@@ -1,4 +1,4 @@
-"""Batched ensembles of independent 1D two-fluid runs (include/pip_ensemble.h)."""
+"""Batched ensembles of independent 1D and 2D two-fluid runs (include/pip_ensemble.h)."""
 from __future__ import annotations
 
 import ctypes
@@ -11,7 +11,7 @@ from .params import PIP_MIXED, PipParams, Settings
 
 
 class Ensemble:
-    """Many 1D runs advanced together by one persistent launch (FP32-mixed form)."""
+    """Many 1D and 2D runs advanced together by one persistent launch (FP32-mixed form)."""
 
     def __init__(self, members: Sequence[Tuple[Settings, np.ndarray, np.ndarray]]):
         self.settings = [s.overrides(precision=PIP_MIXED) for s, _, _ in members]

@@ -188,6 +188,85 @@ def velocity_modes(X, Y, Lx, Ly, seed, amp, kmax):
     return out
 
 
+def lte_nexcite(s: Settings, ro_h: np.ndarray, ro_m: np.ndarray, pr_m: np.ndarray) -> np.ndarray:
+    """Nexcite (6, ...) for set_IR type 4 in local thermodynamic equilibrium: levels 1-5 share
+    rho_n in the Saha-Boltzmann ratios n_k/n_i = n_e g_k/(2 g_i) (2 pi m_e k T/h^2)^(-3/2)
+    exp(chi_k/kT) at the electron temperature and density set_IR type 4 uses
+    (Te_p*T_norm/tfac, rho_i*n_norm/n0fac; PIP_rot.f90:240-258), the form KHnlev.f90:74-93
+    sets its populations with; level 6 is rho_i."""
+    gm = s.gm
+    if s.flag_col % 2 == 1:
+        tfac = s.t_norm / (float(np.float32(5.0) / np.float32(3.0)) * s.f_p_p_ini / s.f_p_ini)
+    else:
+        tfac = s.beta / 2.0 * s.f_p_p_ini * 5.0 / 6.0 / s.f_p_ini
+    te = 0.5 * gm * (pr_m / ro_m) * s.t_norm / tfac
+    ne = ro_m * s.n_norm / s.n0fac
+    kb, me, h = 1.38064852e-23, 9.10938356e-31, 6.62607004e-34
+    chi = np.array([13.6, 3.4, 1.51, 0.85, 0.54]) * 1.602176634e-19
+    g = np.array([2.0, 8.0, 18.0, 32.0, 50.0])
+    saha = (2.0 * PI * me * kb * te / (h * h)) ** -1.5
+    ratio = np.stack([ne * g[k] / 2.0 * saha * np.exp(chi[k] / (kb * te)) for k in range(5)])
+    lev = ratio / ratio.sum(axis=0) * ro_h
+    return np.concatenate([lev, ro_m[None]], axis=0)
+
+
+def _fpp_for(s: Settings, te_p0: float) -> float:
+    """f_p_p_ini (with f_p_ini = 1) that makes set_IR type 4's electron temperature
+    Te_p*T_norm/tfac equal T_norm where Te_p = te_p0 (tfac of PIP_rot.f90:240-248)."""
+    if s.flag_col % 2 == 1:
+        return s.t_norm / te_p0 / float(np.float32(5.0) / np.float32(3.0))
+    return te_p0 * 2.0 / s.beta * 6.0 / 5.0
+
+
+def nlevel_tube(nx: int = 512, **kw):
+    """1D two-fluid shock tube with set_IR type 4 (the 6-level hydrogen model): the Brio-Wu
+    states of brio_wu() (rho 1 / 0.125, p 1 / 0.1, Bx 0.75, By +1 / -1, 50 % neutral by mass),
+    T_norm 6500 K, n_norm 1e17 m^-3, tfac such that the left ion state's electron
+    temperature is T_norm, populations in LTE (lte_nexcite), outflow boundaries.  Returns
+    (settings, U_h, U_m, Nexcite)."""
+    s = Settings(ndim=1, ix0=nx, start=(-0.5, -1.0, -1.0), end=(0.5, 1.0, 1.0),
+                 flag_bnd=[10, 10, 10, 10, 10, 10], n_fraction=0.5, col=100.0, safety=0.3,
+                 tend=0.1, flag_divb=0, flag_ir=4, flag_ir_type=1, t_norm=6500.0,
+                 n_norm=1.0e17, t_ir=1.0e-3)
+    s = s.overrides(**kw)
+    f_n, f_p, f_p_n, f_p_p = fractions(s.n_fraction)
+    if "f_p_p_ini" not in kw:
+        s = s.overrides(f_p_ini=1.0, f_p_p_ini=_fpp_for(s, 0.5 * s.gm * f_p_p / f_p))
+    X, _ = _grid(s)
+    left = X < 0.0
+    ro = np.where(left, 1.0, 0.125)
+    pr = np.where(left, 1.0, 0.1)
+    by = np.where(left, 1.0, -1.0)
+    zero = np.zeros_like(X)
+    bx = np.full_like(X, 0.75)
+    U_h = pv2cq_hd(s, f_n * ro, zero, zero, zero, f_p_n * pr)
+    U_m = pv2cq_mhd(s, f_p * ro, zero, zero, zero, f_p_p * pr, bx, by, zero)
+    nex = lte_nexcite(s, f_n * ro, f_p * ro, f_p_p * pr)
+    return s, U_h, U_m, nex
+
+
+def nlevel_orszag_tang(n: int = 128, **kw):
+    """The two-fluid Orszag-Tang vortex of orszag_tang() with set_IR type 4: T_norm 6500 K,
+    n_norm 1e17 m^-3, tfac such that the uniform initial ion state's electron temperature is
+    T_norm, LTE populations.  Returns (settings, U_h, U_m, Nexcite)."""
+    s0, U_h, U_m = orszag_tang(n, **{k: v for k, v in kw.items()
+                                     if k not in ("flag_ir", "flag_ir_type", "t_norm", "n_norm",
+                                                  "t_ir", "nlev_deriv", "n0fac", "f_p_ini",
+                                                  "f_p_p_ini")})
+    ro_m, pr_m = U_m[0], None
+    f_n, f_p, f_p_n, f_p_p = fractions(s0.n_fraction)
+    pm0 = 5.0 / (12.0 * PI) * f_p_p
+    rm0 = 25.0 / (36.0 * PI) * f_p
+    te_p0 = 0.5 * s0.gm * pm0 / rm0
+    s = s0.overrides(flag_ir=4, flag_ir_type=1, t_norm=6500.0, n_norm=1.0e17, t_ir=1.0e-3)
+    s = s.overrides(**kw)
+    if "f_p_p_ini" not in kw:
+        s = s.overrides(f_p_ini=1.0, f_p_p_ini=_fpp_for(s, te_p0))
+    pr_m = np.full_like(ro_m, pm0)
+    nex = lte_nexcite(s, U_h[0], ro_m, pr_m)
+    return s, U_h, U_m, nex
+
+
 def ensemble_members(n_runs: int = 512, seed: int = 4242):
     """Parameters of the batched ensemble of 1D shock tubes: nx log-uniform in
     [256, 8192], alpha_c log-uniform in [1e-1, 1e4], pressure ratio U[2, 20], density

@@ -21,6 +21,7 @@ PIP_IR_NONE = 0
 PIP_IR_JEFFERY = 1              # set_IR type 1 (PIP_rot.f90:135-149)
 PIP_IR_POPESCU = 2              # set_IR type 2 (PIP_rot.f90:148-170)
 PIP_IR_POPESCU_EQ = 3           # set_IR type 3 (PIP_rot.f90:173-228)
+PIP_IR_NLEVEL = 4               # set_IR type 4, the 6-level hydrogen model (PIP_rot.f90:232-311)
 PIP_IR_POWERLAW = 5
 
 # boundary codes the C ABI accepts (boundary_control types 1, 2 and 10, and the codes
@@ -144,6 +145,15 @@ class Settings:
     vd_cri: float = 0.0         # resi_type 3 threshold on the drift |curl B|/rho_i
     t_norm: float = 0.0         # setting key T_norm (K)
     n_norm: float = 0.0         # setting key n_norm
+    # set_IR type 4: nlevels and flag_rad of setting.txt; the convective derivative of the
+    # excitation update (1 two-point, 4 five-point, 0 none: the reference's s_order 2 leaves
+    # it unset); n0fac, f_p_ini, f_p_p_ini as the initial condition sets them
+    n_levels: int = 5
+    flag_rad: int = 0
+    nlev_deriv: int = 1
+    n0fac: float = 1.0
+    f_p_ini: float = 1.0
+    f_p_p_ini: float = 1.0
     debug_parameter: float = 0.0
     flag_amb: int = 0
     flag_visc: int = 0
@@ -299,16 +309,26 @@ class Settings:
             bad.append("resi_type 3 divides by vd_cri: vd_cri must be > 0")
         if self.flag_amb or self.flag_visc or self.flag_grav:
             bad.append("ambipolar diffusion, viscosity and gravity are not supported")
-        set_ir_laws = (PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ)
+        set_ir_laws = (PIP_IR_JEFFERY, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, PIP_IR_NLEVEL)
         if self.flag_ir not in (PIP_IR_NONE, PIP_IR_POWERLAW) + set_ir_laws:
-            bad.append("flag_ir must be 0, 1, 2, 3 (set_IR types 1-3) or %d" % PIP_IR_POWERLAW)
+            bad.append("flag_ir must be 0, 1, 2, 3, 4 (set_IR types 1-4) or %d" % PIP_IR_POWERLAW)
         elif self.flag_ir in set_ir_laws:
             if not (self.t_norm > 0.0 and self.n_norm > 0.0):
-                bad.append("set_IR types 1-3 need T_norm > 0 and n_norm > 0")
+                bad.append("set_IR types 1-4 need T_norm > 0 and n_norm > 0")
             if self.precision != PIP_FP64:
-                bad.append("set_IR types 1-3 need precision PIP_FP64")
-        if self.flag_ir and self.flag_ir_type not in (1, 2):
-            bad.append("flag_ir_type must be 1 or 2")
+                bad.append("set_IR types 1-4 need precision PIP_FP64")
+        if self.flag_ir == PIP_IR_NLEVEL:
+            if self.n_levels != 5:
+                bad.append("the 6-level model has nlevels = 5")
+            if self.flag_rad not in (0, 1):
+                bad.append("flag_rad >= 2 (radiative rates, get_radrat_fixed) is not built")
+            if self.nlev_deriv not in (0, 1, 4):
+                bad.append("nlev_deriv must be 0, 1 or 4")
+            if self.flag_col % 2 == 0 and not self.beta > 0.0:
+                bad.append("set_IR type 4 with an even flag_col divides by beta")
+        if self.flag_ir and self.flag_ir_type not in (1, 2) and \
+                not (self.flag_ir == PIP_IR_NLEVEL and self.flag_ir_type == 0):
+            bad.append("flag_ir_type must be 1 or 2 (0 with set_IR type 4)")
         for f in range(2 * self.ndim):
             if self.flag_bnd[f] not in SUPPORTED_BND:
                 bad.append("flag_bnd[%d]=%d unsupported" % (f, self.flag_bnd[f]))
@@ -388,7 +408,8 @@ class Settings:
                 "flag_col": "flag_col", "flag_IR": "flag_ir", "flag_IR_type": "flag_ir_type",
                 "flag_heat": "flag_heat", "hc_max": "hc_max", "flag_hll": "flag_hll",
                 "flag_time": "flag_time", "flag_resi": "flag_resi", "flag_amb": "flag_amb",
-                "flag_visc": "flag_visc", "flag_grav": "flag_grav"}
+                "flag_visc": "flag_visc", "flag_grav": "flag_grav", "nlevels": "n_levels",
+                "flag_rad": "flag_rad"}
         reals = {"gm_d": "gm_d", "gm_n": "gm_n", "safety": "safety", "db_clean": "db_clean",
                  "ro_lim": "ro_lim", "pr_lim": "pr_lim", "n_fraction": "n_fraction",
                  "col": "col", "pip_imp_factor": "pip_imp_factor", "t_IR": "t_ir",

@@ -5,6 +5,8 @@ on the device waits for another block), exchanging halos by device copies; the s
 driver over torch.distributed/NCCL moves the same buffers between GPUs.  Checked against
 the single-block run of the same driver (bitwise: the per-cell arithmetic does not depend
 on the split), against pip_run, and against the single-domain oracle."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -165,12 +167,14 @@ def test_device_loop_mixed_matches_pip_run(gpu_lib):
 
 
 @pytest.mark.parametrize("precision", [PIP_FP64, PIP_MIXED])
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 4])
 def test_device_loop_overlapped_exchange_matches_pip_run(gpu_lib, precision, world):
     """The y exchange overlapped with each stage: the first and last tile rows first, the
-    exchange on its own stream while the middle rows compute.  Blocks of 48 or 32 rows hold
-    several tile rows, so both launches of a stage do work; bitwise pip_run's result."""
-    s, Uh, Um = ics.orszag_tang(96, precision=precision)
+    exchange on its own stream while the middle rows compute.  Blocks of 64 or 32 rows hold
+    several tile rows (the mixed kernels' 14-row tiles: 2 with no middle row at 32), so both
+    launches of a stage do work; bitwise pip_run's result (power-of-two splits keep the
+    blocks' grid spacing equal to the single grid's)."""
+    s, Uh, Um = ics.orszag_tang(128, precision=precision)
     st, t, n, hn, mn = device_loop_run(s, Uh, Um, world, 12, overlap=True)
     with capi.Context(s) as c:
         c.upload(Uh, Um)
@@ -180,16 +184,14 @@ def test_device_loop_overlapped_exchange_matches_pip_run(gpu_lib, precision, wor
     assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
 
 
-def test_stage_rows_enforce_their_order(gpu_lib):
+def test_split_stage_enforces_its_order(gpu_lib):
     s, Uh, Um = ics.orszag_tang(32)
     with capi.Context(s) as c:
         c.upload(Uh, Um)
         c.dev_begin(nsteps=2)
         L = capi.lib()
-        assert L.pip_dev_stage_rows(c.h, 1, 2) == capi.PIP_ERR_STATE     # middle rows first
-        assert L.pip_dev_stage_rows(c.h, 2, 1) == capi.PIP_ERR_STATE     # stage 2 before 1
-        assert L.pip_dev_stage_rows(c.h, 1, 1) == capi.PIP_OK
-        assert L.pip_dev_stage(c.h, 2) == capi.PIP_ERR_STATE             # stage 1 unfinished
-        assert L.pip_dev_stage_rows(c.h, 1, 2) == capi.PIP_OK
-        assert L.pip_dev_stage(c.h, 2) == capi.PIP_OK
+        bs = ctypes.c_void_p()
+        assert L.pip_dev_stage_split(c.h, 2, ctypes.byref(bs)) == capi.PIP_ERR_STATE
+        assert L.pip_dev_stage_split(c.h, 1, ctypes.byref(bs)) == capi.PIP_OK and bs.value
+        assert L.pip_dev_stage_split(c.h, 2, ctypes.byref(bs)) == capi.PIP_OK
         c.dev_poll()
