@@ -467,6 +467,7 @@ def measure_ensemble(n_runs=512, t_end=0.1):
         for r, (s, Uh, Um) in enumerate(mem):
             e.upload(r, Uh, Um)
         ms = e.run(t_end=t_end)
+        balance = e.load_balance()
         updates = 0
         bad = 0
         results = []
@@ -486,6 +487,8 @@ def measure_ensemble(n_runs=512, t_end=0.1):
             "value": updates / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
             "cell_updates": updates, "runs_failed": bad, "threads": threads,
             "ctas_per_sm": ctas,
+            "load_balance": {k: (round(v, 4) if isinstance(v, float) else v)
+                             for k, v in balance.items()},
             "vs_fp64_single_runs": {
                 "members_checked": len(errs), "max_rel_l1": max(l1_all),
                 "median_rel_l1": float(statistics.median(l1_all)),

@@ -41,6 +41,13 @@ int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *de
 int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, double *time,
                         int64_t *steps, int *status);
 
+/* Load-balance record of the last launch: for every run, when a thread block took it from
+ * the queue and when it finished, in microseconds of the device's global timer after the
+ * earliest start (-1 for runs no launch has advanced); arrays of n.  slots: the thread
+ * blocks the launch keeps resident (SMs x blocks per SM). */
+int pip_ensemble_timings(pip_ensemble *e, double *start_us, double *end_us);
+int pip_ensemble_slots(pip_ensemble *e, int *slots);
+
 /* Launch configuration: threads per block (128, 256, 512, 1024; not 128 when a run is 2D)
  * and blocks per SM. */
 int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm);

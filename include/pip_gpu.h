@@ -349,6 +349,11 @@ int pip_get_colrat(pip_ctx *ctx, double *colrat);
 int pip_get_ion_pot(pip_ctx *ctx, double *ion_pot);
 int pip_nlevel_gm_rec_ref(pip_ctx *ctx, double *gm_rec_ref);
 
+/* Gm_ion and Gm_rec (ix,jx,kx each) of the last set_IR, for output's "ion" and "rec"
+ * datasets (IO_rot.f90:297-300): contexts that keep the rates between kernels, set_IR types
+ * 1 and 4; PIP_ERR_PARAM for the laws the kernels evaluate in place. */
+int pip_get_ir_rates(pip_ctx *ctx, double *gm_ion, double *gm_rec);
+
 /*
  * Domain decomposition over ranks (one context per rank and device, each holding its own
  * block with ghost cells, as the Fortran code does after set_mpi, MPI_rot.f90:11-41).

@@ -39,12 +39,13 @@ EXPORTS = (
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
     "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
     "pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
-    "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref",
+    "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref", "pip_get_ir_rates",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
     "pip_ensemble_create", "pip_ensemble_destroy", "pip_ensemble_upload", "pip_ensemble_run",
     "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
+    "pip_ensemble_timings", "pip_ensemble_slots",
     # include/pip_adjoint.h
     "pip_adj_create", "pip_adj_destroy", "pip_adj_set_col", "pip_adj_forward",
     "pip_adj_backward", "pip_adj_dt", "pip_adj_stage_vjp", "pip_adj_fold",
@@ -122,8 +123,10 @@ def lib(path: Optional[str] = None):
     L.pip_get_colrat.argtypes = [vp, dp]
     L.pip_get_ion_pot.argtypes = [vp, dp]
     L.pip_nlevel_gm_rec_ref.argtypes = [vp, dp]
+    L.pip_get_ir_rates.argtypes = [vp, dp, dp]
     for name in ("pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
-                 "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref"):
+                 "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref",
+                 "pip_get_ir_rates"):
         getattr(L, name).restype = i
     L.pip_last_cuda_error.argtypes = []
     L.pip_strerror.argtypes = [i]
@@ -143,6 +146,8 @@ def lib(path: Optional[str] = None):
     L.pip_ensemble_member.argtypes = [vp, i, dp, dp, dp, P(ctypes.c_int64), P(i)]
     L.pip_ensemble_set_config.argtypes = [vp, i, i]
     L.pip_ensemble_tune.argtypes = [vp, d, P(i), P(i), P(ctypes.c_float)]
+    L.pip_ensemble_timings.argtypes = [vp, dp, dp]
+    L.pip_ensemble_slots.argtypes = [vp, P(i)]
     L.pip_adj_create.argtypes = [P(PipParams), ctypes.c_int64, i, P(vp)]
     L.pip_adj_destroy.argtypes = [vp]
     L.pip_adj_destroy.restype = None
@@ -153,7 +158,8 @@ def lib(path: Optional[str] = None):
     L.pip_adj_stage_vjp.argtypes = [vp, i, vp, vp, vp, d, dp, dp]
     L.pip_adj_fold.argtypes = [vp, vp]
     for name in ("pip_ensemble_create", "pip_ensemble_upload", "pip_ensemble_run",
-                 "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune"):
+                 "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
+                 "pip_ensemble_timings", "pip_ensemble_slots"):
         getattr(L, name).restype = i
     L.pip_kernels_per_run.restype = ctypes.c_int64
     for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",
@@ -424,15 +430,22 @@ class Context:
         return stop.value, nan.value
 
     # ---- set_IR type 4 (the 6-level hydrogen model)
-    def set_nlevel(self, table: np.ndarray, deriv: int = 1, n0fac: float = 1.0,
-                   f_p_ini: float = 1.0, f_p_p_ini: float = 1.0, n_levels: int = 5,
-                   flag_rad: int = 0) -> None:
-        """The exponential-integral table (rows yn, E0, E1, E2) and the model's settings."""
+    def set_nlevel(self, table: np.ndarray, **override) -> None:
+        """The exponential-integral table (rows yn, E0, E1, E2) and the model's settings:
+        n_levels, flag_rad, deriv (the settings' nlev_deriv), n0fac, f_p_ini, f_p_p_ini from
+        the context's Settings unless given."""
         t = np.ascontiguousarray(table, dtype=np.float64)
         if t.ndim != 2 or t.shape[1] != 4:
             raise ValueError("the table has rows of 4 values (yn, E0, E1, E2)")
-        cfg = PipNlevel(int(n_levels), int(flag_rad), int(deriv), 0, float(n0fac),
-                        float(f_p_ini), float(f_p_p_ini))
+        s = self.s
+        v = dict(n_levels=s.n_levels, flag_rad=s.flag_rad, deriv=s.nlev_deriv, n0fac=s.n0fac,
+                 f_p_ini=s.f_p_ini, f_p_p_ini=s.f_p_p_ini)
+        unknown = set(override) - set(v)
+        if unknown:
+            raise TypeError("unknown settings %s" % sorted(unknown))
+        v.update(override)
+        cfg = PipNlevel(int(v["n_levels"]), int(v["flag_rad"]), int(v["deriv"]), 0,
+                        float(v["n0fac"]), float(v["f_p_ini"]), float(v["f_p_p_ini"]))
         _check(lib().pip_set_nlevel(self.h, ctypes.byref(cfg), _ptr(t), t.shape[0]),
                "pip_set_nlevel")
 
@@ -456,6 +469,13 @@ class Context:
         a = np.empty(self.shape_h[1:])
         _check(lib().pip_get_ion_pot(self.h, _ptr(a)), "pip_get_ion_pot")
         return a
+
+    def ir_rates(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(Gm_ion, Gm_rec) of the last set_IR, each shaped like one plane (set_IR types 1, 4)."""
+        ion = np.empty(self.shape_h[1:])
+        rec = np.empty(self.shape_h[1:])
+        _check(lib().pip_get_ir_rates(self.h, _ptr(ion), _ptr(rec)), "pip_get_ir_rates")
+        return ion, rec
 
     def gm_rec_ref(self) -> float:
         v = ctypes.c_double()

@@ -216,7 +216,6 @@ void ir_law_constants(const pip_params &p, KParams &k) {
     k.nl_odd = p.flag_col % 2 == 1 ? 1 : 0;
     k.nl_en_even = p.beta / p.t_norm / 2.0 / (double)8.6173e-5f;
     k.nl_lim = std::min(p.safety, 0.01);
-    k.nl_gref = 1.0;
     return;
   }
   if (k.irf) {
@@ -887,6 +886,13 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   }
   // cfl of the first step (main.f90:36); later steps get it fused into stage 2
   CK(do_cfl(c, 0));
+  bool halted = false;
+  if (c->kp.irn) {
+    // a negative rate of the 6-level model stops the run before the step, as
+    // get_col_ion_coeff stops the program inside set_IR
+    if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+    halted = h.status != 0;
+  }
   if (c->hc || c->kp.resi == 2 || c->kp.irn) {
     // conduction runs: the stages, post_step's conduction and the ghost fill, then the two
     // cfl calls (rewrite; rewrite + next dt) as separate kernels; the host loop waits on
@@ -897,7 +903,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
     // stages and the cfl calls.
     long long n = 0;
     int total_it = 0;
-    for (;;) {
+    while (!halted) {
       CK(do_stage(c, 1, 1, 0));
       CK(do_stage(c, 2, 1, 0));
       if (c->hc) {
@@ -912,6 +918,10 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
       if (h.done) break;
       CK(do_cfl(c, (int)((n + 1) & 1)));    // the next step's cfl (main.f90:36)
       ++n;
+      if (c->kp.irn) {
+        if (sync_ctrl_to_host(c)) return PIP_ERR_CUDA;
+        if (h.status) break;
+      }
     }
     c->hc_iters = total_it;
     if (device_ms) {
@@ -955,6 +965,7 @@ static int run_loop(pip_ctx *c, int64_t nsteps, double t_end, double *time_out,
   c->cmax = h.cmax;
   if (time_out) *time_out = h.time;
   if (steps_done) *steps_done = h.step;
+  if (h.status == PIP_ERR_RATE) return PIP_ERR_RATE;
   if (h.nan_flag) return PIP_ERR_NAN;
   if (h.status) return h.status;
   return PIP_OK;
@@ -1486,6 +1497,16 @@ int pip_get_ion_pot(pip_ctx *c, double *ion_pot) {
   if (!c->kp.irn) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(cudaMemcpyAsync(ion_pot, c->nl_ip, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIP_OK;
+}
+
+int pip_get_ir_rates(pip_ctx *c, double *gm_ion, double *gm_rec) {
+  if (!c || !gm_ion || !gm_rec) return PIP_ERR_NULL;
+  if (!c->irg) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(cudaMemcpyAsync(gm_ion, c->irg, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(gm_rec, c->irg + c->kp.nc, c->plane_bytes(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PIP_OK;
 }

@@ -45,7 +45,15 @@ struct RunState {
   long long steps;
   int status;         // 0, PIP_ERR_NAN (3) or PIP_ERR_DT (4)
   int pad;
+  unsigned long long t_start, t_end;  // device global timer (ns) when the last launch that
+                                      // advanced the run took it from the queue and left it
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ double finalize_dt(const KParams &p, double red_dt, double red_rho,
                                               double red_gr) {
@@ -341,6 +349,15 @@ __device__ void run_member_2d(const KParams &p, float *Ahi, float *Alo, float *B
   }
   block_minmax<NT>(dtc, rhoc, grc, s_red);
   double dt = finalize_dt(p, dtc, rhoc, grc);
+  // the prologue's PIPbnd after its cfl (Initial_rot.f90:152-159): ghost images of the
+  // rewritten interior, as the single run's pip_fill_ghosts (a no-op on ghosts that already
+  // hold them)
+  __syncthreads();
+  for (long long t = tid; t < (long long)p.nx * p.ny; t += NT) {
+    const int gi = p.m0 + (int)(t % p.nx), gj = p.m1 + (int)(t / p.nx);
+    if (mixed::near_boundary<2>(p, gi, gj)) mixed::write_ghosts<2>(p, gi, gj, Ahi, Alo, NV2);
+  }
+  __syncthreads();
   const int ntx = (p.nx + TX2 - 1) / TX2, nty = (p.ny + TY2 - 1) / TY2, ntiles = ntx * nty;
   bool bad = false;
   for (;;) {
@@ -413,12 +430,14 @@ __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const K
       __syncthreads();
       continue;
     }
+    rs.t_start = global_ns();
     if (HAS2D && p.ndim == 2) {
       // (the host allows 2D members only with NT >= TX2 * TY2 threads)
       if (NT >= TX2 * TY2) {
         if (p.nvm == 9) run_member_2d<NT, 9>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
         else run_member_2d<NT, 8>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
       }
+      rs.t_end = global_ns();
       if (tid == 0) st[r] = rs;
       __syncthreads();
       continue;
@@ -465,6 +484,11 @@ __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const K
     }
     block_minmax<NT>(dtc, rhoc, grc, s_red);
     double dt = finalize_dt(p, dtc, rhoc, grc);
+    // the prologue's PIPbnd after its cfl (Initial_rot.f90:152-159)
+    __syncthreads();
+    for (int i = p.m0 + tid; i < p.ix - p.m0; i += NT)
+      if (mixed::near_boundary<1>(p, i, 0)) mixed::write_ghosts<1>(p, i, 0, Ahi, Alo, NVM + 5);
+    __syncthreads();
     int bad = 0;
     // the time loop (main.f90:31-68) of this run
     for (;;) {
@@ -490,6 +514,7 @@ __global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const K
       block_minmax<NT>(d2, r2, g2, s_red);
       dt = finalize_dt(p, d2, r2, g2);
     }
+    rs.t_end = global_ns();
     if (tid == 0) st[r] = rs;
     __syncthreads();
   }
@@ -759,6 +784,29 @@ int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, d
   if (time) *time = rs.time;
   if (steps) *steps = rs.steps;
   if (status) *status = rs.status;
+  return PIP_OK;
+}
+
+int pip_ensemble_timings(pip_ensemble *e, double *start_us, double *end_us) {
+  if (!e || !start_us || !end_us) return PIP_ERR_NULL;
+  EK(cudaSetDevice(e->device));
+  std::vector<RunState> all((size_t)e->n);
+  EK(cudaMemcpyAsync(all.data(), e->d_st, sizeof(RunState) * e->n, cudaMemcpyDeviceToHost, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  unsigned long long t0 = ~0ull;
+  for (const RunState &r : all)
+    if (r.t_end != 0 && r.t_start < t0) t0 = r.t_start;
+  for (int m = 0; m < e->n; ++m) {
+    const RunState &r = all[(size_t)m];
+    start_us[m] = r.t_end == 0 ? -1.0 : 1.0e-3 * (double)(r.t_start - t0);
+    end_us[m] = r.t_end == 0 ? -1.0 : 1.0e-3 * (double)(r.t_end - t0);
+  }
+  return PIP_OK;
+}
+
+int pip_ensemble_slots(pip_ensemble *e, int *slots) {
+  if (!e || !slots) return PIP_ERR_NULL;
+  *slots = e->sms * e->ctas_per_sm;
   return PIP_OK;
 }
 

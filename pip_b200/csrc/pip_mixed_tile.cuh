@@ -80,30 +80,28 @@ __device__ __forceinline__ void tile_stage(const KParams &p, const float *__rest
 
   // ---- 2. FP32 face fluxes
   const int iend = p.m0 + p.nx, jend = NDIM == 2 ? p.m1 + p.ny : 1;
-  for (int slot = tid; slot < NFX + NFY; slot += NT) {
-    const int xdir = slot < NFX;
-    const int g = xdir ? slot : slot - NFX, w = xdir ? TX + 1 : TX;
-    const int fi = g % w, fj = g / w;
-    int a, s, py, fo, nf, f;
+  for (int f = tid; f < NFX + NFY; f += NT) {
+    // x faces first, then y faces, each in row order (constant divisors in each branch)
+    int a, s, py, fo, nf;
     float *Fout;
-    if (xdir) {
+    if (f < NFX) {
+      const int fi = f % (TX + 1), fj = f / (TX + 1);
       if (i0 + fi - 1 >= iend || (NDIM == 2 && j0 + fj >= jend)) continue;
       a = (NDIM == 2 ? (fj + kH) * RX : 0) + fi + kH - 1;
       s = 1;
       py = 0;
       Fout = sFx;
-      fo = fj * (TX + 1) + fi;
+      fo = f;
       nf = NFX;
-      f = fo;
     } else {
+      const int g = f - NFX, fi = g % TX, fj = g / TX;
       if (i0 + fi >= iend || j0 + fj - 1 >= jend) continue;
       a = (fj + kH - 1) * RX + fi + kH;
       s = RX;
       py = 1;
       Fout = sFy;
-      fo = fj * TX + fi;
+      fo = g;
       nf = NFY;
-      f = NFX + fo;
     }
     {
       // the HLLD of planes 0-7; with Dedner cleaning the normal-field and psi fluxes are the

@@ -82,6 +82,28 @@ class Ensemble:
         capi._check(capi.lib().pip_ensemble_set_config(self.h, int(threads), int(ctas_per_sm)),
                     "pip_ensemble_set_config")
 
+    def load_balance(self) -> dict:
+        """Makespan of the last launch against perfect balance: each run's busy span (device
+        timer) from pip_ensemble_timings; busy fraction = sum of spans / (slots x makespan);
+        the longest run bounds the makespan from below however the queue is ordered."""
+        n = len(self.shapes)
+        t0, t1 = np.empty(n), np.empty(n)
+        capi._check(capi.lib().pip_ensemble_timings(self.h, capi._ptr(t0), capi._ptr(t1)),
+                    "pip_ensemble_timings")
+        slots = ctypes.c_int()
+        capi._check(capi.lib().pip_ensemble_slots(self.h, ctypes.byref(slots)), "pip_ensemble_slots")
+        ran = t1 >= 0
+        span = (t1 - t0)[ran]
+        makespan = float(t1[ran].max() - t0[ran].min())
+        busy = float(span.sum())
+        ideal = max(busy / slots.value, float(span.max()))
+        return {"makespan_us": makespan, "busy_us": busy, "slots": slots.value,
+                "busy_fraction": busy / (slots.value * makespan),
+                "longest_run_us": float(span.max()),
+                "ideal_makespan_us": ideal,
+                "makespan_over_ideal": makespan / ideal,
+                "makespan_over_even_split": makespan / (busy / slots.value)}
+
     def tune(self, t_probe: float) -> Tuple[int, int, float]:
         """Autotune (threads per block, blocks per SM) on a probe run; returns the choice."""
         th, cp, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()

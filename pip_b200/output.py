@@ -34,7 +34,8 @@ from typing import Dict, Optional, Sequence, Tuple
 
 import numpy as np
 
-from .params import PIP_IR_JEFFERY, PIP_IR_NONE, PIP_IR_POPESCU, PIP_IR_POPESCU_EQ, Settings
+from .params import (PIP_IR_JEFFERY, PIP_IR_NLEVEL, PIP_IR_NONE, PIP_IR_POPESCU,
+                     PIP_IR_POPESCU_EQ, Settings)
 
 VAR_M = ("ro_p", "mx_p", "my_p", "mz_p", "en_p", "bx", "by", "bz", "ps")
 VAR_H = ("ro_n", "mx_n", "my_n", "mz_n", "en_n")
@@ -53,6 +54,13 @@ def variables(s: Settings) -> Tuple[str, ...]:
     names += list(VAR_M[: s.nvar_m])
     if s.flag_ir != PIP_IR_NONE:
         names += ["ion", "rec"]
+    if s.flag_ir == PIP_IR_NLEVEL:
+        # the 6-level model's populations and rates (IO_rot.f90:301-310)
+        for i in range(1, 7):
+            names.append("nexcite%d" % i)
+            names += ["colrat%d%d" % (i, j) for j in range(1, 7)]
+        if s.flag_ir_type == 0:
+            names.append("ion_loss")
     return tuple(names) + VAR_H
 
 
@@ -139,7 +147,7 @@ def _create(stem: str, s: Settings, global_shape, time: float, grid) -> Dict[str
 
 
 def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np.ndarray],
-                  eta: Optional[np.ndarray] = None):
+                  eta: Optional[np.ndarray] = None, nlevel: Optional[Dict[str, np.ndarray]] = None):
     planes = {}
     if s.flag_col >= 2:
         if ac is None:
@@ -152,7 +160,21 @@ def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np
             eta = s.eta_field(U_m if s.resi_type in (2, 3) else None)
         planes["et"] = np.asarray(eta).reshape(U_h.shape[1:])
     planes.update({VAR_M[n]: U_m[n] for n in range(s.nvar_m)})
-    if s.flag_ir != PIP_IR_NONE:
+    if s.flag_ir == PIP_IR_NLEVEL:
+        if nlevel is None:
+            raise ValueError("set_IR type 4 writes its populations and rates: pass nlevel")
+        shp = U_h.shape[1:]
+        planes["ion"] = np.asarray(nlevel["ion"]).reshape(shp)
+        planes["rec"] = np.asarray(nlevel["rec"]).reshape(shp)
+        nx = np.asarray(nlevel["nexcite"]).reshape((6,) + shp)
+        cr = np.asarray(nlevel["colrat"]).reshape((6, 6) + shp)
+        for i in range(6):
+            planes["nexcite%d" % (i + 1)] = nx[i]
+            for j in range(6):
+                planes["colrat%d%d" % (i + 1, j + 1)] = cr[i, j]
+        if s.flag_ir_type == 0:
+            planes["ion_loss"] = np.asarray(nlevel["ion_loss"]).reshape(shp)
+    elif s.flag_ir != PIP_IR_NONE:
         planes["ion"], planes["rec"] = ir_rates(s, U_m)
     for n, name in enumerate(VAR_H):
         planes[name] = U_h[n]
@@ -161,16 +183,18 @@ def _state_planes(s: Settings, U_h: np.ndarray, U_m: np.ndarray, ac: Optional[np
 
 def write_output(outdir: str, nout: int, s: Settings, time: float, U_h: np.ndarray,
                  U_m: np.ndarray, ac: Optional[np.ndarray] = None,
-                 eta: Optional[np.ndarray] = None) -> str:
+                 eta: Optional[np.ndarray] = None,
+                 nlevel: Optional[Dict[str, np.ndarray]] = None) -> str:
     """output() of a whole state (global arrays with ghosts, layout (planes, jx, ix)); ac is
     the alpha_c field (pip_get_alpha_c), needed with flag_col 2..7; eta the resistivity
-    field (default: the settings' set_resistivity field)."""
+    field (default: the settings' set_resistivity field); nlevel, with set_IR type 4, the
+    arrays of nlevel_planes (the rates, Nexcite, colrat, ion_pot)."""
     os.makedirs(outdir, exist_ok=True)
     stem = file_stem(outdir, nout)
     x, y, z, dx, dy, dz = s.coordinates()
     where = _create(stem, s, s.shape, time, (x, y, z, dx, dy, dz))
     mm = np.memmap(stem + ".bin", dtype=np.uint8, mode="r+")
-    for name, plane in _state_planes(s, U_h, U_m, ac, eta).items():
+    for name, plane in _state_planes(s, U_h, U_m, ac, eta, nlevel).items():
         off, dims = where[name]
         raw = np.ascontiguousarray(plane, dtype="<f8").view(np.uint8).reshape(-1)
         mm[off: off + raw.size] = raw
@@ -316,6 +340,30 @@ def restart_resistivity(outdir: str, nout: int, s: Settings) -> Optional[np.ndar
     return np.ascontiguousarray(d["et"][0].reshape(jx, ix))
 
 
+def nlevel_planes(ctx, s: Settings) -> Optional[Dict[str, np.ndarray]]:
+    """The 6-level model's output arrays from a context (set_IR type 4): the rates of the last
+    set_IR, Nexcite, colrat and ion_pot; None for the other laws."""
+    if s.flag_ir != PIP_IR_NLEVEL:
+        return None
+    ion, rec = ctx.ir_rates()
+    out = dict(ion=ion, rec=rec, nexcite=ctx.nexcite(), colrat=ctx.colrat())
+    if s.flag_ir_type == 0:
+        out["ion_loss"] = ctx.ion_pot()
+    return out
+
+
+def restart_nexcite(outdir: str, nout: int, s: Settings) -> Optional[np.ndarray]:
+    """Nexcite (6, jx, ix) of output nout, for pip_set_nexcite (set_IR type 4); None for the
+    other laws.  The reference's restart does not read the populations back
+    (reread_variables, IO_rot.f90:574-581); this completes it."""
+    if s.flag_ir != PIP_IR_NLEVEL:
+        return None
+    d = read_output(file_stem(outdir, nout))
+    ix, jx, _ = s.shape
+    return np.ascontiguousarray(np.stack([d["nexcite%d" % i][0].reshape(jx, ix)
+                                          for i in range(1, 7)]))
+
+
 def restart_alpha_c(outdir: str, nout: int, s: Settings) -> Optional[np.ndarray]:
     """The alpha_c field of output nout (jx, ix) that restart reads with flag_col 2..7
     (IO_rot.f90:570-572), for pip_set_alpha_c; None for a constant alpha_c."""
@@ -337,14 +385,14 @@ def run_with_output(ctx, s: Settings, outdir: str, dtout: float, tend: float,
     nout = nout0
     field = (lambda: ctx.alpha_c()) if s.flag_col >= 2 else (lambda: None)
     U_h, U_m = ctx.download()
-    write_output(outdir, nout, s, ctx.time, U_h, U_m, field())
+    write_output(outdir, nout, s, ctx.time, U_h, U_m, field(), nlevel=nlevel_planes(ctx, s))
     st = 0
     while ctx.time < tend:
         nxt = min((nout + 1) * dtout, tend)
         st, t, n = ctx.run(t_end=nxt)
         U_h, U_m = ctx.download()
         nout += 1
-        write_output(outdir, nout, s, t, U_h, U_m, field())
+        write_output(outdir, nout, s, t, U_h, U_m, field(), nlevel=nlevel_planes(ctx, s))
         if st != 0:
             break
     return st, nout, ctx.time

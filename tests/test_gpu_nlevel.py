@@ -31,8 +31,7 @@ def table(n=100000):
 
 def setup_gpu(c, s, Uh, Um, nex, tab):
     c.upload(Uh, Um)
-    c.set_nlevel(tab, deriv=s.nlev_deriv, n0fac=s.n0fac, f_p_ini=s.f_p_ini,
-                 f_p_p_ini=s.f_p_p_ini)
+    c.set_nlevel(tab)          # the settings' n_levels, deriv, n0fac, f_p_ini, f_p_p_ini
     c.set_nexcite(nex)
 
 
@@ -140,7 +139,7 @@ def test_single_calls_against_oracle():
 
 def test_api_rules():
     s, Uh, Um, nex = ics.nlevel_tube(64)
-    tab = table(2000)
+    tab = table()
     with capi.Context(s) as c:
         c.upload(Uh, Um)
         with pytest.raises(capi.PipError) as e:
@@ -181,7 +180,7 @@ def test_negative_rate_stops_the_run():
             c.prologue()
         assert e.value.code == capi.PIP_ERR_RATE
         st, t, n = c.run(3, check=False)
-        assert st == capi.PIP_ERR_RATE
+        assert st == capi.PIP_ERR_RATE and n == 0     # stopped before the first step
     # the device stays usable
     s, Uh, Um, nex = ics.nlevel_tube(64)
     with capi.Context(s) as c:
@@ -189,3 +188,23 @@ def test_negative_rate_stops_the_run():
         c.prologue()
         assert c.run(3)[0] == 0
     torch.cuda.synchronize()
+
+
+def test_output_datasets(tmp_path):
+    from pip_b200 import output
+    s, Uh, Um, nex = ics.nlevel_tube(128, flag_ir_type=0, fp_exact=1)
+    with capi.Context(s) as c:
+        setup_gpu(c, s, Uh, Um, nex, table())
+        c.prologue()
+        st, last, t = output.run_with_output(c, s, str(tmp_path), dtout=0.002, tend=0.004)
+        assert st == 0 and last == 2
+        ion, rec = c.ir_rates()
+        nx, cr, ip = c.nexcite(), c.colrat(), c.ion_pot()
+        gh, gm = c.download()
+    d = output.read_output(output.file_stem(str(tmp_path), 2))
+    assert d["time"] == t
+    assert np.array_equal(d["ion"][0], ion) and np.array_equal(d["rec"][0], rec)
+    assert np.array_equal(d["ion_loss"][0], ip)
+    assert np.array_equal(d["nexcite3"][0], nx[2]) and np.array_equal(d["colrat52"][0], cr[4, 1])
+    assert np.array_equal(output.restart_nexcite(str(tmp_path), 2, s), nx)
+    assert np.array_equal(d["ro_n"][0], gh[0])

@@ -200,3 +200,24 @@ def test_settings():
         Settings(flag_ir=2, flag_ir_type=0, t_norm=1e4, n_norm=1e16).validate()
     t = Settings.from_setting_text("5 :nlevels;\n1 :flag_rad;\n4 :flag_IR;\n0 :flag_IR_type;\n")
     assert (t.n_levels, t.flag_rad, t.flag_ir, t.flag_ir_type) == (5, 1, 4, 0)
+
+
+def test_output_layout(tmp_path):
+    from pip_b200 import output
+    s, Uh, Um, nex = _tube(flag_ir_type=0)
+    names = output.variables(s)
+    i = names.index("rec")
+    assert names[i + 1: i + 8] == ("nexcite1", "colrat11", "colrat12", "colrat13", "colrat14",
+                                   "colrat15", "colrat16")
+    assert names[i + 1 + 6 * 7] == "ion_loss" and names[-5:] == output.VAR_H
+    rng = np.random.default_rng(3)
+    shp = Uh.shape[1:]
+    nl = dict(ion=rng.random(shp), rec=rng.random(shp), nexcite=nex,
+              colrat=rng.random((6, 6) + shp), ion_loss=rng.random(shp))
+    output.write_output(str(tmp_path), 2, s, 0.5, Uh, Um, nlevel=nl)
+    d = output.read_output(output.file_stem(str(tmp_path), 2))
+    assert np.array_equal(d["colrat34"][0], nl["colrat"][2, 3])
+    assert np.array_equal(d["ion_loss"][0], nl["ion_loss"])
+    assert np.array_equal(output.restart_nexcite(str(tmp_path), 2, s), nex)
+    with pytest.raises(ValueError):
+        output.write_output(str(tmp_path), 3, s, 0.5, Uh, Um)
