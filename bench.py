@@ -42,6 +42,9 @@ alpha_c = 1e3, Dedner cleaning, CFL 0.3) with synthetic initial data.
   recomputed at every RK stage), with flag_resi=1, eta_0=1e-4 (resistive_flux on every
   face; margin 3), and with flag_ir=3 (set_IR type 3, the Popescu rates at every stage),
   500 steps each, and their cost over the plain FP64 step.
+* nlevel_hydrogen: the FP64 OT step with set_IR type 4 (the 6-level hydrogen model with the
+  ionisation-potential energy term), 200 steps on the host loop, and its cost over the plain
+  FP64 step.
 """
 from __future__ import annotations
 
@@ -409,6 +412,32 @@ def measure_variant(n, steps, ms_plain, what, **overrides):
             "gpu_launches": launches}
 
 
+def measure_nlevel(n, steps, ms_plain):
+    """The OT n x n FP64 step with set_IR type 4 (the 6-level hydrogen model: rates before
+    every stage and cfl, excitation update after every stage, the cfl terms), stepped by the
+    host loop, against the plain FP64 step."""
+    import torch
+    from pip_b200 import capi, ics
+    s, Uh, Um, nex = ics.nlevel_orszag_tang(n, flag_ir_type=0, t_ir=1.0, nlev_deriv=1)
+    tab = capi.colexp_table(100000)
+    ctx = capi.Context(s)
+    ctx.upload(Uh, Um)
+    ctx.set_nlevel(tab)
+    ctx.set_nexcite(nex)
+    ctx.prologue()
+    ctx.run(nsteps=3)
+    torch.cuda.synchronize()
+    st, t, nstep, ms = ctx.run_timed(nsteps=steps)
+    ctx.close()
+    if st != 0 or nstep != steps:
+        raise RuntimeError("6-level run ended with status %d after %d steps" % (st, nstep))
+    return {"workload": "OT %dx%d FP64, set_IR type 4 (6-level hydrogen, flag_IR_type 0)" % (n, n),
+            "steps": steps, "ms_per_step": ms / steps, "value": n * n * steps / (ms * 1e-3),
+            "unit": UNIT, "over_plain_fp64": (ms / steps) / ms_plain,
+            # per step: 2 x (rates, stage, excitation update) + 2 x (rates, cfl, cfl terms)
+            "gpu_launches": 12 * steps}
+
+
 def measure_adjoint(nsteps=500, K=25):
     """C5: two-fluid linear wave damping 512x256, alpha_c = 10, loss = L2 misfit of the final
     ion vy and neutral density against a forward run with alpha_c = 20 from another seed."""
@@ -691,7 +720,7 @@ def main():
     adjoint = None if args.no_adjoint else measure_adjoint()
     ensemble = None if args.no_ensemble else measure_ensemble()
     conduction = None if args.no_conduction else measure_conduction()
-    alpha_c = resistivity = ionisation = None
+    alpha_c = resistivity = ionisation = nlevel = None
     if not args.no_extra_physics:
         def variant(what, **kw):
             # a failure here must not cost the headline line
@@ -705,6 +734,10 @@ def main():
         ionisation = variant("flag_ir=3 (set_IR type 3 at every stage), T_norm=1.5e4, "
                              "n_norm=1e11, t_IR=10", flag_ir=3, t_norm=1.5e4, n_norm=1.0e11,
                              t_ir=10.0)
+        try:
+            nlevel = measure_nlevel(n, 200, ms64 / args.steps)
+        except Exception as e:  # noqa: BLE001
+            nlevel = {"workload": "set_IR type 4", "error": str(e)}
     whole.__exit__()
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -763,6 +796,7 @@ def main():
         "alpha_c_per_cell": alpha_c,
         "resistivity": resistivity,
         "ionisation_recombination": ionisation,
+        "nlevel_hydrogen": nlevel,
         "e2e": e2e,
         "gpu_launches": mix["launches"],
         "clocks": whole.summary(),

@@ -299,6 +299,41 @@ int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
 int pip_set_hc_wait_limit(pip_ctx *ctx, int polls);
 
 /*
+ * Implicit conduction of a decomposed run: BiCGstabMPI (HC_rot.f90:303-466) for a block
+ * whose y faces border other ranks (pip_set_neighbors; x faces stay physical), driven by
+ * the caller as the reference's loop with its MPI calls in between.  After stage 2 and its
+ * halo exchange (ghost rows hold the neighbours' rows, so te and the matrix next to an
+ * exchanged face are the undecomposed ones):
+ *   pip_hcd_begin(ctx, dt, s)          te, the matrix (folded on physical faces only),
+ *                                      r = b - A te; s = local (r,r), (b,b); SUM over ranks
+ *   exchange vector 1 (r), then pip_hcd_phase(ctx, 0, 0, 0)            p = r
+ *   while sqrt(R/B) > hc_error and count <= hc_max:
+ *     pip_hcd_phase(ctx, 1, 0, s)      Ap = A p; s = (r,r0), (r0,Ap); SUM; alpha = S0/S1;
+ *                                      exchange vector 2 (Ap)
+ *     pip_hcd_phase(ctx, 2, {alpha}, s) t = r - alpha Ap, At; s = (t,At), (At,At); SUM;
+ *                                      omega = S0/S1
+ *     pip_hcd_phase(ctx, 3, {alpha, omega}, 0)   x = x + alpha p + omega t
+ *     pip_hcd_phase(ctx, 4, 0, s)      r = b - A x; s = (r0,r), (r,r); SUM;
+ *                                      beta = S0/(alpha's S0)*alpha/omega, R = S1;
+ *                                      exchange vector 1 (r)
+ *     pip_hcd_phase(ctx, 5, {beta, omega}, 0)    p = r + beta (p - omega Ap); count += 1
+ *   pip_hcd_end(ctx, count)            te back into the ion energy (interior cells), ghosts
+ *                                      of the physical faces; then the state's exchange
+ * A vector exchange moves one row per face: pip_hcd_pack(ctx, vec, f, send) copies the row
+ * the rank across face f (2 = y-, 3 = y+) needs into the device buffer send
+ * (pip_hcd_row_bytes), pip_hcd_unpack(ctx, vec, f, recv) stores the row received from it.
+ * Every scalar is the global one; the reference takes omega from the rank's own sums
+ * (HC_rot.f90:425-427), which makes its iterates depend on the decomposition.  FP64 vectors
+ * for either precision form.  PIP_ERR_PARAM without flag_heat = 1.
+ */
+int pip_hcd_begin(pip_ctx *ctx, double dt, double sums[2]);
+int pip_hcd_phase(pip_ctx *ctx, int phase, const double coef[2], double sums[2]);
+int64_t pip_hcd_row_bytes(pip_ctx *ctx);
+int pip_hcd_pack(pip_ctx *ctx, int vec, int face, void *send);
+int pip_hcd_unpack(pip_ctx *ctx, int vec, int face, const void *recv);
+int pip_hcd_end(pip_ctx *ctx, int iters);
+
+/*
  * set_IR type 4 (flag_ir = PIP_IR_NLEVEL): the 6-level hydrogen model.
  *
  * The Fortran keeps the model's state in globalvar (Nexcite, colrat, ion_pot, Gm_rec_ref)
@@ -365,7 +400,8 @@ int pip_get_ir_rates(pip_ctx *ctx, double *gm_ion, double *gm_rec);
  * pip_fill_ghosts apply flag_bnd to the other faces, as MHDbnd/HDbnd skip faces whose
  * neighbor is not -1 (Boundary_rot.f90:80-90).  With a neighbour on any face, pip_step and
  * pip_run return PIP_ERR_STATE (the exchange must come between the stages: step with
- * pip_stage), and implicit conduction (flag_heat = 1) is not supported (PIP_ERR_PARAM).
+ * pip_stage); with flag_heat = 1 the split is along y and pip_stage(ctx, 2, ...) leaves the
+ * conduction to the pip_hcd_* calls (above).
  *
  * pip_stage runs one RK stage of run_solver (Solver_rot.f90:59-71) with the given dt and
  * Dedner speed cmax: stage 1 then stage 2, each followed by PIPbnd's exchange

@@ -84,6 +84,14 @@ def lib():
         L.orc_gm_rec_ref.restype = d
         L.orc_nlevel_status.argtypes = [vp]
         L.orc_nlevel_status.restype = ctypes.c_int
+        L.orc_hcd_begin.argtypes = [vp, d, dp]
+        L.orc_hcd_begin.restype = ctypes.c_int
+        L.orc_hcd_phase.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.orc_hcd_phase.restype = ctypes.c_int
+        L.orc_hcd_get_row.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.orc_hcd_set_row.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.orc_hcd_end.argtypes = [vp]
+        L.orc_hcd_end.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -240,6 +248,31 @@ class Oracle:
 
     def has_nan(self) -> bool:
         return bool(lib().orc_has_nan(self.h))
+
+    # ---- BiCGstabMPI in phases (orc_hcd_*): vector 0 x, 1 r, 2 Ap
+    def hcd_begin(self, dt: float):
+        s = (ctypes.c_double * 2)()
+        lib().orc_hcd_begin(self.h, float(dt), s)
+        return s[0], s[1]
+
+    def hcd_phase(self, phase: int, c0: float = 0.0, c1: float = 0.0):
+        coef = (ctypes.c_double * 2)(float(c0), float(c1))
+        s = (ctypes.c_double * 2)()
+        if lib().orc_hcd_phase(self.h, int(phase), coef, s):
+            raise ValueError("phase %d" % phase)
+        return s[0], s[1]
+
+    def hcd_get_row(self, vec: int, row: int) -> np.ndarray:
+        out = np.empty(self.shape_h[2])
+        lib().orc_hcd_get_row(self.h, int(vec), int(row), _ptr(out))
+        return out
+
+    def hcd_set_row(self, vec: int, row: int, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        lib().orc_hcd_set_row(self.h, int(vec), int(row), _ptr(v))
+
+    def hcd_end(self) -> None:
+        lib().orc_hcd_end(self.h)
 
     # ---- set_IR type 4 (the 6-level hydrogen model)
     def set_nlevel(self, table: np.ndarray, deriv: int = 1, n0fac: float = 1.0,

@@ -53,6 +53,9 @@ struct orc_ctx {
   double *ion_pot;                   /* globalvar ion_pot: the last irgetionpot, nc values */
   double gm_rec_ref;                 /* Gm_rec_ref */
   int nlev_init;                     /* the prologue's block of set_IR type 4 has run */
+  /* conduction of a decomposed run (orc_hcd_*): te, b, r, r0, p, Ap, t, the matrix and the
+   * primitives of the write-back */
+  double *hcd;                       /* 7 vectors then 9 matrix planes then 8 primitives */
   int nlev_bad;                      /* a negative rate (the reference stops there) */
   struct {
     double gw[6], eion[6], rn[6], bn[6];
@@ -1608,9 +1611,9 @@ static double hc_apply(const orc_ctx *c, const double *mat, const double *v, siz
 
 /* set_matrix_source_MHD2D9 (HC_rot.f90:643-739) for the interior cells (dxc = dx and
  * dyc = dy for s_order = 2, Model_rot.f90:430-431), then set_matrix_boundary
- * (HC_rot.f90:468-529) on all four sides: with one rank per direction every neighbour is
- * -1 (set_mpi_neighbor, MPI_rot.f90:123), so the stencil entries outside the domain are
- * folded onto the boundary row (x-, x+, y-, y+ in that order). */
+ * (HC_rot.f90:468-529) on the sides whose neighbour is -1: the stencil entries outside the
+ * domain are folded onto the boundary row (x-, x+, y-, y+ in that order).  With one rank
+ * per direction every neighbour is -1 (set_mpi_neighbor, MPI_rot.f90:123). */
 static void hc_matrix(const orc_ctx *c, const double *ro, const double *te, const double *bx,
                       const double *by, const double *bz, double dt, double *mat) {
   const pip_params *p = &c->p;
@@ -1663,25 +1666,25 @@ static void hc_matrix(const orc_ctx *c, const double *ro, const double *te, cons
     }
   /* set_matrix_boundary, hc_split = 2 (entries 1..9 of the Fortran are 0..8 here) */
 #define M(n, qq) mat[(size_t)(n) * nc + (qq)]
-  for (int j = js; j <= je; ++j) {       /* x-minus */
+  for (int j = js; j <= je && c->neighbor[0] == -1; ++j) {       /* x-minus */
     const size_t q = (size_t)j * ix + is;
     M(0, q) = M(1, q) + M(0, q); M(1, q) = 0.0;
     M(3, q) = M(3, q) + M(5, q); M(5, q) = 0.0;
     M(4, q) = M(4, q) + M(7, q); M(7, q) = 0.0;
   }
-  for (int j = js; j <= je; ++j) {       /* x-plus */
+  for (int j = js; j <= je && c->neighbor[1] == -1; ++j) {       /* x-plus */
     const size_t q = (size_t)j * ix + ie;
     M(0, q) = M(2, q) + M(0, q); M(2, q) = 0.0;
     M(3, q) = M(3, q) + M(6, q); M(6, q) = 0.0;
     M(4, q) = M(4, q) + M(8, q); M(8, q) = 0.0;
   }
-  for (int i = is; i <= ie; ++i) {       /* y-minus */
+  for (int i = is; i <= ie && c->neighbor[2] == -1; ++i) {       /* y-minus */
     const size_t q = (size_t)js * ix + i;
     M(0, q) = M(3, q) + M(0, q); M(3, q) = 0.0;
     M(1, q) = M(5, q) + M(1, q); M(5, q) = 0.0;
     M(2, q) = M(6, q) + M(2, q); M(6, q) = 0.0;
   }
-  for (int i = is; i <= ie; ++i) {       /* y-plus */
+  for (int i = is; i <= ie && c->neighbor[3] == -1; ++i) {       /* y-plus */
     const size_t q = (size_t)je * ix + i;
     M(0, q) = M(4, q) + M(0, q); M(4, q) = 0.0;
     M(1, q) = M(1, q) + M(7, q); M(7, q) = 0.0;
@@ -1814,6 +1817,149 @@ int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres) {
   }
   free(w); free(te); free(src); free(mat);
   return st;
+}
+
+/* BiCGstabMPI (HC_rot.f90:303-466, hc_split = 2) in the phases of pip_hcd_* for a block
+ * whose faces with a neighbour (orc_set_neighbors) are not folded: begin (cq2pv, te, the
+ * matrix, r = b - A te; sums (r,r), (b,b)), phase 0 (p = r), 1 (Ap = A p; sums (r,r0),
+ * (r0,Ap)), 2 (t = r - alpha Ap, At; sums (t,At), (At,At)), 3 (x += alpha p + omega t), 4
+ * (r = b - A x; sums (r0,r), (r,r)), 5 (p = r + beta (p - omega Ap)), end (the write-back of
+ * orc_conduction).  The caller sums the scalars over the ranks and moves one row of r (after
+ * begin and phase 4) and of Ap (after phase 1) across each exchanged face; t, x and p are
+ * formed on every cell.  Interior sums run in the Fortran array order. */
+enum { HCD_X = 0, HCD_B, HCD_R, HCD_R0, HCD_P, HCD_AP, HCD_T, HCD_NV };
+
+static double *hcd_v(const orc_ctx *c, int k) { return c->hcd + (size_t)k * c->nc; }
+
+int orc_hcd_begin(orc_ctx *c, double dt, double sums[2]) {
+  const pip_params *p = &c->p;
+  const size_t nc = c->nc;
+  const double gm = p->gm;
+  if (!c->hcd) c->hcd = calloc((HCD_NV + 9 + 8) * nc, sizeof(double));
+  memset(c->hcd, 0, sizeof(double) * (HCD_NV + 9) * nc);
+  double *mat = hcd_v(c, HCD_NV), *w = mat + 9 * nc;
+  double *ro = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc, *pr = w + 4 * nc;
+  double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
+  cq2pv_mhd(c, c->U_m, ro, vx, vy, vz, pr, bx, by, bz);
+  double *te = hcd_v(c, HCD_X), *b = hcd_v(c, HCD_B);
+  for (size_t q = 0; q < nc; ++q) {
+    te[q] = gm * (pr[q] / ro[q]);
+    b[q] = te[q];
+  }
+  hc_matrix(c, ro, te, bx, by, bz, dt, mat);
+  const int ix = c->ix, jx = c->jx;
+  const int is = p->margin[0], ie = ix - p->margin[0] - 1, js = p->margin[1], je = jx - p->margin[1] - 1;
+  double *r = hcd_v(c, HCD_R), *r0 = hcd_v(c, HCD_R0), *pk = hcd_v(c, HCD_P);
+  double a0 = 0.0, a1 = 0.0;
+  for (int j = js; j <= je; ++j)
+    for (int i = is; i <= ie; ++i) {
+      const size_t q = (size_t)j * ix + i;
+      double v = b[q];
+      v = v - mat[q] * te[q];
+      v = v - mat[q + nc] * te[q - 1];
+      v = v - mat[q + 2 * nc] * te[q + 1];
+      v = v - mat[q + 3 * nc] * te[q - ix];
+      v = v - mat[q + 4 * nc] * te[q + ix];
+      v = v - mat[q + 5 * nc] * te[q - 1 - ix];
+      v = v - mat[q + 6 * nc] * te[q + 1 - ix];
+      v = v - mat[q + 7 * nc] * te[q - 1 + ix];
+      v = v - mat[q + 8 * nc] * te[q + 1 + ix];
+      r[q] = v;
+      r0[q] = v;
+      pk[q] = v;
+      a0 += v * v;
+      a1 += b[q] * b[q];
+    }
+  sums[0] = a0;
+  sums[1] = a1;
+  return 0;
+}
+
+int orc_hcd_phase(orc_ctx *c, int phase, const double coef[2], double sums[2]) {
+  const pip_params *p = &c->p;
+  const size_t nc = c->nc;
+  const int ix = c->ix, jx = c->jx;
+  const int is = p->margin[0], ie = ix - p->margin[0] - 1, js = p->margin[1], je = jx - p->margin[1] - 1;
+  const double *mat = hcd_v(c, HCD_NV);
+  double *x = hcd_v(c, HCD_X), *b = hcd_v(c, HCD_B), *r = hcd_v(c, HCD_R), *r0 = hcd_v(c, HCD_R0);
+  double *pk = hcd_v(c, HCD_P), *ap = hcd_v(c, HCD_AP), *t = hcd_v(c, HCD_T);
+  double a0 = 0.0, a1 = 0.0;
+  switch (phase) {
+    case 0:
+      for (size_t q = 0; q < nc; ++q) pk[q] = r[q];
+      return 0;
+    case 1:
+      for (int j = js; j <= je; ++j)
+        for (int i = is; i <= ie; ++i) {
+          const size_t q = (size_t)j * ix + i;
+          ap[q] = hc_apply(c, mat, pk, q);
+          a0 = a0 + (r[q] * r0[q]);
+          a1 = a1 + (r0[q] * ap[q]);
+        }
+      break;
+    case 2:
+      for (size_t q = 0; q < nc; ++q) t[q] = r[q] - coef[0] * ap[q];
+      for (int j = js; j <= je; ++j)
+        for (int i = is; i <= ie; ++i) {
+          const size_t q = (size_t)j * ix + i;
+          const double at = hc_apply(c, mat, t, q);
+          a0 = a0 + t[q] * at;
+          a1 = a1 + at * at;
+        }
+      break;
+    case 3:
+      for (size_t q = 0; q < nc; ++q) x[q] = x[q] + coef[0] * pk[q] + coef[1] * t[q];
+      return 0;
+    case 4:
+      for (int j = js; j <= je; ++j)
+        for (int i = is; i <= ie; ++i) {
+          const size_t q = (size_t)j * ix + i;
+          r[q] = b[q] - hc_apply(c, mat, x, q);
+          a0 = a0 + r0[q] * r[q];
+          a1 = a1 + r[q] * r[q];
+        }
+      break;
+    case 5:
+      for (size_t q = 0; q < nc; ++q) pk[q] = r[q] + coef[0] * (pk[q] - coef[1] * ap[q]);
+      return 0;
+    default:
+      return PIP_ERR_PARAM;
+  }
+  sums[0] = a0;
+  sums[1] = a1;
+  return 0;
+}
+
+/* Row `row` of vector vec (0 x, 1 r, 2 Ap), ix values. */
+void orc_hcd_get_row(const orc_ctx *c, int vec, int row, double *out) {
+  const int k = vec == 0 ? HCD_X : vec == 1 ? HCD_R : HCD_AP;
+  memcpy(out, hcd_v(c, k) + (size_t)row * c->ix, sizeof(double) * c->ix);
+}
+void orc_hcd_set_row(orc_ctx *c, int vec, int row, const double *in) {
+  const int k = vec == 0 ? HCD_X : vec == 1 ? HCD_R : HCD_AP;
+  memcpy(hcd_v(c, k) + (size_t)row * c->ix, in, sizeof(double) * c->ix);
+}
+
+int orc_hcd_end(orc_ctx *c) {
+  const size_t nc = c->nc;
+  const double gm = c->p.gm;
+  const double *te = hcd_v(c, HCD_X), *w = hcd_v(c, HCD_NV) + 9 * nc;
+  const double *ro = w, *vx = w + nc, *vy = w + 2 * nc, *vz = w + 3 * nc;
+  const double *bx = w + 5 * nc, *by = w + 6 * nc, *bz = w + 7 * nc;
+  double *U = c->U_m;
+  for (size_t q = 0; q < nc; ++q) {
+    const double pr = (te[q] * ro[q]) / gm;
+    U[q] = ro[q];
+    U[q + nc] = ro[q] * vx[q];
+    U[q + 2 * nc] = ro[q] * vy[q];
+    U[q + 3 * nc] = ro[q] * vz[q];
+    U[q + 4 * nc] = pr / (gm - 1.0) + 0.5 * ro[q] * (vx[q] * vx[q] + vy[q] * vy[q] + vz[q] * vz[q]) +
+                    0.5 * (bx[q] * bx[q] + by[q] * by[q] + bz[q] * bz[q]);
+    U[q + 5 * nc] = bx[q];
+    U[q + 6 * nc] = by[q];
+    U[q + 7 * nc] = bz[q];
+  }
+  return 0;
 }
 
 /* One stage of run_solver, Solver_rot.f90:59-71 with set_flux :124, set_source :162,
@@ -1953,6 +2099,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->ac);
   free(c->eta);
   free(c->etab); free(c->nex); free(c->colrat); free(c->ion_pot);
+  free(c->hcd);
   free(c);
 }
 

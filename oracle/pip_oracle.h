@@ -71,6 +71,15 @@ int orc_run(orc_ctx *c, long nsteps, double t_end, double *time_out, long *steps
 /* HC(U_m,nvar_m,1) (HC_rot.f90:67-140), 9-point matrix + BiCGstab on one rank, over dt;
  * returns PIP_OK or PIP_ERR_ITER; iters/relres may be NULL. */
 int orc_conduction(orc_ctx *c, double dt, int *iters, double *relres);
+/* BiCGstabMPI (HC_rot.f90:303-466) in the phases of pip_hcd_* (include/pip_gpu.h) for a
+ * block with neighbours: orc_hcd_begin (sums (r,r), (b,b)), orc_hcd_phase 0..5 with coef
+ * (alpha; alpha, omega; beta, omega) and sums, rows of vector 0 (x), 1 (r), 2 (Ap) for the
+ * exchange, orc_hcd_end (the write-back of orc_conduction, every cell). */
+int orc_hcd_begin(orc_ctx *c, double dt, double sums[2]);
+int orc_hcd_phase(orc_ctx *c, int phase, const double coef[2], double sums[2]);
+void orc_hcd_get_row(const orc_ctx *c, int vec, int row, double *out);
+void orc_hcd_set_row(orc_ctx *c, int vec, int row, const double *in);
+int orc_hcd_end(orc_ctx *c);
 /* stop_sim's NaN scan (IO_rot.f90:641-668) over both species. */
 int orc_has_nan(const orc_ctx *c);
 

@@ -40,6 +40,8 @@ EXPORTS = (
     "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
     "pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
     "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref", "pip_get_ir_rates",
+    "pip_hcd_begin", "pip_hcd_phase", "pip_hcd_row_bytes", "pip_hcd_pack", "pip_hcd_unpack",
+    "pip_hcd_end",
     # include/pip_bench.h
     "pip_run_timed", "pip_bench_stage_ms", "pip_kernels_per_run", "pip_conduction_iterations",
     # include/pip_ensemble.h
@@ -124,6 +126,15 @@ def lib(path: Optional[str] = None):
     L.pip_get_ion_pot.argtypes = [vp, dp]
     L.pip_nlevel_gm_rec_ref.argtypes = [vp, dp]
     L.pip_get_ir_rates.argtypes = [vp, dp, dp]
+    L.pip_hcd_begin.argtypes = [vp, d, dp]
+    L.pip_hcd_phase.argtypes = [vp, i, dp, dp]
+    L.pip_hcd_row_bytes.argtypes = [vp]
+    L.pip_hcd_row_bytes.restype = ctypes.c_int64
+    L.pip_hcd_pack.argtypes = [vp, i, i, vp]
+    L.pip_hcd_unpack.argtypes = [vp, i, i, vp]
+    L.pip_hcd_end.argtypes = [vp, i]
+    for name in ("pip_hcd_begin", "pip_hcd_phase", "pip_hcd_pack", "pip_hcd_unpack", "pip_hcd_end"):
+        getattr(L, name).restype = i
     for name in ("pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
                  "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref",
                  "pip_get_ir_rates"):
@@ -476,6 +487,32 @@ class Context:
         rec = np.empty(self.shape_h[1:])
         _check(lib().pip_get_ir_rates(self.h, _ptr(ion), _ptr(rec)), "pip_get_ir_rates")
         return ion, rec
+
+    # ---- conduction of a decomposed run (BiCGstabMPI in phases, pip_hcd_*)
+    def hcd_begin(self, dt: float) -> Tuple[float, float]:
+        s = (ctypes.c_double * 2)()
+        _check(lib().pip_hcd_begin(self.h, float(dt), s), "pip_hcd_begin")
+        return s[0], s[1]
+
+    def hcd_phase(self, phase: int, c0: float = 0.0, c1: float = 0.0) -> Tuple[float, float]:
+        coef = (ctypes.c_double * 2)(float(c0), float(c1))
+        s = (ctypes.c_double * 2)()
+        _check(lib().pip_hcd_phase(self.h, int(phase), coef, s), "pip_hcd_phase")
+        return s[0], s[1]
+
+    def hcd_row_bytes(self) -> int:
+        return int(lib().pip_hcd_row_bytes(self.h))
+
+    def hcd_pack(self, vec: int, face: int, send_ptr: int) -> None:
+        _check(lib().pip_hcd_pack(self.h, int(vec), int(face), ctypes.c_void_p(send_ptr)),
+               "pip_hcd_pack")
+
+    def hcd_unpack(self, vec: int, face: int, recv_ptr: int) -> None:
+        _check(lib().pip_hcd_unpack(self.h, int(vec), int(face), ctypes.c_void_p(recv_ptr)),
+               "pip_hcd_unpack")
+
+    def hcd_end(self, iters: int) -> None:
+        _check(lib().pip_hcd_end(self.h, int(iters)), "pip_hcd_end")
 
     def gm_rec_ref(self) -> float:
         v = ctypes.c_double()

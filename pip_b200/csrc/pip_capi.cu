@@ -1208,9 +1208,10 @@ int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
     if (f >= 2 * c->kp.ndim && neighbor[f] != -1) return PIP_ERR_PARAM;
     any = any || neighbor[f] >= 0;
   }
-  // the conduction matrix folds every side of the block (one rank per direction); with eta
-  // recomputed at every stage each rank advances its time by its own cfl_resi bound
-  if (any && (c->hc || c->kp.resi == 2 || c->kp.irn)) return PIP_ERR_PARAM;
+  // with eta recomputed at every stage each rank advances its time by its own cfl_resi
+  // bound; conduction splits along y only (pip_hcd_*)
+  if (any && (c->kp.resi == 2 || c->kp.irn)) return PIP_ERR_PARAM;
+  if (c->hc && (neighbor[0] >= 0 || neighbor[1] >= 0)) return PIP_ERR_PARAM;
   if (set_device(c)) return PIP_ERR_CUDA;
   if (c->stream) CK(cudaStreamSynchronize(c->stream));
   if (c->graph) {
@@ -1248,7 +1249,7 @@ int pip_stage(pip_ctx *c, int stage, double dt, double cmax) {
     c->cmax = cmax;
   }
   CK(do_stage(c, stage, 0, 0));
-  if (stage == 2 && c->hc) {
+  if (stage == 2 && c->hc && !c->exchanged) {   // with neighbours: pip_hcd_* after the exchange
     CK(cudaMemcpyAsync(c->d_dt, &c->ctrl->dt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     int it = 0, st = 0;
     const int r = conduct(c, c->d_dt, &it, nullptr, &st);
@@ -1516,6 +1517,67 @@ int pip_nlevel_gm_rec_ref(pip_ctx *c, double *gm_rec_ref) {
   if (!c->kp.irn) return PIP_ERR_PARAM;
   if (!c->nl_init) return PIP_ERR_STATE;
   *gm_rec_ref = c->kp.nl_gref;
+  return PIP_OK;
+}
+
+__global__ void set_double_kernel(double *dst, double v) { *dst = v; }
+
+int pip_hcd_begin(pip_ctx *c, double dt, double sums[2]) {
+  if (!c || !sums) return PIP_ERR_NULL;
+  if (!c->hc) return PIP_ERR_PARAM;
+  if (!c->uploaded) return PIP_ERR_STATE;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(to_fp64(c));
+  set_double_kernel<<<1, 1, 0, c->stream>>>(c->d_dt, dt);
+  CK(cudaGetLastError());
+  CK(pip::hcd_begin(c->hc, c->kp, c->A, c->d_dt, c->stream, sums));
+  return PIP_OK;
+}
+
+int pip_hcd_phase(pip_ctx *c, int phase, const double coef[2], double sums[2]) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->hc) return PIP_ERR_PARAM;
+  if (phase < 0 || phase > 5) return PIP_ERR_PARAM;
+  if ((phase == 1 || phase == 2 || phase == 4) && !sums) return PIP_ERR_NULL;
+  if ((phase == 2 || phase == 3 || phase == 5) && !coef) return PIP_ERR_NULL;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  double dummy[2];
+  CK(pip::hcd_phase(c->hc, c->kp, phase, coef, c->stream, sums ? sums : dummy));
+  return PIP_OK;
+}
+
+int64_t pip_hcd_row_bytes(pip_ctx *c) { return c ? (int64_t)sizeof(double) * c->kp.ix : 0; }
+
+int pip_hcd_pack(pip_ctx *c, int vec, int face, void *send) {
+  if (!c || !send) return PIP_ERR_NULL;
+  if (!c->hc || (face != 2 && face != 3) || vec < 0 || vec > 2) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  const int row = face == 2 ? c->kp.m1 : c->kp.m1 + c->kp.ny - 1;   // the neighbour's halo row
+  const double *v = pip::hcd_vector(c->hc, vec) + (size_t)row * c->kp.ix;
+  CK(cudaMemcpyAsync(send, v, sizeof(double) * c->kp.ix, cudaMemcpyDeviceToDevice, c->stream));
+  return PIP_OK;
+}
+
+int pip_hcd_unpack(pip_ctx *c, int vec, int face, const void *recv) {
+  if (!c || !recv) return PIP_ERR_NULL;
+  if (!c->hc || (face != 2 && face != 3) || vec < 0 || vec > 2) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  const int row = face == 2 ? c->kp.m1 - 1 : c->kp.m1 + c->kp.ny;
+  double *v = pip::hcd_vector(c->hc, vec) + (size_t)row * c->kp.ix;
+  CK(cudaMemcpyAsync(v, recv, sizeof(double) * c->kp.ix, cudaMemcpyDeviceToDevice, c->stream));
+  return PIP_OK;
+}
+
+int pip_hcd_end(pip_ctx *c, int iters) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->hc) return PIP_ERR_PARAM;
+  if (set_device(c)) return PIP_ERR_CUDA;
+  CK(pip::hcd_end(c->hc, c->kp, c->A, c->stream));
+  CK(c->L->ghosts(c->kp, c->A, c->stream));   // physical faces; the caller exchanges the rest
+  CK(from_fp64(c));
+  CK(cudaStreamSynchronize(c->stream));
+  c->hc_iters = iters;
   return PIP_OK;
 }
 

@@ -94,8 +94,9 @@ struct RowFactors {
 
 // The nine entries of row (i,j), in the reference's neighbour order 0 (i,j), 1 (i-1,j),
 // 2 (i+1,j), 3 (i,j-1), 4 (i,j+1), 5 (i-1,j-1), 6 (i+1,j-1), 7 (i-1,j+1), 8 (i+1,j+1),
-// with set_matrix_boundary's folds on all four sides (HC_rot.f90:468-529; one rank per
-// direction, so every side folds: MPI_rot.f90:123).
+// with set_matrix_boundary's folds (HC_rot.f90:468-529) on the sides without a neighbouring
+// rank (boundary type 0 marks an exchanged face: pip_set_neighbors).  One rank per
+// direction: every side folds (MPI_rot.f90:123).
 template <typename T>
 __device__ __forceinline__ void entries(const KParams &p, const RowFactors<T> &f, int i, int j,
                                         T (&c)[9]) {
@@ -118,22 +119,22 @@ __device__ __forceinline__ void entries(const KParams &p, const RowFactors<T> &f
   c[7] = -(bxyl + byxu);
   c[8] = bxyr + byxu;
   c[0] = T(1) - (c[1] + c[2] + c[3] + c[4]);
-  if (i == p.m0) {                 // x-minus
+  if (i == p.m0 && p.typex[0] != 0) {                 // x-minus
     c[0] = c[1] + c[0]; c[1] = T(0);
     c[3] = c[3] + c[5]; c[5] = T(0);
     c[4] = c[4] + c[7]; c[7] = T(0);
   }
-  if (i == p.m0 + p.nx - 1) {      // x-plus
+  if (i == p.m0 + p.nx - 1 && p.typex[1] != 0) {      // x-plus
     c[0] = c[2] + c[0]; c[2] = T(0);
     c[3] = c[3] + c[6]; c[6] = T(0);
     c[4] = c[4] + c[8]; c[8] = T(0);
   }
-  if (j == p.m1) {                 // y-minus
+  if (j == p.m1 && p.typey[0] != 0) {                 // y-minus
     c[0] = c[3] + c[0]; c[3] = T(0);
     c[1] = c[5] + c[1]; c[5] = T(0);
     c[2] = c[6] + c[2]; c[6] = T(0);
   }
-  if (j == p.m1 + p.ny - 1) {      // y-plus
+  if (j == p.m1 + p.ny - 1 && p.typey[1] != 0) {      // y-plus
     c[0] = c[4] + c[0]; c[4] = T(0);
     c[1] = c[1] + c[7]; c[7] = T(0);
     c[2] = c[2] + c[8]; c[8] = T(0);
@@ -761,6 +762,9 @@ struct HcEngine {
   hc::Scal *sc = nullptr, *sc32 = nullptr;
   hc::Scal *h_sc = nullptr;         // pinned
   int wait_limit = hc::kWaitLimit;  // polls of a staging mbarrier (hc_set_wait_limit)
+  // distributed solve (hcd_*): per-block partial sums on the device and their pinned copy
+  double *dpart = nullptr, *h_dpart = nullptr;
+  int dnb = 0;
 };
 
 void hc_set_wait_limit(HcEngine *e, int polls) {
@@ -775,6 +779,8 @@ void hc_destroy(HcEngine *e) {
                   e->ap32[1], e->part, e->sc, e->sc32};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  if (e->dpart) cudaFree(e->dpart);
+  if (e->h_dpart) cudaFreeHost(e->h_dpart);
   if (e->h_sc) cudaFreeHost(e->h_sc);
   delete e;
 }
@@ -946,6 +952,247 @@ cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, 
   if (relres) *relres = h->relres;
   if (status) *status = h->relres <= tol ? 0 : 5;  // PIP_ERR_ITER
   return cudaSuccess;
+}
+
+
+// ---------------------------------------------------------------- distributed BiCGstab
+//
+// BiCGstabMPI (HC_rot.f90:303-466, hc_split = 2) for a block whose y faces may border other
+// ranks, as phases between which the caller reduces two scalars over the ranks (SUM) and
+// exchanges one halo row of a vector.  The matrix is the single-rank one (face factors and
+// entries(), folded only on faces without a neighbour), so the ranks together hold the rows
+// of the undecomposed matrix bit for bit.  Per iteration:
+//   phase 1  Ap = A p                 sums (r, r0), (r0, Ap)   -> alpha; exchange Ap
+//   phase 2  t = r - alpha Ap; At     sums (t, At), (At, At)   -> omega
+//   phase 3  x = x + alpha p + omega t
+//   phase 4  r = b - A x              sums (r0, r), (r, r)     -> beta, residual; exchange r
+//   phase 5  p = r + beta (p - omega Ap)
+// t, x and p are formed on every cell, so their halo rows follow from the exchanged r and Ap
+// rows (and from x's and p's own consistent halo rows): only Ap and r cross between ranks,
+// one row each way, as the reference's mpiBND of apk and residual (its mpiBND of te is
+// implied here).  The reference takes omega from the rank's own sums (HC_rot.f90:425-427),
+// which makes its iterates depend on the decomposition; here every scalar is the global one,
+// so the ranks iterate as the single domain does (the sums group differently: rounding).
+// Sums: per-block partials in a fixed cell order, added on the host in block order.
+namespace hcd {
+
+using namespace pip::hc;
+constexpr int NT = 256;
+
+__device__ __forceinline__ RowFactors<double> factors(const KParams &p, const double *__restrict__ m,
+                                                      const double *__restrict__ g, int i, int j) {
+  const long long nc = p.nc, ix = p.ix, q = (long long)j * ix + i;
+  RowFactors<double> f;
+  f.eta = m[q];
+  f.fxxl = m[nc + q];
+  f.fxxr = m[nc + q + 1];
+  f.fxyl = m[2 * nc + q];
+  f.fxyr = m[2 * nc + q + 1];
+  f.fyyd = m[3 * nc + q];
+  f.fyyu = m[3 * nc + q + ix];
+  f.fyxd = m[4 * nc + q];
+  f.fyxu = m[4 * nc + q + ix];
+  f.cxl = g[i];
+  f.cxr = g[ix + i];
+  f.idx = g[2 * ix + i];
+  const double *gy = g + 3 * ix;
+  f.cyd = gy[j];
+  f.cyu = gy[p.jx + j];
+  f.idy = gy[2 * p.jx + j];
+  return f;
+}
+
+__device__ __forceinline__ void window(const KParams &p, const double *__restrict__ v, long long q,
+                                       double (&w)[3][3]) {
+#pragma unroll
+  for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+    for (int di = -1; di <= 1; ++di) w[dj + 1][di + 1] = v[q + dj * (long long)p.ix + di];
+}
+
+// Block sums of two values into part[2*block + k] (tree order fixed by the block size).
+__device__ __forceinline__ void block_sums(double a0, double a1, double *part) {
+  __shared__ double s2[2][NT];
+  s2[0][threadIdx.x] = a0;
+  s2[1][threadIdx.x] = a1;
+  __syncthreads();
+  for (int h = NT / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      s2[0][threadIdx.x] += s2[0][threadIdx.x + h];
+      s2[1][threadIdx.x] += s2[1][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s2[0][0];
+    part[2 * blockIdx.x + 1] = s2[1][0];
+  }
+}
+
+// Interior-cell kernels: 0 r = b - A x term by term, r0 = p = r, sums (r,r), (b,b);
+// 1 Ap = A p, sums (r,r0), (r0,Ap); 2 At = A t, sums (t,At), (At,At); 4 r = b - A x, sums
+// (r0,r), (r,r).
+template <int KIND>
+__global__ void __launch_bounds__(NT) spmv_kernel(const KParams p, const double *__restrict__ m,
+                                                  const double *__restrict__ g, const double *__restrict__ v,
+                                                  const double *__restrict__ b, double *r,
+                                                  double *r0, double *out, double *part) {
+  int i, j;
+  const long long t = blockIdx.x * (long long)NT + threadIdx.x;
+  double a0 = 0.0, a1 = 0.0;
+  if (interior_cell(p, t, i, j)) {
+    const long long q = (long long)j * p.ix + i;
+    double w[3][3], c[9];
+    window(p, v, q, w);
+    entries(p, factors(p, m, g, i, j), i, j, c);
+    if (KIND == 0) {
+      const double bq = b[q];
+      double x = bq;
+      x = x - c[0] * w[1][1];
+      x = x - c[1] * w[1][0];
+      x = x - c[2] * w[1][2];
+      x = x - c[3] * w[0][1];
+      x = x - c[4] * w[2][1];
+      x = x - c[5] * w[0][0];
+      x = x - c[6] * w[0][2];
+      x = x - c[7] * w[2][0];
+      x = x - c[8] * w[2][2];
+      r[q] = x;
+      r0[q] = x;
+      out[q] = x;
+      a0 = x * x;
+      a1 = bq * bq;
+    } else if (KIND == 1) {
+      const double av = stencil(c, w);
+      out[q] = av;
+      a0 = r[q] * r0[q];
+      a1 = r0[q] * av;
+    } else if (KIND == 2) {
+      const double at = stencil(c, w);
+      a0 = w[1][1] * at;
+      a1 = at * at;
+    } else {
+      const double x = b[q] - stencil(c, w);
+      r[q] = x;
+      a0 = r0[q] * x;
+      a1 = x * x;
+    }
+  }
+  block_sums(a0, a1, part);
+}
+
+// Every-cell updates: 0 p = r; 2 t = r - c0 Ap; 3 x = x + c0 p + c1 t; 5 p = r + c0 (p - c1 Ap).
+template <int KIND>
+__global__ void __launch_bounds__(NT) axpy_kernel(long long nc, double c0, double c1, const double *r,
+                                                  const double *ap, double *t, double *x, double *pv) {
+  for (long long q = blockIdx.x * (long long)NT + threadIdx.x; q < nc; q += (long long)gridDim.x * NT) {
+    if (KIND == 0) pv[q] = r[q];
+    else if (KIND == 2) t[q] = r[q] - c0 * ap[q];
+    else if (KIND == 3) x[q] = x[q] + c0 * pv[q] + c1 * t[q];
+    else pv[q] = r[q] + c0 * (pv[q] - c1 * ap[q]);
+  }
+}
+
+}  // namespace hcd
+
+namespace {
+
+// Per-block partials of the last spmv_kernel, summed in block order on the host.
+cudaError_t hcd_sums(HcEngine *e, cudaStream_t s, double sums[2]) {
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(e->h_dpart, e->dpart, sizeof(double) * 2 * e->dnb, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return err;
+  double a0 = 0.0, a1 = 0.0;
+  for (int k = 0; k < e->dnb; ++k) {
+    a0 += e->h_dpart[2 * k];
+    a1 += e->h_dpart[2 * k + 1];
+  }
+  sums[0] = a0;
+  sums[1] = a1;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t hcd_begin(HcEngine *e, const KParams &k, double *U, const double *dtp, cudaStream_t s,
+                      double sums[2]) {
+  using namespace hc;
+  const long long nc = k.nc;
+  const int nb = (int)(((long long)k.nx * k.ny + hcd::NT - 1) / hcd::NT);
+  if (nb > e->dnb) {
+    if (e->dpart) cudaFree(e->dpart);
+    if (e->h_dpart) cudaFreeHost(e->h_dpart);
+    e->dpart = nullptr;
+    e->h_dpart = nullptr;
+    e->dnb = 0;
+    cudaError_t err = cudaMalloc(&e->dpart, sizeof(double) * 2 * nb);
+    if (err == cudaSuccess) err = cudaMallocHost(&e->h_dpart, sizeof(double) * 2 * nb);
+    if (err != cudaSuccess) return err;
+    e->dnb = nb;
+  }
+  e->dnb = nb;
+  const int gu = (int)std::min<long long>((nc + 255) / 256, 148 * 8);
+  const int gf = (int)(((long long)(k.nx + 1) * (k.ny + 1) + NT - 1) / NT);
+  // every cell, ghost rows included: the halo rows hold the neighbours' state after the
+  // stage's exchange, so te, b and the face factors next to an exchanged face are the
+  // undecomposed ones
+  setup_kernel<<<gu, 256, 0, s>>>(k, U, e->x[0], e->b, e->kin, e->mag);
+  matrix_kernel<<<gf, NT, 0, s>>>(k, U, e->x[0], dtp, e->m64, nullptr);
+  geometry_kernel<<<(k.ix + k.jx + NT - 1) / NT, NT, 0, s>>>(k, e->g64, nullptr);
+  cudaError_t err = cudaMemsetAsync(e->ap[0], 0, sizeof(double) * (size_t)nc, s);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->t, 0, sizeof(double) * (size_t)nc, s);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->r, 0, sizeof(double) * (size_t)nc, s);
+  if (err == cudaSuccess) err = cudaMemsetAsync(e->p[0], 0, sizeof(double) * (size_t)nc, s);
+  if (err != cudaSuccess) return err;
+  hcd::spmv_kernel<0><<<nb, hcd::NT, 0, s>>>(k, e->m64, e->g64, e->x[0], e->b, e->r, e->r0, e->p[0],
+                                             e->dpart);
+  return hcd_sums(e, s, sums);
+}
+
+cudaError_t hcd_phase(HcEngine *e, const KParams &k, int phase, const double coef[2], cudaStream_t s,
+                      double sums[2]) {
+  const long long nc = k.nc;
+  const int nb = e->dnb;
+  const int ga = (int)std::min<long long>((nc + hcd::NT - 1) / hcd::NT, 148 * 8);
+  const double c0 = coef ? coef[0] : 0.0, c1 = coef ? coef[1] : 0.0;
+  switch (phase) {
+    case 0:
+      hcd::axpy_kernel<0><<<ga, hcd::NT, 0, s>>>(nc, 0.0, 0.0, e->r, nullptr, nullptr, nullptr, e->p[0]);
+      return cudaGetLastError();
+    case 1:
+      hcd::spmv_kernel<1><<<nb, hcd::NT, 0, s>>>(k, e->m64, e->g64, e->p[0], nullptr, e->r, e->r0,
+                                                 e->ap[0], e->dpart);
+      return hcd_sums(e, s, sums);
+    case 2:
+      hcd::axpy_kernel<2><<<ga, hcd::NT, 0, s>>>(nc, c0, 0.0, e->r, e->ap[0], e->t, nullptr, nullptr);
+      hcd::spmv_kernel<2><<<nb, hcd::NT, 0, s>>>(k, e->m64, e->g64, e->t, nullptr, nullptr, nullptr,
+                                                 nullptr, e->dpart);
+      return hcd_sums(e, s, sums);
+    case 3:
+      hcd::axpy_kernel<3><<<ga, hcd::NT, 0, s>>>(nc, c0, c1, nullptr, nullptr, e->t, e->x[0], e->p[0]);
+      return cudaGetLastError();
+    case 4:
+      hcd::spmv_kernel<4><<<nb, hcd::NT, 0, s>>>(k, e->m64, e->g64, e->x[0], e->b, e->r, e->r0,
+                                                 nullptr, e->dpart);
+      return hcd_sums(e, s, sums);
+    case 5:
+      hcd::axpy_kernel<5><<<ga, hcd::NT, 0, s>>>(nc, c0, c1, e->r, e->ap[0], nullptr, nullptr, e->p[0]);
+      return cudaGetLastError();
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+double *hcd_vector(HcEngine *e, int vec) {
+  return vec == 0 ? e->x[0] : vec == 1 ? e->r : vec == 2 ? e->ap[0] : nullptr;
+}
+
+cudaError_t hcd_end(HcEngine *e, const KParams &k, double *U, cudaStream_t s) {
+  const int gi = (int)(((long long)k.nx * k.ny + hc::NT - 1) / hc::NT);
+  hc::writeback_kernel<<<gi, hc::NT, 0, s>>>(k, U, e->x[0], e->kin, e->mag);
+  return cudaGetLastError();
 }
 
 }  // namespace pip

@@ -151,6 +151,20 @@ void hc_destroy(HcEngine *e);
 // Polls of a staging mbarrier before a BiCGstab block gives up and flags the solve as
 // failed (polls < 0: the default); applies from the next solve.
 void hc_set_wait_limit(HcEngine *e, int polls);
+// Distributed BiCGstab (BiCGstabMPI) in phases, for a block with neighbouring ranks across
+// y faces: hcd_begin sets up te, the matrix (folded on the physical faces only) and the
+// residual of the state U (ghost rows holding the neighbours' rows) and returns the local
+// sums (r,r), (b,b); hcd_phase runs phase 0 (p = r), 1 (Ap = A p; sums (r,r0), (r0,Ap)), 2
+// (t = r - coef[0] Ap, At; sums (t,At), (At,At)), 3 (x += coef[0] p + coef[1] t), 4 (r = b - A x;
+// sums (r0,r), (r,r)) or 5 (p = r + coef[0] (p - coef[1] Ap)); hcd_vector gives the device
+// plane of vector 0 (x), 1 (r) or 2 (Ap) for the halo rows; hcd_end writes te back into the
+// energy of the interior cells.
+cudaError_t hcd_begin(HcEngine *e, const KParams &k, double *U, const double *dtp, cudaStream_t s,
+                      double sums[2]);
+cudaError_t hcd_phase(HcEngine *e, const KParams &k, int phase, const double coef[2], cudaStream_t s,
+                      double sums[2]);
+double *hcd_vector(HcEngine *e, int vec);
+cudaError_t hcd_end(HcEngine *e, const KParams &k, double *U, cudaStream_t s);
 cudaError_t hc_run(HcEngine *e, const KParams &k, double *U, const double *dtp, double tol,
                    int hc_max, cudaStream_t s, int *iters, double *relres, int *status);
 

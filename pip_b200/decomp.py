@@ -153,6 +153,12 @@ class TorchComm:
                              group=self.group)
         return float(t.item())
 
+    def allreduce_sums(self, values) -> List[float]:
+        """mpi_allreduce(..., MPI_SUM) of a few doubles (BiCGstabMPI's scalars)."""
+        t = self.torch.tensor(list(values), dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+        return [float(v) for v in t.tolist()]
+
     def reduce_candidates(self, pairs) -> None:
         """cfl's MIN/MAX allreduces on device memory: pairs = [(t_min, t_max)] of this
         process's blocks (one), reduced in place over the ranks on the current stream."""
@@ -182,6 +188,9 @@ class LocalComm:
 
     def allreduce(self, value: float, op: str) -> float:
         return value
+
+    def allreduce_sums(self, values) -> List[float]:
+        return [float(v) for v in values]
 
     def barrier(self) -> None:
         pass
@@ -312,6 +321,26 @@ class DeviceBlock:
         context's stream."""
         return self.torch.cuda.stream(self._stream)
 
+    # conduction of the decomposed run (pip_hcd_*): vector 0 x, 1 r, 2 Ap
+    def hcd_begin(self, dt: float) -> Tuple[float, float]:
+        return self.ctx.hcd_begin(dt)
+
+    def hcd_phase(self, phase: int, c0: float = 0.0, c1: float = 0.0) -> Tuple[float, float]:
+        return self.ctx.hcd_phase(phase, c0, c1)
+
+    def hcd_row_bytes(self) -> int:
+        return self.ctx.hcd_row_bytes()
+
+    def hcd_pack(self, vec: int, face: int, buf) -> int:
+        self.ctx.hcd_pack(vec, face, buf.data_ptr())
+        return self.ctx.hcd_row_bytes()
+
+    def hcd_unpack(self, vec: int, face: int, buf) -> None:
+        self.ctx.hcd_unpack(vec, face, buf.data_ptr())
+
+    def hcd_end(self, iters: int) -> None:
+        self.ctx.hcd_end(iters)
+
     def has_nan(self) -> bool:
         return bool(self.ctx.status()[1])
 
@@ -380,8 +409,82 @@ class DecomposedRun:
                     if e.block.neighbor[recv_face] >= 0:
                         e.unpack(recv_face, self._recv[(r, recv_face)], e.message_bytes(recv_face))
 
+    def _hcd_halo(self, vec: int) -> None:
+        """mpiBND(v, 1) of a BiCGstab vector: one row across each exchanged y face, in the
+        two phases of halo()."""
+        for send_face in (3, 2):
+            recv_face = send_face ^ 1
+            sends, recvs = [], []
+            for e in self.engines:
+                r = e.block.rank
+                if e.block.neighbor[send_face] >= 0:
+                    buf = self._hc_send[(r, send_face)]
+                    n = e.hcd_pack(vec, send_face, buf)
+                    sends.append((r, e.block.neighbor[send_face], buf[:n]))
+                if e.block.neighbor[recv_face] >= 0:
+                    buf = self._hc_recv[(r, recv_face)]
+                    recvs.append((r, e.block.neighbor[recv_face], buf))
+            if not sends and not recvs:
+                continue
+            if len(self.engines) == 1:
+                with self.engines[0].stream():
+                    self.comm.exchange(sends, recvs)
+            else:
+                self.comm.exchange(sends, recvs)
+            for e in self.engines:
+                r = e.block.rank
+                if e.block.neighbor[recv_face] >= 0:
+                    e.hcd_unpack(vec, recv_face, self._hc_recv[(r, recv_face)])
+
+    def _sums(self, parts) -> List[float]:
+        """SUM over this process's blocks (in block order), then over the ranks."""
+        a0 = 0.0
+        a1 = 0.0
+        for s0, s1 in parts:
+            a0 += s0
+            a1 += s1
+        return self.comm.allreduce_sums([a0, a1])
+
+    def conduction(self, dt: float, hc_error: float, hc_max: int) -> Tuple[int, float]:
+        """post_step's HC over dt (Solver_rot.f90:296-303) as BiCGstabMPI (HC_rot.f90:303-466)
+        on the device blocks, then the state's exchange (the closing PIPbnd).  Returns
+        (iterations, relative residual); every rank takes the same steps."""
+        if not hasattr(self, "_hc_send"):
+            self._hc_send, self._hc_recv = {}, {}
+            for e in self.engines:
+                for f in (2, 3):
+                    if e.block.neighbor[f] >= 0:
+                        n = e.hcd_row_bytes()
+                        self._hc_send[(e.block.rank, f)] = e.buffer(n)
+                        self._hc_recv[(e.block.rank, f)] = e.buffer(n)
+        tr, tb = self._sums([e.hcd_begin(dt) for e in self.engines])
+        self._hcd_halo(1)
+        for e in self.engines:
+            e.hcd_phase(0)
+        count = 0
+        while np.sqrt(tr / tb) > hc_error and count <= hc_max:
+            au, ad = self._sums([e.hcd_phase(1) for e in self.engines])
+            alpha = au / ad
+            self._hcd_halo(2)
+            ou, od = self._sums([e.hcd_phase(2, alpha) for e in self.engines])
+            omega = ou / od
+            for e in self.engines:
+                e.hcd_phase(3, alpha, omega)
+            bu, tr = self._sums([e.hcd_phase(4) for e in self.engines])
+            self._hcd_halo(1)
+            beta = bu / au * alpha / omega
+            for e in self.engines:
+                e.hcd_phase(5, beta, omega)
+            count += 1
+        for e in self.engines:
+            e.hcd_end(count)
+        self.halo()
+        self.hc_iterations = count
+        return count, float(np.sqrt(tr / tb))
+
     def step(self) -> float:
-        """cfl; run_solver with PIPbnd's exchange after each stage; cfl (main.f90:36-47)."""
+        """cfl; run_solver with PIPbnd's exchange after each stage (and post_step's
+        conduction with flag_heat = 1); cfl (main.f90:36-47)."""
         dt = min(e.cfl()[0] for e in self.engines)
         dt = self.comm.allreduce(dt, "min")
         cmax = 0.0
@@ -391,6 +494,10 @@ class DecomposedRun:
             for e in self.engines:
                 e.stage(k, dt, cmax)
             self.halo()
+        s = self.engines[0].block.settings
+        if s.flag_heat == 1 and any(n >= 0 for e in self.engines for n in e.block.neighbor):
+            # (a block without neighbours conducts inside its stage 2, as pip_stage does)
+            self.conduction(dt, s.hc_error, s.hc_max)
         for e in self.engines:
             e.cfl()
         self.time += dt

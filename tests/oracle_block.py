@@ -27,6 +27,10 @@ class OracleBlock:
     def stage(self, k, dt, cmax):
         self.o.cmax = cmax
         self.o.stage(k, dt)
+        if k == 2 and self.s.flag_heat == 1 and all(n < 0 for n in self.block.neighbor):
+            # post_step's conduction and PIPbnd of a block without neighbours, as pip_stage
+            self.o.conduction(dt)
+            self.o.fill_ghosts()
 
     def _layers(self, face, pack):
         d = face // 2
@@ -68,6 +72,32 @@ class OracleBlock:
             U[:, :, sl] = msg.reshape(U.shape[0], -1, jx).transpose(0, 2, 1)
         nm = self.s.nvar_m
         self.o.set_state(U[nm:], U[:nm])
+
+    # BiCGstabMPI in phases (the engine protocol of DecomposedRun.conduction)
+    def hcd_begin(self, dt):
+        return self.o.hcd_begin(dt)
+
+    def hcd_phase(self, phase, c0=0.0, c1=0.0):
+        return self.o.hcd_phase(phase, c0, c1)
+
+    def hcd_row_bytes(self):
+        return 8 * self.n[0]
+
+    def hcd_pack(self, vec, face, buf):
+        jx = self.n[1]
+        row = self.m[1] if face == 2 else jx - self.m[1] - 1
+        raw = self.o.hcd_get_row(vec, row).view(np.uint8)
+        buf[: raw.size] = torch.from_numpy(raw.copy())
+        return raw.size
+
+    def hcd_unpack(self, vec, face, buf):
+        jx = self.n[1]
+        row = self.m[1] - 1 if face == 2 else jx - self.m[1]
+        self.o.hcd_set_row(vec, row, buf[: 8 * self.n[0]].numpy().view(np.float64))
+
+    def hcd_end(self, iters):
+        self.o.hcd_end()
+        self.o.fill_ghosts()        # the physical faces; the exchange fills the others
 
     def stream(self):
         import contextlib

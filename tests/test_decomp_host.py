@@ -153,3 +153,52 @@ def test_candidate_reduction_over_two_gloo_ranks():
     want_max = np.maximum(got[0][2], got[1][2])
     for g in got:
         assert np.array_equal(g[3], want_min) and np.array_equal(g[4], want_max)
+
+
+@pytest.mark.parametrize("case,world", [("kh_hc", 2), ("kh_hc", 4), ("kh_hc_generic", 1),
+                                        ("kh_hc_generic", 2), ("kh_hc_generic", 4)])
+def test_conduction_blocks_match_single_domain(case, world):
+    """post_step's implicit conduction of a decomposed run (BiCGstabMPI in phases, global
+    scalars, one row of r and Ap exchanged per face) against the single domain: one block
+    (no neighbours) conducts inside its stage as the single domain does, bitwise; more blocks
+    group the dot products by rank, so the iterates agree to rounding (and the iteration
+    count near the 1e-12 stop may differ)."""
+    nsteps = 4
+    s, uh, um, hist = single_domain(case, nsteps)
+    st, dts, gh, gm = local_run(case, world, nsteps)
+    assert st == 0
+    if world == 1:
+        assert np.array_equal(np.array(dts), hist)
+        assert np.array_equal(gh, uh) and np.array_equal(gm, um)
+        return
+    assert np.allclose(np.array(dts), hist, rtol=1e-11, atol=0)
+    rel = max(np.abs(gh - uh).max() / np.abs(uh).max(), np.abs(gm - um).max() / np.abs(um).max())
+    assert rel <= 1e-11, rel
+
+
+def test_conduction_over_two_gloo_ranks():
+    """The same through a world-size-2 gloo group: the scalars by all_reduce(SUM), the rows
+    by point-to-point messages."""
+    case, nsteps = "kh_hc_generic", 3
+    s, uh, um, hist = single_domain(case, nsteps)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=decomp_worker.rank_main, args=(r, 2, port, case, nsteps, q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        got = sorted((q.get(timeout=180) for _ in procs), key=lambda x: x[0])
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    for rank, st, dts, _, _ in got:
+        assert st == 0, (rank, st, dts)
+        assert np.allclose(np.array(dts), hist, rtol=1e-11, atol=0)
+    gh = decomp.gather(s, [g[3] for g in got])
+    gm = decomp.gather(s, [g[4] for g in got])
+    rel = max(np.abs(gh - uh).max() / np.abs(uh).max(), np.abs(gm - um).max() / np.abs(um).max())
+    assert rel <= 1e-11, rel

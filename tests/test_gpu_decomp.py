@@ -123,8 +123,9 @@ def test_decomposition_rejects(gpu_lib):
     s3, _, _ = ics.kelvin_helmholtz(16, 16, flag_heat=1, kapper=0.1)
     with capi.Context(s3) as c:
         with pytest.raises(capi.PipError) as e:
-            c.set_neighbors([-1, -1, 1, 1])          # conduction folds every side
+            c.set_neighbors([1, -1, -1, -1])         # conduction splits along y only
         assert e.value.code == capi.PIP_ERR_PARAM
+        c.set_neighbors([-1, -1, 1, 1])
 
 
 def device_loop_run(s, Uh, Um, world, nsteps, overlap=False):
@@ -195,3 +196,29 @@ def test_split_stage_enforces_its_order(gpu_lib):
         assert L.pip_dev_stage_split(c.h, 1, ctypes.byref(bs)) == capi.PIP_OK and bs.value
         assert L.pip_dev_stage_split(c.h, 2, ctypes.byref(bs)) == capi.PIP_OK
         c.dev_poll()
+
+
+@pytest.mark.parametrize("case,world", [("kh_hc", 2), ("kh_hc_generic", 1), ("kh_hc_generic", 2),
+                                        ("kh_hc_generic", 4)])
+def test_conduction_blocks_match_single_domain(gpu_lib, case, world):
+    """post_step's conduction of a decomposed run on device blocks (pip_hcd_*: BiCGstabMPI's
+    phases with global scalars, rows of r and Ap exchanged) against pip_run of the whole grid
+    and against the single-domain oracle.  The dot products group by block, so the iterates
+    agree to rounding; one block (no neighbours) conducts inside its stage, as pip_run."""
+    nsteps = 4
+    s, Uh, Um = make_case(case)
+    st, dts, gh, gm = device_run(s, Uh, Um, world, nsteps)
+    assert st == 0
+    with capi.Context(s) as c:
+        c.upload(Uh, Um)
+        st1, t1, n1 = c.run(nsteps)
+        h1, m1 = c.download()
+    assert abs(sum(dts) - t1) <= 1e-11 * t1
+    e = max(rel_l1(interior(gh, s), interior(h1, s)).max(), rel_l1(interior(gm, s), interior(m1, s)).max())
+    assert e <= 1e-11, e
+    o = O.Oracle(s, Uh, Um)
+    ost, ot, on, _ = o.run(nsteps=nsteps)
+    oh, om = o.state()
+    o.close()
+    e2 = max(rel_l1(interior(gh, s), interior(oh, s)).max(), rel_l1(interior(gm, s), interior(om, s)).max())
+    assert e2 <= 1e-10, e2
