@@ -153,7 +153,7 @@ PIP_HD void hllc_vjp(const double (&vl)[5], const double (&vr)[5], const double 
   const double sl = kHllcAcc * (sl_left ? vnl - csl : vnr - csr);
   const double sr = kHllcAcc * (sr_left ? vnl + csl : vnr + csr);
   const double ql = ul[0] * (sl - vnl), qr = ur[0] * (sr - vnr);
-  const double Nn = ur[1] * (sr - vnr) - ul[1] * (sl - vnl) + prl - prr;
+  const double Nn = mul_rn(ur[1], sr - vnr) - mul_rn(ul[1], sl - vnl) + prl - prr;
   const double Dd = qr - ql;
   const double sm = Nn / Dd;
   const double prm = sm * ql - ul[1] * (sl - vnl) + prl;
@@ -471,7 +471,7 @@ PIP_HD int hlld_vjp(const double (&vl)[8], const double (&vr)[8], const double (
     const double f1 = 1.0 / (sr - sl);
     double uh[8], w[8];
     for (int n = 0; n < 8; ++n) {
-      w[n] = sr * ur[n] - sl * ul[n] - fr[n] + fl[n];
+      w[n] = mul_rn(sr, ur[n]) - mul_rn(sl, ul[n]) - fr[n] + fl[n];
       uh[n] = f1 * w[n];
     }
     const double iuh0 = 1.0 / uh[0];

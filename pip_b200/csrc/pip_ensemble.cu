@@ -399,9 +399,10 @@ __device__ void run_member_2d(const KParams &p, float *Ahi, float *Alo, float *B
 
 // Persistent ensemble kernel: CTAs take runs from the queue until it is empty.  HAS2D: the
 // instance that can also step 2D members (its larger register footprint stays out of
-// ensembles of 1D members only).
+// ensembles of 1D members only).  The 1D instance of 256 threads is held to 128 registers,
+// two CTAs per SM, the configuration the tuner most often picks.
 template <int NT, bool HAS2D>
-__global__ void __launch_bounds__(NT) ensemble_kernel(const Member *mem, const KParams *kps,
+__global__ void __launch_bounds__(NT, (NT == 256 && !HAS2D) ? 2 : 1) ensemble_kernel(const Member *mem, const KParams *kps,
                                                       const int *order, int nmem, float *hi,
                                                       float *lo, float *U1, RunState *st,
                                                       unsigned *queue, double t_end,

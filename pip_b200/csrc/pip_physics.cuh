@@ -448,6 +448,27 @@ PIP_HD float rrsqrt(float a) {
 #endif
 }
 
+// A product the compiler may not fuse into an FMA.  At a mirror face (flag_bnd 2-7: the
+// ghost state is the interior state with vn, and Bn or the tangential pairs, negated) the
+// HLL averages sr*u_r - sl*u_l of the symmetric components cancel to exactly +0 only when
+// both products are rounded alone; fused, the residue is one product's rounding error of
+// either sign.  Its sign picks the L* or R* branch (sm) and sign(Bn), whose wall fluxes of
+// vt, Bt and e are equal and opposite, so a fused average flips them from step to step.
+PIP_HD double mul_rn(double a, double b) {
+#if defined(__CUDA_ARCH__)
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+PIP_HD float mul_rn(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+
 // HLLC smooth switch (|s|+s)/max(2s,eps) without a division: 1 for s >= eps/2, 0 for s<=0.
 template <typename R>
 PIP_HD R hllc_switch(R s) {
@@ -481,7 +502,7 @@ PIP_HD void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R g
   const R sl = R(kHllcAcc) * rmin(vn_l - cs_l, vn_r - cs_r);
   const R sr = R(kHllcAcc) * rmax(vn_l + cs_l, vn_r + cs_r);
   const R ql = u_l[0] * (sl - vn_l), qr = u_r[0] * (sr - vn_r);
-  const R sm = (u_r[1] * (sr - vn_r) - u_l[1] * (sl - vn_l) + pr_l - pr_r) / (qr - ql);
+  const R sm = (mul_rn(u_r[1], sr - vn_r) - mul_rn(u_l[1], sl - vn_l) + pr_l - pr_r) / (qr - ql);
   const R pr_m = sm * ql - u_l[1] * (sl - vn_l) + pr_l;
   const R il = R(1) / (sl - sm), ir = R(1) / (sr - sm);
   stl[0] = ql * il;
@@ -560,7 +581,7 @@ PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM
     f1 = R(1) / (sr - sl);
     R uh[8];
 #pragma unroll
-    for (int n = 0; n < 8; ++n) uh[n] = f1 * (sr * u_r[n] - sl * u_l[n] - fr[n] + fl[n]);
+    for (int n = 0; n < 8; ++n) uh[n] = f1 * (mul_rn(sr, u_r[n]) - mul_rn(sl, u_l[n]) - fr[n] + fl[n]);
     const R iuh0 = R(1) / uh[0];
     const R sm = uh[1] * iuh0;
     const R pt = pt_l + v_l[0] * (sl - v_l[1]) * (sm - v_l[1]);

@@ -86,6 +86,16 @@ def test_mixed_exponential_collisions(gpu_lib):
     assert err <= TOL_MIXED, (eh, em)
 
 
+@pytest.mark.parametrize("bnd", [[2, 2, 10, 10], [10, 10, 2, 2], [3, 4, 5, 6]])
+def test_mixed_mirror_walls(gpu_lib, bnd):
+    """Mirror faces: the FP32 HLL averages of vn and Bn must cancel to exactly zero there, as
+    in FP64, or the wall's tangential fluxes take the other side's sign."""
+    s, Uh, Um = ics.orszag_tang(48, flag_bnd=bnd + [1, 1], flag_divb=0)
+    a, b, eh, em = compare(s, Uh, Um, nsteps=40)
+    assert a[1] == b[1] == 40 and abs(a[0] - b[0]) <= 1e-5 * a[0]
+    assert max(eh.max(), em.max()) <= TOL_MIXED, (eh, em)
+
+
 def test_mixed_roundtrip_upload_download(gpu_lib):
     """upload splits FP64 into (hi, lo) and download joins it back to ~2^-48."""
     s, Uh, Um = ics.orszag_tang(40, precision=PIP_MIXED)
