@@ -598,13 +598,37 @@ def measure_conduction(nsteps=1000, kapper=0.01):
     return out
 
 
+# per-variable tables that the printed line carries as their largest entry only (the
+# --detail file keeps them whole), and the load-balance terms it leaves to that file
+PER_VARIABLE = ("per_variable", "l1_fp64_fma_vs_fma_free", "l1_mixed_vs_fp64")
+DETAIL_ONLY = ("busy_us", "ideal_makespan_us", "slots", "longest_run_us", "worst_member",
+               "check_s", "cell_updates", "samples", "samples_under_load", "loss",
+               "dloss_dcol", "checkpoint_every", "target_backward_over_forward",
+               "algorithmic_bytes_per_cell_iteration", "ms_per_step_without_conduction",
+               "bicgstab_iterations", "cell_updates_per_s", "step_achieved_gbs",
+               "hbm_floor_us_per_step", "checkpointed_forward_ms", "members_checked",
+               "max_rel_time_diff", "makespan_us", "after_steps", "bar")
+
+
 def compact(x, top=True):
     """The printed line: the descriptive strings ("how", "note", the sub-records'
-    "workload") dropped -- the module docstring describes each record -- and floats rounded
-    to 4 significant digits, so the whole line stays short."""
+    "workload") dropped -- the module docstring describes each record --, per-variable
+    tables cut to their largest entry, and floats rounded to 4 significant digits, so the
+    whole line stays short."""
     if isinstance(x, dict):
-        return {k: compact(v, False) for k, v in x.items()
-                if k not in ("how", "note") and not (k == "workload" and not top)}
+        out = {}
+        for k, v in x.items():
+            if k in ("how", "note") or (k == "workload" and not top) or k in DETAIL_ONLY:
+                continue
+            if not top and k == "gpu_launches" and v == 2 * x.get("steps", -1) + 1:
+                continue    # a variant's two launches per step and the final cfl
+            if (k in PER_VARIABLE and isinstance(v, dict) and len(v) >= 8 and
+                    all(isinstance(t, (int, float)) for t in v.values())):
+                name = max(v, key=lambda t: v[t])
+                out[k + "_max"] = {"var": name, "value": compact(float(v[name]), False)}
+                continue
+            out[k] = compact(v, False)
+        return out
     if isinstance(x, list):
         return [compact(v, False) for v in x]
     if isinstance(x, float):
