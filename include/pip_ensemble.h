@@ -9,6 +9,14 @@
  * walked in chunks of cells, a 2D run tile by tile (16 x 14 cells) with the single-run
  * stage kernel's tile step.  Per-run arithmetic is that of the single-run FP32-mixed form.
  * An ensemble with a 2D run needs at least 256 threads per block.
+ *
+ * Each launch first estimates every run's work (interior cells x the steps its current dt
+ * gives to the end) and orders the queue by it.  In an ensemble of 1D runs stepped by 256
+ * or 512 threads per block, the runs whose work exceeds a quarter of an even share are each
+ * shared by a thread-block cluster of 4 or 8 blocks (each block a contiguous part of the
+ * cells, the cluster barrier between stages, the dt reduced over the cluster); the rest
+ * go one per block.  A shared run takes the same steps as on one block; its state agrees
+ * to the rounding that FMA contraction gives each kernel instance.
  */
 #ifndef PIP_ENSEMBLE_H
 #define PIP_ENSEMBLE_H
@@ -41,12 +49,24 @@ int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *de
 int pip_ensemble_member(pip_ensemble *e, int member, double *U_h, double *U_m, double *time,
                         int64_t *steps, int *status);
 
-/* Load-balance record of the last launch: for every run, when a thread block took it from
- * the queue and when it finished, in microseconds of the device's global timer after the
- * earliest start (-1 for runs no launch has advanced); arrays of n.  slots: the thread
- * blocks the launch keeps resident (SMs x blocks per SM). */
+/* Load-balance record of the last launch: for every run, when a thread block (or cluster)
+ * took it from the queue and when it finished, in microseconds of the device's global timer
+ * after the earliest start (-1 for runs no launch has advanced); arrays of n.  slots: the
+ * thread blocks the launch keeps resident (SMs x blocks per SM, or resident clusters x
+ * cluster size). */
 int pip_ensemble_timings(pip_ensemble *e, double *start_us, double *end_us);
 int pip_ensemble_slots(pip_ensemble *e, int *slots);
+/* The thread blocks that stepped each run in the last launch that advanced it (1, or the
+ * cluster size for a shared run; 0 for runs no launch has advanced); array of n. */
+int pip_ensemble_blocks(pip_ensemble *e, int *blocks);
+
+/* Cluster sharing of long runs: 0 (default) chosen at each launch from the work estimate,
+ * 1 off, 4 or 8 blocks per cluster; a run is shared when its work exceeds `share` (default
+ * 0.25) times an even share of the total (PIP_ERR_PARAM with a 2D run, with 128 or 1024
+ * threads per block, or share <= 0).  pip_ensemble_plan reports the last launch's choice:
+ * cluster size (1: none), runs shared, blocks launched. */
+int pip_ensemble_set_cluster(pip_ensemble *e, int cluster, double share);
+int pip_ensemble_plan(pip_ensemble *e, int *cluster, int *shared_runs, int *grid);
 
 /* Launch configuration: threads per block (128, 256, 512, 1024; not 128 when a run is 2D)
  * and blocks per SM. */

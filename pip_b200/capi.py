@@ -47,7 +47,8 @@ EXPORTS = (
     # include/pip_ensemble.h
     "pip_ensemble_create", "pip_ensemble_destroy", "pip_ensemble_upload", "pip_ensemble_run",
     "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
-    "pip_ensemble_timings", "pip_ensemble_slots",
+    "pip_ensemble_timings", "pip_ensemble_slots", "pip_ensemble_blocks",
+    "pip_ensemble_set_cluster", "pip_ensemble_plan",
     # include/pip_adjoint.h
     "pip_adj_create", "pip_adj_destroy", "pip_adj_set_col", "pip_adj_forward",
     "pip_adj_backward", "pip_adj_dt", "pip_adj_stage_vjp", "pip_adj_fold",
@@ -159,6 +160,9 @@ def lib(path: Optional[str] = None):
     L.pip_ensemble_tune.argtypes = [vp, d, P(i), P(i), P(ctypes.c_float)]
     L.pip_ensemble_timings.argtypes = [vp, dp, dp]
     L.pip_ensemble_slots.argtypes = [vp, P(i)]
+    L.pip_ensemble_blocks.argtypes = [vp, P(i)]
+    L.pip_ensemble_set_cluster.argtypes = [vp, i, d]
+    L.pip_ensemble_plan.argtypes = [vp, P(i), P(i), P(i)]
     L.pip_adj_create.argtypes = [P(PipParams), ctypes.c_int64, i, P(vp)]
     L.pip_adj_destroy.argtypes = [vp]
     L.pip_adj_destroy.restype = None
@@ -170,7 +174,8 @@ def lib(path: Optional[str] = None):
     L.pip_adj_fold.argtypes = [vp, vp]
     for name in ("pip_ensemble_create", "pip_ensemble_upload", "pip_ensemble_run",
                  "pip_ensemble_member", "pip_ensemble_set_config", "pip_ensemble_tune",
-                 "pip_ensemble_timings", "pip_ensemble_slots"):
+                 "pip_ensemble_timings", "pip_ensemble_slots", "pip_ensemble_blocks",
+                 "pip_ensemble_set_cluster", "pip_ensemble_plan"):
         getattr(L, name).restype = i
     L.pip_kernels_per_run.restype = ctypes.c_int64
     for name in ("pip_upload", "pip_download", "pip_cfl", "pip_step", "pip_run", "pip_set_time",

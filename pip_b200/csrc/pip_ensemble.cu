@@ -12,6 +12,7 @@
 // Packed storage: member r's planes start at off[r] floats in three arrays (hi, lo, U1),
 // NV = 13 planes of ix_r floats each.  A run's KParams (with its dx tables) sits in a
 // device array.  The launch (queue reset + persistent kernel) is captured in a CUDA graph.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,7 +45,7 @@ struct RunState {
   double time, dt;
   long long steps;
   int status;         // 0, PIP_ERR_NAN (3) or PIP_ERR_DT (4)
-  int pad;
+  int blocks;         // thread blocks that stepped it in the last launch that advanced it
   unsigned long long t_start, t_end;  // device global timer (ns) when the last launch that
                                       // advanced the run took it from the queue and left it
 };
@@ -88,21 +89,82 @@ __device__ __forceinline__ void block_minmax(double &dtc, double &rho, double &g
   }
 }
 
+// Barrier of the CTAs that share a member: the cluster barrier (arrive.release /
+// wait.acquire at cluster scope, so the global writes of one CTA's cells and ghosts before
+// it are seen by the others after it), or the block barrier when one CTA owns the member.
+template <int CL>
+__device__ __forceinline__ void member_sync() {
+  if constexpr (CL > 1) cooperative_groups::this_cluster().sync();
+  else __syncthreads();
+}
+
+// The CFL terms and the NaN flag of a member shared by the CL CTAs of a cluster: each CTA's
+// block result goes to its slot in its own shared memory, and after the cluster barrier
+// every CTA reads all CL slots through distributed shared memory and reduces them in rank
+// order (min and max are exact, so every CTA, and a one-CTA run, gets the same dt).  A slot
+// is written again only after the next member_sync, when every CTA has read it.
+template <int CL>
+__device__ __forceinline__ void cluster_minmax(double &dtc, double &rho, double &gr, int &bad,
+                                               double *s_slot, double *s_res) {
+  if constexpr (CL > 1) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x == 0) {
+      s_slot[0] = dtc;
+      s_slot[1] = rho;
+      s_slot[2] = gr;
+      s_slot[3] = bad ? 1.0 : 0.0;
+    }
+    cl.sync();
+    if (threadIdx.x < 32) {
+      const int k = threadIdx.x;
+      double d = 10.0, r = 0.0, g = 0.0, b = 0.0;
+      if (k < CL) {
+        const double *q = cl.map_shared_rank(s_slot, k);
+        d = q[0];
+        r = q[1];
+        g = q[2];
+        b = q[3];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        d = fmin(d, __shfl_xor_sync(0xffffffffu, d, o));
+        r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+        g = fmax(g, __shfl_xor_sync(0xffffffffu, g, o));
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+      }
+      if (k == 0) {
+        s_res[0] = d;
+        s_res[1] = r;
+        s_res[2] = g;
+        s_res[3] = b;
+      }
+    }
+    __syncthreads();
+    dtc = s_res[0];
+    rho = s_res[1];
+    gr = s_res[2];
+    bad = s_res[3] != 0.0;
+    __syncthreads();   // s_res is rewritten by the next reduction
+  }
+}
+
 // One RK stage of a member (the 1D mixed stage kernel's arithmetic, chunk by chunk).
 // Returns, for stage 2 with ep == 2, this thread's CFL terms of the next step.
+// Cells [cbeg, cend) of the interior: all of it for a member one CTA owns, this CTA's part
+// of it for a member a cluster shares.
 template <int NT, int STAGE>
 __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *Alo, float *Bf,
                           double dt, int ep, float *sV, float *sF, double &dtc, double &rhoc,
-                          double &grc, int &bad) {
+                          double &grc, int &bad, int cbeg, int iend) {
   constexpr int CN = NT - 1;          // cells per chunk
   constexpr int RX = CN + 2 * kH;     // region cells
   const int tid = threadIdx.x;
   const long long nc = p.nc;
   const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
   const float igm1f = (float)p.igm1;
-  const int iend = p.m0 + p.nx;
   float *Ohi = STAGE == 1 ? Bf : Ahi;
-  for (int c0 = p.m0; c0 < iend; c0 += CN) {
+  for (int c0 = cbeg; c0 < iend; c0 += CN) {
     const int cn = min(CN, iend - c0);
     // primitives of the chunk and its halo
     for (int idx = tid; idx < cn + 2 * kH; idx += NT) {
@@ -397,26 +459,156 @@ __device__ void run_member_2d(const KParams &p, float *Ahi, float *Alo, float *B
   }
 }
 
+// A 1D member advanced to the end time by CL CTAs (CL = 1: one CTA owns it; CL > 1: the
+// CTAs of a thread-block cluster, rank `rank`, each stepping a contiguous 1/CL of the
+// interior and meeting at the cluster barrier after each stage).  The cells' arithmetic
+// and the reductions are the same for every CL, so a shared member takes the steps a
+// member one CTA owns takes, its state equal up to the FMA contraction of each instance.
+// Not inlined: the cluster kernels call the same one-CTA runner as the plain kernels, so
+// their unshared runs keep its register allocation (inlined next to the shared runner they
+// ran 10% slower per step).
+template <int NT, int CL>
+__device__ __noinline__ void run_member_1d(const KParams &p, float *Ahi, float *Alo, float *B,
+                                           RunState &rs, double t_end, long long max_steps,
+                                           float *sV, float *sF, double *s_red, double *s_slot,
+                                           double *s_res, int rank) {
+  const int tid = threadIdx.x;
+  const long long nc = p.nc;
+  // cfl of the first step: floors of every cell (cq2pv, Scheme_rot.f90:132-179) and the
+  // CFL terms (the mixed cfl kernel's arithmetic)
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  for (int i = rank * NT + tid; i < p.ix; i += NT * CL) {
+    double um[NVM], uh[5];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) um[n] = (double)Ahi[i + n * nc] + (double)Alo[i + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uh[n] = (double)Ahi[i + (NVM + n) * nc] + (double)Alo[i + (NVM + n) * nc];
+    mixed::floors_mhd<NVM>(um, p);
+    mixed::floors_hd(uh, p);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      float h = (float)um[n];
+      Ahi[i + n * nc] = h;
+      Alo[i + n * nc] = (float)(um[n] - (double)h);
+      h = (float)uh[n];
+      Ahi[i + (NVM + n) * nc] = h;
+      Alo[i + (NVM + n) * nc] = (float)(uh[n] - (double)h);
+    }
+    if (i >= p.m0 && i < p.ix - p.m0) {
+      float fm[NVM], fh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) fm[n] = (float)um[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
+      const Prim<float> qm = cq2pv_mhd<float, NVM>(fm, gmf, rolf, prlf);
+      const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
+      const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[0]), p.dz0));
+      dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
+                                    cfl_hd_cell<float>(qh, gmf, sg)));
+    }
+    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (p.ir) {
+      double g1, g2;
+      mixed::ir_rates<NVM>(um, p, g1, g2);
+      grc = fmax(grc, fmax(g1, g2));
+    }
+  }
+  block_minmax<NT>(dtc, rhoc, grc, s_red);
+  int bad = 0;
+  cluster_minmax<CL>(dtc, rhoc, grc, bad, s_slot, s_res);
+  double dt = finalize_dt(p, dtc, rhoc, grc);
+  // the prologue's PIPbnd after its cfl (Initial_rot.f90:152-159)
+  __syncthreads();
+  for (int i = p.m0 + rank * NT + tid; i < p.ix - p.m0; i += NT * CL)
+    if (mixed::near_boundary<1>(p, i, 0)) mixed::write_ghosts<1>(p, i, 0, Ahi, Alo, NVM + 5);
+  member_sync<CL>();
+  const int per = (p.nx + CL - 1) / CL;
+  const int cb = p.m0 + min(p.nx, rank * per), ce = p.m0 + min(p.nx, (rank + 1) * per);
+  // the time loop (main.f90:31-68) of this run
+  for (;;) {
+    const double tn = rs.time + dt;
+    const bool last = (t_end > 0.0 && tn >= t_end) || (max_steps > 0 && rs.steps + 1 >= max_steps);
+    double d1 = 10.0, r1 = 0.0, g1 = 0.0;
+    run_stage<NT, 1>(p, Ahi, Ahi, Alo, B, dt, 0, sV, sF, d1, r1, g1, bad, cb, ce);
+    if constexpr (CL > 1) member_sync<CL>();   // stage 2 reads the others' stage-1 cells
+    double d2 = 10.0, r2 = 0.0, g2 = 0.0;
+    run_stage<NT, 2>(p, B, Ahi, Alo, B, dt, last ? 1 : 2, sV, sF, d2, r2, g2, bad, cb, ce);
+    rs.time = tn;
+    rs.steps += 1;
+    rs.dt = dt;
+    int anybad = __syncthreads_or(bad);
+    if constexpr (CL > 1) {
+      // one exchange per step carries the next dt and the NaN flag; its barrier also
+      // orders this step's stage-2 writes before the next step's stage 1
+      block_minmax<NT>(d2, r2, g2, s_red);
+      cluster_minmax<CL>(d2, r2, g2, anybad, s_slot, s_res);
+    }
+    if (anybad) {
+      rs.status = 3;  // PIP_ERR_NAN
+      break;
+    }
+    if (dt <= 1.0e-12) {
+      rs.status = 4;  // PIP_ERR_DT
+      break;
+    }
+    if (last) break;
+    if constexpr (CL == 1) block_minmax<NT>(d2, r2, g2, s_red);
+    dt = finalize_dt(p, d2, r2, g2);
+  }
+}
+
 // Persistent ensemble kernel: CTAs take runs from the queue until it is empty.  HAS2D: the
 // instance that can also step 2D members (its larger register footprint stays out of
 // ensembles of 1D members only).  The 1D instance of 256 threads is held to 128 registers,
 // two CTAs per SM, the configuration the tuner most often picks.
-template <int NT, bool HAS2D>
-__global__ void __launch_bounds__(NT, (NT == 256 && !HAS2D) ? 2 : 1) ensemble_kernel(const Member *mem, const KParams *kps,
-                                                      const int *order, int nmem, float *hi,
-                                                      float *lo, float *U1, RunState *st,
-                                                      unsigned *queue, double t_end,
-                                                      long long max_steps) {
+//
+// CL > 1 (1D members only): the grid is made of clusters of CL CTAs.  The first nbig entries
+// of the queue order (the runs estimated longest) are taken a cluster at a time, rank 0
+// drawing from queue[1] and the cluster sharing the run; once they are gone every CTA
+// takes the remaining runs alone from queue[0], as with CL = 1.
+template <int NT, bool HAS2D, int CL>
+__global__ void __launch_bounds__(NT, (NT == 256 && !HAS2D) ? 2 : 1)
+    ensemble_kernel(const Member *mem, const KParams *kps, const int *order, int nmem, int nbig,
+                    float *hi, float *lo, float *U1, RunState *st, unsigned *queue,
+                    double t_end, long long max_steps) {
   constexpr int CN = NT - 1, RX = CN + 2 * kH;
   extern __shared__ float smem[];
   float *sV = smem;
   float *sF = sV + NV * RX;
   __shared__ double s_red[3 * (NT / 32)];
+  __shared__ double s_slot[4], s_res[4];
   __shared__ KParams sp;
   __shared__ int s_r;
   const int tid = threadIdx.x;
+  if constexpr (CL > 1) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    for (;;) {
+      if (rank == 0 && tid == 0) s_r = (int)atomicAdd(queue + 1, 1u);
+      cl.sync();
+      const int rq = *cl.map_shared_rank(&s_r, 0);
+      cl.sync();   // read by all before rank 0 draws again or leaves
+      if (rq >= nbig) break;
+      const int r = order[rq];
+      if (tid == 0) sp = kps[mem[r].kp];
+      __syncthreads();
+      const KParams &p = sp;
+      RunState rs = st[r];
+      if (rs.status == 0 && !(t_end > 0.0 && rs.time >= t_end)) {
+        rs.t_start = global_ns();
+        rs.blocks = CL;
+        run_member_1d<NT, CL>(p, hi + mem[r].off, lo + mem[r].off, U1 + mem[r].off, rs, t_end,
+                              max_steps, sV, sF, s_red, s_slot, s_res, rank);
+        rs.t_end = global_ns();
+        if (rank == 0 && tid == 0) st[r] = rs;
+      }
+      __syncthreads();
+    }
+  }
   for (;;) {
-    if (tid == 0) s_r = (int)atomicAdd(queue, 1u);
+    if (tid == 0) s_r = nbig + (int)atomicAdd(queue, 1u);
     __syncthreads();
     const int rq = s_r;
     if (rq >= nmem) return;
@@ -424,7 +616,6 @@ __global__ void __launch_bounds__(NT, (NT == 256 && !HAS2D) ? 2 : 1) ensemble_ke
     if (tid == 0) sp = kps[mem[r].kp];
     __syncthreads();
     const KParams &p = sp;
-    const long long nc = p.nc;
     float *Ahi = hi + mem[r].off, *Alo = lo + mem[r].off, *B = U1 + mem[r].off;
     RunState rs = st[r];
     if (rs.status != 0 || (t_end > 0.0 && rs.time >= t_end)) {
@@ -432,88 +623,15 @@ __global__ void __launch_bounds__(NT, (NT == 256 && !HAS2D) ? 2 : 1) ensemble_ke
       continue;
     }
     rs.t_start = global_ns();
+    rs.blocks = 1;
     if (HAS2D && p.ndim == 2) {
       // (the host allows 2D members only with NT >= TX2 * TY2 threads)
       if (NT >= TX2 * TY2) {
         if (p.nvm == 9) run_member_2d<NT, 9>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
         else run_member_2d<NT, 8>(p, Ahi, Alo, B, rs, t_end, max_steps, smem, s_red);
       }
-      rs.t_end = global_ns();
-      if (tid == 0) st[r] = rs;
-      __syncthreads();
-      continue;
-    }
-    // cfl of the first step: floors of every cell (cq2pv, Scheme_rot.f90:132-179) and the
-    // CFL terms (the mixed cfl kernel's arithmetic)
-    double dtc = 10.0, rhoc = 0.0, grc = 0.0;
-    const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
-    for (int i = tid; i < p.ix; i += NT) {
-      double um[NVM], uh[5];
-#pragma unroll
-      for (int n = 0; n < NVM; ++n) um[n] = (double)Ahi[i + n * nc] + (double)Alo[i + n * nc];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) uh[n] = (double)Ahi[i + (NVM + n) * nc] + (double)Alo[i + (NVM + n) * nc];
-      mixed::floors_mhd<NVM>(um, p);
-      mixed::floors_hd(uh, p);
-#pragma unroll
-      for (int n = 0; n < 5; ++n) {
-        float h = (float)um[n];
-        Ahi[i + n * nc] = h;
-        Alo[i + n * nc] = (float)(um[n] - (double)h);
-        h = (float)uh[n];
-        Ahi[i + (NVM + n) * nc] = h;
-        Alo[i + (NVM + n) * nc] = (float)(uh[n] - (double)h);
-      }
-      if (i >= p.m0 && i < p.ix - p.m0) {
-        float fm[NVM], fh[5];
-#pragma unroll
-        for (int n = 0; n < NVM; ++n) fm[n] = (float)um[n];
-#pragma unroll
-        for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
-        const Prim<float> qm = cq2pv_mhd<float, NVM>(fm, gmf, rolf, prlf);
-        const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
-        const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[0]), p.dz0));
-        dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
-                                      cfl_hd_cell<float>(qh, gmf, sg)));
-      }
-      rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
-      if (p.ir) {
-        double g1, g2;
-        mixed::ir_rates<NVM>(um, p, g1, g2);
-        grc = fmax(grc, fmax(g1, g2));
-      }
-    }
-    block_minmax<NT>(dtc, rhoc, grc, s_red);
-    double dt = finalize_dt(p, dtc, rhoc, grc);
-    // the prologue's PIPbnd after its cfl (Initial_rot.f90:152-159)
-    __syncthreads();
-    for (int i = p.m0 + tid; i < p.ix - p.m0; i += NT)
-      if (mixed::near_boundary<1>(p, i, 0)) mixed::write_ghosts<1>(p, i, 0, Ahi, Alo, NVM + 5);
-    __syncthreads();
-    int bad = 0;
-    // the time loop (main.f90:31-68) of this run
-    for (;;) {
-      const double tn = rs.time + dt;
-      const bool last = (t_end > 0.0 && tn >= t_end) || (max_steps > 0 && rs.steps + 1 >= max_steps);
-      double d1 = 10.0, r1 = 0.0, g1 = 0.0;
-      run_stage<NT, 1>(p, Ahi, Ahi, Alo, B, dt, 0, sV, sF, d1, r1, g1, bad);
-      double d2 = 10.0, r2 = 0.0, g2 = 0.0;
-      run_stage<NT, 2>(p, B, Ahi, Alo, B, dt, last ? 1 : 2, sV, sF, d2, r2, g2, bad);
-      rs.time = tn;
-      rs.steps += 1;
-      rs.dt = dt;
-      const int anybad = __syncthreads_or(bad);
-      if (anybad) {
-        rs.status = 3;  // PIP_ERR_NAN
-        break;
-      }
-      if (dt <= 1.0e-12) {
-        rs.status = 4;  // PIP_ERR_DT
-        break;
-      }
-      if (last) break;
-      block_minmax<NT>(d2, r2, g2, s_red);
-      dt = finalize_dt(p, d2, r2, g2);
+    } else {
+      run_member_1d<NT, 1>(p, Ahi, Alo, B, rs, t_end, max_steps, sV, sF, s_red, s_slot, s_res, 0);
     }
     rs.t_end = global_ns();
     if (tid == 0) st[r] = rs;
@@ -528,17 +646,109 @@ constexpr size_t smem_bytes(int nt, bool has2d) {
   return has2d && smem_2d<9>() > smem_1d(nt) ? smem_2d<9>() : smem_1d(nt);
 }
 
-cudaError_t launch(int nt, bool has2d, int grid, cudaStream_t s, const Member *mem,
-                   const KParams *kps, const int *order, int nmem, float *hi, float *lo,
+// Initial dt of each run from its current state (the prologue's cfl terms without its
+// floors' writes), one CTA per run: the work estimate (interior cells x remaining steps)
+// that orders the queue and picks the runs a cluster shares.
+template <int NT>
+__global__ void __launch_bounds__(NT) dt0_kernel(const Member *mem, const KParams *kps,
+                                                 const float *hi, const float *lo, double *dt0) {
+  __shared__ double s_red[3 * (NT / 32)];
+  const KParams &p = kps[mem[blockIdx.x].kp];
+  const float *Ahi = hi + mem[blockIdx.x].off, *Alo = lo + mem[blockIdx.x].off;
+  const long long nc = p.nc;
+  const int nvm = p.nvm;
+  const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
+  double dtc = 10.0, rhoc = 0.0, grc = 0.0;
+  for (long long q = threadIdx.x; q < nc; q += NT) {
+    double um[NVM], uh[5];
+#pragma unroll
+    for (int n = 0; n < NVM; ++n) um[n] = (double)Ahi[q + n * nc] + (double)Alo[q + n * nc];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) uh[n] = (double)Ahi[q + (nvm + n) * nc] + (double)Alo[q + (nvm + n) * nc];
+    mixed::floors_mhd<NVM>(um, p);
+    mixed::floors_hd(uh, p);
+    const int i = (int)(q % p.ix), j = (int)(q / p.ix);
+    const bool inner = i >= p.m0 && i < p.ix - p.m0 &&
+                       (p.ndim == 1 || (j >= p.m1 && j < p.jx - p.m1));
+    if (inner) {
+      float fm[NVM], fh[5];
+#pragma unroll
+      for (int n = 0; n < NVM; ++n) fm[n] = (float)um[n];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) fh[n] = (float)uh[n];
+      const Prim<float> qm = cq2pv_mhd<float, NVM>(fm, gmf, rolf, prlf);
+      const Prim<float> qh = cq2pv_hd<float>(fh, gmf, rolf, prlf);
+      const float sg = (float)(p.safety * fmin(fmin(p.dx[i], p.dy[p.ndim == 2 ? j : 0]), p.dz0));
+      dtc = fmin(dtc, (double)fminf(cfl_mhd_cell<float>(qm, fm[5], fm[6], fm[7], gmf, sg),
+                                    cfl_hd_cell<float>(qh, gmf, sg)));
+    }
+    rhoc = fmax(rhoc, fmax(um[0] * p.ac, uh[0] * p.ac));
+    if (p.ir) {
+      double g1, g2;
+      mixed::ir_rates<NVM>(um, p, g1, g2);
+      grc = fmax(grc, fmax(g1, g2));
+    }
+  }
+  block_minmax<NT>(dtc, rhoc, grc, s_red);
+  if (threadIdx.x == 0) dt0[blockIdx.x] = finalize_dt(p, dtc, rhoc, grc);
+}
+
+cudaError_t launch_dt0(int n, cudaStream_t s, const Member *mem, const KParams *kps,
+                       const float *hi, const float *lo, double *dt0) {
+  dt0_kernel<256><<<n, 256, 0, s>>>(mem, kps, hi, lo, dt0);
+  return cudaGetLastError();
+}
+
+// Launch configuration of a cluster instance (CL CTAs per cluster along x).
+template <int NT, int CL>
+cudaLaunchConfig_t cluster_config(int grid, cudaStream_t s, cudaLaunchAttribute *at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid, 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
+  cfg.dynamicSmemBytes = smem_bytes(NT, false);
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <int NT, int CL>
+cudaError_t launch_cluster(int grid, cudaStream_t s, const Member *mem, const KParams *kps,
+                           const int *order, int nmem, int nbig, float *hi, float *lo, float *U1,
+                           RunState *st, unsigned *queue, double t_end, long long max_steps) {
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cluster_config<NT, CL>(grid, s, at);
+  return cudaLaunchKernelEx(&cfg, ensemble_kernel<NT, false, CL>, mem, kps, order, nmem, nbig,
+                            hi, lo, U1, st, queue, t_end, max_steps);
+}
+
+cudaError_t launch(int nt, bool has2d, int cl, int grid, cudaStream_t s, const Member *mem,
+                   const KParams *kps, const int *order, int nmem, int nbig, float *hi, float *lo,
                    float *U1, RunState *st, unsigned *queue, double t_end, long long max_steps) {
+  if (cl > 1) {
+    if (has2d) return cudaErrorInvalidValue;
+    if (nt == 256 && cl == 4)
+      return launch_cluster<256, 4>(grid, s, mem, kps, order, nmem, nbig, hi, lo, U1, st, queue, t_end, max_steps);
+    if (nt == 256 && cl == 8)
+      return launch_cluster<256, 8>(grid, s, mem, kps, order, nmem, nbig, hi, lo, U1, st, queue, t_end, max_steps);
+    if (nt == 512 && cl == 4)
+      return launch_cluster<512, 4>(grid, s, mem, kps, order, nmem, nbig, hi, lo, U1, st, queue, t_end, max_steps);
+    if (nt == 512 && cl == 8)
+      return launch_cluster<512, 8>(grid, s, mem, kps, order, nmem, nbig, hi, lo, U1, st, queue, t_end, max_steps);
+    return cudaErrorInvalidValue;
+  }
 #define PIP_ENS_CASE(NTV)                                                                      \
   case NTV:                                                                                    \
     if (has2d)                                                                                 \
-      ensemble_kernel<NTV, true><<<grid, NTV, smem_bytes(NTV, true), s>>>(                     \
-          mem, kps, order, nmem, hi, lo, U1, st, queue, t_end, max_steps);                     \
+      ensemble_kernel<NTV, true, 1><<<grid, NTV, smem_bytes(NTV, true), s>>>(                  \
+          mem, kps, order, nmem, 0, hi, lo, U1, st, queue, t_end, max_steps);                  \
     else                                                                                       \
-      ensemble_kernel<NTV, false><<<grid, NTV, smem_bytes(NTV, false), s>>>(                   \
-          mem, kps, order, nmem, hi, lo, U1, st, queue, t_end, max_steps);                     \
+      ensemble_kernel<NTV, false, 1><<<grid, NTV, smem_bytes(NTV, false), s>>>(                \
+          mem, kps, order, nmem, 0, hi, lo, U1, st, queue, t_end, max_steps);                  \
     break;
   switch (nt) {
     PIP_ENS_CASE(128)
@@ -551,9 +761,9 @@ cudaError_t launch(int nt, bool has2d, int grid, cudaStream_t s, const Member *m
   return cudaGetLastError();
 }
 
-template <int NT, bool HAS2D>
+template <int NT, bool HAS2D, int CL = 1>
 cudaError_t set_smem() {
-  return cudaFuncSetAttribute(ensemble_kernel<NT, HAS2D>,
+  return cudaFuncSetAttribute(ensemble_kernel<NT, HAS2D, CL>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem_bytes(NT, HAS2D));
 }
@@ -563,7 +773,9 @@ cudaError_t prepare() {
   if ((e = set_smem<128, false>()) != cudaSuccess || (e = set_smem<256, false>()) != cudaSuccess ||
       (e = set_smem<512, false>()) != cudaSuccess || (e = set_smem<1024, false>()) != cudaSuccess ||
       (e = set_smem<256, true>()) != cudaSuccess || (e = set_smem<512, true>()) != cudaSuccess ||
-      (e = set_smem<1024, true>()) != cudaSuccess)
+      (e = set_smem<1024, true>()) != cudaSuccess || (e = set_smem<256, false, 4>()) != cudaSuccess ||
+      (e = set_smem<256, false, 8>()) != cudaSuccess || (e = set_smem<512, false, 4>()) != cudaSuccess ||
+      (e = set_smem<512, false, 8>()) != cudaSuccess)
     return e;
   return cudaSuccess;
 }
@@ -572,7 +784,7 @@ template <int NT, bool HAS2D>
 int occupancy() {
   int n = 0;
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &n, ensemble_kernel<NT, HAS2D>, NT, smem_bytes(NT, HAS2D));
+      &n, ensemble_kernel<NT, HAS2D, 1>, NT, smem_bytes(NT, HAS2D));
   return e == cudaSuccess ? n : 0;
 }
 
@@ -584,6 +796,24 @@ int max_ctas_per_sm(int nt, bool has2d) {
     case 1024: return has2d ? occupancy<1024, true>() : occupancy<1024, false>();
     default: return 0;
   }
+}
+
+template <int NT, int CL>
+int cluster_count() {
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cluster_config<NT, CL>(CL, nullptr, at);
+  int n = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveClusters(&n, ensemble_kernel<NT, false, CL>, &cfg);
+  return e == cudaSuccess ? n : 0;
+}
+
+// Clusters of CL CTAs of nt threads the device keeps resident at once (0: no such instance).
+int max_clusters(int nt, int cl) {
+  if (nt == 256 && cl == 4) return cluster_count<256, 4>();
+  if (nt == 256 && cl == 8) return cluster_count<256, 8>();
+  if (nt == 512 && cl == 4) return cluster_count<512, 4>();
+  if (nt == 512 && cl == 8) return cluster_count<512, 8>();
+  return 0;
 }
 
 }  // namespace ens
@@ -613,11 +843,16 @@ struct pip_ensemble {
   RunState *d_st = nullptr;
   unsigned *d_queue = nullptr;
   int threads = 256, ctas_per_sm = 2;
+  int cluster = 0;                                // 0: chosen per launch, 1: off, 4 or 8
+  double share = 0.25;                            // shared: work above share x an even share
   bool has2d = false;                             // some member is 2D
+  double *d_dt0 = nullptr;                        // each run's initial dt (work estimate)
+  std::vector<int> order;                         // queue order of the last launch
+  int cl = 1, nbig = 0, grid = 0;                 // cluster size, shared runs, CTAs launched
   cudaGraphExec_t graph = nullptr;
   double graph_t_end = -1.0;
   long long graph_steps = -1;
-  int graph_threads = 0, graph_ctas = 0;
+  int graph_threads = 0, graph_ctas = 0, graph_cl = 0, graph_nbig = -1, graph_grid = 0;
 };
 
 #define EK(call)                        \
@@ -717,9 +952,11 @@ int pip_ensemble_create(const pip_params *members, int n, pip_ensemble **out) {
   if ((c = cudaMalloc(&e->d_order, sizeof(int) * n)) != cudaSuccess) return fail(c);
   if ((c = cudaMemcpy(e->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice)) != cudaSuccess)
     return fail(c);
+  e->order = order;
   if ((c = cudaMalloc(&e->d_st, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
   if ((c = cudaMemset(e->d_st, 0, sizeof(RunState) * n)) != cudaSuccess) return fail(c);
-  if ((c = cudaMalloc(&e->d_queue, sizeof(unsigned))) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->d_queue, 2 * sizeof(unsigned))) != cudaSuccess) return fail(c);
+  if ((c = cudaMalloc(&e->d_dt0, sizeof(double) * n)) != cudaSuccess) return fail(c);
   long long maxst = 0;
   for (int r = 0; r < n; ++r)
     maxst = std::max(maxst, (long long)(members[r].nvar_m + 5) * members[r].ix * members[r].jx);
@@ -744,6 +981,7 @@ void pip_ensemble_destroy(pip_ensemble *e) {
   cudaFree(e->d_order);
   cudaFree(e->d_st);
   cudaFree(e->d_queue);
+  cudaFree(e->d_dt0);
   cudaFree(e->stage64);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -805,9 +1043,37 @@ int pip_ensemble_timings(pip_ensemble *e, double *start_us, double *end_us) {
   return PIP_OK;
 }
 
+int pip_ensemble_blocks(pip_ensemble *e, int *blocks) {
+  if (!e || !blocks) return PIP_ERR_NULL;
+  EK(cudaSetDevice(e->device));
+  std::vector<RunState> all((size_t)e->n);
+  EK(cudaMemcpyAsync(all.data(), e->d_st, sizeof(RunState) * e->n, cudaMemcpyDeviceToHost, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  for (int m = 0; m < e->n; ++m) blocks[m] = all[(size_t)m].t_end == 0 ? 0 : all[(size_t)m].blocks;
+  return PIP_OK;
+}
+
 int pip_ensemble_slots(pip_ensemble *e, int *slots) {
   if (!e || !slots) return PIP_ERR_NULL;
-  *slots = e->sms * e->ctas_per_sm;
+  *slots = e->grid > 0 ? e->grid : e->sms * e->ctas_per_sm;
+  return PIP_OK;
+}
+
+int pip_ensemble_set_cluster(pip_ensemble *e, int cluster, double share) {
+  if (!e) return PIP_ERR_NULL;
+  if (cluster != 0 && cluster != 1 && cluster != 4 && cluster != 8) return PIP_ERR_PARAM;
+  if (cluster > 1 && (e->has2d || (e->threads != 256 && e->threads != 512))) return PIP_ERR_PARAM;
+  if (!(share > 0.0)) return PIP_ERR_PARAM;
+  e->cluster = cluster;
+  e->share = share;
+  return PIP_OK;
+}
+
+int pip_ensemble_plan(pip_ensemble *e, int *cluster, int *shared_runs, int *grid) {
+  if (!e) return PIP_ERR_NULL;
+  if (cluster) *cluster = e->cl;
+  if (shared_runs) *shared_runs = e->nbig;
+  if (grid) *grid = e->grid;
   return PIP_OK;
 }
 
@@ -823,10 +1089,67 @@ int pip_ensemble_set_config(pip_ensemble *e, int threads, int ctas_per_sm) {
 }
 
 static int ens_enqueue(pip_ensemble *e, double t_end, long long max_steps) {
-  EK(cudaMemsetAsync(e->d_queue, 0, sizeof(unsigned), e->stream));
-  EK(pip::ens::launch(e->threads, e->has2d, e->sms * e->ctas_per_sm, e->stream, e->d_mem, e->d_kp,
-                      e->d_order,
-                      e->n, e->hi, e->lo, e->U1, e->d_st, e->d_queue, t_end, max_steps));
+  EK(cudaMemsetAsync(e->d_queue, 0, 2 * sizeof(unsigned), e->stream));
+  EK(pip::ens::launch(e->threads, e->has2d, e->cl, e->grid, e->stream, e->d_mem, e->d_kp,
+                      e->d_order, e->n, e->nbig, e->hi, e->lo, e->U1, e->d_st, e->d_queue, t_end,
+                      max_steps));
+  return PIP_OK;
+}
+
+// Work estimate and queue order of a launch: each run's interior cells x the steps its
+// initial dt gives to the end (a step limit caps it), runs in decreasing order.  With
+// clusters (1D ensembles of 256 or 512 threads) the runs above `share` (default 0.25) of an
+// even share of the total work are shared by a cluster each: 4 CTAs, or 8 when the longest
+// run exceeds 4 even shares.  cluster = 1 keeps every run on one CTA.
+static int ens_plan(pip_ensemble *e, double t_end, long long max_steps) {
+  const int n = e->n;
+  EK(pip::ens::launch_dt0(n, e->stream, e->d_mem, e->d_kp, e->hi, e->lo, e->d_dt0));
+  std::vector<double> dt0((size_t)n);
+  std::vector<RunState> st((size_t)n);
+  EK(cudaMemcpyAsync(dt0.data(), e->d_dt0, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream));
+  EK(cudaMemcpyAsync(st.data(), e->d_st, sizeof(RunState) * n, cudaMemcpyDeviceToHost, e->stream));
+  EK(cudaStreamSynchronize(e->stream));
+  std::vector<double> work((size_t)n);
+  double total = 0.0, longest = 0.0;
+  for (int r = 0; r < n; ++r) {
+    const pip::KParams &k = e->kp[r];
+    double steps = 1.0;
+    if (st[r].status == 0) {
+      const double left = t_end > 0.0 ? t_end - st[r].time : 0.0;
+      steps = t_end > 0.0 && dt0[r] > 0.0 && std::isfinite(dt0[r]) ? std::max(left / dt0[r], 0.0) + 1.0
+                                                                 : (double)max_steps;
+      if (max_steps > 0) steps = std::min(steps, (double)max_steps);
+    }
+    work[r] = (double)k.nx * (k.ndim == 2 ? (double)k.ny : 1.0) * steps;
+    total += work[r];
+    longest = std::max(longest, work[r]);
+  }
+  std::vector<int> order((size_t)n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  const bool can = !e->has2d && (e->threads == 256 || e->threads == 512) && e->cluster != 1;
+  int cl = 1, nbig = 0, grid = e->sms * e->ctas_per_sm;
+  if (can) {
+    const int c4 = pip::ens::max_clusters(e->threads, 4), c8 = pip::ens::max_clusters(e->threads, 8);
+    const double even4 = c4 > 0 ? total / (4.0 * c4) : 0.0;
+    int want = e->cluster;
+    if (want == 0 && c4 > 0 && longest > 0.75 * even4) want = longest > 4.0 * 4.0 * even4 && c8 > 0 ? 8 : 4;
+    const int cc = want == 4 ? c4 : want == 8 ? c8 : 0;
+    if (cc > 0) {
+      cl = want;
+      grid = cc * cl;
+      const double even = total / (double)grid;
+      while (nbig < n && work[(size_t)order[(size_t)nbig]] > e->share * even) ++nbig;
+    }
+  }
+  if (order != e->order) {
+    EK(cudaMemcpyAsync(e->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream));
+    EK(cudaStreamSynchronize(e->stream));
+    e->order = order;
+  }
+  e->cl = cl;
+  e->nbig = nbig;
+  e->grid = grid;
   return PIP_OK;
 }
 
@@ -834,9 +1157,12 @@ int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *de
   if (!e) return PIP_ERR_NULL;
   if (!(t_end > 0.0) && max_steps <= 0) return PIP_ERR_PARAM;
   EK(cudaSetDevice(e->device));
+  const int pl = ens_plan(e, t_end, max_steps);
+  if (pl != PIP_OK) return pl;
   // one graph per (end time, step limit, configuration): queue reset + persistent kernel
   if (!e->graph || e->graph_t_end != t_end || e->graph_steps != max_steps ||
-      e->graph_threads != e->threads || e->graph_ctas != e->ctas_per_sm) {
+      e->graph_threads != e->threads || e->graph_ctas != e->ctas_per_sm ||
+      e->graph_cl != e->cl || e->graph_nbig != e->nbig || e->graph_grid != e->grid) {
     if (e->graph) cudaGraphExecDestroy(e->graph);
     e->graph = nullptr;
     cudaGraph_t g = nullptr;
@@ -855,6 +1181,9 @@ int pip_ensemble_run(pip_ensemble *e, double t_end, int64_t max_steps, float *de
     e->graph_steps = max_steps;
     e->graph_threads = e->threads;
     e->graph_ctas = e->ctas_per_sm;
+    e->graph_cl = e->cl;
+    e->graph_nbig = e->nbig;
+    e->graph_grid = e->grid;
   }
   cudaEvent_t a = nullptr, b = nullptr;
   if (device_ms) {

@@ -82,24 +82,42 @@ class Ensemble:
         capi._check(capi.lib().pip_ensemble_set_config(self.h, int(threads), int(ctas_per_sm)),
                     "pip_ensemble_set_config")
 
+    def set_cluster(self, cluster: int, share: float = 0.25) -> None:
+        """Cluster sharing of long runs: 0 chosen per launch, 1 off, 4 or 8 blocks; runs
+        whose work exceeds `share` times an even share are shared."""
+        capi._check(capi.lib().pip_ensemble_set_cluster(self.h, int(cluster), float(share)),
+                    "pip_ensemble_set_cluster")
+
+    def plan(self) -> dict:
+        """The last launch's plan: cluster size (1: none), runs shared, blocks launched."""
+        c, nb, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        capi._check(capi.lib().pip_ensemble_plan(self.h, ctypes.byref(c), ctypes.byref(nb),
+                                                 ctypes.byref(g)), "pip_ensemble_plan")
+        return {"cluster": c.value, "shared_runs": nb.value, "grid": g.value}
+
     def load_balance(self) -> dict:
         """Makespan of the last launch against perfect balance: each run's busy span (device
-        timer) from pip_ensemble_timings; busy fraction = sum of spans / (slots x makespan);
-        the longest run bounds the makespan from below however the queue is ordered."""
+        timer) from pip_ensemble_timings times the blocks that stepped it; busy fraction =
+        sum of block-spans / (slots x makespan).  A run on one block bounds the makespan
+        from below by its span; a shared run by its span too, which it cut by its blocks."""
         n = len(self.shapes)
         t0, t1 = np.empty(n), np.empty(n)
         capi._check(capi.lib().pip_ensemble_timings(self.h, capi._ptr(t0), capi._ptr(t1)),
                     "pip_ensemble_timings")
         slots = ctypes.c_int()
         capi._check(capi.lib().pip_ensemble_slots(self.h, ctypes.byref(slots)), "pip_ensemble_slots")
+        blocks = np.zeros(n, dtype=np.int32)
+        capi._check(capi.lib().pip_ensemble_blocks(self.h, blocks.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_int))), "pip_ensemble_blocks")
         ran = t1 >= 0
         span = (t1 - t0)[ran]
         makespan = float(t1[ran].max() - t0[ran].min())
-        busy = float(span.sum())
+        busy = float((span * np.maximum(blocks[ran], 1)).sum())
         ideal = max(busy / slots.value, float(span.max()))
         return {"makespan_us": makespan, "busy_us": busy, "slots": slots.value,
                 "busy_fraction": busy / (slots.value * makespan),
                 "longest_run_us": float(span.max()),
+                "shared_runs": int((blocks[ran] > 1).sum()),
                 "ideal_makespan_us": ideal,
                 "makespan_over_ideal": makespan / ideal,
                 "makespan_over_even_split": makespan / (busy / slots.value)}

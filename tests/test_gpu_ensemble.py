@@ -161,3 +161,52 @@ def test_load_balance_record(gpu_lib):
     assert lb["slots"] > 0 and 0.0 < lb["busy_fraction"] <= 1.0 + 1e-9
     assert lb["makespan_us"] >= lb["longest_run_us"] > 0.0
     assert lb["makespan_over_ideal"] >= 1.0 - 1e-9
+
+
+@pytest.mark.parametrize("threads", [512, 256])
+def test_cluster_shared_runs_match_one_block(gpu_lib, threads):
+    """Runs shared by a thread-block cluster (each block a contiguous part of the cells, the
+    cluster barrier between stages, dt reduced over the cluster) evolve as on one block: the
+    cells' arithmetic and the exact min/max reductions do not depend on the split, so times
+    and step counts are equal; the states agree to the FMA contraction each kernel instance
+    gets (measured 1e-14 on 5 of 10^4 values; a stale neighbour cell would show at 1e-3)."""
+    mem = [ics.shock_tube_member(3000, col=30.0, pratio=6.0, dratio=3.0, ion_frac=0.3),
+           ics.shock_tube_member(2000, col=2.0e3, pratio=12.0, dratio=5.0, ion_frac=0.1),
+           ics.shock_tube_member(700, col=1.0, pratio=4.0, dratio=2.0, ion_frac=0.6)] + \
+        shock_tube_ensemble(n_runs=5, seed=3, nx_max=400)
+    out = {}
+    for cl in (1, 4, 8):
+        with Ensemble(mem) as e:
+            e.set_config(threads, 1)
+            e.set_cluster(cl)
+            e.run(t_end=0.01)
+            plan = e.plan()
+            out[cl] = [e.member(r) for r in range(len(mem))]
+            lb = e.load_balance()
+        if cl == 1:
+            assert plan["cluster"] == 1 and plan["shared_runs"] == 0
+        else:
+            # a handful of runs against >100 slots: every run is above half an even share
+            assert plan["cluster"] == cl and plan["shared_runs"] == len(mem)
+            assert lb["shared_runs"] == len(mem)
+    for cl in (4, 8):
+        for a, b in zip(out[1], out[cl]):
+            assert a[4] == b[4] == 0 and a[3] == b[3] and a[2] == b[2]
+            assert max(rel_l1(a[0], b[0]).max(), rel_l1(a[1], b[1]).max()) <= 1e-12
+
+
+def test_cluster_rules(gpu_lib):
+    with Ensemble([ics.orszag_tang(16)]) as e:
+        with pytest.raises(capi.PipError):
+            e.set_cluster(4)                        # a 2D run: one block per run
+    with Ensemble(members()[:3]) as e:
+        e.set_config(1024, 1)
+        with pytest.raises(capi.PipError):
+            e.set_cluster(4)
+        e.set_config(512, 1)
+        with pytest.raises(capi.PipError):
+            e.set_cluster(3)
+        e.set_cluster(0)
+        e.run(t_end=0.002)
+        assert e.plan()["cluster"] in (4, 8)          # three runs on a whole GPU: shared
+
