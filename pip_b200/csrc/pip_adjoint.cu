@@ -450,47 +450,27 @@ cell_vjp_kernel(const KParams p, const double *__restrict__ Us, const double *__
 }
 
 // Adjoint of the ghost fill (Boundary_rot.f90:54-125 as done by the stage kernels' ghost
-// writes): each interior cell within 2*margin of a boundary (the list `cells`) gathers the
-// cotangents of the ghost cells copied from it (x ghosts, y ghosts and corners, with their
-// sign tables).  Ghost entries are left as they are; consumers read interior cells only.
-__global__ void fold_kernel(const KParams p, double *lam, const int *cells, int ncells) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncells; t += gridDim.x * blockDim.x) {
-    const int gi = cells[t] % p.ix, gj = cells[t] / p.ix;
-    int tx[2 * kMaxMargin], sx[2 * kMaxMargin], ntx = 0;
-    int ty[2 * kMaxMargin], sy[2 * kMaxMargin], nty = 0;
-    for (int s = 0; s < 2; ++s)
-      for (int l = 0; l < p.m0; ++l)
-        if (p.gx[s][l] == gi) {
-          tx[ntx] = s == 0 ? l : p.ix - p.m0 + l;
-          sx[ntx++] = s;
-        }
-    if (p.ndim == 2)
-      for (int s = 0; s < 2; ++s)
-        for (int l = 0; l < p.m1; ++l)
-          if (p.gy[s][l] == gj) {
-            ty[nty] = s == 0 ? l : p.jx - p.m1 + l;
-            sy[nty++] = s;
-          }
-    if (ntx == 0 && nty == 0) continue;
-    const long long nc = p.nc;
-    const long long q = (long long)gj * p.ix + gi;
-    // gather every plane's ghost cotangents first, then add them to the cell: the ghost
-    // cells read here are never fold targets, so the loads need not wait for the stores
-    double add[NV];
-#pragma unroll
-    for (int n = 0; n < NV; ++n) {
-      add[n] = 0.0;
-      for (int a = 0; a < ntx; ++a) {
-        const double g = (double)p.symx[sx[a]][n];
-        add[n] += g * lam[(long long)gj * p.ix + tx[a] + n * nc];
-        for (int b = 0; b < nty; ++b)
-          add[n] += (double)p.symy[sy[b]][n] * g * lam[(long long)ty[b] * p.ix + tx[a] + n * nc];
-      }
-      for (int b = 0; b < nty; ++b)
-        add[n] += (double)p.symy[sy[b]][n] * lam[(long long)ty[b] * p.ix + gi + n * nc];
+// writes): each interior cell that is the source of ghost copies gathers their cotangents
+// (x ghosts, then for each of them its corner ghosts, then y ghosts, with the sign tables
+// folded into a per-plane sign mask).  The gather list is built on the host (fold_plan);
+// one thread per (cell, plane), plane-major so a warp's loads follow the list.  Ghost
+// entries are left as they are; consumers read interior cells only, and no ghost read here
+// is a fold target.
+__global__ void __launch_bounds__(256) fold_kernel(double *lam, long long nc, const int *cells,
+                                                   const int *src, const unsigned short *neg,
+                                                   int ncells, int nent) {
+  const long long total = (long long)ncells * NV;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(t / ncells), k = (int)(t - (long long)n * ncells);
+    double add = 0.0;
+    for (int e = 0; e < nent; ++e) {
+      const int g = src[(long long)e * ncells + k];
+      if (g < 0) break;
+      const double v = lam[g + n * nc];
+      add += ((neg[(long long)e * ncells + k] >> n) & 1) ? -v : v;
     }
-#pragma unroll
-    for (int n = 0; n < NV; ++n) lam[q + n * nc] += add[n];
+    lam[cells[k] + n * nc] += add;
   }
 }
 
@@ -657,8 +637,10 @@ struct pip_adj {
   double *gx = nullptr, *gy = nullptr;            // face-state cotangents (2*13 planes)
   unsigned long long *mx = nullptr, *my = nullptr; // minmod branches per face
   int nbf = 0, nbc = 0;
-  int *d_fold = nullptr;          // interior cells within 2*margin of a boundary
-  int nfold = 0;
+  int *d_fold = nullptr;          // interior cells that are the source of ghost copies
+  int *d_fsrc = nullptr;          // their ghost cells, entry-major (nfent x nfold, -1 = none)
+  unsigned short *d_fneg = nullptr;  // per entry: plane n's sign is negative iff bit n
+  int nfold = 0, nfent = 0;
   DevCtrl *ctrl = nullptr;
   DevCtrl *h_ctrl = nullptr;
   int nb = 0;
@@ -676,18 +658,80 @@ struct pip_adj {
 
 namespace {
 
-int grid_fold(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 4)); }
+int grid_fold(int n) {
+  return std::max(1, std::min((n * pip::adjk::NV + 255) / 256, 148 * 8));
+}
 
-// Interior cells that can be the source of a ghost copy (within 2*margin of a boundary).
-std::vector<int> fold_cells(const KParams &k) {
-  std::vector<int> c;
+// Gather list of the ghost-fill adjoint: for every interior cell within 2*margin of a
+// boundary that is the source of ghost copies (gx/gy: the interior column/row each ghost
+// column/row copies), its ghost cells in the order x ghosts (each followed by its corner
+// ghosts), then y ghosts, with sign masks from the boundary sign tables.
+struct FoldPlan {
+  std::vector<int> cells, src;
+  std::vector<unsigned short> neg;
+  int nent = 0;
+};
+
+FoldPlan fold_plan(const KParams &k) {
+  std::vector<int> cells;
+  std::vector<std::vector<std::pair<int, unsigned short>>> ent;
   const int j0 = k.ndim == 2 ? k.m1 : 0, j1 = k.ndim == 2 ? k.m1 + k.ny : 1;
   for (int j = j0; j < j1; ++j)
-    for (int i = k.m0; i < k.m0 + k.nx; ++i)
-      if (i < 2 * k.m0 || i >= k.ix - 2 * k.m0 ||
-          (k.ndim == 2 && (j < 2 * k.m1 || j >= k.jx - 2 * k.m1)))
-        c.push_back(j * k.ix + i);
-  return c;
+    for (int i = k.m0; i < k.m0 + k.nx; ++i) {
+      if (!(i < 2 * k.m0 || i >= k.ix - 2 * k.m0 ||
+            (k.ndim == 2 && (j < 2 * k.m1 || j >= k.jx - 2 * k.m1))))
+        continue;
+      int tx[2 * pip::kMaxMargin], sx[2 * pip::kMaxMargin], ntx = 0;
+      int ty[2 * pip::kMaxMargin], sy[2 * pip::kMaxMargin], nty = 0;
+      for (int s = 0; s < 2; ++s)
+        for (int l = 0; l < k.m0; ++l)
+          if (k.gx[s][l] == i) {
+            tx[ntx] = s == 0 ? l : k.ix - k.m0 + l;
+            sx[ntx++] = s;
+          }
+      if (k.ndim == 2)
+        for (int s = 0; s < 2; ++s)
+          for (int l = 0; l < k.m1; ++l)
+            if (k.gy[s][l] == j) {
+              ty[nty] = s == 0 ? l : k.jx - k.m1 + l;
+              sy[nty++] = s;
+            }
+      if (ntx == 0 && nty == 0) continue;
+      std::vector<std::pair<int, unsigned short>> e;
+      auto mask = [&](int gxs, int gys) {
+        unsigned short m = 0;
+        for (int n = 0; n < pip::adjk::NV; ++n) {
+          const int sg = (gxs >= 0 ? k.symx[gxs][n] : 1) * (gys >= 0 ? k.symy[gys][n] : 1);
+          if (sg < 0) m = (unsigned short)(m | (1u << n));
+        }
+        return m;
+      };
+      for (int a = 0; a < ntx; ++a) {
+        e.push_back({j * k.ix + tx[a], mask(sx[a], -1)});
+        for (int b = 0; b < nty; ++b) e.push_back({ty[b] * k.ix + tx[a], mask(sx[a], sy[b])});
+      }
+      for (int b = 0; b < nty; ++b) e.push_back({ty[b] * k.ix + i, mask(-1, sy[b])});
+      cells.push_back(j * k.ix + i);
+      ent.push_back(e);
+    }
+  FoldPlan f;
+  f.cells = cells;
+  for (const auto &e : ent) f.nent = std::max(f.nent, (int)e.size());
+  const size_t nf = cells.size();
+  f.src.assign((size_t)f.nent * nf, -1);
+  f.neg.assign((size_t)f.nent * nf, 0);
+  for (size_t c = 0; c < nf; ++c)
+    for (size_t q = 0; q < ent[c].size(); ++q) {
+      f.src[q * nf + c] = ent[c][q].first;
+      f.neg[q * nf + c] = ent[c][q].second;
+    }
+  return f;
+}
+
+void fold(pip_adj *a, double *lam, int grid) {
+  if (a->nfold > 0)
+    pip::adjk::fold_kernel<<<grid, 256, 0, a->stream>>>(lam, a->kp.nc, a->d_fold, a->d_fsrc,
+                                                       a->d_fneg, a->nfold, a->nfent);
 }
 
 cudaError_t launch_vjp(pip_adj *a, int stage, const double *Us, const double *lam, const double *acc,
@@ -796,13 +840,25 @@ int pip_adj_create(const pip_params *p, int64_t max_steps, int checkpoint_every,
   if ((e = cudaMemset(a->gy, 0, sizeof(double) * 2 * 13 * (size_t)k.nc)) != cudaSuccess) return fail(e);
   if ((e = cudaMemset(a->my, 0, sizeof(unsigned long long) * (size_t)k.nc)) != cudaSuccess) return fail(e);
   {
-    const std::vector<int> fc = fold_cells(a->kp);
-    a->nfold = (int)fc.size();
-    if ((e = cudaMalloc(&a->d_fold, sizeof(int) * std::max<size_t>(1, fc.size()))) != cudaSuccess)
+    const FoldPlan fp = fold_plan(a->kp);
+    a->nfold = (int)fp.cells.size();
+    a->nfent = fp.nent;
+    const size_t ne = std::max<size_t>(1, fp.src.size());
+    if ((e = cudaMalloc(&a->d_fold, sizeof(int) * std::max<size_t>(1, fp.cells.size()))) != cudaSuccess)
       return fail(e);
-    if (!fc.empty() && (e = cudaMemcpy(a->d_fold, fc.data(), sizeof(int) * fc.size(),
-                                       cudaMemcpyHostToDevice)) != cudaSuccess)
-      return fail(e);
+    if ((e = cudaMalloc(&a->d_fsrc, sizeof(int) * ne)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&a->d_fneg, sizeof(unsigned short) * ne)) != cudaSuccess) return fail(e);
+    if (!fp.cells.empty()) {
+      if ((e = cudaMemcpy(a->d_fold, fp.cells.data(), sizeof(int) * fp.cells.size(),
+                          cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+      if ((e = cudaMemcpy(a->d_fsrc, fp.src.data(), sizeof(int) * fp.src.size(),
+                          cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+      if ((e = cudaMemcpy(a->d_fneg, fp.neg.data(), sizeof(unsigned short) * fp.neg.size(),
+                          cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+    }
   }
   if ((e = cudaMalloc(&a->p1dot, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&a->p1dac, sizeof(double) * a->nb)) != cudaSuccess) return fail(e);
@@ -841,6 +897,8 @@ void pip_adj_destroy(pip_adj *a) {
   if (a->stream2) cudaStreamDestroy(a->stream2);
   if (a->cand) cudaFree(a->cand);
   if (a->d_fold) cudaFree(a->d_fold);
+  if (a->d_fsrc) cudaFree(a->d_fsrc);
+  if (a->d_fneg) cudaFree(a->d_fneg);
   if (a->mx) cudaFree(a->mx);
   if (a->my) cudaFree(a->my);
   if (a->ctrl) cudaFree(a->ctrl);
@@ -956,10 +1014,10 @@ int pip_adj_backward(pip_adj *a, const double *gN, double *g0, double *g_col, fl
     // reverse sweep
     for (int j = len - 1; j >= 0; --j) {
       const double *dtp = a->dt_hist + n0 + j;
-      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->La, a->d_fold, a->nfold);
+      fold(a, a->La, gf);
       ACK(cudaGetLastError());
       ACK(launch_vjp(a, 2, a->segu[s % 2][j], a->La, nullptr, a->Lb, dtp));
-      pip::adjk::fold_kernel<<<gf, 256, 0, a->stream>>>(kp, a->Lb, a->d_fold, a->nfold);
+      fold(a, a->Lb, gf);
       ACK(cudaGetLastError());
       ACK(launch_vjp(a, 1, zp(s, j), a->Lb, a->La, a->La, dtp));
       pip::adjk::finalize_kernel<<<1, 256, 0, a->stream>>>(kp, a->nb, a->nbc, a->p1dot, a->p1dac, a->p2dot,
@@ -1010,7 +1068,7 @@ int pip_adj_stage_vjp(pip_adj *a, int stage, const double *Us, const double *lam
 int pip_adj_fold(pip_adj *a, double *lam) {
   if (!a || !lam) return PIP_ERR_NULL;
   ACK(cudaSetDevice(a->device));
-  pip::adjk::fold_kernel<<<grid_fold(a->nfold), 256, 0, a->stream>>>(a->kp, lam, a->d_fold, a->nfold);
+  fold(a, lam, grid_fold(a->nfold));
   ACK(cudaGetLastError());
   ACK(cudaStreamSynchronize(a->stream));
   return PIP_OK;
