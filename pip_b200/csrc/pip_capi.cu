@@ -62,6 +62,7 @@ struct pip_ctx {
   double *nl_nex[2] = {nullptr, nullptr};
   int nl_cur = 0;
   double *nl_cr = nullptr, *nl_ip = nullptr, *nl_tab = nullptr, *nl_ref = nullptr;
+  double *nl_rtab = nullptr;
   pip::NlevConst *nl_k = nullptr;
   bool nl_ready = false;              // pip_set_nlevel has run
   bool nl_init = false;               // the fresh-start block (Gm_rec_ref, ion_pot) has run
@@ -766,6 +767,7 @@ void pip_ctx_destroy(pip_ctx *c) {
   cudaFree(c->nl_tab);
   cudaFree(c->nl_ref);
   cudaFree(c->nl_k);
+  cudaFree(c->nl_rtab);
   pip::hc_destroy(c->hc);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1443,9 +1445,23 @@ int pip_set_nlevel(pip_ctx *c, const pip_nlevel *cfg, const double *table, int64
   if (set_device(c)) return PIP_ERR_CUDA;
   CK(cudaStreamSynchronize(c->stream));
   cudaFree(c->nl_tab);
+  cudaFree(c->nl_rtab);
   c->nl_tab = nullptr;
+  c->nl_rtab = nullptr;
   CK(cudaMalloc(&c->nl_tab, sizeof(double) * 4 * (size_t)nrows));
   CK(cudaMemcpy(c->nl_tab, table, sizeof(double) * 4 * (size_t)nrows, cudaMemcpyHostToDevice));
+  {
+    // quadratic-interpolation denominators of each row's three-row stencil (FMA build)
+    std::vector<double> rt(4 * (size_t)nrows, 0.0);
+    for (int64_t r = 0; r + 2 < nrows; ++r) {
+      const double x0 = table[4 * r], x1 = table[4 * (r + 1)], x2 = table[4 * (r + 2)];
+      rt[4 * r] = 1.0 / ((x0 - x1) * (x0 - x2));
+      rt[4 * r + 1] = 1.0 / ((x1 - x0) * (x1 - x2));
+      rt[4 * r + 2] = 1.0 / ((x2 - x0) * (x2 - x1));
+    }
+    CK(cudaMalloc(&c->nl_rtab, sizeof(double) * rt.size()));
+    CK(cudaMemcpy(c->nl_rtab, rt.data(), sizeof(double) * rt.size(), cudaMemcpyHostToDevice));
+  }
   pip::NlevConst k;
   pip::nlev_constants(&k);
   CK(cudaMemcpy(c->nl_k, &k, sizeof k, cudaMemcpyHostToDevice));
@@ -1454,6 +1470,8 @@ int pip_set_nlevel(pip_ctx *c, const pip_nlevel *cfg, const double *table, int64
   kp.nl_ntab = nrows;
   kp.nl_xmin = table[0];
   kp.nl_xrange = table[4 * (nrows - 1)] - table[0];
+  kp.nl_rtab = c->nl_rtab;
+  kp.nl_xsc = (double)nrows / kp.nl_xrange;
   kp.nl_deriv = cfg->deriv;
   kp.nl_n0fac = cfg->n0fac;
   // tfac of set_IR type 4 (PIP_rot.f90:240-248); 5.0/3.0 is a default-real quotient there

@@ -19,6 +19,8 @@ struct NlevConst {
   double xrat[5][5], enn[5][5], rnn[5][5], ann[5][5], bnn[5][5], lgt[5][5];
   double an0[5], bn0[5], lgi[5];
   double eev[6];     // IRgetionpot's level energies (eV, default-real literals)
+  // reciprocal forms of the FMA build: 1/xrat, gw(a)/gw(b), gw(a)/gw(6)/2
+  double ixrat[5][5], gwq[5][5], gwh[5];
 };
 
 // Scalars and tables of one simulation, passed by value to every kernel.
@@ -70,6 +72,9 @@ struct KParams {
   const double *nl_tab;
   long long nl_ntab;
   double nl_xmin, nl_xrange;
+  const double *nl_rtab;  // FMA build: per table row r, 1/((x0-x1)(x0-x2)), 1/((x1-x0)(x1-x2)),
+                          // 1/((x2-x0)(x2-x1)) of its rows r, r+1, r+2 (4 doubles a row)
+  double nl_xsc;          // ntab / xrange
   const NlevConst *nl_k;
   double *nl_nex, *nl_nex2, *nl_cr, *nl_ip;
   int nl_deriv;      // convective derivative: 0 none, 1 two-point, 4 five-point

@@ -69,6 +69,11 @@ void nlev_constants(NlevConst *k) {
       g2 = (-1.0 / ri) * (0.6282 - 0.5598 / ri + 0.5299 / (ri * ri));
       g3 = (1.0 / ri) * (1.0 / ri) * (0.3887 - 1.181 / ri + 1.470 / (ri * ri));
     }
+    for (int b = a + 1; b < 5; ++b) {
+      k->ixrat[a][b] = 1.0 / k->xrat[a][b];
+      k->gwq[a][b] = k->gw[a] / k->gw[b];
+    }
+    k->gwh[a] = k->gw[a] / k->gw[5] / 2.0;
     k->an0[a] = 32.0 / 3.0 / std::sqrt(3.0) / pi * ri + g1 / 3.0 + g2 / 4.0 + g3 / 5.0;
     k->bn0[a] = 2.0 / 3.0 * (ri * ri) * (5.0 + bn[a]);
     k->lgi[a] = std::log(2.0 * (ri * ri));

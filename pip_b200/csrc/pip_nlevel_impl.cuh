@@ -33,9 +33,19 @@ struct NlW {
   const double *r0;
   double w0, w1, w2;
 };
+// The FMA build multiplies by the rows' precomputed reciprocal denominators (nl_rtab) and
+// finds the row with a product, falling back to the reference's quotient when the product
+// lies within 1e-9 of a row boundary (a few ulps from the quotient), so both pick the same
+// row.
 __device__ __forceinline__ NlW nl_weights(const KParams &p, double z) {
   const long long n = p.nl_ntab;
+#if PIP_RCP
+  const double t = (z - p.nl_xmin) * p.nl_xsc;
+  double f = floor(t);
+  if (t - f < 1.0e-9 || f + 1.0 - t < 1.0e-9) f = floor((z - p.nl_xmin) / p.nl_xrange * (double)n);
+#else
   const double f = floor((z - p.nl_xmin) / p.nl_xrange * (double)n);
+#endif
   long long xi;
   if (!(f > 0.0)) xi = 1;
   else if (f >= (double)n) xi = n - 1;
@@ -44,9 +54,16 @@ __device__ __forceinline__ NlW nl_weights(const KParams &p, double z) {
   NlW w;
   w.r0 = p.nl_tab + 4 * (xi - 1);
   const double x0 = __ldg(w.r0), x1 = __ldg(w.r0 + 4), x2 = __ldg(w.r0 + 8);
+#if PIP_RCP
+  const double *rt = p.nl_rtab + 4 * (xi - 1);
+  w.w0 = ((z - x1) * (z - x2)) * __ldg(rt);
+  w.w1 = ((z - x0) * (z - x2)) * __ldg(rt + 1);
+  w.w2 = ((z - x0) * (z - x1)) * __ldg(rt + 2);
+#else
   w.w0 = ((z - x1) * (z - x2)) / ((x0 - x1) * (x0 - x2));
   w.w1 = ((z - x0) * (z - x2)) / ((x1 - x0) * (x1 - x2));
   w.w2 = ((z - x0) * (z - x1)) / ((x2 - x0) * (x2 - x1));
+#endif
   return w;
 }
 __device__ __forceinline__ double nl_eval(const NlW &w, int i) {
@@ -56,9 +73,67 @@ __device__ __forceinline__ double nl_eval(const NlW &w, int i) {
 // get_col_ion_coeff on one cell of electron temperature te [K] and density ne: colrat into
 // cr[a*6+b] = colrat(a+1,b+1), the sums gi = sum max(N(ii)*colrat(ii,6),0) and
 // gr = sum max(N(6)*colrat(6,ii),0); true where the reference stops on a negative rate.
+// The FMA build divides once by kboltz*te and once by each y and z, and multiplies by the
+// reciprocal constants (ixrat, gwq, gwh); the rates then differ from the reference's by a
+// few ulps.
 __device__ __forceinline__ bool nl_cell(const KParams &p, const NlevConst &k, double te,
                                         double ne, const double (&nx)[6], double (&cr)[36],
                                         double &gi, double &gr) {
+#if PIP_RCP
+  bool bad = false;
+  const double s = sqrt(8.0 * kNlKb * te / kNlPi / kNlMe);
+  const double ikt = 1.0 / (kNlKb * te);
+#pragma unroll
+  for (int m = 0; m < 36; ++m) cr[m] = 0.0;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const double ri = (double)(a + 1);
+    const double pre = ne * s * 2.0 * (ri * ri) * kNlPi * (kNlA0 * kNlA0);
+#pragma unroll
+    for (int b = a + 1; b < 5; ++b) {
+      const double enn = k.enn[a][b];
+      const double yhat = enn * ikt;
+      const double zhat = k.rnn[a][b] + enn * ikt;
+      const double iy = 1.0 / yhat, iz = 1.0 / zhat;
+      const NlW wy = nl_weights(p, yhat), wz = nl_weights(p, zhat);
+      const double E1y = nl_eval(wy, 1), E1z = nl_eval(wz, 1);
+      const double E2y = nl_eval(wy, 2), E2z = nl_eval(wz, 2);
+      const double ann = k.ann[a][b];
+      const double colex = pre * k.ixrat[a][b] * (yhat * yhat) *
+                           (ann * ((iy + 0.5) * E1y - (iz + 0.5) * E1z) +
+                            (k.bnn[a][b] - ann * k.lgt[a][b]) * (E2y * iy - E2z * iz));
+      cr[a * 6 + b] = k.gwq[a][b] * colex;
+      cr[b * 6 + a] = colex * exp(-((k.eion[a] - k.eion[b]) * ikt));
+    }
+    const double yn = k.eion[a] * ikt;
+    const double zn = k.rn[a] + k.eion[a] * ikt;
+    const double iyn = 1.0 / yn, izn = 1.0 / zn;
+    const NlW wy = nl_weights(p, yn), wz = nl_weights(p, zn);
+    const double E1y = nl_eval(wy, 1), E1z = nl_eval(wz, 1);
+    const double E2y = nl_eval(wy, 2), E2z = nl_eval(wz, 2);
+    const double E0y = nl_eval(wy, 0), E0z = nl_eval(wz, 0);
+    const double ziyn = E0y - 2.0 * E1y + E2y, zizn = E0z - 2.0 * E1z + E2z;
+    const double an0 = k.an0[a];
+    const double colex = pre * (yn * yn) *
+                         (an0 * (E1y * iyn - E1z * izn) + (k.bn0[a] - an0 * k.lgi[a]) * (ziyn - zizn));
+    bad |= colex < 0.0;
+    cr[a * 6 + 5] = colex * exp(-((k.eion[5] - k.eion[a]) * ikt));
+  }
+  const double saha =
+      pow(2.0 * kNlPi * kNlMehat * kNlKbhat * te / kNlHhat / kNlHhat * kNlE14, -3.0 / 2.0);
+  double si = 0.0, sr = 0.0;
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    cr[30 + a] = ne * cr[a * 6 + 5] * k.gwh[a] * saha * exp(k.eion[a] * ikt);
+    si = si + fmax(nx[a] * cr[a * 6 + 5], 0.0);
+    sr = sr + fmax(nx[5] * cr[30 + a], 0.0);
+  }
+#pragma unroll
+  for (int m = 0; m < 36; ++m) bad |= cr[m] < 0.0;
+  gi = si;
+  gr = sr;
+  return bad;
+#else
   bool bad = false;
   const double s = sqrt(8.0 * kNlKb * te / kNlPi / kNlMe);
 #pragma unroll
@@ -109,6 +184,7 @@ __device__ __forceinline__ bool nl_cell(const KParams &p, const NlevConst &k, do
   gi = si;
   gr = sr;
   return bad;
+#endif
 }
 
 // IRgetionpot (PIP_rot.f90:1162-1235) of one cell.
@@ -236,6 +312,12 @@ __global__ void __launch_bounds__(128) nlev_update_kernel(const __grid_constant_
   const double dts = stage == 1 ? dt / 2.0 : dt / 1.0;
   const long long nc = p.nc, n = (long long)p.nx * p.ny;
   const double g = p.nl_gref, tir = p.nl_tir;
+#if PIP_RCP
+  const double cg = tir / g;   // x/g*tir as x*cg
+#define PIP_NL_GT(x) ((x) * cg)
+#else
+#define PIP_NL_GT(x) ((x) / g * tir)
+#endif
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = p.m0 + (int)(t % p.nx), j = p.m1 + (int)(t / p.nx);
@@ -244,14 +326,14 @@ __global__ void __launch_bounds__(128) nlev_update_kernel(const __grid_constant_
 #pragma unroll
     for (int m = 0; m < 6; ++m) nx[m] = p.nl_nex[q + m * nc];
     for (int jj = 0; jj < 5; ++jj)
-      d[5] = d[5] + nx[jj] * nl_cr(p, q, jj, 5) / g * tir - nx[5] * nl_cr(p, q, 5, jj) / g * tir;
+      d[5] = d[5] + PIP_NL_GT(nx[jj] * nl_cr(p, q, jj, 5)) - PIP_NL_GT(nx[5] * nl_cr(p, q, 5, jj));
 #pragma unroll
     for (int ii = 0; ii < 5; ++ii)
-      d[ii] = d[ii] + nx[5] * nl_cr(p, q, 5, ii) / g * tir - nx[ii] * nl_cr(p, q, ii, 5) / g * tir;
+      d[ii] = d[ii] + PIP_NL_GT(nx[5] * nl_cr(p, q, 5, ii)) - PIP_NL_GT(nx[ii] * nl_cr(p, q, ii, 5));
 #pragma unroll
     for (int ii = 0; ii < 5; ++ii)
       for (int jj = 0; jj < 5; ++jj)
-        d[ii] = d[ii] + nx[jj] * nl_cr(p, q, jj, ii) / g * tir - nx[ii] * nl_cr(p, q, ii, jj) / g * tir;
+        d[ii] = d[ii] + PIP_NL_GT(nx[jj] * nl_cr(p, q, jj, ii)) - PIP_NL_GT(nx[ii] * nl_cr(p, q, ii, jj));
     double o[6];
 #pragma unroll
     for (int ii = 0; ii < 5; ++ii) {
@@ -266,6 +348,7 @@ __global__ void __launch_bounds__(128) nlev_update_kernel(const __grid_constant_
     if (near_boundary<NDIM>(p, i, j)) write_ghosts<NDIM>(p, i, j, p.nl_nex2, 6, true);
   }
 }
+#undef PIP_NL_GT
 
 // cfl_pip_ir's type-4 terms and cfl_pip_ir_nexcite (Scheme_rot.f90:315-335) over every cell,
 // after the cfl kernel: max of the rates, with flag_IR_type 0 get_Pr_MHD's energy rewrite and
@@ -277,6 +360,12 @@ __global__ void __launch_bounds__(256) nlev_cfl_kernel(const __grid_constant__ K
                                                        int slot) {
   const long long nc = p.nc;
   const double g = p.nl_gref, tir = p.nl_tir, gm = p.gm;
+#if PIP_RCP
+  const double cg = tir / g;
+#define PIP_NL_GT(x) ((x) * cg)
+#else
+#define PIP_NL_GT(x) ((x) / g * tir)
+#endif
   double gmax = 0.0, ipmax = 1.0e-5, nxmax = 1.0e-5;
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < nc; q += (long long)gridDim.x * 256) {
     const int i = (int)(q % p.ix), j = (int)(q / p.ix);
@@ -298,10 +387,11 @@ __global__ void __launch_bounds__(256) nlev_cfl_kernel(const __grid_constant__ K
     for (int ii = 0; ii < 5; ++ii) {
       double d = 0.0;
       for (int jj = 0; jj < 6; ++jj)
-        d = d + nx[jj] * nl_cr(p, q, jj, ii) / g * tir - nx[ii] * nl_cr(p, q, ii, jj) / g * tir;
+        d = d + PIP_NL_GT(nx[jj] * nl_cr(p, q, jj, ii)) - PIP_NL_GT(nx[ii] * nl_cr(p, q, ii, jj));
       nxmax = fmax(nxmax, d - nl_conv<NDIM, NVM>(p, U, ii, q, i, j));
     }
   }
+#undef PIP_NL_GT
   // block maxima (exact), then one atomic per block on the ordered bits of the positive values
   __shared__ double red[3][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
