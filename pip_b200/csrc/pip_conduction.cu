@@ -48,14 +48,21 @@ namespace hc {
 
 constexpr int NT = 256;             // one-thread-per-cell kernels
 constexpr int SX = 128;             // BiCGstab kernels: interior columns (threads) per block
-// Pipeline of the BiCGstab kernels: NS stages of RS rows each (compile-time tuning).
+// Pipeline of the BiCGstab kernels: NS stages of RS rows each (compile-time tuning; the
+// FP32 kernels stage half the bytes per row and may keep more groups in flight).
 #ifndef PIP_HC_STAGES
 #define PIP_HC_STAGES 2
+#endif
+#ifndef PIP_HC_STAGES32
+#define PIP_HC_STAGES32 PIP_HC_STAGES
 #endif
 #ifndef PIP_HC_ROWS
 #define PIP_HC_ROWS 2
 #endif
-constexpr int NS = PIP_HC_STAGES;   // pipeline stages (row groups staged ahead)
+template <typename T>
+__host__ __device__ constexpr int stages() {
+  return sizeof(T) == 4 ? PIP_HC_STAGES32 : PIP_HC_STAGES;
+}
 constexpr int RS = PIP_HC_ROWS;     // rows per stage: one wait and one block barrier per group
 constexpr int SLOT = 136;           // elements per staged row segment (SX + 2 + alignment)
 constexpr int kWaitLimit = 1 << 22; // polls of an mbarrier before a block gives up
@@ -158,8 +165,10 @@ __device__ __forceinline__ T stencil(const T (&c)[9], const T (&w)[3][3]) {
 }
 
 // Block sums of 2 values into part[k*nb + block]; returns true in thread 0 of the last
-// block to finish, which then holds the totals (summed in block order) in tot[].
-template <int NTB>
+// block to finish, which then holds the totals (summed in block order) in tot[].  NTB
+// threads per block; the last block's sum over the blocks runs on its first NR threads
+// (strided slices, then a tree), so the order of the additions depends on NR only.
+template <int NTB, int NR = NTB>
 __device__ bool reduce2(double a, double b, double *part, unsigned int *counter, double (&tot)[2]) {
   __shared__ double s[2][NTB / 32];
   __shared__ bool s_last;
@@ -191,15 +200,18 @@ __device__ bool reduce2(double a, double b, double *part, unsigned int *counter,
   // the last block: totals in block order (each thread a strided slice, then a tree)
   __threadfence();
   double x = 0.0, y = 0.0;
-  for (unsigned int k = threadIdx.x; k < nb; k += NTB) {
-    x += part[k];
-    y += part[nb + k];
+  if (threadIdx.x < NR)
+    for (unsigned int k = threadIdx.x; k < nb; k += NR) {
+      x += part[k];
+      y += part[nb + k];
+    }
+  __shared__ double s2[2][NR];
+  if (threadIdx.x < NR) {
+    s2[0][threadIdx.x] = x;
+    s2[1][threadIdx.x] = y;
   }
-  __shared__ double s2[2][NTB];
-  s2[0][threadIdx.x] = x;
-  s2[1][threadIdx.x] = y;
   __syncthreads();
-  for (int h = NTB / 2; h > 0; h >>= 1) {
+  for (int h = NR / 2; h > 0; h >>= 1) {
     if ((int)threadIdx.x < h) {
       s2[0][threadIdx.x] += s2[0][threadIdx.x + h];
       s2[1][threadIdx.x] += s2[1][threadIdx.x + h];
@@ -321,6 +333,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -347,8 +362,8 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
 // The four BiCGstab kernels share one body.  A block owns SX interior columns starting at
 // i0 and a contiguous range of rows [ja, jb); the rows of a column block are divided evenly
 // among its blocks (one wave over the SMs).  Rows are staged in groups of RS, NS groups
-// ahead, as row segments copied into shared memory (one bulk copy per segment, one
-// mbarrier per stage; the block waits and synchronises once per group).  For row j:
+// ahead, as row segments copied into shared memory (one bulk copy per segment, a full and
+// an empty mbarrier per stage, see the block layout below).  For row j:
 //   window vectors (row j+1, columns i0-1 .. i0+SX)   -- the vector A is applied to is
 //                                                        formed from these at each point
 //   own vectors    (row j, columns i0 .. i0+SX-1)
@@ -373,7 +388,8 @@ __host__ __device__ constexpr int n_copies() {
 
 template <typename T, int KIND>
 __host__ __device__ constexpr size_t stage_smem() {
-  return (size_t)NS * RS * n_copies<KIND>() * SLOT * sizeof(T) + NS * sizeof(unsigned long long);
+  return (size_t)stages<T>() * RS * n_copies<KIND>() * SLOT * sizeof(T) +
+         2 * stages<T>() * sizeof(unsigned long long);
 }
 
 template <typename T>
@@ -408,222 +424,255 @@ __device__ __forceinline__ void copy_desc(const BicgArgs<T> &a, long long nc, in
   }
 }
 
+// Block layout: SX consumer threads (one interior column each) and one producer warp
+// (threads SX .. SX+31) that stages the row groups.  Stage st has a `full` barrier (the
+// producer's expect_tx arrival plus the bytes of its copies) and an `empty` barrier (one
+// arrival per consumer warp when it has read the group), so neither side waits at a block
+// barrier inside the row loop: a consumer warp waits only for its group's bytes, the
+// producer only for the stage it refills.  Every wait is bounded; a wait that runs out
+// sets the shared fault flag, the others stop at their next wait, and the producer lets
+// the copies it issued land before the block leaves.
+constexpr int kConsumerWarps = SX / 32;
+constexpr int kBlock = SX + 32;
+
 template <typename T, int KIND>
-__global__ void __launch_bounds__(SX) bicg_kernel(const KParams p, const BicgArgs<T> a) {
+__global__ void __launch_bounds__(kBlock) bicg_kernel(const KParams p, const BicgArgs<T> a) {
   constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
   constexpr int NCP = n_copies<KIND>();
+  constexpr int NS = stages<T>();
   Scal *sc = a.sc;
   if (sc->done || sc->fault) return;
   const int wait_limit = sc->wait_limit;
   extern __shared__ __align__(128) unsigned char smem[];
   T *buf = reinterpret_cast<T *>(smem);
-  unsigned long long *bar =
+  unsigned long long *full =
       reinterpret_cast<unsigned long long *>(smem + (size_t)NS * RS * NCP * SLOT * sizeof(T));
-  static_assert(RS * NCP <= 32, "one lane of warp 0 per staged copy");
+  unsigned long long *empty = full + NS;
+  static_assert(RS * NCP <= 32, "one lane of the producer warp per staged copy");
+  __shared__ int off[NS][RS][NCP];
+  __shared__ volatile int s_fault;
 
   const int t = threadIdx.x;
+  const bool producer = t >= SX;
   const int cb = blockIdx.x % a.ncb, rb = blockIdx.x / a.ncb;
   const int i0 = p.m0 + cb * SX, i = i0 + t;
-  const bool active = i < p.m0 + p.nx;
+  const bool active = !producer && i < p.m0 + p.nx;
   const int ja = p.m1 + (int)((long long)p.ny * rb / a.nrb);
   const int jb = p.m1 + (int)((long long)p.ny * (rb + 1) / a.nrb);
   const int nrows = jb - ja;
+  const int ngroups = (nrows + RS - 1) / RS;
   const long long ix = p.ix, nc = p.nc;
 
-  // Warp 0 stages row groups: lane rr*NCP + c owns copy c of row rr of a group (its source
-  // address at row ja + rr, the length and the allocation end), so a group's copies are set
-  // up in parallel.  The first element of that copy inside its staged segment goes to
-  // off[stage][rr][c] for the consumers.
-  __shared__ int off[NS][RS][NCP];
-  const int lane = t & 31;
-  const int lrow = lane / NCP, lcopy = lane % NCP;
-  uintptr_t c_addr = 0, c_cap = 0;
-  uint32_t c_len = 0;
-  if (t < 32 && lane < RS * NCP) {
-    const T *base, *lim;
-    int dj, di, n;
-    copy_desc<T, KIND>(a, nc, lcopy, base, dj, di, n, lim);
-    c_addr = (uintptr_t)(base + ((long long)(ja + lrow + dj) * ix + i0 + di));
-    c_len = (uint32_t)(n * sizeof(T));
-    c_cap = (uintptr_t)lim & ~(uintptr_t)15;
-  }
-  const uintptr_t row_bytes = (uintptr_t)ix * sizeof(T);
-  auto issue = [&](int g) {       // warp 0: stage rows ja + g*RS .. of group g
-    const int st = g % NS;
-    const uint32_t bs = smem_addr(&bar[st]);
-    uintptr_t a0 = 0;
-    uint32_t bytes = 0;
-    if (lane < RS * NCP && g * RS + lrow < nrows) {
-      const uintptr_t ad = c_addr + (uintptr_t)(g * RS) * row_bytes;
-      a0 = ad & ~(uintptr_t)15;
-      uintptr_t end = (ad + c_len + 15) & ~(uintptr_t)15;
-      if (end > c_cap) end = c_cap;
-      bytes = (uint32_t)(end - a0);
-      off[st][lrow][lcopy] = (int)((ad - a0) / sizeof(T));
-    }
-    uint32_t total = bytes;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
-    if (lane == 0) mbar_expect_tx(bs, total);
-    __syncwarp();
-    if (bytes)
-      bulk_load(smem_addr(buf + ((size_t)(st * RS + lrow) * NCP + lcopy) * SLOT), (const void *)a0,
-                bytes, bs);
-  };
-  const int ngroups = (nrows + RS - 1) / RS;
-
   if (t == 0) {
-    for (int st = 0; st < NS; ++st) mbar_init(smem_addr(&bar[st]), 1u);
+    for (int st = 0; st < NS; ++st) {
+      mbar_init(smem_addr(&full[st]), 1u);
+      mbar_init(smem_addr(&empty[st]), (uint32_t)kConsumerWarps);
+    }
+    s_fault = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
-  if (t < 32)
-    for (int g = 0; g < NS && g < ngroups; ++g) issue(g);
-  __syncthreads();                // off[][][] of the first stages
 
-  // scalars of the update formed at each point
-  T s1 = T(0), s2 = T(0);
-  bool first = false;
-  if (KIND == K1) {
-    first = sc->count == 0;
-    s1 = (T)sc->beta;
-    s2 = (T)sc->omega;
-  } else if (KIND == K2) {
-    s1 = (T)sc->alpha;
-  } else if (KIND == K3) {
-    s1 = (T)sc->alpha;
-    s2 = (T)sc->omega;
-  }
-  auto form = [&](const T (&v)[3]) -> T {
-    if (KIND == KINIT) return v[0];
-    if (KIND == K1) return first ? v[0] : v[2] + s1 * (v[0] - s2 * v[1]);
-    if (KIND == K2) return v[0] - s1 * v[1];
-    return v[0] + s1 * v[1] + s2 * v[2];
-  };
-
-  T w[3][3];
-  RowFactors<T> f;
-  if (active && nrows > 0) {
-#pragma unroll
-    for (int dr = 0; dr < 2; ++dr)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const long long k = (long long)(ja - 1 + dr) * ix + i - 1 + d;
-        T v[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = c < NW ? a.w[c][k] : T(0);
-        w[dr][d] = form(v);
-      }
-    f.cxl = a.g[i];
-    f.cxr = a.g[ix + i];
-    f.idx = a.g[2 * ix + i];
-  }
-  const T *gy = a.g + 3 * ix;
   double acc0 = 0.0, acc1 = 0.0;
-  bool fault = false;
-  int g = 0;
-  for (; g < ngroups; ++g) {
-    const int st = g % NS;
-    const bool ok = mbar_wait(smem_addr(&bar[st]), (uint32_t)((g / NS) & 1), wait_limit);
-    if (__syncthreads_or(!ok)) {
-      fault = true;
-      break;
+  if (producer) {
+    // lane rr*NCP + c owns copy c of row rr of a group: its source address at row ja + rr,
+    // the length and the allocation end; the first element of that copy inside its staged
+    // segment goes to off[stage][rr][c] for the consumers
+    const int lane = t - SX;
+    const int lrow = lane / NCP, lcopy = lane % NCP;
+    uintptr_t c_addr = 0, c_cap = 0;
+    uint32_t c_len = 0;
+    if (lane < RS * NCP) {
+      const T *base, *lim;
+      int dj, di, n;
+      copy_desc<T, KIND>(a, nc, lcopy, base, dj, di, n, lim);
+      c_addr = (uintptr_t)(base + ((long long)(ja + lrow + dj) * ix + i0 + di));
+      c_len = (uint32_t)(n * sizeof(T));
+      c_cap = (uintptr_t)lim & ~(uintptr_t)15;
     }
-#pragma unroll
-    for (int rr = 0; rr < RS; ++rr) {
-    const int r = g * RS + rr, j = ja + r;
-    if (r >= nrows) break;
-    const T *sb = buf + (size_t)(st * RS + rr) * NCP * SLOT;
-    const int *of = off[st][rr];
-    if (active) {
-      const long long q = (long long)j * ix + i;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        T v[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = c < NW ? sb[c * SLOT + of[c] + t + d] : T(0);
-        w[2][d] = form(v);
+    const uintptr_t row_bytes = (uintptr_t)ix * sizeof(T);
+    int issued = 0;
+    for (int g = 0; g < ngroups; ++g) {
+      const int st = g % NS;
+      if (g >= NS) {
+        // the consumers' reads of group g - NS free the stage
+        const bool ok = mbar_wait(smem_addr(&empty[st]), (uint32_t)((g / NS - 1) & 1), wait_limit);
+        if (!ok || s_fault) {
+          if (!ok) s_fault = 1;
+          break;
+        }
       }
-      T own[2];
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-        own[c] = c < NO ? sb[(NW + c) * SLOT + of[NW + c] + t] : T(0);
-      constexpr int mc = NW + NO;
-      f.eta = sb[mc * SLOT + of[mc] + t];
-      f.fxxl = sb[(mc + 1) * SLOT + of[mc + 1] + t];
-      f.fxxr = sb[(mc + 1) * SLOT + of[mc + 1] + t + 1];
-      f.fxyl = sb[(mc + 2) * SLOT + of[mc + 2] + t];
-      f.fxyr = sb[(mc + 2) * SLOT + of[mc + 2] + t + 1];
-      f.fyyd = sb[(mc + 3) * SLOT + of[mc + 3] + t];
-      f.fyyu = sb[(mc + 4) * SLOT + of[mc + 4] + t];
-      f.fyxd = sb[(mc + 5) * SLOT + of[mc + 5] + t];
-      f.fyxu = sb[(mc + 6) * SLOT + of[mc + 6] + t];
-      f.cyd = gy[j];
-      f.cyu = gy[p.jx + j];
-      f.idy = gy[2 * p.jx + j];
-      T c[9];
-      entries(p, f, i, j, c);
-      if (KIND == KINIT) {
-        // r = b - A x term by term, as the reference's initial residual
-        const T bq = own[0];
-        T v = bq;
-        v = v - c[0] * w[1][1];
-        v = v - c[1] * w[1][0];
-        v = v - c[2] * w[1][2];
-        v = v - c[3] * w[0][1];
-        v = v - c[4] * w[2][1];
-        v = v - c[5] * w[0][0];
-        v = v - c[6] * w[0][2];
-        v = v - c[7] * w[2][0];
-        v = v - c[8] * w[2][2];
-        a.out[0][q] = v;
-        a.out[1][q] = v;
-        a.out[2][q] = v;
-        acc0 += (double)v * (double)v;
-        acc1 += (double)bq * (double)bq;
-      } else if (KIND == K1) {
-        a.out[0][q] = w[1][1];
-        const T av = stencil(c, w);
-        a.out[1][q] = av;
-        const double r0q = (double)own[1];
-        acc0 += (double)own[0] * r0q;
-        acc1 += r0q * (double)av;
-      } else if (KIND == K2) {
-        a.out[0][q] = w[1][1];
-        const T at = stencil(c, w);
-        acc0 += (double)w[1][1] * (double)at;
-        acc1 += (double)at * (double)at;
-      } else {
-        a.out[0][q] = w[1][1];
-        const T v = own[0] - stencil(c, w);
-        a.out[1][q] = v;
-        acc0 += (double)own[1] * (double)v;
-        acc1 += (double)v * (double)v;
+      uintptr_t a0 = 0;
+      uint32_t bytes = 0;
+      if (lane < RS * NCP && g * RS + lrow < nrows) {
+        const uintptr_t ad = c_addr + (uintptr_t)(g * RS) * row_bytes;
+        a0 = ad & ~(uintptr_t)15;
+        uintptr_t end = (ad + c_len + 15) & ~(uintptr_t)15;
+        if (end > c_cap) end = c_cap;
+        bytes = (uint32_t)(end - a0);
+        off[st][lrow][lcopy] = (int)((ad - a0) / sizeof(T));
       }
+      uint32_t total = bytes;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        w[0][d] = w[1][d];
-        w[1][d] = w[2][d];
-      }
+      for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+      const uint32_t fb = smem_addr(&full[st]);
+      __syncwarp();                               // every lane's off[st] before the arrival
+      if (lane == 0) mbar_expect_tx(fb, total);   // releases off[st] to the consumers
+      __syncwarp();
+      if (bytes)
+        bulk_load(smem_addr(buf + ((size_t)(st * RS + lrow) * NCP + lcopy) * SLOT),
+                  (const void *)a0, bytes, fb);
+      issued = g + 1;
     }
+    // let every copy in flight land before the block can leave (the consumers have waited
+    // for all of them on the normal path; after a fault some were never waited for)
+    if (lane == 0)
+      for (int g = issued - NS > 0 ? issued - NS : 0; g < issued; ++g)
+        mbar_wait(smem_addr(&full[g % NS]), (uint32_t)((g / NS) & 1), kWaitLimit);
+    __syncwarp();
+  } else {
+    // scalars of the update formed at each point
+    T s1 = T(0), s2 = T(0);
+    bool first = false;
+    if (KIND == K1) {
+      first = sc->count == 0;
+      s1 = (T)sc->beta;
+      s2 = (T)sc->omega;
+    } else if (KIND == K2) {
+      s1 = (T)sc->alpha;
+    } else if (KIND == K3) {
+      s1 = (T)sc->alpha;
+      s2 = (T)sc->omega;
     }
-    __syncthreads();              // stage st is free again
-    if (t < 32 && g + NS < ngroups) issue(g + NS);
+    auto form = [&](const T (&v)[3]) -> T {
+      if (KIND == KINIT) return v[0];
+      if (KIND == K1) return first ? v[0] : v[2] + s1 * (v[0] - s2 * v[1]);
+      if (KIND == K2) return v[0] - s1 * v[1];
+      return v[0] + s1 * v[1] + s2 * v[2];
+    };
+
+    T w[3][3];
+    RowFactors<T> f;
+    if (active && nrows > 0) {
+#pragma unroll
+      for (int dr = 0; dr < 2; ++dr)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const long long k = (long long)(ja - 1 + dr) * ix + i - 1 + d;
+          T v[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) v[c] = c < NW ? a.w[c][k] : T(0);
+          w[dr][d] = form(v);
+        }
+      f.cxl = a.g[i];
+      f.cxr = a.g[ix + i];
+      f.idx = a.g[2 * ix + i];
+    }
+    const T *gy = a.g + 3 * ix;
+    const int lane = t & 31;
+    for (int g = 0; g < ngroups; ++g) {
+      const int st = g % NS;
+      bool ok = false;
+      for (int k = 0; k < wait_limit && !ok; ++k) {
+        ok = mbar_try_wait(smem_addr(&full[st]), (uint32_t)((g / NS) & 1));
+        if (!ok && s_fault) break;
+      }
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) s_fault = 1;
+        break;
+      }
+#pragma unroll
+      for (int rr = 0; rr < RS; ++rr) {
+        const int r = g * RS + rr, j = ja + r;
+        if (r >= nrows) break;
+        const T *sb = buf + (size_t)(st * RS + rr) * NCP * SLOT;
+        const int *of = off[st][rr];
+        if (active) {
+          const long long q = (long long)j * ix + i;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            T v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] = c < NW ? sb[c * SLOT + of[c] + t + d] : T(0);
+            w[2][d] = form(v);
+          }
+          T own[2];
+#pragma unroll
+          for (int c = 0; c < 2; ++c)
+            own[c] = c < NO ? sb[(NW + c) * SLOT + of[NW + c] + t] : T(0);
+          constexpr int mc = NW + NO;
+          f.eta = sb[mc * SLOT + of[mc] + t];
+          f.fxxl = sb[(mc + 1) * SLOT + of[mc + 1] + t];
+          f.fxxr = sb[(mc + 1) * SLOT + of[mc + 1] + t + 1];
+          f.fxyl = sb[(mc + 2) * SLOT + of[mc + 2] + t];
+          f.fxyr = sb[(mc + 2) * SLOT + of[mc + 2] + t + 1];
+          f.fyyd = sb[(mc + 3) * SLOT + of[mc + 3] + t];
+          f.fyyu = sb[(mc + 4) * SLOT + of[mc + 4] + t];
+          f.fyxd = sb[(mc + 5) * SLOT + of[mc + 5] + t];
+          f.fyxu = sb[(mc + 6) * SLOT + of[mc + 6] + t];
+          f.cyd = gy[j];
+          f.cyu = gy[p.jx + j];
+          f.idy = gy[2 * p.jx + j];
+          T c[9];
+          entries(p, f, i, j, c);
+          if (KIND == KINIT) {
+            // r = b - A x term by term, as the reference's initial residual
+            const T bq = own[0];
+            T v = bq;
+            v = v - c[0] * w[1][1];
+            v = v - c[1] * w[1][0];
+            v = v - c[2] * w[1][2];
+            v = v - c[3] * w[0][1];
+            v = v - c[4] * w[2][1];
+            v = v - c[5] * w[0][0];
+            v = v - c[6] * w[0][2];
+            v = v - c[7] * w[2][0];
+            v = v - c[8] * w[2][2];
+            a.out[0][q] = v;
+            a.out[1][q] = v;
+            a.out[2][q] = v;
+            acc0 += (double)v * (double)v;
+            acc1 += (double)bq * (double)bq;
+          } else if (KIND == K1) {
+            a.out[0][q] = w[1][1];
+            const T av = stencil(c, w);
+            a.out[1][q] = av;
+            const double r0q = (double)own[1];
+            acc0 += (double)own[0] * r0q;
+            acc1 += r0q * (double)av;
+          } else if (KIND == K2) {
+            a.out[0][q] = w[1][1];
+            const T at = stencil(c, w);
+            acc0 += (double)w[1][1] * (double)at;
+            acc1 += (double)at * (double)at;
+          } else {
+            a.out[0][q] = w[1][1];
+            const T v = own[0] - stencil(c, w);
+            a.out[1][q] = v;
+            acc0 += (double)own[1] * (double)v;
+            acc1 += (double)v * (double)v;
+          }
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            w[0][d] = w[1][d];
+            w[1][d] = w[2][d];
+          }
+        }
+      }
+      __syncwarp();                // the warp's reads of stage st are done
+      if (lane == 0) mbar_arrive(smem_addr(&empty[st]));
+    }
   }
-  if (fault) {
-    // a staged group never arrived: flag it, let the copies still in flight land (bounded
-    // by the default limit, whatever the limit of the waits above), and leave the scalars
-    // alone (the host reads the flag and stops; later kernels of the solve return at once)
-    if (t == 0) {
-      atomicExch(&sc->fault, 1);
-      for (int k = g; k < ngroups && k < g + NS; ++k)
-        mbar_wait(smem_addr(&bar[k % NS]), (uint32_t)((k / NS) & 1), kWaitLimit);
-    }
+  __syncthreads();
+  if (s_fault) {
+    // a staged group never arrived (or its stage was never freed): flag it and leave the
+    // scalars alone (the host reads the flag and stops; later kernels return at once)
+    if (t == 0) atomicExch(&sc->fault, 1);
     return;
   }
   double tot[2];
-  if (reduce2<SX>(acc0, acc1, a.part, &sc->blocks_done, tot)) {
+  if (reduce2<kBlock, SX>(acc0, acc1, a.part, &sc->blocks_done, tot)) {
     if (KIND == KINIT) {
       sc->rr = tot[0];
       sc->bb = tot[1];
@@ -700,7 +749,7 @@ cudaError_t kind_blocks(int *bps) {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int n = 0;
   if (err == cudaSuccess)
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bicg_kernel<T, KIND>, SX, smem);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bicg_kernel<T, KIND>, kBlock, smem);
   if (err == cudaSuccess) *bps = std::min(*bps, std::max(n, 1));
   return err;
 }
@@ -725,7 +774,7 @@ template <typename T, int KIND>
 void launch(const Grid &g, const KParams &k, BicgArgs<T> a, cudaStream_t s) {
   a.ncb = g.ncb;
   a.nrb = g.nrb;
-  bicg_kernel<T, KIND><<<g.nb, SX, stage_smem<T, KIND>(), s>>>(k, a);
+  bicg_kernel<T, KIND><<<g.nb, kBlock, stage_smem<T, KIND>(), s>>>(k, a);
 }
 
 template <typename T>
