@@ -436,7 +436,8 @@ constexpr int kConsumerWarps = SX / 32;
 constexpr int kBlock = SX + 32;
 
 template <typename T, int KIND>
-__global__ void __launch_bounds__(kBlock) bicg_kernel(const KParams p, const BicgArgs<T> a) {
+__global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KParams p,
+                                                     const __grid_constant__ BicgArgs<T> a) {
   constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
   constexpr int NCP = n_copies<KIND>();
   constexpr int NS = stages<T>();

@@ -325,6 +325,7 @@ __global__ void __launch_bounds__(128) nlev_update_kernel(const __grid_constant_
     double nx[6], d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int m = 0; m < 6; ++m) nx[m] = p.nl_nex[q + m * nc];
+#pragma unroll
     for (int jj = 0; jj < 5; ++jj)
       d[5] = d[5] + PIP_NL_GT(nx[jj] * nl_cr(p, q, jj, 5)) - PIP_NL_GT(nx[5] * nl_cr(p, q, 5, jj));
 #pragma unroll
@@ -332,6 +333,7 @@ __global__ void __launch_bounds__(128) nlev_update_kernel(const __grid_constant_
       d[ii] = d[ii] + PIP_NL_GT(nx[5] * nl_cr(p, q, 5, ii)) - PIP_NL_GT(nx[ii] * nl_cr(p, q, ii, 5));
 #pragma unroll
     for (int ii = 0; ii < 5; ++ii)
+#pragma unroll
       for (int jj = 0; jj < 5; ++jj)
         d[ii] = d[ii] + PIP_NL_GT(nx[jj] * nl_cr(p, q, jj, ii)) - PIP_NL_GT(nx[ii] * nl_cr(p, q, ii, jj));
     double o[6];
