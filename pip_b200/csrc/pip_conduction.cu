@@ -441,9 +441,6 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
   constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
   constexpr int NCP = n_copies<KIND>();
   constexpr int NS = stages<T>();
-  Scal *sc = a.sc;
-  if (sc->done || sc->fault) return;
-  const int wait_limit = sc->wait_limit;
   extern __shared__ __align__(128) unsigned char smem[];
   T *buf = reinterpret_cast<T *>(smem);
   unsigned long long *full =
@@ -473,6 +470,13 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  // Launched as a programmatic dependent of the solve's previous kernel: everything above
+  // reads only the arguments; the vectors and scalars that kernel wrote are read after it
+  // has completed.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  Scal *sc = a.sc;
+  if (sc->done || sc->fault) return;
+  const int wait_limit = sc->wait_limit;
   __syncthreads();
 
   double acc0 = 0.0, acc1 = 0.0;
@@ -665,6 +669,9 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
       if (lane == 0) mbar_arrive(smem_addr(&empty[st]));
     }
   }
+  // the next kernel of the solve may start its launch (it waits for this one to complete
+  // before it reads anything this one writes)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   __syncthreads();
   if (s_fault) {
     // a staged group never arrived (or its stage was never freed): flag it and leave the
@@ -775,7 +782,18 @@ template <typename T, int KIND>
 void launch(const Grid &g, const KParams &k, BicgArgs<T> a, cudaStream_t s) {
   a.ncb = g.ncb;
   a.nrb = g.nrb;
-  bicg_kernel<T, KIND><<<g.nb, kBlock, stage_smem<T, KIND>(), s>>>(k, a);
+  // programmatic dependent launch: the kernel's set-up overlaps the previous kernel's tail
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)g.nb, 1, 1);
+  cfg.blockDim = dim3(kBlock, 1, 1);
+  cfg.dynamicSmemBytes = stage_smem<T, KIND>();
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, bicg_kernel<T, KIND>, k, a);
 }
 
 template <typename T>
