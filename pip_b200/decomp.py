@@ -132,9 +132,12 @@ def gather(s: Settings, parts: Sequence[np.ndarray]) -> np.ndarray:
 # ---------------------------------------------------------------------- transports
 class TorchComm:
     """Reductions and point-to-point messages between processes through
-    ``torch.distributed`` (NCCL for device buffers, gloo for host buffers)."""
+    ``torch.distributed`` (NCCL for device buffers, gloo for host buffers).  staged: the
+    transport takes host buffers only (gloo) while the blocks' buffers are on the device;
+    each message and reduction then goes through a host copy, ordered after the work
+    queued on the current stream."""
 
-    def __init__(self, device=None, group=None):
+    def __init__(self, device=None, group=None, staged: bool = False):
         import torch
         import torch.distributed as dist
         self.dist = dist
@@ -143,6 +146,7 @@ class TorchComm:
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.device = device if device is not None else "cpu"
+        self.staged = staged
 
     def barrier(self) -> None:
         self.dist.barrier(group=self.group)
@@ -163,8 +167,13 @@ class TorchComm:
         """cfl's MIN/MAX allreduces on device memory: pairs = [(t_min, t_max)] of this
         process's blocks (one), reduced in place over the ranks on the current stream."""
         for t_min, t_max in pairs:
-            self.dist.all_reduce(t_min, op=self.dist.ReduceOp.MIN, group=self.group)
-            self.dist.all_reduce(t_max, op=self.dist.ReduceOp.MAX, group=self.group)
+            for t, op in ((t_min, self.dist.ReduceOp.MIN), (t_max, self.dist.ReduceOp.MAX)):
+                if self.staged and t.is_cuda:
+                    h = t.cpu()                      # after the stream's queued work
+                    self.dist.all_reduce(h, op=op, group=self.group)
+                    t.copy_(h)
+                else:
+                    self.dist.all_reduce(t, op=op, group=self.group)
 
     def exchange(self, sends, recvs) -> None:
         """sends: [(src_rank, dst_rank, tensor)], recvs: [(dst_rank, src_rank, tensor)] for
@@ -172,6 +181,18 @@ class TorchComm:
         receives go out as one batch (one NCCL group), so two ranks that send to each other
         do not wait on each other's receive."""
         P2POp = self.dist.P2POp
+        if self.staged:
+            hs = [(dst, t.cpu() if t.is_cuda else t) for _, dst, t in sends]
+            hr = [(src, t, self.torch.empty_like(t, device="cpu") if t.is_cuda else t)
+                  for _, src, t in recvs]
+            ops = [P2POp(self.dist.irecv, h, src, self.group) for src, _, h in hr]
+            ops += [P2POp(self.dist.isend, h, dst, self.group) for dst, h in hs]
+            for q in self.dist.batch_isend_irecv(ops):
+                q.wait()
+            for _, t, h in hr:
+                if t is not h:
+                    t.copy_(h)
+            return
         ops = [P2POp(self.dist.irecv, t, src, self.group) for _, src, t in recvs]
         ops += [P2POp(self.dist.isend, t, dst, self.group) for _, dst, t in sends]
         # with NCCL the transfer starts after the current stream's work (the packing) and

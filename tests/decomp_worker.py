@@ -59,3 +59,36 @@ def reduce_main(rank, world, port, q):
         dist.destroy_process_group()
     except Exception as e:
         q.put((rank, "error", repr(e), None, None))
+
+
+def device_rank_main(rank, world, port, case, nsteps, device_loop, q):
+    """One rank of a gloo group stepping its block on a GPU context (cuda:0, shared by the
+    ranks: the host sequences each rank's launches and the messages go through host
+    copies, so no kernel waits for another rank)."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    for p in (here, os.path.dirname(here)):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from pip_b200 import decomp
+    from decomp_cases import make_case
+    try:
+        torch.cuda.set_device(0)
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                                world_size=world, timeout=datetime.timedelta(seconds=60))
+        s, Uh, Um = make_case(case)
+        b = decomp.block_of(s, world, rank)
+        eng = decomp.DeviceBlock(b, decomp.scatter(s, Uh, world, rank),
+                                 decomp.scatter(s, Um, world, rank))
+        run = decomp.DecomposedRun([eng], decomp.TorchComm("cpu", staged=True),
+                                   divb=s.divb == 1)
+        st = run.run_device(nsteps) if device_loop else run.run(nsteps)
+        uh, um = eng.download()
+        q.put((rank, st, run.dt_history, uh, um))
+        run.close()
+        dist.destroy_process_group()
+    except Exception as e:   # reported to the parent, which fails the test
+        q.put((rank, "error", repr(e), None, None))
+

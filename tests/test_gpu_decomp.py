@@ -222,3 +222,51 @@ def test_conduction_blocks_match_single_domain(gpu_lib, case, world):
     o.close()
     e2 = max(rel_l1(interior(gh, s), interior(oh, s)).max(), rel_l1(interior(gm, s), interior(om, s)).max())
     assert e2 <= 1e-10, e2
+
+
+def _free_port():
+    import socket
+    with socket.socket() as k:
+        k.bind(("127.0.0.1", 0))
+        return k.getsockname()[1]
+
+
+@pytest.mark.parametrize("case,device_loop", [("ot", False), ("kh", True)])
+def test_two_processes_over_gloo(gpu_lib, case, device_loop):
+    """The transport path of a multi-GPU run with device blocks: two processes in a gloo
+    group, each stepping its block on a GPU context (both on this GPU; the host sequences
+    each process's launches), halos and cfl reductions through torch.distributed with host
+    staging.  Bitwise the single block's result (host-driven) or pip_run's (device loop)."""
+    import multiprocessing as mp
+    import decomp_worker
+    nsteps = 6
+    s, Uh, Um = make_case(case)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=decomp_worker.device_rank_main,
+                         args=(r, 2, port, case, nsteps, device_loop, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        got = sorted((q.get(timeout=240) for _ in procs), key=lambda x: x[0])
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    for rank, st, dts, _, _ in got:
+        assert st == 0, (rank, st, dts)
+    hn = decomp.gather(s, [g[3] for g in got])
+    mn = decomp.gather(s, [g[4] for g in got])
+    if device_loop:
+        with capi.Context(s) as c:
+            c.upload(Uh, Um)
+            st1, t1, n1 = c.run(nsteps=nsteps)
+            rh, rm = c.download()
+        assert st1 == 0 and n1 == nsteps
+    else:
+        st1, dt1, rh, rm = device_run(s, Uh, Um, 1, nsteps)
+        assert st1 == 0 and got[0][2] == dt1 == got[1][2]
+    assert np.array_equal(hn, rh) and np.array_equal(mn, rm)
+
