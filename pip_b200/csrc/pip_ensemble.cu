@@ -27,6 +27,7 @@
 #include "pip_kernels.cuh"
 #include "pip_mixed_cell.cuh"
 #include "pip_mixed_tile.cuh"
+#include "pip_pair.cuh"
 #include "pip_physics.cuh"
 
 namespace pip {
@@ -196,7 +197,7 @@ __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *
         }
         vl[0] = fmaxf(vl[0], rolf);
         vr[0] = fmaxf(vr[0], rolf);
-        hlld_flux_rcp<float, NVM>(vl, vr, fx, gmf, igm1f, 0.0f);
+        pair::hlld_flux(vl, vr, fx, gmf, igm1f);
 #pragma unroll
         for (int n = 0; n < NVM; ++n) sF[n * NT + tid] = fx[n];
       }
@@ -211,7 +212,7 @@ __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *
         }
         vl[0] = fmaxf(vl[0], rolf);
         vr[0] = fmaxf(vr[0], rolf);
-        hllc_flux_rcp<float>(vl, vr, fx, gmf, igm1f);
+        pair::hllc_flux(vl, vr, fx, gmf, igm1f);
 #pragma unroll
         for (int n = 0; n < 5; ++n) sF[(NVM + n) * NT + tid] = fx[n];
       }

@@ -6,6 +6,7 @@
 
 #include "pip_kernels.cuh"
 #include "pip_mixed_cell.cuh"
+#include "pip_pair.cuh"
 #include "pip_physics.cuh"
 
 namespace pip {
@@ -13,7 +14,8 @@ namespace mixed {
 
 // One RK stage on the TX x TY cells from (i0, j0) (the arithmetic is that of run_solver's
 // stage, see the FP64 stage_kernel): FP32 primitives of the tile and its kH-cell halo, FP32
-// face fluxes (HLLD on the ion planes 0-7, HLLC on the neutral ones; with NVM == 9 the
+// face fluxes (HLLD on the ion planes 0-7, HLLC on the neutral ones, each face's left and
+// right work paired in packed FP32x2 arithmetic, pip_pair.cuh; with NVM == 9 the
 // normal-field and psi fluxes in FP64), then per cell the FP64 source and the compensated
 // update into Ohi (and Olo in stage 2) with the ghost images.  Stage 1: Us = U0hi = A.hi;
 // stage 2: Us = U1, U0 = A.hi + A.lo.  staged: sV already holds the raw planes of the tile
@@ -34,7 +36,6 @@ __device__ __forceinline__ void tile_stage(const KParams &p, const float *__rest
   const int tid = threadIdx.x;
   const float gmf = (float)p.gm, rolf = (float)p.ro_lim, prlf = (float)p.pr_lim;
   const float igm1f = (float)p.igm1;
-  const float cmaxf = (float)cmax;
   const long long nc = p.nc;
   if (STAGE == 1) ep = 0;   // stage 1 is never followed by a cfl
 
@@ -117,7 +118,7 @@ __device__ __forceinline__ void tile_stage(const KParams &p, const float *__rest
       }
       vl[0] = fmaxf(vl[0], rolf);
       vr[0] = fmaxf(vr[0], rolf);
-      hlld_flux_rcp<float, 8>(vl, vr, fx, gmf, igm1f, cmaxf);
+      pair::hlld_flux(vl, vr, fx, gmf, igm1f);
 #pragma unroll
       for (int n = 0; n < 8; ++n) {
         if (NVM == 9 && n == 5) continue;
@@ -151,7 +152,7 @@ __device__ __forceinline__ void tile_stage(const KParams &p, const float *__rest
       }
       vl[0] = fmaxf(vl[0], rolf);
       vr[0] = fmaxf(vr[0], rolf);
-      hllc_flux_rcp<float>(vl, vr, fx, gmf, igm1f);
+      pair::hllc_flux(vl, vr, fx, gmf, igm1f);
 #pragma unroll
       for (int n = 0; n < 5; ++n) {
         const int dst = py ? (n == 1 ? 2 : n == 2 ? 1 : n) : n;

@@ -104,3 +104,32 @@ def test_mixed_roundtrip_upload_download(gpu_lib):
         h, m = c.download()
     np.testing.assert_allclose(h, Uh, rtol=1e-13, atol=1e-300)
     np.testing.assert_allclose(m, Um, rtol=1e-13, atol=1e-300)
+
+
+def test_paired_solvers_match_scalar(tmp_path):
+    """The mixed form's FP32 HLLD/HLLC with each face's left and right work in packed FP32x2
+    arithmetic (pip_pair.cuh) against the scalar reciprocal forms, over 2^20 seeded faces per
+    kind, differences relative to the face's flux scale.  Unrelated random states (kind 0,
+    with supersonic faces) carry the FP32 cancellation of the energy flux between branches;
+    nearby states, mirror pairs and near-zero Bn stay at rounding."""
+    import os
+    import re
+    import subprocess
+    from pip_b200 import build as b
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = tmp_path / "pair_flux_check"
+    subprocess.run([b.nvcc()] + b.ARCH + ["-O3", "-std=c++17", "--expt-relaxed-constexpr",
+                    "-ftz=true", "-prec-div=false", "-prec-sqrt=false",
+                    os.path.join(here, "pair_flux_check.cu"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    print(out)
+    kinds = {int(m.group(1)): (float(m.group(2)), float(m.group(3)))
+             for m in re.finditer(r"kind (\d) faces \d+ hlld_max (\S+) hllc_max (\S+)", out)}
+    assert sorted(kinds) == [0, 1, 2, 3]
+    assert max(kinds[0]) <= 1e-3
+    for k in (1, 2, 3):
+        assert max(kinds[k]) <= 1e-5, (k, kinds[k])
+    side = re.search(r"supersonic_left (\d+) supersonic_right (\d+) subsonic (\d+)", out)
+    assert all(int(x) > 0 for x in side.groups())
+    assert re.search(r"nonfinite 0", out)
+
