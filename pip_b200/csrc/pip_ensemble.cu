@@ -27,7 +27,6 @@
 #include "pip_kernels.cuh"
 #include "pip_mixed_cell.cuh"
 #include "pip_mixed_tile.cuh"
-#include "pip_pair.cuh"
 #include "pip_physics.cuh"
 
 namespace pip {
@@ -197,7 +196,7 @@ __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *
         }
         vl[0] = fmaxf(vl[0], rolf);
         vr[0] = fmaxf(vr[0], rolf);
-        pair::hlld_flux(vl, vr, fx, gmf, igm1f);
+        hlld_flux_rcp<float, NVM>(vl, vr, fx, gmf, igm1f, 0.0f);
 #pragma unroll
         for (int n = 0; n < NVM; ++n) sF[n * NT + tid] = fx[n];
       }
@@ -212,7 +211,7 @@ __device__ void run_stage(const KParams &p, const float *Us, float *Ahi, float *
         }
         vl[0] = fmaxf(vl[0], rolf);
         vr[0] = fmaxf(vr[0], rolf);
-        pair::hllc_flux(vl, vr, fx, gmf, igm1f);
+        hllc_flux_rcp<float>(vl, vr, fx, gmf, igm1f);
 #pragma unroll
         for (int n = 0; n < 5; ++n) sF[(NVM + n) * NT + tid] = fx[n];
       }
