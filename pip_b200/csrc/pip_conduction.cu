@@ -77,6 +77,7 @@ struct Scal {
   int count, hc_max, done, fault;
   unsigned int blocks_done;
   int wait_limit;                 // polls of a staging mbarrier before a block gives up
+  unsigned int body;              // k3 launches of the solve's device-side loop
 };
 
 __device__ __forceinline__ bool interior_cell(const KParams &p, long long t, int &i, int &j) {
@@ -401,6 +402,8 @@ struct BicgArgs {
   double *part;
   Scal *sc;
   int ncb, nrb;              // column blocks, row ranges per column block
+  cudaGraphConditionalHandle loop;  // k3 in the device-side loop: its while condition
+  int in_loop;
 };
 
 // Copy c of a row: its source plane, row offset, first column offset (from i0), number of
@@ -475,6 +478,12 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
   // has completed.
   asm volatile("griddepcontrol.wait;" ::: "memory");
   Scal *sc = a.sc;
+  if (KIND == K3 && a.in_loop && blockIdx.x == 0 && t == 0) {
+    // the loop ends once the solve has stopped (converged, out of iterations or faulted);
+    // the count of k3 launches bounds it whatever the scalars say
+    const unsigned int b = ++sc->body;
+    if (sc->done || sc->fault || b > (unsigned int)sc->hc_max + 8u) cudaGraphSetConditional(a.loop, 0u);
+  }
   if (sc->done || sc->fault) return;
   const int wait_limit = sc->wait_limit;
   __syncthreads();
@@ -702,6 +711,7 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
       sc->count = sc->count + 1;
       sc->relres = sqrt(tot[1] / sc->bb);
       sc->done = !(sc->relres > sc->tol && sc->count <= sc->hc_max);
+      if (a.in_loop && sc->done) cudaGraphSetConditional(a.loop, 0u);
     }
   }
 }
@@ -743,6 +753,7 @@ __global__ void set_scal_kernel(Scal *sc, double tol, int hc_max, int wait_limit
   sc->fault = 0;
   sc->count = 0;
   sc->blocks_done = 0u;
+  sc->body = 0u;
 }
 
 // One wave of BiCGstab blocks: ncb column blocks x nrb row ranges.
@@ -833,6 +844,11 @@ struct HcEngine {
   // distributed solve (hcd_*): per-block partial sums on the device and their pinned copy
   double *dpart = nullptr, *h_dpart = nullptr;
   int dnb = 0;
+  // the BiCGstab iterations as a device-side loop (a conditional while node over two
+  // iterations, k3 ending it), FP64 [0] and FP32 [1]; built at the first solve; a device
+  // that cannot build it runs the host-checked groups instead
+  cudaGraphExec_t loop[2] = {nullptr, nullptr};
+  bool no_loop[2] = {false, false};
 };
 
 void hc_set_wait_limit(HcEngine *e, int polls) {
@@ -847,6 +863,8 @@ void hc_destroy(HcEngine *e) {
                   e->ap32[1], e->part, e->sc, e->sc32};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  for (cudaGraphExec_t g : e->loop)
+    if (g) cudaGraphExecDestroy(g);
   if (e->dpart) cudaFree(e->dpart);
   if (e->h_dpart) cudaFreeHost(e->h_dpart);
   if (e->h_sc) cudaFreeHost(e->h_sc);
@@ -911,9 +929,56 @@ cudaError_t hc_create(const KParams &k, bool mixed, HcEngine **out) {
 
 namespace {
 
-// BiCGstab on the interior cells from x[0] until the stop flag of sc is set; the host reads
-// the flag every `group` iterations.  On return h holds the scalars; the iterate is in
-// x[h->count & 1].
+// Two BiCGstab iterations (the double-buffered vectors' two parities) into the body of a
+// conditional while node; k3 of the loop ends it (sets the condition to 0) once the solve has
+// stopped.  The arguments (the engine's buffers and scalars) are fixed, so the loop graph is
+// built once per precision.
+template <typename T>
+cudaError_t build_loop(const hc::Grid &gr, const KParams &k, const T *m, const T *g,
+                       T *const (&x)[2], const T *b, T *r, T *r0, T *const (&pv)[2],
+                       T *const (&ap)[2], T *tv, double *part, hc::Scal *sc, cudaStream_t s,
+                       cudaGraphExec_t *out) {
+  using namespace hc;
+  cudaGraph_t graph = nullptr;
+  cudaError_t err = cudaGraphCreate(&graph, 0);
+  if (err != cudaSuccess) return err;
+  cudaGraphConditionalHandle cond;
+  err = cudaGraphConditionalHandleCreate(&cond, graph, 1u, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (err == cudaSuccess) err = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  if (err == cudaSuccess)
+    err = cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return err;
+  }
+  for (int a = 0; a < 2; ++a) {
+    const int z = a ^ 1;
+    launch<T, K1>(gr, k, make_args<T>(m, g, {pv[a], ap[a], r}, {r, r0}, {pv[z], ap[z]}, part, sc), s);
+    launch<T, K2>(gr, k, make_args<T>(m, g, {r, ap[z]}, {}, {tv}, part, sc), s);
+    BicgArgs<T> a3 = make_args<T>(m, g, {x[a], pv[z], tv}, {b, r0}, {x[z], r}, part, sc);
+    a3.loop = cond;
+    a3.in_loop = 1;
+    launch<T, K3>(gr, k, a3, s);
+  }
+  cudaGraph_t captured = nullptr;
+  err = cudaStreamEndCapture(s, &captured);
+  if (err == cudaSuccess) err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  return err;
+}
+
+// BiCGstab on the interior cells from x[0] until the stop flag of sc is set: the iterations
+// run as the device-side loop (one host wait per solve), or, where that loop cannot be built,
+// in groups after which the host reads the flag.  On return h holds the scalars; the iterate
+// is in x[h->count & 1].
 template <typename T>
 cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T *m, const T *g,
                      T *const (&x)[2], const T *b, T *r, T *r0, T *const (&pv)[2],
@@ -922,6 +987,23 @@ cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T 
   using namespace hc;
   set_scal_kernel<<<1, 1, 0, s>>>(sc, tol, hc_max, e->wait_limit);
   launch<T, KINIT>(gr, k, make_args<T>(m, g, {x[0]}, {b}, {r, r0, pv[0]}, e->part, sc), s);
+  const int li = sizeof(T) == 8 ? 0 : 1;
+  if (!e->loop[li] && !e->no_loop[li]) {
+    if (build_loop<T>(gr, k, m, g, x, b, r, r0, pv, ap, tv, e->part, sc, s, &e->loop[li]) !=
+        cudaSuccess) {
+      cudaGetLastError();           // (a failed build leaves no error behind)
+      e->loop[li] = nullptr;
+      e->no_loop[li] = true;
+    }
+  }
+  if (e->loop[li]) {
+    cudaError_t err = cudaGraphLaunch(e->loop[li], s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(h, sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return err;
+    if (h->fault) return cudaErrorLaunchTimeout;
+    return cudaSuccess;
+  }
   const int group = 4;
   for (int it = 0; it <= hc_max; it += group) {
     for (int u = 0; u < group; ++u) {
