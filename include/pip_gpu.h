@@ -298,6 +298,15 @@ int pip_conduction(pip_ctx *ctx, double dt, int *iters, double *relres);
  * flag_heat = 1. */
 int pip_set_hc_wait_limit(pip_ctx *ctx, int polls);
 
+/* Diagnostic; no counterpart in the reference.  How a BiCGstab solve schedules its
+ * iterations: device_loop = 1 (the default) as one device-side loop (a CUDA graph whose
+ * conditional while node runs the iterations until the last kernel of an iteration ends it:
+ * one host wait per solve; a device or stream that cannot build that graph falls back to
+ * 0), 0 in groups of four after each of which the host reads the stop flag.  Both run the
+ * same kernels on the same buffers, so the results and iteration counts are identical.
+ * PIP_ERR_PARAM without flag_heat = 1 or for another value. */
+int pip_set_hc_loop(pip_ctx *ctx, int device_loop);
+
 /*
  * Implicit conduction of a decomposed run: BiCGstabMPI (HC_rot.f90:303-466) for a block
  * whose y faces border other ranks (pip_set_neighbors; x faces stay physical), driven by

@@ -37,7 +37,8 @@ EXPORTS = (
     "pip_halo_unpack", "pip_ctx_stream", "pip_set_cmax_scale", "pip_dev_begin", "pip_dev_stage",
     "pip_dev_stage_split", "pip_set_halo_stream",
     "pip_dev_candidates", "pip_dev_poll", "pip_coefficients", "pip_get_alpha_c",
-    "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_resi_dt",
+    "pip_set_alpha_c", "pip_set_resistivity", "pip_set_hc_wait_limit", "pip_set_hc_loop",
+    "pip_resi_dt",
     "pip_colexp_table", "pip_set_nlevel", "pip_set_nexcite", "pip_get_nexcite",
     "pip_get_colrat", "pip_get_ion_pot", "pip_nlevel_gm_rec_ref", "pip_get_ir_rates",
     "pip_hcd_begin", "pip_hcd_phase", "pip_hcd_row_bytes", "pip_hcd_pack", "pip_hcd_unpack",
@@ -103,6 +104,7 @@ def lib(path: Optional[str] = None):
     L.pip_status.argtypes = [vp, P(i), P(i)]
     L.pip_conduction.argtypes = [vp, d, P(i), dp]
     L.pip_set_hc_wait_limit.argtypes = [vp, i]
+    L.pip_set_hc_loop.argtypes = [vp, i]
     L.pip_step_noalloc.argtypes = [P(PipParams), vp, d, d, vp]
     L.pip_set_neighbors.argtypes = [vp, P(i)]
     L.pip_stage.argtypes = [vp, i, d, d]
@@ -309,6 +311,11 @@ class Context:
     def set_hc_wait_limit(self, polls: int) -> None:
         """Polls of the BiCGstab staging waits from the next solve on (< 0: the default)."""
         _check(lib().pip_set_hc_wait_limit(self.h, int(polls)), "pip_set_hc_wait_limit")
+
+    def set_hc_loop(self, device_loop: bool) -> None:
+        """BiCGstab iterations as one device-side loop (True, the default) or in host-checked
+        groups (False)."""
+        _check(lib().pip_set_hc_loop(self.h, 1 if device_loop else 0), "pip_set_hc_loop")
 
     @property
     def conduction_iterations(self) -> int:

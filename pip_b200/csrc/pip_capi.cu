@@ -1202,6 +1202,13 @@ int pip_set_hc_wait_limit(pip_ctx *c, int polls) {
   return PIP_OK;
 }
 
+int pip_set_hc_loop(pip_ctx *c, int device_loop) {
+  if (!c) return PIP_ERR_NULL;
+  if (!c->hc || (device_loop != 0 && device_loop != 1)) return PIP_ERR_PARAM;
+  pip::hc_set_loop(c->hc, device_loop);
+  return PIP_OK;
+}
+
 int pip_set_neighbors(pip_ctx *c, const int neighbor[4]) {
   if (!c || !neighbor) return PIP_ERR_NULL;
   bool any = false;

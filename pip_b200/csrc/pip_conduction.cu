@@ -849,10 +849,15 @@ struct HcEngine {
   // that cannot build it runs the host-checked groups instead
   cudaGraphExec_t loop[2] = {nullptr, nullptr};
   bool no_loop[2] = {false, false};
+  bool host_groups = false;         // hc_set_loop(e, 0): the host-checked groups regardless
 };
 
 void hc_set_wait_limit(HcEngine *e, int polls) {
   if (e) e->wait_limit = polls < 0 ? hc::kWaitLimit : polls;
+}
+
+void hc_set_loop(HcEngine *e, int device_loop) {
+  if (e) e->host_groups = device_loop == 0;
 }
 
 void hc_destroy(HcEngine *e) {
@@ -988,7 +993,7 @@ cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T 
   set_scal_kernel<<<1, 1, 0, s>>>(sc, tol, hc_max, e->wait_limit);
   launch<T, KINIT>(gr, k, make_args<T>(m, g, {x[0]}, {b}, {r, r0, pv[0]}, e->part, sc), s);
   const int li = sizeof(T) == 8 ? 0 : 1;
-  if (!e->loop[li] && !e->no_loop[li]) {
+  if (!e->host_groups && !e->loop[li] && !e->no_loop[li]) {
     if (build_loop<T>(gr, k, m, g, x, b, r, r0, pv, ap, tv, e->part, sc, s, &e->loop[li]) !=
         cudaSuccess) {
       cudaGetLastError();           // (a failed build leaves no error behind)
@@ -996,7 +1001,7 @@ cudaError_t bicgstab(HcEngine *e, const hc::Grid &gr, const KParams &k, const T 
       e->no_loop[li] = true;
     }
   }
-  if (e->loop[li]) {
+  if (!e->host_groups && e->loop[li]) {
     cudaError_t err = cudaGraphLaunch(e->loop[li], s);
     if (err == cudaSuccess) err = cudaMemcpyAsync(h, sc, sizeof(Scal), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);

@@ -156,6 +156,7 @@ void hc_destroy(HcEngine *e);
 // Polls of a staging mbarrier before a BiCGstab block gives up and flags the solve as
 // failed (polls < 0: the default); applies from the next solve.
 void hc_set_wait_limit(HcEngine *e, int polls);
+void hc_set_loop(HcEngine *e, int device_loop);
 // Distributed BiCGstab (BiCGstabMPI) in phases, for a block with neighbouring ranks across
 // y faces: hcd_begin sets up te, the matrix (folded on the physical faces only) and the
 // residual of the state U (ghost rows holding the neighbours' rows) and returns the local

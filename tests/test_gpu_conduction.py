@@ -170,3 +170,40 @@ def test_expired_staging_wait_is_reported_and_the_context_recovers(gpu_lib, prec
         gh, gm = c.download()
     assert again == ref and ref[0] == 0
     assert np.array_equal(gh, rh) and np.array_equal(gm, rm)
+
+
+@pytest.mark.parametrize("precision", [PIP_FP64, PIP_MIXED])
+def test_device_loop_and_host_checked_groups_agree(gpu_lib, precision):
+    """The BiCGstab iterations as one device-side loop (a conditional while node that the
+    last kernel of an iteration ends) and in host-checked groups of four run the same
+    kernels on the same buffers: identical iterates, counts and residuals, over several
+    solves in a row, and the groups report an expired staging wait the same way."""
+    import ctypes
+    s, o, Uh0, Um0 = kh_case(kapper=1.0)
+    dt, _ = o.cfl()
+    h0, m0 = o.state()
+    o.close()
+    s = s.overrides(precision=precision)
+    out = {}
+    for loop in (True, False):
+        with capi.Context(s) as c:
+            c.set_hc_loop(loop)
+            c.upload(h0, m0)
+            res = [c.conduction(dt) for _ in range(3)]
+            c.pipbnd()
+            out[loop] = (res, c.download())
+    (ra, (ah, am)), (rb, (bh, bm)) = out[True], out[False]
+    assert ra == rb and all(r[0] == 0 and r[1] > 0 for r in ra)
+    assert np.array_equal(ah, bh) and np.array_equal(am, bm)
+    L = capi.lib()
+    with capi.Context(s) as c:
+        c.set_hc_loop(False)
+        c.set_hc_wait_limit(0)
+        c.upload(h0, m0)
+        st = L.pip_conduction(c.h, float(dt), ctypes.byref(ctypes.c_int()),
+                              ctypes.byref(ctypes.c_double()))
+        assert st == capi.PIP_ERR_CUDA and L.pip_last_cuda_error() == 702
+        assert L.pip_set_hc_loop(c.h, 2) == capi.PIP_ERR_PARAM
+    plain, _, _ = ics.orszag_tang(16)
+    with capi.Context(plain) as c:
+        assert L.pip_set_hc_loop(c.h, 1) == capi.PIP_ERR_PARAM
