@@ -48,22 +48,30 @@ namespace hc {
 
 constexpr int NT = 256;             // one-thread-per-cell kernels
 constexpr int SX = 128;             // BiCGstab kernels: interior columns (threads) per block
-// Pipeline of the BiCGstab kernels: NS stages of RS rows each (compile-time tuning; the
-// FP32 kernels stage half the bytes per row and may keep more groups in flight).
+// Pipeline of the BiCGstab kernels: NS stages of RS rows each, per precision (compile-time
+// tuning, measured on KH 2048x1024: FP64 4 stages of 1 row, 122 us per iteration against
+// 125 with 2 of 2; FP32 2 stages of 2 rows, 120 us against 123 with 4 of 1).
 #ifndef PIP_HC_STAGES
-#define PIP_HC_STAGES 2
-#endif
-#ifndef PIP_HC_STAGES32
-#define PIP_HC_STAGES32 PIP_HC_STAGES
+#define PIP_HC_STAGES 4
 #endif
 #ifndef PIP_HC_ROWS
-#define PIP_HC_ROWS 2
+#define PIP_HC_ROWS 1
+#endif
+#ifndef PIP_HC_STAGES32
+#define PIP_HC_STAGES32 2
+#endif
+#ifndef PIP_HC_ROWS32
+#define PIP_HC_ROWS32 2
 #endif
 template <typename T>
 __host__ __device__ constexpr int stages() {
   return sizeof(T) == 4 ? PIP_HC_STAGES32 : PIP_HC_STAGES;
 }
-constexpr int RS = PIP_HC_ROWS;     // rows per stage: one wait and one block barrier per group
+// rows per stage: one wait per group
+template <typename T>
+__host__ __device__ constexpr int rows() {
+  return sizeof(T) == 4 ? PIP_HC_ROWS32 : PIP_HC_ROWS;
+}
 constexpr int SLOT = 136;           // elements per staged row segment (SX + 2 + alignment)
 constexpr int kWaitLimit = 1 << 22; // polls of an mbarrier before a block gives up
 constexpr double kEpsi = 1.0e-5;    // HC_rot.f90:17
@@ -389,7 +397,7 @@ __host__ __device__ constexpr int n_copies() {
 
 template <typename T, int KIND>
 __host__ __device__ constexpr size_t stage_smem() {
-  return (size_t)stages<T>() * RS * n_copies<KIND>() * SLOT * sizeof(T) +
+  return (size_t)stages<T>() * rows<T>() * n_copies<KIND>() * SLOT * sizeof(T) +
          2 * stages<T>() * sizeof(unsigned long long);
 }
 
@@ -443,7 +451,7 @@ __global__ void __launch_bounds__(kBlock) bicg_kernel(const __grid_constant__ KP
                                                      const __grid_constant__ BicgArgs<T> a) {
   constexpr int NW = KindShape<KIND>::nw, NO = KindShape<KIND>::no;
   constexpr int NCP = n_copies<KIND>();
-  constexpr int NS = stages<T>();
+  constexpr int NS = stages<T>(), RS = rows<T>();
   extern __shared__ __align__(128) unsigned char smem[];
   T *buf = reinterpret_cast<T *>(smem);
   unsigned long long *full =
