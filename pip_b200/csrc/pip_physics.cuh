@@ -36,6 +36,28 @@ template <> PIP_HD float rmax<float>(float a, float b) { return std::fmax(a, b);
 template <> PIP_HD float rmin<float>(float a, float b) { return std::fmin(a, b); }
 PIP_HD double rsqrt_(double a) { return std::sqrt(a); }
 PIP_HD float rsqrt_(float a) { return std::sqrt(a); }
+// Reciprocal of the folded-division (rcp) forms below.  FP64 on the device: the hardware's
+// approximate reciprocal (PTX rcp.approx.ftz.f64) refined by two Newton-Raphson steps,
+// r <- r + r (1 - x r), each an error-compensated pair of FMAs, which take the seed's
+// relative error e to about e^2 and then to the FP64 rounding level: within 1 ulp of the
+// correctly rounded 1/x for normal x whose reciprocal is normal (tests/rcp_check.cu checks
+// it against the IEEE division), inline and without branches.  Subnormal x or 1/x
+// flush to zero and x = 0 gives NaN, outside the physical range of the denominators it
+// serves (densities, wave-speed differences, the HLLD star denominators behind the HLLC-G
+// guard).  FP32 and the host: the plain quotient.
+PIP_HD double rcp_(double x) {
+#if defined(__CUDA_ARCH__)
+  double r, e;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+#else
+  return 1.0 / x;
+#endif
+}
+PIP_HD float rcp_(float x) { return 1.0f / x; }
 PIP_HD double rabs(double a) { return std::fabs(a); }
 PIP_HD float rabs(float a) { return std::fabs(a); }
 PIP_HD double rsign1(double b) { return std::copysign(1.0, b); }
@@ -124,7 +146,7 @@ template <typename R, int NVM>
 PIP_HD Prim<R> cq2pv_mhd_rcp(R (&u)[NVM], R gm, R igm1, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
-  const R inv = R(1) / de;
+  const R inv = rcp_(de);
   R vx = u[1] * inv, vy = u[2] * inv, vz = u[3] * inv;
   const R kin = vx * vx + vy * vy + vz * vz;
   const R bb = u[5] * u[5] + u[6] * u[6] + u[7] * u[7];
@@ -143,7 +165,7 @@ template <typename R>
 PIP_HD Prim<R> cq2pv_hd_rcp(R (&u)[5], R gm, R igm1, R ro_lim, R pr_lim) {
   Prim<R> q;
   R de = u[0];
-  const R inv = R(1) / de;
+  const R inv = rcp_(de);
   R vx = u[1] * inv, vy = u[2] * inv, vz = u[3] * inv;
   const R kin = vx * vx + vy * vy + vz * vz;
   R pr = (gm - R(1)) * (u[4] - R(0.5) * de * kin);
@@ -504,7 +526,7 @@ PIP_HD void hllc_flux_rcp(const R (&v_l)[5], const R (&v_r)[5], R (&flx)[5], R g
   const R ql = u_l[0] * (sl - vn_l), qr = u_r[0] * (sr - vn_r);
   const R sm = (mul_rn(u_r[1], sr - vn_r) - mul_rn(u_l[1], sl - vn_l) + pr_l - pr_r) / (qr - ql);
   const R pr_m = sm * ql - u_l[1] * (sl - vn_l) + pr_l;
-  const R il = R(1) / (sl - sm), ir = R(1) / (sr - sm);
+  const R il = rcp_(sl - sm), ir = rcp_(sr - sm);
   stl[0] = ql * il;
   str[0] = qr * ir;
   stl[1] = stl[0] * sm;
@@ -578,14 +600,14 @@ PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM
 #pragma unroll
     for (int n = 0; n < 8; ++n) out[n] = fr[n];
   } else {
-    f1 = R(1) / (sr - sl);
+    f1 = rcp_(sr - sl);
     R uh[8];
 #pragma unroll
     for (int n = 0; n < 8; ++n) uh[n] = f1 * (mul_rn(sr, u_r[n]) - mul_rn(sl, u_l[n]) - fr[n] + fl[n]);
-    const R iuh0 = R(1) / uh[0];
+    const R iuh0 = rcp_(uh[0]);
     const R sm = uh[1] * iuh0;
     const R pt = pt_l + v_l[0] * (sl - v_l[1]) * (sm - v_l[1]);
-    const R ilm = R(1) / (sl - sm), irm = R(1) / (sr - sm);
+    const R ilm = rcp_(sl - sm), irm = rcp_(sr - sm);
     const R ro_l1 = v_l[0] * (sl - v_l[1]) * ilm;
     const R ro_r1 = v_r[0] * (sr - v_r[1]) * irm;
     const R rs_l = rrsqrt(ro_l1), rs_r = rrsqrt(ro_r1);
@@ -620,7 +642,7 @@ PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM
     } else {
       R ul1[8], ur1[8];
       const R dl = v_l[0] * (sl - v_l[1]);
-      f1 = R(1) / (dl * (sl - sm) - bn2);
+      f1 = rcp_(dl * (sl - sm) - bn2);
       const R gl = f1 * (dl * (sl - v_l[1]) - bn2);
       ul1[5] = bn;
       ul1[6] = v_l[6] * gl;
@@ -635,7 +657,7 @@ PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM
       ul1[3] = ro_l1 * vz_l1;
 
       const R dr = v_r[0] * (sr - v_r[1]);
-      f1 = R(1) / (dr * (sr - sm) - bn2);
+      f1 = rcp_(dr * (sr - sm) - bn2);
       const R gr = f1 * (dr * (sr - v_r[1]) - bn2);
       ur1[5] = bn;
       ur1[6] = v_r[6] * gr;
@@ -666,7 +688,7 @@ PIP_HD void hlld_flux_rcp(const R (&v_l)[NVM], const R (&v_r)[NVM], R (&flx)[NVM
       } else {
         const R ro_ls = ro_l1 * rs_l;   // sqrt(ro_l1)
         const R ro_rs = ro_r1 * rs_r;
-        f1 = R(1) / (ro_ls + ro_rs);
+        f1 = rcp_(ro_ls + ro_rs);
         const R f2 = rsign1(bn);
         const R vy_2 = f1 * (ro_ls * vy_l1 + ro_rs * vy_r1 + (ur1[6] - ul1[6]) * f2);
         const R vz_2 = f1 * (ro_ls * vz_l1 + ro_rs * vz_r1 + (ur1[7] - ul1[7]) * f2);

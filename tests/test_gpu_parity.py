@@ -258,3 +258,22 @@ def test_run_respects_t_end_and_resumes(gpu_lib):
     assert t2 == o[1]
     np.testing.assert_array_equal(a[0], o[3])
     np.testing.assert_array_equal(a[1], o[4])
+
+
+def test_newton_reciprocal_within_one_ulp(tmp_path):
+    """The FP64 reciprocal of the folded-division solver forms (pip_physics.cuh rcp_: the
+    hardware seed and two Newton-Raphson steps) stays within one ulp of the IEEE division
+    over 2^22 seeded normal values of every exponent and both signs."""
+    import os
+    import re
+    import subprocess
+    from pip_b200 import build as b
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = tmp_path / "rcp_check"
+    subprocess.run([b.nvcc()] + b.ARCH + ["-O3", "-std=c++17", "--expt-relaxed-constexpr",
+                    os.path.join(here, "rcp_check.cu"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    print(out)
+    m = re.search(r"values (\d+) max_ulp (\d+) differ (\d+) nonfinite (\d+)", out)
+    assert m and int(m.group(1)) == 1 << 22
+    assert int(m.group(2)) <= 1 and int(m.group(4)) == 0
