@@ -72,9 +72,9 @@ FP64_BYTES_PER_CELL_STAGE2 = 3 * 14 * 8
 MIXED_BYTES_PER_CELL_STEP = 14 * (8 + 20)
 MIXED_BYTES_PER_CELL_STAGE2 = 14 * 20
 # FP64 pipe busy time per step of the FP64 stage kernels on OT 1024^2, from an ncu --set full
-# capture of both kernels (pipe-active fraction x duration, stage 1 0.4188 x 278.5 us +
-# stage 2 0.3919 x 303.3 us): the compute floor of the FP64 path
-FP64_PIPE_US_PER_STEP = 0.4188 * 278.5 + 0.3919 * 303.3
+# capture of both kernels (pipe-active fraction x duration, stage 1 0.4500 x 254.5 us +
+# stage 2 0.4217 x 278.5 us): the compute floor of the FP64 path
+FP64_PIPE_US_PER_STEP = 0.4500 * 254.5 + 0.4217 * 278.5
 L1_NAMES = ["ro_n", "mx_n", "my_n", "mz_n", "en_n", "ro_p", "mx_p", "my_p", "mz_p", "en_p",
             "bx", "by", "bz", "ps"]
 
